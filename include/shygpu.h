@@ -1,0 +1,225 @@
+/*
+ * shygpu.h -- C ABI of the B200 implementation of SHYFEM's semi-implicit
+ * time step (zeta assembly + sparse Krylov solve + vertical momentum column
+ * solve + 3D scalar transport).
+ *
+ * Two families of entry points:
+ *
+ *  1. The reference's own linear-system ("simsys") interface, with gfortran's
+ *     by-reference calling convention and trailing-underscore names, so that
+ *     SHYFEM's `hydro_zeta`/`hydro` link against this library instead of
+ *     src/shyfem/simsys_spkaux.f90.  The element data that the reference
+ *     passes through module globals (`mod_zeta_system :: kn(3), hia(3,3),
+ *     hik(3)`, simsys_spkaux.f90:75-83) travels through the C-visible
+ *     struct `shy_zeta_system` below, which a Fortran `bind(C)` interface
+ *     names directly.
+ *
+ *  2. Whole-phase entries that keep every basin's state resident in device
+ *     memory and advance whole time steps (`shyfem_run`'s loop body,
+ *     src/shyfem/shyfem_subs.f90:569-658) for one or many basins per launch.
+ *
+ * All arrays use the reference's Fortran column-major layouts: `(nlv,nel)`
+ * is `a[ie*nlv + l]`, `(3,nel)` is `a[ie*3 + ii]`, `(0:nlv,nkn)` is
+ * `a[k*(nlv+1) + l]`.  Node and element numbers are 1-based.  Every function
+ * returns 0 on success and a SHY_E* code otherwise; `shygpu_last_error()`
+ * gives the message.  The library has no CPU fallback: without a usable
+ * CUDA device every compute entry returns SHY_ECUDA.
+ */
+#ifndef SHYGPU_H
+#define SHYGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHY_EVDIM 19          /* entries of ev(evdim,nel), evgeom.f90:300-318 */
+#define SHY_MAX_LAYERS 32     /* layers per column held by one warp segment  */
+#define SHY_MAX_TIDE 4        /* harmonic constituents per level boundary    */
+#define SHY_MAX_CONZ 8        /* passive tracers per basin                   */
+
+enum shy_status {
+  SHY_OK = 0,
+  SHY_EARG = 1,       /* bad argument or size                            */
+  SHY_ECUDA = 2,      /* CUDA runtime error / no device                  */
+  SHY_ENOCONV = 3,    /* Krylov solve did not reach its tolerance        */
+  SHY_ESINGULAR = 4,  /* zero pivot in a column or node solve            */
+  SHY_EDEPTH = 5,     /* non-positive layer thickness                    */
+  SHY_EISTOT = 6,     /* transport sub-step count above the limit        */
+  SHY_ENAN = 7,       /* non-finite value in the state                   */
+  SHY_ESTATE = 8,     /* call out of order (e.g. solve before initialize)*/
+  SHY_ECAPACITY = 9   /* request does not fit the device memory budget   */
+};
+
+/* ------------------------------------------------------------------ */
+/* Static description of one basin (host pointers, copied at create)   */
+/* ------------------------------------------------------------------ */
+typedef struct shy_basin {
+  int32_t nkn, nel, nlv;        /* nodes, elements, layers (nlvdi == nlv)   */
+  const int32_t *nen3v;         /* (3,nel) 1-based           basin::nen3v  */
+  const float *xgv, *ygv;       /* (nkn) cartesian [m]       basin::xgv    */
+  const float *hm3v;            /* (3,nel) depth at vertices basin::hm3v   */
+  const float *hlv;             /* (nlv) bottom depth of z-layer l  levels  */
+  const float *hldv;            /* (nlv) nominal layer thickness    levels  */
+  const int32_t *ilhv;          /* (nel) layers in element          levels  */
+  const int32_t *ilhkv;         /* (nkn) layers at node             levels  */
+  const float *czv;             /* (nel) friction parameter  (chezy.f90)    */
+  const float *fcorv;           /* (nel) Coriolis parameter [1/s]           */
+  const float *visv;            /* (0:nlv,nkn) vertical viscosity           */
+  const float *difv;            /* (0:nlv,nkn) vertical diffusivity         */
+  const float *tauxnv, *tauynv; /* (nkn) wind stress / rho0  (mod_meteo)    */
+  const float *ppv;             /* (nkn) atmospheric pressure term          */
+  const float *rqv;             /* (nkn) flux boundary values (system_add_rhs) */
+  const int32_t *bnd_index;     /* (nkn) 0 or the level-boundary number b>0 */
+  int32_t nbnd, ntide;          /* level boundaries, constituents each      */
+  const float *tide;            /* (4,ntide,nbnd): ampli, period, phase, zref
+                                   (bnd_admin.f90:1304-1320, summed)        */
+} shy_basin;
+
+/* Parameters under their `.str` names (src/shyfem/def_para.f90).          */
+typedef struct shy_params {
+  double dt;                 /* time step [s]                               */
+  double dtime0;             /* time of the initial state [s]               */
+  float azpar, ampar, afpar; /* semi-implicit weights        :666-668       */
+  float atpar, adpar, aapar; /* vertical implicit weights    :684-686       */
+  float grav, rowass;        /*                              :782-784       */
+  float vismol, difmol;      /* molecular viscosity/diffusivity :993-995    */
+  float hzoff;               /* minimum depth for friction   :745           */
+  float ahpar;               /* horizontal viscosity         :1023          */
+  float rstol;               /* transport Courant limit      :1055          */
+  float thpar, shpar, chpar; /* horizontal diffusivity T, S, tracers        */
+  int32_t ireib;             /* friction type                :766           */
+  int32_t ibarcl;            /* baroclinic pressure (1) or not (0)          */
+  int32_t ilin;              /* 1: linear momentum (no advective terms)     */
+  int32_t itemp, isalt;      /* transport temperature / salinity            */
+  int32_t nconz;             /* passive tracers                             */
+  int32_t istot_max;         /* transport sub-step limit (scal3sh: 1000)    */
+  float solver_rtol;         /* Krylov stop ||r|| <= rtol*||r0|| + atol     */
+  float solver_atol;         /*   (sparskit_admin.f90:270-277: 1e-8, 1e-8)  */
+  int32_t solver_maxit;      /* iteration limit (sparskit_admin.f90:141)    */
+} shy_params;
+
+/* Host views of one basin's state, reference layouts.  NULL members are
+ * skipped by set/get.                                                      */
+typedef struct shy_state {
+  float *znv;      /* (nkn) water level                         mod_hydro    */
+  float *zenv;     /* (3,nel) water level at element vertices   mod_hydro    */
+  float *utlnv;    /* (nlv,nel) transport in x                  mod_hydro    */
+  float *vtlnv;    /* (nlv,nel) transport in y                  mod_hydro    */
+  float *unv;      /* (nel) barotropic transport in x       mod_hydro_baro   */
+  float *vnv;      /* (nel) barotropic transport in y                        */
+  float *hdknv;    /* (nlv,nkn) layer thickness at nodes  mod_layer_thickness*/
+  float *hdenv;    /* (nlv,nel) layer thickness at elements                  */
+  float *wlnv;     /* (0:nlv,nkn) vertical velocity             mod_hydro_vel*/
+  float *tempv;    /* (nlv,nkn) temperature                     mod_ts       */
+  float *saltv;    /* (nlv,nkn) salinity                        mod_ts       */
+  float *rhov;     /* (nlv,nkn) density anomaly rho'            mod_ts       */
+  float *conzv;    /* (nlv,nkn,nconz) passive tracers                        */
+} shy_state;
+
+/* Per-step diagnostics of one basin (last completed step).               */
+typedef struct shy_step_info {
+  int32_t status;        /* SHY_OK or the first error of the step          */
+  int32_t krylov_iters;  /* inner Krylov iterations of the zeta solve      */
+  int32_t refinements;   /* FP64 residual refinement sweeps                */
+  int32_t istot;         /* transport sub-steps of the last scalar pass    */
+  double resid0;         /* ||b - A z_guess|| (FP64)                       */
+  double resid;          /* final ||b - A z|| (FP64)                       */
+  double volume;         /* total water volume, FP64 sum (vol_mass)        */
+  double dtime;          /* model time of the state [s]                    */
+} shy_step_info;
+
+typedef struct shygpu_model shygpu_model;   /* opaque, device-resident    */
+
+/* ------------------------------------------------------------------ */
+/* Geometry (init only)                                                */
+/* ------------------------------------------------------------------ */
+
+/* set_ev (src/utils/shyutil/evgeom.f90:167-320): shape-function gradients
+ * b = ev(4:6), c = ev(7:9), aj = area/24 = ev(10), angles, heights and side
+ * lengths for each element, cartesian coordinates.  ev is (SHY_EVDIM,nel). */
+int shygpu_set_ev(int32_t nkn, int32_t nel, const int32_t *nen3v,
+                  const float *xgv, const float *ygv, float *ev);
+
+/* ------------------------------------------------------------------ */
+/* Whole-phase, device-resident entries                                */
+/* ------------------------------------------------------------------ */
+
+/* shyfem_initialize's part for the step (shyfem_subs.f90:358-506): geometry,
+ * areas (set_area), diffusion weights (diffweight), element neighbours, the
+ * zeta-system sparsity (coo_init_new) and its gather maps, for `nbasin`
+ * independent basins advanced together.  params has one entry per basin.  */
+int shygpu_create(int32_t nbasin, const shy_basin *basins,
+                  const shy_params *params, shygpu_model **model);
+int shygpu_destroy(shygpu_model *model);
+
+/* Upload a basin's state (znv, utlnv, vtlnv, tempv, saltv, conzv are read;
+ * zenv, layer thicknesses and rhov are derived as sp111(1)/barocl(0) do).  */
+int shygpu_set_state(shygpu_model *model, int32_t ibasin, const shy_state *st);
+/* Download any subset of a basin's state.                                 */
+int shygpu_get_state(shygpu_model *model, int32_t ibasin, shy_state *st);
+
+/* `nsteps` iterations of shyfem_run's loop body for every basin:
+ * copy_uvz/copy_depth, sp111(2) level boundaries, hydro
+ * (hydrodynamic.f90:284-485) and run_scalar (shyfem_subs.f90:975-1028).
+ * Returns the first non-zero status of any basin.                         */
+int shygpu_run(shygpu_model *model, int32_t nsteps);
+
+/* The same step split at the reference's phase boundaries:
+ * new_step = copy_uvz + copy_depth + sp111(2); hydro = hydrodynamic.f90:284;
+ * scalar = run_scalar (barocl T/S + rhoset + tracers).                    */
+int shygpu_new_step(shygpu_model *model);
+int shygpu_hydro(shygpu_model *model);
+int shygpu_scalar(shygpu_model *model);
+
+int shygpu_step_info(shygpu_model *model, int32_t ibasin, shy_step_info *info);
+/* Device bytes held by the model (admission by HBM footprint).            */
+int64_t shygpu_model_bytes(const shygpu_model *model);
+/* Bytes a model of these basins would hold, without allocating.           */
+int64_t shygpu_footprint(int32_t nbasin, const shy_basin *basins,
+                         const shy_params *params);
+
+/* Kernel launches issued by this process so far (for accounting).         */
+int64_t shygpu_launch_count(void);
+const char *shygpu_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* The reference's simsys interface (src/shyfem/simsys_spkaux.f90)     */
+/* gfortran by-reference convention; element data in shy_zeta_system.  */
+/* ------------------------------------------------------------------ */
+
+/* mod_zeta_system :: kn(3), hia(3,3), hik(3)  (simsys_spkaux.f90:75-83).
+ * hia is column-major like the Fortran array: hia[(m-1)*3 + (n-1)].      */
+typedef struct shy_zeta_system_t {
+  int32_t kn[3];
+  float hia[9];
+  float hik[3];
+} shy_zeta_system_t;
+extern shy_zeta_system_t shy_zeta_system;
+
+/* Registration that replaces the module state system_initialize reads
+ * (basin :: nkn, nel, nen3v).  Must precede system_initialize_.           */
+int shygpu_simsys_register(int32_t nkn, int32_t nel, const int32_t *nen3v);
+/* Solver controls (defaults 1e-8, 1e-8, 1000 as sparskit_admin.f90).      */
+int shygpu_simsys_set_tolerance(double rtol, double atol, int32_t maxit);
+/* Assembled matrix of the last solve, CSR rows = nodes (FP64 values, as
+ * the reference's c2coo) and its right-hand side, for inspection.         */
+int shygpu_simsys_get_matrix(int32_t *n, int32_t *nnz, int32_t *rowptr,
+                             int32_t *col, double *val, double *rhs);
+int shygpu_simsys_iterations(void);
+
+void system_initialize_(void);                      /* :85   */
+void system_init_(void);                            /* :137  */
+void system_set_explicit_(void);                    /* :160  */
+void system_assemble_(const int32_t *ie);           /* :533  */
+void system_add_rhs_(const float *dt, const int32_t *n, const float *array); /* :687 */
+void system_solve_(const int32_t *n, const float *z);                        /* :454 */
+void system_get_(const int32_t *n, float *z);                                /* :638 */
+void system_finalize_(void);                        /* :722  */
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SHYGPU_H */

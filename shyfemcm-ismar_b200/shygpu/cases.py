@@ -1,0 +1,226 @@
+"""Seeded synthetic basins (meshes, layers, forcing, initial state).
+
+SHYFEM reads a basin from a `.bas` file made by `shypre` from a `.grd` mesh and a
+`.str` parameter file (src/shyfem/shyfem_subs.f90:326-327).  No dataset ships
+with the reference for the semi-implicit step, so every workload here is a
+seeded synthetic basin of the named shape:
+
+* `channel_case`   -- 2D barotropic tidal channel, 61 x 13 nodes, 10 km x 2 km,
+                      M2 elevation on the x=0 boundary, quadratic friction.
+* `basin3d_case`   -- 3D baroclinic basin, ~20k nodes on 50 km x 30 km, 20
+                      z-layers 1..5 m thick, Gaussian-bump bathymetry 5..60 m,
+                      T/S linear in depth plus seeded noise, 10 m/s wind, M2 0.3 m.
+* `ensemble_cases` -- independent basins with log-uniform node counts.
+
+All arrays use the reference's layouts: Fortran column-major `(nlv, nel)` /
+`(nlv, nkn)` stored here as C arrays `[nel][nlv]` (layer index fastest), node
+and element numbers 1-based in `nen3v` like `basin :: nen3v(3,nel)`.
+
+The structure of a case follows the reference's module state:
+`basin` (nkn, nel, nen3v, xgv, ygv, hm3v), `levels` (nlv, hlv, hldv, ilhv,
+ilhkv), boundary tables (`bnd_admin.f90`: ibtyp=1 level boundaries with
+`ampli/period/phase/zref`), forcing (`mod_meteo`: tauxnv, tauynv, ppv) and
+parameters under their `.str` names (`def_para.f90`).
+"""
+from __future__ import annotations
+
+import math
+import numpy as np
+
+M2_PERIOD = 44714.0   # s, principal lunar semidiurnal
+S2_PERIOD = 43200.0   # s, principal solar semidiurnal
+
+# default parameters under their SHYFEM names (src/shyfem/def_para.f90)
+DEFAULT_PARAMS = dict(
+    dt=60.0,            # time step [s]
+    azpar=0.5, ampar=0.5, afpar=0.5,   # def_para.f90:666-668
+    atpar=1.0, adpar=1.0, aapar=1.0,   # def_para.f90:684-686
+    grav=9.81, rowass=1025.0,          # def_para.f90:782-784
+    vismol=1.0e-6, difmol=1.0e-6,      # def_para.f90:993-995
+    ireib=5, czdef=2.5e-3,             # quadratic friction, cd const (chezy.f90:330)
+    hzoff=0.05,                        # def_para.f90:745
+    ahpar=0.0,                         # horizontal viscosity (def_para.f90:1023)
+    ibarcl=0,                          # baroclinic terms (def_para.f90:1132)
+    ilin=1,                            # linear momentum (def_para.f90:584)
+    rstol=1.0,                         # transport Courant limit (def_para.f90:1055)
+    thpar=0.0, shpar=0.0, chpar=0.0,   # horizontal diffusivity of T, S, tracers
+    itemp=0, isalt=0, nconz=0,
+    icor=0,
+)
+
+
+def _smooth_field(x, y, rng, n_modes=6, scale=1.0):
+    """Sum of seeded low-wavenumber sinusoids normalised to [-scale, scale]."""
+    lx = x.max() - x.min() + 1e-9
+    ly = y.max() - y.min() + 1e-9
+    f = np.zeros_like(x)
+    for _ in range(n_modes):
+        kx = rng.integers(1, 4) * math.pi / lx
+        ky = rng.integers(1, 4) * math.pi / ly
+        ph1, ph2 = rng.uniform(0, 2 * math.pi, 2)
+        f += rng.uniform(0.5, 1.0) * np.sin(kx * x + ph1) * np.cos(ky * y + ph2)
+    m = np.abs(f).max()
+    return f * (scale / m if m > 0 else 0.0)
+
+
+def structured_triangles(nx, ny, lx, ly, jitter, seed):
+    """Regular nx x ny node grid, interior nodes jittered by +-jitter*spacing,
+    each quad split on a seeded random diagonal.  Nodes are numbered row by
+    row (x fastest), which keeps the sparsity band narrow like `shypre`'s
+    bandwidth-reducing renumbering.  Returns x, y, nen3v (1-based, (3,nel)
+    counter-clockwise), and the node (i, j) grid indices."""
+    rng = np.random.default_rng(seed)
+    dx = lx / (nx - 1)
+    dy = ly / (ny - 1)
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    x = (ii * dx).astype(np.float64).ravel()
+    y = (jj * dy).astype(np.float64).ravel()
+    interior = ((ii > 0) & (ii < nx - 1) & (jj > 0) & (jj < ny - 1)).ravel()
+    x[interior] += rng.uniform(-jitter, jitter, interior.sum()) * dx
+    y[interior] += rng.uniform(-jitter, jitter, interior.sum()) * dy
+    node = lambda i, j: j * nx + i
+    tris = []
+    diag = rng.integers(0, 2, size=(ny - 1, nx - 1))
+    for j in range(ny - 1):
+        for i in range(nx - 1):
+            a, b, c, d = node(i, j), node(i + 1, j), node(i + 1, j + 1), node(i, j + 1)
+            if diag[j, i]:
+                tris.append((a, b, c)); tris.append((a, c, d))
+            else:
+                tris.append((a, b, d)); tris.append((b, c, d))
+    nen3v = np.asarray(tris, dtype=np.int32) + 1     # 1-based like the reference
+    return x, y, nen3v, ii.ravel(), jj.ravel()
+
+
+def z_layers(thick):
+    """hldv (nominal thickness) and hlv (bottom depth of each layer)."""
+    hldv = np.asarray(thick, dtype=np.float64)
+    hlv = np.cumsum(hldv)
+    return hlv, hldv
+
+
+def layer_counts(nen3v, hm3v, hlv, hldv, nkn):
+    """Layers per element (`ilhv`) and per node (`ilhkv`).  The bottom layer
+    of an element must have positive thickness at every vertex
+    (`hlast = htot - hlv(lmax-1) > 0`, elems_dealing.f90:1045-1047), and a
+    bottom layer thinner than a quarter of its nominal thickness is merged
+    into the layer above (the intent of `hlvmin`, def_para.f90:942)."""
+    nlv = len(hlv)
+    hmin = hm3v.min(axis=1)
+    lmax = 1 + np.searchsorted(hlv, hmin, side="left")
+    lmax = np.minimum(lmax, nlv)
+    for _ in range(2):
+        hl_prev = np.where(lmax > 1, hlv[np.maximum(lmax - 2, 0)], 0.0)
+        thin = (lmax > 1) & ((hmin - hl_prev) < 0.25 * hldv[lmax - 1])
+        lmax = np.where(thin, lmax - 1, lmax)
+    ilhv = lmax.astype(np.int32)
+    ilhkv = np.zeros(nkn, dtype=np.int32)
+    np.maximum.at(ilhkv, nen3v.ravel() - 1, np.repeat(ilhv, 3))
+    return ilhv, ilhkv
+
+
+def _finish(case):
+    """Fill derived defaults shared by all cases."""
+    nkn, nel, nlv = case["nkn"], case["nel"], case["nlv"]
+    p = dict(DEFAULT_PARAMS)
+    p.update(case.get("params", {}))
+    case["params"] = p
+    case.setdefault("czv", np.full(nel, p["czdef"], np.float32))
+    case.setdefault("fcorv", np.zeros(nel, np.float32))
+    case.setdefault("visv", np.zeros((nkn, nlv + 1), np.float32))
+    case.setdefault("difv", np.zeros((nkn, nlv + 1), np.float32))
+    case.setdefault("tauxnv", np.zeros(nkn, np.float32))
+    case.setdefault("tauynv", np.zeros(nkn, np.float32))
+    case.setdefault("ppv", np.zeros(nkn, np.float32))
+    case.setdefault("rqv", np.zeros(nkn, np.float32))
+    case.setdefault("znv", np.zeros(nkn, np.float32))
+    case.setdefault("utlnv", np.zeros((nel, nlv), np.float32))
+    case.setdefault("vtlnv", np.zeros((nel, nlv), np.float32))
+    case.setdefault("tempv", np.zeros((nkn, nlv), np.float32))
+    case.setdefault("saltv", np.zeros((nkn, nlv), np.float32))
+    nc = p["nconz"]
+    case.setdefault("conzv", np.zeros((max(nc, 0), nkn, nlv), np.float32))
+    for k in ("hlv", "hldv", "hm3v", "xgv", "ygv"):
+        case[k] = np.ascontiguousarray(case[k], dtype=np.float32)
+    case["nen3v"] = np.ascontiguousarray(case["nen3v"], dtype=np.int32)
+    return case
+
+
+def channel_case(nx=61, ny=13, lx=10.0e3, ly=2.0e3, seed=1, dt=60.0,
+                 ampli=0.5, depth=10.0, ddepth=2.0):
+    """2D barotropic tidal channel (one layer, FP64 reference run)."""
+    x, y, nen3v, ii, jj = structured_triangles(nx, ny, lx, ly, 0.2, seed)
+    rng = np.random.default_rng(seed + 101)
+    hk = depth + _smooth_field(x, y, rng, scale=ddepth)
+    nkn, nel = x.size, nen3v.shape[0]
+    hm3v = hk[nen3v - 1]
+    hlv, hldv = np.array([1.0e4]), np.array([1.0e4])   # one layer covering all depths
+    ilhv = np.ones(nel, np.int32)
+    ilhkv = np.ones(nkn, np.int32)
+    bnd = np.zeros(nkn, np.int32)
+    bnd[ii == 0] = 1                                  # ibtyp=1 level boundary at x=0
+    tide = np.array([[[ampli, M2_PERIOD, 0.0, 0.0]]], np.float32)   # (nbnd, ntide, 4)
+    case = dict(name=f"channel2d_{nkn}", nkn=nkn, nel=nel, nlv=1, nen3v=nen3v,
+                xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
+                bnd_index=bnd, tide=tide, seed=seed,
+                params=dict(dt=dt))
+    return _finish(case)
+
+
+def basin3d_case(nkn_target=20000, lx=50.0e3, ly=30.0e3, seed=2, dt=120.0,
+                 nlv=20, ampli=0.3, wind=10.0, baroclinic=True, ts=True):
+    """3D baroclinic basin with z-layers, wind, M2 boundary and T/S."""
+    ny = max(3, int(round(math.sqrt(nkn_target * ly / lx))))
+    nx = max(3, int(round(nkn_target / ny)))
+    x, y, nen3v, ii, jj = structured_triangles(nx, ny, lx, ly, 0.2, seed)
+    rng = np.random.default_rng(seed + 202)
+    nkn, nel = x.size, nen3v.shape[0]
+    # Gaussian-bump bathymetry spanning 5..60 m
+    h = np.zeros(nkn)
+    for _ in range(8):
+        cx, cy = rng.uniform(0, lx), rng.uniform(0, ly)
+        s = rng.uniform(0.1, 0.3) * min(lx, ly)
+        h += rng.uniform(0.3, 1.0) * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * s * s))
+    h = 5.0 + 55.0 * (h - h.min()) / (h.max() - h.min())
+    thick = np.linspace(1.0, 5.0, nlv)
+    thick *= 60.0 / thick.sum()
+    hlv, hldv = z_layers(thick)
+    hlv[-1] = max(hlv[-1], h.max() + 1.0)
+    hm3v = h[nen3v - 1]
+    ilhv, ilhkv = layer_counts(nen3v, hm3v, hlv, hldv, nkn)
+    bnd = np.zeros(nkn, np.int32)
+    bnd[ii == 0] = 1
+    tide = np.array([[[ampli, M2_PERIOD, 0.0, 0.0]]], np.float32)
+    params = dict(dt=dt, ibarcl=1 if baroclinic else 0,
+                  itemp=1 if ts else 0, isalt=1 if ts else 0)
+    # uniform wind stress, normalised by water density as in mod_meteo (tauxnv = tau/rho0)
+    rhoair, cd = 1.225, 2.5e-3
+    taux = rhoair / 1025.0 * cd * wind * wind
+    zc = np.zeros((nkn, nlv))
+    # layer-centre depth at each node for T/S initialisation
+    zc[:] = (hlv - 0.5 * hldv)[None, :]
+    noise = np.random.default_rng(seed + 303)
+    tempv = 20.0 - 10.0 * zc / 60.0 + 0.2 * noise.standard_normal((nkn, nlv))
+    saltv = 30.0 + 8.0 * zc / 60.0 + 0.2 * noise.standard_normal((nkn, nlv))
+    case = dict(name=f"basin3d_{nkn}x{nlv}", nkn=nkn, nel=nel, nlv=nlv, nen3v=nen3v,
+                xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
+                bnd_index=bnd, tide=tide, seed=seed, params=params,
+                tauxnv=np.full(nkn, taux, np.float32),
+                tempv=tempv.astype(np.float32), saltv=saltv.astype(np.float32))
+    return _finish(case)
+
+
+def ensemble_cases(n, nkn_lo=5000, nkn_hi=100000, nlv=10, seed=4, dt=60.0):
+    """Independent basins with log-uniform node counts and seeded aspect
+    ratios and wind perturbations (sigma = 3 m/s)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        nk = int(math.exp(rng.uniform(math.log(nkn_lo), math.log(nkn_hi))))
+        aspect = rng.uniform(2.0, 6.0)
+        ly = 2.0e3 * math.sqrt(nk / 793.0)
+        c = basin3d_case(nkn_target=nk, lx=aspect * ly, ly=ly, seed=seed * 1000 + m, dt=dt,
+                         nlv=nlv, ampli=0.5, wind=10.0 + 3.0 * rng.standard_normal(),
+                         baroclinic=False, ts=False)
+        out.append(c)
+    return out
