@@ -1,0 +1,375 @@
+#!/usr/bin/env python
+"""bench.py -- node*layer*steps/s of SHYFEM's semi-implicit step on B200.
+
+Workload at N=1 (the 3D baroclinic basin): ~20k nodes / ~39.7k triangles on
+50 km x 30 km, 20 z-layers 1..5 m thick, Gaussian-bump bathymetry 5..60 m,
+temperature and salinity transported, baroclinic pressure, 10 m/s wind,
+M2 0.3 m level boundary, dt = 120 s.  Seeded synthetic input of that shape
+(no dataset ships with the reference).  One bench "step" is one model time
+step (shyfem_run's loop body: hydro + run_scalar) of that basin.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl shygpu|reference]
+                  [--workload basin3d|ensemble]
+
+N > 1 runs one process per GPU, each advancing its own replica (replicas
+only: the step has no exchange between basins), value = all ranks' units /
+max-over-ranks time.  `--impl reference` times the CPU restatement of the
+reference's algorithm (the oracle) on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "shyfemcm-ismar_b200"))
+
+METRIC = "node*layer*steps/s"
+PEAKS_FILE = ROOT / "MEASURED_PEAKS.json"
+FALLBACK_HBM = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--impl", default="shygpu", choices=["shygpu", "reference"])
+    p.add_argument("--workload", default="basin3d", choices=["basin3d", "ensemble"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def make_cases(workload, rank=0):
+    from shygpu import cases
+    if workload == "basin3d":
+        return [cases.basin3d_case(nkn_target=20000, seed=2 + 1000 * rank)]
+    return cases.ensemble_cases(64, seed=4 + 1000 * rank)
+
+
+def units_per_step(case_list):
+    return sum(c["nkn"] * c["nlv"] for c in case_list)
+
+
+def workload_config(workload, case_list, l2):
+    if workload == "basin3d":
+        c = case_list[0]
+        return {"workload": "basin3d_baroclinic_ts", "nkn": c["nkn"], "nel": c["nel"],
+                "nlv": c["nlv"], "dt_s": c["params"]["dt"], "tracers": "T,S",
+                "forcing": "10 m/s wind, M2 0.3 m", "l2": l2}
+    return {"workload": "ensemble_64_basins", "basins": len(case_list),
+            "nkn_total": sum(c["nkn"] for c in case_list), "nlv": case_list[0]["nlv"],
+            "dt_s": case_list[0]["params"]["dt"], "l2": l2}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.rows = []
+        self.stop_flag = False
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append((time.time(), line.strip()))
+
+    def summary(self, t0, t1):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sel = [r for t, r in self.rows if t0 - 0.15 <= t <= t1 + 0.15] or [r for _, r in self.rows]
+        for r in sel:
+            parts = [x.strip() for x in r.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch of each kernel (FP32 state, compulsory traffic)
+# ---------------------------------------------------------------------------
+def algorithmic_bytes(case_list, infos, nsc, cor=False):
+    nkn = sum(c["nkn"] for c in case_list)
+    nel = sum(c["nel"] for c in case_list)
+    NL = sum(int(c["ilhv"].sum()) for c in case_list)          # active element-layers
+    NK = sum(int(c["ilhkv"].sum()) for c in case_list)         # active node-layers
+    NI = sum(c["nkn"] * (c["nlv"] + 1) for c in case_list)     # node interfaces
+    nnz = 7 * nkn
+    iters = sum(i.krylov_iters for i in infos)
+    outer = sum(max(i.refinements, 1) for i in infos)
+    b = {}
+    b["column"] = NL * (24 + (4 if cor else 0)) + nel * (12 + 32 + 16 + 8 + 48) + NK * 4 + NI * 4 + nkn * 12
+    b["zeta"] = (nel * (48 + 36 + 12) + nnz * (4 + 12 + 4) + nkn * (4 + 4 + 4 + 4 + 20)
+                 + iters * (8 * nnz + 48 * nkn) + outer * (12 * nnz + 20 * nkn))
+    b["final"] = NL * (24 + (4 if cor else 0)) + nel * (12 + 32 + 16 + 16 + 4 + 8 + 12) + nkn * 4
+    b["node"] = NL * 16 + nel * (12 + 32 + 16 + 4) + NK * 12 + nkn * 20 + NI * 4
+    b["stab"] = NL * 24 + nel * (36 + 32 + 16 + 4 + 12) + NK * 8 + NI * 8
+    b["reduce"] = nkn * 8
+    b["conz"] = NL * 28 + nel * (32 + 16 + 4 + 12) + NK * (8 * nsc + 8 + 8) + NI * 8
+    return b
+
+
+def load_peak():
+    try:
+        d = json.loads(PEAKS_FILE.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline / reference arm: the oracle on host cores
+# ---------------------------------------------------------------------------
+def _oracle_worker(args):
+    workload, seed_rank, nsteps, warm = args
+    sys.path.insert(0, str(ROOT / "oracle"))
+    sys.path.insert(0, str(ROOT / "shyfemcm-ismar_b200"))
+    import shyref
+    cl = make_cases(workload, seed_rank)
+    if workload == "ensemble":
+        cl = cl[:2]
+    ms = [shyref.OracleModel(c) for c in cl]
+    for m in ms:
+        m.run(warm)
+    t0 = time.perf_counter()
+    for m in ms:
+        m.run(nsteps)
+    dt = time.perf_counter() - t0
+    return units_per_step(cl) * nsteps, dt
+
+
+def cpu_baseline(workload, nproc, nsteps, warm=1):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_oracle_worker, [(workload, 10 + i, nsteps, warm) for i in range(nproc)])
+    wall = time.perf_counter() - t0
+    units = sum(r[0] for r in res)
+    tmax = max(r[1] for r in res)
+    return units / tmax, tmax, wall
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    nproc = os.cpu_count() or 1
+    # each bench step: one time step of each of nproc independent replicas
+    steps = max(1, a.steps if a.steps <= 40 else 20)
+    value, tmax, wall = cpu_baseline(a.workload, nproc, steps, warm=min(a.warmup, 2))
+    cl = make_cases(a.workload)
+    if a.workload == "ensemble":
+        cl = cl[:2]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
+            "n_gpus": a.gpus, "steps": steps, "warmup": min(a.warmup, 2),
+            "ms_per_step": 1000.0 * tmax / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(a.workload, cl, "n/a (CPU)"),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": nproc, "kind": "port",
+                             "sample": f"{steps} steps of {nproc} independent replicas, one per core; "
+                                       "FP64 C++ restatement of the reference step (oracle/shyref.cpp)"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# the GPU arm
+# ---------------------------------------------------------------------------
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+        return
+    import torch
+    import torch.distributed as dist
+    import shygpu
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    os.environ.setdefault("SHYGPU_NO_BUILD", "1")
+    os.environ["CUDA_VISIBLE_DEVICES_HINT"] = str(local)
+
+    case_list = make_cases(a.workload, rank)
+    model = shygpu.Model(case_list)
+    model.set_state_all()
+    stream = torch.cuda.ExternalStream(model.stream())
+    units = units_per_step(case_list)
+    L2_FLUSH = 256 << 20
+    flush = torch.empty(L2_FLUSH // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- warm-up ----
+    model.run(max(a.warmup, 3))
+    # ---- device-timed region: K single steps, L2 flushed between them ----
+    sampler = ClockSampler(local)
+    time.sleep(1.0)
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    lib = shygpu.lib()
+    launches0 = lib.shygpu_launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    t_wall0 = time.time()
+    with torch.cuda.stream(stream):
+        for i in range(a.steps):
+            flush.fill_(float(i))
+            ev0[i].record(stream)
+            lib.shygpu_enqueue(model.h, 1)
+            ev1[i].record(stream)
+    torch.cuda.synchronize()
+    t_wall1 = time.time()
+    shygpu.check(lib.shygpu_sync(model.h), "step")
+    launches = lib.shygpu_launch_count() - launches0
+    ms_total = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
+    barrier()
+    clocks = sampler.summary(t_wall0, t_wall1)
+    if world > 1:
+        t = torch.tensor([ms_total], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / a.steps
+    value = world * units * a.steps / (ms_total / 1000.0)
+
+    # ---- end to end through the public API: forcing in, water level and
+    #      transports out, every step, pinned host buffers ----
+    c0 = case_list[0]
+    nb = len(case_list)
+    taux = [torch.from_numpy(np.ascontiguousarray(c["tauxnv"])).pin_memory() for c in case_list]
+    tauy = [torch.from_numpy(np.ascontiguousarray(c["tauynv"])).pin_memory() for c in case_list]
+    outs = []
+    for c in case_list:
+        outs.append(dict(znv=torch.empty(c["nkn"], dtype=torch.float32).pin_memory(),
+                         utlnv=torch.empty(c["nel"] * c["nlv"], dtype=torch.float32).pin_memory(),
+                         vtlnv=torch.empty(c["nel"] * c["nlv"], dtype=torch.float32).pin_memory()))
+    from shygpu import abi
+    import ctypes as C
+    states = []
+    for o in outs:
+        s = abi.ShyState()
+        for k, v in o.items():
+            setattr(s, k, C.cast(C.c_void_p(v.data_ptr()), abi.f32p))
+        states.append(s)
+    h2d = sum(c["nkn"] * 8 for c in case_list)
+    d2h = sum((c["nkn"] + 2 * c["nel"] * c["nlv"]) * 4 for c in case_list)
+    e2e_steps = min(a.steps, 200)
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(e2e_steps):
+        for b in range(nb):
+            lib.shygpu_set_forcing(model.h, b, taux[b].data_ptr(), tauy[b].data_ptr(), None, None)
+        shygpu.check(lib.shygpu_run(model.h, 1), "run")
+        for b in range(nb):
+            shygpu.check(lib.shygpu_get_state(model.h, b, C.byref(states[b])), "get_state")
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * units * e2e_steps / e2e_s
+
+    # ---- live per-kernel times for the roofline (eager launches with events) ----
+    prof = model.profile_steps(20)
+    infos = [model.info(b) for b in range(nb)]
+    nsc = int(c0["params"]["itemp"]) + int(c0["params"]["isalt"]) + int(c0["params"]["nconz"])
+    algo = algorithmic_bytes(case_list, infos, nsc)
+    tot_ms = sum(v[0] for v in prof.values())
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_n = prof[dom]
+    peak, peak_kind = load_peak()
+    achieved = algo[dom] / (dom_ms / dom_n / 1000.0) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get(a.workload, {}).get(dom)
+        except Exception:
+            traffic = None
+    kernels = {k: {"ms_per_launch": (v[0] / v[1] if v[1] else 0.0), "share": v[0] / tot_ms if tot_ms else 0,
+                   "launches": v[1], "algorithmic_bytes": algo[k],
+                   "gbs": (algo[k] / (v[0] / v[1] / 1000.0) / 1e9) if v[1] and v[0] > 0 else 0.0}
+               for k, v in prof.items()}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": dict(workload_config(a.workload, case_list,
+                                       "flushed between timed steps (256 MiB write)"),
+                       parallelism=f"replicas{world}"),
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                "path": "shygpu_set_forcing + shygpu_run(1) + shygpu_get_state(znv, utlnv, vtlnv)"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic},
+        "kernels": kernels,
+        "solver": {"krylov_iters_last_step": infos[0].krylov_iters,
+                   "refinements": infos[0].refinements, "resid": infos[0].resid},
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        nproc = 1
+        v, tmax, _ = cpu_baseline(a.workload, nproc, 20, warm=1)
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": nproc, "kind": "port",
+                                "sample": "20 time steps of the same basin, FP64 C++ restatement "
+                                          "of the reference step (oracle/shyref.cpp), 1 thread"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    model.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

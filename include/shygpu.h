@@ -165,6 +165,10 @@ int shygpu_get_state(shygpu_model *model, int32_t ibasin, shy_state *st);
  * (hydrodynamic.f90:284-485) and run_scalar (shyfem_subs.f90:975-1028).
  * Returns the first non-zero status of any basin.                         */
 int shygpu_run(shygpu_model *model, int32_t nsteps);
+/* shygpu_run split in two: queue the steps on the model's stream and return
+ * at once; then wait for them and report the first error of any basin.   */
+int shygpu_enqueue(shygpu_model *model, int32_t nsteps);
+int shygpu_sync(shygpu_model *model);
 
 /* The same step split at the reference's phase boundaries:
  * new_step = copy_uvz + copy_depth + sp111(2); hydro = hydrodynamic.f90:284;
@@ -174,6 +178,32 @@ int shygpu_hydro(shygpu_model *model);
 int shygpu_scalar(shygpu_model *model);
 
 int shygpu_step_info(shygpu_model *model, int32_t ibasin, shy_step_info *info);
+
+/* Per-step forcing of a basin from host memory (pinned for overlap):
+ * tauxnv, tauynv, ppv, rqv (nkn each); NULL members are left unchanged.
+ * The copies are queued on the model's stream ahead of the next step,
+ * like the meteo/boundary reads that precede hydro in shyfem_run.        */
+int shygpu_set_forcing(shygpu_model *model, int32_t ibasin, const float *tauxnv,
+                       const float *tauynv, const float *ppv, const float *rqv);
+
+/* Tuning options by name: "use_graph" (CUDA-graph replay of whole steps,
+ * the transport sub-step loop as a device-driven conditional node; default
+ * 1), "cluster_size" and "zeta_threads" (shape of the per-basin cluster of
+ * the zeta solve), "inner_rtol" (residual reduction of each FP32 Krylov
+ * sweep), "max_outer" (FP64 refinement sweeps), "symmetric" (CG instead of
+ * BiCGStab; refused when Coriolis makes the system non-symmetric).        */
+int shygpu_set_option(shygpu_model *model, const char *name, double value);
+double shygpu_get_option(shygpu_model *model, const char *name);
+
+/* The CUDA stream every launch of the model goes to (cudaStream_t).      */
+void *shygpu_model_stream(shygpu_model *model);
+
+/* Run `nsteps` steps with CUDA events between the kernels of each step and
+ * return the summed device time per kernel kind in ms_out[SHY_NKERNEL] and
+ * the launches per kind in count_out (kinds: column, zeta, final, node,
+ * stab, reduce, conz).                                                    */
+#define SHY_NKERNEL 7
+int shygpu_profile_steps(shygpu_model *model, int32_t nsteps, double *ms_out, int32_t *count_out);
 /* Device bytes held by the model (admission by HBM footprint).            */
 int64_t shygpu_model_bytes(const shygpu_model *model);
 /* Bytes a model of these basins would hold, without allocating.           */

@@ -42,6 +42,7 @@ def _lib():
     lib.shyref_step_info.argtypes = [C.c_void_p, C.POINTER(abi.ShyStepInfo)]
     lib.shyref_get_state64.argtypes = [C.c_void_p] + [d_p] * 11
     lib.shyref_last_system.argtypes = [C.c_void_p, i_p, d_p, d_p]
+    lib.shyref_element_system.argtypes = [d_p, d_p] + [C.c_double] * 6 + [d_p] + [C.c_double] * 4 + [d_p, d_p]
     lib.shyref_spk_solve.argtypes = [C.c_int, i_p, i_p, d_p, d_p, d_p, C.c_double, C.c_double,
                                      C.c_int, i_p, d_p, d_p]
     return lib

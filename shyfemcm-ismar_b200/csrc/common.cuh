@@ -1,0 +1,244 @@
+// common.cuh -- device data model and warp-segment primitives.
+//
+// Layout.  Every basin of a model lives in one set of flat arrays: global
+// element index e in [0,NEL), node index k in [0,NKN).  Column arrays keep
+// the reference's Fortran layout with the layer index fastest and a common
+// stride NLV (the largest nlv of the model's basins):
+//   element-layer  a[e*NLV + l]        (utlnv, vtlnv, hdenv, ...)
+//   node-layer     a[k*NLV + l]        (hdknv, tempv, saltv, rhov, ...)
+//   interface      a[k*(NLV+1) + l]    (wlnv, visv, difv)
+// One warp segment of S lanes (S = next power of two >= NLV, S | 32) owns
+// one column: lane l is layer l.  A segment reads a column as one contiguous
+// run, and vertical recurrences (tridiagonal solves, prefix sums over
+// layers) run across lanes with shuffles.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define SHY_FLAGF 1.23456e+23f      // mkonst :: flag, "no value" for rzv
+#define SHY_FLAGD 1.23456e+23
+
+namespace shy {
+
+constexpr int kMaxScal = 10;        // T, S and up to 8 passive tracers
+constexpr int kMaxTide = 4;
+
+// per-basin parameters (device memory)
+struct BasinPar {
+  double dt;
+  double dtime0;
+  float az, am, af, at, ad, aa;
+  float grav, rowass, vismol, difmol, hzoff, ahpar, rstol;
+  float rkpar[kMaxScal];      // horizontal diffusivity per scalar
+  int ireib, ibarcl, nsc;     // nsc: scalars transported (T, S, tracers)
+  int itemp, isalt;
+  int istot_max;
+  int k0, nk, e0, ne, nlv;    // node/element ranges
+  int tide_off, ntide;        // tide table offset (floats) and constituents
+  float rtol, atol;
+  int maxit;
+  int has_cor;
+  int is_temp[kMaxScal];      // scalar s is temperature (no clipping at 1e-15)
+};
+
+// per-basin results of the last step (device memory)
+struct BasinOut {
+  double dtime;
+  double resid0, resid;
+  double volume;
+  int status;
+  int iters, refinements;
+  int istot;
+  float stab[kMaxScal];       // stability index (as float bits, max-reduced)
+};
+
+// everything a kernel needs, passed by value
+struct Dev {
+  int nbasin, NKN, NEL, NLV, S, nsc_max;
+  BasinPar *par;
+  BasinOut *out;
+  // mesh (static)
+  int4 *enode;        // {k1,k2,k3,basin}, global node numbers
+  float *ev8;         // [e*8]: b1 b2 b3 c1 c2 c3 aj(=area/24) dd-unused
+  float4 *hm3v;       // {h1,h2,h3,hev}
+  int *ilhv, *ilhkv;
+  float *czv, *fcorv;
+  int *ieltv;         // [e*3+ii] neighbour opposite vertex ii, global, -1 none
+  float *wdif;        // [e*9 + ii*3+iii]
+  float *difhv;       // [e*NLV+l]
+  int *kbnd;          // [k] level-boundary number (basin-local, 1-based) or 0
+  float *tide;        // [(b-1)*ntide*4 + c*4 + {ampli,period,phase,zref}] + tide_off
+  float *visv, *difv; // [k*(NLV+1)+l]
+  float *taux, *tauy, *ppv, *rqv;
+  float *hlv, *hldv;  // [b*NLV + l]
+  float *areakv;      // [k*NLV+l]
+  // zeta system
+  int *rowptr, *col;          // CSR over all nodes (block diagonal)
+  int *slot_ptr, *slot_src;   // gather of element entries per CSR slot
+  int *inc_ptr, *inc;         // node -> (e*3+ii) incidence, increasing e
+  double *val64, *rhs64, *x64;
+  float *val32, *dinv32, *r32, *p32, *q32, *z32, *e32, *s32, *t32, *rh32, *v32;
+  // element system written by the column kernel (SoA): hia[c*NEL+e], hik[c*NEL+e]
+  float *hia, *hik;
+  // state, [0] = new, [1] = old (swapped per step)
+  float *zn, *zo;             // [k]
+  float *zen, *zeo;           // [e*3+ii]
+  float *un, *vn, *uo, *vo;   // [e*NLV+l]
+  float *hkn, *hko;           // [k*NLV+l]
+  float *hen, *heo;           // [e*NLV+l]
+  float *unv, *vnv;           // [e]
+  float *wl;                  // [k*(NLV+1)+l]
+  float *rho;                 // [k*NLV+l]
+  float *ddx, *ddxi;          // [e*NLV+l] A^-1 H (real / imaginary part with Coriolis)
+  float *sc_in, *sc_out;      // [s*NKN*NLV + k*NLV + l] scalars at step start / end
+  float *scr0, *scr1;         // intermediate transport sub-steps
+  float *cbnd;                // boundary values of the scalars, same layout
+  double *vol_node;           // [k]
+  float *stab_node;           // [s*NKN + k]
+  int *imax;                  // largest transport sub-step count of the step (all basins)
+  int *subj;                  // sub-step index of the device-driven sub-step loop
+  unsigned long long *nsub_launched;   // transport launches made by that loop
+};
+
+// ---------------------------------------------------------------------------
+// warp-segment helpers (width S is a power of two dividing 32)
+// ---------------------------------------------------------------------------
+// Shuffles name only the lanes of the calling segment, so segments of one
+// warp may follow different control flow (they can belong to different
+// basins); all lanes of a segment always execute a shuffle together.
+template <int S>
+__device__ __forceinline__ unsigned seg_mask() {
+  if constexpr (S == 32) return 0xffffffffu;
+  else return ((1u << S) - 1u) << ((threadIdx.x & 31) & ~(S - 1));
+}
+template <int S, typename T>
+__device__ __forceinline__ T seg_up(T v, int d) {   // value from lane l-d (same segment)
+  return __shfl_up_sync(seg_mask<S>(), v, d, S);
+}
+template <int S, typename T>
+__device__ __forceinline__ T seg_down(T v, int d) { // value from lane l+d (same segment)
+  return __shfl_down_sync(seg_mask<S>(), v, d, S);
+}
+template <int S, typename T>
+__device__ __forceinline__ T seg_bcast(T v, int src) {
+  return __shfl_sync(seg_mask<S>(), v, src, S);
+}
+template <int S, typename T>
+__device__ __forceinline__ T seg_sum(T v) {         // sum over the segment, all lanes get it
+#pragma unroll
+  for (int d = S / 2; d > 0; d >>= 1) v += __shfl_xor_sync(seg_mask<S>(), v, d, S);
+  return v;
+}
+template <int S>
+__device__ __forceinline__ float seg_max(float v) {
+#pragma unroll
+  for (int d = S / 2; d > 0; d >>= 1) v = fmaxf(v, __shfl_xor_sync(seg_mask<S>(), v, d, S));
+  return v;
+}
+// inclusive prefix sum from the top (lane 0) down
+template <int S, typename T>
+__device__ __forceinline__ T seg_scan_down(T v, int lane) {
+#pragma unroll
+  for (int d = 1; d < S; d <<= 1) {
+    T o = __shfl_up_sync(seg_mask<S>(), v, d, S);
+    if (lane >= d) v += o;
+  }
+  return v;
+}
+// inclusive suffix sum from the bottom (lane S-1) up
+template <int S, typename T>
+__device__ __forceinline__ T seg_scan_up(T v, int lane) {
+#pragma unroll
+  for (int d = 1; d < S; d <<= 1) {
+    T o = __shfl_down_sync(seg_mask<S>(), v, d, S);
+    if (lane + d < S) v += o;
+  }
+  return v;
+}
+
+// Parallel cyclic reduction of a tridiagonal system a x_{l-1} + b x_l + c x_{l+1}
+// = d across the S lanes of a segment (Hockney 1965; Hockney & Jesshope).
+// Lanes outside the system carry the identity row (a=c=d=0, b=1) and the
+// last row of the system has c = 0, so no coupling leaks across the border.
+// NR right-hand sides share the factorisation.
+template <int S, int NR>
+__device__ __forceinline__ void pcr_solve(double a, double b, double c, double (&d)[NR], int lane) {
+#pragma unroll
+  for (int s = 1; s < S; s <<= 1) {
+    double am = seg_up<S>(a, s), bm = seg_up<S>(b, s), cm = seg_up<S>(c, s);
+    double ap = seg_down<S>(a, s), bp = seg_down<S>(b, s), cp = seg_down<S>(c, s);
+    double dm[NR], dp[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) { dm[r] = seg_up<S>(d[r], s); dp[r] = seg_down<S>(d[r], s); }
+    bool hasm = lane >= s, hasp = lane + s < S;
+    if (!hasm) { am = 0.; bm = 1.; cm = 0.; }
+    if (!hasp) { ap = 0.; bp = 1.; cp = 0.; }
+    double k1 = hasm ? a / bm : 0.;
+    double k2 = hasp ? c / bp : 0.;
+    double na = -am * k1, nc = -cp * k2;
+    double nb = b - cm * k1 - ap * k2;
+#pragma unroll
+    for (int r = 0; r < NR; r++) d[r] = d[r] - (hasm ? dm[r] * k1 : 0.) - (hasp ? dp[r] * k2 : 0.);
+    a = na; b = nb; c = nc;
+  }
+#pragma unroll
+  for (int r = 0; r < NR; r++) d[r] = d[r] / b;
+}
+
+// complex arithmetic on double2 (x = real, y = imaginary)
+__device__ __forceinline__ double2 cmul(double2 p, double2 q) {
+  return make_double2(p.x * q.x - p.y * q.y, p.x * q.y + p.y * q.x);
+}
+__device__ __forceinline__ double2 cdiv(double2 p, double2 q) {
+  double den = q.x * q.x + q.y * q.y;
+  return make_double2((p.x * q.x + p.y * q.y) / den, (p.y * q.x - p.x * q.y) / den);
+}
+__device__ __forceinline__ double2 csub(double2 p, double2 q) { return make_double2(p.x - q.x, p.y - q.y); }
+template <int S>
+__device__ __forceinline__ double2 seg_up2(double2 v, int d) {
+  return make_double2(seg_up<S>(v.x, d), seg_up<S>(v.y, d));
+}
+template <int S>
+__device__ __forceinline__ double2 seg_down2(double2 v, int d) {
+  return make_double2(seg_down<S>(v.x, d), seg_down<S>(v.y, d));
+}
+
+// PCR for a complex tridiagonal with real off-diagonals a, c and complex
+// diagonal b (the u/v column system with Coriolis, where u + i v is the
+// unknown): NR complex right-hand sides.
+template <int S, int NR>
+__device__ __forceinline__ void pcr_solve_c(double a, double2 b, double c, double2 (&d)[NR], int lane) {
+  double2 A = make_double2(a, 0.), C = make_double2(c, 0.);
+#pragma unroll
+  for (int s = 1; s < S; s <<= 1) {
+    double2 am = seg_up2<S>(A, s), bm = seg_up2<S>(b, s), cm = seg_up2<S>(C, s);
+    double2 ap = seg_down2<S>(A, s), bp = seg_down2<S>(b, s), cp = seg_down2<S>(C, s);
+    double2 dm[NR], dp[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) { dm[r] = seg_up2<S>(d[r], s); dp[r] = seg_down2<S>(d[r], s); }
+    bool hasm = lane >= s, hasp = lane + s < S;
+    double2 z = make_double2(0., 0.), one = make_double2(1., 0.);
+    if (!hasm) { am = z; bm = one; cm = z; }
+    if (!hasp) { ap = z; bp = one; cp = z; }
+    double2 k1 = hasm ? cdiv(A, bm) : z;
+    double2 k2 = hasp ? cdiv(C, bp) : z;
+    double2 na = make_double2(-(cmul(am, k1).x), -(cmul(am, k1).y));
+    double2 nc = make_double2(-(cmul(cp, k2).x), -(cmul(cp, k2).y));
+    double2 nb = csub(csub(b, cmul(cm, k1)), cmul(ap, k2));
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      if (hasm) d[r] = csub(d[r], cmul(dm[r], k1));
+      if (hasp) d[r] = csub(d[r], cmul(dp[r], k2));
+    }
+    A = na; b = nb; C = nc;
+  }
+#pragma unroll
+  for (int r = 0; r < NR; r++) d[r] = cdiv(d[r], b);
+}
+
+__device__ __forceinline__ void atomic_max_pos(float *addr, float v) {
+  // v >= 0: the ordering of non-negative IEEE floats matches their int bits
+  atomicMax(reinterpret_cast<int *>(addr), __float_as_int(v));
+}
+
+}  // namespace shy

@@ -1,0 +1,1165 @@
+// host.cu -- C ABI of libshygpu: model set-up, state transfer, the step
+// driver (eager launches or CUDA-graph replay), and the reference's simsys
+// interface.  Init-time work (geometry, sparsity pattern, gather maps) runs
+// on the host once, as shyfem_initialize does; every time step runs on the
+// device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/shygpu.h"
+#include "common.cuh"
+#include "launch.h"
+
+
+using namespace shy;
+
+// ---------------------------------------------------------------------------
+// errors and accounting
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+static std::atomic<long long> g_launches{0};
+
+static int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CUDA_TRY(x)                                                                   \
+  do {                                                                                \
+    cudaError_t _e = (x);                                                             \
+    if (_e != cudaSuccess)                                                            \
+      return fail(SHY_ECUDA, "%s failed: %s (%s:%d)", #x, cudaGetErrorString(_e), __FILE__, \
+                  __LINE__);                                                          \
+  } while (0)
+
+extern "C" const char *shygpu_last_error(void) { return g_err.c_str(); }
+// launches counted on the host, plus those the device-driven sub-step loops
+// of live models made (read from each model's device counter)
+static std::vector<const void *> g_models;
+static int64_t device_launches(const void *m);
+extern "C" int64_t shygpu_launch_count(void) {
+  int64_t n = g_launches.load();
+  for (const void *m : g_models) n += device_launches(m);
+  return n;
+}
+
+static int device_ok() {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    return fail(SHY_ECUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+  return SHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// geometry: set_ev (src/utils/shyutil/evgeom.f90:167-320), FP64
+// ---------------------------------------------------------------------------
+static void adjust_bc(double &v1, double &v2, double &v3) {   // evgeom.f90:1007-1040
+  double vv = v1 + v2 + v3;
+  if (vv == 0.) return;
+  if (v1 == 0.) { v2 = v2 - vv / 2.; v3 = -v2; }
+  else if (v2 == 0.) { v3 = v3 - vv / 2.; v1 = -v3; }
+  else if (v3 == 0.) { v1 = v1 - vv / 2.; v2 = -v1; }
+  else { v1 = v1 - vv / 3.; v2 = v2 - vv / 3.; v3 = v3 - vv / 3.; v3 = -v1 - v2; }
+}
+
+static int compute_ev(int nkn, int nel, const int32_t *nen3v, const float *xgv, const float *ygv,
+                      std::vector<double> &ev) {
+  ev.assign((size_t)SHY_EVDIM * nel, 0.);
+  const double rad = 180. / (4. * std::atan(1.));
+  for (int ie = 0; ie < nel; ie++) {
+    int k[3];
+    for (int i = 0; i < 3; i++) {
+      k[i] = nen3v[3 * ie + i] - 1;
+      if (k[i] < 0 || k[i] >= nkn) return fail(SHY_EARG, "set_ev: element %d has node %d out of range", ie + 1, k[i] + 1);
+    }
+    double x1 = xgv[k[0]], y1 = ygv[k[0]], x2 = xgv[k[1]], y2 = ygv[k[1]], x3 = xgv[k[2]], y3 = ygv[k[2]];
+    double a1 = x2 * y3 - x3 * y2, a2 = x3 * y1 - x1 * y3, a3 = x1 * y2 - x2 * y1;
+    double aj = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1);
+    if (aj <= 0) return fail(SHY_EARG, "set_ev: element %d has non-positive area", ie + 1);
+    double aji = 1. / aj;
+    double b1 = (y2 - y3) * aji, c1 = (x3 - x2) * aji;
+    double b2 = (y3 - y1) * aji, c2 = (x1 - x3) * aji;
+    double b3 = (y1 - y2) * aji, c3 = (x2 - x1) * aji;
+    a1 *= aji; a2 *= aji; a3 *= aji;
+    adjust_bc(b1, b2, b3);
+    adjust_bc(c1, c2, c3);
+    double ss1 = (x3 - x2) * (x3 - x2) + (y3 - y2) * (y3 - y2), s1 = std::sqrt(ss1);
+    double ss2 = (x3 - x1) * (x3 - x1) + (y3 - y1) * (y3 - y1), s2 = std::sqrt(ss2);
+    double ss3 = (x2 - x1) * (x2 - x1) + (y2 - y1) * (y2 - y1), s3 = std::sqrt(ss3);
+    double *e = &ev[(size_t)ie * SHY_EVDIM];
+    e[0] = a1; e[1] = a2; e[2] = a3;
+    e[3] = b1; e[4] = b2; e[5] = b3;
+    e[6] = c1; e[7] = c2; e[8] = c3;
+    e[9] = aj / 24.;
+    e[10] = std::acos((ss2 + ss3 - ss1) / (2. * s2 * s3)) * rad;
+    e[11] = std::acos((ss1 + ss3 - ss2) / (2. * s1 * s3)) * rad;
+    e[12] = std::acos((ss1 + ss2 - ss3) / (2. * s1 * s2)) * rad;
+    e[13] = aj * std::sqrt(b1 * b1 + c1 * c1);
+    e[14] = aj * std::sqrt(b2 * b2 + c2 * c2);
+    e[15] = aj * std::sqrt(b3 * b3 + c3 * c3);
+    e[16] = s1; e[17] = s2; e[18] = s3;
+  }
+  return SHY_OK;
+}
+
+extern "C" int shygpu_set_ev(int32_t nkn, int32_t nel, const int32_t *nen3v, const float *xgv,
+                             const float *ygv, float *ev) {
+  if (nkn <= 0 || nel <= 0 || !nen3v || !xgv || !ygv || !ev) return fail(SHY_EARG, "set_ev: bad arguments");
+  std::vector<double> e;
+  int st = compute_ev(nkn, nel, nen3v, xgv, ygv, e);
+  if (st) return st;
+  for (size_t i = 0; i < e.size(); i++) ev[i] = (float)e[i];
+  return SHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// sparsity pattern (construct_node_list + coo_init_new, coo_matrix.f90:51-400)
+// and the gather maps that replace the element scatter of system_assemble
+// ---------------------------------------------------------------------------
+struct Pattern {
+  std::vector<int> rowptr, col;          // local CSR (0-based)
+  std::vector<int> slot_ptr, slot_src;   // per slot: (ie*9 + 3i+j), increasing ie
+  std::vector<int> inc_ptr, inc;         // per node: (ie*3 + ii), increasing ie
+};
+
+static int build_pattern(int nkn, int nel, const int *nv /*0-based*/, Pattern &P) {
+  std::vector<std::vector<int>> nl(nkn);
+  for (int ie = 0; ie < nel; ie++)
+    for (int ii = 0; ii < 3; ii++) {
+      int k1 = nv[3 * ie + ii], k2 = nv[3 * ie + (ii + 1) % 3];
+      nl[k1].push_back(k2);
+      nl[k2].push_back(k1);
+    }
+  P.rowptr.assign(nkn + 1, 0);
+  P.col.clear();
+  for (int k = 0; k < nkn; k++) {
+    nl[k].push_back(k);
+    std::sort(nl[k].begin(), nl[k].end());
+    nl[k].erase(std::unique(nl[k].begin(), nl[k].end()), nl[k].end());
+    P.rowptr[k + 1] = P.rowptr[k] + (int)nl[k].size();
+    P.col.insert(P.col.end(), nl[k].begin(), nl[k].end());
+  }
+  int nnz = P.rowptr[nkn];
+  std::vector<int> ijp((size_t)9 * nel);
+  std::vector<int> cnt(nnz, 0);
+  for (int ie = 0; ie < nel; ie++)
+    for (int i = 0; i < 3; i++) {
+      int ki = nv[3 * ie + i];
+      for (int j = 0; j < 3; j++) {
+        int kj = nv[3 * ie + j];
+        int *b = &P.col[P.rowptr[ki]], *e = &P.col[P.rowptr[ki + 1]];
+        int *f = std::lower_bound(b, e, kj);
+        if (f == e || *f != kj) return fail(SHY_EARG, "coo_init: internal error (pattern)");
+        int slot = P.rowptr[ki] + (int)(f - b);
+        ijp[(size_t)9 * ie + 3 * i + j] = slot;
+        cnt[slot]++;
+      }
+    }
+  P.slot_ptr.assign(nnz + 1, 0);
+  for (int s = 0; s < nnz; s++) P.slot_ptr[s + 1] = P.slot_ptr[s] + cnt[s];
+  P.slot_src.assign(P.slot_ptr[nnz], 0);
+  std::vector<int> fillp(P.slot_ptr.begin(), P.slot_ptr.end() - 1);
+  for (int ie = 0; ie < nel; ie++)
+    for (int c = 0; c < 9; c++) {
+      int slot = ijp[(size_t)9 * ie + c];
+      P.slot_src[fillp[slot]++] = 9 * ie + c;
+    }
+  std::vector<int> ic(nkn, 0);
+  for (int ie = 0; ie < nel; ie++)
+    for (int ii = 0; ii < 3; ii++) ic[nv[3 * ie + ii]]++;
+  P.inc_ptr.assign(nkn + 1, 0);
+  for (int k = 0; k < nkn; k++) P.inc_ptr[k + 1] = P.inc_ptr[k] + ic[k];
+  P.inc.assign(P.inc_ptr[nkn], 0);
+  std::vector<int> fi(P.inc_ptr.begin(), P.inc_ptr.end() - 1);
+  for (int ie = 0; ie < nel; ie++)
+    for (int ii = 0; ii < 3; ii++) P.inc[fi[nv[3 * ie + ii]]++] = 3 * ie + ii;
+  return SHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// device allocation helpers
+// ---------------------------------------------------------------------------
+struct Arena {
+  std::vector<void *> ptrs;
+  int64_t bytes = 0;
+  template <typename T>
+  int alloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) return fail(SHY_ECAPACITY, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
+    cudaMemset(*p, 0, n * sizeof(T));
+    ptrs.push_back(*p);
+    bytes += (int64_t)(n * sizeof(T));
+    return SHY_OK;
+  }
+  template <typename T>
+  int upload(T **p, const std::vector<T> &h) {
+    int st = alloc(p, h.size());
+    if (st) return st;
+    if (!h.empty()) {
+      cudaError_t e = cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) return fail(SHY_ECUDA, "upload: %s", cudaGetErrorString(e));
+    }
+    return SHY_OK;
+  }
+  void release() {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+    bytes = 0;
+  }
+};
+
+#define ST_TRY(x)            \
+  do {                       \
+    int _s = (x);            \
+    if (_s) return _s;       \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// the model
+// ---------------------------------------------------------------------------
+struct shygpu_model {
+  int nbasin = 0, NKN = 0, NEL = 0, NLV = 0, S = 1, nsc_max = 0, NNZ = 0;
+  bool cor = false;
+  std::vector<BasinPar> par;
+  std::vector<int> nlv_b;
+  Arena arena;
+  Dev base{};                        // static pointers
+  int *kbas = nullptr;               // node -> basin
+  float *zbuf[2], *zebuf[2], *ubuf[2], *vbuf[2], *hkbuf[2], *hebuf[2], *scbuf[2];
+  int cur = 0, sc_cur = 0;
+  cudaStream_t stream = nullptr;
+  // options
+  int nsub = 2, use_graph = 1, CL = 8, zthreads = 1024, max_outer = 12, sym = 1;
+  float inner_rtol = 1e-4f;
+  // graphs keyed by (cur, sc_cur)
+  cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+  int launches_per_step = 0;
+  bool state_set = false;
+  std::vector<BasinOut> out_h;
+};
+
+static int64_t device_launches(const void *mv) {
+  const shygpu_model *m = (const shygpu_model *)mv;
+  unsigned long long n = 0;
+  if (m->base.nsub_launched && m->stream) {
+    cudaStreamSynchronize(m->stream);
+    cudaMemcpy(&n, m->base.nsub_launched, sizeof n, cudaMemcpyDeviceToHost);
+  }
+  return (int64_t)n;
+}
+
+static void drop_graphs(shygpu_model *m) {
+  for (int a = 0; a < 2; a++)
+    for (int b = 0; b < 2; b++)
+      if (m->graph[a][b]) { cudaGraphExecDestroy(m->graph[a][b]); m->graph[a][b] = nullptr; }
+}
+
+static Dev dev_for_step(const shygpu_model *m, int newi) {
+  Dev d = m->base;
+  int oldi = 1 - newi;
+  d.zn = m->zbuf[newi]; d.zo = m->zbuf[oldi];
+  d.zen = m->zebuf[newi]; d.zeo = m->zebuf[oldi];
+  d.un = m->ubuf[newi]; d.uo = m->ubuf[oldi];
+  d.vn = m->vbuf[newi]; d.vo = m->vbuf[oldi];
+  d.hkn = m->hkbuf[newi]; d.hko = m->hkbuf[oldi];
+  d.hen = m->hebuf[newi]; d.heo = m->hebuf[oldi];
+  return d;
+}
+
+static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P, int *NLVo) {
+  int64_t nkn = 0, nel = 0, NLV = 1, nnz = 0, nsc = 0;
+  for (int b = 0; b < nbasin; b++) {
+    nkn += B[b].nkn; nel += B[b].nel;
+    NLV = std::max<int64_t>(NLV, B[b].nlv);
+    nnz += 7LL * B[b].nkn + 16;
+    nsc = std::max<int64_t>(nsc, (P[b].itemp ? 1 : 0) + (P[b].isalt ? 1 : 0) + std::max(0, P[b].nconz));
+  }
+  if (NLVo) *NLVo = (int)NLV;
+  int64_t el = nel * (4 * 16 + 8 * 4 + 12 * 4 + 4 * 4 + NLV * 4 * (2 * 2 + 2 * 1 + 2 + 1 + 2 + 1)) ;
+  int64_t nd = nkn * (4 * 12 + 8 * 6 + NLV * 4 * (2 + 1 + 1) + (NLV + 1) * 4 * 3 + nsc * NLV * 4 * 3);
+  int64_t sy = nnz * (4 + 8 + 4 + 4 * 3);
+  return el + nd + sy;
+}
+
+extern "C" int64_t shygpu_footprint(int32_t nbasin, const shy_basin *basins, const shy_params *params) {
+  if (nbasin <= 0 || !basins || !params) return -1;
+  return footprint_of(nbasin, basins, params, nullptr);
+}
+
+extern "C" int64_t shygpu_model_bytes(const shygpu_model *m) { return m ? m->arena.bytes : -1; }
+
+extern "C" int shygpu_destroy(shygpu_model *m) {
+  if (!m) return SHY_OK;
+  auto it = std::find(g_models.begin(), g_models.end(), (const void *)m);
+  if (it != g_models.end()) {
+    g_launches += device_launches(m);
+    g_models.erase(it);
+  }
+  drop_graphs(m);
+  m->arena.release();
+  if (m->stream) cudaStreamDestroy(m->stream);
+  delete m;
+  return SHY_OK;
+}
+
+// A cluster shape is used only after the occupancy query says that at least
+// one such cluster fits the device (clusters above 8 CTAs need the
+// non-portable attribute set first).
+static int check_cluster_shape(int CL, int threads) {
+  if (CL > 8) {
+    cudaError_t e = zeta_kernel_setup(CL);
+    if (e != cudaSuccess) return fail(SHY_EARG, "cluster size %d not available: %s", CL, cudaGetErrorString(e));
+  }
+  int n = zeta_max_active_clusters(CL, threads);
+  if (n < 1) return fail(SHY_EARG, "a cluster of %d CTAs x %d threads does not fit the device", CL, threads);
+  return SHY_OK;
+}
+
+static int next_pow2(int n) {
+  int s = 1;
+  while (s < n) s <<= 1;
+  return s;
+}
+
+extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_params *Pp,
+                             shygpu_model **out) {
+  if (!out) return fail(SHY_EARG, "create: model pointer is NULL");
+  *out = nullptr;
+  if (nbasin <= 0 || !B || !Pp) return fail(SHY_EARG, "create: no basins");
+  ST_TRY(device_ok());
+  shygpu_model *m = new shygpu_model();
+  auto bail = [&](int st) { shygpu_destroy(m); return st; };
+  int NLV = 1;
+  for (int b = 0; b < nbasin; b++) {
+    const shy_basin &bs = B[b];
+    if (bs.nkn < 3 || bs.nel < 1 || bs.nlv < 1) return bail(fail(SHY_EARG, "basin %d: empty mesh", b));
+    if (bs.nlv > SHY_MAX_LAYERS) return bail(fail(SHY_EARG, "basin %d: nlv=%d above %d", b, bs.nlv, SHY_MAX_LAYERS));
+    if (!bs.nen3v || !bs.xgv || !bs.ygv || !bs.hm3v || !bs.hlv || !bs.hldv || !bs.ilhv || !bs.ilhkv)
+      return bail(fail(SHY_EARG, "basin %d: missing mesh arrays", b));
+    if (bs.ntide > SHY_MAX_TIDE) return bail(fail(SHY_EARG, "basin %d: ntide above %d", b, SHY_MAX_TIDE));
+    if (Pp[b].nconz < 0 || Pp[b].nconz > SHY_MAX_CONZ) return bail(fail(SHY_EARG, "basin %d: nconz", b));
+    if (Pp[b].ireib != 0 && Pp[b].ireib != 5) return bail(fail(SHY_EARG, "basin %d: ireib=%d not supported (0 or 5)", b, Pp[b].ireib));
+    if (Pp[b].ilin == 0) return bail(fail(SHY_EARG, "basin %d: non-linear momentum (ilin=0) not supported", b));
+    if (!(Pp[b].dt > 0)) return bail(fail(SHY_EARG, "basin %d: dt must be positive", b));
+    NLV = std::max(NLV, bs.nlv);
+  }
+  m->nbasin = nbasin; m->NLV = NLV; m->S = next_pow2(NLV);
+  m->par.resize(nbasin);
+  m->nlv_b.resize(nbasin);
+  int NKN = 0, NEL = 0;
+  for (int b = 0; b < nbasin; b++) { NKN += B[b].nkn; NEL += B[b].nel; }
+  m->NKN = NKN; m->NEL = NEL;
+
+  std::vector<int4> enode(NEL);
+  std::vector<float> ev8((size_t)8 * NEL), czv(NEL), fcorv(NEL), wdif((size_t)9 * NEL);
+  std::vector<float4> hm3v(NEL);
+  std::vector<int> ilhv(NEL), ilhkv(NKN), ieltv((size_t)3 * NEL), kbnd(NKN), kbas(NKN);
+  std::vector<float> difhv((size_t)NEL * NLV, 1.f);
+  std::vector<float> visv((size_t)NKN * (NLV + 1), 0.f), difv((size_t)NKN * (NLV + 1), 0.f);
+  std::vector<float> taux(NKN), tauy(NKN), ppv(NKN), rqv(NKN), areakv((size_t)NKN * NLV, 0.f);
+  std::vector<float> hlv((size_t)nbasin * NLV, 0.f), hldv((size_t)nbasin * NLV, 0.f), tide;
+  std::vector<int> rowptr(1, 0), col, slot_ptr(1, 0), slot_src, inc_ptr(1, 0), inc;
+  int k0 = 0, e0 = 0;
+  int nsc_max = 0;
+  for (int b = 0; b < nbasin; b++) {
+    const shy_basin &bs = B[b];
+    const shy_params &p = Pp[b];
+    const int nkn = bs.nkn, nel = bs.nel, nlv = bs.nlv;
+    m->nlv_b[b] = nlv;
+    std::vector<double> ev;
+    ST_TRY(compute_ev(nkn, nel, bs.nen3v, bs.xgv, bs.ygv, ev));
+    std::vector<int> nv((size_t)3 * nel);
+    for (size_t i = 0; i < nv.size(); i++) nv[i] = bs.nen3v[i] - 1;
+    for (int ie = 0; ie < nel; ie++) {
+      const double *e = &ev[(size_t)ie * SHY_EVDIM];
+      int ge = e0 + ie;
+      enode[ge] = make_int4(k0 + nv[3 * ie], k0 + nv[3 * ie + 1], k0 + nv[3 * ie + 2], b);
+      for (int j = 0; j < 6; j++) ev8[(size_t)8 * ge + j] = (float)e[3 + j];
+      ev8[(size_t)8 * ge + 6] = (float)e[9];
+      ev8[(size_t)8 * ge + 7] = 0.f;
+      double h1 = bs.hm3v[3 * ie], h2 = bs.hm3v[3 * ie + 1], h3 = bs.hm3v[3 * ie + 2];
+      hm3v[ge] = make_float4((float)h1, (float)h2, (float)h3, (float)((h1 + h2 + h3) / 3.));
+      int il = bs.ilhv[ie];
+      if (il < 1 || il > nlv) return bail(fail(SHY_EARG, "basin %d: ilhv(%d)=%d outside 1..%d", b, ie + 1, il, nlv));
+      ilhv[ge] = il;
+      czv[ge] = bs.czv ? bs.czv[ie] : 0.f;
+      fcorv[ge] = bs.fcorv ? bs.fcorv[ie] : 0.f;
+      if (fcorv[ge] != 0.f) m->cor = true;
+      // diffweight, idtype = 2 (diffusion_admin.f90:178-330)
+      double bc[3][3] = {{0}};
+      for (int i = 0; i < 3; i++) {
+        int ia = (i + 1) % 3, ib = (i + 2) % 3;
+        double w = 1. / (e[13 + i] * e[13 + i]) * (2. / 3.);
+        bc[ia][ib] = -w; bc[ib][ia] = -w;
+      }
+      for (int ii = 0; ii < 3; ii++) {
+        double w = 0.;
+        for (int iii = 0; iii < 3; iii++) w += bc[ii][iii];
+        bc[ii][ii] = -w;
+      }
+      for (int ii = 0; ii < 3; ii++)
+        for (int iii = 0; iii < 3; iii++) wdif[(size_t)9 * ge + 3 * ii + iii] = (float)bc[ii][iii];
+    }
+    // element neighbours
+    {
+      std::vector<std::vector<int>> incl(nkn);
+      for (int ie = 0; ie < nel; ie++)
+        for (int ii = 0; ii < 3; ii++) incl[nv[3 * ie + ii]].push_back(ie);
+      for (int ie = 0; ie < nel; ie++)
+        for (int ii = 0; ii < 3; ii++) {
+          int k1 = nv[3 * ie + (ii + 1) % 3], k2 = nv[3 * ie + (ii + 2) % 3];
+          int nb = -1;
+          for (int je : incl[k1]) {
+            if (je == ie) continue;
+            if (nv[3 * je] == k2 || nv[3 * je + 1] == k2 || nv[3 * je + 2] == k2) { nb = je; break; }
+          }
+          ieltv[(size_t)3 * (e0 + ie) + ii] = nb < 0 ? -1 : e0 + nb;
+        }
+    }
+    for (int k = 0; k < nkn; k++) {
+      int gk = k0 + k;
+      int il = bs.ilhkv[k];
+      if (il < 1 || il > nlv) return bail(fail(SHY_EARG, "basin %d: ilhkv(%d)=%d outside 1..%d", b, k + 1, il, nlv));
+      ilhkv[gk] = il;
+      kbas[gk] = b;
+      int kb = bs.bnd_index ? bs.bnd_index[k] : 0;
+      if (kb < 0 || kb > bs.nbnd) return bail(fail(SHY_EARG, "basin %d: bnd_index(%d)=%d outside 0..%d", b, k + 1, kb, bs.nbnd));
+      kbnd[gk] = kb;
+      taux[gk] = bs.tauxnv ? bs.tauxnv[k] : 0.f;
+      tauy[gk] = bs.tauynv ? bs.tauynv[k] : 0.f;
+      ppv[gk] = bs.ppv ? bs.ppv[k] : 0.f;
+      rqv[gk] = bs.rqv ? bs.rqv[k] : 0.f;
+      for (int l = 0; l <= nlv; l++) {
+        visv[(size_t)gk * (NLV + 1) + l] = bs.visv ? bs.visv[(size_t)k * (nlv + 1) + l] : 0.f;
+        difv[(size_t)gk * (NLV + 1) + l] = bs.difv ? bs.difv[(size_t)k * (nlv + 1) + l] : 0.f;
+      }
+    }
+    // set_area (elems_dealing.f90:658-705)
+    {
+      std::vector<double> ak((size_t)nkn * nlv, 0.);
+      for (int ie = 0; ie < nel; ie++) {
+        double areafv = 12. * ev[(size_t)ie * SHY_EVDIM + 9] / 3.;
+        for (int ii = 0; ii < 3; ii++) {
+          int k = nv[3 * ie + ii];
+          if (bs.ilhv[ie] > bs.ilhkv[k]) return bail(fail(SHY_EARG, "basin %d: ilhv(%d) above ilhkv of its node", b, ie + 1));
+          for (int l = 0; l < bs.ilhv[ie]; l++) ak[(size_t)k * nlv + l] += areafv;
+        }
+      }
+      for (int k = 0; k < nkn; k++)
+        for (int l = 0; l < nlv; l++) areakv[(size_t)(k0 + k) * NLV + l] = (float)ak[(size_t)k * nlv + l];
+    }
+    for (int l = 0; l < nlv; l++) { hlv[(size_t)b * NLV + l] = bs.hlv[l]; hldv[(size_t)b * NLV + l] = bs.hldv[l]; }
+    // pattern + gather maps, shifted to global numbering
+    Pattern pt;
+    ST_TRY(build_pattern(nkn, nel, nv.data(), pt));
+    int nnz0 = (int)col.size(), src0 = (int)slot_src.size(), inc0 = (int)inc.size();
+    for (int k = 0; k < nkn; k++) rowptr.push_back(nnz0 + pt.rowptr[k + 1]);
+    for (int c : pt.col) col.push_back(k0 + c);
+    for (size_t s = 0; s + 1 < pt.slot_ptr.size(); s++) slot_ptr.push_back(src0 + pt.slot_ptr[s + 1]);
+    for (int v : pt.slot_src) slot_src.push_back(9 * e0 + v);
+    for (int k = 0; k < nkn; k++) inc_ptr.push_back(inc0 + pt.inc_ptr[k + 1]);
+    for (int v : pt.inc) inc.push_back(3 * e0 + v);
+    // parameters
+    BasinPar &bp = m->par[b];
+    memset(&bp, 0, sizeof bp);
+    bp.dt = p.dt; bp.dtime0 = p.dtime0;
+    bp.az = p.azpar; bp.am = p.ampar; bp.af = p.afpar; bp.at = p.atpar; bp.ad = p.adpar; bp.aa = p.aapar;
+    bp.grav = p.grav; bp.rowass = p.rowass; bp.vismol = p.vismol; bp.difmol = p.difmol;
+    bp.hzoff = p.hzoff; bp.ahpar = p.ahpar; bp.rstol = p.rstol > 0 ? p.rstol : 1.f;
+    bp.ireib = p.ireib; bp.ibarcl = p.ibarcl;
+    bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
+    int ns = 0;
+    if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }
+    if (bp.isalt) { bp.rkpar[ns] = p.shpar; bp.is_temp[ns] = 0; ns++; }
+    for (int c = 0; c < p.nconz; c++) { bp.rkpar[ns] = p.chpar; bp.is_temp[ns] = 0; ns++; }
+    bp.nsc = ns;
+    nsc_max = std::max(nsc_max, ns);
+    bp.istot_max = p.istot_max > 0 ? p.istot_max : 1000;
+    bp.k0 = k0; bp.nk = nkn; bp.e0 = e0; bp.ne = nel; bp.nlv = nlv;
+    bp.tide_off = (int)tide.size(); bp.ntide = bs.ntide;
+    for (int i = 0; i < 4 * bs.ntide * bs.nbnd; i++) tide.push_back(bs.tide[i]);
+    bp.rtol = p.solver_rtol > 0 ? p.solver_rtol : 1e-8f;
+    bp.atol = p.solver_atol > 0 ? p.solver_atol : 1e-8f;
+    bp.maxit = p.solver_maxit > 0 ? p.solver_maxit : 1000;
+    bp.has_cor = 0;
+    for (int ie = 0; ie < nel; ie++) bp.has_cor |= fcorv[e0 + ie] != 0.f;
+    k0 += nkn; e0 += nel;
+  }
+  m->nsc_max = nsc_max;
+  m->NNZ = (int)col.size();
+  if (m->cor) m->sym = 0;          // Coriolis makes the zeta system non-symmetric
+
+  // ---- device upload ----
+  Arena &A = m->arena;
+  Dev &d = m->base;
+  d.nbasin = nbasin; d.NKN = NKN; d.NEL = NEL; d.NLV = NLV; d.S = m->S; d.nsc_max = nsc_max;
+  ST_TRY(A.upload(&d.par, m->par) ? bail(SHY_ECAPACITY) : 0);
+  std::vector<BasinOut> outs(nbasin);
+  memset(outs.data(), 0, sizeof(BasinOut) * nbasin);
+  for (int b = 0; b < nbasin; b++) outs[b].dtime = Pp[b].dtime0;
+  if (A.upload(&d.out, outs) || A.upload(&d.enode, enode) || A.upload(&d.ev8, ev8) ||
+      A.upload(&d.hm3v, hm3v) || A.upload(&d.ilhv, ilhv) || A.upload(&d.ilhkv, ilhkv) ||
+      A.upload(&d.czv, czv) || A.upload(&d.fcorv, fcorv) || A.upload(&d.ieltv, ieltv) ||
+      A.upload(&d.wdif, wdif) || A.upload(&d.difhv, difhv) || A.upload(&d.kbnd, kbnd) ||
+      A.upload(&d.tide, tide) || A.upload(&d.visv, visv) || A.upload(&d.difv, difv) ||
+      A.upload(&d.taux, taux) || A.upload(&d.tauy, tauy) || A.upload(&d.ppv, ppv) ||
+      A.upload(&d.rqv, rqv) || A.upload(&d.hlv, hlv) || A.upload(&d.hldv, hldv) ||
+      A.upload(&d.areakv, areakv) || A.upload(&d.rowptr, rowptr) || A.upload(&d.col, col) ||
+      A.upload(&d.slot_ptr, slot_ptr) || A.upload(&d.slot_src, slot_src) ||
+      A.upload(&d.inc_ptr, inc_ptr) || A.upload(&d.inc, inc) || A.upload(&m->kbas, kbas))
+    return bail(SHY_ECAPACITY);
+  const size_t nnz = col.size(), EL = (size_t)NEL * NLV, NL = (size_t)NKN * NLV;
+  const size_t NSC = (size_t)std::max(nsc_max, 1) * NL;
+  if (A.alloc(&d.val64, nnz) || A.alloc(&d.rhs64, NKN) || A.alloc(&d.x64, NKN) ||
+      A.alloc(&d.val32, nnz) || A.alloc(&d.dinv32, NKN) || A.alloc(&d.r32, NKN) ||
+      A.alloc(&d.p32, NKN) || A.alloc(&d.q32, NKN) || A.alloc(&d.z32, NKN) ||
+      A.alloc(&d.e32, NKN) || A.alloc(&d.s32, NKN) || A.alloc(&d.t32, NKN) ||
+      A.alloc(&d.rh32, NKN) || A.alloc(&d.v32, NKN) || A.alloc(&d.hia, (size_t)9 * NEL) ||
+      A.alloc(&d.hik, (size_t)3 * NEL) || A.alloc(&d.unv, NEL) || A.alloc(&d.vnv, NEL) ||
+      A.alloc(&d.wl, (size_t)NKN * (NLV + 1)) || A.alloc(&d.rho, NL) || A.alloc(&d.ddx, EL) ||
+      A.alloc(&d.ddxi, m->cor ? EL : 1) || A.alloc(&d.cbnd, NSC) || A.alloc(&d.vol_node, NKN) ||
+      A.alloc(&d.scr0, nsc_max > 0 ? NSC : 1) || A.alloc(&d.scr1, nsc_max > 0 ? NSC : 1) ||
+      A.alloc(&d.imax, 1) || A.alloc(&d.subj, 1) || A.alloc(&d.nsub_launched, 1) ||
+      A.alloc(&d.stab_node, 1))
+    return bail(SHY_ECAPACITY);
+  for (int i = 0; i < 2; i++) {
+    if (A.alloc(&m->zbuf[i], NKN) || A.alloc(&m->zebuf[i], (size_t)3 * NEL) ||
+        A.alloc(&m->ubuf[i], EL) || A.alloc(&m->vbuf[i], EL) || A.alloc(&m->hkbuf[i], NL) ||
+        A.alloc(&m->hebuf[i], EL) || A.alloc(&m->scbuf[i], NSC))
+      return bail(SHY_ECAPACITY);
+  }
+  if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(SHY_ECUDA, "stream creation failed"));
+  // zeta solver launch shape: one cluster per basin
+  int maxn = 0;
+  for (int b = 0; b < nbasin; b++) maxn = std::max(maxn, B[b].nkn);
+  m->CL = maxn >= 16384 ? 8 : (maxn >= 4096 ? 4 : (maxn >= 1024 ? 2 : 1));
+  m->zthreads = maxn >= 4096 ? 1024 : 512;
+  {
+    int st = check_cluster_shape(m->CL, m->zthreads);
+    if (st) return bail(st);
+  }
+  m->out_h.resize(nbasin);
+  g_models.push_back(m);
+  *out = m;
+  return SHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// options
+// ---------------------------------------------------------------------------
+extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value) {
+  if (!m || !name) return fail(SHY_EARG, "set_option: bad arguments");
+  std::string n(name);
+  int iv = (int)value;
+  if (n == "use_graph") m->use_graph = iv != 0;
+  else if (n == "cluster_size" || n == "zeta_threads") {
+    int CL = m->CL, th = m->zthreads;
+    if (n == "cluster_size") {
+      if (iv < 1 || iv > 16 || (iv & (iv - 1))) return fail(SHY_EARG, "cluster_size: power of two 1..16");
+      CL = iv;
+    } else {
+      if (iv < 64 || iv > 1024 || iv % 32) return fail(SHY_EARG, "zeta_threads: multiple of 32 in 64..1024");
+      th = iv;
+    }
+    ST_TRY(check_cluster_shape(CL, th));
+    m->CL = CL; m->zthreads = th;
+  }
+  else if (n == "inner_rtol") { if (!(value > 0 && value < 1)) return fail(SHY_EARG, "inner_rtol in (0,1)"); m->inner_rtol = (float)value; }
+  else if (n == "max_outer") { if (iv < 1 || iv > 100) return fail(SHY_EARG, "max_outer 1..100"); m->max_outer = iv; }
+  else if (n == "symmetric") { if (iv && m->cor) return fail(SHY_EARG, "Coriolis: the system is not symmetric"); m->sym = iv != 0; }
+  else return fail(SHY_EARG, "unknown option '%s'", name);
+  drop_graphs(m);
+  return SHY_OK;
+}
+
+extern "C" double shygpu_get_option(shygpu_model *m, const char *name) {
+  if (!m || !name) return -1;
+  std::string n(name);
+  if (n == "use_graph") return m->use_graph;
+  if (n == "cluster_size") return m->CL;
+  if (n == "zeta_threads") return m->zthreads;
+  if (n == "inner_rtol") return m->inner_rtol;
+  if (n == "max_outer") return m->max_outer;
+  if (n == "symmetric") return m->sym;
+  if (n == "launches_per_step") return m->launches_per_step;
+  return -1;
+}
+
+// ---------------------------------------------------------------------------
+// state transfer (reference layouts <-> device layout)
+// ---------------------------------------------------------------------------
+static int copy_cols(float *dev, const float *host, int n, int nlv, int NLV, int off, bool to_dev,
+                     cudaStream_t st) {
+  // host (n, nlv) rows  <->  device rows [off + i][NLV]
+  cudaError_t e;
+  if (to_dev)
+    e = cudaMemcpy2DAsync(dev + (size_t)off * NLV, (size_t)NLV * 4, host, (size_t)nlv * 4, (size_t)nlv * 4, n,
+                          cudaMemcpyHostToDevice, st);
+  else
+    e = cudaMemcpy2DAsync((void *)host, (size_t)nlv * 4, dev + (size_t)off * NLV, (size_t)NLV * 4, (size_t)nlv * 4, n,
+                          cudaMemcpyDeviceToHost, st);
+  if (e != cudaSuccess) return fail(SHY_ECUDA, "state copy: %s", cudaGetErrorString(e));
+  return SHY_OK;
+}
+
+static int scalar_index(const BasinPar &bp, int which, int c) {
+  // which: 0 temp, 1 salt, 2 tracer c
+  if (which == 0) return bp.itemp ? 0 : -1;
+  if (which == 1) return bp.isalt ? (bp.itemp ? 1 : 0) : -1;
+  return bp.itemp + bp.isalt + c;
+}
+
+extern "C" int shygpu_set_state(shygpu_model *m, int32_t ib, const shy_state *s) {
+  if (!m || !s || ib < 0 || ib >= m->nbasin) return fail(SHY_EARG, "set_state: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  const int NLV = m->NLV, nlv = bp.nlv;
+  cudaStream_t st = m->stream;
+  const int c = m->cur;
+  drop_graphs(m);
+  if (s->znv) CUDA_TRY(cudaMemcpyAsync(m->zbuf[c] + bp.k0, s->znv, (size_t)bp.nk * 4, cudaMemcpyHostToDevice, st));
+  if (s->utlnv) ST_TRY(copy_cols(m->ubuf[c], s->utlnv, bp.ne, nlv, NLV, bp.e0, true, st));
+  if (s->vtlnv) ST_TRY(copy_cols(m->vbuf[c], s->vtlnv, bp.ne, nlv, NLV, bp.e0, true, st));
+  const size_t SN = (size_t)m->NKN * NLV;
+  int iT = scalar_index(bp, 0, 0), iS = scalar_index(bp, 1, 0);
+  if (iT >= 0 && s->tempv) ST_TRY(copy_cols(m->scbuf[m->sc_cur] + iT * SN, s->tempv, bp.nk, nlv, NLV, bp.k0, true, st));
+  if (iS >= 0 && s->saltv) ST_TRY(copy_cols(m->scbuf[m->sc_cur] + iS * SN, s->saltv, bp.nk, nlv, NLV, bp.k0, true, st));
+  if (s->conzv)
+    for (int cc = 0; cc < bp.nsc - bp.itemp - bp.isalt; cc++)
+      ST_TRY(copy_cols(m->scbuf[m->sc_cur] + scalar_index(bp, 2, cc) * SN, s->conzv + (size_t)cc * bp.nk * nlv,
+                       bp.nk, nlv, NLV, bp.k0, true, st));
+  // boundary values of the scalars: the initial columns
+  for (int sc = 0; sc < bp.nsc; sc++)
+    CUDA_TRY(cudaMemcpyAsync(m->base.cbnd + sc * SN + (size_t)bp.k0 * NLV, m->scbuf[m->sc_cur] + sc * SN + (size_t)bp.k0 * NLV,
+                             (size_t)bp.nk * NLV * 4, cudaMemcpyDeviceToDevice, st));
+  // derived state: zenv (setzev), layer thickness (setdepth), rho (barocl(0))
+  Dev d = dev_for_step(m, c);
+  d.sc_in = m->scbuf[m->sc_cur];
+  launch_elem(d, 1, 1, st, m->cor);
+  launch_node(d, m->kbas, 0, 1, 0, st);
+  launch_reduce(d, m->nsub, 0, st);
+  if (m->nsc_max > 0) launch_node(d, m->kbas, 3, 0, 0, st);
+  g_launches += 3 + (m->nsc_max > 0);
+  CUDA_TRY(cudaStreamSynchronize(st));
+  CUDA_TRY(cudaGetLastError());
+  std::vector<BasinOut> o(m->nbasin);
+  CUDA_TRY(cudaMemcpy(o.data(), m->base.out, sizeof(BasinOut) * m->nbasin, cudaMemcpyDeviceToHost));
+  if (o[ib].status) return fail(o[ib].status, "set_state: basin %d invalid initial state (%s)", ib,
+                                o[ib].status == SHY_EDEPTH ? "non-positive layer thickness" : "error");
+  m->state_set = true;
+  return SHY_OK;
+}
+
+extern "C" int shygpu_get_state(shygpu_model *m, int32_t ib, shy_state *s) {
+  if (!m || !s || ib < 0 || ib >= m->nbasin) return fail(SHY_EARG, "get_state: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  const int NLV = m->NLV, nlv = bp.nlv, c = m->cur;
+  cudaStream_t st = m->stream;
+  CUDA_TRY(cudaStreamSynchronize(st));
+  if (s->znv) CUDA_TRY(cudaMemcpyAsync(s->znv, m->zbuf[c] + bp.k0, (size_t)bp.nk * 4, cudaMemcpyDeviceToHost, st));
+  if (s->zenv) CUDA_TRY(cudaMemcpyAsync(s->zenv, m->zebuf[c] + 3 * (size_t)bp.e0, (size_t)bp.ne * 12, cudaMemcpyDeviceToHost, st));
+  if (s->utlnv) ST_TRY(copy_cols(m->ubuf[c], s->utlnv, bp.ne, nlv, NLV, bp.e0, false, st));
+  if (s->vtlnv) ST_TRY(copy_cols(m->vbuf[c], s->vtlnv, bp.ne, nlv, NLV, bp.e0, false, st));
+  if (s->unv) CUDA_TRY(cudaMemcpyAsync(s->unv, m->base.unv + bp.e0, (size_t)bp.ne * 4, cudaMemcpyDeviceToHost, st));
+  if (s->vnv) CUDA_TRY(cudaMemcpyAsync(s->vnv, m->base.vnv + bp.e0, (size_t)bp.ne * 4, cudaMemcpyDeviceToHost, st));
+  if (s->hdknv) ST_TRY(copy_cols(m->hkbuf[c], s->hdknv, bp.nk, nlv, NLV, bp.k0, false, st));
+  if (s->hdenv) ST_TRY(copy_cols(m->hebuf[c], s->hdenv, bp.ne, nlv, NLV, bp.e0, false, st));
+  if (s->wlnv) ST_TRY(copy_cols(m->base.wl, s->wlnv, bp.nk, nlv + 1, NLV + 1, bp.k0, false, st));
+  if (s->rhov) ST_TRY(copy_cols(m->base.rho, s->rhov, bp.nk, nlv, NLV, bp.k0, false, st));
+  const size_t SN = (size_t)m->NKN * NLV;
+  int iT = scalar_index(bp, 0, 0), iS = scalar_index(bp, 1, 0);
+  if (iT >= 0 && s->tempv) ST_TRY(copy_cols(m->scbuf[m->sc_cur] + iT * SN, s->tempv, bp.nk, nlv, NLV, bp.k0, false, st));
+  if (iS >= 0 && s->saltv) ST_TRY(copy_cols(m->scbuf[m->sc_cur] + iS * SN, s->saltv, bp.nk, nlv, NLV, bp.k0, false, st));
+  if (s->conzv)
+    for (int cc = 0; cc < bp.nsc - bp.itemp - bp.isalt; cc++)
+      ST_TRY(copy_cols(m->scbuf[m->sc_cur] + scalar_index(bp, 2, cc) * SN, s->conzv + (size_t)cc * bp.nk * nlv,
+                       bp.nk, nlv, NLV, bp.k0, false, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return SHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// the step
+// ---------------------------------------------------------------------------
+static int enqueue_hydro(shygpu_model *m, const Dev &d) {
+  launch_elem(d, 0, 0, m->stream, m->cor);
+  ZetaArgs za{};
+  za.zguess = d.zo; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
+  za.explicit_mode = 0; za.inner_rtol = m->inner_rtol; za.max_outer = m->max_outer; za.sym = m->sym;
+  cudaError_t e = launch_zeta(d, za, m->CL, m->zthreads, 0, m->nbasin, m->stream);
+  if (e != cudaSuccess) return fail(SHY_ECUDA, "zeta solve launch: %s", cudaGetErrorString(e));
+  launch_elem(d, 1, 0, m->stream, m->cor);
+  launch_node(d, m->kbas, 0, 0, 0, m->stream);
+  return SHY_OK;
+}
+
+// stability index and per-basin reductions (the part of run_scalar before
+// the sub-step loop)
+static void enqueue_scalar_head(shygpu_model *m, const Dev &d) {
+  if (m->nsc_max > 0) launch_node(d, m->kbas, 1, 0, 0, m->stream);   // k_stab
+  launch_reduce(d, 0, 1, m->stream);
+}
+
+// eager sub-step loop: the host reads the step's largest sub-step count
+static int enqueue_scalar(shygpu_model *m, Dev d, int sc_cur, int *nconz) {
+  enqueue_scalar_head(m, d);
+  *nconz = 0;
+  if (m->nsc_max > 0) {
+    int imax = 0;
+    CUDA_TRY(cudaMemcpyAsync(&imax, d.imax, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+    CUDA_TRY(cudaStreamSynchronize(m->stream));
+    d.sc_in = m->scbuf[sc_cur];
+    d.sc_out = m->scbuf[1 - sc_cur];
+    for (int j = 0; j < imax && j < 1000; j++) launch_node(d, m->kbas, 2, j, 0, m->stream);
+    *nconz = imax;
+  }
+  return SHY_OK;
+}
+
+// launches of one step apart from the transport sub-steps
+static int count_launches(const shygpu_model *m) {
+  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0);
+}
+
+static int enqueue_step(shygpu_model *m) {
+  int newi = 1 - m->cur;
+  Dev d = dev_for_step(m, newi);
+  ST_TRY(enqueue_hydro(m, d));
+  int nconz = 0;
+  ST_TRY(enqueue_scalar(m, d, m->sc_cur, &nconz));
+  g_launches += nconz;
+  return SHY_OK;
+}
+
+static void advance_host(shygpu_model *m) {
+  m->cur = 1 - m->cur;
+  if (m->nsc_max > 0) m->sc_cur = 1 - m->sc_cur;
+}
+
+static int check_outputs(shygpu_model *m) {
+  CUDA_TRY(cudaMemcpyAsync(m->out_h.data(), m->base.out, sizeof(BasinOut) * m->nbasin, cudaMemcpyDeviceToHost, m->stream));
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  for (int b = 0; b < m->nbasin; b++) {
+    int s = m->out_h[b].status;
+    if (s) {
+      const char *why = s == SHY_ENOCONV ? "zeta solve did not converge"
+                        : s == SHY_EDEPTH ? "non-positive layer thickness"
+                        : s == SHY_EISTOT ? "transport sub-steps above the limit or the captured sub-step budget (option 'substeps')"
+                        : s == SHY_ESINGULAR ? "zero pivot in a vertical transport system"
+                        : "error";
+      for (int q = 0; q < m->nbasin; q++)
+        cudaMemsetAsync(&m->base.out[q].status, 0, sizeof(int), m->stream);
+      return fail(s, "basin %d at t=%.1f: %s", b, m->out_h[b].dtime, why);
+    }
+  }
+  return SHY_OK;
+}
+
+// One step as a CUDA graph: the hydro kernels and the stability/reduction
+// kernels captured in order, then a conditional WHILE node whose body is one
+// transport sub-step plus the loop control, so the device decides how many
+// sub-steps run (scal3sh's istot) without a host round trip.
+static int build_graph(shygpu_model *m, int cur, int sc_cur) {
+  cudaGraph_t g = nullptr;
+  CUDA_TRY(cudaGraphCreate(&g, 0));
+  auto bail = [&](int st) { cudaGraphDestroy(g); return st; };
+  cudaGraphConditionalHandle h = 0;
+  if (m->nsc_max > 0) {
+    cudaError_t e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "conditional handle: %s", cudaGetErrorString(e)));
+  }
+  int newi = 1 - cur;
+  Dev d = dev_for_step(m, newi);
+  cudaError_t e = cudaStreamBeginCaptureToGraph(m->stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "graph capture: %s", cudaGetErrorString(e)));
+  int st = enqueue_hydro(m, d);
+  if (!st) enqueue_scalar_head(m, d);
+  cudaGraph_t gc = nullptr;
+  e = cudaStreamEndCapture(m->stream, &gc);
+  if (st) return bail(st);
+  if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "graph capture: %s", cudaGetErrorString(e)));
+  if (m->nsc_max > 0) {
+    // the leaf of the captured chain
+    size_t n = 0;
+    CUDA_TRY(cudaGraphGetNodes(g, nullptr, &n));
+    std::vector<cudaGraphNode_t> nodes(n);
+    CUDA_TRY(cudaGraphGetNodes(g, nodes.data(), &n));
+    cudaGraphNode_t leaf = nullptr;
+    for (auto nd : nodes) {
+      size_t nout = 0;
+      CUDA_TRY(cudaGraphNodeGetDependentNodes(nd, nullptr, &nout));
+      if (nout == 0) leaf = nd;
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cnode;
+    e = cudaGraphAddNode(&cnode, g, &leaf, leaf ? 1 : 0, &cp);
+    if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "conditional node: %s", cudaGetErrorString(e)));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(m->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "body capture: %s", cudaGetErrorString(e)));
+    Dev db = d;
+    db.sc_in = m->scbuf[sc_cur];
+    db.sc_out = m->scbuf[1 - sc_cur];
+    launch_node(db, m->kbas, 2, -1, 0, m->stream);    // sub-step index from the device
+    launch_subctl(db, h, m->stream);
+    cudaGraph_t gb = nullptr;
+    e = cudaStreamEndCapture(m->stream, &gb);
+    if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "body capture: %s", cudaGetErrorString(e)));
+  }
+  e = cudaGraphInstantiate(&m->graph[cur][sc_cur], g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return fail(SHY_ECUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  return SHY_OK;
+}
+
+extern "C" int shygpu_enqueue(shygpu_model *m, int32_t nsteps) {
+  if (!m) return fail(SHY_EARG, "enqueue: model is NULL");
+  if (!m->state_set) return fail(SHY_ESTATE, "enqueue: set_state has not been called");
+  if (nsteps < 0) return fail(SHY_EARG, "enqueue: nsteps < 0");
+  m->launches_per_step = count_launches(m);
+  for (int i = 0; i < nsteps; i++) {
+    if (m->use_graph) {
+      if (!m->graph[m->cur][m->sc_cur]) ST_TRY(build_graph(m, m->cur, m->sc_cur));
+      CUDA_TRY(cudaGraphLaunch(m->graph[m->cur][m->sc_cur], m->stream));
+    } else {
+      ST_TRY(enqueue_step(m));
+    }
+    g_launches += m->launches_per_step;
+    advance_host(m);
+  }
+  CUDA_TRY(cudaGetLastError());
+  return SHY_OK;
+}
+
+extern "C" int shygpu_sync(shygpu_model *m) {
+  if (!m) return fail(SHY_EARG, "sync: model is NULL");
+  return check_outputs(m);
+}
+
+extern "C" int shygpu_run(shygpu_model *m, int32_t nsteps) {
+  ST_TRY(shygpu_enqueue(m, nsteps));
+  return check_outputs(m);
+}
+
+// phases at the reference's boundaries (eager launches)
+extern "C" int shygpu_new_step(shygpu_model *m) {
+  if (!m || !m->state_set) return fail(SHY_ESTATE, "new_step: no state");
+  return SHY_OK;     // copy_uvz/copy_depth/sp111 happen inside the next hydro
+}
+
+extern "C" int shygpu_hydro(shygpu_model *m) {
+  if (!m || !m->state_set) return fail(SHY_ESTATE, "hydro: no state");
+  Dev d = dev_for_step(m, 1 - m->cur);
+  ST_TRY(enqueue_hydro(m, d));
+  g_launches += 4;
+  m->cur = 1 - m->cur;
+  CUDA_TRY(cudaGetLastError());
+  return check_outputs(m);
+}
+
+extern "C" int shygpu_scalar(shygpu_model *m) {
+  if (!m || !m->state_set) return fail(SHY_ESTATE, "scalar: no state");
+  Dev d = dev_for_step(m, m->cur);     // the state hydro just produced is "new"
+  int nconz = 0;
+  ST_TRY(enqueue_scalar(m, d, m->sc_cur, &nconz));
+  g_launches += 1 + (m->nsc_max > 0 ? 1 : 0) + nconz;
+  if (m->nsc_max > 0) m->sc_cur = 1 - m->sc_cur;
+  CUDA_TRY(cudaGetLastError());
+  return check_outputs(m);
+}
+
+extern "C" int shygpu_set_forcing(shygpu_model *m, int32_t ib, const float *taux, const float *tauy,
+                                  const float *ppv, const float *rqv) {
+  if (!m || ib < 0 || ib >= m->nbasin) return fail(SHY_EARG, "set_forcing: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  const size_t nb = (size_t)bp.nk * 4;
+  if (taux) CUDA_TRY(cudaMemcpyAsync(m->base.taux + bp.k0, taux, nb, cudaMemcpyHostToDevice, m->stream));
+  if (tauy) CUDA_TRY(cudaMemcpyAsync(m->base.tauy + bp.k0, tauy, nb, cudaMemcpyHostToDevice, m->stream));
+  if (ppv) CUDA_TRY(cudaMemcpyAsync(m->base.ppv + bp.k0, ppv, nb, cudaMemcpyHostToDevice, m->stream));
+  if (rqv) CUDA_TRY(cudaMemcpyAsync(m->base.rqv + bp.k0, rqv, nb, cudaMemcpyHostToDevice, m->stream));
+  return SHY_OK;
+}
+
+extern "C" void *shygpu_model_stream(shygpu_model *m) { return m ? (void *)m->stream : nullptr; }
+
+extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_out, int32_t *count_out) {
+  if (!m || !ms_out || !count_out || nsteps < 1) return fail(SHY_EARG, "profile_steps: bad arguments");
+  if (!m->state_set) return fail(SHY_ESTATE, "profile_steps: set_state has not been called");
+  const int NK = SHY_NKERNEL;
+  for (int i = 0; i < NK; i++) { ms_out[i] = 0.; count_out[i] = 0; }
+  cudaEvent_t ev[32];
+  for (int i = 0; i < 32; i++) CUDA_TRY(cudaEventCreate(&ev[i]));
+  int st = SHY_OK;
+  for (int s = 0; s < nsteps && !st; s++) {
+    Dev d = dev_for_step(m, 1 - m->cur);
+    int kind[32], n = 0;
+    cudaEventRecord(ev[n], m->stream);
+    launch_elem(d, 0, 0, m->stream, m->cor); kind[n] = 0; cudaEventRecord(ev[++n], m->stream);
+    ZetaArgs za{};
+    za.zguess = d.zo; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
+    za.inner_rtol = m->inner_rtol; za.max_outer = m->max_outer; za.sym = m->sym;
+    if (launch_zeta(d, za, m->CL, m->zthreads, 0, m->nbasin, m->stream) != cudaSuccess) { st = fail(SHY_ECUDA, "zeta launch"); break; }
+    kind[n] = 1; cudaEventRecord(ev[++n], m->stream);
+    launch_elem(d, 1, 0, m->stream, m->cor); kind[n] = 2; cudaEventRecord(ev[++n], m->stream);
+    launch_node(d, m->kbas, 0, 0, 0, m->stream); kind[n] = 3; cudaEventRecord(ev[++n], m->stream);
+    if (m->nsc_max > 0) { launch_node(d, m->kbas, 1, 0, 0, m->stream); kind[n] = 4; cudaEventRecord(ev[++n], m->stream); }
+    launch_reduce(d, 0, 1, m->stream); kind[n] = 5; cudaEventRecord(ev[++n], m->stream);
+    if (m->nsc_max > 0) {
+      int imax = 0;
+      CUDA_TRY(cudaMemcpyAsync(&imax, d.imax, sizeof(int), cudaMemcpyDeviceToHost, m->stream));
+      CUDA_TRY(cudaStreamSynchronize(m->stream));
+      cudaEventRecord(ev[n], m->stream);
+      d.sc_in = m->scbuf[m->sc_cur];
+      d.sc_out = m->scbuf[1 - m->sc_cur];
+      for (int j = 0; j < imax && n < 30; j++) {
+        launch_node(d, m->kbas, 2, j, 0, m->stream);
+        kind[n] = 6; cudaEventRecord(ev[++n], m->stream);
+      }
+    }
+    g_launches += n;
+    CUDA_TRY(cudaEventSynchronize(ev[n]));
+    for (int i = 0; i < n; i++) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      ms_out[kind[i]] += ms;
+      count_out[kind[i]] += 1;
+    }
+    advance_host(m);
+  }
+  for (int i = 0; i < 32; i++) cudaEventDestroy(ev[i]);
+  if (st) return st;
+  CUDA_TRY(cudaGetLastError());
+  return check_outputs(m);
+}
+
+extern "C" int shygpu_step_info(shygpu_model *m, int32_t ib, shy_step_info *info) {
+  if (!m || !info || ib < 0 || ib >= m->nbasin) return fail(SHY_EARG, "step_info: bad arguments");
+  BasinOut o;
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  CUDA_TRY(cudaMemcpy(&o, m->base.out + ib, sizeof o, cudaMemcpyDeviceToHost));
+  info->status = o.status;
+  info->krylov_iters = o.iters;
+  info->refinements = o.refinements;
+  info->istot = o.istot;
+  info->resid0 = o.resid0;
+  info->resid = o.resid;
+  info->volume = o.volume;
+  info->dtime = o.dtime;
+  return SHY_OK;
+}
+
+// ===========================================================================
+// simsys: the reference's linear-system interface (simsys_spkaux.f90)
+// ===========================================================================
+shy_zeta_system_t shy_zeta_system;
+
+namespace {
+struct Simsys {
+  bool registered = false, initialized = false, explicit_mode = false;
+  int nkn = 0, nel = 0, nnz = 0;
+  std::vector<int> nv;                // 0-based nen3v
+  Arena arena;
+  Dev d{};
+  float *stage_h = nullptr;           // pinned [nel][12]: hia(3x3 row-major i,j), hik(3)
+  float *stage_d = nullptr;
+  float *z_d = nullptr, *zout_d = nullptr;
+  float dt_rhs = 0.f;
+  std::vector<float> rqv_h;
+  double rtol = 1e-8, atol = 1e-8;
+  int maxit = 1000;
+  int last_iters = 0;
+  cudaStream_t st = nullptr;
+};
+Simsys g_sys;
+
+[[noreturn]] void simsys_stop(const char *where) {
+  // the reference stops the program on solver errors (sparskit_admin.f90:322-325)
+  fprintf(stderr, "error stop %s: %s\n", where, g_err.c_str());
+  fflush(stderr);
+  exit(1);
+}
+}  // namespace
+
+extern "C" int shygpu_simsys_register(int32_t nkn, int32_t nel, const int32_t *nen3v) {
+  if (nkn < 1 || nel < 1 || !nen3v) return fail(SHY_EARG, "simsys_register: bad arguments");
+  g_sys.arena.release();
+  if (g_sys.stage_h) { cudaFreeHost(g_sys.stage_h); g_sys.stage_h = nullptr; }
+  g_sys.nkn = nkn; g_sys.nel = nel;
+  g_sys.nv.resize((size_t)3 * nel);
+  for (size_t i = 0; i < g_sys.nv.size(); i++) {
+    g_sys.nv[i] = nen3v[i] - 1;
+    if (g_sys.nv[i] < 0 || g_sys.nv[i] >= nkn) return fail(SHY_EARG, "simsys_register: node out of range");
+  }
+  g_sys.registered = true;
+  g_sys.initialized = false;
+  return SHY_OK;
+}
+
+extern "C" int shygpu_simsys_set_tolerance(double rtol, double atol, int32_t maxit) {
+  if (!(rtol > 0) || !(atol >= 0) || maxit < 1) return fail(SHY_EARG, "simsys_set_tolerance: bad arguments");
+  g_sys.rtol = rtol; g_sys.atol = atol; g_sys.maxit = maxit;
+  return SHY_OK;
+}
+
+static int simsys_init_impl() {
+  if (!g_sys.registered) return fail(SHY_ESTATE, "system_initialize: call shygpu_simsys_register first");
+  ST_TRY(device_ok());
+  Pattern pt;
+  ST_TRY(build_pattern(g_sys.nkn, g_sys.nel, g_sys.nv.data(), pt));
+  Arena &A = g_sys.arena;
+  Dev &d = g_sys.d;
+  memset(&d, 0, sizeof d);
+  d.nbasin = 1; d.NKN = g_sys.nkn; d.NEL = g_sys.nel; d.NLV = 1; d.S = 1;
+  g_sys.nnz = pt.rowptr[g_sys.nkn];
+  std::vector<BasinPar> par(1);
+  memset(par.data(), 0, sizeof(BasinPar));
+  par[0].nk = g_sys.nkn; par[0].ne = g_sys.nel; par[0].nlv = 1;
+  par[0].rtol = (float)g_sys.rtol; par[0].atol = (float)g_sys.atol; par[0].maxit = g_sys.maxit;
+  std::vector<BasinOut> out(1);
+  memset(out.data(), 0, sizeof(BasinOut));
+  const size_t n = g_sys.nkn, nnz = g_sys.nnz;
+  if (A.upload(&d.par, par) || A.upload(&d.out, out) || A.upload(&d.rowptr, pt.rowptr) ||
+      A.upload(&d.col, pt.col) || A.upload(&d.slot_ptr, pt.slot_ptr) ||
+      A.upload(&d.slot_src, pt.slot_src) || A.upload(&d.inc_ptr, pt.inc_ptr) ||
+      A.upload(&d.inc, pt.inc) || A.alloc(&d.val64, nnz) || A.alloc(&d.val32, nnz) ||
+      A.alloc(&d.rhs64, n) || A.alloc(&d.x64, n) || A.alloc(&d.dinv32, n) || A.alloc(&d.r32, n) ||
+      A.alloc(&d.p32, n) || A.alloc(&d.q32, n) || A.alloc(&d.z32, n) || A.alloc(&d.e32, n) ||
+      A.alloc(&d.s32, n) || A.alloc(&d.t32, n) || A.alloc(&d.rh32, n) || A.alloc(&d.v32, n) ||
+      A.alloc(&d.rqv, n) || A.alloc(&g_sys.stage_d, (size_t)12 * g_sys.nel) ||
+      A.alloc(&g_sys.z_d, n) || A.alloc(&g_sys.zout_d, n))
+    return SHY_ECAPACITY;
+  d.zn = g_sys.zout_d;
+  CUDA_TRY(cudaMallocHost((void **)&g_sys.stage_h, sizeof(float) * 12 * g_sys.nel));
+  memset(g_sys.stage_h, 0, sizeof(float) * 12 * g_sys.nel);
+  g_sys.rqv_h.assign(n, 0.f);
+  if (!g_sys.st) CUDA_TRY(cudaStreamCreateWithFlags(&g_sys.st, cudaStreamNonBlocking));
+  g_sys.initialized = true;
+  g_sys.explicit_mode = false;
+  return SHY_OK;
+}
+
+extern "C" void system_initialize_(void) {           // simsys_spkaux.f90:85
+  if (simsys_init_impl()) simsys_stop("system_initialize");
+}
+
+extern "C" void system_init_(void) {                  // :137 zero matrix and rhs
+  if (!g_sys.initialized) { fail(SHY_ESTATE, "system not initialized"); simsys_stop("system_init"); }
+  memset(g_sys.stage_h, 0, sizeof(float) * 12 * g_sys.nel);
+  std::fill(g_sys.rqv_h.begin(), g_sys.rqv_h.end(), 0.f);
+  g_sys.dt_rhs = 0.f;
+}
+
+extern "C" void system_set_explicit_(void) { g_sys.explicit_mode = true; }   // :160
+
+extern "C" void system_assemble_(const int32_t *ie) {   // :533
+  int e = *ie - 1;
+  if (!g_sys.initialized || e < 0 || e >= g_sys.nel) {
+    fail(SHY_EARG, "system_assemble: element %d outside 1..%d", *ie, g_sys.nel);
+    simsys_stop("system_assemble");
+  }
+  for (int i = 0; i < 3; i++)
+    if (shy_zeta_system.kn[i] - 1 != g_sys.nv[3 * e + i]) {
+      fail(SHY_EARG, "system_assemble: kn of element %d differ from the registered nen3v", *ie);
+      simsys_stop("system_assemble");
+    }
+  float *s = g_sys.stage_h + (size_t)12 * e;
+  // accumulate (the reference adds into its COO, an element assembled twice adds twice)
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) s[3 * i + j] += shy_zeta_system.hia[3 * j + i];
+  for (int i = 0; i < 3; i++) s[9 + i] += shy_zeta_system.hik[i];
+  if (g_sys.explicit_mode)
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        if (i != j && shy_zeta_system.hia[3 * j + i] != 0.f) {
+          fail(SHY_EARG, "system_assemble: non diag elems /= 0 in explicit mode");
+          simsys_stop("system_assemble");
+        }
+}
+
+extern "C" void system_add_rhs_(const float *dt, const int32_t *n, const float *array) {   // :687
+  if (!g_sys.initialized || *n != g_sys.nkn) { fail(SHY_EARG, "system_add_rhs: n != nkn"); simsys_stop("system_add_rhs"); }
+  // rvec2d(k) += dt*array(k): several calls add up
+  for (int k = 0; k < *n; k++) g_sys.rqv_h[k] += *dt * array[k];
+  g_sys.dt_rhs = 1.f;
+}
+
+static int simsys_solve_impl(int n, const float *z) {
+  if (!g_sys.initialized) return fail(SHY_ESTATE, "system_solve: not initialized");
+  if (n != g_sys.nkn) return fail(SHY_EARG, "system_solve: n=%d but the system has %d nodes", n, g_sys.nkn);
+  cudaStream_t st = g_sys.st;
+  Dev d = g_sys.d;
+  BasinPar par;
+  memset(&par, 0, sizeof par);
+  par.nk = g_sys.nkn; par.ne = g_sys.nel; par.nlv = 1;
+  par.dt = 1.0;                         // rqv already holds dt*array
+  par.rtol = (float)g_sys.rtol; par.atol = (float)g_sys.atol; par.maxit = g_sys.maxit;
+  CUDA_TRY(cudaMemcpyAsync(d.par, &par, sizeof par, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(&d.out->status, 0, sizeof(int), st));
+  CUDA_TRY(cudaMemcpyAsync(g_sys.stage_d, g_sys.stage_h, sizeof(float) * 12 * g_sys.nel, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(d.rqv, g_sys.rqv_h.data(), sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(g_sys.z_d, z, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+  ZetaArgs za{};
+  za.zguess = g_sys.z_d; za.hia = g_sys.stage_d; za.hik = g_sys.stage_d + 9; za.cs = 1; za.es = 12;
+  za.explicit_mode = g_sys.explicit_mode; za.inner_rtol = 1e-4f; za.max_outer = 12; za.sym = 0;
+  int CL = n >= 16384 ? 8 : (n >= 4096 ? 4 : (n >= 1024 ? 2 : 1));
+  int threads = n >= 4096 ? 1024 : 512;
+  ST_TRY(check_cluster_shape(CL, threads));
+  cudaError_t e = launch_zeta(d, za, CL, threads, 0, 1, st);
+  if (e != cudaSuccess) return fail(SHY_ECUDA, "system_solve launch: %s", cudaGetErrorString(e));
+  g_launches += 1;
+  BasinOut o;
+  CUDA_TRY(cudaMemcpyAsync(&o, d.out, sizeof o, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  g_sys.last_iters = o.iters;
+  if (o.status) return fail(o.status, "system_solve: error solving matrix (status %d)", o.status);
+  return SHY_OK;
+}
+
+extern "C" void system_solve_(const int32_t *n, const float *z) {   // :454
+  if (simsys_solve_impl(*n, z)) simsys_stop("spk_solve_system");
+}
+
+extern "C" void system_get_(const int32_t *n, float *z) {           // :638
+  if (!g_sys.initialized || *n != g_sys.nkn) { fail(SHY_EARG, "system_get: n != nkn"); simsys_stop("system_get"); }
+  if (cudaMemcpy(z, g_sys.zout_d, sizeof(float) * (*n), cudaMemcpyDeviceToHost) != cudaSuccess) {
+    fail(SHY_ECUDA, "system_get: copy failed");
+    simsys_stop("system_get");
+  }
+}
+
+extern "C" void system_finalize_(void) {}                           // :722
+
+extern "C" int shygpu_simsys_iterations(void) { return g_sys.last_iters; }
+
+extern "C" int shygpu_simsys_get_matrix(int32_t *n, int32_t *nnz, int32_t *rowptr, int32_t *col,
+                                        double *val, double *rhs) {
+  if (!g_sys.initialized) return fail(SHY_ESTATE, "simsys_get_matrix: not initialized");
+  if (n) *n = g_sys.nkn;
+  if (nnz) *nnz = g_sys.nnz;
+  if (rowptr) CUDA_TRY(cudaMemcpy(rowptr, g_sys.d.rowptr, sizeof(int) * (g_sys.nkn + 1), cudaMemcpyDeviceToHost));
+  if (col) CUDA_TRY(cudaMemcpy(col, g_sys.d.col, sizeof(int) * g_sys.nnz, cudaMemcpyDeviceToHost));
+  if (val) CUDA_TRY(cudaMemcpy(val, g_sys.d.val64, sizeof(double) * g_sys.nnz, cudaMemcpyDeviceToHost));
+  if (rhs) CUDA_TRY(cudaMemcpy(rhs, g_sys.d.rhs64, sizeof(double) * g_sys.nkn, cudaMemcpyDeviceToHost));
+  return SHY_OK;
+}

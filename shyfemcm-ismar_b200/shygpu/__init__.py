@@ -1,1 +1,304 @@
-"""shygpu: B200 implementation of SHYFEM's semi-implicit step (host side)."""
+"""shygpu: SHYFEM's semi-implicit time step on B200 (host side).
+
+This package is the host-side mirror of the reference's interface for the
+step, over the C ABI of `libshygpu.so` (include/shygpu.h):
+
+* `Model`   -- many basins advanced together on one GPU with device-resident
+               state: `run(nsteps)` is `shyfem_run`'s loop body
+               (src/shyfem/shyfem_subs.f90:569-658), `hydro()` and `scalar()`
+               are its `hydro` / `run_scalar` phases.
+* `Shyfem`  -- shyfem_initialize / shyfem_run / shyfem_finalize for one basin
+               (shyfem_subs.f90:285, 551, 668).
+* `simsys`  -- the reference's linear-system interface (system_initialize,
+               system_init, system_assemble, system_add_rhs, system_solve,
+               system_get; simsys_spkaux.f90:85-722).
+
+There is no CPU fallback: every compute call raises `ShyError` when the
+CUDA library cannot run.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import abi, cases  # noqa: F401
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libshygpu.so"
+
+_lib = None
+
+
+class ShyError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{abi.STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+def lib():
+    """Load libshygpu.so (building it first when the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if os.environ.get("SHYGPU_NO_BUILD") != "1":
+        try:
+            from . import build as _build
+            _build.build()
+        except Exception as exc:                    # no nvcc: use what is there
+            if not LIB_PATH.exists():
+                raise ShyError(2, f"libshygpu.so missing and could not be built: {exc}")
+    if not LIB_PATH.exists():
+        raise ShyError(2, f"libshygpu.so not found at {LIB_PATH}")
+    L = C.CDLL(str(LIB_PATH))
+    L.shygpu_last_error.restype = C.c_char_p
+    L.shygpu_launch_count.restype = C.c_int64
+    L.shygpu_model_bytes.restype = C.c_int64
+    L.shygpu_model_bytes.argtypes = [C.c_void_p]
+    L.shygpu_footprint.restype = C.c_int64
+    L.shygpu_footprint.argtypes = [C.c_int32, C.POINTER(abi.ShyBasin), C.POINTER(abi.ShyParams)]
+    L.shygpu_create.argtypes = [C.c_int32, C.POINTER(abi.ShyBasin), C.POINTER(abi.ShyParams),
+                                C.POINTER(C.c_void_p)]
+    L.shygpu_destroy.argtypes = [C.c_void_p]
+    L.shygpu_set_state.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyState)]
+    L.shygpu_get_state.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyState)]
+    L.shygpu_run.argtypes = [C.c_void_p, C.c_int32]
+    L.shygpu_enqueue.argtypes = [C.c_void_p, C.c_int32]
+    L.shygpu_sync.argtypes = [C.c_void_p]
+    L.shygpu_hydro.argtypes = [C.c_void_p]
+    L.shygpu_scalar.argtypes = [C.c_void_p]
+    L.shygpu_new_step.argtypes = [C.c_void_p]
+    L.shygpu_step_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyStepInfo)]
+    L.shygpu_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
+    L.shygpu_get_option.argtypes = [C.c_void_p, C.c_char_p]
+    L.shygpu_get_option.restype = C.c_double
+    L.shygpu_set_ev.argtypes = [C.c_int32, C.c_int32, abi.i32p, abi.f32p, abi.f32p, abi.f32p]
+    L.shygpu_simsys_register.argtypes = [C.c_int32, C.c_int32, abi.i32p]
+    L.shygpu_simsys_set_tolerance.argtypes = [C.c_double, C.c_double, C.c_int32]
+    L.shygpu_simsys_get_matrix.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)] + [C.c_void_p] * 4
+    L.shygpu_set_forcing.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 4
+    L.shygpu_model_stream.argtypes = [C.c_void_p]
+    L.shygpu_model_stream.restype = C.c_void_p
+    L.shygpu_profile_steps.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+    _lib = L
+    return L
+
+
+def check(code, what=""):
+    if code != 0:
+        msg = lib().shygpu_last_error().decode(errors="replace")
+        raise ShyError(code, f"{what}: {msg}" if what else msg)
+
+
+def set_ev(case):
+    """Element geometry ev(19, nel) through the library (evgeom.f90 set_ev)."""
+    nkn, nel = case["nkn"], case["nel"]
+    ev = np.zeros((nel, abi.SHY_EVDIM), np.float32)
+    nen = np.ascontiguousarray(case["nen3v"], np.int32)
+    x = np.ascontiguousarray(case["xgv"], np.float32)
+    y = np.ascontiguousarray(case["ygv"], np.float32)
+    check(lib().shygpu_set_ev(nkn, nel, abi.ptr(nen, abi.i32p), abi.ptr(x), abi.ptr(y), abi.ptr(ev)),
+          "set_ev")
+    return ev
+
+
+class Model:
+    """Independent basins advanced together; state stays on the device."""
+
+    def __init__(self, case_list, **param_over):
+        if isinstance(case_list, dict):
+            case_list = [case_list]
+        self.cases = list(case_list)
+        self._args = [abi.BasinArgs(c) for c in self.cases]
+        n = len(self.cases)
+        self._basins = (abi.ShyBasin * n)(*[a.struct for a in self._args])
+        self._params = (abi.ShyParams * n)(*[abi.make_params(c, **param_over) for c in self.cases])
+        h = C.c_void_p()
+        check(lib().shygpu_create(n, self._basins, self._params, C.byref(h)), "shygpu_create")
+        self.h = h
+        self._closed = False
+
+    # -- options ----------------------------------------------------------
+    def set_option(self, name, value):
+        check(lib().shygpu_set_option(self.h, name.encode(), float(value)), f"set_option {name}")
+
+    def get_option(self, name):
+        return lib().shygpu_get_option(self.h, name.encode())
+
+    # -- state ------------------------------------------------------------
+    def set_state(self, ib=0, case=None):
+        case = case if case is not None else self.cases[ib]
+        buf = abi.StateBuffers(case, fill_from_case=True)
+        st = buf.struct(only=("znv", "utlnv", "vtlnv", "tempv", "saltv", "conzv"))
+        check(lib().shygpu_set_state(self.h, ib, C.byref(st)), "set_state")
+
+    def set_state_all(self):
+        for i in range(len(self.cases)):
+            self.set_state(i)
+
+    def get_state(self, ib=0, fields=None):
+        buf = abi.StateBuffers(self.cases[ib])
+        st = buf.struct(only=fields)
+        check(lib().shygpu_get_state(self.h, ib, C.byref(st)), "get_state")
+        return {k: v for k, v in buf.arrays.items() if fields is None or k in fields}
+
+    # -- time stepping ----------------------------------------------------
+    def run(self, nsteps=1):
+        check(lib().shygpu_run(self.h, int(nsteps)), "shygpu_run")
+
+    def hydro(self):
+        check(lib().shygpu_hydro(self.h), "shygpu_hydro")
+
+    def scalar(self):
+        check(lib().shygpu_scalar(self.h), "shygpu_scalar")
+
+    def info(self, ib=0):
+        i = abi.ShyStepInfo()
+        check(lib().shygpu_step_info(self.h, ib, C.byref(i)), "step_info")
+        return i
+
+    def nbytes(self):
+        return lib().shygpu_model_bytes(self.h)
+
+    def stream(self):
+        """The model's cudaStream_t as an integer handle."""
+        return lib().shygpu_model_stream(self.h)
+
+    def set_forcing(self, ib, tauxnv=None, tauynv=None, ppv=None, rqv=None):
+        """Queue per-step forcing (host arrays, pinned for overlap)."""
+        def p(a):
+            return None if a is None else a.ctypes.data
+        for a in (tauxnv, tauynv, ppv, rqv):
+            if a is not None and (a.dtype != np.float32 or not a.flags.c_contiguous):
+                raise ValueError("forcing arrays must be contiguous float32")
+        check(lib().shygpu_set_forcing(self.h, ib, p(tauxnv), p(tauynv), p(ppv), p(rqv)),
+              "set_forcing")
+
+    KERNELS = ("column", "zeta", "final", "node", "stab", "reduce", "conz")
+
+    def profile_steps(self, nsteps):
+        """Per-kernel device time (ms, summed) and launch counts over nsteps."""
+        ms = (C.c_double * 7)()
+        cnt = (C.c_int32 * 7)()
+        check(lib().shygpu_profile_steps(self.h, int(nsteps), ms, cnt), "profile_steps")
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(self.KERNELS)}
+
+    def close(self):
+        if not self._closed and getattr(self, "h", None):
+            lib().shygpu_destroy(self.h)
+            self._closed = True
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def footprint(case_list, **param_over):
+    """Device bytes a Model of these basins would hold (admission control)."""
+    args = [abi.BasinArgs(c) for c in case_list]
+    n = len(case_list)
+    basins = (abi.ShyBasin * n)(*[a.struct for a in args])
+    params = (abi.ShyParams * n)(*[abi.make_params(c, **param_over) for c in case_list])
+    return lib().shygpu_footprint(n, basins, params)
+
+
+class Shyfem:
+    """shyfem_initialize / shyfem_run / shyfem_finalize for one basin."""
+
+    def __init__(self):
+        self.model = None
+        self.case = None
+
+    def initialize(self, case, **param_over):
+        self.case = case
+        self.model = Model([case], **param_over)
+        self.model.set_state(0)
+        return self
+
+    def run(self, dtstep):
+        """Advance by dtstep seconds (a whole number of time steps)."""
+        dt = self.case["params"]["dt"]
+        n = int(round(dtstep / dt))
+        if abs(n * dt - dtstep) > 1e-6 * dt:
+            raise ValueError("dtstep must be a multiple of dt")
+        self.model.run(n)
+
+    def finalize(self):
+        if self.model is not None:
+            self.model.close()
+            self.model = None
+
+
+class _Simsys:
+    """The reference's system_* calls (simsys_spkaux.f90) on the GPU solver."""
+
+    def register(self, nkn, nel, nen3v):
+        nen = np.ascontiguousarray(nen3v, np.int32)
+        self._nen = nen
+        check(lib().shygpu_simsys_register(nkn, nel, abi.ptr(nen, abi.i32p)), "simsys_register")
+
+    def set_tolerance(self, rtol=1e-8, atol=1e-8, maxit=1000):
+        check(lib().shygpu_simsys_set_tolerance(rtol, atol, maxit), "simsys_set_tolerance")
+
+    def system_initialize(self):
+        lib().system_initialize_()
+
+    def system_init(self):
+        lib().system_init_()
+
+    def system_set_explicit(self):
+        lib().system_set_explicit_()
+
+    def system_assemble(self, ie, kn, hia, hik):
+        """kn(3) 1-based, hia(3,3) with hia[n,m] = hia(n+1,m+1), hik(3)."""
+        zs = abi_zeta()
+        zs.kn[:] = [int(k) for k in kn]
+        zs.hia[:] = [float(v) for v in np.asarray(hia, np.float32).T.ravel()]   # column-major
+        zs.hik[:] = [float(v) for v in hik]
+        ie_c = C.c_int32(int(ie))
+        lib().system_assemble_(C.byref(ie_c))
+
+    def system_add_rhs(self, dt, array):
+        a = np.ascontiguousarray(array, np.float32)
+        dt_c, n_c = C.c_float(dt), C.c_int32(a.size)
+        lib().system_add_rhs_(C.byref(dt_c), C.byref(n_c), abi.ptr(a))
+
+    def system_solve(self, z):
+        zz = np.ascontiguousarray(z, np.float32)
+        n_c = C.c_int32(zz.size)
+        lib().system_solve_(C.byref(n_c), abi.ptr(zz))
+
+    def system_get(self, n):
+        z = np.zeros(n, np.float32)
+        n_c = C.c_int32(n)
+        lib().system_get_(C.byref(n_c), abi.ptr(z))
+        return z
+
+    def get_matrix(self, n, nnz):
+        rowptr = np.zeros(n + 1, np.int32)
+        col = np.zeros(nnz, np.int32)
+        val = np.zeros(nnz, np.float64)
+        rhs = np.zeros(n, np.float64)
+        nn, zz = C.c_int32(0), C.c_int32(0)
+        check(lib().shygpu_simsys_get_matrix(C.byref(nn), C.byref(zz), rowptr.ctypes.data,
+                                             col.ctypes.data, val.ctypes.data, rhs.ctypes.data),
+              "simsys_get_matrix")
+        return rowptr, col, val, rhs
+
+    def iterations(self):
+        return lib().shygpu_simsys_iterations()
+
+
+class ZetaSystem(C.Structure):
+    _fields_ = [("kn", C.c_int32 * 3), ("hia", C.c_float * 9), ("hik", C.c_float * 3)]
+
+
+def abi_zeta():
+    return ZetaSystem.in_dll(lib(), "shy_zeta_system")
+
+
+simsys = _Simsys()

@@ -1,0 +1,141 @@
+"""GPU step against the FP64 CPU oracle (parity tests proper).
+
+Tolerances (the targets of the step): water level within 1 mm, tracers
+within 1e-4 relative; transports within 1e-3 of their maximum magnitude;
+layer thicknesses and vertical velocities to single-precision accuracy of
+their scale.  Runs go through the C ABI (shygpu.Model over libshygpu.so).
+"""
+import numpy as np
+import pytest
+
+import shygpu
+import shyref
+from shygpu import cases
+
+pytestmark = pytest.mark.gpu
+
+ZETA_TOL = 1.0e-3          # m
+TRACER_RTOL = 1.0e-4
+
+
+def run_both(case, nsteps, **opts):
+    g = shygpu.Model(case)
+    for k, v in opts.items():
+        g.set_option(k, v)
+    g.set_state(0)
+    o = shyref.OracleModel(case)
+    g.run(nsteps)
+    o.run(nsteps)
+    return g, o
+
+
+def active_mask(case, node=True):
+    nlv = case["nlv"]
+    il = case["ilhkv"] if node else case["ilhv"]
+    return np.arange(nlv)[None, :] < il[:, None]
+
+
+def test_channel_2d_one_day_tide(channel):
+    """Config 1: 2D channel, M2 0.5 m, dt 60 s, one simulated day."""
+    g, o = run_both(channel, 1440)
+    sg, so = g.get_state(0), o.state()
+    dz = np.abs(sg["znv"] - so["znv"]).max()
+    assert dz <= ZETA_TOL, dz
+    umax = np.abs(so["utlnv"]).max()
+    assert np.abs(sg["utlnv"] - so["utlnv"]).max() <= 1e-3 * umax
+    ig, io = g.info(0), o.info()
+    assert abs(ig.dtime - io.dtime) < 1e-6
+    assert abs(ig.volume - io.volume) <= 1e-6 * io.volume
+
+
+def test_basin3d_baroclinic_ts(small3d):
+    """Config 2 shape at test size: z-layers, wind, M2, T/S, baroclinic."""
+    g, o = run_both(small3d, 120)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    m = active_mask(small3d)
+    for f in ("tempv", "saltv"):
+        rel = np.abs(sg[f] - so[f])[m].max() / np.abs(so[f][m]).max()
+        assert rel <= TRACER_RTOL, (f, rel)
+    me = active_mask(small3d, node=False)
+    umax = np.abs(so["utlnv"][me]).max()
+    assert np.abs(sg["utlnv"] - so["utlnv"])[me].max() <= 1e-3 * umax
+    assert np.abs(sg["hdknv"] - so["hdknv"])[m].max() <= 1e-4
+    wmax = np.abs(so["wlnv"]).max()
+    assert np.abs(sg["wlnv"] - so["wlnv"]).max() <= 2e-3 * wmax
+    assert np.abs(sg["rhov"] - so["rhov"])[m].max() <= 1e-3
+
+
+def test_coriolis_column_solve():
+    """Coriolis couples u and v (penta system, complex PCR on the GPU)."""
+    c = cases.basin3d_case(nkn_target=800, nlv=8, baroclinic=False, ts=False)
+    c["fcorv"] = np.full(c["nel"], 1.0e-4, np.float32)
+    g, o = run_both(c, 60)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    me = active_mask(c, node=False)
+    umax = np.abs(so["vtlnv"][me]).max()
+    assert np.abs(sg["vtlnv"] - so["vtlnv"])[me].max() <= 1e-3 * umax
+
+
+def test_batch_equals_alone():
+    """Basins advanced together give the same bits as each advanced alone."""
+    cs = [cases.basin3d_case(nkn_target=n, nlv=nl, seed=s)
+          for n, nl, s in ((600, 6, 11), (1100, 10, 12), (400, 10, 13))]
+    gb = shygpu.Model(cs)
+    gb.set_state_all()
+    gb.run(20)
+    for i, c in enumerate(cs):
+        ga = shygpu.Model(c)
+        ga.set_state(0)
+        ga.run(20)
+        a, b = ga.get_state(0), gb.get_state(i)
+        for f in ("znv", "utlnv", "tempv", "saltv", "wlnv"):
+            assert np.array_equal(a[f], b[f]), (i, f)
+
+
+def test_graph_equals_eager_and_deterministic(small3d):
+    runs = []
+    for use_graph in (1, 0, 1):
+        g = shygpu.Model(small3d)
+        g.set_option("use_graph", use_graph)
+        g.set_state(0)
+        g.run(15)
+        runs.append(g.get_state(0))
+    for f in ("znv", "utlnv", "tempv", "wlnv", "rhov"):
+        assert np.array_equal(runs[0][f], runs[1][f]), f
+        assert np.array_equal(runs[0][f], runs[2][f]), f
+
+
+def test_split_phases_equal_run(channel):
+    a = shygpu.Model(channel)
+    a.set_state(0)
+    a.run(5)
+    b = shygpu.Model(channel)
+    b.set_state(0)
+    for _ in range(5):
+        b.hydro()
+        b.scalar()
+    assert np.array_equal(a.get_state(0)["znv"], b.get_state(0)["znv"])
+
+
+def test_transport_substeps():
+    """A long time step makes the transport sub-step (istot > 1, scal3sh);
+    the device-driven sub-step loop (graph) and the eager loop both match."""
+    c = cases.basin3d_case(nkn_target=900, nlv=10, dt=900.0, wind=20.0)
+    o = shyref.OracleModel(c)
+    o.run(12)
+    assert o.info().istot > 1
+    so = o.state()
+    m = active_mask(c)
+    for use_graph in (1, 0):
+        g = shygpu.Model(c)
+        g.set_option("use_graph", use_graph)
+        g.set_state(0)
+        g.run(12)
+        assert g.info(0).istot == o.info().istot
+        sg = g.get_state(0)
+        assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+        for f in ("tempv", "saltv"):
+            rel = np.abs(sg[f] - so[f])[m].max() / np.abs(so[f][m]).max()
+            assert rel <= TRACER_RTOL, (use_graph, f, rel)
