@@ -201,8 +201,8 @@ void *shygpu_model_stream(shygpu_model *model);
 /* Run `nsteps` steps with CUDA events between the kernels of each step and
  * return the summed device time per kernel kind in ms_out[SHY_NKERNEL] and
  * the launches per kind in count_out (kinds: column, zeta, final, node,
- * stab, reduce, conz).                                                    */
-#define SHY_NKERNEL 7
+ * stab, reduce, conz, rho).                                               */
+#define SHY_NKERNEL 8
 int shygpu_profile_steps(shygpu_model *model, int32_t nsteps, double *ms_out, int32_t *count_out);
 /* Device bytes held by the model (admission by HBM footprint).            */
 int64_t shygpu_model_bytes(const shygpu_model *model);

@@ -49,6 +49,7 @@ struct BasinOut {
   int status;
   int iters, refinements;
   int istot;
+  int steps;                  // steps completed since the state was set
   float stab[kMaxScal];       // stability index (as float bits, max-reduced)
 };
 
@@ -72,6 +73,8 @@ struct Dev {
   float *taux, *tauy, *ppv, *rqv;
   float *hlv, *hldv;  // [b*NLV + l]
   float *areakv;      // [k*NLV+l]
+  float2 *avol;       // [k*NLV+l] transport weights: {sum aj4 of elements with layer
+                      //  l+1, sum aj4 of elements whose bottom layer is l}
   // zeta system
   int *rowptr, *col;          // CSR over all nodes (block diagonal)
   int *slot_ptr, *slot_src;   // gather of element entries per CSR slot
@@ -87,6 +90,7 @@ struct Dev {
   float *hkn, *hko;           // [k*NLV+l]
   float *hen, *heo;           // [e*NLV+l]
   float *unv, *vnv;           // [e]
+  float *usv, *vsv;           // [e*NLV+l] az*U^{n+1} + (1-az)*U^n of the step
   float *wl;                  // [k*(NLV+1)+l]
   float *rho;                 // [k*NLV+l]
   float *ddx, *ddxi;          // [e*NLV+l] A^-1 H (real / imaginary part with Coriolis)
@@ -183,6 +187,80 @@ __device__ __forceinline__ void pcr_solve(double a, double b, double c, double (
   }
 #pragma unroll
   for (int r = 0; r < NR; r++) d[r] = d[r] / b;
+}
+
+// PCR in single precision with NR right-hand sides (same scheme as pcr_solve)
+template <int S, int NR>
+__device__ __forceinline__ void pcr_solve_f(float a, float b, float c, float (&d)[NR], int lane) {
+#pragma unroll
+  for (int s = 1; s < S; s <<= 1) {
+    float am = seg_up<S>(a, s), bm = seg_up<S>(b, s), cm = seg_up<S>(c, s);
+    float ap = seg_down<S>(a, s), bp = seg_down<S>(b, s), cp = seg_down<S>(c, s);
+    float dm[NR], dp[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) { dm[r] = seg_up<S>(d[r], s); dp[r] = seg_down<S>(d[r], s); }
+    const bool hasm = lane >= s, hasp = lane + s < S;
+    const float k1 = hasm ? __fdividef(a, bm) : 0.f;
+    const float k2 = hasp ? __fdividef(c, bp) : 0.f;
+    const float na = hasm ? -am * k1 : 0.f, nc = hasp ? -cp * k2 : 0.f;
+    const float nb = b - (hasm ? cm * k1 : 0.f) - (hasp ? ap * k2 : 0.f);
+#pragma unroll
+    for (int r = 0; r < NR; r++) d[r] = d[r] - (hasm ? dm[r] * k1 : 0.f) - (hasp ? dp[r] * k2 : 0.f);
+    a = na; b = nb; c = nc;
+  }
+  const float rb = 1.f / b;
+#pragma unroll
+  for (int r = 0; r < NR; r++) d[r] = d[r] * rb;
+}
+
+// complex single precision (x = real, y = imaginary)
+__device__ __forceinline__ float2 cmulf(float2 p, float2 q) {
+  return make_float2(p.x * q.x - p.y * q.y, p.x * q.y + p.y * q.x);
+}
+__device__ __forceinline__ float2 cdivf(float2 p, float2 q) {
+  const float r = 1.f / (q.x * q.x + q.y * q.y);
+  return make_float2((p.x * q.x + p.y * q.y) * r, (p.y * q.x - p.x * q.y) * r);
+}
+template <int S>
+__device__ __forceinline__ float2 seg_up2f(float2 v, int d) {
+  return make_float2(seg_up<S>(v.x, d), seg_up<S>(v.y, d));
+}
+template <int S>
+__device__ __forceinline__ float2 seg_down2f(float2 v, int d) {
+  return make_float2(seg_down<S>(v.x, d), seg_down<S>(v.y, d));
+}
+
+// single-precision PCR of the complex column system (Coriolis): real
+// off-diagonals a, c, complex diagonal b, NR complex right-hand sides
+template <int S, int NR>
+__device__ __forceinline__ void pcr_solve_cf(float a, float2 b, float c, float2 (&d)[NR], int lane) {
+  float2 A = make_float2(a, 0.f), C = make_float2(c, 0.f);
+  const float2 z = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int s = 1; s < S; s <<= 1) {
+    float2 am = seg_up2f<S>(A, s), bm = seg_up2f<S>(b, s), cm = seg_up2f<S>(C, s);
+    float2 ap = seg_down2f<S>(A, s), bp = seg_down2f<S>(b, s), cp = seg_down2f<S>(C, s);
+    float2 dm[NR], dp[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) { dm[r] = seg_up2f<S>(d[r], s); dp[r] = seg_down2f<S>(d[r], s); }
+    const bool hasm = lane >= s, hasp = lane + s < S;
+    const float2 k1 = hasm ? cdivf(A, bm) : z;
+    const float2 k2 = hasp ? cdivf(C, bp) : z;
+    const float2 t1 = cmulf(am, k1), t2 = cmulf(cp, k2);
+    const float2 na = hasm ? make_float2(-t1.x, -t1.y) : z;
+    const float2 nc = hasp ? make_float2(-t2.x, -t2.y) : z;
+    float2 nb = b;
+    if (hasm) { const float2 t = cmulf(cm, k1); nb.x -= t.x; nb.y -= t.y; }
+    if (hasp) { const float2 t = cmulf(ap, k2); nb.x -= t.x; nb.y -= t.y; }
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      if (hasm) { const float2 t = cmulf(dm[r], k1); d[r].x -= t.x; d[r].y -= t.y; }
+      if (hasp) { const float2 t = cmulf(dp[r], k2); d[r].x -= t.x; d[r].y -= t.y; }
+    }
+    A = na; b = nb; C = nc;
+  }
+#pragma unroll
+  for (int r = 0; r < NR; r++) d[r] = cdivf(d[r], b);
 }
 
 // complex arithmetic on double2 (x = real, y = imaginary)

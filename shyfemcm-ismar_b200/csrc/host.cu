@@ -237,6 +237,7 @@ struct Arena {
 struct shygpu_model {
   int nbasin = 0, NKN = 0, NEL = 0, NLV = 0, S = 1, nsc_max = 0, NNZ = 0;
   bool cor = false;
+  bool has_rho = false;              // some basin updates rho' from transported T and S
   std::vector<BasinPar> par;
   std::vector<int> nlv_b;
   Arena arena;
@@ -247,6 +248,12 @@ struct shygpu_model {
   cudaStream_t stream = nullptr;
   // options
   int nsub = 2, use_graph = 1, CL = 8, zthreads = 1024, max_outer = 12, sym = 1;
+  int zvariant = 1;                  // 1: shared-memory zeta solver when it fits
+  bool use_sm = false;
+  ZetaShape zs;
+  std::vector<int> rowptr_h, col_h;  // global CSR pattern (host copy)
+  int *zmap_ptrs[3] = {nullptr, nullptr, nullptr};
+  ZetaMaps zm;
   float inner_rtol = 1e-4f;
   // graphs keyed by (cur, sc_cur)
   cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -269,6 +276,115 @@ static void drop_graphs(shygpu_model *m) {
   for (int a = 0; a < 2; a++)
     for (int b = 0; b < 2; b++)
       if (m->graph[a][b]) { cudaGraphExecDestroy(m->graph[a][b]); m->graph[a][b] = nullptr; }
+}
+
+static int check_cluster_shape(int CL, int threads, size_t smem);
+
+// Launch shape of the zeta solver.  The shared-memory variant keeps each
+// CTA's rows (row pointers, packed columns, FP32 values) and seven FP32
+// vectors in shared memory; it is used for symmetric systems when every
+// basin's largest CTA slice fits, else the global-memory variant.
+static void free_zeta_maps(shygpu_model *m) {
+  for (int *&p : m->zmap_ptrs) { if (p) cudaFree(p); p = nullptr; }
+  m->zm = ZetaMaps();
+}
+
+// Local column indices, halo slots and push lists of the shared-memory
+// zeta solver for cluster size CL (rows of basin b split in CL contiguous
+// slices of ceil(nk/CL) rows).
+static int build_zeta_maps(shygpu_model *m, int CL, ZetaShape &zs) {
+  const int NKN = m->NKN;
+  const std::vector<int> &rp = m->rowptr_h;
+  std::vector<int> loc(rp[NKN], 0);
+  std::vector<std::vector<int>> pushl(NKN);
+  for (int b = 0; b < m->nbasin; b++) {
+    const BasinPar &bp = m->par[b];
+    const int cb = (bp.nk + CL - 1) / CL;
+    zs.chunk = std::max(zs.chunk, cb);
+    for (int q = 0; q < CL; q++) {
+      const int a = bp.k0 + std::min(bp.nk, q * cb), e = bp.k0 + std::min(bp.nk, (q + 1) * cb);
+      const int nloc = e - a;
+      zs.nnzcap = std::max(zs.nnzcap, rp[e] - rp[a]);
+      std::vector<int> halo;
+      for (int s = rp[a]; s < rp[e]; s++) {
+        const int c = m->col_h[s];
+        if (c < a || c >= e) halo.push_back(c);
+      }
+      std::sort(halo.begin(), halo.end());
+      halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
+      zs.halocap = std::max(zs.halocap, (int)halo.size());
+      for (int s = rp[a]; s < rp[e]; s++) {
+        const int c = m->col_h[s];
+        if (c >= a && c < e) loc[s] = c - a;
+        else loc[s] = nloc + (int)(std::lower_bound(halo.begin(), halo.end(), c) - halo.begin());
+      }
+      for (size_t h = 0; h < halo.size(); h++)     // the owner of halo[h] pushes into slot nloc+h of q
+        pushl[halo[h]].push_back((q << 24) | (nloc + (int)h));
+    }
+  }
+  std::vector<int> pptr(NKN + 1, 0), push;
+  for (int i = 0; i < NKN; i++) {
+    pptr[i + 1] = pptr[i] + (int)pushl[i].size();
+    push.insert(push.end(), pushl[i].begin(), pushl[i].end());
+  }
+  free_zeta_maps(m);
+  int *dl = nullptr, *dp = nullptr, *dq = nullptr;
+  CUDA_TRY(cudaMalloc(&dl, sizeof(int) * std::max<size_t>(loc.size(), 1)));
+  m->zmap_ptrs[0] = dl;
+  CUDA_TRY(cudaMalloc(&dp, sizeof(int) * pptr.size()));
+  m->zmap_ptrs[1] = dp;
+  CUDA_TRY(cudaMalloc(&dq, sizeof(int) * std::max<size_t>(push.size(), 1)));
+  m->zmap_ptrs[2] = dq;
+  CUDA_TRY(cudaMemcpy(dl, loc.data(), sizeof(int) * loc.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dp, pptr.data(), sizeof(int) * pptr.size(), cudaMemcpyHostToDevice));
+  if (!push.empty()) CUDA_TRY(cudaMemcpy(dq, push.data(), sizeof(int) * push.size(), cudaMemcpyHostToDevice));
+  m->zm.loc = dl; m->zm.push_ptr = dp; m->zm.push = dq;
+  return SHY_OK;
+}
+
+static int choose_zeta_shape(shygpu_model *m, int CL, int threads) {
+  const size_t kSmemMax = 227 * 1024;
+  ZetaShape zs;
+  zs.CL = CL; zs.threads = threads;
+  bool fits = m->sym && m->zvariant;
+  if (fits) {
+    for (int b = 0; b < m->nbasin; b++) {      // capacity before building maps
+      const BasinPar &bp = m->par[b];
+      const int cb = (bp.nk + CL - 1) / CL;
+      zs.chunk = std::max(zs.chunk, cb);
+      for (int q = 0; q < CL; q++) {
+        int a = bp.k0 + std::min(bp.nk, q * cb), e = bp.k0 + std::min(bp.nk, (q + 1) * cb);
+        zs.nnzcap = std::max(zs.nnzcap, m->rowptr_h[e] - m->rowptr_h[a]);
+      }
+    }
+    // rows, columns, values, seven vectors (the u vector with its halo)
+    zs.smem = (size_t)4 * (zs.chunk + 1) + (size_t)8 * zs.nnzcap + (size_t)28 * zs.chunk;
+    fits = zs.smem + 8 * 1024 <= kSmemMax;
+    if (fits) {
+      ST_TRY(build_zeta_maps(m, CL, zs));
+      zs.smem = (size_t)4 * (zs.chunk + 1) + (size_t)8 * zs.nnzcap + (size_t)28 * zs.chunk +
+                (size_t)4 * zs.halocap;
+      zs.smem = (zs.smem + 15) & ~(size_t)15;
+      fits = zs.smem <= kSmemMax && check_cluster_shape(CL, threads, zs.smem) == SHY_OK;
+    }
+  }
+  if (fits) {
+    m->use_sm = true;
+    m->zs = zs;
+  } else {
+    ST_TRY(check_cluster_shape(CL, threads, 0));
+    m->use_sm = false;
+  }
+  m->CL = CL;
+  m->zthreads = threads;
+  return SHY_OK;
+}
+
+static int launch_zeta_any(shygpu_model *m, const Dev &d, const ZetaArgs &za) {
+  cudaError_t e = m->use_sm ? launch_zeta_sm(d, za, m->zs, m->zm, m->stream)
+                            : launch_zeta(d, za, m->CL, m->zthreads, 0, m->nbasin, m->stream);
+  if (e != cudaSuccess) return fail(SHY_ECUDA, "zeta solve launch: %s", cudaGetErrorString(e));
+  return SHY_OK;
 }
 
 static Dev dev_for_step(const shygpu_model *m, int newi) {
@@ -313,6 +429,7 @@ extern "C" int shygpu_destroy(shygpu_model *m) {
     g_models.erase(it);
   }
   drop_graphs(m);
+  free_zeta_maps(m);
   m->arena.release();
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
@@ -322,13 +439,11 @@ extern "C" int shygpu_destroy(shygpu_model *m) {
 // A cluster shape is used only after the occupancy query says that at least
 // one such cluster fits the device (clusters above 8 CTAs need the
 // non-portable attribute set first).
-static int check_cluster_shape(int CL, int threads) {
-  if (CL > 8) {
-    cudaError_t e = zeta_kernel_setup(CL);
-    if (e != cudaSuccess) return fail(SHY_EARG, "cluster size %d not available: %s", CL, cudaGetErrorString(e));
-  }
-  int n = zeta_max_active_clusters(CL, threads);
-  if (n < 1) return fail(SHY_EARG, "a cluster of %d CTAs x %d threads does not fit the device", CL, threads);
+static int check_cluster_shape(int CL, int threads, size_t smem) {
+  cudaError_t e = zeta_kernel_setup(CL, smem);
+  if (e != cudaSuccess) return fail(SHY_EARG, "cluster size %d / %zu B shared memory not available: %s", CL, smem, cudaGetErrorString(e));
+  int n = zeta_max_active_clusters(CL, threads, smem);
+  if (n < 1) return fail(SHY_EARG, "a cluster of %d CTAs x %d threads (%zu B shared) does not fit the device", CL, threads, smem);
   return SHY_OK;
 }
 
@@ -374,6 +489,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   std::vector<float> difhv((size_t)NEL * NLV, 1.f);
   std::vector<float> visv((size_t)NKN * (NLV + 1), 0.f), difv((size_t)NKN * (NLV + 1), 0.f);
   std::vector<float> taux(NKN), tauy(NKN), ppv(NKN), rqv(NKN), areakv((size_t)NKN * NLV, 0.f);
+  std::vector<float2> avol((size_t)NKN * NLV, make_float2(0.f, 0.f));
   std::vector<float> hlv((size_t)nbasin * NLV, 0.f), hldv((size_t)nbasin * NLV, 0.f), tide;
   std::vector<int> rowptr(1, 0), col, slot_ptr(1, 0), slot_src, inc_ptr(1, 0), inc;
   int k0 = 0, e0 = 0;
@@ -464,6 +580,20 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       }
       for (int k = 0; k < nkn; k++)
         for (int l = 0; l < nlv; l++) areakv[(size_t)(k0 + k) * NLV + l] = (float)ak[(size_t)k * nlv + l];
+      // transport weights per node layer: sums of aj4 = 4*aj over the elements
+      // that continue below the layer and over those that end at it
+      std::vector<double> at((size_t)nkn * nlv, 0.), af((size_t)nkn * nlv, 0.);
+      for (int ie = 0; ie < nel; ie++) {
+        const double aj4 = 4. * ev[(size_t)ie * SHY_EVDIM + 9];
+        const int le = bs.ilhv[ie];
+        for (int ii = 0; ii < 3; ii++) {
+          const int k = nv[3 * ie + ii];
+          for (int l = 0; l < le; l++) (l + 1 < le ? at : af)[(size_t)k * nlv + l] += aj4;
+        }
+      }
+      for (int k = 0; k < nkn; k++)
+        for (int l = 0; l < nlv; l++)
+          avol[(size_t)(k0 + k) * NLV + l] = make_float2((float)at[(size_t)k * nlv + l], (float)af[(size_t)k * nlv + l]);
     }
     for (int l = 0; l < nlv; l++) { hlv[(size_t)b * NLV + l] = bs.hlv[l]; hldv[(size_t)b * NLV + l] = bs.hldv[l]; }
     // pattern + gather maps, shifted to global numbering
@@ -503,6 +633,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     k0 += nkn; e0 += nel;
   }
   m->nsc_max = nsc_max;
+  for (int b = 0; b < nbasin; b++)
+    m->has_rho |= m->par[b].ibarcl > 0 && m->par[b].itemp && m->par[b].isalt;
   m->NNZ = (int)col.size();
   if (m->cor) m->sym = 0;          // Coriolis makes the zeta system non-symmetric
 
@@ -521,7 +653,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       A.upload(&d.tide, tide) || A.upload(&d.visv, visv) || A.upload(&d.difv, difv) ||
       A.upload(&d.taux, taux) || A.upload(&d.tauy, tauy) || A.upload(&d.ppv, ppv) ||
       A.upload(&d.rqv, rqv) || A.upload(&d.hlv, hlv) || A.upload(&d.hldv, hldv) ||
-      A.upload(&d.areakv, areakv) || A.upload(&d.rowptr, rowptr) || A.upload(&d.col, col) ||
+      A.upload(&d.areakv, areakv) || A.upload(&d.avol, avol) ||
+      A.upload(&d.rowptr, rowptr) || A.upload(&d.col, col) ||
       A.upload(&d.slot_ptr, slot_ptr) || A.upload(&d.slot_src, slot_src) ||
       A.upload(&d.inc_ptr, inc_ptr) || A.upload(&d.inc, inc) || A.upload(&m->kbas, kbas))
     return bail(SHY_ECAPACITY);
@@ -533,6 +666,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       A.alloc(&d.e32, NKN) || A.alloc(&d.s32, NKN) || A.alloc(&d.t32, NKN) ||
       A.alloc(&d.rh32, NKN) || A.alloc(&d.v32, NKN) || A.alloc(&d.hia, (size_t)9 * NEL) ||
       A.alloc(&d.hik, (size_t)3 * NEL) || A.alloc(&d.unv, NEL) || A.alloc(&d.vnv, NEL) ||
+      A.alloc(&d.usv, EL) || A.alloc(&d.vsv, EL) ||
       A.alloc(&d.wl, (size_t)NKN * (NLV + 1)) || A.alloc(&d.rho, NL) || A.alloc(&d.ddx, EL) ||
       A.alloc(&d.ddxi, m->cor ? EL : 1) || A.alloc(&d.cbnd, NSC) || A.alloc(&d.vol_node, NKN) ||
       A.alloc(&d.scr0, nsc_max > 0 ? NSC : 1) || A.alloc(&d.scr1, nsc_max > 0 ? NSC : 1) ||
@@ -547,13 +681,14 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   }
   if (cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(SHY_ECUDA, "stream creation failed"));
-  // zeta solver launch shape: one cluster per basin
+  // zeta solver launch shape: one cluster per basin, about 2k rows per CTA
+  m->rowptr_h = rowptr;
+  m->col_h = col;
   int maxn = 0;
   for (int b = 0; b < nbasin; b++) maxn = std::max(maxn, B[b].nkn);
-  m->CL = maxn >= 16384 ? 8 : (maxn >= 4096 ? 4 : (maxn >= 1024 ? 2 : 1));
-  m->zthreads = maxn >= 4096 ? 1024 : 512;
   {
-    int st = check_cluster_shape(m->CL, m->zthreads);
+    int CL = std::min(16, next_pow2((maxn + 2047) / 2048));
+    int st = choose_zeta_shape(m, CL, maxn >= 4096 ? 1024 : 512);
     if (st) return bail(st);
   }
   m->out_h.resize(nbasin);
@@ -579,12 +714,19 @@ extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value
       if (iv < 64 || iv > 1024 || iv % 32) return fail(SHY_EARG, "zeta_threads: multiple of 32 in 64..1024");
       th = iv;
     }
-    ST_TRY(check_cluster_shape(CL, th));
-    m->CL = CL; m->zthreads = th;
+    ST_TRY(choose_zeta_shape(m, CL, th));
+  }
+  else if (n == "zeta_variant") {   // 0: vectors in global memory, 1: shared memory when it fits
+    m->zvariant = iv != 0;
+    ST_TRY(choose_zeta_shape(m, m->CL, m->zthreads));
   }
   else if (n == "inner_rtol") { if (!(value > 0 && value < 1)) return fail(SHY_EARG, "inner_rtol in (0,1)"); m->inner_rtol = (float)value; }
   else if (n == "max_outer") { if (iv < 1 || iv > 100) return fail(SHY_EARG, "max_outer 1..100"); m->max_outer = iv; }
-  else if (n == "symmetric") { if (iv && m->cor) return fail(SHY_EARG, "Coriolis: the system is not symmetric"); m->sym = iv != 0; }
+  else if (n == "symmetric") {
+    if (iv && m->cor) return fail(SHY_EARG, "Coriolis: the system is not symmetric");
+    m->sym = iv != 0;
+    ST_TRY(choose_zeta_shape(m, m->CL, m->zthreads));
+  }
   else return fail(SHY_EARG, "unknown option '%s'", name);
   drop_graphs(m);
   return SHY_OK;
@@ -599,6 +741,7 @@ extern "C" double shygpu_get_option(shygpu_model *m, const char *name) {
   if (n == "inner_rtol") return m->inner_rtol;
   if (n == "max_outer") return m->max_outer;
   if (n == "symmetric") return m->sym;
+  if (n == "zeta_variant") return m->use_sm ? 1 : 0;
   if (n == "launches_per_step") return m->launches_per_step;
   return -1;
 }
@@ -634,6 +777,7 @@ extern "C" int shygpu_set_state(shygpu_model *m, int32_t ib, const shy_state *s)
   cudaStream_t st = m->stream;
   const int c = m->cur;
   drop_graphs(m);
+  CUDA_TRY(cudaMemsetAsync(&m->base.out[ib].steps, 0, sizeof(int), st));   // no earlier level yet
   if (s->znv) CUDA_TRY(cudaMemcpyAsync(m->zbuf[c] + bp.k0, s->znv, (size_t)bp.nk * 4, cudaMemcpyHostToDevice, st));
   if (s->utlnv) ST_TRY(copy_cols(m->ubuf[c], s->utlnv, bp.ne, nlv, NLV, bp.e0, true, st));
   if (s->vtlnv) ST_TRY(copy_cols(m->vbuf[c], s->vtlnv, bp.ne, nlv, NLV, bp.e0, true, st));
@@ -701,10 +845,9 @@ extern "C" int shygpu_get_state(shygpu_model *m, int32_t ib, shy_state *s) {
 static int enqueue_hydro(shygpu_model *m, const Dev &d) {
   launch_elem(d, 0, 0, m->stream, m->cor);
   ZetaArgs za{};
-  za.zguess = d.zo; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
+  za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
   za.explicit_mode = 0; za.inner_rtol = m->inner_rtol; za.max_outer = m->max_outer; za.sym = m->sym;
-  cudaError_t e = launch_zeta(d, za, m->CL, m->zthreads, 0, m->nbasin, m->stream);
-  if (e != cudaSuccess) return fail(SHY_ECUDA, "zeta solve launch: %s", cudaGetErrorString(e));
+  ST_TRY(launch_zeta_any(m, d, za));
   launch_elem(d, 1, 0, m->stream, m->cor);
   launch_node(d, m->kbas, 0, 0, 0, m->stream);
   return SHY_OK;
@@ -729,13 +872,14 @@ static int enqueue_scalar(shygpu_model *m, Dev d, int sc_cur, int *nconz) {
     d.sc_out = m->scbuf[1 - sc_cur];
     for (int j = 0; j < imax && j < 1000; j++) launch_node(d, m->kbas, 2, j, 0, m->stream);
     *nconz = imax;
+    if (m->has_rho) { launch_node(d, m->kbas, 4, 0, 0, m->stream); *nconz += 1; }
   }
   return SHY_OK;
 }
 
 // launches of one step apart from the transport sub-steps
 static int count_launches(const shygpu_model *m) {
-  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0);
+  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0) + (m->has_rho ? 1 : 0);
 }
 
 static int enqueue_step(shygpu_model *m) {
@@ -826,6 +970,14 @@ static int build_graph(shygpu_model *m, int cur, int sc_cur) {
     cudaGraph_t gb = nullptr;
     e = cudaStreamEndCapture(m->stream, &gb);
     if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "body capture: %s", cudaGetErrorString(e)));
+    if (m->has_rho) {           // rhoset after the sub-step loop
+      e = cudaStreamBeginCaptureToGraph(m->stream, g, &cnode, nullptr, 1, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "graph capture: %s", cudaGetErrorString(e)));
+      launch_node(db, m->kbas, 4, 0, 0, m->stream);
+      cudaGraph_t gr = nullptr;
+      e = cudaStreamEndCapture(m->stream, &gr);
+      if (e != cudaSuccess) return bail(fail(SHY_ECUDA, "graph capture: %s", cudaGetErrorString(e)));
+    }
   }
   e = cudaGraphInstantiate(&m->graph[cur][sc_cur], g, 0);
   cudaGraphDestroy(g);
@@ -917,9 +1069,9 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
     cudaEventRecord(ev[n], m->stream);
     launch_elem(d, 0, 0, m->stream, m->cor); kind[n] = 0; cudaEventRecord(ev[++n], m->stream);
     ZetaArgs za{};
-    za.zguess = d.zo; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
+    za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
     za.inner_rtol = m->inner_rtol; za.max_outer = m->max_outer; za.sym = m->sym;
-    if (launch_zeta(d, za, m->CL, m->zthreads, 0, m->nbasin, m->stream) != cudaSuccess) { st = fail(SHY_ECUDA, "zeta launch"); break; }
+    if ((st = launch_zeta_any(m, d, za)) != SHY_OK) break;
     kind[n] = 1; cudaEventRecord(ev[++n], m->stream);
     launch_elem(d, 1, 0, m->stream, m->cor); kind[n] = 2; cudaEventRecord(ev[++n], m->stream);
     launch_node(d, m->kbas, 0, 0, 0, m->stream); kind[n] = 3; cudaEventRecord(ev[++n], m->stream);
@@ -936,6 +1088,7 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
         launch_node(d, m->kbas, 2, j, 0, m->stream);
         kind[n] = 6; cudaEventRecord(ev[++n], m->stream);
       }
+      if (m->has_rho) { launch_node(d, m->kbas, 4, 0, 0, m->stream); kind[n] = 7; cudaEventRecord(ev[++n], m->stream); }
     }
     g_launches += n;
     CUDA_TRY(cudaEventSynchronize(ev[n]));
@@ -1124,7 +1277,7 @@ static int simsys_solve_impl(int n, const float *z) {
   za.explicit_mode = g_sys.explicit_mode; za.inner_rtol = 1e-4f; za.max_outer = 12; za.sym = 0;
   int CL = n >= 16384 ? 8 : (n >= 4096 ? 4 : (n >= 1024 ? 2 : 1));
   int threads = n >= 4096 ? 1024 : 512;
-  ST_TRY(check_cluster_shape(CL, threads));
+  ST_TRY(check_cluster_shape(CL, threads, 0));
   cudaError_t e = launch_zeta(d, za, CL, threads, 0, 1, st);
   if (e != cudaSuccess) return fail(SHY_ECUDA, "system_solve launch: %s", cudaGetErrorString(e));
   g_launches += 1;

@@ -1,0 +1,233 @@
+// k_conz.cuh -- one sub-step of 3D scalar transport for every scalar of a
+// node column: conz3d_omp (concentration_omp.f90:65-350) with the element
+// part conz3d_element (:355-755, vertical fluxes of vertical_flux_ie,
+// tvd_admin.f90:930-1019, without vertical TVD) gathered per node in element
+// order, the node part conz3d_nodes (:757-888: vertical tridiagonal system),
+// the level-boundary values of bndo_impbc (bndo.f90:700-760); and rhoset
+// (baroclinic.f90:654-710) once temperature and salinity are final.
+//
+// One warp segment per node column (lane = layer).  In conz3d_element the
+// storage, vertical-diffusion and vertical-advection terms of node k depend
+// on an element e only through its weight aj4 = 4*aj and through whether
+// layer l+1 exists in e (presentl(l+1), and wl(ilevel) = 0 at the element's
+// bottom).  Their sum over the elements of k is therefore the node's own
+// column terms weighted by two static sums, A_t = sum of aj4 over elements
+// that continue below layer l and A_f = sum over elements whose bottom layer
+// is l (Dev::avol).  Only the horizontal fluxes (and horizontal diffusion)
+// need the loop over the incident elements.  Scalars with the same sub-step
+// count share that loop and one PCR solve of the vertical system.  FP32.
+// Included by step.cu.
+#pragma once
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace shy {
+
+// v[i] for a run-time i in 0..2 through selects (no local-memory array)
+__device__ __forceinline__ float sel3(const float (&v)[3], int i) {
+  return i == 0 ? v[0] : (i == 1 ? v[1] : v[2]);
+}
+
+__device__ __forceinline__ float clipc(float v, bool is_temp) {
+  return (!is_temp && v < 1.e-15f) ? 0.f : v;   // scal3sh: where(cnv < 1e-15) cnv = 0
+}
+
+template <int S, int NR>
+__global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg) {
+  const int j = j_arg >= 0 ? j_arg : *d.subj;   // sub-step index: argument or device counter
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k0 = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  const bool valid = k0 < d.NKN;
+  const int k = valid ? k0 : d.NKN - 1;
+  const int NLV = d.NLV, I = NLV + 1;
+  const int b = kbas[k];
+  const BasinPar &P = d.par[b];
+  const BasinOut &O = d.out[b];
+  const int nsc = P.nsc;
+  const int lmax = d.ilhkv[k];
+  const bool act = lane < lmax;
+  const size_t o = (size_t)k * NLV + lane;
+  const size_t SN = (size_t)d.NKN * NLV;
+  const int isact = j + 1;
+  unsigned todo = 0;
+  for (int s = 0; s < nsc; s++)
+    if (isact <= (int)O.stab[s]) todo |= 1u << s;
+  if (todo == 0) return;                        // the whole segment skips together
+  const float ad = P.ad, adt = 1.f - ad, aa = P.aa, aat = 1.f - aa;
+  const float hko = act ? d.hko[o] : 0.f, hkn = act ? d.hkn[o] : 0.f;
+  const float rvptop = act ? d.difv[(size_t)k * I + lane] + P.difmol : 0.f;
+  const float rvpbot = act ? d.difv[(size_t)k * I + lane + 1] + P.difmol : 0.f;
+  const float wt = act ? d.wl[(size_t)k * I + lane] : 0.f;
+  const float wb = act ? d.wl[(size_t)k * I + lane + 1] : 0.f;
+  const float2 av = act ? d.avol[o] : make_float2(0.f, 0.f);
+  const float At = av.x, A = av.x + av.y;      // continuing elements, all elements
+  const bool isbnd = d.kbnd[k] > 0;
+  const int pbeg = d.inc_ptr[k], pend = d.inc_ptr[k + 1];
+  const bool up_ok = lane > 0, dn_ok = lane + 1 < lmax;
+  while (todo) {
+    // a group: scalars with the sub-step count of the first pending one
+    const int s0 = __ffs(todo) - 1;
+    const int istot = (int)O.stab[s0];
+    int sidx[NR];
+    int nm = 0;
+#pragma unroll
+    for (int r = 0; r < NR; r++) sidx[r] = -1;
+    for (int s = s0; s < nsc && nm < NR; s++)
+      if ((todo >> s & 1u) && (int)O.stab[s] == istot) { sidx[nm++] = s; todo &= ~(1u << s); }
+    const float rstot = istot;
+    const float rso = (isact - 1) / rstot, rsn = isact / rstot, rsot = 1.f - rso, rsnt = 1.f - rsn;
+    const float dt = (float)P.dt / rstot;
+    const float *cin_base = isact == 1 ? d.sc_in : (isact & 1 ? d.scr1 : d.scr0);
+    float *cout_base = isact == istot ? d.sc_out : (isact & 1 ? d.scr0 : d.scr1);
+    // node column: thickness, vertical diffusion conductances
+    const float hold = rso * hkn + rsot * hko, hnew = rsn * hkn + rsnt * hko;
+    const float holdm = seg_up<S>(hold, 1), holdp = seg_down<S>(hold, 1);
+    const float hnewm = seg_up<S>(hnew, 1), hnewp = seg_down<S>(hnew, 1);
+    const float hmotop = up_ok ? 2.f * rvptop / (holdm + hold) : 0.f;
+    const float hmobot = dn_ok ? 2.f * rvpbot / (hold + holdp) : 0.f;
+    const float hmntop = up_ok ? 2.f * rvptop / (hnewm + hnew) : 0.f;
+    const float hmnbot = dn_ok ? 2.f * rvpbot / (hnew + hnewp) : 0.f;
+    float cl[NR], cm1[NR], cp1[NR], hs[NR];
+    bool istmp[NR];
+    float rk[NR];
+    bool anyrk = false;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const int s = sidx[r] < 0 ? 0 : sidx[r];
+      istmp[r] = P.is_temp[s] != 0;
+      rk[r] = sidx[r] < 0 ? 0.f : P.rkpar[s];
+      anyrk |= rk[r] != 0.f;
+      const float v = (act && sidx[r] >= 0) ? clipc(cin_base[s * SN + o], istmp[r]) : 0.f;
+      cl[r] = v;
+      cm1[r] = seg_up<S>(v, 1);
+      cp1[r] = seg_down<S>(v, 1);
+      if (!up_ok) cm1[r] = 0.f;
+      if (!dn_ok) cp1[r] = 0.f;
+      hs[r] = 0.f;
+    }
+    // horizontal fluxes: sum over the incident elements of aj4*(3*fl - hdif)
+    if (act) {
+      for (int p = pbeg; p < pend; p++) {
+        const int q = d.inc[p];
+        const int e = q / 3, ii = q - 3 * e;
+        if (lane >= d.ilhv[e]) continue;
+        const float4 e0 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8);
+        const float4 e1 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8 + 4);
+        const float bb[3] = {e0.x, e0.y, e0.z}, cc[3] = {e0.w, e1.x, e1.y};
+        const float aj4 = 4.f * e1.z;
+        const size_t oe = (size_t)e * NLV + lane;
+        const float us = d.usv[oe], vs = d.vsv[oe];
+        float f3[3];
+        int itot = 0, isum = 0;
+#pragma unroll
+        for (int jj = 0; jj < 3; jj++) {
+          f3[jj] = us * bb[jj] + vs * cc[jj];
+          if (f3[jj] < 0.f) { itot++; isum += jj + 1; }
+        }
+        if (itot == 0 && !anyrk) continue;      // no horizontal flux for this vertex
+        const int4 en = d.enode[e];
+        const float hmed = anyrk ? rso * d.hen[oe] + rsot * d.heo[oe] : 0.f;
+        const float dfh = anyrk ? d.difhv[oe] : 0.f;
+        const int kja = ii == 0 ? en.y : en.x, kjb = ii == 2 ? en.y : en.z;
+        const float fii = sel3(f3, ii);
+#pragma unroll
+        for (int r = 0; r < NR; r++) {
+          if (sidx[r] < 0) continue;
+          const float *cs = cin_base + sidx[r] * SN;
+          const float ca = clipc(cs[(size_t)kja * NLV + lane], istmp[r]);
+          const float cb = clipc(cs[(size_t)kjb * NLV + lane], istmp[r]);
+          // concentrations of vertices 0,1,2 (own value at ii, the others in order)
+          const float c3[3] = {ii == 0 ? cl[r] : ca, ii == 1 ? cl[r] : (ii == 0 ? ca : cb), ii == 2 ? cl[r] : cb};
+          float fl;
+          if (itot == 1) fl = fii * sel3(c3, isum - 1);
+          else if (itot == 2) {
+            // flux into the vertex with f >= 0 balances the two outflows
+            const float fc = fii * cl[r];
+            fl = (ii == 5 - isum) ? fc - (f3[0] * c3[0] + f3[1] * c3[1] + f3[2] * c3[2]) : fc;
+          } else fl = 0.f;
+          float hdif = 0.f;
+          if (rk[r] != 0.f) {
+            float wdiff = 0.f;
+#pragma unroll
+            for (int iii = 0; iii < 3; iii++) wdiff += d.wdif[(size_t)e * 9 + 3 * iii + ii] * c3[iii];
+            hdif = 3.f * rk[r] * dfh * hmed * wdiff;
+          }
+          hs[r] += aj4 * (3.f * fl - hdif);
+        }
+      }
+    }
+    // storage, vertical diffusion and vertical advection, summed over the
+    // elements through A_t (layer l+1 present) and A (all elements)
+    const float w0 = up_ok ? wt : 0.f;               // top interface (0 at the surface)
+    float clc_b = ad * hmntop, clmm = -ad * hmntop;  // parts every element has
+    if (w0 >= 0.f) clc_b += aa * w0; else clmm += aa * w0;
+    float clc_x = ad * hmnbot, clpp = -ad * hmnbot;  // parts of elements that continue below
+    if (wb > 0.f) clpp -= aa * wb; else clc_x -= aa * wb;
+    const float clo = A * dt * clmm;
+    const float chi = At * dt * clpp;
+    const float cdg = A * (dt * clc_b + hnew) + At * dt * clc_x;
+    float res[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const float c = cl[r];
+      const float vtop = up_ok ? wt * (wt > 0.f ? c : cm1[r]) : 0.f;
+      const float vbot = wb * (wb > 0.f ? cp1[r] : c);
+      const float fw = aat * (A * vtop - At * vbot);
+      const float fd = adt * (At * (c - cp1[r]) * hmobot - A * (cm1[r] - c) * hmotop);
+      res[r] = A * hold * c + dt * (hs[r] - fw - fd);
+    }
+    // vertical system of the node column (conz3d_nodes :841-868)
+    if ((P.aa == 0.f && P.ad == 0.f) || P.nlv == 1) {
+#pragma unroll
+      for (int r = 0; r < NR; r++) res[r] = (act && cdg != 0.f) ? res[r] / cdg : res[r];
+    } else {
+      if (act && cdg == 0.f && valid) set_status(&d.out[b], SHY_ESINGULAR);
+#pragma unroll
+      for (int r = 0; r < NR; r++) res[r] = act ? res[r] : 0.f;
+      pcr_solve_f<S, NR>(act ? clo : 0.f, act ? cdg : 1.f, act ? chi : 0.f, res, lane);
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      if (sidx[r] < 0) continue;
+      const int s = sidx[r];
+      float cf = act ? res[r] : 0.f;
+      if (act && isbnd) cf = d.cbnd[s * SN + o];      // bndo_impbc
+      if (valid && lane < NLV) cout_base[s * SN + o] = cf;
+    }
+  }
+}
+
+// rhoset (baroclinic.f90:654-710) once temperature and salinity are final:
+// one pass, the pressure from the previous rho' (rhoset_shell(1)), z-layers
+// (hlayer = hldv).  d.sc_out holds the step's final scalars.
+template <int S>
+__global__ void __launch_bounds__(256) k_rho(Dev d, const int *kbas) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k0 = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  const bool valid = k0 < d.NKN;
+  const int k = valid ? k0 : d.NKN - 1;
+  const int NLV = d.NLV;
+  const int b = kbas[k];
+  const BasinPar &P = d.par[b];
+  if (!(P.ibarcl > 0 && P.itemp && P.isalt)) return;
+  const int lmax = d.ilhkv[k];
+  const bool act = lane < lmax;
+  const size_t o = (size_t)k * NLV + lane;
+  const size_t SN = (size_t)d.NKN * NLV;
+  const float *hld = d.hldv + (size_t)b * NLV;
+  const double hh = lane < NLV ? 0.5 * (double)hld[lane] : 0.;
+  const double rold = act ? (double)d.rho[o] : 0.;
+  const double dpresc = rold * P.grav * hh;
+  const double depth = seg_scan_down<S>(act ? 2. * hh : 0., lane) - hh;
+  const double pbc = seg_scan_down<S>(act ? 2. * dpresc : 0., lane) - dpresc;
+  if (act && valid) {
+    const double t = d.sc_out[o], s = d.sc_out[SN + o];    // T is scalar 0, S scalar 1
+    const double rho0 = P.rowass, sigma0 = rho0 - 1000.;
+    const double pres = 1.e-5 * (rho0 * P.grav * depth + pbc);
+    d.rho[o] = (float)(sigma_stp_d(s > 0. ? s : 0., t, (double)(float)pres) - sigma0);
+  }
+}
+
+}  // namespace shy

@@ -1,0 +1,78 @@
+// k_final.cuh -- hydro_transports_final, setzev, element layer thickness
+// Included by step.cu (one translation unit).
+#pragma once
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace shy {
+
+// ===========================================================================
+// k_final: hydro_transports_final + setzev + element layer thickness
+// ===========================================================================
+template <int S, bool COR>
+__global__ void __launch_bounds__(256) k_final(Dev d, int init_only) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e0 = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  const bool valid = e0 < d.NEL;
+  const int e = valid ? e0 : d.NEL - 1;
+  const int NLV = d.NLV;
+  const int4 en = d.enode[e];
+  const BasinPar &P = d.par[en.w];
+  const int kn[3] = {en.x, en.y, en.z};
+  const int ilevel = d.ilhv[e];
+  const bool act = lane < ilevel;
+  const size_t o = (size_t)e * NLV + lane;
+  const float *evp = d.ev8 + (size_t)e * 8;
+  double zn3[3];
+#pragma unroll
+  for (int ii = 0; ii < 3; ii++) zn3[ii] = d.zn[kn[ii]];
+  if (!init_only) {
+    const double beta = P.dt * (double)P.grav * P.am;
+    double bz = 0., cz = 0.;
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) {
+      double dz = zn3[ii] - (double)d.zeo[3 * e + ii];
+      bz += dz * evp[ii];
+      cz += dz * evp[3 + ii];
+    }
+    double u = 0., v = 0.;
+    if (act) {
+      double re = d.ddx[o], im = COR ? (double)d.ddxi[o] : 0.;
+      double du = beta * (re * bz - im * cz);
+      double dv = beta * (im * bz + re * cz);
+      u = (double)(float)((double)d.un[o] - du);
+      v = (double)(float)((double)d.vn[o] - dv);
+      if (valid) { d.un[o] = (float)u; d.vn[o] = (float)v; }
+    }
+    // the time-weighted transports az*U^{n+1} + (1-az)*U^n that hydro_vertical,
+    // conzstab and conz3d use (hydrodynamic.f90:1681-1683, concentration_omp.f90:566)
+    if (valid && lane < d.NLV) {
+      const double az = P.az;
+      d.usv[o] = act ? (float)(az * u + (1. - az) * (double)d.uo[o]) : 0.f;
+      d.vsv[o] = act ? (float)(az * v + (1. - az) * (double)d.vo[o]) : 0.f;
+    }
+    double um = seg_sum<S>(u), vm = seg_sum<S>(v);
+    if (lane == 0 && valid) { d.unv[e] = (float)um; d.vnv[e] = (float)vm; }
+  }
+  // setzev and the element part of setdepth (z-layers)
+  if (lane == 0 && valid) {
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) d.zen[3 * e + ii] = (float)zn3[ii];
+  }
+  const float4 hm = d.hm3v[e];
+  double zmed = (zn3[0] + zn3[1] + zn3[2]) / 3.;
+  const float *hld = d.hldv + (size_t)en.w * NLV;
+  const float *hlv = d.hlv + (size_t)en.w * NLV;
+  double h = 0.;
+  if (act) {
+    if (ilevel == 1) h = hm.w + zmed;
+    else if (lane < ilevel - 1) h = (double)hld[lane] + (lane == 0 ? zmed : 0.);
+    else h = (double)hm.w - hlv[ilevel - 2];
+    if (!(h > 0.) && valid) set_status(&d.out[en.w], SHY_EDEPTH);
+  }
+  if (valid && lane < NLV) d.hen[o] = (float)h;
+}
+
+
+}  // namespace shy

@@ -1,0 +1,228 @@
+// k_node.cuh -- nodal layer thickness, vertical velocity, stability index, reductions, initial rho
+// Included by step.cu (one translation unit).
+#pragma once
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace shy {
+
+// ===========================================================================
+// k_node: nodal layer thickness, vertical velocity, node volume
+// ===========================================================================
+template <int S>
+__global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_only) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k0 = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  const bool valid = k0 < d.NKN;
+  const int k = valid ? k0 : d.NKN - 1;
+  const int NLV = d.NLV;
+  const int b = kbas[k];
+  const BasinPar &P = d.par[b];
+  const int lmax = d.ilhkv[k];
+  const bool act = lane < lmax;
+  const double z = d.zn[k];
+  const float *hld = d.hldv + (size_t)b * NLV;
+  const float *hlv = d.hlv + (size_t)b * NLV;
+  const double hldl = lane < NLV ? (double)hld[lane] : 0.;
+  double hsum = 0., vf = 0., va = 0.;
+  for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
+    const int q = d.inc[p];
+    const int e = q / 3, ii = q - 3 * e;
+    const int le = d.ilhv[e];
+    if (lane >= le) continue;
+    const float *evp = d.ev8 + (size_t)e * 8;
+    const double aj = evp[6];
+    const double areafv = 4. * aj;            // 12*aj/3
+    const float4 hm = d.hm3v[e];
+    const double htot = ii == 0 ? hm.x : (ii == 1 ? hm.y : hm.z);
+    double hl;
+    if (le == 1) hl = htot + z;
+    else if (lane < le - 1) hl = hldl + (lane == 0 ? z : 0.);
+    else hl = htot - hlv[le - 2];
+    hsum += areafv * hl;
+    if (!init_only) {
+      const double bb = evp[ii], cc = evp[3 + ii];
+      const size_t oe = (size_t)e * NLV + lane;
+      double ff = (double)d.usv[oe] * bb + (double)d.vsv[oe] * cc;   // az*ffn + azt*ffo
+      const double aj4 = 4. * aj;
+      vf += 3. * aj4 * ff;
+      va += aj4;
+    }
+  }
+  const size_t o = (size_t)k * NLV + lane;
+  const double area = act ? (double)d.areakv[o] : 0.;
+  double hk = act && area > 0. ? hsum / area : 0.;
+  float hkf = (float)hk;
+  if (act && !(hkf > 0.f) && valid) set_status(&d.out[b], SHY_EDEPTH);
+  if (valid && lane < NLV) d.hkn[o] = act ? hkf : 0.f;
+  // node volume (masscont: sum of real hdknv*areakv in double)
+  double vol = act ? (double)(hkf * (float)area) : 0.;
+  vol = seg_sum<S>(vol);
+  if (lane == 0 && valid) d.vol_node[k] = vol;
+  if (init_only) return;
+  // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771)
+  const int I = NLV + 1;
+  double dv = 0.;
+  if (act && P.nlv > 1) {
+    double voln = (double)(hkf * (float)area), volo = (double)(d.hko[o] * (float)area);
+    dv = vf - (voln - volo) / P.dt;
+  }
+  double wtop = seg_scan_up<S>(dv, lane);      // flux through the top interface of layer lane
+  if (lane == 0) wtop = 0.;                     // wlnv(lmin-1) = 0
+  if (lane >= 1 && act && va > 0.) wtop /= va;
+  if (!act || P.nlv == 1 || d.kbnd[k] > 0) wtop = 0.;
+  if (valid) {
+    if (lane < I) d.wl[(size_t)k * I + lane] = (float)wtop;
+    if (lane == 0 && S < I) d.wl[(size_t)k * I + S] = 0.f;
+    if (lane == 0 && S == NLV) d.wl[(size_t)k * I + NLV] = 0.f;
+  }
+}
+
+// ===========================================================================
+// k_stab: conzstab stability index per node, max-reduced per basin/scalar
+// ===========================================================================
+template <int S>
+__global__ void __launch_bounds__(256) k_stab(Dev d, const int *kbas) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k0 = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  const bool valid = k0 < d.NKN;
+  const int k = valid ? k0 : d.NKN - 1;
+  const int NLV = d.NLV, I = NLV + 1;
+  const int b = kbas[k];
+  const BasinPar &P = d.par[b];
+  if (P.nsc == 0) return;
+  const int lmax = d.ilhkv[k];
+  const bool act = lane < lmax;
+  const double adt = 1. - (double)P.ad, aat = 1. - (double)P.aa;
+  const size_t o = (size_t)k * NLV + lane;
+  const double hold = act ? (double)d.hko[o] : 0., hnew = act ? (double)d.hkn[o] : 0.;
+  const double rvptop = act ? (double)d.difv[(size_t)k * I + lane] + P.difmol : 0.;
+  const double rvpbot = act ? (double)d.difv[(size_t)k * I + lane + 1] + P.difmol : 0.;
+  float rk_prev = -1.f;
+  float stab = 0.f;
+  for (int s = 0; s < P.nsc; s++) {
+    const float rkpar = P.rkpar[s];
+    if (rkpar != rk_prev) {
+      rk_prev = rkpar;
+      double chigh = 0., clow = 0., cn = 0., cdiag = 0.;
+      if (act) {
+        for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
+          const int q = d.inc[p];
+          const int e = q / 3, ii = q - 3 * e;
+          const int le = d.ilhv[e];
+          if (lane >= le) continue;
+          const int4 en = d.enode[e];
+          const int kn[3] = {en.x, en.y, en.z};
+          const float *evp = d.ev8 + (size_t)e * 8;
+          const double aj4 = 4. * (double)evp[6];
+          const size_t oe = (size_t)e * NLV + lane;
+          const double us = d.usv[oe], vs = d.vsv[oe];
+          double coadv = 0., ciadv = 0.;
+          for (int jj = 0; jj <= ii; jj++) {
+            const double f = us * evp[jj] + vs * evp[3 + jj];
+            double wt = lane == 0 ? 0. : (double)d.wl[(size_t)kn[jj] * I + lane];
+            double wb = lane + 1 == le ? 0. : (double)d.wl[(size_t)kn[jj] * I + lane + 1];
+            double fwin = 0., fwout = 0.;
+            if (wt > 0.) fwout += aat * wt; else fwin -= aat * wt;
+            if (wb > 0.) fwin += aat * wb; else fwout -= aat * wb;
+            const double chadv = aj4 * 3. * f;
+            if (chadv < 0.) coadv = aj4 * fwout - chadv;
+            else ciadv = aj4 * fwin + chadv;
+          }
+          chigh += fmax(coadv, ciadv);
+          const double rk3 = 3. * (double)rkpar * d.difhv[oe];
+          clow += aj4 * rk3 * hold * (double)d.wdif[(size_t)e * 9 + 4 * ii];
+          const double hdv = d.heo[oe];
+          const double hdvm = lane > 0 ? (double)d.heo[oe - 1] : 0.;
+          const double hdvp = lane + 1 < le ? (double)d.heo[oe + 1] : 0.;
+          const double hmtop = lane > 0 ? 2. * rvptop / (hdvm + hdv) : 0.;
+          const double hmbot = lane + 1 < le ? 2. * rvpbot / (hdv + hdvp) : 0.;
+          cn += aj4 * adt * (hmtop + hmbot);
+          cdiag += aj4 * fmin(hold, hnew);
+        }
+      }
+      double r = (act && cdiag > 0.) ? (chigh + clow + cn) / cdiag : 0.;
+      stab = seg_max<S>((float)r);
+    }
+    if (lane == 0 && valid && d.kbnd[k] == 0) atomic_max_pos(&d.out[b].stab[s], stab);
+  }
+}
+
+// ===========================================================================
+// k_reduce: per basin (one block each): volume, sub-step counts, time
+// ===========================================================================
+__global__ void __launch_bounds__(1024) k_reduce(Dev d, int nsub, int advance) {
+  const int b = blockIdx.x;
+  const BasinPar &P = d.par[b];
+  BasinOut &O = d.out[b];
+  __shared__ double part[1024];
+  double s = 0.;
+  for (int k = threadIdx.x; k < P.nk; k += blockDim.x) s += d.vol_node[P.k0 + k];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = 512; w > 0; w >>= 1) {
+    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    O.volume = part[0];
+    if (advance) {
+      int mx = 1;
+      for (int sc = 0; sc < P.nsc; sc++) {
+        // scal3sh: sindex = stabind/rstol, rindex = dt*sindex, istot = 1 + rindex
+        float sindex = O.stab[sc] / P.rstol;
+        float rindex = (float)P.dt * sindex;
+        int ist = 1 + (int)rindex;
+        O.stab[sc] = (float)ist;       // now holds the sub-step count of scalar sc
+        mx = ist > mx ? ist : mx;
+        if (ist > P.istot_max) set_status(&O, SHY_EISTOT);
+
+      }
+      O.istot = mx;
+      atomicMax(d.imax, mx);
+      O.dtime += P.dt;
+      O.steps += 1;
+    }
+  }
+}
+
+// rhoset for the initial state (barocl(0): rhov = 0, then rhoset_shell(3)),
+// temperature and salinity taken from the scalar buffer d.sc_in
+template <int S>
+__global__ void __launch_bounds__(256) k_rhoset(Dev d, const int *kbas) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k0 = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  const bool valid = k0 < d.NKN;
+  const int k = valid ? k0 : d.NKN - 1;
+  const int NLV = d.NLV;
+  const int b = kbas[k];
+  const BasinPar &P = d.par[b];
+  const int lmax = d.ilhkv[k];
+  const bool act = lane < lmax;
+  const size_t o = (size_t)k * NLV + lane;
+  if (!(P.ibarcl > 0 && P.itemp && P.isalt)) {
+    if (valid && lane < NLV) d.rho[o] = 0.f;
+    return;
+  }
+  const size_t SN = (size_t)d.NKN * NLV;
+  const float *tv = d.sc_in, *sv = d.sc_in + SN;     // T is scalar 0, S scalar 1
+  const float *hld = d.hldv + (size_t)b * NLV;
+  const double hh = lane < NLV ? 0.5 * (double)hld[lane] : 0.;
+  const double depth = seg_scan_down<S>(act ? 2. * hh : 0., lane) - hh;
+  double r = 0.;
+  const double t = act ? (double)tv[o] : 0., sal = act ? (double)sv[o] : 0.;
+  for (int it = 0; it < 3; it++) {
+    const double dpresc = r * P.grav * hh;
+    double pbc = seg_scan_down<S>(act ? 2. * dpresc : 0., lane) - dpresc;
+    const double rho0 = P.rowass, sigma0 = rho0 - 1000.;
+    double pres = 1.e-5 * (rho0 * P.grav * depth + pbc);
+    r = act ? (double)(float)(sigma_stp_d(sal > 0. ? sal : 0., t, (double)(float)pres) - sigma0) : 0.;
+  }
+  if (valid && lane < NLV) d.rho[o] = (float)r;
+}
+
+
+}  // namespace shy

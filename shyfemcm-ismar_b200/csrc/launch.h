@@ -9,6 +9,7 @@ namespace shy {
 // arguments of the zeta assembly + solve kernel
 struct ZetaArgs {
   const float *zguess;  // initial guess (the old water level, system_solve's z)
+  const float *zprev;   // the level one step earlier (for the extrapolated start), or null
   const float *hia;     // element matrices: hia[c*cs + e*es], c = 3*i + j
   const float *hik;     // element right-hand sides: hik[i*cs + e*es]
   int cs, es;
@@ -24,9 +25,28 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
 void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStream_t st);
 void launch_reduce(const Dev &d, int nsub, int advance, cudaStream_t st);
 void launch_subctl(const Dev &d, cudaGraphConditionalHandle h, cudaStream_t st);
+// shape of the shared-memory zeta solver: CL CTAs of `threads` per basin,
+// rows per CTA (capacity) and nonzeros per CTA (capacity), dynamic smem
+struct ZetaShape {
+  int CL = 0, threads = 0, chunk = 0, nnzcap = 0, halocap = 0;
+  size_t smem = 0;
+};
+
+// maps of the shared-memory zeta solver for one cluster shape:
+// loc[s]  -- local shared-memory column index of CSR slot s (own rows first,
+//            then the CTA's halo slots)
+// push    -- for each row (push_ptr[i]..push_ptr[i+1]) the halo slots of other
+//            CTAs that hold a copy of it, packed (rank << 24) | slot
+struct ZetaMaps {
+  const int *loc = nullptr, *push_ptr = nullptr, *push = nullptr;
+};
+
 cudaError_t launch_zeta(const Dev &d, const ZetaArgs &za, int CL, int threads, int b_first, int nb,
                         cudaStream_t st);
-cudaError_t zeta_kernel_setup(int CL);
-int zeta_max_active_clusters(int CL, int threads);
+cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs, const ZetaMaps &zm,
+                           cudaStream_t st);
+// smem > 0 prepares the shared-memory variant for that many dynamic bytes
+cudaError_t zeta_kernel_setup(int CL, size_t smem);
+int zeta_max_active_clusters(int CL, int threads, size_t smem);
 
 }  // namespace shy

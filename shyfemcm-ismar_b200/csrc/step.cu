@@ -1,0 +1,165 @@
+// step.cu -- the semi-implicit step on sm_100a (kernels in k_*.cuh).
+//
+// Per time step, for all basins of a model at once:
+//   k_column  hydro_transports + hydro_intern + hydro_zeta element part
+//             (hydrodynamic.f90:758-864, 868-1416, 488-733): one warp segment per
+//             element column, vertical system by PCR across lanes, 3x3 element
+//             system of the zeta equation written per element.
+//   k_zeta    system_init/assemble/add_rhs/solve/get (simsys_spkaux.f90:137-705,
+//             sparskit_admin.f90:115-334): one thread-block cluster per basin;
+//             atomic-free gather assembly into CSR in element order (FP64), then
+//             FP32 preconditioned Krylov iterations inside FP64 residual
+//             refinement, all in one persistent launch.
+//   k_final   hydro_transports_final + setzev + element part of setdepth
+//             (hydrodynamic.f90:1468-1578, wetdry.f90:594, elems_dealing.f90:1063-1097).
+//   k_node    nodal part of setdepth + hydro_vertical + per-node volume
+//             (elems_dealing.f90:1010-1137, hydrodynamic.f90:1582-1781).
+//   k_stab    conzstab (concentration.f90:1573-2080): transport stability index.
+//   k_reduce  per basin: total volume (vol_mass), sub-step counts, model time.
+//   k_conz    conz3d_omp (concentration_omp.f90:65-888) for all scalars of a
+//             node column, vertical system by PCR, bndo_impbc, and rhoset
+//             (baroclinic.f90:654-710) after the last sub-step.
+#include <cooperative_groups.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/shygpu.h"
+#include "common.cuh"
+#include "launch.h"
+#include "physics.cuh"
+#include "k_column.cuh"
+#include "k_final.cuh"
+#include "k_node.cuh"
+#include "k_conz.cuh"
+#include "k_zeta.cuh"
+#include "k_zeta_global.cuh"
+
+// ---------------------------------------------------------------------------
+// launch wrappers (host side)
+// ---------------------------------------------------------------------------
+namespace shy {
+
+template <int S>
+static void launch_elem_S(const Dev &d, int which, int init_only, cudaStream_t st, bool cor) {
+  const int threads = 256;
+  const long long nt = (long long)d.NEL * S;
+  const int blocks = (int)((nt + threads - 1) / threads);
+  if (which == 0) {
+    if (cor) k_column<S, true><<<blocks, threads, 0, st>>>(d);
+    else k_column<S, false><<<blocks, threads, 0, st>>>(d);
+  } else {
+    if (cor) k_final<S, true><<<blocks, threads, 0, st>>>(d, init_only);
+    else k_final<S, false><<<blocks, threads, 0, st>>>(d, init_only);
+  }
+}
+
+template <int S>
+static void launch_node_S(const Dev &d, const int *kbas, int which, int a, int b, cudaStream_t st) {
+  const int threads = 256;
+  const long long nt = (long long)d.NKN * S;
+  const int blocks = (int)((nt + threads - 1) / threads);
+  switch (which) {
+    case 0: k_node<S><<<blocks, threads, 0, st>>>(d, kbas, a); break;
+    case 1: k_stab<S><<<blocks, threads, 0, st>>>(d, kbas); break;
+    case 2:   // right-hand sides per PCR: scalars transported together
+      if (d.nsc_max <= 1) k_conz<S, 1><<<blocks, threads, 0, st>>>(d, kbas, a);
+      else if (d.nsc_max <= 2) k_conz<S, 2><<<blocks, threads, 0, st>>>(d, kbas, a);
+      else if (d.nsc_max <= 4) k_conz<S, 4><<<blocks, threads, 0, st>>>(d, kbas, a);
+      else k_conz<S, kMaxScal><<<blocks, threads, 0, st>>>(d, kbas, a);
+      break;
+    case 3: k_rhoset<S><<<blocks, threads, 0, st>>>(d, kbas); break;
+    case 4: k_rho<S><<<blocks, threads, 0, st>>>(d, kbas); break;
+  }
+}
+
+void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool cor) {
+  switch (d.S) {
+    case 1: launch_elem_S<1>(d, which, init_only, st, cor); break;
+    case 2: launch_elem_S<2>(d, which, init_only, st, cor); break;
+    case 4: launch_elem_S<4>(d, which, init_only, st, cor); break;
+    case 8: launch_elem_S<8>(d, which, init_only, st, cor); break;
+    case 16: launch_elem_S<16>(d, which, init_only, st, cor); break;
+    default: launch_elem_S<32>(d, which, init_only, st, cor); break;
+  }
+}
+
+void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStream_t st) {
+  switch (d.S) {
+    case 1: launch_node_S<1>(d, kbas, which, a, b, st); break;
+    case 2: launch_node_S<2>(d, kbas, which, a, b, st); break;
+    case 4: launch_node_S<4>(d, kbas, which, a, b, st); break;
+    case 8: launch_node_S<8>(d, kbas, which, a, b, st); break;
+    case 16: launch_node_S<16>(d, kbas, which, a, b, st); break;
+    default: launch_node_S<32>(d, kbas, which, a, b, st); break;
+  }
+}
+
+// control of the device-driven transport sub-step loop (body of a CUDA-graph
+// WHILE node): advance the sub-step index and keep looping while any basin
+// has sub-steps left (scal3sh's isact = 1..istot, concentration.f90:728).
+__global__ void k_subctl(Dev d, cudaGraphConditionalHandle h) {
+  const int nj = *d.subj + 1;
+  *d.subj = nj;
+  *d.nsub_launched += 2;
+  cudaGraphSetConditional(h, nj < *d.imax ? 1u : 0u);
+}
+
+void launch_subctl(const Dev &d, cudaGraphConditionalHandle h, cudaStream_t st) {
+  k_subctl<<<1, 1, 0, st>>>(d, h);
+}
+
+void launch_reduce(const Dev &d, int nsub, int advance, cudaStream_t st) {
+  k_reduce<<<d.nbasin, 1024, 0, st>>>(d, nsub, advance);
+}
+
+static cudaLaunchConfig_t zeta_config(int CL, int threads, int nclusters, size_t smem, cudaStream_t st,
+                                      cudaLaunchAttribute *attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nclusters * CL, 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+cudaError_t launch_zeta(const Dev &d, const ZetaArgs &za, int CL, int threads, int b_first,
+                        int nb, cudaStream_t st) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = zeta_config(CL, threads, nb, 0, st, attr);
+  return cudaLaunchKernelEx(&cfg, k_zeta, d, za, CL, b_first);
+}
+
+cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs, const ZetaMaps &zm,
+                           cudaStream_t st) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = zeta_config(zs.CL, zs.threads, d.nbasin, zs.smem, st, attr);
+  return cudaLaunchKernelEx(&cfg, k_zeta_sm, d, za, zs, zm);
+}
+
+cudaError_t zeta_kernel_setup(int CL, size_t smem) {
+  cudaError_t e = cudaSuccess;
+  if (CL > 8) {
+    e = cudaFuncSetAttribute(k_zeta, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_zeta_sm, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  }
+  if (e == cudaSuccess && smem > 0)
+    e = cudaFuncSetAttribute(k_zeta_sm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return e;
+}
+
+int zeta_max_active_clusters(int CL, int threads, size_t smem) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = zeta_config(CL, threads, 1, smem, nullptr, attr);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, smem > 0 ? (const void *)k_zeta_sm : (const void *)k_zeta, &cfg) != cudaSuccess)
+    return -1;
+  return n;
+}
+
+}  // namespace shy

@@ -176,12 +176,12 @@ class Model:
         check(lib().shygpu_set_forcing(self.h, ib, p(tauxnv), p(tauynv), p(ppv), p(rqv)),
               "set_forcing")
 
-    KERNELS = ("column", "zeta", "final", "node", "stab", "reduce", "conz")
+    KERNELS = ("column", "zeta", "final", "node", "stab", "reduce", "conz", "rho")
 
     def profile_steps(self, nsteps):
         """Per-kernel device time (ms, summed) and launch counts over nsteps."""
-        ms = (C.c_double * 7)()
-        cnt = (C.c_int32 * 7)()
+        ms = (C.c_double * 8)()
+        cnt = (C.c_int32 * 8)()
         check(lib().shygpu_profile_steps(self.h, int(nsteps), ms, cnt), "profile_steps")
         return {k: (ms[i], cnt[i]) for i, k in enumerate(self.KERNELS)}
 

@@ -16,8 +16,8 @@ PKG = HERE.parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = HERE / "libshygpu.so"
-SOURCES = ["kernels.cu", "host.cu"]
-HEADERS = ["common.cuh", "launch.h"]
+SOURCES = ["step.cu", "host.cu"]
+HEADERS = ["common.cuh", "launch.h", "physics.cuh", "k_column.cuh", "k_final.cuh", "k_node.cuh", "k_conz.cuh", "k_zeta.cuh", "k_zeta_global.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
