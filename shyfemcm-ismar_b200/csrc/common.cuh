@@ -79,6 +79,8 @@ struct Dev {
   int *rowptr, *col;          // CSR over all nodes (block diagonal)
   int *slot_ptr, *slot_src;   // gather of element entries per CSR slot
   int *inc_ptr, *inc;         // node -> (e*3+ii) incidence, increasing e
+  int4 *incx;                 // the same entries packed: {e, ii | ilhv(e) << 2,
+                              //  node of the next vertex, node of the one after}
   double *val64, *rhs64, *x64;
   float *val32, *dinv32, *r32, *p32, *q32, *z32, *e32, *s32, *t32, *rh32, *v32;
   // element system written by the column kernel (SoA): hia[c*NEL+e], hik[c*NEL+e]

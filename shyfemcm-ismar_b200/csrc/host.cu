@@ -234,6 +234,9 @@ struct Arena {
 // ---------------------------------------------------------------------------
 // the model
 // ---------------------------------------------------------------------------
+static const int kMaxZetaClasses = 10;  // zeta launch classes: 2 variants x cluster sizes 1..16
+static int next_pow2(int n);
+
 struct shygpu_model {
   int nbasin = 0, NKN = 0, NEL = 0, NLV = 0, S = 1, nsc_max = 0, NNZ = 0;
   bool cor = false;
@@ -247,10 +250,12 @@ struct shygpu_model {
   int cur = 0, sc_cur = 0;
   cudaStream_t stream = nullptr;
   // options
-  int nsub = 2, use_graph = 1, CL = 8, zthreads = 1024, max_outer = 12, sym = 1;
+  int nsub = 2, use_graph = 1, max_outer = 12, sym = 1;
   int zvariant = 1;                  // 1: shared-memory zeta solver when it fits
-  bool use_sm = false;
-  ZetaShape zs;
+  int zforce_CL = 0, zforce_threads = 0;   // > 0: one launch class with this shape
+  std::vector<ZetaClass> zcl;        // launch classes of the zeta solver
+  cudaStream_t side[kMaxZetaClasses] = {};
+  cudaEvent_t ev_fork = nullptr, ev_join[kMaxZetaClasses] = {};
   std::vector<int> rowptr_h, col_h;  // global CSR pattern (host copy)
   int *zmap_ptrs[3] = {nullptr, nullptr, nullptr};
   ZetaMaps zm;
@@ -280,54 +285,140 @@ static void drop_graphs(shygpu_model *m) {
 
 static int check_cluster_shape(int CL, int threads, size_t smem);
 
-// Launch shape of the zeta solver.  The shared-memory variant keeps each
-// CTA's rows (row pointers, packed columns, FP32 values) and seven FP32
-// vectors in shared memory; it is used for symmetric systems when every
-// basin's largest CTA slice fits, else the global-memory variant.
-static void free_zeta_maps(shygpu_model *m) {
+// ---------------------------------------------------------------------------
+// Launch plan of the zeta solver.  Basins are grouped into classes with one
+// cluster shape each (at most 1250 rows per CTA, 640 threads); the
+// classes' launches run concurrently.  The shared-memory variant keeps each
+// CTA's rows (row pointers, local columns, FP32 values) and seven FP32
+// vectors plus a halo in shared memory; it serves symmetric systems whose
+// slices fit 227 KB, the global-memory variant the rest.
+// ---------------------------------------------------------------------------
+static const size_t kSmemMax = 227 * 1024;
+
+static void free_zeta_plan(shygpu_model *m) {
   for (int *&p : m->zmap_ptrs) { if (p) cudaFree(p); p = nullptr; }
   m->zm = ZetaMaps();
+  for (ZetaClass &c : m->zcl)
+    if (c.d_blist) cudaFree(c.d_blist);
+  m->zcl.clear();
 }
 
-// Local column indices, halo slots and push lists of the shared-memory
-// zeta solver for cluster size CL (rows of basin b split in CL contiguous
-// slices of ceil(nk/CL) rows).
-static int build_zeta_maps(shygpu_model *m, int CL, ZetaShape &zs) {
+// rows of CTA q of basin bp for cluster size CL
+static inline void cta_rows(const BasinPar &bp, int CL, int q, int &a, int &e) {
+  const int cb = (bp.nk + CL - 1) / CL;
+  a = bp.k0 + std::min(bp.nk, q * cb);
+  e = bp.k0 + std::min(bp.nk, (q + 1) * cb);
+}
+
+// sorted non-local columns of the rows a..e
+static std::vector<int> halo_of(const shygpu_model *m, int a, int e) {
+  std::vector<int> halo;
+  for (int s = m->rowptr_h[a]; s < m->rowptr_h[e]; s++) {
+    const int c = m->col_h[s];
+    if (c < a || c >= e) halo.push_back(c);
+  }
+  std::sort(halo.begin(), halo.end());
+  halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
+  return halo;
+}
+
+static size_t sm_bytes(const ZetaShape &zs) {
+  size_t b = (size_t)4 * (zs.chunk + 1) + (size_t)8 * zs.nnzcap + (size_t)28 * zs.chunk + (size_t)4 * zs.halocap;
+  return (b + 15) & ~(size_t)15;
+}
+
+static int build_zeta_plan_impl(shygpu_model *m, int forceCL, int forceThreads);
+
+// forceCL > 0: one class with that shape for every basin.  A plan that
+// cannot be built leaves no plan (the step then refuses to run).
+static int build_zeta_plan(shygpu_model *m, int forceCL, int forceThreads) {
+  const int st = build_zeta_plan_impl(m, forceCL, forceThreads);
+  if (st != SHY_OK) free_zeta_plan(m);
+  return st;
+}
+
+static int build_zeta_plan_impl(shygpu_model *m, int forceCL, int forceThreads) {
+  free_zeta_plan(m);
   const int NKN = m->NKN;
-  const std::vector<int> &rp = m->rowptr_h;
-  std::vector<int> loc(rp[NKN], 0);
+  std::vector<int> loc(m->rowptr_h[NKN], 0);
   std::vector<std::vector<int>> pushl(NKN);
   for (int b = 0; b < m->nbasin; b++) {
     const BasinPar &bp = m->par[b];
-    const int cb = (bp.nk + CL - 1) / CL;
-    zs.chunk = std::max(zs.chunk, cb);
-    for (int q = 0; q < CL; q++) {
-      const int a = bp.k0 + std::min(bp.nk, q * cb), e = bp.k0 + std::min(bp.nk, (q + 1) * cb);
-      const int nloc = e - a;
-      zs.nnzcap = std::max(zs.nnzcap, rp[e] - rp[a]);
-      std::vector<int> halo;
-      for (int s = rp[a]; s < rp[e]; s++) {
-        const int c = m->col_h[s];
-        if (c < a || c >= e) halo.push_back(c);
+    int CL, th;
+    if (forceCL > 0) { CL = forceCL; th = forceThreads; }
+    else {
+      // the thread count depends on nothing but the variant, so that the
+      // reduction order of a basin is the same alone and in any batch
+      CL = std::min(16, next_pow2((bp.nk + 1249) / 1250));
+      th = 640;
+    }
+    bool sm = m->sym && m->zvariant;
+    ZetaShape zs;
+    zs.CL = CL; zs.threads = th;
+    std::vector<std::vector<int>> halos(CL);
+    if (sm) {
+      for (int q = 0; q < CL; q++) {
+        int a, e;
+        cta_rows(bp, CL, q, a, e);
+        zs.chunk = std::max(zs.chunk, e - a);
+        zs.nnzcap = std::max(zs.nnzcap, m->rowptr_h[e] - m->rowptr_h[a]);
+        halos[q] = halo_of(m, a, e);
+        zs.halocap = std::max(zs.halocap, (int)halos[q].size());
       }
-      std::sort(halo.begin(), halo.end());
-      halo.erase(std::unique(halo.begin(), halo.end()), halo.end());
-      zs.halocap = std::max(zs.halocap, (int)halo.size());
-      for (int s = rp[a]; s < rp[e]; s++) {
-        const int c = m->col_h[s];
-        if (c >= a && c < e) loc[s] = c - a;
-        else loc[s] = nloc + (int)(std::lower_bound(halo.begin(), halo.end(), c) - halo.begin());
+      sm = sm_bytes(zs) <= kSmemMax;
+    }
+    if (!sm && forceCL <= 0) { CL = std::min(16, next_pow2((bp.nk + 4095) / 4096)); th = 1024; }
+    // the class of this variant and cluster size (its CTAs take the largest
+    // thread count any of its basins wants)
+    ZetaClass *cls = nullptr;
+    for (ZetaClass &c : m->zcl)
+      if (c.sm == sm && c.CL == CL) cls = &c;
+    if (!cls) {
+      m->zcl.emplace_back();
+      cls = &m->zcl.back();
+      cls->sm = sm; cls->CL = CL; cls->threads = th;
+      cls->zs.CL = CL;
+    }
+    cls->threads = std::max(cls->threads, th);
+    cls->zs.threads = cls->threads;
+    cls->basins.push_back(b);
+    if (sm) {
+      cls->zs.chunk = std::max(cls->zs.chunk, zs.chunk);
+      cls->zs.nnzcap = std::max(cls->zs.nnzcap, zs.nnzcap);
+      cls->zs.halocap = std::max(cls->zs.halocap, zs.halocap);
+      for (int q = 0; q < CL; q++) {
+        int a, e;
+        cta_rows(bp, CL, q, a, e);
+        const int nloc = e - a;
+        const std::vector<int> &halo = halos[q];
+        for (int s = m->rowptr_h[a]; s < m->rowptr_h[e]; s++) {
+          const int c = m->col_h[s];
+          if (c >= a && c < e) loc[s] = c - a;
+          else loc[s] = nloc + (int)(std::lower_bound(halo.begin(), halo.end(), c) - halo.begin());
+        }
+        for (size_t h = 0; h < halo.size(); h++)   // the owner of halo[h] pushes into slot nloc+h of q
+          pushl[halo[h]].push_back((q << 24) | (nloc + (int)h));
       }
-      for (size_t h = 0; h < halo.size(); h++)     // the owner of halo[h] pushes into slot nloc+h of q
-        pushl[halo[h]].push_back((q << 24) | (nloc + (int)h));
     }
   }
+  // validate every class shape (occupancy with its shared memory)
+  size_t maxsm = 0;
+  int maxCL = 1;
+  for (ZetaClass &c : m->zcl) {
+    if (c.sm) { c.zs.smem = sm_bytes(c.zs); maxsm = std::max(maxsm, c.zs.smem); }
+    maxCL = std::max(maxCL, c.CL);
+  }
+  for (ZetaClass &c : m->zcl) ST_TRY(check_cluster_shape(c.CL, c.threads, c.sm ? c.zs.smem : 0));
+  if (maxsm > 0 || maxCL > 8) {
+    cudaError_t e = zeta_kernel_setup(maxCL, maxsm);
+    if (e != cudaSuccess) return fail(SHY_ECUDA, "zeta kernel setup: %s", cudaGetErrorString(e));
+  }
+  // maps and basin lists on the device
   std::vector<int> pptr(NKN + 1, 0), push;
   for (int i = 0; i < NKN; i++) {
     pptr[i + 1] = pptr[i] + (int)pushl[i].size();
     push.insert(push.end(), pushl[i].begin(), pushl[i].end());
   }
-  free_zeta_maps(m);
   int *dl = nullptr, *dp = nullptr, *dq = nullptr;
   CUDA_TRY(cudaMalloc(&dl, sizeof(int) * std::max<size_t>(loc.size(), 1)));
   m->zmap_ptrs[0] = dl;
@@ -339,51 +430,35 @@ static int build_zeta_maps(shygpu_model *m, int CL, ZetaShape &zs) {
   CUDA_TRY(cudaMemcpy(dp, pptr.data(), sizeof(int) * pptr.size(), cudaMemcpyHostToDevice));
   if (!push.empty()) CUDA_TRY(cudaMemcpy(dq, push.data(), sizeof(int) * push.size(), cudaMemcpyHostToDevice));
   m->zm.loc = dl; m->zm.push_ptr = dp; m->zm.push = dq;
+  for (ZetaClass &c : m->zcl) {
+    CUDA_TRY(cudaMalloc(&c.d_blist, sizeof(int) * c.basins.size()));
+    CUDA_TRY(cudaMemcpy(c.d_blist, c.basins.data(), sizeof(int) * c.basins.size(), cudaMemcpyHostToDevice));
+  }
+  if ((int)m->zcl.size() > kMaxZetaClasses) return fail(SHY_EARG, "too many zeta launch classes");
+  m->zforce_CL = forceCL;
+  m->zforce_threads = forceThreads;
   return SHY_OK;
 }
 
-static int choose_zeta_shape(shygpu_model *m, int CL, int threads) {
-  const size_t kSmemMax = 227 * 1024;
-  ZetaShape zs;
-  zs.CL = CL; zs.threads = threads;
-  bool fits = m->sym && m->zvariant;
-  if (fits) {
-    for (int b = 0; b < m->nbasin; b++) {      // capacity before building maps
-      const BasinPar &bp = m->par[b];
-      const int cb = (bp.nk + CL - 1) / CL;
-      zs.chunk = std::max(zs.chunk, cb);
-      for (int q = 0; q < CL; q++) {
-        int a = bp.k0 + std::min(bp.nk, q * cb), e = bp.k0 + std::min(bp.nk, (q + 1) * cb);
-        zs.nnzcap = std::max(zs.nnzcap, m->rowptr_h[e] - m->rowptr_h[a]);
-      }
-    }
-    // rows, columns, values, seven vectors (the u vector with its halo)
-    zs.smem = (size_t)4 * (zs.chunk + 1) + (size_t)8 * zs.nnzcap + (size_t)28 * zs.chunk;
-    fits = zs.smem + 8 * 1024 <= kSmemMax;
-    if (fits) {
-      ST_TRY(build_zeta_maps(m, CL, zs));
-      zs.smem = (size_t)4 * (zs.chunk + 1) + (size_t)8 * zs.nnzcap + (size_t)28 * zs.chunk +
-                (size_t)4 * zs.halocap;
-      zs.smem = (zs.smem + 15) & ~(size_t)15;
-      fits = zs.smem <= kSmemMax && check_cluster_shape(CL, threads, zs.smem) == SHY_OK;
+// all classes' launches; with more than one class they fork from the model's
+// stream onto side streams and join back (also inside graph capture)
+static int launch_zeta_plan(shygpu_model *m, const Dev &d, ZetaArgs za) {
+  const int nc = (int)m->zcl.size();
+  if (nc == 0) return fail(SHY_ESTATE, "zeta solver: no launch plan (an option set an unusable shape)");
+  if (nc > 1) CUDA_TRY(cudaEventRecord(m->ev_fork, m->stream));
+  for (int i = 0; i < nc; i++) {
+    const ZetaClass &c = m->zcl[i];
+    cudaStream_t st = nc > 1 ? m->side[i] : m->stream;
+    if (nc > 1) CUDA_TRY(cudaStreamWaitEvent(st, m->ev_fork, 0));
+    za.blist = c.d_blist;
+    cudaError_t e = c.sm ? launch_zeta_sm(d, za, c.zs, m->zm, (int)c.basins.size(), st)
+                         : launch_zeta(d, za, c.CL, c.threads, (int)c.basins.size(), st);
+    if (e != cudaSuccess) return fail(SHY_ECUDA, "zeta solve launch: %s", cudaGetErrorString(e));
+    if (nc > 1) {
+      CUDA_TRY(cudaEventRecord(m->ev_join[i], st));
+      CUDA_TRY(cudaStreamWaitEvent(m->stream, m->ev_join[i], 0));
     }
   }
-  if (fits) {
-    m->use_sm = true;
-    m->zs = zs;
-  } else {
-    ST_TRY(check_cluster_shape(CL, threads, 0));
-    m->use_sm = false;
-  }
-  m->CL = CL;
-  m->zthreads = threads;
-  return SHY_OK;
-}
-
-static int launch_zeta_any(shygpu_model *m, const Dev &d, const ZetaArgs &za) {
-  cudaError_t e = m->use_sm ? launch_zeta_sm(d, za, m->zs, m->zm, m->stream)
-                            : launch_zeta(d, za, m->CL, m->zthreads, 0, m->nbasin, m->stream);
-  if (e != cudaSuccess) return fail(SHY_ECUDA, "zeta solve launch: %s", cudaGetErrorString(e));
   return SHY_OK;
 }
 
@@ -429,7 +504,12 @@ extern "C" int shygpu_destroy(shygpu_model *m) {
     g_models.erase(it);
   }
   drop_graphs(m);
-  free_zeta_maps(m);
+  free_zeta_plan(m);
+  for (int i = 0; i < kMaxZetaClasses; i++) {
+    if (m->side[i]) cudaStreamDestroy(m->side[i]);
+    if (m->ev_join[i]) cudaEventDestroy(m->ev_join[i]);
+  }
+  if (m->ev_fork) cudaEventDestroy(m->ev_fork);
   m->arena.release();
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
@@ -492,6 +572,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   std::vector<float2> avol((size_t)NKN * NLV, make_float2(0.f, 0.f));
   std::vector<float> hlv((size_t)nbasin * NLV, 0.f), hldv((size_t)nbasin * NLV, 0.f), tide;
   std::vector<int> rowptr(1, 0), col, slot_ptr(1, 0), slot_src, inc_ptr(1, 0), inc;
+  std::vector<int4> incx;
   int k0 = 0, e0 = 0;
   int nsc_max = 0;
   for (int b = 0; b < nbasin; b++) {
@@ -605,7 +686,12 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     for (size_t s = 0; s + 1 < pt.slot_ptr.size(); s++) slot_ptr.push_back(src0 + pt.slot_ptr[s + 1]);
     for (int v : pt.slot_src) slot_src.push_back(9 * e0 + v);
     for (int k = 0; k < nkn; k++) inc_ptr.push_back(inc0 + pt.inc_ptr[k + 1]);
-    for (int v : pt.inc) inc.push_back(3 * e0 + v);
+    for (int v : pt.inc) {
+      inc.push_back(3 * e0 + v);
+      const int el = v / 3, ii = v - 3 * el;
+      const int ja = ii == 0 ? 1 : 0, jb = ii == 2 ? 1 : 2;    // the other two vertices, in order
+      incx.push_back(make_int4(e0 + el, ii | (bs.ilhv[el] << 2), k0 + nv[3 * el + ja], k0 + nv[3 * el + jb]));
+    }
     // parameters
     BasinPar &bp = m->par[b];
     memset(&bp, 0, sizeof bp);
@@ -656,7 +742,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       A.upload(&d.areakv, areakv) || A.upload(&d.avol, avol) ||
       A.upload(&d.rowptr, rowptr) || A.upload(&d.col, col) ||
       A.upload(&d.slot_ptr, slot_ptr) || A.upload(&d.slot_src, slot_src) ||
-      A.upload(&d.inc_ptr, inc_ptr) || A.upload(&d.inc, inc) || A.upload(&m->kbas, kbas))
+      A.upload(&d.inc_ptr, inc_ptr) || A.upload(&d.inc, inc) || A.upload(&d.incx, incx) ||
+      A.upload(&m->kbas, kbas))
     return bail(SHY_ECAPACITY);
   const size_t nnz = col.size(), EL = (size_t)NEL * NLV, NL = (size_t)NKN * NLV;
   const size_t NSC = (size_t)std::max(nsc_max, 1) * NL;
@@ -684,11 +771,14 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   // zeta solver launch shape: one cluster per basin, about 2k rows per CTA
   m->rowptr_h = rowptr;
   m->col_h = col;
-  int maxn = 0;
-  for (int b = 0; b < nbasin; b++) maxn = std::max(maxn, B[b].nkn);
+  if (cudaEventCreateWithFlags(&m->ev_fork, cudaEventDisableTiming) != cudaSuccess)
+    return bail(fail(SHY_ECUDA, "event creation failed"));
+  for (int i = 0; i < kMaxZetaClasses; i++)
+    if (cudaStreamCreateWithFlags(&m->side[i], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&m->ev_join[i], cudaEventDisableTiming) != cudaSuccess)
+      return bail(fail(SHY_ECUDA, "stream creation failed"));
   {
-    int CL = std::min(16, next_pow2((maxn + 2047) / 2048));
-    int st = choose_zeta_shape(m, CL, maxn >= 4096 ? 1024 : 512);
+    int st = build_zeta_plan(m, 0, 0);
     if (st) return bail(st);
   }
   m->out_h.resize(nbasin);
@@ -706,26 +796,33 @@ extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value
   int iv = (int)value;
   if (n == "use_graph") m->use_graph = iv != 0;
   else if (n == "cluster_size" || n == "zeta_threads") {
-    int CL = m->CL, th = m->zthreads;
+    // one launch class with this shape for every basin (0 returns to the automatic plan)
+    int CL = m->zforce_CL > 0 ? m->zforce_CL : (m->zcl.empty() ? 1 : m->zcl[0].CL);
+    int th = m->zforce_threads > 0 ? m->zforce_threads : (m->zcl.empty() ? 512 : m->zcl[0].threads);
     if (n == "cluster_size") {
-      if (iv < 1 || iv > 16 || (iv & (iv - 1))) return fail(SHY_EARG, "cluster_size: power of two 1..16");
+      if (iv != 0 && (iv < 1 || iv > 16 || (iv & (iv - 1)))) return fail(SHY_EARG, "cluster_size: power of two 1..16");
       CL = iv;
     } else {
-      if (iv < 64 || iv > 1024 || iv % 32) return fail(SHY_EARG, "zeta_threads: multiple of 32 in 64..1024");
+      if (iv != 0 && (iv < 64 || iv > 1024 || iv % 32)) return fail(SHY_EARG, "zeta_threads: multiple of 32 in 64..1024");
       th = iv;
     }
-    ST_TRY(choose_zeta_shape(m, CL, th));
+    if (CL == 0 || th == 0) ST_TRY(build_zeta_plan(m, 0, 0));
+    else if (int st = build_zeta_plan(m, CL, th)) {
+      drop_graphs(m);
+      build_zeta_plan(m, 0, 0);   // back to the automatic plan, report the refused shape
+      return st;
+    }
   }
   else if (n == "zeta_variant") {   // 0: vectors in global memory, 1: shared memory when it fits
     m->zvariant = iv != 0;
-    ST_TRY(choose_zeta_shape(m, m->CL, m->zthreads));
+    ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
   }
   else if (n == "inner_rtol") { if (!(value > 0 && value < 1)) return fail(SHY_EARG, "inner_rtol in (0,1)"); m->inner_rtol = (float)value; }
   else if (n == "max_outer") { if (iv < 1 || iv > 100) return fail(SHY_EARG, "max_outer 1..100"); m->max_outer = iv; }
   else if (n == "symmetric") {
     if (iv && m->cor) return fail(SHY_EARG, "Coriolis: the system is not symmetric");
     m->sym = iv != 0;
-    ST_TRY(choose_zeta_shape(m, m->CL, m->zthreads));
+    ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
   }
   else return fail(SHY_EARG, "unknown option '%s'", name);
   drop_graphs(m);
@@ -736,12 +833,13 @@ extern "C" double shygpu_get_option(shygpu_model *m, const char *name) {
   if (!m || !name) return -1;
   std::string n(name);
   if (n == "use_graph") return m->use_graph;
-  if (n == "cluster_size") return m->CL;
-  if (n == "zeta_threads") return m->zthreads;
+  if (n == "cluster_size") return m->zcl.empty() ? -1 : m->zcl[0].CL;
+  if (n == "zeta_threads") return m->zcl.empty() ? -1 : m->zcl[0].threads;
+  if (n == "zeta_classes") return (double)m->zcl.size();
   if (n == "inner_rtol") return m->inner_rtol;
   if (n == "max_outer") return m->max_outer;
   if (n == "symmetric") return m->sym;
-  if (n == "zeta_variant") return m->use_sm ? 1 : 0;
+  if (n == "zeta_variant") return m->zcl.empty() ? -1 : (m->zcl[0].sm ? 1 : 0);
   if (n == "launches_per_step") return m->launches_per_step;
   return -1;
 }
@@ -847,7 +945,7 @@ static int enqueue_hydro(shygpu_model *m, const Dev &d) {
   ZetaArgs za{};
   za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
   za.explicit_mode = 0; za.inner_rtol = m->inner_rtol; za.max_outer = m->max_outer; za.sym = m->sym;
-  ST_TRY(launch_zeta_any(m, d, za));
+  ST_TRY(launch_zeta_plan(m, d, za));
   launch_elem(d, 1, 0, m->stream, m->cor);
   launch_node(d, m->kbas, 0, 0, 0, m->stream);
   return SHY_OK;
@@ -1071,7 +1169,7 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
     ZetaArgs za{};
     za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
     za.inner_rtol = m->inner_rtol; za.max_outer = m->max_outer; za.sym = m->sym;
-    if ((st = launch_zeta_any(m, d, za)) != SHY_OK) break;
+    if ((st = launch_zeta_plan(m, d, za)) != SHY_OK) break;
     kind[n] = 1; cudaEventRecord(ev[++n], m->stream);
     launch_elem(d, 1, 0, m->stream, m->cor); kind[n] = 2; cudaEventRecord(ev[++n], m->stream);
     launch_node(d, m->kbas, 0, 0, 0, m->stream); kind[n] = 3; cudaEventRecord(ev[++n], m->stream);
@@ -1137,6 +1235,7 @@ struct Simsys {
   float *stage_h = nullptr;           // pinned [nel][12]: hia(3x3 row-major i,j), hik(3)
   float *stage_d = nullptr;
   float *z_d = nullptr, *zout_d = nullptr;
+  int *d_blist0 = nullptr;            // the one-entry basin list {0} of the solve launch
   float dt_rhs = 0.f;
   std::vector<float> rqv_h;
   double rtol = 1e-8, atol = 1e-8;
@@ -1200,7 +1299,8 @@ static int simsys_init_impl() {
       A.alloc(&d.p32, n) || A.alloc(&d.q32, n) || A.alloc(&d.z32, n) || A.alloc(&d.e32, n) ||
       A.alloc(&d.s32, n) || A.alloc(&d.t32, n) || A.alloc(&d.rh32, n) || A.alloc(&d.v32, n) ||
       A.alloc(&d.rqv, n) || A.alloc(&g_sys.stage_d, (size_t)12 * g_sys.nel) ||
-      A.alloc(&g_sys.z_d, n) || A.alloc(&g_sys.zout_d, n))
+      A.alloc(&g_sys.z_d, n) || A.alloc(&g_sys.zout_d, n) ||
+      A.upload(&g_sys.d_blist0, std::vector<int>(1, 0)))
     return SHY_ECAPACITY;
   d.zn = g_sys.zout_d;
   CUDA_TRY(cudaMallocHost((void **)&g_sys.stage_h, sizeof(float) * 12 * g_sys.nel));
@@ -1278,7 +1378,8 @@ static int simsys_solve_impl(int n, const float *z) {
   int CL = n >= 16384 ? 8 : (n >= 4096 ? 4 : (n >= 1024 ? 2 : 1));
   int threads = n >= 4096 ? 1024 : 512;
   ST_TRY(check_cluster_shape(CL, threads, 0));
-  cudaError_t e = launch_zeta(d, za, CL, threads, 0, 1, st);
+  za.blist = g_sys.d_blist0;
+  cudaError_t e = launch_zeta(d, za, CL, threads, 1, st);
   if (e != cudaSuccess) return fail(SHY_ECUDA, "system_solve launch: %s", cudaGetErrorString(e));
   g_launches += 1;
   BasinOut o;

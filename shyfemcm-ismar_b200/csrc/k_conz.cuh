@@ -108,10 +108,11 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
     }
     // horizontal fluxes: sum over the incident elements of aj4*(3*fl - hdif)
     if (act) {
+#pragma unroll 2
       for (int p = pbeg; p < pend; p++) {
-        const int q = d.inc[p];
-        const int e = q / 3, ii = q - 3 * e;
-        if (lane >= d.ilhv[e]) continue;
+        const int4 ix = d.incx[p];           // element, vertex | layers, other two nodes
+        const int e = ix.x, ii = ix.y & 3;
+        if (lane >= (ix.y >> 2)) continue;
         const float4 e0 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8);
         const float4 e1 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8 + 4);
         const float bb[3] = {e0.x, e0.y, e0.z}, cc[3] = {e0.w, e1.x, e1.y};
@@ -126,10 +127,9 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
           if (f3[jj] < 0.f) { itot++; isum += jj + 1; }
         }
         if (itot == 0 && !anyrk) continue;      // no horizontal flux for this vertex
-        const int4 en = d.enode[e];
         const float hmed = anyrk ? rso * d.hen[oe] + rsot * d.heo[oe] : 0.f;
         const float dfh = anyrk ? d.difhv[oe] : 0.f;
-        const int kja = ii == 0 ? en.y : en.x, kjb = ii == 2 ? en.y : en.z;
+        const int kja = ix.z, kjb = ix.w;
         const float fii = sel3(f3, ii);
 #pragma unroll
         for (int r = 0; r < NR; r++) {

@@ -26,10 +26,10 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   const float *hlv = d.hlv + (size_t)b * NLV;
   const double hldl = lane < NLV ? (double)hld[lane] : 0.;
   double hsum = 0., vf = 0., va = 0.;
+#pragma unroll 2
   for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
-    const int q = d.inc[p];
-    const int e = q / 3, ii = q - 3 * e;
-    const int le = d.ilhv[e];
+    const int4 ix = d.incx[p];
+    const int e = ix.x, ii = ix.y & 3, le = ix.y >> 2;
     if (lane >= le) continue;
     const float *evp = d.ev8 + (size_t)e * 8;
     const double aj = evp[6];

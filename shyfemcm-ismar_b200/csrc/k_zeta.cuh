@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(1024) k_zeta_sm(Dev d, ZetaArgs za, ZetaShape 
   cg::cluster_group cl = cg::this_cluster();
   const int CL = zs.CL, chunk = zs.chunk;
   const int rank = (int)cl.block_rank();
-  const int b = (int)(blockIdx.x / CL);
+  const int b = za.blist[blockIdx.x / CL];
   const BasinPar &P = d.par[b];
   BasinOut &O = d.out[b];
   extern __shared__ __align__(16) unsigned char smem[];

@@ -10,10 +10,10 @@ namespace shy {
 // ---------------------------------------------------------------------------
 // global-memory variant
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_zeta(Dev d, ZetaArgs za, int CL, int b_first) {
+__global__ void __launch_bounds__(1024) k_zeta(Dev d, ZetaArgs za, int CL) {
   cg::cluster_group cl = cg::this_cluster();
   const int rank = (int)cl.block_rank();
-  const int b = b_first + (int)(blockIdx.x / CL);
+  const int b = za.blist[blockIdx.x / CL];
   const BasinPar &P = d.par[b];
   BasinOut &O = d.out[b];
   __shared__ double wbuf[4 * 32];

@@ -2,12 +2,15 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace shy {
 
 // arguments of the zeta assembly + solve kernel
 struct ZetaArgs {
+  const int *blist;     // basin of each cluster of the launch (cluster c solves blist[c])
   const float *zguess;  // initial guess (the old water level, system_solve's z)
   const float *zprev;   // the level one step earlier (for the extrapolated start), or null
   const float *hia;     // element matrices: hia[c*cs + e*es], c = 3*i + j
@@ -41,10 +44,19 @@ struct ZetaMaps {
   const int *loc = nullptr, *push_ptr = nullptr, *push = nullptr;
 };
 
-cudaError_t launch_zeta(const Dev &d, const ZetaArgs &za, int CL, int threads, int b_first, int nb,
-                        cudaStream_t st);
+// a group of basins solved by one launch with one cluster shape
+struct ZetaClass {
+  bool sm = false;                 // shared-memory variant (else global memory)
+  int CL = 1, threads = 512;
+  ZetaShape zs;                    // capacities of the shared-memory variant
+  std::vector<int> basins;
+  int *d_blist = nullptr;          // device copy of basins
+};
+
+// nb clusters of CL CTAs; cluster c solves basin za.blist[c]
+cudaError_t launch_zeta(const Dev &d, const ZetaArgs &za, int CL, int threads, int nb, cudaStream_t st);
 cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs, const ZetaMaps &zm,
-                           cudaStream_t st);
+                           int nb, cudaStream_t st);
 // smem > 0 prepares the shared-memory variant for that many dynamic bytes
 cudaError_t zeta_kernel_setup(int CL, size_t smem);
 int zeta_max_active_clusters(int CL, int threads, size_t smem);

@@ -128,17 +128,16 @@ static cudaLaunchConfig_t zeta_config(int CL, int threads, int nclusters, size_t
   return cfg;
 }
 
-cudaError_t launch_zeta(const Dev &d, const ZetaArgs &za, int CL, int threads, int b_first,
-                        int nb, cudaStream_t st) {
+cudaError_t launch_zeta(const Dev &d, const ZetaArgs &za, int CL, int threads, int nb, cudaStream_t st) {
   cudaLaunchAttribute attr[1];
   cudaLaunchConfig_t cfg = zeta_config(CL, threads, nb, 0, st, attr);
-  return cudaLaunchKernelEx(&cfg, k_zeta, d, za, CL, b_first);
+  return cudaLaunchKernelEx(&cfg, k_zeta, d, za, CL);
 }
 
 cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs, const ZetaMaps &zm,
-                           cudaStream_t st) {
+                           int nb, cudaStream_t st) {
   cudaLaunchAttribute attr[1];
-  cudaLaunchConfig_t cfg = zeta_config(zs.CL, zs.threads, d.nbasin, zs.smem, st, attr);
+  cudaLaunchConfig_t cfg = zeta_config(zs.CL, zs.threads, nb, zs.smem, st, attr);
   return cudaLaunchKernelEx(&cfg, k_zeta_sm, d, za, zs, zm);
 }
 

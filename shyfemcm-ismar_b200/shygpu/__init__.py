@@ -40,10 +40,12 @@ class ShyError(RuntimeError):
 
 def lib():
     """Load libshygpu.so (building it first when the sources are newer)."""
-    global _lib
+    global _lib, LIB_PATH
     if _lib is not None:
         return _lib
-    if os.environ.get("SHYGPU_NO_BUILD") != "1":
+    if os.environ.get("SHYGPU_LIB"):                # an alternative build of the same ABI
+        LIB_PATH = Path(os.environ["SHYGPU_LIB"])
+    elif os.environ.get("SHYGPU_NO_BUILD") != "1":
         try:
             from . import build as _build
             _build.build()
