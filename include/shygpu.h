@@ -239,6 +239,30 @@ int shygpu_simsys_get_matrix(int32_t *n, int32_t *nnz, int32_t *rowptr,
                              int32_t *col, double *val, double *rhs);
 int shygpu_simsys_iterations(void);
 
+/* Solve A x = rhs for one sparse system whose CSR arrays (0-based, rows with
+ * their diagonal stored), right-hand side, start x0 and result x are all in
+ * device memory, without allocating any device memory.  This entry point
+ * has no counterpart in the reference: it serves callers that cannot let a
+ * solver take device memory (a model embedded in a framework whose memory
+ * pool owns the GPU, a server that admits work by an exact memory budget, a
+ * time loop that must not stall other streams on cudaMalloc/cudaFree).  The
+ * solver is the one of system_solve_ (Jacobi-preconditioned CG when
+ * symmetric != 0, else BiCGStab, FP32 inside FP64 refinement, stop when
+ * ||r|| <= rtol*||r0|| + atol); its work vectors live in a fixed 5 MiB
+ * array inside the library.  At most 65536 rows and 524288 stored entries:
+ * larger systems return SHY_ECAPACITY.  The first call on a device, with
+ * that device current, looks the array up and must come before any stream
+ * capture begins.  There is one such array per device, so calls that
+ * overlap on one device race: serialise them.  x may equal x0.  The call
+ * waits for the solve on `stream` (a cudaStream_t, NULL = default stream);
+ * *iterations (optional) receives the Krylov iteration count.            */
+int shygpu_csr_solve_static(int32_t n, int32_t nnz, const int32_t *rowptr,
+                            const int32_t *col, const double *val,
+                            const double *rhs, const float *x0, float *x,
+                            double rtol, double atol, int32_t maxit,
+                            int32_t symmetric, void *stream,
+                            int32_t *iterations);
+
 void system_initialize_(void);                      /* :85   */
 void system_init_(void);                            /* :137  */
 void system_set_explicit_(void);                    /* :160  */

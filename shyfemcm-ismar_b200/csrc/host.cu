@@ -47,6 +47,13 @@ static int fail(int code, const char *fmt, ...) {
   } while (0)
 
 extern "C" const char *shygpu_last_error(void) { return g_err.c_str(); }
+
+// error and launch accounting for entry points defined in other files
+namespace shy {
+int external_fail(int code, const char *msg) { return fail(code, "%s", msg); }
+void external_count_launch() { g_launches += 1; }
+}  // namespace shy
+
 // launches counted on the host, plus those the device-driven sub-step loops
 // of live models made (read from each model's device counter)
 static std::vector<const void *> g_models;
