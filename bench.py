@@ -1,15 +1,21 @@
 #!/usr/bin/env python
 """bench.py -- node*layer*steps/s of SHYFEM's semi-implicit step on B200.
 
-Workload at N=1 (the 3D baroclinic basin): ~20k nodes / ~39.7k triangles on
-50 km x 30 km, 20 z-layers 1..5 m thick, Gaussian-bump bathymetry 5..60 m,
-temperature and salinity transported, baroclinic pressure, 10 m/s wind,
-M2 0.3 m level boundary, dt = 120 s.  Seeded synthetic input of that shape
-(no dataset ships with the reference).  One bench "step" is one model time
-step (shyfem_run's loop body: hydro + run_scalar) of that basin.
+Default workload at N=1 (the batched ensemble): 64 independent basins with
+node counts log-uniform in 5k..100k (2.1M nodes, 4.2M triangles in total),
+each a jittered triangle mesh with Gaussian-bump bathymetry 5..60 m and 10
+z-layers, uniform wind of 10 m/s plus a seeded per-basin perturbation of
+sigma 3 m/s, M2 0.5 m level boundary, dt = 60 s; seeded synthetic input of
+that shape (no dataset ships with the reference).  All basins advance in
+one CUDA-graph step.  One bench "step" is one model time step (hydro, the
+body of shyfem_run's loop) of every basin.  Beside it the line reports the
+plain single-run form: the same basins advanced one model at a time.
+
+`--workload basin3d` times the 3D baroclinic basin instead (~20k nodes, 20
+z-layers, temperature and salinity transported, dt = 120 s).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl shygpu|reference]
-                  [--workload basin3d|ensemble]
+                  [--workload ensemble|basin3d]
 
 N > 1 runs one process per GPU, each advancing its own replica (replicas
 only: the step has no exchange between basins), value = all ranks' units /
@@ -41,11 +47,12 @@ FALLBACK_HBM = 6650.0
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=1000)
-    p.add_argument("--warmup", type=int, default=20)
+    p.add_argument("--steps", type=int, default=400)
+    p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="shygpu", choices=["shygpu", "reference"])
-    p.add_argument("--workload", default="basin3d", choices=["basin3d", "ensemble"])
+    p.add_argument("--workload", default="ensemble", choices=["ensemble", "basin3d"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
     return p.parse_args()
 
 
@@ -66,9 +73,38 @@ def workload_config(workload, case_list, l2):
         return {"workload": "basin3d_baroclinic_ts", "nkn": c["nkn"], "nel": c["nel"],
                 "nlv": c["nlv"], "dt_s": c["params"]["dt"], "tracers": "T,S",
                 "forcing": "10 m/s wind, M2 0.3 m", "l2": l2}
-    return {"workload": "ensemble_64_basins", "basins": len(case_list),
-            "nkn_total": sum(c["nkn"] for c in case_list), "nlv": case_list[0]["nlv"],
-            "dt_s": case_list[0]["params"]["dt"], "l2": l2}
+    return {"workload": "ensemble_64_basins_5k_100k_nodes", "basins": len(case_list),
+            "nkn_total": sum(c["nkn"] for c in case_list),
+            "nel_total": sum(c["nel"] for c in case_list), "nlv": case_list[0]["nlv"],
+            "dt_s": case_list[0]["params"]["dt"], "forcing": "10 +- 3 m/s wind, M2 0.5 m",
+            "l2": l2}
+
+
+def plain_gpu(case_list, steps, lib):
+    """The plain single-run GPU form: each basin in a model of its own,
+    advanced alone (CUDA-graph step), one basin after the other; device
+    time summed over the basins."""
+    import torch
+    import shygpu
+    total_ms = 0.0
+    units = 0
+    for c in case_list:
+        m = shygpu.Model([c])
+        m.set_state_all()
+        m.run(3)
+        st = torch.cuda.ExternalStream(m.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        with torch.cuda.stream(st):
+            e0.record(st)
+            lib.shygpu_enqueue(m.h, steps)
+            e1.record(st)
+        torch.cuda.synchronize()
+        shygpu.check(lib.shygpu_sync(m.h), "plain step")
+        total_ms += e0.elapsed_time(e1)
+        units += c["nkn"] * c["nlv"] * steps
+        m.close()
+    return units / (total_ms / 1000.0), total_ms / steps
 
 
 # ---------------------------------------------------------------------------
@@ -135,12 +171,13 @@ def algorithmic_bytes(case_list, infos, nsc, cor=False):
     NK = sum(int(c["ilhkv"].sum()) for c in case_list)         # active node-layers
     NI = sum(c["nkn"] * (c["nlv"] + 1) for c in case_list)     # node interfaces
     nnz = 7 * nkn
-    iters = sum(i.krylov_iters for i in infos)
-    outer = sum(max(i.refinements, 1) for i in infos)
+    # Krylov traffic per basin: its own iterations over its own rows
+    kry = sum(i.krylov_iters * (8 * 7 * c["nkn"] + 48 * c["nkn"])
+              + max(i.refinements, 1) * (12 * 7 * c["nkn"] + 20 * c["nkn"])
+              for c, i in zip(case_list, infos))
     b = {}
     b["column"] = NL * (24 + (4 if cor else 0)) + nel * (12 + 32 + 16 + 8 + 48) + NK * 4 + NI * 4 + nkn * 12
-    b["zeta"] = (nel * (48 + 36 + 12) + nnz * (4 + 12 + 4) + nkn * (4 + 4 + 4 + 4 + 20)
-                 + iters * (8 * nnz + 48 * nkn) + outer * (12 * nnz + 20 * nkn))
+    b["zeta"] = nel * (48 + 36 + 12) + nnz * (4 + 12 + 4) + nkn * (4 + 4 + 4 + 4 + 20) + kry
     b["final"] = NL * (24 + (4 if cor else 0)) + nel * (12 + 32 + 16 + 16 + 4 + 8 + 12) + nkn * 4
     b["node"] = NL * 16 + nel * (12 + 32 + 16 + 4) + NK * 12 + nkn * 20 + NI * 4
     b["stab"] = NL * 24 + nel * (36 + 32 + 16 + 4 + 12) + NK * 8 + NI * 8
@@ -358,11 +395,19 @@ def main():
         "solver": {"krylov_iters_last_step": infos[0].krylov_iters,
                    "refinements": infos[0].refinements, "resid": infos[0].resid},
     }
+    if a.workload == "ensemble" and not a.no_plain:
+        psteps = min(a.steps, 40)
+        pv, pms = plain_gpu(case_list, psteps, lib)
+        line["plain_gpu"] = {"value": pv, "unit": METRIC, "ms_per_step": pms, "steps": psteps,
+                             "form": "one model per basin, basins advanced one after the other"}
+        line["batched_over_plain"] = value / pv
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         nproc = 1
         v, tmax, _ = cpu_baseline(a.workload, nproc, 20, warm=1)
+        what = ("the first 2 basins of an ensemble drawn by the same generator"
+                if a.workload == "ensemble" else "the same basin")
         line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": nproc, "kind": "port",
-                                "sample": "20 time steps of the same basin, FP64 C++ restatement "
+                                "sample": f"20 time steps of {what}, FP64 C++ restatement "
                                           "of the reference step (oracle/shyref.cpp), 1 thread"}
     if rank == 0:
         print(json.dumps(line), flush=True)

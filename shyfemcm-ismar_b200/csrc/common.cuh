@@ -83,6 +83,8 @@ struct Dev {
                               //  node of the next vertex, node of the one after}
   double *val64, *rhs64, *x64;
   float *val32, *dinv32, *r32, *p32, *q32, *z32, *e32, *s32, *t32, *rh32, *v32;
+  float4 *cg4[2];                 // device-wide CG: {r, w = A D^-1 r, s, 1/diag} per row, two generations
+  float2 *cg2;                    // device-wide CG: {p, e} per row
   // element system written by the column kernel (SoA): hia[c*NEL+e], hik[c*NEL+e]
   float *hia, *hik;
   // state, [0] = new, [1] = old (swapped per step)

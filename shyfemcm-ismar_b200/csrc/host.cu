@@ -305,9 +305,67 @@ static const size_t kSmemMax = 227 * 1024;
 static void free_zeta_plan(shygpu_model *m) {
   for (int *&p : m->zmap_ptrs) { if (p) cudaFree(p); p = nullptr; }
   m->zm = ZetaMaps();
-  for (ZetaClass &c : m->zcl)
+  for (ZetaClass &c : m->zcl) {
     if (c.d_blist) cudaFree(c.d_blist);
+    if (c.grid) {
+      cudaFree((void *)c.gp.seg); cudaFree((void *)c.gp.bseg); cudaFree((void *)c.gp.cseg);
+      cudaFree(c.gp.partial); cudaFree(c.gp.ctr);
+    }
+  }
   m->zcl.clear();
+}
+
+// The device-wide class: every basin in one cooperative launch.  The rows of
+// all basins (contiguous, basin after basin) are cut into G equal slices, one
+// per CTA, and each slice at the basin boundaries into segments.  Returns
+// SHY_EARG when a slice would hold more segments than one CTA reduces.
+template <typename T>
+static int upload_plan(T **dst, const std::vector<T> &h) {
+  CUDA_TRY(cudaMalloc((void **)dst, sizeof(T) * std::max<size_t>(h.size(), 1)));
+  if (!h.empty()) CUDA_TRY(cudaMemcpy(*dst, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+  return SHY_OK;
+}
+
+static int build_grid_class(shygpu_model *m) {
+  const long long N = m->NKN;
+  const int cap = zeta_grid_capacity();
+  if (cap < 1) return fail(SHY_ECUDA, "zeta grid solver: no resident CTA fits the device");
+  const int G = (int)std::max<long long>(1, std::min<long long>(cap, N / 64));
+  std::vector<int4> seg;
+  std::vector<int2> cseg(G), bseg(m->nbasin, make_int2(0, 0));
+  int b = 0;
+  for (int c = 0; c < G; c++) {
+    long long r0 = N * c / G;
+    const long long r1 = N * (c + 1) / G;
+    cseg[c].x = (int)seg.size();
+    while (r0 < r1) {
+      while (m->par[b].k0 + m->par[b].nk <= r0) b++;
+      const long long e = std::min<long long>(r1, m->par[b].k0 + m->par[b].nk);
+      seg.push_back(make_int4((int)r0, (int)e, b, r0 == m->par[b].k0 ? 1 : 0));
+      r0 = e;
+    }
+    cseg[c].y = (int)seg.size();
+    if (cseg[c].y - cseg[c].x > zeta_grid_max_segments())
+      return fail(SHY_EARG, "zeta grid solver: %d basins in one CTA's rows", cseg[c].y - cseg[c].x);
+  }
+  for (int s = (int)seg.size() - 1; s >= 0; s--) bseg[seg[s].z].x = s;
+  for (size_t s = 0; s < seg.size(); s++) bseg[seg[s].z].y = (int)s + 1;
+  m->zcl.emplace_back();
+  ZetaClass &c = m->zcl.back();
+  c.grid = true;
+  c.G = G;
+  c.threads = 0;
+  c.CL = 0;
+  for (int i = 0; i < m->nbasin; i++) c.basins.push_back(i);
+  c.gp.nseg = (int)seg.size();
+  int4 *dseg = nullptr; int2 *dbs = nullptr, *dcs = nullptr;
+  ST_TRY(upload_plan(&dseg, seg)); c.gp.seg = dseg;
+  ST_TRY(upload_plan(&dbs, bseg)); c.gp.bseg = dbs;
+  ST_TRY(upload_plan(&dcs, cseg)); c.gp.cseg = dcs;
+  CUDA_TRY(cudaMalloc(&c.gp.partial, sizeof(double) * 8 * std::max<size_t>(seg.size(), 1)));
+  CUDA_TRY(cudaMalloc(&c.gp.ctr, 8 * sizeof(unsigned)));
+  CUDA_TRY(cudaMemset(c.gp.ctr, 0, 8 * sizeof(unsigned)));
+  return SHY_OK;
 }
 
 // rows of CTA q of basin bp for cluster size CL
@@ -347,6 +405,33 @@ static int build_zeta_plan(shygpu_model *m, int forceCL, int forceThreads) {
 static int build_zeta_plan_impl(shygpu_model *m, int forceCL, int forceThreads) {
   free_zeta_plan(m);
   const int NKN = m->NKN;
+  // the device-wide solver when asked for, or when a basin of a symmetric
+  // system is too large for the shared-memory cluster solver
+  bool grid = m->sym && m->zvariant == 2 && forceCL <= 0;
+  if (m->sym && m->zvariant == 1 && forceCL <= 0)
+    for (int b = 0; b < m->nbasin && !grid; b++) {
+      const BasinPar &bp = m->par[b];
+      const int CL = std::min(16, next_pow2((bp.nk + 1249) / 1250));
+      ZetaShape zs;
+      for (int q = 0; q < CL; q++) {
+        int a, e;
+        cta_rows(bp, CL, q, a, e);
+        zs.chunk = std::max(zs.chunk, e - a);
+        zs.nnzcap = std::max(zs.nnzcap, m->rowptr_h[e] - m->rowptr_h[a]);
+        zs.halocap = std::max(zs.halocap, (int)halo_of(m, a, e).size());
+      }
+      if (sm_bytes(zs) > kSmemMax) grid = true;
+    }
+  if (grid) {
+    const int st = build_grid_class(m);
+    if (st == SHY_OK) {
+      m->zforce_CL = forceCL;
+      m->zforce_threads = forceThreads;
+      return SHY_OK;
+    }
+    if (st != SHY_EARG) return st;
+    free_zeta_plan(m);   // too many basins per CTA: fall back to cluster classes
+  }
   std::vector<int> loc(m->rowptr_h[NKN], 0);
   std::vector<std::vector<int>> pushl(NKN);
   for (int b = 0; b < m->nbasin; b++) {
@@ -458,8 +543,9 @@ static int launch_zeta_plan(shygpu_model *m, const Dev &d, ZetaArgs za) {
     cudaStream_t st = nc > 1 ? m->side[i] : m->stream;
     if (nc > 1) CUDA_TRY(cudaStreamWaitEvent(st, m->ev_fork, 0));
     za.blist = c.d_blist;
-    cudaError_t e = c.sm ? launch_zeta_sm(d, za, c.zs, m->zm, (int)c.basins.size(), st)
-                         : launch_zeta(d, za, c.CL, c.threads, (int)c.basins.size(), st);
+    cudaError_t e = c.grid ? launch_zeta_grid(d, za, c.gp, c.G, st)
+                  : c.sm   ? launch_zeta_sm(d, za, c.zs, m->zm, (int)c.basins.size(), st)
+                           : launch_zeta(d, za, c.CL, c.threads, (int)c.basins.size(), st);
     if (e != cudaSuccess) return fail(SHY_ECUDA, "zeta solve launch: %s", cudaGetErrorString(e));
     if (nc > 1) {
       CUDA_TRY(cudaEventRecord(m->ev_join[i], st));
@@ -491,7 +577,7 @@ static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P,
   }
   if (NLVo) *NLVo = (int)NLV;
   int64_t el = nel * (4 * 16 + 8 * 4 + 12 * 4 + 4 * 4 + NLV * 4 * (2 * 2 + 2 * 1 + 2 + 1 + 2 + 1)) ;
-  int64_t nd = nkn * (4 * 12 + 8 * 6 + NLV * 4 * (2 + 1 + 1) + (NLV + 1) * 4 * 3 + nsc * NLV * 4 * 3);
+  int64_t nd = nkn * (4 * 12 + 8 * 6 + 40 + NLV * 4 * (2 + 1 + 1) + (NLV + 1) * 4 * 3 + nsc * NLV * 4 * 3);
   int64_t sy = nnz * (4 + 8 + 4 + 4 * 3);
   return el + nd + sy;
 }
@@ -758,7 +844,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       A.alloc(&d.val32, nnz) || A.alloc(&d.dinv32, NKN) || A.alloc(&d.r32, NKN) ||
       A.alloc(&d.p32, NKN) || A.alloc(&d.q32, NKN) || A.alloc(&d.z32, NKN) ||
       A.alloc(&d.e32, NKN) || A.alloc(&d.s32, NKN) || A.alloc(&d.t32, NKN) ||
-      A.alloc(&d.rh32, NKN) || A.alloc(&d.v32, NKN) || A.alloc(&d.hia, (size_t)9 * NEL) ||
+      A.alloc(&d.rh32, NKN) || A.alloc(&d.v32, NKN) || A.alloc(&d.cg4[0], NKN) ||
+      A.alloc(&d.cg4[1], NKN) || A.alloc(&d.cg2, NKN) || A.alloc(&d.hia, (size_t)9 * NEL) ||
       A.alloc(&d.hik, (size_t)3 * NEL) || A.alloc(&d.unv, NEL) || A.alloc(&d.vnv, NEL) ||
       A.alloc(&d.usv, EL) || A.alloc(&d.vsv, EL) ||
       A.alloc(&d.wl, (size_t)NKN * (NLV + 1)) || A.alloc(&d.rho, NL) || A.alloc(&d.ddx, EL) ||
@@ -820,8 +907,11 @@ extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value
       return st;
     }
   }
-  else if (n == "zeta_variant") {   // 0: vectors in global memory, 1: shared memory when it fits
-    m->zvariant = iv != 0;
+  else if (n == "zeta_variant") {
+    // 0: vectors in global memory; 1: shared memory when every basin fits a
+    // cluster, else the device-wide solver; 2: the device-wide solver
+    if (iv < 0 || iv > 2) return fail(SHY_EARG, "zeta_variant: 0, 1 or 2");
+    m->zvariant = iv;
     ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
   }
   else if (n == "inner_rtol") { if (!(value > 0 && value < 1)) return fail(SHY_EARG, "inner_rtol in (0,1)"); m->inner_rtol = (float)value; }
@@ -846,7 +936,8 @@ extern "C" double shygpu_get_option(shygpu_model *m, const char *name) {
   if (n == "inner_rtol") return m->inner_rtol;
   if (n == "max_outer") return m->max_outer;
   if (n == "symmetric") return m->sym;
-  if (n == "zeta_variant") return m->zcl.empty() ? -1 : (m->zcl[0].sm ? 1 : 0);
+  if (n == "zeta_variant") return m->zcl.empty() ? -1 : (m->zcl[0].grid ? 2 : (m->zcl[0].sm ? 1 : 0));
+  if (n == "zeta_grid_ctas") return m->zcl.empty() ? -1 : m->zcl[0].G;
   if (n == "launches_per_step") return m->launches_per_step;
   return -1;
 }

@@ -1,0 +1,389 @@
+// k_zeta_grid.cuh -- zeta assembly + solve for basins larger than one
+// thread-block cluster can hold: one persistent cooperative launch over the
+// whole device for every basin of the model.
+//
+// Each CTA owns a contiguous slice of the model's rows (all basins' rows are
+// contiguous), cut at basin boundaries into segments; a basin's segments are
+// consecutive.  The solver is the one of k_zeta_sm (system_solve,
+// sparskit_admin.f90:115-334, with the reference's stop test
+// ||r|| <= rtol*||r0|| + atol, spk_iters.f90:3304-3360): FP64 residual
+// refinement around Jacobi-preconditioned Chronopoulos-Gear CG in FP32, the
+// extrapolated start 2 z^n - z^(n-1).  Every basin runs its own state
+// machine; all basins advance in lock step through "super-steps" separated
+// by one grid barrier.  One CG iteration is one super-step: a row needs its
+// neighbours' new preconditioned residual u_j = D_j^-1 (r_j - a (w_j + b s_j))
+// for the product A u, and computes it from their values of the previous
+// iteration (kept in a second generation of the vectors) with the iteration
+// scalars a, b that every row of the basin shares, so no barrier separates
+// the vector update from the matrix-vector product.  In a super-step each segment does the work of its
+// basin's stage and writes its partial sums; after the barrier every CTA
+// that holds a segment of the basin sums that basin's partials in segment
+// order (the same bits in every CTA) and takes the same stage decision.
+// A basin that has finished idles until every basin has.
+//
+// The grid barrier is an arrival counter with a bounded wait: a CTA that
+// waits longer than kGridSpinLimit polls marks every basin of the launch
+// with SHY_ECUDA and leaves, and so do the others when they see the abort
+// flag.  The launch is cooperative, so all CTAs are resident together.
+// Vectors written by other CTAs are read with ordinary (L1-cached) loads:
+// no CTA reads, in a super-step, what another writes in the same one, and
+// the barrier's acquire makes the previous super-step's writes visible.
+// Included by step.cu.
+#pragma once
+#include "k_zeta.cuh"
+
+namespace shy {
+
+constexpr int kGridThreads = 512;
+constexpr int kGridMaxSeg = kGridThreads / 32;   // segments per CTA (one warp reduces each)
+constexpr long long kGridSpinLimit = 1LL << 24;  // ~ seconds with the back-off below
+constexpr int kGridPartialUnroll = 8;           // partial sums a lane loads at once
+
+enum GridStage : int { G_RES = 0, G_XTRP, G_SPMV0, G_ITER, G_FIX, G_FINISH, G_DONE };
+
+// per-basin solver state, one copy in each CTA holding a segment of it
+struct GridState {
+  int stage, first, conv, outer, inner, iters, basin, owner, cur;
+  double tol, itol2, rn, resid0, alpha, beta, gamma;
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// bar-th grid barrier (bar = 1, 2, ...).  Arrivals count up in ctr[0] with
+// a release reduction; the CTA that completes a barrier publishes its number
+// in ctr[5] (release), which the others poll with acquire loads (read-only
+// polling keeps the counter's atomics uncontended).  The CTA barriers on
+// both sides extend the release and the acquire to every thread of the CTA.
+// Returns false on timeout/abort (ctr[4]).  *act (when not null) receives
+// ctr[act_idx] read after the barrier, once for the CTA.
+__device__ __forceinline__ bool grid_barrier(unsigned *ctr, unsigned bar, int *s_ok, unsigned act_idx,
+                                             unsigned *s_act) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    unsigned old;
+    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(ctr) : "memory");
+    if (old + 1u == bar * gridDim.x) {
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctr + 5), "r"(bar) : "memory");
+    } else {
+      long long spins = 0;
+      while (ld_acquire_u32(ctr + 5) < bar) {
+        if (ld_acquire_u32(ctr + 4) != 0u || ++spins > kGridSpinLimit) {
+          atomicExch(ctr + 4, 1u);
+          ok = 0;
+          break;
+        }
+        if (spins > 256) __nanosleep(32);
+      }
+    }
+    if (s_act) *s_act = ld_acquire_u32(ctr + act_idx);
+    *s_ok = ok;
+  }
+  __syncthreads();
+  return *s_ok != 0;
+}
+
+// the new preconditioned residual of a row from its values of the previous
+// iteration q = {r, w, s, 1/diag}: s' = w + b s, r' = r - a s', u' = r'/diag.
+// Rows and their neighbours evaluate the same expression, so the same bits.
+__device__ __forceinline__ float cg_unext(const float4 q, float fa, float fb, float &s_new, float &r_new) {
+  s_new = q.y + fb * q.z;
+  r_new = q.x - fa * s_new;
+  return q.w * r_new;
+}
+
+// one row of A u' in FP32, u' of every entry's row from the previous
+// generation (fa = fb = 0 and r only: u = r/diag); the row's entries are
+// fetched eight at a time, all loads issued before the products
+// (memory-level parallelism for the short rows of a triangle mesh); the sum
+// runs in slot order
+__device__ __forceinline__ float grid_spmv_row(const Dev &d, int i, const float4 *qg, float fa, float fb) {
+  const int s0 = d.rowptr[i], s1 = d.rowptr[i + 1];
+  float w = 0.f;
+  for (int s = s0; s < s1; s += 8) {
+    int c[8];
+    float v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const bool ok = s + k < s1;
+      c[k] = ok ? d.col[s + k] : i;
+      v[k] = ok ? d.val32[s + k] : 0.f;
+    }
+    float4 x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = qg[c[k]];
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+      if (s + k < s1) {
+        float sn, rn;
+        w += v[k] * cg_unext(x[k], fa, fb, sn, rn);
+      }
+  }
+  return w;
+}
+
+// FP64 residual of one row: rhs - A*x
+__device__ __forceinline__ double grid_resid_row(const Dev &d, int i) {
+  const int s0 = d.rowptr[i], s1 = d.rowptr[i + 1];
+  double t = d.rhs64[i];
+  for (int s = s0; s < s1; s += 8) {
+    int c[8];
+    double v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const bool ok = s + k < s1;
+      c[k] = ok ? d.col[s + k] : i;
+      v[k] = ok ? d.val64[s + k] : 0.;
+    }
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) x[k] = d.x64[c[k]];
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+      if (s + k < s1) t -= v[k] * x[k];
+  }
+  return t;
+}
+
+// block-wide sum of NV doubles; the totals land in thread 0
+template <int NV>
+__device__ __forceinline__ void block_sum0(double (&v)[NV], double *red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; k++) {
+    double x = v[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    if (lane == 0) red[k * 32 + warp] = x;
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+      double x = lane < nw ? red[k * 32 + lane] : 0.;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      v[k] = x;
+    }
+  }
+  __syncthreads();   // red may be reused right after
+}
+
+__global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs za, GridPlan gp) {
+  __shared__ GridState gs[kGridMaxSeg];
+  __shared__ double red[3 * 32];
+  __shared__ int s_ok;
+  __shared__ unsigned s_act;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int2 cs = gp.cseg[blockIdx.x];
+  const int nseg = cs.y - cs.x;
+  unsigned bar = 0;
+
+  if (tid < nseg) {
+    const int4 sg = gp.seg[cs.x + tid];
+    GridState &g = gs[tid];
+    g.stage = G_RES; g.first = 1; g.conv = 0; g.outer = 0; g.inner = 0; g.iters = 0; g.cur = 0;
+    g.basin = sg.z; g.owner = sg.w;
+    g.tol = g.itol2 = g.rn = g.resid0 = g.alpha = g.beta = g.gamma = 0.;
+  }
+  if (blockIdx.x == 0 && tid == 0 && d.imax) { *d.imax = 0; *d.subj = 0; }
+
+  // ---- assembly (FP64 gather in element order), Jacobi diagonal, start ----
+  for (int q = 0; q < nseg; q++) {
+    const int4 sg = gp.seg[cs.x + q];
+    const BasinPar &P = d.par[sg.z];
+    if (sg.w && tid < kMaxScal) d.out[sg.z].stab[tid] = 0.f;   // reset for k_stab's max
+    const float dtf = (float)P.dt;
+    for (int i = sg.x + tid; i < sg.y; i += nth) {
+      double diag, rhs;
+      assemble_row(d, za, i, dtf, diag, rhs);
+      d.dinv32[i] = diag != 0. ? (float)(1. / diag) : 1.f;
+      const double x0 = za.explicit_mode ? (diag != 0. ? rhs / diag : 0.) : (double)za.zguess[i];
+      d.x64[i] = x0;
+      if (za.explicit_mode) d.zn[i] = (float)x0;
+    }
+  }
+  if (za.explicit_mode) {   // system_set_explicit: no coupling between rows, no barrier
+    __syncthreads();
+    if (tid < nseg && gs[tid].owner) {
+      BasinOut &O = d.out[gs[tid].basin];
+      O.iters = 0; O.refinements = 0; O.resid0 = 0.; O.resid = 0.;
+    }
+    return;
+  }
+  if (!grid_barrier(gp.ctr, ++bar, &s_ok, 0, nullptr)) goto aborted;
+
+  for (unsigned k = 0;; k++) {
+    const int par = (int)(k & 1u);
+    // ---- the work of each segment's stage ----
+    for (int q = 0; q < nseg; q++) {
+      const int4 sg = gp.seg[cs.x + q];
+      const int a = sg.x, e = sg.y;
+      const int stage = gs[q].stage;
+      double v[3] = {0., 0., 0.};
+      if (stage == G_RES) {
+        float4 *qo = d.cg4[gs[q].cur];
+        for (int i = a + tid; i < e; i += nth) {
+          const double t = grid_resid_row(d, i);
+          qo[i] = make_float4((float)t, 0.f, 0.f, d.dinv32[i]);
+          d.cg2[i] = make_float2(0.f, 0.f);
+          v[0] += t * t;
+        }
+      } else if (stage == G_XTRP) {
+        // z_guess = 2 z^n - z^{n-1}: smooth in time, a smaller starting residual
+        for (int i = a + tid; i < e; i += nth) d.x64[i] = 2. * (double)za.zguess[i] - (double)za.zprev[i];
+      } else if (stage == G_SPMV0) {
+        // w = A u with u = r/diag (fa = 0 and s = 0 leave r, so u = r/diag)
+        const float4 *qi = d.cg4[gs[q].cur];
+        float4 *qo = d.cg4[gs[q].cur ^ 1];
+        for (int i = a + tid; i < e; i += nth) {
+          const float w = grid_spmv_row(d, i, qi, 0.f, 0.f);
+          const float4 me = qi[i];
+          const float u = me.w * me.x;
+          qo[i] = make_float4(me.x, w, 0.f, me.w);
+          v[0] += (double)me.x * u;
+          v[1] += (double)w * u;
+          v[2] += (double)me.x * me.x;
+        }
+      } else if (stage == G_ITER) {
+        // p = u + b p, s = w + b s, e += a p, r -= a s, u = r/diag, w = A u
+        const float fa = (float)gs[q].alpha, fb = (float)gs[q].beta;
+        const float4 *qi = d.cg4[gs[q].cur];
+        float4 *qo = d.cg4[gs[q].cur ^ 1];
+        for (int i = a + tid; i < e; i += nth) {
+          const float4 me = qi[i];
+          const float2 pe = d.cg2[i];
+          const float p = me.w * me.x + fb * pe.x;
+          float sn, rn;
+          const float u = cg_unext(me, fa, fb, sn, rn);
+          const float w = grid_spmv_row(d, i, qi, fa, fb);
+          qo[i] = make_float4(rn, w, sn, me.w);
+          d.cg2[i] = make_float2(p, pe.y + fa * p);
+          v[0] += (double)rn * u;
+          v[1] += (double)w * u;
+          v[2] += (double)rn * rn;
+        }
+      } else if (stage == G_FIX) {
+        for (int i = a + tid; i < e; i += nth) d.x64[i] += (double)d.cg2[i].y;
+      } else if (stage == G_FINISH) {
+        for (int i = a + tid; i < e; i += nth) d.zn[i] = (float)d.x64[i];
+      }
+      if (stage == G_RES || stage == G_SPMV0 || stage == G_ITER) {
+        block_sum0<3>(v, red);
+        if (tid == 0) {
+          double *pp = gp.partial + ((size_t)par * gp.nseg + (cs.x + q)) * 4;
+          __stcg(pp + 0, v[0]); __stcg(pp + 1, v[1]); __stcg(pp + 2, v[2]);
+        }
+      }
+    }
+    __syncthreads();
+    // ---- finished basins leave the machine; count the active ones ----
+    if (tid == 0) {
+      unsigned nact = 0;
+      for (int q = 0; q < nseg; q++) {
+        GridState &g = gs[q];
+        if (g.stage == G_FINISH) {
+          if (g.owner) {
+            BasinOut &O = d.out[g.basin];
+            O.iters = g.iters;
+            O.refinements = g.outer;
+            O.resid0 = g.resid0;
+            O.resid = g.rn;
+            if (!g.conv) set_status(&O, SHY_ENOCONV);
+          }
+          g.stage = G_DONE;
+        }
+        if (g.owner && g.stage != G_DONE) nact++;
+      }
+      if (nact) atomicAdd(gp.ctr + 1 + k % 3, nact);
+      if (blockIdx.x == 0) gp.ctr[1 + (k + 1) % 3] = 0u;   // the counter of super-step k+3
+    }
+    if (!grid_barrier(gp.ctr, ++bar, &s_ok, 1 + k % 3, &s_act)) goto aborted;
+    if (s_act == 0u) break;
+    // ---- per-basin sums over its segments, the same in every CTA; next stage ----
+    {
+      const int warp = tid >> 5, lane = tid & 31;
+      if (warp < nseg) {
+        GridState &g = gs[warp];
+        const int st = g.stage;
+        if (st == G_RES || st == G_SPMV0 || st == G_ITER) {
+          const int2 bs = gp.bseg[g.basin];
+          double tot[3] = {0., 0., 0.};
+          // up to 32*kGridPartialUnroll partials per round, all loads issued first
+          for (int s0 = bs.x; s0 < bs.y; s0 += 32 * kGridPartialUnroll) {
+            double pv[kGridPartialUnroll][3];
+#pragma unroll
+            for (int u = 0; u < kGridPartialUnroll; u++) {
+              const int s = s0 + u * 32 + lane;
+              const double *pp = gp.partial + ((size_t)par * gp.nseg + (s < bs.y ? s : bs.x)) * 4;
+              pv[u][0] = __ldcg(pp + 0); pv[u][1] = __ldcg(pp + 1); pv[u][2] = __ldcg(pp + 2);
+            }
+#pragma unroll
+            for (int u = 0; u < kGridPartialUnroll; u++)
+              if (s0 + u * 32 + lane < bs.y) { tot[0] += pv[u][0]; tot[1] += pv[u][1]; tot[2] += pv[u][2]; }
+          }
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) tot[c] += __shfl_xor_sync(0xffffffffu, tot[c], o);
+          if (lane == 0) {
+            const BasinPar &P = d.par[g.basin];
+            if (st == G_RES) {
+              const double rn = sqrt(tot[0]);
+              bool next = true;
+              if (g.first) {
+                g.first = 0;
+                g.tol = (double)P.rtol * rn + (double)P.atol;
+                g.resid0 = rn;
+                if (za.zprev != nullptr && d.out[g.basin].steps > 0 && rn > g.tol) { g.stage = G_XTRP; next = false; }
+              }
+              if (next) {
+                g.rn = rn;
+                if (rn <= g.tol) { g.conv = 1; g.stage = G_FINISH; }
+                else if (g.outer >= za.max_outer) g.stage = G_FINISH;
+                else {
+                  const double it = fmax((double)za.inner_rtol * rn, 0.25 * g.tol);
+                  g.itol2 = it * it;
+                  g.stage = G_SPMV0;
+                }
+              }
+            } else if (st == G_SPMV0) {
+              g.cur ^= 1;
+              g.gamma = tot[0];
+              g.alpha = g.gamma / tot[1];
+              g.beta = 0.;
+              g.inner = 0;
+              g.stage = G_ITER;
+            } else {   // G_ITER
+              g.cur ^= 1;
+              g.iters++;
+              g.inner++;
+              const bool stop = !(tot[2] > g.itol2) || !(tot[0] == tot[0]) || g.inner >= P.maxit;
+              if (stop) g.stage = G_FIX;
+              else {
+                const double beta = tot[0] / g.gamma;
+                g.alpha = tot[0] / (tot[1] - beta * tot[0] / g.alpha);
+                g.beta = beta;
+                g.gamma = tot[0];
+              }
+            }
+          }
+        } else if (lane == 0) {
+          if (st == G_XTRP) g.stage = G_RES;
+          else if (st == G_FIX) { g.outer++; g.stage = G_RES; }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  return;
+
+aborted:
+  if (tid < nseg && gs[tid].owner) set_status(&d.out[gs[tid].basin], SHY_ECUDA);
+}
+
+}  // namespace shy

@@ -1,4 +1,4 @@
-// launch.h -- host-side launch interface of the kernels in kernels.cu.
+// launch.h -- host-side launch interface of the kernels in step.cu.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -44,8 +44,22 @@ struct ZetaMaps {
   const int *loc = nullptr, *push_ptr = nullptr, *push = nullptr;
 };
 
+// the device-wide zeta solver (k_zeta_grid): CTA c owns the row segments
+// cseg[c].x .. cseg[c].y-1; segment s = {row0, row1, basin, first segment of
+// its basin}; basin b's segments are bseg[b].x .. bseg[b].y-1
+struct GridPlan {
+  int nseg = 0;
+  const int4 *seg = nullptr;
+  const int2 *bseg = nullptr, *cseg = nullptr;
+  double *partial = nullptr;       // [2][nseg][4] partial sums of the segments
+  unsigned *ctr = nullptr;         // [8]: barrier arrivals, 3 active counts, abort flag
+};
+
 // a group of basins solved by one launch with one cluster shape
 struct ZetaClass {
+  bool grid = false;               // device-wide cooperative variant (all basins, one launch)
+  int G = 0;                       // its CTAs
+  GridPlan gp;
   bool sm = false;                 // shared-memory variant (else global memory)
   int CL = 1, threads = 512;
   ZetaShape zs;                    // capacities of the shared-memory variant
@@ -57,6 +71,11 @@ struct ZetaClass {
 cudaError_t launch_zeta(const Dev &d, const ZetaArgs &za, int CL, int threads, int nb, cudaStream_t st);
 cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs, const ZetaMaps &zm,
                            int nb, cudaStream_t st);
+// the device-wide variant: G CTAs of kGridThreads, cooperative; clears gp.ctr first
+cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &gp, int G, cudaStream_t st);
+// CTAs of k_zeta_grid that fit the device at once (0 on error)
+int zeta_grid_capacity();
+int zeta_grid_max_segments();
 // smem > 0 prepares the shared-memory variant for that many dynamic bytes
 cudaError_t zeta_kernel_setup(int CL, size_t smem);
 int zeta_max_active_clusters(int CL, int threads, size_t smem);

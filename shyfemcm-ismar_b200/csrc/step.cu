@@ -9,7 +9,9 @@
 //             sparskit_admin.f90:115-334): one thread-block cluster per basin;
 //             atomic-free gather assembly into CSR in element order (FP64), then
 //             FP32 preconditioned Krylov iterations inside FP64 residual
-//             refinement, all in one persistent launch.
+//             refinement, all in one persistent launch.  k_zeta_grid does the
+//             same for basins too large for a cluster: one cooperative launch
+//             over the whole device.
 //   k_final   hydro_transports_final + setzev + element part of setdepth
 //             (hydrodynamic.f90:1468-1578, wetdry.f90:594, elems_dealing.f90:1063-1097).
 //   k_node    nodal part of setdepth + hydro_vertical + per-node volume
@@ -33,6 +35,7 @@
 #include "k_conz.cuh"
 #include "k_zeta.cuh"
 #include "k_zeta_global.cuh"
+#include "k_zeta_grid.cuh"
 
 // ---------------------------------------------------------------------------
 // launch wrappers (host side)
@@ -140,6 +143,31 @@ cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs
   cudaLaunchConfig_t cfg = zeta_config(zs.CL, zs.threads, nb, zs.smem, st, attr);
   return cudaLaunchKernelEx(&cfg, k_zeta_sm, d, za, zs, zm);
 }
+
+cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &gp, int G, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(gp.ctr, 0, 8 * sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute attr[1];
+  cfg.gridDim = dim3(G, 1, 1);
+  cfg.blockDim = dim3(kGridThreads, 1, 1);
+  cfg.stream = st;
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_zeta_grid, d, za, gp);
+}
+
+int zeta_grid_capacity() {
+  int dev = 0, nsm = 0, nb = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_zeta_grid, kGridThreads, 0) != cudaSuccess) return 0;
+  return nb * nsm;
+}
+
+int zeta_grid_max_segments() { return kGridMaxSeg; }
 
 cudaError_t zeta_kernel_setup(int CL, size_t smem) {
   cudaError_t e = cudaSuccess;

@@ -139,3 +139,37 @@ def test_transport_substeps():
         for f in ("tempv", "saltv"):
             rel = np.abs(sg[f] - so[f])[m].max() / np.abs(so[f][m]).max()
             assert rel <= TRACER_RTOL, (use_graph, f, rel)
+
+
+def test_device_wide_zeta_solver(small3d):
+    """The cooperative device-wide zeta solver (the one large basins use)
+    against the oracle on the config-2-shaped test basin."""
+    g, o = run_both(small3d, 120, zeta_variant=2)
+    assert g.get_option("zeta_variant") == 2
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    m = active_mask(small3d)
+    for f in ("tempv", "saltv"):
+        rel = np.abs(sg[f] - so[f])[m].max() / np.abs(so[f][m]).max()
+        assert rel <= TRACER_RTOL, (f, rel)
+    assert g.info(0).krylov_iters > 0
+
+
+def test_large_basin_in_a_mix():
+    """A basin too large for one cluster sends the whole batch to the
+    device-wide solver; every member's result matches its run alone to the
+    solver's tolerance."""
+    cs = [cases.basin3d_case(nkn_target=n, nlv=4, seed=s, baroclinic=False, ts=False)
+          for n, s in ((50000, 21), (700, 22), (3000, 23))]
+    gb = shygpu.Model(cs)
+    assert gb.get_option("zeta_variant") == 2
+    gb.set_state_all()
+    gb.run(20)
+    for i, c in enumerate(cs):
+        ga = shygpu.Model(c)
+        ga.set_state(0)
+        ga.run(20)
+        a, b = ga.get_state(0), gb.get_state(i)
+        assert np.abs(a["znv"] - b["znv"]).max() <= 1e-5, i
+        umax = np.abs(a["utlnv"]).max()
+        assert np.abs(a["utlnv"] - b["utlnv"]).max() <= 1e-4 * umax, i
