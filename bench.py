@@ -56,11 +56,11 @@ def parse():
     return p.parse_args()
 
 
-def make_cases(workload, rank=0):
+def make_cases(workload, rank=0, first=None):
     from shygpu import cases
     if workload == "basin3d":
         return [cases.basin3d_case(nkn_target=20000, seed=2 + 1000 * rank)]
-    return cases.ensemble_cases(64, seed=4 + 1000 * rank)
+    return cases.ensemble_cases(64, seed=4 + 1000 * rank, first=first)
 
 
 def units_per_step(case_list):
@@ -183,6 +183,7 @@ def algorithmic_bytes(case_list, infos, nsc, cor=False):
     b["stab"] = NL * 24 + nel * (36 + 32 + 16 + 4 + 12) + NK * 8 + NI * 8
     b["reduce"] = nkn * 8
     b["conz"] = NL * 28 + nel * (32 + 16 + 4 + 12) + NK * (8 * nsc + 8 + 8) + NI * 8
+    b["rho"] = NK * (8 + 4 + 4)     # T, S read, layer depth read, rho written
     return b
 
 
@@ -202,9 +203,7 @@ def _oracle_worker(args):
     sys.path.insert(0, str(ROOT / "oracle"))
     sys.path.insert(0, str(ROOT / "shyfemcm-ismar_b200"))
     import shyref
-    cl = make_cases(workload, seed_rank)
-    if workload == "ensemble":
-        cl = cl[:2]
+    cl = make_cases(workload, seed_rank, first=2)
     ms = [shyref.OracleModel(c) for c in cl]
     for m in ms:
         m.run(warm)
@@ -235,9 +234,7 @@ def run_reference(a):
     # each bench step: one time step of each of nproc independent replicas
     steps = max(1, a.steps if a.steps <= 40 else 20)
     value, tmax, wall = cpu_baseline(a.workload, nproc, steps, warm=min(a.warmup, 2))
-    cl = make_cases(a.workload)
-    if a.workload == "ensemble":
-        cl = cl[:2]
+    cl = make_cases(a.workload, first=2)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
             "n_gpus": a.gpus, "steps": steps, "warmup": min(a.warmup, 2),
             "ms_per_step": 1000.0 * tmax / steps, "higher_is_better": True, "scaling": "weak",

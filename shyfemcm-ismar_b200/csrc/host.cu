@@ -308,17 +308,20 @@ static void free_zeta_plan(shygpu_model *m) {
   for (ZetaClass &c : m->zcl) {
     if (c.d_blist) cudaFree(c.d_blist);
     if (c.grid) {
-      cudaFree((void *)c.gp.seg); cudaFree((void *)c.gp.bseg); cudaFree((void *)c.gp.cseg);
+      cudaFree((void *)c.gp.tile); cudaFree((void *)c.gp.btile); cudaFree((void *)c.gp.cslot);
+      cudaFree((void *)c.gp.cnslot); cudaFree((void *)c.gp.cowner);
       cudaFree(c.gp.partial); cudaFree(c.gp.ctr);
     }
   }
   m->zcl.clear();
 }
 
-// The device-wide class: every basin in one cooperative launch.  The rows of
-// all basins (contiguous, basin after basin) are cut into G equal slices, one
-// per CTA, and each slice at the basin boundaries into segments.  Returns
-// SHY_EARG when a slice would hold more segments than one CTA reduces.
+// The device-wide class: every basin in one cooperative launch.  Each
+// basin's rows are cut into tiles of kGridTileRows (the tile boundaries, and
+// so the reduction order, depend on the basin alone); tile t goes to CTA
+// t % G, so a basin's tiles sit on consecutive CTAs and the work left when
+// only a few basins still iterate spreads over many CTAs.  Returns SHY_EARG
+// when a CTA would hold more tiles or basins than it can.
 template <typename T>
 static int upload_plan(T **dst, const std::vector<T> &h) {
   CUDA_TRY(cudaMalloc((void **)dst, sizeof(T) * std::max<size_t>(h.size(), 1)));
@@ -326,30 +329,39 @@ static int upload_plan(T **dst, const std::vector<T> &h) {
   return SHY_OK;
 }
 
+static const int kGridTileRows = 1024;
+
 static int build_grid_class(shygpu_model *m) {
-  const long long N = m->NKN;
   const int cap = zeta_grid_capacity();
   if (cap < 1) return fail(SHY_ECUDA, "zeta grid solver: no resident CTA fits the device");
-  const int G = (int)std::max<long long>(1, std::min<long long>(cap, N / 64));
-  std::vector<int4> seg;
-  std::vector<int2> cseg(G), bseg(m->nbasin, make_int2(0, 0));
-  int b = 0;
-  for (int c = 0; c < G; c++) {
-    long long r0 = N * c / G;
-    const long long r1 = N * (c + 1) / G;
-    cseg[c].x = (int)seg.size();
-    while (r0 < r1) {
-      while (m->par[b].k0 + m->par[b].nk <= r0) b++;
-      const long long e = std::min<long long>(r1, m->par[b].k0 + m->par[b].nk);
-      seg.push_back(make_int4((int)r0, (int)e, b, r0 == m->par[b].k0 ? 1 : 0));
-      r0 = e;
-    }
-    cseg[c].y = (int)seg.size();
-    if (cseg[c].y - cseg[c].x > zeta_grid_max_segments())
-      return fail(SHY_EARG, "zeta grid solver: %d basins in one CTA's rows", cseg[c].y - cseg[c].x);
+  const int MS = zeta_grid_max_slots();
+  std::vector<int4> tile;
+  std::vector<int2> btile(m->nbasin, make_int2(0, 0));
+  for (int b = 0; b < m->nbasin; b++) {
+    const BasinPar &bp = m->par[b];
+    btile[b].x = (int)tile.size();
+    for (int r = 0; r < bp.nk; r += kGridTileRows)
+      tile.push_back(make_int4(bp.k0 + r, bp.k0 + std::min(bp.nk, r + kGridTileRows), b, 0));
+    btile[b].y = (int)tile.size();
   }
-  for (int s = (int)seg.size() - 1; s >= 0; s--) bseg[seg[s].z].x = s;
-  for (size_t s = 0; s < seg.size(); s++) bseg[seg[s].z].y = (int)s + 1;
+  const int T = (int)tile.size();
+  const int G = std::max(1, std::min(cap, T));
+  if ((T + G - 1) / G > zeta_grid_max_tiles())
+    return fail(SHY_EARG, "zeta grid solver: %d tiles for %d CTAs", T, G);
+  std::vector<int> cslot((size_t)G * MS, -1), cnslot(G, 0), cowner(G, 0);
+  for (int t = 0; t < T; t++) {
+    const int c = t % G, b = tile[t].z;
+    int sl = -1;
+    for (int k = 0; k < cnslot[c]; k++)
+      if (cslot[(size_t)c * MS + k] == b) sl = k;
+    if (sl < 0) {
+      if (cnslot[c] >= MS) return fail(SHY_EARG, "zeta grid solver: more than %d basins in one CTA", MS);
+      sl = cnslot[c]++;
+      cslot[(size_t)c * MS + sl] = b;
+    }
+    tile[t].w = sl;
+    if (t == btile[b].x) cowner[c] |= 1 << sl;
+  }
   m->zcl.emplace_back();
   ZetaClass &c = m->zcl.back();
   c.grid = true;
@@ -357,12 +369,14 @@ static int build_grid_class(shygpu_model *m) {
   c.threads = 0;
   c.CL = 0;
   for (int i = 0; i < m->nbasin; i++) c.basins.push_back(i);
-  c.gp.nseg = (int)seg.size();
-  int4 *dseg = nullptr; int2 *dbs = nullptr, *dcs = nullptr;
-  ST_TRY(upload_plan(&dseg, seg)); c.gp.seg = dseg;
-  ST_TRY(upload_plan(&dbs, bseg)); c.gp.bseg = dbs;
-  ST_TRY(upload_plan(&dcs, cseg)); c.gp.cseg = dcs;
-  CUDA_TRY(cudaMalloc(&c.gp.partial, sizeof(double) * 8 * std::max<size_t>(seg.size(), 1)));
+  c.gp.ntile = T;
+  int4 *dt = nullptr; int2 *dbt = nullptr; int *dcs = nullptr, *dcn = nullptr, *dco = nullptr;
+  ST_TRY(upload_plan(&dt, tile)); c.gp.tile = dt;
+  ST_TRY(upload_plan(&dbt, btile)); c.gp.btile = dbt;
+  ST_TRY(upload_plan(&dcs, cslot)); c.gp.cslot = dcs;
+  ST_TRY(upload_plan(&dcn, cnslot)); c.gp.cnslot = dcn;
+  ST_TRY(upload_plan(&dco, cowner)); c.gp.cowner = dco;
+  CUDA_TRY(cudaMalloc(&c.gp.partial, sizeof(double) * 8 * std::max<size_t>(tile.size(), 1)));
   CUDA_TRY(cudaMalloc(&c.gp.ctr, 8 * sizeof(unsigned)));
   CUDA_TRY(cudaMemset(c.gp.ctr, 0, 8 * sizeof(unsigned)));
   return SHY_OK;

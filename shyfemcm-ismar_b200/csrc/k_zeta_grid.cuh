@@ -35,7 +35,8 @@
 namespace shy {
 
 constexpr int kGridThreads = 512;
-constexpr int kGridMaxSeg = kGridThreads / 32;   // segments per CTA (one warp reduces each)
+constexpr int kGridMaxSlots = kGridThreads / 32; // basins per CTA (one warp reduces each)
+constexpr int kGridMaxTiles = 32;                // tiles per CTA
 constexpr long long kGridSpinLimit = 1LL << 24;  // ~ seconds with the back-off below
 constexpr int kGridPartialUnroll = 8;           // partial sums a lane loads at once
 
@@ -149,56 +150,83 @@ __device__ __forceinline__ double grid_resid_row(const Dev &d, int i) {
   return t;
 }
 
-// block-wide sum of NV doubles; the totals land in thread 0
-template <int NV>
-__device__ __forceinline__ void block_sum0(double (&v)[NV], double *red) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int k = 0; k < NV; k++) {
-    double x = v[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    if (lane == 0) red[k * 32 + warp] = x;
-  }
-  __syncthreads();
-  if (warp == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; k++) {
-      double x = lane < nw ? red[k * 32 + lane] : 0.;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-      v[k] = x;
+// the stage decision of one basin after the sums tot of its partials (the
+// same inputs, so the same decision, in every CTA holding a tile of it)
+__device__ __forceinline__ void grid_transition(GridState &g, const double (&tot)[3], const Dev &d,
+                                                const ZetaArgs &za) {
+  const int st = g.stage;
+  const BasinPar &P = d.par[g.basin];
+  if (st == G_RES) {
+    const double rn = sqrt(tot[0]);
+    bool next = true;
+    if (g.first) {
+      g.first = 0;
+      g.tol = (double)P.rtol * rn + (double)P.atol;
+      g.resid0 = rn;
+      if (za.zprev != nullptr && d.out[g.basin].steps > 0 && rn > g.tol) { g.stage = G_XTRP; next = false; }
+    }
+    if (next) {
+      g.rn = rn;
+      if (rn <= g.tol) { g.conv = 1; g.stage = G_FINISH; }
+      else if (g.outer >= za.max_outer) g.stage = G_FINISH;
+      else {
+        const double it = fmax((double)za.inner_rtol * rn, 0.25 * g.tol);
+        g.itol2 = it * it;
+        g.stage = G_SPMV0;
+      }
+    }
+  } else if (st == G_SPMV0) {
+    g.cur ^= 1;
+    g.gamma = tot[0];
+    g.alpha = g.gamma / tot[1];
+    g.beta = 0.;
+    g.inner = 0;
+    g.stage = G_ITER;
+  } else {   // G_ITER
+    g.cur ^= 1;
+    g.iters++;
+    g.inner++;
+    const bool stop = !(tot[2] > g.itol2) || !(tot[0] == tot[0]) || g.inner >= P.maxit;
+    if (stop) g.stage = G_FIX;
+    else {
+      const double beta = tot[0] / g.gamma;
+      g.alpha = tot[0] / (tot[1] - beta * tot[0] / g.alpha);
+      g.beta = beta;
+      g.gamma = tot[0];
     }
   }
-  __syncthreads();   // red may be reused right after
 }
 
 __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs za, GridPlan gp) {
-  __shared__ GridState gs[kGridMaxSeg];
-  __shared__ double red[3 * 32];
+  __shared__ GridState gs[kGridMaxSlots];
+  __shared__ int4 s_tile[kGridMaxTiles];
+  __shared__ double wred[kGridMaxTiles * (kGridThreads / 32) * 3];
   __shared__ int s_ok;
   __shared__ unsigned s_act;
   const int tid = threadIdx.x, nth = blockDim.x;
-  const int2 cs = gp.cseg[blockIdx.x];
-  const int nseg = cs.y - cs.x;
+  const int c = blockIdx.x, G = gridDim.x;
+  const int nslot = gp.cnslot[c];
+  const int ntl = (gp.ntile - c + G - 1) / G;      // this CTA's tiles: c, c+G, c+2G, ...
   unsigned bar = 0;
 
-  if (tid < nseg) {
-    const int4 sg = gp.seg[cs.x + tid];
+  if (tid < nslot) {
     GridState &g = gs[tid];
     g.stage = G_RES; g.first = 1; g.conv = 0; g.outer = 0; g.inner = 0; g.iters = 0; g.cur = 0;
-    g.basin = sg.z; g.owner = sg.w;
+    g.basin = gp.cslot[c * kGridMaxSlots + tid];
+    g.owner = (gp.cowner[c] >> tid) & 1;
     g.tol = g.itol2 = g.rn = g.resid0 = g.alpha = g.beta = g.gamma = 0.;
   }
+  if (tid < ntl) s_tile[tid] = gp.tile[c + tid * G];
   if (blockIdx.x == 0 && tid == 0 && d.imax) { *d.imax = 0; *d.subj = 0; }
+  __syncthreads();
 
   // ---- assembly (FP64 gather in element order), Jacobi diagonal, start ----
-  for (int q = 0; q < nseg; q++) {
-    const int4 sg = gp.seg[cs.x + q];
-    const BasinPar &P = d.par[sg.z];
-    if (sg.w && tid < kMaxScal) d.out[sg.z].stab[tid] = 0.f;   // reset for k_stab's max
+  for (int q = 0; q < ntl; q++) {
+    const int4 tl = s_tile[q];
+    const BasinPar &P = d.par[tl.z];
+    if (tl.x == P.k0 && tid < kMaxScal) d.out[tl.z].stab[tid] = 0.f;   // reset for k_stab's max
     const float dtf = (float)P.dt;
-    for (int i = sg.x + tid; i < sg.y; i += nth) {
+    for (int i = tl.x + tid; i < tl.y; i += nth) {
       double diag, rhs;
       assemble_row(d, za, i, dtf, diag, rhs);
       d.dinv32[i] = diag != 0. ? (float)(1. / diag) : 1.f;
@@ -208,8 +236,7 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
     }
   }
   if (za.explicit_mode) {   // system_set_explicit: no coupling between rows, no barrier
-    __syncthreads();
-    if (tid < nseg && gs[tid].owner) {
+    if (tid < nslot && gs[tid].owner) {
       BasinOut &O = d.out[gs[tid].basin];
       O.iters = 0; O.refinements = 0; O.resid0 = 0.; O.resid = 0.;
     }
@@ -219,14 +246,15 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
 
   for (unsigned k = 0;; k++) {
     const int par = (int)(k & 1u);
-    // ---- the work of each segment's stage ----
-    for (int q = 0; q < nseg; q++) {
-      const int4 sg = gp.seg[cs.x + q];
-      const int a = sg.x, e = sg.y;
-      const int stage = gs[q].stage;
+    // ---- the work of each tile's stage ----
+    for (int q = 0; q < ntl; q++) {
+      const int4 tl = s_tile[q];
+      const int a = tl.x, e = tl.y;
+      GridState &g = gs[tl.w];
+      const int stage = g.stage;
       double v[3] = {0., 0., 0.};
       if (stage == G_RES) {
-        float4 *qo = d.cg4[gs[q].cur];
+        float4 *qo = d.cg4[g.cur];
         for (int i = a + tid; i < e; i += nth) {
           const double t = grid_resid_row(d, i);
           qo[i] = make_float4((float)t, 0.f, 0.f, d.dinv32[i]);
@@ -238,8 +266,8 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
         for (int i = a + tid; i < e; i += nth) d.x64[i] = 2. * (double)za.zguess[i] - (double)za.zprev[i];
       } else if (stage == G_SPMV0) {
         // w = A u with u = r/diag (fa = 0 and s = 0 leave r, so u = r/diag)
-        const float4 *qi = d.cg4[gs[q].cur];
-        float4 *qo = d.cg4[gs[q].cur ^ 1];
+        const float4 *qi = d.cg4[g.cur];
+        float4 *qo = d.cg4[g.cur ^ 1];
         for (int i = a + tid; i < e; i += nth) {
           const float w = grid_spmv_row(d, i, qi, 0.f, 0.f);
           const float4 me = qi[i];
@@ -251,9 +279,9 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
         }
       } else if (stage == G_ITER) {
         // p = u + b p, s = w + b s, e += a p, r -= a s, u = r/diag, w = A u
-        const float fa = (float)gs[q].alpha, fb = (float)gs[q].beta;
-        const float4 *qi = d.cg4[gs[q].cur];
-        float4 *qo = d.cg4[gs[q].cur ^ 1];
+        const float fa = (float)g.alpha, fb = (float)g.beta;
+        const float4 *qi = d.cg4[g.cur];
+        float4 *qo = d.cg4[g.cur ^ 1];
         for (int i = a + tid; i < e; i += nth) {
           const float4 me = qi[i];
           const float2 pe = d.cg2[i];
@@ -273,10 +301,36 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
         for (int i = a + tid; i < e; i += nth) d.zn[i] = (float)d.x64[i];
       }
       if (stage == G_RES || stage == G_SPMV0 || stage == G_ITER) {
-        block_sum0<3>(v, red);
-        if (tid == 0) {
-          double *pp = gp.partial + ((size_t)par * gp.nseg + (cs.x + q)) * 4;
-          __stcg(pp + 0, v[0]); __stcg(pp + 1, v[1]); __stcg(pp + 2, v[2]);
+        // warp sums now, the sum over warps once all tiles are done (no CTA
+        // barrier between tiles, so warps run ahead into the next tile)
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v[cc] += __shfl_xor_sync(0xffffffffu, v[cc], o);
+        }
+        if ((tid & 31) == 0) {
+          double *w = wred + ((size_t)q * (kGridThreads / 32) + (tid >> 5)) * 3;
+          w[0] = v[0]; w[1] = v[1]; w[2] = v[2];
+        }
+      }
+    }
+    __syncthreads();
+    // tile partials: warp w sums the warp sums of tiles w, w+16, ... in a fixed tree
+    {
+      const int warp = tid >> 5, lane = tid & 31;
+      for (int q = warp; q < ntl; q += kGridThreads / 32) {
+        const int stage = gs[s_tile[q].w].stage;
+        if (stage != G_RES && stage != G_SPMV0 && stage != G_ITER) continue;
+        double x[3];
+#pragma unroll
+        for (int cc = 0; cc < 3; cc++) {
+          x[cc] = lane < kGridThreads / 32 ? wred[((size_t)q * (kGridThreads / 32) + lane) * 3 + cc] : 0.;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) x[cc] += __shfl_xor_sync(0xffffffffu, x[cc], o);
+        }
+        if (lane == 0) {
+          double *pp = gp.partial + ((size_t)par * gp.ntile + (c + q * G)) * 4;
+          __stcg(pp + 0, x[0]); __stcg(pp + 1, x[1]); __stcg(pp + 2, x[2]);
         }
       }
     }
@@ -284,7 +338,7 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
     // ---- finished basins leave the machine; count the active ones ----
     if (tid == 0) {
       unsigned nact = 0;
-      for (int q = 0; q < nseg; q++) {
+      for (int q = 0; q < nslot; q++) {
         GridState &g = gs[q];
         if (g.stage == G_FINISH) {
           if (g.owner) {
@@ -304,74 +358,33 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
     }
     if (!grid_barrier(gp.ctr, ++bar, &s_ok, 1 + k % 3, &s_act)) goto aborted;
     if (s_act == 0u) break;
-    // ---- per-basin sums over its segments, the same in every CTA; next stage ----
+    // ---- per-basin sums over its tiles, the same in every CTA; next stage ----
     {
       const int warp = tid >> 5, lane = tid & 31;
-      if (warp < nseg) {
+      if (warp < nslot) {
         GridState &g = gs[warp];
         const int st = g.stage;
         if (st == G_RES || st == G_SPMV0 || st == G_ITER) {
-          const int2 bs = gp.bseg[g.basin];
+          const int2 bt = gp.btile[g.basin];
           double tot[3] = {0., 0., 0.};
           // up to 32*kGridPartialUnroll partials per round, all loads issued first
-          for (int s0 = bs.x; s0 < bs.y; s0 += 32 * kGridPartialUnroll) {
+          for (int s0 = bt.x; s0 < bt.y; s0 += 32 * kGridPartialUnroll) {
             double pv[kGridPartialUnroll][3];
 #pragma unroll
             for (int u = 0; u < kGridPartialUnroll; u++) {
               const int s = s0 + u * 32 + lane;
-              const double *pp = gp.partial + ((size_t)par * gp.nseg + (s < bs.y ? s : bs.x)) * 4;
+              const double *pp = gp.partial + ((size_t)par * gp.ntile + (s < bt.y ? s : bt.x)) * 4;
               pv[u][0] = __ldcg(pp + 0); pv[u][1] = __ldcg(pp + 1); pv[u][2] = __ldcg(pp + 2);
             }
 #pragma unroll
             for (int u = 0; u < kGridPartialUnroll; u++)
-              if (s0 + u * 32 + lane < bs.y) { tot[0] += pv[u][0]; tot[1] += pv[u][1]; tot[2] += pv[u][2]; }
+              if (s0 + u * 32 + lane < bt.y) { tot[0] += pv[u][0]; tot[1] += pv[u][1]; tot[2] += pv[u][2]; }
           }
 #pragma unroll
-          for (int c = 0; c < 3; c++)
+          for (int cc = 0; cc < 3; cc++)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) tot[c] += __shfl_xor_sync(0xffffffffu, tot[c], o);
-          if (lane == 0) {
-            const BasinPar &P = d.par[g.basin];
-            if (st == G_RES) {
-              const double rn = sqrt(tot[0]);
-              bool next = true;
-              if (g.first) {
-                g.first = 0;
-                g.tol = (double)P.rtol * rn + (double)P.atol;
-                g.resid0 = rn;
-                if (za.zprev != nullptr && d.out[g.basin].steps > 0 && rn > g.tol) { g.stage = G_XTRP; next = false; }
-              }
-              if (next) {
-                g.rn = rn;
-                if (rn <= g.tol) { g.conv = 1; g.stage = G_FINISH; }
-                else if (g.outer >= za.max_outer) g.stage = G_FINISH;
-                else {
-                  const double it = fmax((double)za.inner_rtol * rn, 0.25 * g.tol);
-                  g.itol2 = it * it;
-                  g.stage = G_SPMV0;
-                }
-              }
-            } else if (st == G_SPMV0) {
-              g.cur ^= 1;
-              g.gamma = tot[0];
-              g.alpha = g.gamma / tot[1];
-              g.beta = 0.;
-              g.inner = 0;
-              g.stage = G_ITER;
-            } else {   // G_ITER
-              g.cur ^= 1;
-              g.iters++;
-              g.inner++;
-              const bool stop = !(tot[2] > g.itol2) || !(tot[0] == tot[0]) || g.inner >= P.maxit;
-              if (stop) g.stage = G_FIX;
-              else {
-                const double beta = tot[0] / g.gamma;
-                g.alpha = tot[0] / (tot[1] - beta * tot[0] / g.alpha);
-                g.beta = beta;
-                g.gamma = tot[0];
-              }
-            }
-          }
+            for (int o = 16; o > 0; o >>= 1) tot[cc] += __shfl_xor_sync(0xffffffffu, tot[cc], o);
+          if (lane == 0) grid_transition(g, tot, d, za);
         } else if (lane == 0) {
           if (st == G_XTRP) g.stage = G_RES;
           else if (st == G_FIX) { g.outer++; g.stage = G_RES; }
@@ -383,7 +396,7 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
   return;
 
 aborted:
-  if (tid < nseg && gs[tid].owner) set_status(&d.out[gs[tid].basin], SHY_ECUDA);
+  if (tid < nslot && gs[tid].owner) set_status(&d.out[gs[tid].basin], SHY_ECUDA);
 }
 
 }  // namespace shy

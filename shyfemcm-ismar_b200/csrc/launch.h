@@ -44,15 +44,18 @@ struct ZetaMaps {
   const int *loc = nullptr, *push_ptr = nullptr, *push = nullptr;
 };
 
-// the device-wide zeta solver (k_zeta_grid): CTA c owns the row segments
-// cseg[c].x .. cseg[c].y-1; segment s = {row0, row1, basin, first segment of
-// its basin}; basin b's segments are bseg[b].x .. bseg[b].y-1
+// the device-wide zeta solver (k_zeta_grid).  Each basin's rows are cut into
+// tiles of a fixed row count (the last one shorter); tile t = {row0, row1,
+// basin, slot} is worked by CTA t % G, where `slot` indexes the CTA's table
+// of basins: cslot[c*16 + slot] is the basin, bit slot of cowner[c] says the
+// CTA holds the basin's first tile; basin b's tiles are btile[b].x .. .y-1
 struct GridPlan {
-  int nseg = 0;
-  const int4 *seg = nullptr;
-  const int2 *bseg = nullptr, *cseg = nullptr;
-  double *partial = nullptr;       // [2][nseg][4] partial sums of the segments
-  unsigned *ctr = nullptr;         // [8]: barrier arrivals, 3 active counts, abort flag
+  int ntile = 0;
+  const int4 *tile = nullptr;
+  const int2 *btile = nullptr;
+  const int *cslot = nullptr, *cnslot = nullptr, *cowner = nullptr;
+  double *partial = nullptr;       // [2][ntile][4] partial sums of the tiles
+  unsigned *ctr = nullptr;         // [8]: barrier arrivals, 3 active counts, abort flag, release
 };
 
 // a group of basins solved by one launch with one cluster shape
@@ -75,7 +78,8 @@ cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs
 cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &gp, int G, cudaStream_t st);
 // CTAs of k_zeta_grid that fit the device at once (0 on error)
 int zeta_grid_capacity();
-int zeta_grid_max_segments();
+int zeta_grid_max_slots();   // basins one CTA can hold
+int zeta_grid_max_tiles();   // tiles one CTA can hold
 // smem > 0 prepares the shared-memory variant for that many dynamic bytes
 cudaError_t zeta_kernel_setup(int CL, size_t smem);
 int zeta_max_active_clusters(int CL, int threads, size_t smem);

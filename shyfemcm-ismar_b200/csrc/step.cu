@@ -167,7 +167,8 @@ int zeta_grid_capacity() {
   return nb * nsm;
 }
 
-int zeta_grid_max_segments() { return kGridMaxSeg; }
+int zeta_grid_max_slots() { return kGridMaxSlots; }
+int zeta_grid_max_tiles() { return kGridMaxTiles; }
 
 cudaError_t zeta_kernel_setup(int CL, size_t smem) {
   cudaError_t e = cudaSuccess;

@@ -210,12 +210,13 @@ def basin3d_case(nkn_target=20000, lx=50.0e3, ly=30.0e3, seed=2, dt=120.0,
     return _finish(case)
 
 
-def ensemble_cases(n, nkn_lo=5000, nkn_hi=100000, nlv=10, seed=4, dt=60.0):
+def ensemble_cases(n, nkn_lo=5000, nkn_hi=100000, nlv=10, seed=4, dt=60.0, first=None):
     """Independent basins with log-uniform node counts and seeded aspect
-    ratios and wind perturbations (sigma = 3 m/s)."""
+    ratios and wind perturbations (sigma = 3 m/s).  `first` builds only the
+    first members of the same ensemble."""
     rng = np.random.default_rng(seed)
     out = []
-    for m in range(n):
+    for m in range(n if first is None else min(first, n)):
         nk = int(math.exp(rng.uniform(math.log(nkn_lo), math.log(nkn_hi))))
         aspect = rng.uniform(2.0, 6.0)
         ly = 2.0e3 * math.sqrt(nk / 793.0)
