@@ -2,9 +2,10 @@
 // thread-block cluster can hold: one persistent cooperative launch over the
 // whole device for every basin of the model.
 //
-// Each CTA owns a contiguous slice of the model's rows (all basins' rows are
-// contiguous), cut at basin boundaries into segments; a basin's segments are
-// consecutive.  The solver is the one of k_zeta_sm (system_solve,
+// Each basin's rows are cut into tiles of 1024 rows, and tile t is worked by
+// CTA t % G, so the tiles of a basin sit on consecutive CTAs and the work of
+// the few basins still iterating late in a solve spreads over many CTAs.
+// The solver is the one of k_zeta_sm (system_solve,
 // sparskit_admin.f90:115-334, with the reference's stop test
 // ||r|| <= rtol*||r0|| + atol, spk_iters.f90:3304-3360): FP64 residual
 // refinement around Jacobi-preconditioned Chronopoulos-Gear CG in FP32, the
@@ -15,11 +16,12 @@
 // for the product A u, and computes it from their values of the previous
 // iteration (kept in a second generation of the vectors) with the iteration
 // scalars a, b that every row of the basin shares, so no barrier separates
-// the vector update from the matrix-vector product.  In a super-step each segment does the work of its
-// basin's stage and writes its partial sums; after the barrier every CTA
-// that holds a segment of the basin sums that basin's partials in segment
-// order (the same bits in every CTA) and takes the same stage decision.
-// A basin that has finished idles until every basin has.
+// the vector update from the matrix-vector product.  In a super-step each
+// tile does the work of its basin's stage and writes its partial sums; after
+// the barrier every CTA that holds a tile of the basin sums that basin's
+// partials in tile order (the same bits in every CTA, and the same alone or
+// in any batch) and takes the same stage decision.  A basin that has
+// finished idles until every basin has.
 //
 // The grid barrier is an arrival counter with a bounded wait: a CTA that
 // waits longer than kGridSpinLimit polls marks every basin of the launch
