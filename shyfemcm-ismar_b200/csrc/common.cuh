@@ -56,6 +56,7 @@ struct BasinOut {
 // everything a kernel needs, passed by value
 struct Dev {
   int nbasin, NKN, NEL, NLV, S, nsc_max;
+  int col_threads;              // column kernel: 1 one thread per column, 0 one warp segment
   BasinPar *par;
   BasinOut *out;
   // mesh (static)

@@ -835,6 +835,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   Arena &A = m->arena;
   Dev &d = m->base;
   d.nbasin = nbasin; d.NKN = NKN; d.NEL = NEL; d.NLV = NLV; d.S = m->S; d.nsc_max = nsc_max;
+  d.col_threads = 1;
   ST_TRY(A.upload(&d.par, m->par) ? bail(SHY_ECAPACITY) : 0);
   std::vector<BasinOut> outs(nbasin);
   memset(outs.data(), 0, sizeof(BasinOut) * nbasin);
@@ -928,6 +929,9 @@ extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value
     m->zvariant = iv;
     ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
   }
+  else if (n == "column_threads") {   // 1: one thread per column when it has at most 16 layers
+    m->base.col_threads = iv != 0;
+  }
   else if (n == "inner_rtol") { if (!(value > 0 && value < 1)) return fail(SHY_EARG, "inner_rtol in (0,1)"); m->inner_rtol = (float)value; }
   else if (n == "max_outer") { if (iv < 1 || iv > 100) return fail(SHY_EARG, "max_outer 1..100"); m->max_outer = iv; }
   else if (n == "symmetric") {
@@ -947,6 +951,7 @@ extern "C" double shygpu_get_option(shygpu_model *m, const char *name) {
   if (n == "cluster_size") return m->zcl.empty() ? -1 : m->zcl[0].CL;
   if (n == "zeta_threads") return m->zcl.empty() ? -1 : m->zcl[0].threads;
   if (n == "zeta_classes") return (double)m->zcl.size();
+  if (n == "column_threads") return m->base.col_threads;
   if (n == "inner_rtol") return m->inner_rtol;
   if (n == "max_outer") return m->max_outer;
   if (n == "symmetric") return m->sym;

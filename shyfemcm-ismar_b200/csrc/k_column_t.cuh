@@ -1,0 +1,265 @@
+// k_column_t.cuh -- the column kernel with one thread per element column,
+// for shallow columns (at most L layers): hydro_transports / hydro_intern /
+// hydro_zeta element part (hydrodynamic.f90:758-864, 868-1416, 488-733).
+//
+// The same arithmetic as k_column (k_column.cuh), which spreads a column's
+// layers over the lanes of a warp segment and solves the vertical system
+// by parallel cyclic reduction.  For short columns most of k_column's work
+// is per element (the FP64 barotropic terms, the 3x3 element system, the
+// level boundary), done once per segment while the other lanes idle, and a
+// 10-layer column leaves 6 of 16 lanes empty.  Here each thread walks its
+// column top to bottom: the layer coefficients of hydro_intern
+// (:1098-1304) on a sliding window of the layer above and below, a Thomas
+// sweep for the tridiagonal system (the reference's tria_multi,
+// penta.f90:333-372; FP32 here as k_column's PCR), and the element system
+// with all 32 lanes of a warp busy on 32 elements.
+// Included by step.cu.
+#pragma once
+#include "common.cuh"
+#include "physics.cuh"
+
+namespace shy {
+
+template <int L, bool COR>
+__global__ void __launch_bounds__(128) k_column_t(Dev d) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.NEL) return;
+  const int NLV = d.NLV;
+  const int4 en = d.enode[e];
+  const BasinPar &P = d.par[en.w];
+  const int kn[3] = {en.x, en.y, en.z};
+  const int ilevel = d.ilhv[e];
+  const double dt = P.dt;
+  const float *evp = d.ev8 + (size_t)e * 8;
+  double b[3], c[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) { b[i] = evp[i]; c[i] = evp[3 + i]; }
+  const double aj = evp[6];
+
+  // barotropic terms (hydro_intern :1011-1041), FP64 like the reference
+  double bz = 0., cz = 0., bpres = 0., cpres = 0., tx = 0., ty = 0.;
+#pragma unroll
+  for (int ii = 0; ii < 3; ii++) {
+    const double zz = d.zeo[3 * e + ii];
+    bz += zz * b[ii]; cz += zz * c[ii];
+    const double pp = d.ppv[kn[ii]];
+    bpres += pp * b[ii]; cpres += pp * c[ii];
+    tx += d.taux[kn[ii]]; ty += d.tauy[kn[ii]];
+  }
+  const double drittl = 1. / 3.;
+  tx *= drittl; ty *= drittl;
+  const double gammat = COR ? (double)d.fcorv[e] : 0.;
+  const double gamma = (double)P.af * dt * gammat;
+
+  // the column (inactive layers read as zero)
+  const size_t o = (size_t)e * NLV;
+  float h[L], u[L], v[L];
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    const bool act = l < ilevel;
+    h[l] = act ? d.heo[o + l] : 0.f;
+    u[l] = act ? d.uo[o + l] : 0.f;
+    v[l] = act ? d.vo[o + l] : 0.f;
+  }
+  const int I = NLV + 1;
+  const float aux = (float)dt * P.at;
+  const bool explicit_visc = P.ahpar > 0.f;
+  const bool barocl = P.ibarcl > 0 && P.ibarcl != 3 && P.ibarcl != 5;
+  const float area = 12.f * (float)aj;
+  const float *hld = d.hldv + (size_t)en.w * NLV;
+  const float raux = P.grav / P.rowass;
+
+  // forward Thomas sweep as the layer coefficients are formed
+  float cp[L];
+  float dp0[L], dp1[L], dp2[L];            // real: rhs ppx, ppy, h
+  float2 cpc[COR ? L : 1], dq0[COR ? L : 1], dq1[COR ? L : 1];   // complex: ppx+i ppy, h
+  float alev_t = P.vismol;
+  if (0 < ilevel)
+    alev_t += (d.visv[(size_t)kn[0] * I] + d.visv[(size_t)kn[1] * I] + d.visv[(size_t)kn[2] * I]) * (1.f / 3.f);
+  float brm = 0.f, crm = 0.f, hhm = 0.f;   // baroclinic values of the layer above
+  float pxs = 0.f, pys = 0.f;              // their running sums from the surface
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    if (l >= ilevel) break;
+    const bool bfirst = l == 0, blast = l == ilevel - 1;
+    const float hhi = h[l], uui = u[l], vvi = v[l];
+    float hhip = blast ? 0.f : h[l + 1 < L ? l + 1 : l];
+    float uuip = blast ? uui : u[l + 1 < L ? l + 1 : l];
+    float vvip = blast ? vvi : v[l + 1 < L ? l + 1 : l];
+    const float hhim = bfirst ? 0.f : h[l > 0 ? l - 1 : 0];
+    const float uuim = bfirst ? uui : u[l > 0 ? l - 1 : 0];
+    const float vvim = bfirst ? vvi : v[l > 0 ? l - 1 : 0];
+    const float rhact = hhi > 0.f ? 1.f / hhi : 0.f;
+    const float rhactp = hhip > 0.f ? 1.f / hhip : 0.f;
+    const float rhactm = hhim > 0.f ? 1.f / hhim : 0.f;
+    // element viscosity at the bottom interface (:1098-1104)
+    const float alev_b = P.vismol + (d.visv[(size_t)kn[0] * I + l + 1] + d.visv[(size_t)kn[1] * I + l + 1] +
+                                     d.visv[(size_t)kn[2] * I + l + 1]) * (1.f / 3.f);
+    float rhp = 0.f, rhm = 0.f;
+    if (hhi > 0.f) {
+      if (hhip > 0.f) rhp = 2.f * alev_b / (hhi + hhip);
+      if (hhim > 0.f) rhm = 2.f * alev_t / (hhi + hhim);
+    }
+    alev_t = alev_b;
+    float aa = aux * rhact * (rhm + rhp);
+    float aat = rhact * (rhm + rhp);
+    const float bb = aux * rhactp * rhp, bbt = rhactp * rhp;
+    const float cc = aux * rhactm * rhm, cct = rhactm * rhm;
+    float ppx = 0.f, ppy = 0.f;
+    if (bfirst) { ppx -= (float)tx; ppy -= (float)ty; }
+    if (blast) {
+      // bottom_friction (chezy.f90:239-398), ireib 5: rr = cd |U_b| / h^2
+      const float uv = sqrtf(uui * uui + vvi * vvi);
+      const float hzg = hhi < P.hzoff ? P.hzoff : hhi;
+      float rr = 0.f;
+      if (P.ireib == 5) rr = d.czv[e] * uv / (hzg * hzg);
+      aa += (float)dt * rr;
+      aat += rr;
+    }
+    // explicit terms fxv/fyv (set_explicit, explicit.f90:123-213)
+    float fx = 0.f, fy = 0.f;
+    if (explicit_visc) {                 // set_diff_horizontal (:389-493)
+      for (int ii = 0; ii < 3; ii++) {
+        int iei = d.ieltv[3 * e + ii];
+        if (iei < 0) iei = e;
+        if (l >= d.ilhv[iei]) continue;
+        const float areai = 12.f * d.ev8[(size_t)iei * 8 + 6];
+        const float ui = d.uo[(size_t)iei * NLV + l], vi = d.vo[(size_t)iei * NLV + l];
+        const float anu = P.ahpar * d.difhv[o + l];
+        const float ai = 2.f * anu / (area + areai);
+        fx -= ai * (ui - uui);
+        fy -= ai * (vi - vvi);
+      }
+    }
+    if (barocl) {
+      // set_barocl_new_interface for z-layers (explicit.f90:1226-1530)
+      float br = 0.f, cr = 0.f;
+#pragma unroll
+      for (int ii = 0; ii < 3; ii++) {
+        const float rp = d.rho[(size_t)kn[ii] * NLV + l];
+        br += (float)b[ii] * rp; cr += (float)c[ii] * rp;
+      }
+      const float hlayer = hld[l];
+      const float hh = 0.5f * hlayer;
+      const float brup = bfirst ? br : brm, crup = bfirst ? cr : crm, hhup = bfirst ? 0.f : hhm;
+      const float hint = hh + hhup;
+      pxs += hint * 0.5f * (br + brup);
+      pys += hint * 0.5f * (cr + crup);
+      brm = br; crm = cr; hhm = hh;
+      fx += raux * hlayer * pxs;
+      fy += raux * hlayer * pys;
+    }
+    ppx += aat * uui - bbt * uuip - cct * uuim - (float)gammat * vvi + (float)(P.grav * hhi * bz) +
+           (hhi / P.rowass) * (float)bpres + fx;
+    ppy += aat * vvi - bbt * vvip - cct * vvim + (float)gammat * uui + (float)(P.grav * hhi * cz) +
+           (hhi / P.rowass) * (float)cpres + fy;
+    // vertical system (hydrodynamic.f90:1270-1343): -cc, 1+aa (+ i gamma), -bb
+    const float lo = bfirst ? 0.f : -cc;
+    const float up = blast ? 0.f : -bb;
+    const float dg = 1.f + aa;
+    if constexpr (!COR) {
+      const float cprev = bfirst ? 0.f : cp[l > 0 ? l - 1 : 0];
+      const float rden = 1.f / (dg - lo * cprev);
+      cp[l] = up * rden;
+      dp0[l] = (ppx - (bfirst ? 0.f : lo * dp0[l > 0 ? l - 1 : 0])) * rden;
+      dp1[l] = (ppy - (bfirst ? 0.f : lo * dp1[l > 0 ? l - 1 : 0])) * rden;
+      dp2[l] = (hhi - (bfirst ? 0.f : lo * dp2[l > 0 ? l - 1 : 0])) * rden;
+    } else {
+      const float2 cprev = bfirst ? make_float2(0.f, 0.f) : cpc[l > 0 ? l - 1 : 0];
+      const float2 den = make_float2(dg - lo * cprev.x, (float)gamma - lo * cprev.y);
+      const float2 one = make_float2(1.f, 0.f);
+      const float2 rden = cdivf(one, den);
+      cpc[l] = make_float2(up * rden.x, up * rden.y);
+      float2 r0 = make_float2(ppx, ppy), r1 = make_float2(hhi, 0.f);
+      if (!bfirst) {
+        const float2 p0 = dq0[l > 0 ? l - 1 : 0], p1 = dq1[l > 0 ? l - 1 : 0];
+        r0.x -= lo * p0.x; r0.y -= lo * p0.y;
+        r1.x -= lo * p1.x; r1.y -= lo * p1.y;
+      }
+      dq0[l] = cmulf(r0, rden);
+      dq1[l] = cmulf(r1, rden);
+    }
+  }
+
+  // back substitution, new transports, layer sums of hydro_zeta
+  double dbb = 0., dcb = 0., uold = 0., vold = 0., uh = 0., vh = 0.;
+  float x0 = 0.f, x1 = 0.f, x2 = 0.f;
+  float2 y0 = make_float2(0.f, 0.f), y1 = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int l = L - 1; l >= 0; l--) {
+    if (l >= NLV) continue;
+    const bool act = l < ilevel;
+    float solu = 0.f, solv = 0.f, hre = 0.f, him = 0.f;
+    if (act) {
+      const bool blast = l == ilevel - 1;
+      if constexpr (!COR) {
+        x0 = dp0[l] - (blast ? 0.f : cp[l] * x0);
+        x1 = dp1[l] - (blast ? 0.f : cp[l] * x1);
+        x2 = dp2[l] - (blast ? 0.f : cp[l] * x2);
+        solu = x0; solv = x1; hre = x2;
+      } else {
+        if (blast) { y0 = dq0[l]; y1 = dq1[l]; }
+        else {
+          const float2 t0 = cmulf(cpc[l], y0), t1 = cmulf(cpc[l], y1);
+          y0 = make_float2(dq0[l].x - t0.x, dq0[l].y - t0.y);
+          y1 = make_float2(dq1[l].x - t1.x, dq1[l].y - t1.y);
+        }
+        solu = y0.x; solv = y0.y; hre = y1.x; him = y1.y;
+      }
+    }
+    const float uhat = act ? (float)(u[l] - dt * solu) : 0.f;
+    const float vhat = act ? (float)(v[l] - dt * solv) : 0.f;
+    d.un[o + l] = uhat;
+    d.vn[o + l] = vhat;
+    d.ddx[o + l] = act ? hre : 0.f;
+    if (COR) d.ddxi[o + l] = act ? him : 0.f;
+    if (act) {
+      dbb += (double)hre; dcb += (double)him;
+      uold += (double)u[l]; vold += (double)v[l];
+      uh += (double)uhat; vh += (double)vhat;
+    }
+  }
+
+  // hydro_zeta (hydrodynamic.f90:604-733): the element system
+  // ddxv(ju) = Re, ddxv(jv) = Im, ddyv(ju) = -Im, ddyv(jv) = Re
+  const double dbc = -dcb, dcc = dbb;
+  const double az = P.az, am = P.am;
+  const double ut = az * uh + (1. - az) * uold;
+  const double vt = az * vh + (1. - az) * vold;
+  const double delta = dt * dt * az * am * (double)P.grav;
+  double z[3], hia[3][3], hik[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) z[i] = d.zeo[3 * e + i];
+#pragma unroll
+  for (int n = 0; n < 3; n++) {
+#pragma unroll
+    for (int m = 0; m < 3; m++) {
+      const double abn = b[n] * (b[m] * dbb + c[m] * dbc);
+      const double acn = c[n] * (b[m] * dcb + c[m] * dcc);
+      hia[n][m] = aj * ((n == m ? 4. : 0.) + 12. * delta * (abn + acn));
+    }
+    hik[n] = hia[n][0] * z[0] + hia[n][1] * z[1] + hia[n][2] * z[2] + 12. * aj * dt * (ut * b[n] + vt * c[n]);
+  }
+  // level boundary conditions (:688-704), rzv at the new time (sp111)
+  const double tnew = d.out[en.w].dtime + dt;
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    const int kb = d.kbnd[kn[i]];
+    if (kb > 0) {
+      const double rw = level_bc(d, P, kb, tnew);
+      const int j1 = (i + 1) % 3, j2 = (i + 2) % 3;
+      hik[j1] -= rw * hia[j1][i];
+      hik[j2] -= rw * hia[j2][i];
+      hia[i][j1] = 0.; hia[i][j2] = 0.; hia[j1][i] = 0.; hia[j2][i] = 0.;
+      hik[i] = rw * hia[i][i];
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < 3; n++) {
+#pragma unroll
+    for (int m = 0; m < 3; m++) d.hia[(size_t)(3 * n + m) * d.NEL + e] = (float)hia[n][m];
+    d.hik[(size_t)n * d.NEL + e] = (float)hik[n];
+  }
+}
+
+}  // namespace shy

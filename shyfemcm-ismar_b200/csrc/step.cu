@@ -4,7 +4,9 @@
 //   k_column  hydro_transports + hydro_intern + hydro_zeta element part
 //             (hydrodynamic.f90:758-864, 868-1416, 488-733): one warp segment per
 //             element column, vertical system by PCR across lanes, 3x3 element
-//             system of the zeta equation written per element.
+//             system of the zeta equation written per element; k_column_t, the
+//             same with one thread per column (Thomas sweep) for columns of at
+//             most 16 layers.
 //   k_zeta    system_init/assemble/add_rhs/solve/get (simsys_spkaux.f90:137-705,
 //             sparskit_admin.f90:115-334): one thread-block cluster per basin;
 //             atomic-free gather assembly into CSR in element order (FP64), then
@@ -30,6 +32,7 @@
 #include "launch.h"
 #include "physics.cuh"
 #include "k_column.cuh"
+#include "k_column_t.cuh"
 #include "k_final.cuh"
 #include "k_node.cuh"
 #include "k_conz.cuh"
@@ -75,7 +78,19 @@ static void launch_node_S(const Dev &d, const int *kbas, int which, int a, int b
   }
 }
 
+template <int L>
+static void launch_column_t(const Dev &d, cudaStream_t st, bool cor) {
+  const int blocks = (d.NEL + 127) / 128;
+  if (cor) k_column_t<L, true><<<blocks, 128, 0, st>>>(d);
+  else k_column_t<L, false><<<blocks, 128, 0, st>>>(d);
+}
+
 void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool cor) {
+  if (which == 0 && d.col_threads && d.NLV <= 16) {
+    if (d.NLV <= 8) launch_column_t<8>(d, st, cor);
+    else launch_column_t<16>(d, st, cor);
+    return;
+  }
   switch (d.S) {
     case 1: launch_elem_S<1>(d, which, init_only, st, cor); break;
     case 2: launch_elem_S<2>(d, which, init_only, st, cor); break;

@@ -48,9 +48,13 @@ def test_channel_2d_one_day_tide(channel):
     assert abs(ig.volume - io.volume) <= 1e-6 * io.volume
 
 
-def test_basin3d_baroclinic_ts(small3d):
-    """Config 2 shape at test size: z-layers, wind, M2, T/S, baroclinic."""
-    g, o = run_both(small3d, 120)
+@pytest.mark.parametrize("column_threads", [1, 0])
+def test_basin3d_baroclinic_ts(small3d, column_threads):
+    """Config 2 shape at test size: z-layers, wind, M2, T/S, baroclinic;
+    the column kernel with one thread per column and with one warp segment
+    per column."""
+    g, o = run_both(small3d, 120, column_threads=column_threads)
+    assert g.get_option("column_threads") == column_threads
     sg, so = g.get_state(0), o.state()
     assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
     m = active_mask(small3d)
@@ -71,6 +75,7 @@ def test_coriolis_column_solve():
     c = cases.basin3d_case(nkn_target=800, nlv=8, baroclinic=False, ts=False)
     c["fcorv"] = np.full(c["nel"], 1.0e-4, np.float32)
     g, o = run_both(c, 60)
+    assert g.get_option("column_threads") == 1
     sg, so = g.get_state(0), o.state()
     assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
     me = active_mask(c, node=False)
