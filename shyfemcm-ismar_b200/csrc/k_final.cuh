@@ -74,5 +74,75 @@ __global__ void __launch_bounds__(256) k_final(Dev d, int init_only) {
   if (valid && lane < NLV) d.hen[o] = (float)h;
 }
 
+// ===========================================================================
+// k_final_t: the same with one thread per element column (shallow columns):
+// the per-element FP64 terms once per element, the layers in a loop
+// ===========================================================================
+template <bool COR>
+__global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= d.NEL) return;
+  const int NLV = d.NLV;
+  const int4 en = d.enode[e];
+  const BasinPar &P = d.par[en.w];
+  const int kn[3] = {en.x, en.y, en.z};
+  const int ilevel = d.ilhv[e];
+  const size_t o = (size_t)e * NLV;
+  const float *evp = d.ev8 + (size_t)e * 8;
+  double zn3[3];
+#pragma unroll
+  for (int ii = 0; ii < 3; ii++) zn3[ii] = d.zn[kn[ii]];
+  if (!init_only) {
+    const double beta = P.dt * (double)P.grav * P.am;
+    double bz = 0., cz = 0.;
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) {
+      const double dz = zn3[ii] - (double)d.zeo[3 * e + ii];
+      bz += dz * evp[ii];
+      cz += dz * evp[3 + ii];
+    }
+    const double az = P.az;
+    double um = 0., vm = 0.;
+#pragma unroll 4
+    for (int l = 0; l < NLV; l++) {
+      const bool act = l < ilevel;
+      double u = 0., v = 0.;
+      if (act) {
+        const double re = d.ddx[o + l], im = COR ? (double)d.ddxi[o + l] : 0.;
+        const double du = beta * (re * bz - im * cz);
+        const double dv = beta * (im * bz + re * cz);
+        u = (double)(float)((double)d.un[o + l] - du);
+        v = (double)(float)((double)d.vn[o + l] - dv);
+        d.un[o + l] = (float)u;
+        d.vn[o + l] = (float)v;
+      }
+      // az*U^{n+1} + (1-az)*U^n for hydro_vertical, conzstab and conz3d
+      d.usv[o + l] = act ? (float)(az * u + (1. - az) * (double)d.uo[o + l]) : 0.f;
+      d.vsv[o + l] = act ? (float)(az * v + (1. - az) * (double)d.vo[o + l]) : 0.f;
+      um += u; vm += v;
+    }
+    d.unv[e] = (float)um;
+    d.vnv[e] = (float)vm;
+  }
+  // setzev and the element part of setdepth (z-layers)
+#pragma unroll
+  for (int ii = 0; ii < 3; ii++) d.zen[3 * e + ii] = (float)zn3[ii];
+  const float4 hm = d.hm3v[e];
+  const double zmed = (zn3[0] + zn3[1] + zn3[2]) / 3.;
+  const float *hld = d.hldv + (size_t)en.w * NLV;
+  const float *hlv = d.hlv + (size_t)en.w * NLV;
+  bool bad = false;
+  for (int l = 0; l < NLV; l++) {
+    double h = 0.;
+    if (l < ilevel) {
+      if (ilevel == 1) h = hm.w + zmed;
+      else if (l < ilevel - 1) h = (double)hld[l] + (l == 0 ? zmed : 0.);
+      else h = (double)hm.w - hlv[ilevel - 2];
+      if (!(h > 0.)) bad = true;
+    }
+    d.hen[o + l] = (float)h;
+  }
+  if (bad) set_status(&d.out[en.w], SHY_EDEPTH);
+}
 
 }  // namespace shy

@@ -91,6 +91,12 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
     else launch_column_t<16>(d, st, cor);
     return;
   }
+  if (which == 1 && d.col_threads && d.NLV <= 16) {
+    const int blocks = (d.NEL + 255) / 256;
+    if (cor) k_final_t<true><<<blocks, 256, 0, st>>>(d, init_only);
+    else k_final_t<false><<<blocks, 256, 0, st>>>(d, init_only);
+    return;
+  }
   switch (d.S) {
     case 1: launch_elem_S<1>(d, which, init_only, st, cor); break;
     case 2: launch_elem_S<2>(d, which, init_only, st, cor); break;
