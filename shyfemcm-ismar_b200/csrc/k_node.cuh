@@ -80,6 +80,96 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
 }
 
 // ===========================================================================
+// k_node_t: the same with one thread per node column (shallow columns): the
+// incident elements are walked once, each adding to the FP64 sums of all
+// its layers (in element order, as k_node); then the node's layers in turn
+// ===========================================================================
+template <int L>
+__global__ void __launch_bounds__(128) k_node_t(Dev d, const int *kbas, int init_only) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= d.NKN) return;
+  const int NLV = d.NLV, I = NLV + 1;
+  const int b = kbas[k];
+  const BasinPar &P = d.par[b];
+  const int lmax = d.ilhkv[k];
+  const double z = d.zn[k];
+  const float *hld = d.hldv + (size_t)b * NLV;
+  const float *hlv = d.hlv + (size_t)b * NLV;
+  double hsum[L], vf[L], va[L];
+#pragma unroll
+  for (int l = 0; l < L; l++) { hsum[l] = 0.; vf[l] = 0.; va[l] = 0.; }
+  for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
+    const int4 ix = d.incx[p];
+    const int e = ix.x, ii = ix.y & 3, le = ix.y >> 2;
+    const float *evp = d.ev8 + (size_t)e * 8;
+    const double aj = evp[6];
+    const double areafv = 4. * aj;            // 12*aj/3
+    const float4 hm = d.hm3v[e];
+    const double htot = ii == 0 ? hm.x : (ii == 1 ? hm.y : hm.z);
+    const double bb = evp[ii], cc = evp[3 + ii];
+    const size_t oe = (size_t)e * NLV;
+    const double hbot = le >= 2 ? htot - hlv[le - 2] : 0.;
+#pragma unroll
+    for (int l = 0; l < L; l++) {
+      if (l >= le) break;
+      double hl;
+      if (le == 1) hl = htot + z;
+      else if (l < le - 1) hl = (double)hld[l] + (l == 0 ? z : 0.);
+      else hl = hbot;
+      hsum[l] += areafv * hl;
+      if (!init_only) {
+        const double ff = (double)d.usv[oe + l] * bb + (double)d.vsv[oe + l] * cc;   // az*ffn + azt*ffo
+        const double aj4 = 4. * aj;
+        vf[l] += 3. * aj4 * ff;
+        va[l] += aj4;
+      }
+    }
+  }
+  const size_t o = (size_t)k * NLV;
+  double vol = 0.;
+  float hkf[L];
+  double area[L];
+  bool bad = false;
+#pragma unroll
+  for (int l = 0; l < L; l++) {
+    hkf[l] = 0.f; area[l] = 0.;
+    if (l >= NLV) continue;
+    const bool act = l < lmax;
+    area[l] = act ? (double)d.areakv[o + l] : 0.;
+    const double hk = act && area[l] > 0. ? hsum[l] / area[l] : 0.;
+    hkf[l] = (float)hk;
+    if (act && !(hkf[l] > 0.f)) bad = true;
+    d.hkn[o + l] = act ? hkf[l] : 0.f;
+    // node volume (masscont: sum of real hdknv*areakv in double)
+    vol += act ? (double)(hkf[l] * (float)area[l]) : 0.;
+  }
+  if (bad) set_status(&d.out[b], SHY_EDEPTH);
+  d.vol_node[k] = vol;
+  if (init_only) return;
+  // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771)
+  const bool wzero = P.nlv == 1 || d.kbnd[k] > 0;
+  double acc = 0.;                             // flux through the top of layer l
+#pragma unroll
+  for (int l = L - 1; l >= 0; l--) {
+    if (l >= NLV) continue;
+    const bool act = l < lmax;
+    double dv = 0.;
+    if (act && P.nlv > 1) {
+      const double voln = (double)(hkf[l] * (float)area[l]);
+      const double volo = (double)(d.hko[o + l] * (float)area[l]);
+      dv = vf[l] - (voln - volo) / P.dt;
+    }
+    acc += dv;
+    double wtop = acc;
+    if (l == 0) wtop = 0.;                     // wlnv(lmin-1) = 0
+    if (l >= 1 && act && va[l] > 0.) wtop /= va[l];
+    if (!act || wzero) wtop = 0.;
+    d.wl[(size_t)k * I + l] = (float)wtop;
+  }
+  d.wl[(size_t)k * I + NLV] = 0.f;
+}
+
+// ===========================================================================
 // k_stab: conzstab stability index per node, max-reduced per basin/scalar
 // ===========================================================================
 template <int S>

@@ -108,6 +108,12 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
 }
 
 void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStream_t st) {
+  if (which == 0 && d.col_threads && d.NLV <= 16) {
+    const int blocks = (d.NKN + 127) / 128;
+    if (d.NLV <= 8) k_node_t<8><<<blocks, 128, 0, st>>>(d, kbas, a);
+    else k_node_t<16><<<blocks, 128, 0, st>>>(d, kbas, a);
+    return;
+  }
   switch (d.S) {
     case 1: launch_node_S<1>(d, kbas, which, a, b, st); break;
     case 2: launch_node_S<2>(d, kbas, which, a, b, st); break;
