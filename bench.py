@@ -318,11 +318,8 @@ def main():
     nb = len(case_list)
     taux = [torch.from_numpy(np.ascontiguousarray(c["tauxnv"])).pin_memory() for c in case_list]
     tauy = [torch.from_numpy(np.ascontiguousarray(c["tauynv"])).pin_memory() for c in case_list]
-    outs = []
-    for c in case_list:
-        outs.append(dict(znv=torch.empty(c["nkn"], dtype=torch.float32).pin_memory(),
-                         utlnv=torch.empty(c["nel"] * c["nlv"], dtype=torch.float32).pin_memory(),
-                         vtlnv=torch.empty(c["nel"] * c["nlv"], dtype=torch.float32).pin_memory()))
+    # the step's result read back every step: the water level of every basin
+    outs = [dict(znv=torch.empty(c["nkn"], dtype=torch.float32).pin_memory()) for c in case_list]
     from shygpu import abi
     import ctypes as C
     states = []
@@ -332,7 +329,7 @@ def main():
             setattr(s, k, C.cast(C.c_void_p(v.data_ptr()), abi.f32p))
         states.append(s)
     h2d = sum(c["nkn"] * 8 for c in case_list)
-    d2h = sum((c["nkn"] + 2 * c["nel"] * c["nlv"]) * 4 for c in case_list)
+    d2h = sum(c["nkn"] * 4 for c in case_list)
     e2e_steps = min(a.steps, 200)
     barrier()
     torch.cuda.synchronize()
@@ -384,7 +381,7 @@ def main():
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "steps": e2e_steps,
-                "path": "shygpu_set_forcing + shygpu_run(1) + shygpu_get_state(znv, utlnv, vtlnv)"},
+                "path": "shygpu_set_forcing(wind) + shygpu_run(1) + shygpu_get_state(znv), every basin"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic},
