@@ -201,6 +201,15 @@ static int build_pattern(int nkn, int nel, const int *nv /*0-based*/, Pattern &P
 // ---------------------------------------------------------------------------
 // device allocation helpers
 // ---------------------------------------------------------------------------
+// a copy of v with `extra` trailing entries of value `fill`: slack for the
+// 16-byte rounded bulk copies of the staged zeta solver (rowptr, col)
+template <typename T>
+static std::vector<T> padded(const std::vector<T> &v, size_t extra, T fill) {
+  std::vector<T> r(v);
+  r.resize(v.size() + extra, fill);
+  return r;
+}
+
 struct Arena {
   std::vector<void *> ptrs;
   int64_t bytes = 0;
@@ -259,6 +268,7 @@ struct shygpu_model {
   // options
   int nsub = 2, use_graph = 1, max_outer = 12, sym = 1;
   int zvariant = 1;                  // 1: shared-memory zeta solver when it fits
+  int zstage = 0;                    // device-wide solver: 1 TMA-staged tiles when they fit
   int zforce_CL = 0, zforce_threads = 0;   // > 0: one launch class with this shape
   std::vector<ZetaClass> zcl;        // launch classes of the zeta solver
   cudaStream_t side[kMaxZetaClasses] = {};
@@ -309,7 +319,7 @@ static void free_zeta_plan(shygpu_model *m) {
     if (c.d_blist) cudaFree(c.d_blist);
     if (c.grid) {
       cudaFree((void *)c.gp.tile); cudaFree((void *)c.gp.btile); cudaFree((void *)c.gp.cslot);
-      cudaFree((void *)c.gp.cnslot); cudaFree((void *)c.gp.cowner);
+      cudaFree((void *)c.gp.cnslot); cudaFree((void *)c.gp.cowner); cudaFree((void *)c.gp.tnz);
       cudaFree(c.gp.partial); cudaFree(c.gp.ctr);
     }
   }
@@ -317,7 +327,7 @@ static void free_zeta_plan(shygpu_model *m) {
 }
 
 // The device-wide class: every basin in one cooperative launch.  Each
-// basin's rows are cut into tiles of kGridTileRows (the tile boundaries, and
+// basin's rows are cut into tiles of a fixed row count (the tile boundaries, and
 // so the reduction order, depend on the basin alone); tile t goes to CTA
 // t % G, so a basin's tiles sit on consecutive CTAs and the work left when
 // only a few basins still iterate spreads over many CTAs.  Returns SHY_EARG
@@ -329,21 +339,29 @@ static int upload_plan(T **dst, const std::vector<T> &h) {
   return SHY_OK;
 }
 
-static const int kGridTileRows = 1024;
-
 static int build_grid_class(shygpu_model *m) {
-  const int cap = zeta_grid_capacity();
-  if (cap < 1) return fail(SHY_ECUDA, "zeta grid solver: no resident CTA fits the device");
   const int MS = zeta_grid_max_slots();
   std::vector<int4> tile;
-  std::vector<int2> btile(m->nbasin, make_int2(0, 0));
+  std::vector<int2> btile(m->nbasin, make_int2(0, 0)), tnz;
+  int nzcap = 0;
+  const int TR = zeta_grid_tile_rows();
   for (int b = 0; b < m->nbasin; b++) {
     const BasinPar &bp = m->par[b];
     btile[b].x = (int)tile.size();
-    for (int r = 0; r < bp.nk; r += kGridTileRows)
-      tile.push_back(make_int4(bp.k0 + r, bp.k0 + std::min(bp.nk, r + kGridTileRows), b, 0));
+    for (int r = 0; r < bp.nk; r += TR) {
+      const int r0 = bp.k0 + r, r1 = bp.k0 + std::min(bp.nk, r + TR);
+      tile.push_back(make_int4(r0, r1, b, 0));
+      tnz.push_back(make_int2(m->rowptr_h[r0], m->rowptr_h[r1]));
+      nzcap = std::max(nzcap, m->rowptr_h[r1] - m->rowptr_h[r0]);
+    }
     btile[b].y = (int)tile.size();
   }
+  // the TMA-staged form when asked for and its two buffers fit one CTA per SM
+  bool staged = m->zstage != 0;
+  size_t smem = staged ? zeta_grid_stage_smem(nzcap) : 0;
+  int cap = staged ? zeta_grid_capacity(true, smem) : 0;
+  if (cap < 1) { staged = false; smem = 0; cap = zeta_grid_capacity(false, 0); }
+  if (cap < 1) return fail(SHY_ECUDA, "zeta grid solver: no resident CTA fits the device");
   const int T = (int)tile.size();
   const int G = std::max(1, std::min(cap, T));
   if ((T + G - 1) / G > zeta_grid_max_tiles())
@@ -365,6 +383,8 @@ static int build_grid_class(shygpu_model *m) {
   m->zcl.emplace_back();
   ZetaClass &c = m->zcl.back();
   c.grid = true;
+  c.staged = staged;
+  c.gsmem = smem;
   c.G = G;
   c.threads = 0;
   c.CL = 0;
@@ -376,6 +396,9 @@ static int build_grid_class(shygpu_model *m) {
   ST_TRY(upload_plan(&dcs, cslot)); c.gp.cslot = dcs;
   ST_TRY(upload_plan(&dcn, cnslot)); c.gp.cnslot = dcn;
   ST_TRY(upload_plan(&dco, cowner)); c.gp.cowner = dco;
+  int2 *dnz = nullptr;
+  ST_TRY(upload_plan(&dnz, tnz)); c.gp.tnz = dnz;
+  c.gp.nzcap = nzcap;
   CUDA_TRY(cudaMalloc(&c.gp.partial, sizeof(double) * 8 * std::max<size_t>(tile.size(), 1)));
   CUDA_TRY(cudaMalloc(&c.gp.ctr, 8 * sizeof(unsigned)));
   CUDA_TRY(cudaMemset(c.gp.ctr, 0, 8 * sizeof(unsigned)));
@@ -557,7 +580,7 @@ static int launch_zeta_plan(shygpu_model *m, const Dev &d, ZetaArgs za) {
     cudaStream_t st = nc > 1 ? m->side[i] : m->stream;
     if (nc > 1) CUDA_TRY(cudaStreamWaitEvent(st, m->ev_fork, 0));
     za.blist = c.d_blist;
-    cudaError_t e = c.grid ? launch_zeta_grid(d, za, c.gp, c.G, st)
+    cudaError_t e = c.grid ? launch_zeta_grid(d, za, c.gp, c.G, c.staged, c.gsmem, st)
                   : c.sm   ? launch_zeta_sm(d, za, c.zs, m->zm, (int)c.basins.size(), st)
                            : launch_zeta(d, za, c.CL, c.threads, (int)c.basins.size(), st);
     if (e != cudaSuccess) return fail(SHY_ECUDA, "zeta solve launch: %s", cudaGetErrorString(e));
@@ -848,7 +871,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       A.upload(&d.taux, taux) || A.upload(&d.tauy, tauy) || A.upload(&d.ppv, ppv) ||
       A.upload(&d.rqv, rqv) || A.upload(&d.hlv, hlv) || A.upload(&d.hldv, hldv) ||
       A.upload(&d.areakv, areakv) || A.upload(&d.avol, avol) ||
-      A.upload(&d.rowptr, rowptr) || A.upload(&d.col, col) ||
+      A.upload(&d.rowptr, padded(rowptr, 4, rowptr.back())) || A.upload(&d.col, padded(col, 4, 0)) ||
       A.upload(&d.slot_ptr, slot_ptr) || A.upload(&d.slot_src, slot_src) ||
       A.upload(&d.inc_ptr, inc_ptr) || A.upload(&d.inc, inc) || A.upload(&d.incx, incx) ||
       A.upload(&m->kbas, kbas))
@@ -856,11 +879,11 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   const size_t nnz = col.size(), EL = (size_t)NEL * NLV, NL = (size_t)NKN * NLV;
   const size_t NSC = (size_t)std::max(nsc_max, 1) * NL;
   if (A.alloc(&d.val64, nnz) || A.alloc(&d.rhs64, NKN) || A.alloc(&d.x64, NKN) ||
-      A.alloc(&d.val32, nnz) || A.alloc(&d.dinv32, NKN) || A.alloc(&d.r32, NKN) ||
+      A.alloc(&d.val32, nnz + 4) || A.alloc(&d.dinv32, NKN) || A.alloc(&d.r32, NKN) ||
       A.alloc(&d.p32, NKN) || A.alloc(&d.q32, NKN) || A.alloc(&d.z32, NKN) ||
       A.alloc(&d.e32, NKN) || A.alloc(&d.s32, NKN) || A.alloc(&d.t32, NKN) ||
       A.alloc(&d.rh32, NKN) || A.alloc(&d.v32, NKN) || A.alloc(&d.cg4[0], NKN) ||
-      A.alloc(&d.cg4[1], NKN) || A.alloc(&d.cg2, NKN) || A.alloc(&d.hia, (size_t)9 * NEL) ||
+      A.alloc(&d.cg4[1], NKN) || A.alloc(&d.cg2, NKN + 2) || A.alloc(&d.hia, (size_t)9 * NEL) ||
       A.alloc(&d.hik, (size_t)3 * NEL) || A.alloc(&d.unv, NEL) || A.alloc(&d.vnv, NEL) ||
       A.alloc(&d.usv, EL) || A.alloc(&d.vsv, EL) ||
       A.alloc(&d.wl, (size_t)NKN * (NLV + 1)) || A.alloc(&d.rho, NL) || A.alloc(&d.ddx, EL) ||
@@ -929,6 +952,10 @@ extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value
     m->zvariant = iv;
     ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
   }
+  else if (n == "zeta_stage") {   // device-wide solver: 1 TMA-staged tiles, 0 global loads
+    m->zstage = iv != 0;
+    ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
+  }
   else if (n == "column_threads") {   // 1: one thread per column when it has at most 16 layers
     m->base.col_threads = iv != 0;
   }
@@ -957,6 +984,7 @@ extern "C" double shygpu_get_option(shygpu_model *m, const char *name) {
   if (n == "symmetric") return m->sym;
   if (n == "zeta_variant") return m->zcl.empty() ? -1 : (m->zcl[0].grid ? 2 : (m->zcl[0].sm ? 1 : 0));
   if (n == "zeta_grid_ctas") return m->zcl.empty() ? -1 : m->zcl[0].G;
+  if (n == "zeta_stage") return m->zcl.empty() || !m->zcl[0].grid ? m->zstage : (m->zcl[0].staged ? 1 : 0);
   if (n == "launches_per_step") return m->launches_per_step;
   return -1;
 }

@@ -36,9 +36,10 @@
 
 namespace shy {
 
-constexpr int kGridThreads = 512;
-constexpr int kGridMaxSlots = kGridThreads / 32; // basins per CTA (one warp reduces each)
+constexpr int kGridMaxSlots = 32;                // basins per CTA
 constexpr int kGridMaxTiles = 32;                // tiles per CTA
+constexpr int kGridTileRows = 1024;              // rows per tile
+constexpr long long kMbarSpinLimit = 1LL << 22;  // try_wait polls before a staged copy counts as lost
 constexpr long long kGridSpinLimit = 1LL << 24;  // ~ seconds with the back-off below
 constexpr int kGridPartialUnroll = 8;           // partial sums a lane loads at once
 
@@ -152,6 +153,80 @@ __device__ __forceinline__ double grid_resid_row(const Dev &d, int i) {
   return t;
 }
 
+// ---------------------------------------------------------------------------
+// TMA staging of a tile (the staged form): one bulk copy each of the tile's
+// row pointers, its CSR column indices and FP32 values, its {r, w, s, 1/diag}
+// rows and its {p, e} rows into a shared-memory buffer, completing on that
+// buffer's mbarrier.  Every copy starts 16-byte aligned (ranges rounded out
+// to 16 bytes; the arrays carry the slack) and moves a multiple of 16 bytes.
+// ---------------------------------------------------------------------------
+struct StageLayout {   // byte offsets inside one buffer
+  int row, col, val, q4, pe, bytes;
+};
+
+__host__ __device__ inline StageLayout stage_layout(int nzcap) {
+  StageLayout L;
+  L.row = 0;
+  L.col = L.row + (kGridTileRows + 8) * 4;
+  const int cb = ((nzcap + 8) * 4 + 15) & ~15;
+  L.val = L.col + cb;
+  L.q4 = L.val + cb;
+  L.pe = L.q4 + kGridTileRows * 16;
+  L.bytes = (L.pe + (kGridTileRows + 2) * 8 + 127) & ~127;
+  return L;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, int bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
+// thread 0: copy tile rows [a,e), entries [nz0,nz1) into the buffer at sbuf
+__device__ __forceinline__ void stage_issue(const Dev &d, const StageLayout &L, uint32_t sbuf, uint32_t mbar,
+                                            int a, int e, int nz0, int nz1, const float4 *qg) {
+  const int ra = a & ~3, rc = ((e + 1 - ra) + 3) & ~3;
+  const int ca = nz0 & ~3, cc = ((nz1 - ca) + 3) & ~3;
+  const int pa = a & ~1, pc = ((e - pa) + 1) & ~1;
+  const int bytes = rc * 4 + 2 * cc * 4 + (e - a) * 16 + pc * 8;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+  bulk_g2s(sbuf + L.row, d.rowptr + ra, rc * 4, mbar);
+  bulk_g2s(sbuf + L.col, d.col + ca, cc * 4, mbar);
+  bulk_g2s(sbuf + L.val, d.val32 + ca, cc * 4, mbar);
+  bulk_g2s(sbuf + L.q4, qg + a, (e - a) * 16, mbar);
+  bulk_g2s(sbuf + L.pe, d.cg2 + pa, pc * 8, mbar);
+}
+
+// bounded wait for an mbarrier phase; false when it did not complete
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long long it = 0; it < kMbarSpinLimit; it++) {
+    uint32_t done;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                 " selp.u32 %0, 1, 0, p;\n}" : "=r"(done) : "r"(mbar), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// A u' for one row from a staged tile: entries, and u' of rows inside the
+// tile, from shared memory; u' of rows outside it from global memory
+__device__ __forceinline__ float staged_spmv_row(const int *scol, const float *sval, int s0, int s1,
+                                                 const float4 *sq, int a, int R, const float4 *qg,
+                                                 float fa, float fb) {
+  float w = 0.f;
+  for (int m = s0; m < s1; m++) {
+    const int c = scol[m];
+    const float4 x = (unsigned)(c - a) < (unsigned)R ? sq[c - a] : qg[c];
+    float sn, rn;
+    w += sval[m] * cg_unext(x, fa, fb, sn, rn);
+  }
+  return w;
+}
+
 // the stage decision of one basin after the sums tot of its partials (the
 // same inputs, so the same decision, in every CTA holding a tile of it)
 __device__ __forceinline__ void grid_transition(GridState &g, const double (&tot)[3], const Dev &d,
@@ -199,17 +274,36 @@ __device__ __forceinline__ void grid_transition(GridState &g, const double (&tot
   }
 }
 
-__global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs za, GridPlan gp) {
+// NT threads per CTA.  STAGED: the CG products read each tile's data from
+// TMA-staged shared memory (two buffers, the next tile's copy in flight
+// while one is worked; one CTA of 1024 threads per SM); otherwise straight
+// from global memory (two CTAs of 512 threads per SM).
+template <int NT, bool STAGED>
+__global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArgs za, GridPlan gp) {
+  constexpr int NW = NT / 32;
   __shared__ GridState gs[kGridMaxSlots];
   __shared__ int4 s_tile[kGridMaxTiles];
-  __shared__ double wred[kGridMaxTiles * (kGridThreads / 32) * 3];
+  __shared__ int2 s_tnz[STAGED ? kGridMaxTiles : 1];
+  __shared__ double wred[kGridMaxTiles * NW * 3];
   __shared__ int s_ok;
   __shared__ unsigned s_act;
+  extern __shared__ __align__(128) unsigned char dsm[];
   const int tid = threadIdx.x, nth = blockDim.x;
   const int c = blockIdx.x, G = gridDim.x;
   const int nslot = gp.cnslot[c];
   const int ntl = (gp.ntile - c + G - 1) / G;      // this CTA's tiles: c, c+G, c+2G, ...
   unsigned bar = 0;
+  const StageLayout SL = stage_layout(gp.nzcap);
+  uint32_t mbar[2] = {0u, 0u}, sbuf[2] = {0u, 0u}, phase[2] = {0u, 0u};
+  if (STAGED) {
+    mbar[0] = smem_u32(dsm); mbar[1] = mbar[0] + 8;
+    sbuf[0] = smem_u32(dsm + 128); sbuf[1] = sbuf[0] + SL.bytes;
+    if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar[0]) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar[1]) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+  }
 
   if (tid < nslot) {
     GridState &g = gs[tid];
@@ -218,7 +312,10 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
     g.owner = (gp.cowner[c] >> tid) & 1;
     g.tol = g.itol2 = g.rn = g.resid0 = g.alpha = g.beta = g.gamma = 0.;
   }
-  if (tid < ntl) s_tile[tid] = gp.tile[c + tid * G];
+  if (tid < ntl) {
+    s_tile[tid] = gp.tile[c + tid * G];
+    if constexpr (STAGED) s_tnz[tid] = gp.tnz[c + tid * G];
+  }
   if (blockIdx.x == 0 && tid == 0 && d.imax) { *d.imax = 0; *d.subj = 0; }
   __syncthreads();
 
@@ -244,18 +341,89 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
     }
     return;
   }
+  if (STAGED) asm volatile("fence.proxy.async.global;" ::: "memory");
   if (!grid_barrier(gp.ctr, ++bar, &s_ok, 0, nullptr)) goto aborted;
 
   for (unsigned k = 0;; k++) {
     const int par = (int)(k & 1u);
     // ---- the work of each tile's stage ----
+    int iq = 0;                                     // thread 0: next tile to stage
+    auto staged_stage = [&](int st) { return STAGED && (st == G_SPMV0 || st == G_ITER); };
+    auto issue_next = [&](int b) {                  // thread 0 only
+      while (iq < ntl && !staged_stage(gs[s_tile[iq].w].stage)) iq++;
+      if (iq < ntl) {
+        const int4 tl = s_tile[iq];
+        const int2 nz = s_tnz[iq];
+        stage_issue(d, SL, sbuf[b], mbar[b], tl.x, tl.y, nz.x, nz.y, d.cg4[gs[tl.w].cur]);
+        iq++;
+      }
+    };
+    if (STAGED && tid == 0) {
+      asm volatile("fence.proxy.async.global;" ::: "memory");
+      issue_next(0);
+      issue_next(1);
+    }
+    int js = 0;                                     // staged tiles worked so far
     for (int q = 0; q < ntl; q++) {
       const int4 tl = s_tile[q];
       const int a = tl.x, e = tl.y;
       GridState &g = gs[tl.w];
       const int stage = g.stage;
       double v[3] = {0., 0., 0.};
-      if (stage == G_RES) {
+      if (staged_stage(stage)) {
+        const int b = js & 1;
+        if (tid == 0) s_ok = mbar_wait(mbar[b], phase[b]) ? 1 : 0;
+        __syncthreads();
+        if (!s_ok) {
+          if (tid == 0) {
+            atomicExch(gp.ctr + 4, 1u);
+            mbar_wait(mbar[b], phase[b]);           // let the copies in flight land
+            mbar_wait(mbar[b ^ 1], phase[b ^ 1]);
+          }
+          __syncthreads();
+          goto aborted;
+        }
+        phase[b] ^= 1u;
+        const unsigned char *buf = dsm + 128 + (size_t)b * SL.bytes;
+        const int2 nz = s_tnz[q];
+        const int *srow = reinterpret_cast<const int *>(buf + SL.row) + (a - (a & ~3));
+        const int *scol = reinterpret_cast<const int *>(buf + SL.col) + (nz.x - (nz.x & ~3));
+        const float *sval = reinterpret_cast<const float *>(buf + SL.val) + (nz.x - (nz.x & ~3));
+        const float4 *sq = reinterpret_cast<const float4 *>(buf + SL.q4);
+        const float2 *spe = reinterpret_cast<const float2 *>(buf + SL.pe) + (a - (a & ~1));
+        const float4 *qi = d.cg4[g.cur];
+        float4 *qo = d.cg4[g.cur ^ 1];
+        const int R = e - a;
+        const float fa = stage == G_ITER ? (float)g.alpha : 0.f;
+        const float fb = stage == G_ITER ? (float)g.beta : 0.f;
+        for (int j = tid; j < R; j += nth) {
+          const int i = a + j;
+          const float4 me = sq[j];
+          const float w = staged_spmv_row(scol, sval, srow[j] - nz.x, srow[j + 1] - nz.x, sq, a, R, qi, fa, fb);
+          if (stage == G_SPMV0) {
+            // w = A u with u = r/diag (fa = 0 and s = 0 leave r, so u = r/diag)
+            const float u = me.w * me.x;
+            qo[i] = make_float4(me.x, w, 0.f, me.w);
+            v[0] += (double)me.x * u;
+            v[1] += (double)w * u;
+            v[2] += (double)me.x * me.x;
+          } else {
+            // p = u + b p, s = w + b s, e += a p, r -= a s, u = r/diag, w = A u
+            const float2 pe = spe[j];
+            const float p = me.w * me.x + fb * pe.x;
+            float sn, rn;
+            const float u = cg_unext(me, fa, fb, sn, rn);
+            qo[i] = make_float4(rn, w, sn, me.w);
+            d.cg2[i] = make_float2(p, pe.y + fa * p);
+            v[0] += (double)rn * u;
+            v[1] += (double)w * u;
+            v[2] += (double)rn * rn;
+          }
+        }
+        __syncthreads();                            // buffer b read by every thread
+        if (tid == 0) issue_next(b);
+        js++;
+      } else if (stage == G_RES) {
         float4 *qo = d.cg4[g.cur];
         for (int i = a + tid; i < e; i += nth) {
           const double t = grid_resid_row(d, i);
@@ -311,22 +479,22 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
           for (int o = 16; o > 0; o >>= 1) v[cc] += __shfl_xor_sync(0xffffffffu, v[cc], o);
         }
         if ((tid & 31) == 0) {
-          double *w = wred + ((size_t)q * (kGridThreads / 32) + (tid >> 5)) * 3;
+          double *w = wred + ((size_t)q * NW + (tid >> 5)) * 3;
           w[0] = v[0]; w[1] = v[1]; w[2] = v[2];
         }
       }
     }
     __syncthreads();
-    // tile partials: warp w sums the warp sums of tiles w, w+16, ... in a fixed tree
+    // tile partials: warp w sums the warp sums of tiles w, w+NW, ... in a fixed tree
     {
       const int warp = tid >> 5, lane = tid & 31;
-      for (int q = warp; q < ntl; q += kGridThreads / 32) {
+      for (int q = warp; q < ntl; q += NW) {
         const int stage = gs[s_tile[q].w].stage;
         if (stage != G_RES && stage != G_SPMV0 && stage != G_ITER) continue;
         double x[3];
 #pragma unroll
         for (int cc = 0; cc < 3; cc++) {
-          x[cc] = lane < kGridThreads / 32 ? wred[((size_t)q * (kGridThreads / 32) + lane) * 3 + cc] : 0.;
+          x[cc] = lane < NW ? wred[((size_t)q * NW + lane) * 3 + cc] : 0.;
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) x[cc] += __shfl_xor_sync(0xffffffffu, x[cc], o);
         }
@@ -358,13 +526,15 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
       if (nact) atomicAdd(gp.ctr + 1 + k % 3, nact);
       if (blockIdx.x == 0) gp.ctr[1 + (k + 1) % 3] = 0u;   // the counter of super-step k+3
     }
+    // the next super-step may read these writes through the async proxy
+    if (STAGED) asm volatile("fence.proxy.async.global;" ::: "memory");
     if (!grid_barrier(gp.ctr, ++bar, &s_ok, 1 + k % 3, &s_act)) goto aborted;
     if (s_act == 0u) break;
     // ---- per-basin sums over its tiles, the same in every CTA; next stage ----
-    {
-      const int warp = tid >> 5, lane = tid & 31;
-      if (warp < nslot) {
-        GridState &g = gs[warp];
+    for (int sl = tid >> 5; sl < nslot; sl += NW) {
+      const int lane = tid & 31;
+      {
+        GridState &g = gs[sl];
         const int st = g.stage;
         if (st == G_RES || st == G_SPMV0 || st == G_ITER) {
           const int2 bt = gp.btile[g.basin];
@@ -374,8 +544,8 @@ __global__ void __launch_bounds__(kGridThreads, 2) k_zeta_grid(Dev d, ZetaArgs z
             double pv[kGridPartialUnroll][3];
 #pragma unroll
             for (int u = 0; u < kGridPartialUnroll; u++) {
-              const int s = s0 + u * 32 + lane;
-              const double *pp = gp.partial + ((size_t)par * gp.ntile + (s < bt.y ? s : bt.x)) * 4;
+              const int sx = s0 + u * 32 + lane;
+              const double *pp = gp.partial + ((size_t)par * gp.ntile + (sx < bt.y ? sx : bt.x)) * 4;
               pv[u][0] = __ldcg(pp + 0); pv[u][1] = __ldcg(pp + 1); pv[u][2] = __ldcg(pp + 2);
             }
 #pragma unroll

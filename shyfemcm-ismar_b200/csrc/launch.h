@@ -54,6 +54,8 @@ struct GridPlan {
   const int4 *tile = nullptr;
   const int2 *btile = nullptr;
   const int *cslot = nullptr, *cnslot = nullptr, *cowner = nullptr;
+  const int2 *tnz = nullptr;       // per tile: its CSR entries rowptr[row0] .. rowptr[row1]
+  int nzcap = 0;                   // most CSR entries of any tile (staged buffer size)
   double *partial = nullptr;       // [2][ntile][4] partial sums of the tiles
   unsigned *ctr = nullptr;         // [8]: barrier arrivals, 3 active counts, abort flag, release
 };
@@ -61,7 +63,9 @@ struct GridPlan {
 // a group of basins solved by one launch with one cluster shape
 struct ZetaClass {
   bool grid = false;               // device-wide cooperative variant (all basins, one launch)
+  bool staged = false;             // its TMA-staged form
   int G = 0;                       // its CTAs
+  size_t gsmem = 0;                // its dynamic shared memory
   GridPlan gp;
   bool sm = false;                 // shared-memory variant (else global memory)
   int CL = 1, threads = 512;
@@ -74,12 +78,17 @@ struct ZetaClass {
 cudaError_t launch_zeta(const Dev &d, const ZetaArgs &za, int CL, int threads, int nb, cudaStream_t st);
 cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs, const ZetaMaps &zm,
                            int nb, cudaStream_t st);
-// the device-wide variant: G CTAs of kGridThreads, cooperative; clears gp.ctr first
-cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &gp, int G, cudaStream_t st);
+// the device-wide variant: G CTAs, cooperative; clears gp.ctr first.  staged:
+// the TMA-staged form with `smem` bytes of dynamic shared memory
+cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &gp, int G, bool staged,
+                             size_t smem, cudaStream_t st);
 // CTAs of k_zeta_grid that fit the device at once (0 on error)
-int zeta_grid_capacity();
+int zeta_grid_capacity(bool staged, size_t smem);
+// dynamic shared memory of the staged form for tiles of at most nzcap entries
+size_t zeta_grid_stage_smem(int nzcap);
 int zeta_grid_max_slots();   // basins one CTA can hold
 int zeta_grid_max_tiles();   // tiles one CTA can hold
+int zeta_grid_tile_rows();   // rows per tile
 // smem > 0 prepares the shared-memory variant for that many dynamic bytes
 cudaError_t zeta_kernel_setup(int CL, size_t smem);
 int zeta_max_active_clusters(int CL, int threads, size_t smem);

@@ -171,31 +171,47 @@ cudaError_t launch_zeta_sm(const Dev &d, const ZetaArgs &za, const ZetaShape &zs
   return cudaLaunchKernelEx(&cfg, k_zeta_sm, d, za, zs, zm);
 }
 
-cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &gp, int G, cudaStream_t st) {
+cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &gp, int G, bool staged,
+                             size_t smem, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(gp.ctr, 0, 8 * sizeof(unsigned), st);
   if (e != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
   cudaLaunchAttribute attr[1];
   cfg.gridDim = dim3(G, 1, 1);
-  cfg.blockDim = dim3(kGridThreads, 1, 1);
+  cfg.blockDim = dim3(staged ? 1024 : 512, 1, 1);
+  cfg.dynamicSmemBytes = staged ? smem : 0;
   cfg.stream = st;
   attr[0].id = cudaLaunchAttributeCooperative;
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_zeta_grid, d, za, gp);
+  if (staged) return cudaLaunchKernelEx(&cfg, k_zeta_grid<1024, true>, d, za, gp);
+  return cudaLaunchKernelEx(&cfg, k_zeta_grid<512, false>, d, za, gp);
 }
 
-int zeta_grid_capacity() {
+size_t zeta_grid_stage_smem(int nzcap) { return 128 + 2 * (size_t)stage_layout(nzcap).bytes; }
+
+int zeta_grid_capacity(bool staged, size_t smem) {
   int dev = 0, nsm = 0, nb = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_zeta_grid, kGridThreads, 0) != cudaSuccess) return 0;
+  if (staged) {
+    if (cudaFuncSetAttribute(k_zeta_grid<1024, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_zeta_grid<1024, true>, 1024, smem) != cudaSuccess)
+      return 0;
+  } else if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_zeta_grid<512, false>, 512, 0) != cudaSuccess) {
+    return 0;
+  }
   return nb * nsm;
 }
 
 int zeta_grid_max_slots() { return kGridMaxSlots; }
 int zeta_grid_max_tiles() { return kGridMaxTiles; }
+int zeta_grid_tile_rows() { return kGridTileRows; }
 
 cudaError_t zeta_kernel_setup(int CL, size_t smem) {
   cudaError_t e = cudaSuccess;

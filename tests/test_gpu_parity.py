@@ -146,11 +146,14 @@ def test_transport_substeps():
             assert rel <= TRACER_RTOL, (use_graph, f, rel)
 
 
-def test_device_wide_zeta_solver(small3d):
-    """The cooperative device-wide zeta solver (the one large basins use)
-    against the oracle on the config-2-shaped test basin."""
-    g, o = run_both(small3d, 120, zeta_variant=2)
+@pytest.mark.parametrize("zeta_stage", [1, 0])
+def test_device_wide_zeta_solver(small3d, zeta_stage):
+    """The cooperative device-wide zeta solver (the one large basins use),
+    with its tiles staged into shared memory by TMA bulk copies and with
+    plain global loads, against the oracle on the config-2-shaped basin."""
+    g, o = run_both(small3d, 120, zeta_variant=2, zeta_stage=zeta_stage)
     assert g.get_option("zeta_variant") == 2
+    assert g.get_option("zeta_stage") == zeta_stage
     sg, so = g.get_state(0), o.state()
     assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
     m = active_mask(small3d)
