@@ -263,6 +263,42 @@ int shygpu_csr_solve_static(int32_t n, int32_t nnz, const int32_t *rowptr,
                             int32_t symmetric, void *stream,
                             int32_t *iterations);
 
+/* ------------------------------------------------------------------ */
+/* Serving: a continuous-batching request loop (no counterpart in the   */
+/* reference, which runs one simulation per process).  A request is a   */
+/* basin, its parameters, its initial state and a step count; it is     */
+/* admitted in arrival order once a slot is free and its footprint      */
+/* (shygpu_footprint) fits the rest of the HBM budget, then runs with   */
+/* its state resident on the device, concurrently with the other runs,  */
+/* in quanta of `quantum_steps` CUDA-graph steps.  Inputs are copied at */
+/* submit; results (znv, utlnv, vtlnv and the transported scalars) are  */
+/* copied to host memory when the run finishes.  One host thread at a  */
+/* time drives a server.                                                */
+/* ------------------------------------------------------------------ */
+typedef struct shygpu_server shygpu_server;
+enum { SHY_REQ_QUEUED = 0, SHY_REQ_ACTIVE = 1, SHY_REQ_DONE = 2, SHY_REQ_FAILED = 3 };
+int shygpu_serve_create(int64_t hbm_budget_bytes, int32_t max_active,
+                        int32_t quantum_steps, shygpu_server **server);
+int shygpu_serve_submit(shygpu_server *server, const shy_basin *basin,
+                        const shy_params *params, const shy_state *initial,
+                        int32_t nsteps, int64_t *request_id);
+/* Retire finished runs, launch the next quantum of every run whose last
+ * one has finished, admit queued requests.  block != 0 first waits for
+ * the oldest quantum in flight.  Counts of active, queued and newly
+ * finished requests are returned through the (optional) pointers.       */
+int shygpu_serve_progress(shygpu_server *server, int32_t block,
+                          int32_t *n_active, int32_t *n_queued,
+                          int32_t *n_finished);
+/* state SHY_REQ_*; times in seconds since the server was created        */
+int shygpu_serve_status(shygpu_server *server, int64_t request_id,
+                        int32_t *state, int32_t *steps_enqueued,
+                        double *t_submit, double *t_admit, double *t_done);
+int shygpu_serve_result(shygpu_server *server, int64_t request_id,
+                        shy_state *out, shy_step_info *info);
+int shygpu_serve_release(shygpu_server *server, int64_t request_id);
+int64_t shygpu_serve_used(shygpu_server *server);   /* admitted footprint */
+int shygpu_serve_destroy(shygpu_server *server);
+
 void system_initialize_(void);                      /* :85   */
 void system_init_(void);                            /* :137  */
 void system_set_explicit_(void);                    /* :160  */

@@ -84,6 +84,17 @@ def lib():
     L.shygpu_model_stream.argtypes = [C.c_void_p]
     L.shygpu_model_stream.restype = C.c_void_p
     L.shygpu_profile_steps.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_int32)]
+    L.shygpu_serve_create.argtypes = [C.c_int64, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    L.shygpu_serve_submit.argtypes = [C.c_void_p, C.POINTER(abi.ShyBasin), C.POINTER(abi.ShyParams),
+                                      C.POINTER(abi.ShyState), C.c_int32, C.POINTER(C.c_int64)]
+    L.shygpu_serve_progress.argtypes = [C.c_void_p, C.c_int32] + [C.POINTER(C.c_int32)] * 3
+    L.shygpu_serve_status.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_int32), C.POINTER(C.c_int32)] + \
+        [C.POINTER(C.c_double)] * 3
+    L.shygpu_serve_result.argtypes = [C.c_void_p, C.c_int64, C.POINTER(abi.ShyState), C.POINTER(abi.ShyStepInfo)]
+    L.shygpu_serve_release.argtypes = [C.c_void_p, C.c_int64]
+    L.shygpu_serve_used.argtypes = [C.c_void_p]
+    L.shygpu_serve_used.restype = C.c_int64
+    L.shygpu_serve_destroy.argtypes = [C.c_void_p]
     _lib = L
     return L
 
@@ -190,6 +201,76 @@ class Model:
     def close(self):
         if not self._closed and getattr(self, "h", None):
             lib().shygpu_destroy(self.h)
+            self._closed = True
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request loop (shygpu_serve_*): forecast runs are
+    admitted by HBM footprint, run concurrently with their state resident
+    on the device, and return their final state."""
+
+    QUEUED, ACTIVE, DONE, FAILED = 0, 1, 2, 3
+
+    def __init__(self, hbm_budget, max_active=8, quantum_steps=60):
+        h = C.c_void_p()
+        check(lib().shygpu_serve_create(int(hbm_budget), int(max_active), int(quantum_steps), C.byref(h)),
+              "serve_create")
+        self.h = h
+        self._cases = {}
+        self._closed = False
+
+    def submit(self, case, nsteps, **param_over):
+        """Queue a run of `nsteps` steps from the case's initial state."""
+        args = abi.BasinArgs(case)
+        params = abi.make_params(case, **param_over)
+        buf = abi.StateBuffers(case, fill_from_case=True)
+        st = buf.struct(only=("znv", "utlnv", "vtlnv", "tempv", "saltv", "conzv"))
+        rid = C.c_int64()
+        check(lib().shygpu_serve_submit(self.h, C.byref(args.struct), C.byref(params), C.byref(st),
+                                        int(nsteps), C.byref(rid)), "serve_submit")
+        self._cases[rid.value] = case
+        return rid.value
+
+    def progress(self, block=False):
+        """One pass of the loop; returns (active, queued, finished now)."""
+        a, q, f = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().shygpu_serve_progress(self.h, 1 if block else 0, C.byref(a), C.byref(q), C.byref(f)),
+              "serve_progress")
+        return a.value, q.value, f.value
+
+    def status(self, rid):
+        """(state, steps enqueued, t_submit, t_admit, t_done) in seconds."""
+        st, n = C.c_int32(), C.c_int32()
+        ts, ta, td = C.c_double(), C.c_double(), C.c_double()
+        check(lib().shygpu_serve_status(self.h, rid, C.byref(st), C.byref(n), C.byref(ts), C.byref(ta),
+                                        C.byref(td)), "serve_status")
+        return st.value, n.value, ts.value, ta.value, td.value
+
+    def result(self, rid, release=True):
+        """Final state arrays (znv, utlnv, vtlnv and the scalars) and info."""
+        case = self._cases[rid]
+        buf = abi.StateBuffers(case)
+        st = buf.struct(only=("znv", "utlnv", "vtlnv", "tempv", "saltv", "conzv"))
+        info = abi.ShyStepInfo()
+        check(lib().shygpu_serve_result(self.h, rid, C.byref(st), C.byref(info)), "serve_result")
+        if release:
+            check(lib().shygpu_serve_release(self.h, rid), "serve_release")
+            del self._cases[rid]
+        out = {k: buf.arrays[k] for k in ("znv", "utlnv", "vtlnv", "tempv", "saltv", "conzv")}
+        return out, info
+
+    def used(self):
+        return lib().shygpu_serve_used(self.h)
+
+    def close(self):
+        if not self._closed and getattr(self, "h", None):
+            lib().shygpu_serve_destroy(self.h)
             self._closed = True
 
     def __del__(self):
