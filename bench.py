@@ -50,7 +50,9 @@ def parse():
     p.add_argument("--steps", type=int, default=400)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="shygpu", choices=["shygpu", "reference"])
-    p.add_argument("--workload", default="ensemble", choices=["ensemble", "basin3d"])
+    p.add_argument("--workload", default="ensemble", choices=["ensemble", "basin3d", "serve"])
+    p.add_argument("--serve-requests", type=int, default=30,
+                   help="serve workload: requests of the Poisson stream (20/min)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     return p.parse_args()
@@ -60,6 +62,8 @@ def make_cases(workload, rank=0, first=None):
     from shygpu import cases
     if workload == "basin3d":
         return [cases.basin3d_case(nkn_target=20000, seed=2 + 1000 * rank)]
+    if workload == "serve":
+        return [c for _, c, _ in cases.serve_requests(first or 30, seed=5 + 1000 * rank)]
     return cases.ensemble_cases(64, seed=4 + 1000 * rank, first=first)
 
 
@@ -248,12 +252,139 @@ def run_reference(a):
 
 
 # ---------------------------------------------------------------------------
+# the serving workload: a Poisson stream of forecast requests
+# ---------------------------------------------------------------------------
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(math.ceil(q / 100.0 * len(xs))) - 1))
+    return xs[k]
+
+
+def run_serve(a):
+    """Requests arrive at their (seeded) Poisson times in wall-clock time and
+    are served by shygpu.Server; latency = finish - submit on the server's
+    clock.  Beside it the plain path: one run at a time in arrival order,
+    each run's service time measured alone (create + set_state + steps) on
+    a 288-step sample scaled to its horizon, queued FIFO on the same
+    arrival times."""
+    import torch
+    import shygpu
+    from shygpu import cases
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    os.environ.setdefault("SHYGPU_NO_BUILD", "1")
+    reqs = cases.serve_requests(a.serve_requests, seed=5 + 1000 * rank)
+    lib = shygpu.lib()
+    # warm the library and the CUDA context on a small run
+    w = shygpu.Model(cases.channel_case())
+    w.set_state(0)
+    w.run(3)
+    w.close()
+    free, _ = torch.cuda.mem_get_info()
+    srv = shygpu.Server(int(0.8 * free), max_active=16, quantum_steps=60)
+    sampler = ClockSampler(local)
+    launches0 = lib.shygpu_launch_count()
+    pending = list(reqs)
+    ids = []
+    t_wall0 = time.time()
+    t0 = time.perf_counter()
+    while True:
+        now = time.perf_counter() - t0
+        while pending and pending[0][0] <= now:
+            arr, c, n = pending.pop(0)
+            ids.append((srv.submit(c, n), c, n, arr))
+        act, queued, _ = srv.progress(block=False)
+        if not pending and act == 0 and queued == 0:
+            break
+        if act == 0 and queued == 0:
+            time.sleep(min(0.01, max(0.0, pending[0][0] - now)))
+        else:
+            time.sleep(0.0005)
+    t_wall1 = time.time()
+    clocks = sampler.summary(t_wall0, t_wall1)
+    launches = lib.shygpu_launch_count() - launches0
+    lat, units, t_first, t_last, failed = [], 0, None, None, 0
+    for rid, c, n, arr in ids:
+        st, steps, ts, ta, td = srv.status(rid)
+        if st != shygpu.Server.DONE:
+            failed += 1
+            continue
+        lat.append(td - ts)
+        units += c["nkn"] * c["nlv"] * n
+        t_first = ts if t_first is None else min(t_first, ts)
+        t_last = td if t_last is None else max(t_last, td)
+        srv.result(rid)
+    srv.close()
+    span = t_last - t_first
+    value = units / span
+    # plain path: each run alone, FIFO on the same arrival times
+    service = []
+    for arr, c, n in reqs:
+        t_c = time.perf_counter()
+        m = shygpu.Model(c)
+        m.set_state(0)
+        torch.cuda.synchronize()
+        t_create = time.perf_counter() - t_c
+        m.run(3)
+        st = torch.cuda.ExternalStream(m.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st):
+            e0.record(st)
+            lib.shygpu_enqueue(m.h, 288)
+            e1.record(st)
+        torch.cuda.synchronize()
+        shygpu.check(lib.shygpu_sync(m.h), "plain run")
+        service.append(t_create + e0.elapsed_time(e1) / 1000.0 * n / 288.0)
+        m.close()
+    finish, plain_lat = 0.0, []
+    for (arr, c, n), sv in zip(reqs, service):
+        finish = max(arr, finish) + sv
+        plain_lat.append(finish - arr)
+    plain_value = units / (finish - reqs[0][0])
+    h2d = sum(c["nkn"] * 4 + 2 * c["nel"] * c["nlv"] * 4 for _, c, _ in reqs)
+    d2h = h2d
+    steps_total = sum(n for _, _, n in reqs)
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world,
+        "steps": steps_total, "warmup": 3, "ms_per_step": 1000.0 * span / steps_total,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "serve_poisson_20_per_min", "requests": len(reqs),
+                   "nkn_range": [2000, 200000], "nlv": 10, "horizon_steps": 2880, "dt_s": 60.0,
+                   "admission": "HBM footprint, 80% of free memory, 16 slots, 60-step quanta",
+                   "l2": "inputs larger than L2", "parallelism": f"replicas{world}"},
+        "latency_s": {"p50": pct(lat, 50), "p99": pct(lat, 99), "max": max(lat) if lat else None},
+        "failed": failed,
+        "plain_gpu": {"value": plain_value, "unit": METRIC,
+                      "latency_s": {"p50": pct(plain_lat, 50), "p99": pct(plain_lat, 99)},
+                      "form": "one run at a time in arrival order; service time measured alone "
+                              "(create + set_state + 288 steps, scaled to the horizon)"},
+        "served_over_plain": value / plain_value,
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": h2d / steps_total,
+                "d2h_bytes_per_step": d2h / steps_total,
+                "path": "shygpu_serve_submit + shygpu_serve_progress + shygpu_serve_result (host arrays in and out)"},
+        "roofline": None,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # the GPU arm
 # ---------------------------------------------------------------------------
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+        return
+    if a.workload == "serve":
+        run_serve(a)
         return
     import torch
     import torch.distributed as dist

@@ -225,3 +225,29 @@ def ensemble_cases(n, nkn_lo=5000, nkn_hi=100000, nlv=10, seed=4, dt=60.0, first
                          baroclinic=False, ts=False)
         out.append(c)
     return out
+
+
+def serve_requests(n, rate_per_min=20.0, nkn_lo=2000, nkn_hi=200000, nlv=10, seed=5, dt=60.0,
+                   horizon_steps=2880):
+    """A forecast request stream: Poisson arrivals at `rate_per_min`, basins
+    with log-uniform node counts, 10 z-layers, a 48 h horizon at dt = 60 s,
+    and per-request seeded M2 boundary tides (amplitude 0.1..0.5 m, random
+    phase) and winds (10 m/s, sigma 3 m/s).  Aspect ratios 1.5..3 keep the
+    largest basins well short of quarter-wave resonance with M2, so the
+    2 m surface layer stays wet over the horizon.  Returns [(arrival_s,
+    case, nsteps)]."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for m in range(n):
+        t += rng.exponential(60.0 / rate_per_min)
+        nk = int(math.exp(rng.uniform(math.log(nkn_lo), math.log(nkn_hi))))
+        aspect = rng.uniform(1.5, 3.0)
+        ly = 2.0e3 * math.sqrt(nk / 793.0)
+        c = basin3d_case(nkn_target=nk, lx=aspect * ly, ly=ly, seed=seed * 1000 + m, dt=dt, nlv=nlv,
+                         ampli=float(rng.uniform(0.1, 0.5)), wind=10.0 + 3.0 * rng.standard_normal(),
+                         baroclinic=False, ts=False)
+        c["tide"][..., 2] = float(rng.uniform(0.0, M2_PERIOD))   # phase [s]
+        c["name"] = f"request{m}_{c['nkn']}"
+        out.append((t, c, horizon_steps))
+    return out
