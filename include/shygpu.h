@@ -98,6 +98,9 @@ typedef struct shy_params {
   float solver_rtol;         /* Krylov stop ||r|| <= rtol*||r0|| + atol     */
   float solver_atol;         /*   (sparskit_admin.f90:270-277: 1e-8, 1e-8)  */
   int32_t solver_maxit;      /* iteration limit (sparskit_admin.f90:141)    */
+  int32_t nsigma;            /* sigma layers (levels :: nsigma): 0 z-layers, */
+                             /*   nlv pure sigma (hlv/hldv sigma values < 0) */
+  float hsigma;              /* depth limit of the sigma layers (hsigma)    */
 } shy_params;
 
 /* Host views of one basin's state, reference layouts.  NULL members are

@@ -503,14 +503,41 @@ void set_ieltv(Model &m) {
     }
 }
 
-// setdepth for z-layers (elems_dealing.f90:930-1160) with nsigma = 0 and no
-// z-adaptive layers (compute_zadaptive_info returns nadapt = ladapt = 0,
-// zadaptutil.f90:321-324).
+// setdepth (elems_dealing.f90:930-1160) for z-layers (nsigma = 0) and for
+// pure sigma layers (nsigma = nlv), without z-adaptive layers
+// (compute_zadaptive_info returns nadapt = ladapt = 0, zadaptutil.f90:321-324).
 int setdepth(Model &m, std::vector<double> &hdkn, std::vector<double> &hden,
              const std::vector<double> &zenv) {
   int nlv = m.nlv;
   hdkn.assign((size_t)nlv * m.nkn, 0.);
   hden.assign((size_t)nlv * m.nel, 0.);
+  if (m.p.nsigma > 0) {
+    // sigma layers: the thickness is the sigma fraction -hldv(l) of the
+    // total depth min(h, hsigma) + z, at the nodes from each element's
+    // vertex values in element order (:1010-1025, the last element writes),
+    // at the elements from hev and the mean water level (:1075-1085)
+    const double hsigma = (double)(float)(m.p.hsigma > 0.f ? m.p.hsigma : 10000.f);
+    for (int ie = 0; ie < m.nel; ie++) {
+      double zmed = 0.;
+      for (int ii = 0; ii < 3; ii++) {
+        const int k = m.nen3v[3 * ie + ii];
+        const double z = zenv[3 * ie + ii];
+        zmed += z;
+        const double hsig = std::min(m.hm3v[3 * ie + ii], hsigma) + z;
+        for (int l = 1; l <= m.p.nsigma; l++) hdkn[(size_t)k * nlv + l - 1] = -hsig * m.hldv[l - 1];
+      }
+      zmed /= 3.;
+      const double hsig = std::min(m.hev[ie], hsigma) + zmed;
+      for (int l = 1; l <= m.p.nsigma; l++) {
+        hden[(size_t)ie * nlv + l - 1] = -hsig * m.hldv[l - 1];
+        if (hden[(size_t)ie * nlv + l - 1] <= 0.) return fail(SHY_EDEPTH, "setdepth: no layer depth in element");
+      }
+    }
+    for (int k = 0; k < m.nkn; k++)
+      for (int l = 1; l <= m.ilhkv[k]; l++)
+        if (hdkn[(size_t)k * nlv + l - 1] <= 0.) return fail(SHY_EDEPTH, "setdepth: no layer depth in node");
+    return SHY_OK;
+  }
   double hl[3][SHY_MAX_LAYERS > 64 ? SHY_MAX_LAYERS : 64];
   for (int ie = 0; ie < m.nel; ie++) {
     double areafv = 12. * m.ev[(size_t)ie * SHY_EVDIM + 9] / 3.;
@@ -1382,6 +1409,7 @@ void *shyref_create(const shy_basin *B, const shy_params *P) {
   m->nkn = B->nkn; m->nel = B->nel; m->nlv = B->nlv; m->p = *P;
   int nkn = m->nkn, nel = m->nel, nlv = m->nlv;
   if (nlv < 1 || nlv > SHY_MAX_LAYERS) { fail(SHY_EARG, "shyref_create: nlv"); delete m; return nullptr; }
+  if (P->nsigma != 0 && P->nsigma != nlv) { fail(SHY_EARG, "shyref_create: nsigma 0 or nlv"); delete m; return nullptr; }
   m->nen3v.resize((size_t)3 * nel);
   for (size_t i = 0; i < m->nen3v.size(); i++) m->nen3v[i] = B->nen3v[i] - 1;
   std::vector<double> x = dv(B->xgv, nkn), y = dv(B->ygv, nkn);

@@ -39,6 +39,8 @@ struct BasinPar {
   int maxit;
   int has_cor;
   int is_temp[kMaxScal];      // scalar s is temperature (no clipping at 1e-15)
+  int nsigma;                 // 0: z-layers; nlv: pure sigma layers
+  float hsigma;               // depth limit of the sigma layers
 };
 
 // per-basin results of the last step (device memory)

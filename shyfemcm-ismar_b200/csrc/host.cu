@@ -683,6 +683,10 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     if (Pp[b].ireib != 0 && Pp[b].ireib != 5) return bail(fail(SHY_EARG, "basin %d: ireib=%d not supported (0 or 5)", b, Pp[b].ireib));
     if (Pp[b].ilin == 0) return bail(fail(SHY_EARG, "basin %d: non-linear momentum (ilin=0) not supported", b));
     if (!(Pp[b].dt > 0)) return bail(fail(SHY_EARG, "basin %d: dt must be positive", b));
+    if (Pp[b].nsigma != 0 && Pp[b].nsigma != bs.nlv)
+      return bail(fail(SHY_EARG, "basin %d: nsigma=%d: z-layers (0) or pure sigma layers (nlv) only", b, Pp[b].nsigma));
+    if (Pp[b].nsigma > 0 && Pp[b].ibarcl > 0)
+      return bail(fail(SHY_EARG, "basin %d: baroclinic terms on sigma layers not supported", b));
     NLV = std::max(NLV, bs.nlv);
   }
   m->nbasin = nbasin; m->NLV = NLV; m->S = next_pow2(NLV);
@@ -830,6 +834,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     bp.grav = p.grav; bp.rowass = p.rowass; bp.vismol = p.vismol; bp.difmol = p.difmol;
     bp.hzoff = p.hzoff; bp.ahpar = p.ahpar; bp.rstol = p.rstol > 0 ? p.rstol : 1.f;
     bp.ireib = p.ireib; bp.ibarcl = p.ibarcl;
+    bp.nsigma = p.nsigma; bp.hsigma = p.hsigma > 0.f ? p.hsigma : 10000.f;
     bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
     int ns = 0;
     if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }

@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(256) k_final(Dev d, int init_only) {
     double um = seg_sum<S>(u), vm = seg_sum<S>(v);
     if (lane == 0 && valid) { d.unv[e] = (float)um; d.vnv[e] = (float)vm; }
   }
-  // setzev and the element part of setdepth (z-layers)
+  // setzev and the element part of setdepth (z-layers or pure sigma layers)
   if (lane == 0 && valid) {
 #pragma unroll
     for (int ii = 0; ii < 3; ii++) d.zen[3 * e + ii] = (float)zn3[ii];
@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(256) k_final(Dev d, int init_only) {
   const float *hlv = d.hlv + (size_t)en.w * NLV;
   double h = 0.;
   if (act) {
-    if (ilevel == 1) h = hm.w + zmed;
+    if (P.nsigma > 0) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[lane];   // :1079-1083
+    else if (ilevel == 1) h = hm.w + zmed;
     else if (lane < ilevel - 1) h = (double)hld[lane] + (lane == 0 ? zmed : 0.);
     else h = (double)hm.w - hlv[ilevel - 2];
     if (!(h > 0.) && valid) set_status(&d.out[en.w], SHY_EDEPTH);
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
     d.unv[e] = (float)um;
     d.vnv[e] = (float)vm;
   }
-  // setzev and the element part of setdepth (z-layers)
+  // setzev and the element part of setdepth (z-layers or pure sigma layers)
 #pragma unroll
   for (int ii = 0; ii < 3; ii++) d.zen[3 * e + ii] = (float)zn3[ii];
   const float4 hm = d.hm3v[e];
@@ -135,7 +136,8 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
   for (int l = 0; l < NLV; l++) {
     double h = 0.;
     if (l < ilevel) {
-      if (ilevel == 1) h = hm.w + zmed;
+      if (P.nsigma > 0) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // :1079-1083
+      else if (ilevel == 1) h = hm.w + zmed;
       else if (l < ilevel - 1) h = (double)hld[l] + (l == 0 ? zmed : 0.);
       else h = (double)hm.w - hlv[ilevel - 2];
       if (!(h > 0.)) bad = true;

@@ -26,6 +26,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   const float *hlv = d.hlv + (size_t)b * NLV;
   const double hldl = lane < NLV ? (double)hld[lane] : 0.;
   double hsum = 0., vf = 0., va = 0.;
+  double hsig_h = 0.;                         // sigma: depth of the last incident element's vertex
 #pragma unroll 2
   for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
     const int4 ix = d.incx[p];
@@ -36,6 +37,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
     const double areafv = 4. * aj;            // 12*aj/3
     const float4 hm = d.hm3v[e];
     const double htot = ii == 0 ? hm.x : (ii == 1 ? hm.y : hm.z);
+    hsig_h = htot;
     double hl;
     if (le == 1) hl = htot + z;
     else if (lane < le - 1) hl = hldl + (lane == 0 ? z : 0.);
@@ -53,6 +55,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   const size_t o = (size_t)k * NLV + lane;
   const double area = act ? (double)d.areakv[o] : 0.;
   double hk = act && area > 0. ? hsum / area : 0.;
+  if (P.nsigma > 0 && act) hk = -(fmin(hsig_h, (double)P.hsigma) + z) * hldl;   // sigma (:1019-1025)
   float hkf = (float)hk;
   if (act && !(hkf > 0.f) && valid) set_status(&d.out[b], SHY_EDEPTH);
   if (valid && lane < NLV) d.hkn[o] = act ? hkf : 0.f;
@@ -96,6 +99,7 @@ __global__ void __launch_bounds__(128) k_node_t(Dev d, const int *kbas, int init
   const float *hld = d.hldv + (size_t)b * NLV;
   const float *hlv = d.hlv + (size_t)b * NLV;
   double hsum[L], vf[L], va[L];
+  double hsig_h = 0.;                         // sigma: depth of the last incident element's vertex
 #pragma unroll
   for (int l = 0; l < L; l++) { hsum[l] = 0.; vf[l] = 0.; va[l] = 0.; }
   for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
@@ -109,6 +113,7 @@ __global__ void __launch_bounds__(128) k_node_t(Dev d, const int *kbas, int init
     const double bb = evp[ii], cc = evp[3 + ii];
     const size_t oe = (size_t)e * NLV;
     const double hbot = le >= 2 ? htot - hlv[le - 2] : 0.;
+    hsig_h = htot;
 #pragma unroll
     for (int l = 0; l < L; l++) {
       if (l >= le) break;
@@ -136,7 +141,8 @@ __global__ void __launch_bounds__(128) k_node_t(Dev d, const int *kbas, int init
     if (l >= NLV) continue;
     const bool act = l < lmax;
     area[l] = act ? (double)d.areakv[o + l] : 0.;
-    const double hk = act && area[l] > 0. ? hsum[l] / area[l] : 0.;
+    double hk = act && area[l] > 0. ? hsum[l] / area[l] : 0.;
+    if (P.nsigma > 0 && act) hk = -(fmin(hsig_h, (double)P.hsigma) + z) * (double)hld[l];   // sigma (:1019-1025)
     hkf[l] = (float)hk;
     if (act && !(hkf[l] > 0.f)) bad = true;
     d.hkn[o + l] = act ? hkf[l] : 0.f;

@@ -48,6 +48,7 @@ class ShyParams(C.Structure):
         ("itemp", C.c_int32), ("isalt", C.c_int32), ("nconz", C.c_int32),
         ("istot_max", C.c_int32),
         ("solver_rtol", C.c_float), ("solver_atol", C.c_float), ("solver_maxit", C.c_int32),
+        ("nsigma", C.c_int32), ("hsigma", C.c_float),
     ]
 
 
@@ -126,6 +127,8 @@ def make_params(case, **over):
     s.solver_rtol = float(p.get("solver_rtol", 1e-8))
     s.solver_atol = float(p.get("solver_atol", 1e-8))
     s.solver_maxit = int(p.get("solver_maxit", 1000))
+    s.nsigma = int(p.get("nsigma", 0))
+    s.hsigma = float(p.get("hsigma", 10000.0))
     return s
 
 

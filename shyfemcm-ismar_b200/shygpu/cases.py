@@ -210,6 +210,44 @@ def basin3d_case(nkn_target=20000, lx=50.0e3, ly=30.0e3, seed=2, dt=120.0,
     return _finish(case)
 
 
+def lagoon_case(nkn_target=3000, lx=12.0e3, ly=6.0e3, seed=7, dt=30.0, nlv=30, ntracer=3,
+                hmin=1.5, hmax=30.0):
+    """Tidal lagoon on pure sigma layers (the large-lagoon config's vertical
+    grid): a jittered triangle mesh deepening from `hmin` at the closed end
+    to `hmax` at the open boundary with seeded smooth relief, `nlv` equal
+    sigma layers (hlv = -l/nlv, nsigma = nlv), an M2 + S2 level boundary of
+    0.8 m total amplitude, and `ntracer` passive tracers starting from
+    seeded Gaussian patches.  Barotropic (sigma layers without baroclinic
+    terms)."""
+    ny = max(3, int(round(math.sqrt(nkn_target * ly / lx))))
+    nx = max(3, int(round(nkn_target / ny)))
+    x, y, nen3v, ii, jj = structured_triangles(nx, ny, lx, ly, 0.2, seed)
+    rng = np.random.default_rng(seed + 404)
+    nkn, nel = x.size, nen3v.shape[0]
+    ramp = 1.0 - x / lx                               # deep at x = 0 (open boundary)
+    h = hmin + (hmax - hmin) * ramp ** 1.5 + _smooth_field(x, y, rng, scale=0.3 * hmin)
+    h = np.maximum(h, hmin)
+    hm3v = h[nen3v - 1]
+    hlv = -np.arange(1, nlv + 1, dtype=np.float64) / nlv
+    hldv = np.full(nlv, -1.0 / nlv)
+    ilhv = np.full(nel, nlv, np.int32)
+    ilhkv = np.full(nkn, nlv, np.int32)
+    bnd = np.zeros(nkn, np.int32)
+    bnd[ii == 0] = 1
+    tide = np.array([[[0.5, M2_PERIOD, 0.0, 0.0], [0.3, S2_PERIOD, 3600.0, 0.0]]], np.float32)
+    conz = np.zeros((ntracer, nkn, nlv), np.float32)
+    for t in range(ntracer):
+        cx, cy = rng.uniform(0.3 * lx, 0.9 * lx), rng.uniform(0.2 * ly, 0.8 * ly)
+        s = rng.uniform(0.05, 0.15) * lx
+        conz[t] = (10.0 * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * s * s)))[:, None]
+    params = dict(dt=dt, nsigma=nlv, hsigma=10000.0, nconz=ntracer, chpar=0.0)
+    case = dict(name=f"lagoon_sigma_{nkn}x{nlv}", nkn=nkn, nel=nel, nlv=nlv, nen3v=nen3v,
+                xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
+                bnd_index=bnd, tide=tide, seed=seed, params=params, conzv=conz,
+                tauxnv=np.full(nkn, 1.0e-4, np.float32))
+    return _finish(case)
+
+
 def ensemble_cases(n, nkn_lo=5000, nkn_hi=100000, nlv=10, seed=4, dt=60.0, first=None):
     """Independent basins with log-uniform node counts and seeded aspect
     ratios and wind perturbations (sigma = 3 m/s).  `first` builds only the

@@ -181,3 +181,22 @@ def test_large_basin_in_a_mix():
         assert np.abs(a["znv"] - b["znv"]).max() <= 1e-5, i
         umax = np.abs(a["utlnv"]).max()
         assert np.abs(a["utlnv"] - b["utlnv"]).max() <= 1e-4 * umax, i
+
+
+@pytest.mark.parametrize("nlv", [12, 30])
+def test_lagoon_sigma_layers_tracers(nlv):
+    """The lagoon config's vertical grid at test size: pure sigma layers,
+    M2 + S2 boundary, three passive tracers (12 layers: thread-per-column
+    kernels; 30 layers: warp-segment kernels)."""
+    c = cases.lagoon_case(nkn_target=900, nlv=nlv)
+    g, o = run_both(c, 80)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    assert np.abs(sg["hdknv"] - so["hdknv"]).max() <= 1e-4 * np.abs(so["hdknv"]).max()
+    umax = np.abs(so["utlnv"]).max()
+    assert np.abs(sg["utlnv"] - so["utlnv"]).max() <= 1e-3 * umax
+    cmax = np.abs(so["conzv"]).max()
+    assert np.abs(sg["conzv"] - so["conzv"]).max() <= TRACER_RTOL * cmax
+    wmax = np.abs(so["wlnv"]).max()
+    assert np.abs(sg["wlnv"] - so["wlnv"]).max() <= 2e-3 * wmax
+    assert abs(g.info(0).volume - o.info().volume) <= 1e-6 * o.info().volume
