@@ -269,6 +269,7 @@ struct shygpu_model {
   int nsub = 2, use_graph = 1, max_outer = 12, sym = 1;
   int zvariant = 1;                  // 1: shared-memory zeta solver when it fits
   int zstage = 0;                    // device-wide solver: 1 TMA-staged tiles when they fit
+  int zbar_test = 0;                 // device-wide solver: 1 makes every grid barrier time out
   int zforce_CL = 0, zforce_threads = 0;   // > 0: one launch class with this shape
   std::vector<ZetaClass> zcl;        // launch classes of the zeta solver
   cudaStream_t side[kMaxZetaClasses] = {};
@@ -390,6 +391,9 @@ static int build_grid_class(shygpu_model *m) {
   c.CL = 0;
   for (int i = 0; i < m->nbasin; i++) c.basins.push_back(i);
   c.gp.ntile = T;
+  // the barrier timeout test: one arrival that never comes, a short poll limit
+  c.gp.phantom = m->zbar_test ? 1u : 0u;
+  c.gp.spin_limit = m->zbar_test ? (1LL << 14) : zeta_grid_spin_limit();
   int4 *dt = nullptr; int2 *dbt = nullptr; int *dcs = nullptr, *dcn = nullptr, *dco = nullptr;
   ST_TRY(upload_plan(&dt, tile)); c.gp.tile = dt;
   ST_TRY(upload_plan(&dbt, btile)); c.gp.btile = dbt;
@@ -957,6 +961,13 @@ extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value
     m->zvariant = iv;
     ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
   }
+  else if (n == "zeta_barrier_timeout_test") {
+    // failure detection: the device-wide solver's barrier waits for one
+    // arrival more than it has CTAs, so every wait runs out (after a short
+    // poll limit) and the step reports SHY_ECUDA; 0 restores the solver
+    m->zbar_test = iv != 0;
+    ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
+  }
   else if (n == "zeta_stage") {   // device-wide solver: 1 TMA-staged tiles, 0 global loads
     m->zstage = iv != 0;
     ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
@@ -1155,6 +1166,7 @@ static int check_outputs(shygpu_model *m) {
                         : s == SHY_EDEPTH ? "non-positive layer thickness"
                         : s == SHY_EISTOT ? "transport sub-steps above the limit or the captured sub-step budget (option 'substeps')"
                         : s == SHY_ESINGULAR ? "zero pivot in a vertical transport system"
+                        : s == SHY_ECUDA ? "a wait of the device-wide zeta solver ran out (grid barrier)"
                         : "error";
       for (int q = 0; q < m->nbasin; q++)
         cudaMemsetAsync(&m->base.out[q].status, 0, sizeof(int), m->stream);

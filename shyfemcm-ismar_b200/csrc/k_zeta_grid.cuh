@@ -24,7 +24,7 @@
 // finished idles until every basin has.
 //
 // The grid barrier is an arrival counter with a bounded wait: a CTA that
-// waits longer than kGridSpinLimit polls marks every basin of the launch
+// waits longer than the plan's poll limit (kGridSpinLimit by default) marks every basin of the launch
 // with SHY_ECUDA and leaves, and so do the others when they see the abort
 // flag.  The launch is cooperative, so all CTAs are resident together.
 // Vectors written by other CTAs are read with ordinary (L1-cached) loads:
@@ -40,7 +40,7 @@ constexpr int kGridMaxSlots = 32;                // basins per CTA
 constexpr int kGridMaxTiles = 32;                // tiles per CTA
 constexpr int kGridTileRows = 1024;              // rows per tile
 constexpr long long kMbarSpinLimit = 1LL << 22;  // try_wait polls before a staged copy counts as lost
-constexpr long long kGridSpinLimit = 1LL << 24;  // ~ seconds with the back-off below
+constexpr long long kGridSpinLimit = 1LL << 24;  // default poll limit: ~ seconds with the back-off below
 constexpr int kGridPartialUnroll = 8;           // partial sums a lane loads at once
 
 enum GridStage : int { G_RES = 0, G_XTRP, G_SPMV0, G_ITER, G_FIX, G_FINISH, G_DONE };
@@ -64,19 +64,20 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
 // both sides extend the release and the acquire to every thread of the CTA.
 // Returns false on timeout/abort (ctr[4]).  *act (when not null) receives
 // ctr[act_idx] read after the barrier, once for the CTA.
-__device__ __forceinline__ bool grid_barrier(unsigned *ctr, unsigned bar, int *s_ok, unsigned act_idx,
+__device__ __forceinline__ bool grid_barrier(const GridPlan &gp, unsigned bar, int *s_ok, unsigned act_idx,
                                              unsigned *s_act) {
+  unsigned *ctr = gp.ctr;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
     unsigned old;
     asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(ctr) : "memory");
-    if (old + 1u == bar * gridDim.x) {
+    if (old + 1u == bar * (gridDim.x + gp.phantom)) {
       asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctr + 5), "r"(bar) : "memory");
     } else {
       long long spins = 0;
       while (ld_acquire_u32(ctr + 5) < bar) {
-        if (ld_acquire_u32(ctr + 4) != 0u || ++spins > kGridSpinLimit) {
+        if (ld_acquire_u32(ctr + 4) != 0u || ++spins > gp.spin_limit) {
           atomicExch(ctr + 4, 1u);
           ok = 0;
           break;
@@ -342,7 +343,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
     return;
   }
   if (STAGED) asm volatile("fence.proxy.async.global;" ::: "memory");
-  if (!grid_barrier(gp.ctr, ++bar, &s_ok, 0, nullptr)) goto aborted;
+  if (!grid_barrier(gp, ++bar, &s_ok, 0, nullptr)) goto aborted;
 
   for (unsigned k = 0;; k++) {
     const int par = (int)(k & 1u);
@@ -528,7 +529,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
     }
     // the next super-step may read these writes through the async proxy
     if (STAGED) asm volatile("fence.proxy.async.global;" ::: "memory");
-    if (!grid_barrier(gp.ctr, ++bar, &s_ok, 1 + k % 3, &s_act)) goto aborted;
+    if (!grid_barrier(gp, ++bar, &s_ok, 1 + k % 3, &s_act)) goto aborted;
     if (s_act == 0u) break;
     // ---- per-basin sums over its tiles, the same in every CTA; next stage ----
     for (int sl = tid >> 5; sl < nslot; sl += NW) {

@@ -58,6 +58,8 @@ struct GridPlan {
   int nzcap = 0;                   // most CSR entries of any tile (staged buffer size)
   double *partial = nullptr;       // [2][ntile][4] partial sums of the tiles
   unsigned *ctr = nullptr;         // [8]: barrier arrivals, 3 active counts, abort flag, release
+  unsigned phantom = 0;            // arrivals the barrier waits for beyond its CTAs (0; 1 in the timeout test)
+  long long spin_limit = 0;        // polls before a barrier wait gives up
 };
 
 // a group of basins solved by one launch with one cluster shape
@@ -89,6 +91,7 @@ size_t zeta_grid_stage_smem(int nzcap);
 int zeta_grid_max_slots();   // basins one CTA can hold
 int zeta_grid_max_tiles();   // tiles one CTA can hold
 int zeta_grid_tile_rows();   // rows per tile
+long long zeta_grid_spin_limit();   // default barrier poll limit
 // smem > 0 prepares the shared-memory variant for that many dynamic bytes
 cudaError_t zeta_kernel_setup(int CL, size_t smem);
 int zeta_max_active_clusters(int CL, int threads, size_t smem);

@@ -212,6 +212,7 @@ int zeta_grid_capacity(bool staged, size_t smem) {
 int zeta_grid_max_slots() { return kGridMaxSlots; }
 int zeta_grid_max_tiles() { return kGridMaxTiles; }
 int zeta_grid_tile_rows() { return kGridTileRows; }
+long long zeta_grid_spin_limit() { return kGridSpinLimit; }
 
 cudaError_t zeta_kernel_setup(int CL, size_t smem) {
   cudaError_t e = cudaSuccess;
