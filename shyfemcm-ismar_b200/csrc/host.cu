@@ -13,6 +13,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <queue>
 #include <vector>
 
 #include "../../include/shygpu.h"
@@ -321,6 +322,7 @@ static void free_zeta_plan(shygpu_model *m) {
     if (c.grid) {
       cudaFree((void *)c.gp.tile); cudaFree((void *)c.gp.btile); cudaFree((void *)c.gp.cslot);
       cudaFree((void *)c.gp.cnslot); cudaFree((void *)c.gp.cowner); cudaFree((void *)c.gp.tnz);
+      cudaFree((void *)c.gp.cptr); cudaFree((void *)c.gp.clist);
       cudaFree(c.gp.partial); cudaFree(c.gp.ctr);
     }
   }
@@ -329,10 +331,11 @@ static void free_zeta_plan(shygpu_model *m) {
 
 // The device-wide class: every basin in one cooperative launch.  Each
 // basin's rows are cut into tiles of a fixed row count (the tile boundaries, and
-// so the reduction order, depend on the basin alone); tile t goes to CTA
-// t % G, so a basin's tiles sit on consecutive CTAs and the work left when
-// only a few basins still iterate spreads over many CTAs.  Returns SHY_EARG
-// when a CTA would hold more tiles or basins than it can.
+// so the reduction order, depend on the basin alone); the tiles are dealt
+// to CTAs so that every CTA has about the same rows, and a basin's tiles
+// spread over many CTAs, so the work left when only a few basins still
+// iterate is shared out.  Returns SHY_EARG when a CTA would hold more tiles
+// or basins than it can.
 template <typename T>
 static int upload_plan(T **dst, const std::vector<T> &h) {
   CUDA_TRY(cudaMalloc((void **)dst, sizeof(T) * std::max<size_t>(h.size(), 1)));
@@ -365,22 +368,47 @@ static int build_grid_class(shygpu_model *m) {
   if (cap < 1) return fail(SHY_ECUDA, "zeta grid solver: no resident CTA fits the device");
   const int T = (int)tile.size();
   const int G = std::max(1, std::min(cap, T));
-  if ((T + G - 1) / G > zeta_grid_max_tiles())
-    return fail(SHY_EARG, "zeta grid solver: %d tiles for %d CTAs", T, G);
-  std::vector<int> cslot((size_t)G * MS, -1), cnslot(G, 0), cowner(G, 0);
-  for (int t = 0; t < T; t++) {
-    const int c = t % G, b = tile[t].z;
-    int sl = -1;
-    for (int k = 0; k < cnslot[c]; k++)
-      if (cslot[(size_t)c * MS + k] == b) sl = k;
-    if (sl < 0) {
-      if (cnslot[c] >= MS) return fail(SHY_EARG, "zeta grid solver: more than %d basins in one CTA", MS);
-      sl = cnslot[c]++;
-      cslot[(size_t)c * MS + sl] = b;
-    }
-    tile[t].w = sl;
-    if (t == btile[b].x) cowner[c] |= 1 << sl;
+  // tiles to CTAs, largest first to the CTA with the fewest rows so far
+  // (ties: the lower CTA): every CTA ends within one tile of the mean, and a
+  // basin's tiles spread over many CTAs
+  std::vector<int> order(T);
+  for (int t = 0; t < T; t++) order[t] = t;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return tile[x].y - tile[x].x > tile[y].y - tile[y].x;
+  });
+  typedef std::pair<long long, int> Load;
+  std::priority_queue<Load, std::vector<Load>, std::greater<Load>> heap;
+  for (int c = 0; c < G; c++) heap.push(Load(0, c));
+  std::vector<std::vector<int>> ctl(G);
+  for (int t : order) {
+    Load l = heap.top();
+    heap.pop();
+    ctl[l.second].push_back(t);
+    heap.push(Load(l.first + (tile[t].y - tile[t].x), l.second));
   }
+  std::vector<int> cptr(G + 1, 0), clist;
+  for (int c = 0; c < G; c++) {
+    std::sort(ctl[c].begin(), ctl[c].end());
+    if ((int)ctl[c].size() > zeta_grid_max_tiles())
+      return fail(SHY_EARG, "zeta grid solver: %d tiles in one CTA", (int)ctl[c].size());
+    clist.insert(clist.end(), ctl[c].begin(), ctl[c].end());
+    cptr[c + 1] = (int)clist.size();
+  }
+  std::vector<int> cslot((size_t)G * MS, -1), cnslot(G, 0), cowner(G, 0);
+  for (int c = 0; c < G; c++)
+    for (int t : ctl[c]) {
+      const int b = tile[t].z;
+      int sl = -1;
+      for (int k = 0; k < cnslot[c]; k++)
+        if (cslot[(size_t)c * MS + k] == b) sl = k;
+      if (sl < 0) {
+        if (cnslot[c] >= MS) return fail(SHY_EARG, "zeta grid solver: more than %d basins in one CTA", MS);
+        sl = cnslot[c]++;
+        cslot[(size_t)c * MS + sl] = b;
+      }
+      tile[t].w = sl;
+      if (t == btile[b].x) cowner[c] |= 1 << sl;
+    }
   m->zcl.emplace_back();
   ZetaClass &c = m->zcl.back();
   c.grid = true;
@@ -402,6 +430,9 @@ static int build_grid_class(shygpu_model *m) {
   ST_TRY(upload_plan(&dco, cowner)); c.gp.cowner = dco;
   int2 *dnz = nullptr;
   ST_TRY(upload_plan(&dnz, tnz)); c.gp.tnz = dnz;
+  int *dcp = nullptr, *dcl = nullptr;
+  ST_TRY(upload_plan(&dcp, cptr)); c.gp.cptr = dcp;
+  ST_TRY(upload_plan(&dcl, clist)); c.gp.clist = dcl;
   c.gp.nzcap = nzcap;
   CUDA_TRY(cudaMalloc(&c.gp.partial, sizeof(double) * 8 * std::max<size_t>(tile.size(), 1)));
   CUDA_TRY(cudaMalloc(&c.gp.ctr, 8 * sizeof(unsigned)));

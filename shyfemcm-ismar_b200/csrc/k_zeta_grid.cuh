@@ -2,9 +2,10 @@
 // thread-block cluster can hold: one persistent cooperative launch over the
 // whole device for every basin of the model.
 //
-// Each basin's rows are cut into tiles of 1024 rows, and tile t is worked by
-// CTA t % G, so the tiles of a basin sit on consecutive CTAs and the work of
-// the few basins still iterating late in a solve spreads over many CTAs.
+// Each basin's rows are cut into tiles of 1024 rows, dealt to the CTAs so
+// that each has about the same rows and a basin's tiles spread over many
+// CTAs, so the work of the few basins still iterating late in a solve is
+// shared out.
 // The solver is the one of k_zeta_sm (system_solve,
 // sparskit_admin.f90:115-334, with the reference's stop test
 // ||r|| <= rtol*||r0|| + atol, spk_iters.f90:3304-3360): FP64 residual
@@ -284,15 +285,16 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
   constexpr int NW = NT / 32;
   __shared__ GridState gs[kGridMaxSlots];
   __shared__ int4 s_tile[kGridMaxTiles];
+  __shared__ int s_tid[kGridMaxTiles];
   __shared__ int2 s_tnz[STAGED ? kGridMaxTiles : 1];
   __shared__ double wred[kGridMaxTiles * NW * 3];
   __shared__ int s_ok;
   __shared__ unsigned s_act;
   extern __shared__ __align__(128) unsigned char dsm[];
   const int tid = threadIdx.x, nth = blockDim.x;
-  const int c = blockIdx.x, G = gridDim.x;
+  const int c = blockIdx.x;
   const int nslot = gp.cnslot[c];
-  const int ntl = (gp.ntile - c + G - 1) / G;      // this CTA's tiles: c, c+G, c+2G, ...
+  const int t0 = gp.cptr[c], ntl = gp.cptr[c + 1] - t0;   // this CTA's tiles: clist[t0 ..]
   unsigned bar = 0;
   const StageLayout SL = stage_layout(gp.nzcap);
   uint32_t mbar[2] = {0u, 0u}, sbuf[2] = {0u, 0u}, phase[2] = {0u, 0u};
@@ -314,8 +316,10 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
     g.tol = g.itol2 = g.rn = g.resid0 = g.alpha = g.beta = g.gamma = 0.;
   }
   if (tid < ntl) {
-    s_tile[tid] = gp.tile[c + tid * G];
-    if constexpr (STAGED) s_tnz[tid] = gp.tnz[c + tid * G];
+    const int t = gp.clist[t0 + tid];
+    s_tid[tid] = t;
+    s_tile[tid] = gp.tile[t];
+    if constexpr (STAGED) s_tnz[tid] = gp.tnz[t];
   }
   if (blockIdx.x == 0 && tid == 0 && d.imax) { *d.imax = 0; *d.subj = 0; }
   __syncthreads();
@@ -500,7 +504,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
           for (int o = 16; o > 0; o >>= 1) x[cc] += __shfl_xor_sync(0xffffffffu, x[cc], o);
         }
         if (lane == 0) {
-          double *pp = gp.partial + ((size_t)par * gp.ntile + (c + q * G)) * 4;
+          double *pp = gp.partial + ((size_t)par * gp.ntile + s_tid[q]) * 4;
           __stcg(pp + 0, x[0]); __stcg(pp + 1, x[1]); __stcg(pp + 2, x[2]);
         }
       }

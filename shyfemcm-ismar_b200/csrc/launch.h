@@ -46,7 +46,7 @@ struct ZetaMaps {
 
 // the device-wide zeta solver (k_zeta_grid).  Each basin's rows are cut into
 // tiles of a fixed row count (the last one shorter); tile t = {row0, row1,
-// basin, slot} is worked by CTA t % G, where `slot` indexes the CTA's table
+// basin, slot} is worked by one CTA (cptr/clist), where `slot` indexes the CTA's table
 // of basins: cslot[c*16 + slot] is the basin, bit slot of cowner[c] says the
 // CTA holds the basin's first tile; basin b's tiles are btile[b].x .. .y-1
 struct GridPlan {
@@ -55,6 +55,8 @@ struct GridPlan {
   const int2 *btile = nullptr;
   const int *cslot = nullptr, *cnslot = nullptr, *cowner = nullptr;
   const int2 *tnz = nullptr;       // per tile: its CSR entries rowptr[row0] .. rowptr[row1]
+  const int *cptr = nullptr;       // CTA c works tiles clist[cptr[c]] .. clist[cptr[c+1]-1]
+  const int *clist = nullptr;
   int nzcap = 0;                   // most CSR entries of any tile (staged buffer size)
   double *partial = nullptr;       // [2][ntile][4] partial sums of the tiles
   unsigned *ctr = nullptr;         // [8]: barrier arrivals, 3 active counts, abort flag, release
