@@ -58,26 +58,29 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned *p) {
   return v;
 }
 
-// bar-th grid barrier (bar = 1, 2, ...).  Arrivals count up in ctr[0] with
-// a release reduction; the CTA that completes a barrier publishes its number
-// in ctr[5] (release), which the others poll with acquire loads (read-only
-// polling keeps the counter's atomics uncontended).  The CTA barriers on
-// both sides extend the release and the acquire to every thread of the CTA.
-// Returns false on timeout/abort (ctr[4]).  *act (when not null) receives
-// ctr[act_idx] read after the barrier, once for the CTA.
+// bar-th grid barrier (bar = 1, 2, ...).  Arrivals count up in ctr[0]; the
+// CTA that completes a barrier reads the active-basin count ctr[act_idx]
+// (when act_idx != 0) and publishes 2*bar + (count == 0) in ctr[5] with a
+// release store, which the others poll with acquire loads (read-only
+// polling keeps the counter's atomics uncontended, and nobody reads the
+// count after the barrier).  The CTA barriers on both sides extend the
+// release and the acquire to every thread of the CTA.  Returns false on
+// timeout/abort (ctr[4]).  *s_act receives 0 when no basin is active.
 __device__ __forceinline__ bool grid_barrier(const GridPlan &gp, unsigned bar, int *s_ok, unsigned act_idx,
                                              unsigned *s_act) {
   unsigned *ctr = gp.ctr;
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
-    unsigned old;
-    asm volatile("atom.add.release.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(ctr) : "memory");
+    unsigned old, flag = 0u;
+    asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(ctr) : "memory");
     if (old + 1u == bar * (gridDim.x + gp.phantom)) {
-      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctr + 5), "r"(bar) : "memory");
+      const unsigned none = act_idx != 0u && ld_acquire_u32(ctr + act_idx) == 0u ? 1u : 0u;
+      flag = 2u * bar + none;
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(ctr + 5), "r"(flag) : "memory");
     } else {
       long long spins = 0;
-      while (ld_acquire_u32(ctr + 5) < bar) {
+      while (((flag = ld_acquire_u32(ctr + 5)) >> 1) < bar) {
         if (ld_acquire_u32(ctr + 4) != 0u || ++spins > gp.spin_limit) {
           atomicExch(ctr + 4, 1u);
           ok = 0;
@@ -86,7 +89,7 @@ __device__ __forceinline__ bool grid_barrier(const GridPlan &gp, unsigned bar, i
         if (spins > 256) __nanosleep(32);
       }
     }
-    if (s_act) *s_act = ld_acquire_u32(ctr + act_idx);
+    if (s_act) *s_act = (flag & 1u) ? 0u : 1u;
     *s_ok = ok;
   }
   __syncthreads();
@@ -308,11 +311,13 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
     }
   }
 
+  __shared__ int2 s_bt[kGridMaxSlots];
   if (tid < nslot) {
     GridState &g = gs[tid];
     g.stage = G_RES; g.first = 1; g.conv = 0; g.outer = 0; g.inner = 0; g.iters = 0; g.cur = 0;
     g.basin = gp.cslot[c * kGridMaxSlots + tid];
     g.owner = (gp.cowner[c] >> tid) & 1;
+    s_bt[tid] = gp.btile[g.basin];
     g.tol = g.itol2 = g.rn = g.resid0 = g.alpha = g.beta = g.gamma = 0.;
   }
   if (tid < ntl) {
@@ -542,7 +547,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
         GridState &g = gs[sl];
         const int st = g.stage;
         if (st == G_RES || st == G_SPMV0 || st == G_ITER) {
-          const int2 bt = gp.btile[g.basin];
+          const int2 bt = s_bt[sl];
           double tot[3] = {0., 0., 0.};
           // up to 32*kGridPartialUnroll partials per round, all loads issued first
           for (int s0 = bt.x; s0 < bt.y; s0 += 32 * kGridPartialUnroll) {
