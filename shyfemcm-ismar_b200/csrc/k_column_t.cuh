@@ -21,7 +21,7 @@
 namespace shy {
 
 template <int L, bool COR>
-__global__ void __launch_bounds__(128) k_column_t(Dev d) {
+__global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.NEL) return;
   const int NLV = d.NLV;

@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
 // its layers (in element order, as k_node); then the node's layers in turn
 // ===========================================================================
 template <int L>
-__global__ void __launch_bounds__(128) k_node_t(Dev d, const int *kbas, int init_only) {
+__global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int init_only) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.NKN) return;
   const int NLV = d.NLV, I = NLV + 1;
