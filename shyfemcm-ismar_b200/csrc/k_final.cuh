@@ -147,4 +147,107 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
   if (bad) set_status(&d.out[en.w], SHY_EDEPTH);
 }
 
+// ===========================================================================
+// k_final_w: k_final_t without Coriolis, with the layer arrays of a warp's
+// 32 element columns (one contiguous run of 32*NLV values, since a column
+// is contiguous and the elements are consecutive) moved between global and
+// shared memory by the whole warp in coalesced passes; each thread then
+// works its own column in shared memory as k_final_t does.
+// ===========================================================================
+template <int L>
+__global__ void __launch_bounds__(128) k_final_w(Dev d, int init_only) {
+  __shared__ float sb[4][5][32 * L];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w0 = (blockIdx.x * 4 + warp) * 32;         // first element of this warp
+  if (w0 >= d.NEL) return;                              // whole warps only
+  const int nw = min(32, d.NEL - w0);
+  const int NLV = d.NLV, cnt = nw * NLV;
+  const size_t base = (size_t)w0 * NLV;
+  float *bA = sb[warp][0], *bU = sb[warp][1], *bV = sb[warp][2], *bUo = sb[warp][3], *bVo = sb[warp][4];
+  const bool valid = lane < nw;
+  const int e = w0 + (valid ? lane : 0);
+  const int4 en = d.enode[e];
+  const BasinPar &P = d.par[en.w];
+  const int kn[3] = {en.x, en.y, en.z};
+  const int ilevel = d.ilhv[e];
+  const int ol = lane * NLV;                            // this thread's column in the buffers
+  const float *evp = d.ev8 + (size_t)e * 8;
+  double zn3[3];
+#pragma unroll
+  for (int ii = 0; ii < 3; ii++) zn3[ii] = d.zn[kn[ii]];
+  if (!init_only) {
+    for (int j = lane; j < cnt; j += 32) {
+      bA[j] = d.ddx[base + j];
+      bU[j] = d.un[base + j];
+      bV[j] = d.vn[base + j];
+      bUo[j] = d.uo[base + j];
+      bVo[j] = d.vo[base + j];
+    }
+    __syncwarp();
+    if (valid) {
+      const double beta = P.dt * (double)P.grav * P.am;
+      double bz = 0., cz = 0.;
+#pragma unroll
+      for (int ii = 0; ii < 3; ii++) {
+        const double dz = zn3[ii] - (double)d.zeo[3 * e + ii];
+        bz += dz * evp[ii];
+        cz += dz * evp[3 + ii];
+      }
+      const double az = P.az;
+      double um = 0., vm = 0.;
+      for (int l = 0; l < NLV; l++) {
+        const bool act = l < ilevel;
+        double u = 0., v = 0.;
+        if (act) {
+          const double re = bA[ol + l];
+          const double du = beta * (re * bz);
+          const double dv = beta * (re * cz);
+          u = (double)(float)((double)bU[ol + l] - du);
+          v = (double)(float)((double)bV[ol + l] - dv);
+          bU[ol + l] = (float)u;
+          bV[ol + l] = (float)v;
+        }
+        // az*U^{n+1} + (1-az)*U^n for hydro_vertical, conzstab and conz3d
+        bUo[ol + l] = act ? (float)(az * u + (1. - az) * (double)bUo[ol + l]) : 0.f;
+        bVo[ol + l] = act ? (float)(az * v + (1. - az) * (double)bVo[ol + l]) : 0.f;
+        um += u; vm += v;
+      }
+      d.unv[e] = (float)um;
+      d.vnv[e] = (float)vm;
+    }
+    __syncwarp();
+    for (int j = lane; j < cnt; j += 32) {
+      d.un[base + j] = bU[j];
+      d.vn[base + j] = bV[j];
+      d.usv[base + j] = bUo[j];
+      d.vsv[base + j] = bVo[j];
+    }
+    __syncwarp();
+  }
+  // setzev and the element part of setdepth (z-layers or pure sigma layers)
+  if (valid) {
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) d.zen[3 * e + ii] = (float)zn3[ii];
+    const float4 hm = d.hm3v[e];
+    const double zmed = (zn3[0] + zn3[1] + zn3[2]) / 3.;
+    const float *hld = d.hldv + (size_t)en.w * NLV;
+    const float *hlv = d.hlv + (size_t)en.w * NLV;
+    bool bad = false;
+    for (int l = 0; l < NLV; l++) {
+      double h = 0.;
+      if (l < ilevel) {
+        if (P.nsigma > 0) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // :1079-1083
+        else if (ilevel == 1) h = hm.w + zmed;
+        else if (l < ilevel - 1) h = (double)hld[l] + (l == 0 ? zmed : 0.);
+        else h = (double)hm.w - hlv[ilevel - 2];
+        if (!(h > 0.)) bad = true;
+      }
+      bA[ol + l] = (float)h;
+    }
+    if (bad) set_status(&d.out[en.w], SHY_EDEPTH);
+  }
+  __syncwarp();
+  for (int j = lane; j < cnt; j += 32) d.hen[base + j] = bA[j];
+}
+
 }  // namespace shy

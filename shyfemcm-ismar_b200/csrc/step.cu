@@ -92,9 +92,13 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
     return;
   }
   if (which == 1 && d.col_threads && d.NLV <= 16) {
-    const int blocks = (d.NEL + 255) / 256;
-    if (cor) k_final_t<true><<<blocks, 256, 0, st>>>(d, init_only);
-    else k_final_t<false><<<blocks, 256, 0, st>>>(d, init_only);
+    if (cor) {
+      k_final_t<true><<<(d.NEL + 255) / 256, 256, 0, st>>>(d, init_only);
+    } else {
+      const int blocks = (d.NEL + 127) / 128;            // 4 warps of 32 elements
+      if (d.NLV <= 8) k_final_w<8><<<blocks, 128, 0, st>>>(d, init_only);
+      else k_final_w<16><<<blocks, 128, 0, st>>>(d, init_only);
+    }
     return;
   }
   switch (d.S) {
