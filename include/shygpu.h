@@ -101,6 +101,8 @@ typedef struct shy_params {
   int32_t nsigma;            /* sigma layers (levels :: nsigma): 0 z-layers, */
                              /*   nlv pure sigma (hlv/hldv sigma values < 0) */
   float hsigma;              /* depth limit of the sigma layers (hsigma)    */
+  int32_t wetdry;            /* 1: wetting and drying of elements (setweg) */
+  float hzmin, hzon, volmin; /* its thresholds       def_para.f90:744-746,1762 */
 } shy_params;
 
 /* Host views of one basin's state, reference layouts.  NULL members are

@@ -443,6 +443,10 @@ struct Model {
   std::vector<double> rfricv, fxv, fyv, ddxv, ddyv;
   std::vector<double> c2coo, rvec2d;
   double dtime = 0.;
+  // wetting and drying (mod_geom_dynamic :: iwegv, iwetv, inodv)
+  std::vector<int> iwegv, iwetv, inodv;
+  std::vector<double> uov, vov;             // barotropic transports of the old level
+  double dtime_weg = -1.;                   // setweg's dtime_old
   shy_step_info info{};
   // solver controls
   double rtol = 1e-8, atol = 1e-8;
@@ -887,6 +891,20 @@ void element_system(Model &m, int ie, int kn[3], double hia[3][3], double hik[3]
       hik[i] = rw * hia[i][i];
     }
   }
+  if (m.p.wetdry && m.iwegv[ie] != 0) {       // excluded (dry) element (:710-727)
+    const double hh999 = aj * 12.;
+    for (int n = 0; n < 3; n++) {
+      for (int mm = 0; mm < 3; mm++) hia[n][mm] = hh999 * (b[n] * b[mm] + c[n] * c[mm]);
+      hik[n] = 0.;
+    }
+    for (int n = 0; n < 3; n++) {
+      const int in = m.inodv[kn[n]];
+      if (in != 0 && in != -2) {              // iskbnd: boundary of the wet domain
+        for (int mm = 0; mm < 3; mm++) hia[n][mm] = 0.;
+        hik[n] = 0.;
+      }
+    }
+  }
 }
 
 void hydro_zeta_assemble(Model &m) {
@@ -901,7 +919,8 @@ void hydro_zeta_assemble(Model &m) {
       m.rvec2d[kn[i]] += hik[i];
     }
   }
-  for (int k = 0; k < m.nkn; k++) m.rvec2d[k] += m.p.dt * m.rqv[k];
+  for (int k = 0; k < m.nkn; k++)             // adjust_mass_flux: none out of the system
+    if (!(m.p.wetdry && m.inodv[k] == -2)) m.rvec2d[k] += m.p.dt * m.rqv[k];
 }
 
 int zeta_solve(Model &m) {    // system_solve -> spk_solve_system (sparskit_admin.f90:115-334)
@@ -1252,10 +1271,241 @@ int scal3sh(Model &m, std::vector<double> &cnv, double rkpar, bool is_temp,
   return SHY_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Wetting and drying of elements on z-layers (wetdry.f90, topo_update.f90,
+// bnd_routines.f90), used when the basin asks for it (shy_params::wetdry).
+// ---------------------------------------------------------------------------
+// setweg (wetdry.f90:128-345): iweich 0 first call (sets the minimum depth),
+// 1 take away below hzmin (the hydro loop repeats), 2 take away below hzoff,
+// 3 add back where the depth reached hzon.  Returns the number of changes.
+int setweg(Model &m, int iweich, double dtime) {
+  const double hzmin = m.p.hzmin, hzoff = m.p.hzoff, hzon = m.p.hzon, volmin = m.p.volmin;
+  const int iwait = 5;                       // :176
+  const bool bsigma = m.p.nsigma > 0;
+  const bool bnewtime = dtime != m.dtime_weg;
+  int iwh = 0;
+  if (bsigma && iweich >= 1) return 0;       // :220
+  if (iweich == 0) {
+    for (int ie = 0; ie < m.nel; ie++) {
+      const double aomega = m.ev[(size_t)ie * SHY_EVDIM + 9];
+      double zmin = hzmin + volmin / (4. * aomega);
+      if (zmin > hzoff) zmin = hzmin + 0.5 * (hzmin + hzoff);
+      int iweg = 0;
+      for (int ii = 0; ii < 3; ii++) {
+        const double hzg = m.zenv[3 * ie + ii] + m.hm3v[3 * ie + ii];
+        if (hzg < hzoff) iweg++;
+        if (hzg < zmin) {
+          m.zenv[3 * ie + ii] = zmin - m.hm3v[3 * ie + ii];
+          if (bsigma) m.znv[m.nen3v[3 * ie + ii]] = m.zenv[3 * ie + ii];
+        }
+      }
+      if (bsigma) iweg = 0;
+      m.iwegv[ie] = iweg;
+      if (iweg == 0) m.iwetv[ie] = 1;
+      if (iweg > 0) iwh++;
+    }
+  } else if (iweich == 1 || iweich == 2) {
+    const double hzlim = iweich == 1 ? hzmin : hzoff;
+    for (int ie = 0; ie < m.nel; ie++) {
+      if (m.iwegv[ie] != 0) continue;
+      int iweg = 0;
+      for (int ii = 0; ii < 3; ii++)
+        if (m.znv[m.nen3v[3 * ie + ii]] + m.hm3v[3 * ie + ii] < hzlim) iweg++;
+      if (iweg > 0) {
+        iwh++;
+        m.iwetv[ie] = 0;
+        m.iwegv[ie] = iweg;
+      }
+    }
+  } else if (iweich == 3) {
+    for (int ie = 0; ie < m.nel; ie++) {
+      if (m.iwegv[ie] <= 0) continue;
+      int iweg = 0;
+      double hztot = 0.;
+      for (int ii = 0; ii < 3; ii++) {
+        const double hzg = m.znv[m.nen3v[3 * ie + ii]] + m.hm3v[3 * ie + ii];
+        hztot += hzg;
+        if (hzg < hzon) iweg++;
+      }
+      hztot /= 3.;
+      if (hztot >= hzon && -m.iwetv[ie] > iwait) iweg = 0;     // new algorithm (:306-312)
+      if (iweg == 0) {
+        iwh++;
+        m.iwetv[ie] = 0;
+        m.iwegv[ie] = 0;
+      }
+    }
+  }
+  for (int ie = 0; ie < m.nel; ie++)          // :322-331
+    if (bnewtime || m.iwetv[ie] == 0) m.iwetv[ie] += m.iwegv[ie] == 0 ? 1 : -1;
+  m.dtime_weg = dtime;
+  return iwh;
+}
+
+// setnod (topo_update.f90:166-260): 0 internal, > 0 open boundary, -1
+// boundary of the wet domain, -2 out of the system; from the angles of the
+// wet elements around each node
+int setnod(Model &m) {
+  std::vector<double> winkv(m.nkn, 0.);
+  for (int ie = 0; ie < m.nel; ie++)
+    if (m.iwegv[ie] == 0)
+      for (int ii = 0; ii < 3; ii++) winkv[m.nen3v[3 * ie + ii]] += m.ev[(size_t)ie * SHY_EVDIM + 10 + ii];
+  for (int k = 0; k < m.nkn; k++) {
+    if (winkv[k] > 359.99) m.inodv[k] = 0;
+    else if (winkv[k] == 0.) m.inodv[k] = -2;
+    else m.inodv[k] = -1;
+  }
+  for (int k = 0; k < m.nkn; k++)            // level boundaries (ibtyp 1)
+    if (m.bnd[k] > 0) {
+      if (m.inodv[k] != -1) return fail(SHY_EDEPTH, "setnod: error for open boundary node (dry boundary)");
+      m.inodv[k] = m.bnd[k];
+    }
+  return SHY_OK;
+}
+
+// setznv (wetdry.f90:619-712): nodal levels from the wet elements' vertex
+// levels (the larger where they differ), area-weighted from the dry ones
+// where a node has no wet element
+void setznv(Model &m) {
+  std::vector<double> v1(m.nkn, 0.), v2(m.nkn, 0.);
+  std::vector<char> set(m.nkn, 0);
+  for (int ie = 0; ie < m.nel; ie++) {
+    if (m.iwegv[ie] == 0) {
+      for (int ii = 0; ii < 3; ii++) {
+        const int k = m.nen3v[3 * ie + ii];
+        double z = m.zenv[3 * ie + ii];
+        if (set[k] && m.znv[k] != z) z = std::max(z, m.znv[k]);
+        m.znv[k] = z;
+        set[k] = 1;
+      }
+    } else {
+      const double area = 4. * m.ev[(size_t)ie * SHY_EVDIM + 9];
+      for (int ii = 0; ii < 3; ii++) {
+        const int k = m.nen3v[3 * ie + ii];
+        v1[k] += m.zenv[3 * ie + ii] * area;
+        v2[k] += area;
+      }
+    }
+  }
+  for (int k = 0; k < m.nkn; k++)
+    if (!set[k]) m.znv[k] = v1[k] / v2[k];
+}
+
+// setuvd (wetdry.f90:350-590): level and barotropic transport of each dry
+// element, the element's volume kept, no vertex below hzmin
+int setuvd(Model &m) {
+  const double dt = m.p.dt, hzmin = m.p.hzmin, az = m.p.azpar, azt = 1. - az, eps = 1.e-5;
+  for (int ie = 0; ie < m.nel; ie++) {
+    if (m.iwegv[ie] <= 0) continue;
+    const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+    const double uo = m.uov[ie], vo = m.vov[ie];
+    const double axdt = 3. * dt, adt = 1. / axdt;
+    double zn[3], b[3], c[3], z[3], h[3];
+    double zm = 0.;
+    for (int ii = 0; ii < 3; ii++) {
+      zn[ii] = m.zenv[3 * ie + ii];
+      zm += zn[ii];
+      b[ii] = e[3 + ii]; c[ii] = e[6 + ii];
+      h[ii] = m.hm3v[3 * ie + ii];
+    }
+    const double zmed = zm / 3.;
+    int itot = 0, isum = 0;
+    for (int ii = 0; ii < 3; ii++) {
+      if (zmed + h[ii] < hzmin) { z[ii] = hzmin - h[ii]; itot++; isum += ii + 1; }
+      else z[ii] = zmed;
+      zm -= z[ii];
+    }
+    if (itot == 1) {
+      const int i1 = isum % 3, i2 = (i1 + 1) % 3, is = isum - 1;    // 0-based mod(isum,3)+1 etc.
+      if (z[i1] + zm * 0.5 + h[i1] < hzmin) {
+        z[i1] = hzmin - h[i1];
+        z[i2] = 3. * zmed - z[i1] - z[is];
+      } else if (z[i2] + zm * 0.5 + h[i2] < hzmin) {
+        z[i2] = hzmin - h[i2];
+        z[i1] = 3. * zmed - z[i2] - z[is];
+      } else {
+        z[i1] += 0.5 * zm;
+        z[i2] += 0.5 * zm;
+      }
+    } else if (itot == 2) {
+      const int i1 = 6 - isum - 1;
+      z[i1] += zm;
+    } else if (itot == 3) {
+      return fail(SHY_EDEPTH, "setuvd: z computation");
+    }
+    zm = 0.;
+    for (int ii = 0; ii < 3; ii++) {
+      zm += z[ii];
+      if (z[ii] + h[ii] < hzmin - eps) return fail(SHY_EDEPTH, "setuvd: z computation");
+    }
+    if (std::fabs(zm - 3. * zmed) > eps) return fail(SHY_EDEPTH, "setuvd: z computation");
+    double d1 = (z[0] - zn[0]) * adt - azt * (b[0] * uo + c[0] * vo);
+    double d2 = (z[1] - zn[1]) * adt - azt * (b[1] * uo + c[1] * vo);
+    double det = 1. / (b[0] * c[1] - b[1] * c[0]);
+    double u = det * (c[1] * d1 - c[0] * d2);
+    double v = det * (-b[1] * d1 + b[0] * d2);
+    itot = 0;
+    for (int ii = 0; ii < 3; ii++) {
+      const double zz = axdt * (b[ii] * (azt * uo + az * u) + c[ii] * (azt * vo + az * v)) + zn[ii];
+      if (zz + h[ii] < hzmin - eps) itot++;
+    }
+    if (itot > 0) {                          // a node is drying: the velocity that keeps z
+      if (az == 0.) return fail(SHY_EARG, "setuvd: drying with az=0 not possible");
+      d1 = (z[0] - zn[0]) * adt - azt * (b[0] * uo + c[0] * vo);
+      d2 = (z[1] - zn[1]) * adt - azt * (b[1] * uo + c[1] * vo);
+      det = 1. / (az * (b[0] * c[1] - b[1] * c[0]));
+      u = det * (c[1] * d1 - c[0] * d2);
+      v = det * (-b[1] * d1 + b[0] * d2);
+    }
+    itot = 0;
+    zm = 0.;
+    for (int ii = 0; ii < 3; ii++) {
+      const double zz = axdt * (b[ii] * (azt * uo + az * u) + c[ii] * (azt * vo + az * v)) + zn[ii];
+      if (zz + h[ii] < hzmin - eps) itot++;
+      m.zenv[3 * ie + ii] = zz;
+      zm += zz;
+    }
+    if (std::fabs(zm - 3. * zmed) > eps) return fail(SHY_EDEPTH, "setuvd: z computation");
+    if (itot > 0) return fail(SHY_EDEPTH, "setuvd: u/v computation");
+    m.unv[ie] = u;
+    m.vnv[ie] = v;
+  }
+  return SHY_OK;
+}
+
+// baro2l (transforms.f90:437-480): the barotropic transport of each dry
+// element spread over its layers by their thickness
+void baro2l(Model &m) {
+  if (m.p.nsigma > 0) return;
+  for (int ie = 0; ie < m.nel; ie++) {
+    if (m.iwegv[ie] <= 0) continue;
+    const int ilevel = m.ilhv[ie];
+    double htot = 0.;
+    for (int l = 1; l <= ilevel; l++) htot += m.hdenv[(size_t)ie * m.nlv + l - 1];
+    for (int l = 1; l <= ilevel; l++) {
+      const double weight = m.hdenv[(size_t)ie * m.nlv + l - 1] / htot;
+      m.utlnv[(size_t)ie * m.nlv + l - 1] = m.unv[ie] * weight;
+      m.vtlnv[(size_t)ie * m.nlv + l - 1] = m.vnv[ie] * weight;
+    }
+  }
+}
+
 int init_state(Model &m) {
   m.zenv.assign((size_t)3 * m.nel, 0.);
   for (int ie = 0; ie < m.nel; ie++)
     for (int ii = 0; ii < 3; ii++) m.zenv[3 * ie + ii] = m.znv[m.nen3v[3 * ie + ii]];
+  m.iwegv.assign(m.nel, 0); m.iwetv.assign(m.nel, 0); m.inodv.assign(m.nkn, 0);
+  m.dtime_weg = -1.;
+  if (m.p.wetdry) {                          // sp111 init: setweg(0) and setznv (bnd_routines.f90:413-415)
+    setweg(m, 0, m.dtime);
+    setznv(m);
+  }
+  m.unv.assign(m.nel, 0.); m.vnv.assign(m.nel, 0.);
+  for (int ie = 0; ie < m.nel; ie++)
+    for (int l = 0; l < m.ilhv[ie]; l++) {
+      m.unv[ie] += m.utlnv[(size_t)ie * m.nlv + l];
+      m.vnv[ie] += m.vtlnv[(size_t)ie * m.nlv + l];
+    }
   int st = setdepth(m, m.hdknv, m.hdenv, m.zenv);
   if (st) return st;
   m.zov = m.znv; m.zeov = m.zenv; m.utlov = m.utlnv; m.vtlov = m.vtlnv;
@@ -1269,12 +1519,17 @@ int init_state(Model &m) {
 }
 
 int step(Model &m) {
+  if (m.p.wetdry) {                          // set_dry (shyfem_subs.f90:578) at the old time
+    setweg(m, 2, m.dtime);
+    setweg(m, 3, m.dtime);
+  }
   // copy_uvz + copy_depth (transforms.f90:523; shyfem_subs.f90:589-591)
   m.dtime += m.p.dt;
   m.zov = m.znv; m.zeov = m.zenv; m.utlov = m.utlnv; m.vtlov = m.vtlnv;
+  m.uov = m.unv; m.vov = m.vnv;
   m.hdkov = m.hdknv; m.hdeov = m.hdenv;
   set_rzv(m);                                     // sp111(2)
-  // hydro (hydrodynamic.f90:284-485), no wet/dry loop
+  // hydro (hydrodynamic.f90:284-485)
   int st = bottom_friction(m);
   if (st) return st;
   set_explicit(m);
@@ -1284,12 +1539,28 @@ int step(Model &m) {
     st = hydro_intern(m, ie);
     if (st) return st;
   }
-  hydro_zeta_assemble(m);
-  st = zeta_solve(m);
-  if (st) return st;
+  int krylov = 0;
+  for (;;) {                                      // the loop over a changing domain (:374-404)
+    if (m.p.wetdry) {
+      st = setnod(m);
+      if (st) return st;
+    }
+    hydro_zeta_assemble(m);
+    st = zeta_solve(m);
+    if (st) return st;
+    krylov += m.info.krylov_iters;
+    if (!m.p.wetdry || setweg(m, 1, m.dtime) == 0) break;
+  }
+  m.info.krylov_iters = krylov;
   hydro_transports_final(m);
-  for (int ie = 0; ie < m.nel; ie++)              // setzev
-    for (int ii = 0; ii < 3; ii++) m.zenv[3 * ie + ii] = m.znv[m.nen3v[3 * ie + ii]];
+  for (int ie = 0; ie < m.nel; ie++)              // setzev: elements in the system
+    if (!m.p.wetdry || m.iwegv[ie] == 0)
+      for (int ii = 0; ii < 3; ii++) m.zenv[3 * ie + ii] = m.znv[m.nen3v[3 * ie + ii]];
+  if (m.p.wetdry) {
+    st = setuvd(m);
+    if (st) return st;
+    baro2l(m);
+  }
   st = setdepth(m, m.hdknv, m.hdenv, m.zenv);     // make_new_depth
   if (st) return st;
   hydro_vertical(m);
@@ -1477,6 +1748,17 @@ int shyref_run(void *h, int nsteps) {
     int st = step(m);
     if (st) return st;
   }
+  return SHY_OK;
+}
+
+// wet/dry state: iwegv (nel), iwetv (nel), inodv (nkn); any may be NULL
+int shyref_wetdry(void *h, int *iwegv, int *iwetv, int *inodv) {
+  Model *m = (Model *)h;
+  for (int ie = 0; ie < m->nel; ie++) {
+    if (iwegv) iwegv[ie] = m->iwegv.empty() ? 0 : m->iwegv[ie];
+    if (iwetv) iwetv[ie] = m->iwetv.empty() ? 0 : m->iwetv[ie];
+  }
+  if (inodv) for (int k = 0; k < m->nkn; k++) inodv[k] = m->inodv.empty() ? 0 : m->inodv[k];
   return SHY_OK;
 }
 

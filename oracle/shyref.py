@@ -167,6 +167,17 @@ class OracleModel:
         check(lib.shyref_get_state64(self.h, *[dptr(out[k]) for k in order]), "get_state")
         return out
 
+    def wetdry(self):
+        """(iwegv, iwetv, inodv): dry-element marks, their counters, node kinds."""
+        c = self.case
+        iweg = np.zeros(c["nel"], np.int32)
+        iwet = np.zeros(c["nel"], np.int32)
+        inod = np.zeros(c["nkn"], np.int32)
+        i32 = C.POINTER(C.c_int)
+        lib.shyref_wetdry(self.h, iweg.ctypes.data_as(i32), iwet.ctypes.data_as(i32),
+                          inod.ctypes.data_as(i32))
+        return iweg, iwet, inod
+
     def last_system(self):
         nnz = C.c_int(0)
         lib.shyref_last_system(self.h, C.byref(nnz), None, None)

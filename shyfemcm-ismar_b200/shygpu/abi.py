@@ -49,6 +49,7 @@ class ShyParams(C.Structure):
         ("istot_max", C.c_int32),
         ("solver_rtol", C.c_float), ("solver_atol", C.c_float), ("solver_maxit", C.c_int32),
         ("nsigma", C.c_int32), ("hsigma", C.c_float),
+        ("wetdry", C.c_int32), ("hzmin", C.c_float), ("hzon", C.c_float), ("volmin", C.c_float),
     ]
 
 
@@ -129,6 +130,10 @@ def make_params(case, **over):
     s.solver_maxit = int(p.get("solver_maxit", 1000))
     s.nsigma = int(p.get("nsigma", 0))
     s.hsigma = float(p.get("hsigma", 10000.0))
+    s.wetdry = int(p.get("wetdry", 0))
+    s.hzmin = float(p.get("hzmin", 0.01))
+    s.hzon = float(p.get("hzon", 0.10))
+    s.volmin = float(p.get("volmin", 1.0))
     return s
 
 

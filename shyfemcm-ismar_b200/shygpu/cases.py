@@ -248,6 +248,35 @@ def lagoon_case(nkn_target=3000, lx=12.0e3, ly=6.0e3, seed=7, dt=30.0, nlv=30, n
     return _finish(case)
 
 
+def flat_case(nx=41, ny=9, lx=8.0e3, ly=1.6e3, seed=9, dt=60.0, nlv=1, ampli=1.0,
+              hdeep=3.0, hshallow=-0.6):
+    """Tidal flat for wetting and drying: a channel deepening linearly from
+    `hshallow` (negative: land above the rest level) at the closed end to
+    `hdeep` at the open boundary, M2 of `ampli`, `nlv` z-layers of 1 m
+    (the last one reaching the bottom).  The flat dries at low water and
+    floods at high water (setweg)."""
+    x, y, nen3v, ii, jj = structured_triangles(nx, ny, lx, ly, 0.2, seed)
+    rng = np.random.default_rng(seed + 505)
+    nkn, nel = x.size, nen3v.shape[0]
+    h = hdeep + (hshallow - hdeep) * x / lx + _smooth_field(x, y, rng, scale=0.15)
+    hm3v = h[nen3v - 1]
+    if nlv == 1:
+        hlv, hldv = np.array([1.0e4]), np.array([1.0e4])
+        ilhv = np.ones(nel, np.int32)
+        ilhkv = np.ones(nkn, np.int32)
+    else:
+        hlv, hldv = z_layers(np.ones(nlv))
+        hlv[-1] = max(hlv[-1], h.max() + 1.0)
+        ilhv, ilhkv = layer_counts(nen3v, np.maximum(hm3v, 0.1), hlv, hldv, nkn)
+    bnd = np.zeros(nkn, np.int32)
+    bnd[ii == 0] = 1
+    tide = np.array([[[ampli, M2_PERIOD, -M2_PERIOD / 4.0, 0.0]]], np.float32)   # start at low water
+    case = dict(name=f"flat_{nkn}x{nlv}", nkn=nkn, nel=nel, nlv=nlv, nen3v=nen3v,
+                xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
+                bnd_index=bnd, tide=tide, seed=seed, params=dict(dt=dt, wetdry=1))
+    return _finish(case)
+
+
 def ensemble_cases(n, nkn_lo=5000, nkn_hi=100000, nlv=10, seed=4, dt=60.0, first=None):
     """Independent basins with log-uniform node counts and seeded aspect
     ratios and wind perturbations (sigma = 3 m/s).  `first` builds only the
