@@ -182,6 +182,13 @@ int shygpu_new_step(shygpu_model *model);
 int shygpu_hydro(shygpu_model *model);
 int shygpu_scalar(shygpu_model *model);
 
+/* Wetting and drying state of basin ib (mod_geom_dynamic): per element the
+ * number of its vertices that took it out of the system (0: in it) and its
+ * wet/dry step counter (iwetv), per node 0 internal, > 0 open boundary, -1
+ * boundary of the wet domain, -2 out of the system (inodv, as of the last
+ * solve).  Zeros for a model without wetting and drying.                 */
+int shygpu_get_wetdry(shygpu_model *model, int32_t ibasin, int32_t *iwegv,
+                      int32_t *iwetv, int32_t *inodv);
 int shygpu_step_info(shygpu_model *model, int32_t ibasin, shy_step_info *info);
 
 /* Per-step forcing of a basin from host memory (pinned for overlap):

@@ -583,7 +583,8 @@ int setdepth(Model &m, std::vector<double> &hdkn, std::vector<double> &hden,
     }
     for (int l = lmin; l <= lmax; l++)
       if (hden[(size_t)ie * nlv + l - 1] <= 0.)
-        return fail(SHY_EDEPTH, "setdepth: no layer depth in element");
+        return fail(SHY_EDEPTH, "setdepth: no layer depth in element " + std::to_string(ie + 1) +
+                                    " layer " + std::to_string(l));
   }
   for (int k = 0; k < m.nkn; k++) {
     for (int l = 1; l <= m.ilhkv[k]; l++) {

@@ -41,6 +41,8 @@ struct BasinPar {
   int is_temp[kMaxScal];      // scalar s is temperature (no clipping at 1e-15)
   int nsigma;                 // 0: z-layers; nlv: pure sigma layers
   float hsigma;               // depth limit of the sigma layers
+  int wetdry;                 // wetting and drying of elements (z-layers)
+  float hzmin, hzon, volmin;  // its thresholds
 };
 
 // per-basin results of the last step (device memory)
@@ -59,6 +61,7 @@ struct BasinOut {
 struct Dev {
   int nbasin, NKN, NEL, NLV, S, nsc_max;
   int col_threads;              // column kernel: 1 one thread per column, 0 one warp segment
+  int any_wd;                   // some basin has wetting and drying (thread-per-column forms)
   BasinPar *par;
   BasinOut *out;
   // mesh (static)
@@ -86,6 +89,12 @@ struct Dev {
                               //  node of the next vertex, node of the one after}
   double *val64, *rhs64, *x64;
   float *val32, *dinv32, *r32, *p32, *q32, *z32, *e32, *s32, *t32, *rh32, *v32;
+  // wetting and drying: per element the number of dry vertices (0: in the
+  // system) and the wet/dry step counter; per node its kind (0 internal,
+  // > 0 open boundary, -1 boundary of the wet domain, -2 out of the system)
+  // and whether its full fan of elements closes (360 degrees)
+  int *iweg, *iwet, *inod;
+  unsigned char *kfull;
   float4 *cg4[2];                 // device-wide CG: {r, w = A D^-1 r, s, 1/diag} per row, two generations
   float2 *cg2;                    // device-wide CG: {p, e} per row
   // element system written by the column kernel (SoA): hia[c*NEL+e], hik[c*NEL+e]

@@ -258,6 +258,7 @@ struct shygpu_model {
   int nbasin = 0, NKN = 0, NEL = 0, NLV = 0, S = 1, nsc_max = 0, NNZ = 0;
   bool cor = false;
   bool has_rho = false;              // some basin updates rho' from transported T and S
+  bool any_wd = false;               // some basin has wetting and drying
   std::vector<BasinPar> par;
   std::vector<int> nlv_b;
   Arena arena;
@@ -722,6 +723,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: nsigma=%d: z-layers (0) or pure sigma layers (nlv) only", b, Pp[b].nsigma));
     if (Pp[b].nsigma > 0 && Pp[b].ibarcl > 0)
       return bail(fail(SHY_EARG, "basin %d: baroclinic terms on sigma layers not supported", b));
+    if (Pp[b].wetdry && !(Pp[b].hzmin > 0.f && Pp[b].hzoff >= Pp[b].hzmin && Pp[b].hzon >= Pp[b].hzoff))
+      return bail(fail(SHY_EARG, "basin %d: wetting and drying needs 0 < hzmin <= hzoff <= hzon", b));
     NLV = std::max(NLV, bs.nlv);
   }
   m->nbasin = nbasin; m->NLV = NLV; m->S = next_pow2(NLV);
@@ -735,6 +738,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   std::vector<float> ev8((size_t)8 * NEL), czv(NEL), fcorv(NEL), wdif((size_t)9 * NEL);
   std::vector<float4> hm3v(NEL);
   std::vector<int> ilhv(NEL), ilhkv(NKN), ieltv((size_t)3 * NEL), kbnd(NKN), kbas(NKN);
+  std::vector<unsigned char> kfull(NKN, 0);
   std::vector<float> difhv((size_t)NEL * NLV, 1.f);
   std::vector<float> visv((size_t)NKN * (NLV + 1), 0.f), difv((size_t)NKN * (NLV + 1), 0.f);
   std::vector<float> taux(NKN), tauy(NKN), ppv(NKN), rqv(NKN), areakv((size_t)NKN * NLV, 0.f);
@@ -753,6 +757,12 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     ST_TRY(compute_ev(nkn, nel, bs.nen3v, bs.xgv, bs.ygv, ev));
     std::vector<int> nv((size_t)3 * nel);
     for (size_t i = 0; i < nv.size(); i++) nv[i] = bs.nen3v[i] - 1;
+    {   // nodes whose fan of elements closes (angles sum to 360 degrees, setnod)
+      std::vector<double> wink(nkn, 0.);
+      for (int ie = 0; ie < nel; ie++)
+        for (int ii = 0; ii < 3; ii++) wink[nv[3 * ie + ii]] += (float)ev[(size_t)ie * SHY_EVDIM + 10 + ii];
+      for (int k = 0; k < nkn; k++) kfull[k0 + k] = wink[k] > 359.99 ? 1 : 0;
+    }
     for (int ie = 0; ie < nel; ie++) {
       const double *e = &ev[(size_t)ie * SHY_EVDIM];
       int ge = e0 + ie;
@@ -870,6 +880,9 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     bp.hzoff = p.hzoff; bp.ahpar = p.ahpar; bp.rstol = p.rstol > 0 ? p.rstol : 1.f;
     bp.ireib = p.ireib; bp.ibarcl = p.ibarcl;
     bp.nsigma = p.nsigma; bp.hsigma = p.hsigma > 0.f ? p.hsigma : 10000.f;
+    bp.wetdry = p.wetdry ? 1 : 0;
+    bp.hzmin = p.hzmin; bp.hzon = p.hzon; bp.volmin = p.volmin;
+    m->any_wd |= bp.wetdry != 0;
     bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
     int ns = 0;
     if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }
@@ -893,12 +906,17 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     m->has_rho |= m->par[b].ibarcl > 0 && m->par[b].itemp && m->par[b].isalt;
   m->NNZ = (int)col.size();
   if (m->cor) m->sym = 0;          // Coriolis makes the zeta system non-symmetric
+  if (m->any_wd) {
+    if (NLV > 16) return bail(fail(SHY_EARG, "wetting and drying: at most 16 layers"));
+    m->sym = 0;                    // a dry element's rows are not symmetric (hydrodynamic.f90:718-724)
+  }
 
   // ---- device upload ----
   Arena &A = m->arena;
   Dev &d = m->base;
   d.nbasin = nbasin; d.NKN = NKN; d.NEL = NEL; d.NLV = NLV; d.S = m->S; d.nsc_max = nsc_max;
   d.col_threads = 1;
+  d.any_wd = m->any_wd ? 1 : 0;
   ST_TRY(A.upload(&d.par, m->par) ? bail(SHY_ECAPACITY) : 0);
   std::vector<BasinOut> outs(nbasin);
   memset(outs.data(), 0, sizeof(BasinOut) * nbasin);
@@ -931,6 +949,9 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       A.alloc(&d.scr0, nsc_max > 0 ? NSC : 1) || A.alloc(&d.scr1, nsc_max > 0 ? NSC : 1) ||
       A.alloc(&d.imax, 1) || A.alloc(&d.subj, 1) || A.alloc(&d.nsub_launched, 1) ||
       A.alloc(&d.stab_node, 1))
+    return bail(SHY_ECAPACITY);
+  if (m->any_wd && (A.alloc(&d.iweg, NEL) || A.alloc(&d.iwet, NEL) || A.alloc(&d.inod, NKN) ||
+                    A.upload(&d.kfull, kfull)))
     return bail(SHY_ECAPACITY);
   for (int i = 0; i < 2; i++) {
     if (A.alloc(&m->zbuf[i], NKN) || A.alloc(&m->zebuf[i], (size_t)3 * NEL) ||
@@ -1068,6 +1089,9 @@ extern "C" int shygpu_set_state(shygpu_model *m, int32_t ib, const shy_state *s)
   const int c = m->cur;
   drop_graphs(m);
   CUDA_TRY(cudaMemsetAsync(&m->base.out[ib].steps, 0, sizeof(int), st));   // no earlier level yet
+  // a set-up of another basin derives this one's state too, and may have
+  // flagged it while its levels were still unset
+  CUDA_TRY(cudaMemsetAsync(&m->base.out[ib].status, 0, sizeof(int), st));
   if (s->znv) CUDA_TRY(cudaMemcpyAsync(m->zbuf[c] + bp.k0, s->znv, (size_t)bp.nk * 4, cudaMemcpyHostToDevice, st));
   if (s->utlnv) ST_TRY(copy_cols(m->ubuf[c], s->utlnv, bp.ne, nlv, NLV, bp.e0, true, st));
   if (s->vtlnv) ST_TRY(copy_cols(m->vbuf[c], s->vtlnv, bp.ne, nlv, NLV, bp.e0, true, st));
@@ -1086,6 +1110,10 @@ extern "C" int shygpu_set_state(shygpu_model *m, int32_t ib, const shy_state *s)
   // derived state: zenv (setzev), layer thickness (setdepth), rho (barocl(0))
   Dev d = dev_for_step(m, c);
   d.sc_in = m->scbuf[m->sc_cur];
+  if (m->any_wd) {                 // setweg(0) and setznv (bnd_routines.f90:413-415)
+    launch_wetdry(d, m->kbas, 1, ib, st);
+    launch_wetdry(d, m->kbas, 2, ib, st);
+  }
   launch_elem(d, 1, 1, st, m->cor);
   launch_node(d, m->kbas, 0, 1, 0, st);
   launch_reduce(d, m->nsub, 0, st);
@@ -1133,6 +1161,7 @@ extern "C" int shygpu_get_state(shygpu_model *m, int32_t ib, shy_state *s) {
 // the step
 // ---------------------------------------------------------------------------
 static int enqueue_hydro(shygpu_model *m, const Dev &d) {
+  if (m->any_wd) launch_wetdry(d, m->kbas, 0, -1, m->stream);    // set_dry
   launch_elem(d, 0, 0, m->stream, m->cor);
   ZetaArgs za{};
   za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
@@ -1169,7 +1198,7 @@ static int enqueue_scalar(shygpu_model *m, Dev d, int sc_cur, int *nconz) {
 
 // launches of one step apart from the transport sub-steps
 static int count_launches(const shygpu_model *m) {
-  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0) + (m->has_rho ? 1 : 0);
+  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0) + (m->has_rho ? 1 : 0) + (m->any_wd ? 1 : 0);
 }
 
 static int enqueue_step(shygpu_model *m) {
@@ -1358,6 +1387,7 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
     Dev d = dev_for_step(m, 1 - m->cur);
     int kind[32], n = 0;
     cudaEventRecord(ev[n], m->stream);
+    if (m->any_wd) launch_wetdry(d, m->kbas, 0, -1, m->stream);     // set_dry, timed with the column
     launch_elem(d, 0, 0, m->stream, m->cor); kind[n] = 0; cudaEventRecord(ev[++n], m->stream);
     ZetaArgs za{};
     za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
@@ -1395,6 +1425,22 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
   if (st) return st;
   CUDA_TRY(cudaGetLastError());
   return check_outputs(m);
+}
+
+extern "C" int shygpu_get_wetdry(shygpu_model *m, int32_t ib, int32_t *iwegv, int32_t *iwetv, int32_t *inodv) {
+  if (!m || ib < 0 || ib >= m->nbasin) return fail(SHY_EARG, "get_wetdry: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  if (!m->any_wd) {
+    if (iwegv) memset(iwegv, 0, sizeof(int32_t) * bp.ne);
+    if (iwetv) memset(iwetv, 0, sizeof(int32_t) * bp.ne);
+    if (inodv) memset(inodv, 0, sizeof(int32_t) * bp.nk);
+    return SHY_OK;
+  }
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  if (iwegv) CUDA_TRY(cudaMemcpy(iwegv, m->base.iweg + bp.e0, sizeof(int32_t) * bp.ne, cudaMemcpyDeviceToHost));
+  if (iwetv) CUDA_TRY(cudaMemcpy(iwetv, m->base.iwet + bp.e0, sizeof(int32_t) * bp.ne, cudaMemcpyDeviceToHost));
+  if (inodv) CUDA_TRY(cudaMemcpy(inodv, m->base.inod + bp.k0, sizeof(int32_t) * bp.nk, cudaMemcpyDeviceToHost));
+  return SHY_OK;
 }
 
 extern "C" int shygpu_step_info(shygpu_model *m, int32_t ib, shy_step_info *info) {

@@ -2,6 +2,7 @@
 // Included by step.cu (one translation unit).
 #pragma once
 #include "common.cuh"
+#include "k_wetdry.cuh"
 #include "physics.cuh"
 
 namespace shy {
@@ -90,10 +91,34 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
   const int ilevel = d.ilhv[e];
   const size_t o = (size_t)e * NLV;
   const float *evp = d.ev8 + (size_t)e * 8;
-  double zn3[3];
+  const float4 hm = d.hm3v[e];
+  const bool dry = wd_basin(P) && d.iweg[e] > 0;   // out of the system (wetting and drying)
+  double zn3[3], zv[3];
 #pragma unroll
-  for (int ii = 0; ii < 3; ii++) zn3[ii] = d.zn[kn[ii]];
-  if (!init_only) {
+  for (int ii = 0; ii < 3; ii++) { zn3[ii] = d.zn[kn[ii]]; zv[ii] = zn3[ii]; }
+  if (!init_only && dry) {
+    // setuvd: the element's new vertex levels and barotropic transport from
+    // continuity; baro2l: that transport over the layers by their thickness
+    double zo3[3], ub = 0., vb = 0.;
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) zo3[ii] = d.zeo[3 * e + ii];
+    if (!wd_setuvd(P, evp, hm, zo3, (double)d.unv[e], (double)d.vnv[e], zv, ub, vb))
+      set_status(&d.out[en.w], SHY_EDEPTH);
+    double htot = 0.;
+    for (int l = 0; l < ilevel; l++) htot += d.heo[o + l];
+    const double az = P.az;
+    for (int l = 0; l < NLV; l++) {
+      const bool act = l < ilevel;
+      const double w = act ? (double)d.heo[o + l] / htot : 0.;
+      const float u = (float)(ub * w), v = (float)(vb * w);
+      d.un[o + l] = u;
+      d.vn[o + l] = v;
+      d.usv[o + l] = act ? (float)(az * u + (1. - az) * (double)d.uo[o + l]) : 0.f;
+      d.vsv[o + l] = act ? (float)(az * v + (1. - az) * (double)d.vo[o + l]) : 0.f;
+    }
+    d.unv[e] = (float)ub;
+    d.vnv[e] = (float)vb;
+  } else if (!init_only) {
     const double beta = P.dt * (double)P.grav * P.am;
     double bz = 0., cz = 0.;
 #pragma unroll
@@ -124,12 +149,22 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
     }
     d.unv[e] = (float)um;
     d.vnv[e] = (float)vm;
-  }
-  // setzev and the element part of setdepth (z-layers or pure sigma layers)
+  } else {
+    // the initial state: barotropic transports; a dry element keeps the
+    // vertex levels the set-up gave it
+    double um = 0., vm = 0.;
+    for (int l = 0; l < ilevel; l++) { um += d.un[o + l]; vm += d.vn[o + l]; }
+    d.unv[e] = (float)um;
+    d.vnv[e] = (float)vm;
+    if (dry)
 #pragma unroll
-  for (int ii = 0; ii < 3; ii++) d.zen[3 * e + ii] = (float)zn3[ii];
-  const float4 hm = d.hm3v[e];
-  const double zmed = (zn3[0] + zn3[1] + zn3[2]) / 3.;
+      for (int ii = 0; ii < 3; ii++) zv[ii] = d.zen[3 * e + ii];
+  }
+  // setzev (elements in the system) and the element part of setdepth
+  // (z-layers or pure sigma layers) from the vertex levels
+#pragma unroll
+  for (int ii = 0; ii < 3; ii++) d.zen[3 * e + ii] = (float)zv[ii];
+  const double zmed = (zv[0] + zv[1] + zv[2]) / 3.;
   const float *hld = d.hldv + (size_t)en.w * NLV;
   const float *hlv = d.hlv + (size_t)en.w * NLV;
   bool bad = false;

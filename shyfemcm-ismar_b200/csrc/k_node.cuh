@@ -114,12 +114,14 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
     const size_t oe = (size_t)e * NLV;
     const double hbot = le >= 2 ? htot - hlv[le - 2] : 0.;
     hsig_h = htot;
+    // setdepth takes the element's vertex level (a dry element's differs)
+    const double ze = P.wetdry ? (double)d.zen[3 * e + ii] : z;
 #pragma unroll
     for (int l = 0; l < L; l++) {
       if (l >= le) break;
       double hl;
-      if (le == 1) hl = htot + z;
-      else if (l < le - 1) hl = (double)hld[l] + (l == 0 ? z : 0.);
+      if (le == 1) hl = htot + ze;
+      else if (l < le - 1) hl = (double)hld[l] + (l == 0 ? ze : 0.);
       else hl = hbot;
       hsum[l] += areafv * hl;
       if (!init_only) {

@@ -108,14 +108,14 @@ __device__ __forceinline__ void cluster_sum_w0(cg::cluster_group &cl, const floa
 // one row of the assembly: FP64 gather of the element entries of every slot
 // (element order), the rhs, the diagonal
 __device__ __forceinline__ void assemble_row(const Dev &d, const ZetaArgs &za, int i, float dtf,
-                                             double &diag, double &rhs) {
+                                             double &diag, double &rhs, bool wd = false) {
   diag = 0.;
   for (int s = d.rowptr[i]; s < d.rowptr[i + 1]; s++) {
     double v = 0.;
     for (int t = d.slot_ptr[s]; t < d.slot_ptr[s + 1]; t++) {
       const int src = d.slot_src[t];
       const int e = src / 9, c = src - 9 * e;
-      v += (double)za.hia[(size_t)c * za.cs + (size_t)e * za.es];
+      v += (double)__ldcg(&za.hia[(size_t)c * za.cs + (size_t)e * za.es]);
     }
     d.val64[s] = v;
     d.val32[s] = (float)v;
@@ -125,9 +125,11 @@ __device__ __forceinline__ void assemble_row(const Dev &d, const ZetaArgs &za, i
   for (int p = d.inc_ptr[i]; p < d.inc_ptr[i + 1]; p++) {
     const int q = d.inc[p];
     const int e = q / 3, ii = q - 3 * e;
-    rhs += (double)za.hik[(size_t)ii * za.cs + (size_t)e * za.es];
+    rhs += (double)__ldcg(&za.hik[(size_t)ii * za.cs + (size_t)e * za.es]);
   }
-  rhs += (double)(dtf * d.rqv[i]);
+  // adjust_mass_flux (bnd_routines.f90:1185-1210): with wetting and drying
+  // (wd) no flux enters a node out of the system
+  if (!(wd && d.inod[i] == -2)) rhs += (double)(dtf * d.rqv[i]);
   d.rhs64[i] = rhs;
 }
 

@@ -27,6 +27,9 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
 // which: 0 k_node(init_only=a), 1 k_stab, 2 k_conz(j=a, nsub=b), 3 k_rhoset
 void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStream_t st);
 void launch_reduce(const Dev &d, int nsub, int advance, cudaStream_t st);
+// wetting and drying: 0 set_dry at the step's start, 1 the initial state's
+// setweg(0) (and zenv from znv), 2 setznv; basin >= 0 limits 1 and 2 to it
+void launch_wetdry(const Dev &d, const int *kbas, int which, int basin, cudaStream_t st);
 void launch_subctl(const Dev &d, cudaGraphConditionalHandle h, cudaStream_t st);
 // shape of the shared-memory zeta solver: CL CTAs of `threads` per basin,
 // rows per CTA (capacity) and nonzeros per CTA (capacity), dynamic smem

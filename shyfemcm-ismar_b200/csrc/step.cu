@@ -37,6 +37,7 @@
 #include "k_node.cuh"
 #include "k_conz.cuh"
 #include "k_zeta.cuh"
+#include "k_wetdry.cuh"
 #include "k_zeta_global.cuh"
 #include "k_zeta_grid.cuh"
 
@@ -86,14 +87,16 @@ static void launch_column_t(const Dev &d, cudaStream_t st, bool cor) {
 }
 
 void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool cor) {
-  if (which == 0 && d.col_threads && d.NLV <= 16) {
+  const bool thr = (d.col_threads || d.any_wd) && d.NLV <= 16;
+  if (which == 0 && thr) {
     if (d.NLV <= 8) launch_column_t<8>(d, st, cor);
     else launch_column_t<16>(d, st, cor);
     return;
   }
-  if (which == 1 && d.col_threads && d.NLV <= 16) {
-    if (cor) {
-      k_final_t<true><<<(d.NEL + 255) / 256, 256, 0, st>>>(d, init_only);
+  if (which == 1 && thr) {
+    if (cor || d.any_wd) {
+      if (cor) k_final_t<true><<<(d.NEL + 255) / 256, 256, 0, st>>>(d, init_only);
+      else k_final_t<false><<<(d.NEL + 255) / 256, 256, 0, st>>>(d, init_only);
     } else {
       const int blocks = (d.NEL + 127) / 128;            // 4 warps of 32 elements
       if (d.NLV <= 8) k_final_w<8><<<blocks, 128, 0, st>>>(d, init_only);
@@ -112,7 +115,7 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
 }
 
 void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStream_t st) {
-  if (which == 0 && d.col_threads && d.NLV <= 16) {
+  if (which == 0 && (d.col_threads || d.any_wd) && d.NLV <= 16) {
     const int blocks = (d.NKN + 127) / 128;
     if (d.NLV <= 8) k_node_t<8><<<blocks, 128, 0, st>>>(d, kbas, a);
     else k_node_t<16><<<blocks, 128, 0, st>>>(d, kbas, a);
@@ -136,6 +139,12 @@ __global__ void k_subctl(Dev d, cudaGraphConditionalHandle h) {
   *d.subj = nj;
   *d.nsub_launched += 2;
   cudaGraphSetConditional(h, nj < *d.imax ? 1u : 0u);
+}
+
+void launch_wetdry(const Dev &d, const int *kbas, int which, int basin, cudaStream_t st) {
+  if (which == 0) k_wd_set<<<(d.NEL + 255) / 256, 256, 0, st>>>(d);
+  else if (which == 1) k_wd_init<<<(d.NEL + 255) / 256, 256, 0, st>>>(d, basin);
+  else k_wd_znv<<<(d.NKN + 255) / 256, 256, 0, st>>>(d, kbas, basin);
 }
 
 void launch_subctl(const Dev &d, cudaGraphConditionalHandle h, cudaStream_t st) {

@@ -73,6 +73,7 @@ def lib():
     L.shygpu_scalar.argtypes = [C.c_void_p]
     L.shygpu_new_step.argtypes = [C.c_void_p]
     L.shygpu_step_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyStepInfo)]
+    L.shygpu_get_wetdry.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3
     L.shygpu_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
     L.shygpu_get_option.argtypes = [C.c_void_p, C.c_char_p]
     L.shygpu_get_option.restype = C.c_double
@@ -171,6 +172,17 @@ class Model:
         i = abi.ShyStepInfo()
         check(lib().shygpu_step_info(self.h, ib, C.byref(i)), "step_info")
         return i
+
+    def wetdry(self, ib=0):
+        """(iwegv, iwetv, inodv) of basin ib: the element and node wet/dry
+        state as the reference's mod_geom_dynamic holds it."""
+        c = self.cases[ib]
+        iweg = np.zeros(c["nel"], np.int32)
+        iwet = np.zeros(c["nel"], np.int32)
+        inod = np.zeros(c["nkn"], np.int32)
+        check(lib().shygpu_get_wetdry(self.h, ib, iweg.ctypes.data, iwet.ctypes.data,
+                                      inod.ctypes.data), "get_wetdry")
+        return iweg, iwet, inod
 
     def nbytes(self):
         return lib().shygpu_model_bytes(self.h)

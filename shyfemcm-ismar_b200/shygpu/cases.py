@@ -252,9 +252,10 @@ def flat_case(nx=41, ny=9, lx=8.0e3, ly=1.6e3, seed=9, dt=60.0, nlv=1, ampli=1.0
               hdeep=3.0, hshallow=-0.6):
     """Tidal flat for wetting and drying: a channel deepening linearly from
     `hshallow` (negative: land above the rest level) at the closed end to
-    `hdeep` at the open boundary, M2 of `ampli`, `nlv` z-layers of 1 m
-    (the last one reaching the bottom).  The flat dries at low water and
-    floods at high water (setweg)."""
+    `hdeep` at the open boundary, M2 of `ampli`, `nlv` z-layers: the first
+    `ampli` + 0.5 m thick (a surface layer must stay thicker than the tide
+    takes away), then 1 m, the last one reaching the bottom.  The flat
+    dries at low water and floods at high water (setweg)."""
     x, y, nen3v, ii, jj = structured_triangles(nx, ny, lx, ly, 0.2, seed)
     rng = np.random.default_rng(seed + 505)
     nkn, nel = x.size, nen3v.shape[0]
@@ -265,12 +266,12 @@ def flat_case(nx=41, ny=9, lx=8.0e3, ly=1.6e3, seed=9, dt=60.0, nlv=1, ampli=1.0
         ilhv = np.ones(nel, np.int32)
         ilhkv = np.ones(nkn, np.int32)
     else:
-        hlv, hldv = z_layers(np.ones(nlv))
+        hlv, hldv = z_layers(np.r_[ampli + 0.5, np.ones(nlv - 1)])
         hlv[-1] = max(hlv[-1], h.max() + 1.0)
         ilhv, ilhkv = layer_counts(nen3v, np.maximum(hm3v, 0.1), hlv, hldv, nkn)
     bnd = np.zeros(nkn, np.int32)
     bnd[ii == 0] = 1
-    tide = np.array([[[ampli, M2_PERIOD, -M2_PERIOD / 4.0, 0.0]]], np.float32)   # start at low water
+    tide = np.array([[[ampli, M2_PERIOD, 0.0, 0.0]]], np.float32)   # from the rest level, rising
     case = dict(name=f"flat_{nkn}x{nlv}", nkn=nkn, nel=nel, nlv=nlv, nen3v=nen3v,
                 xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
                 bnd_index=bnd, tide=tide, seed=seed, params=dict(dt=dt, wetdry=1))
