@@ -91,7 +91,8 @@ typedef struct shy_params {
   float thpar, shpar, chpar; /* horizontal diffusivity T, S, tracers        */
   int32_t ireib;             /* friction type                :766           */
   int32_t ibarcl;            /* baroclinic pressure (1) or not (0)          */
-  int32_t ilin;              /* 1: linear momentum (no advective terms)     */
+  int32_t ilin;              /* 1: linear momentum; 0: explicit upwind      */
+                             /*   advection (set_advective, itlin 0, avpar 0) */
   int32_t itemp, isalt;      /* transport temperature / salinity            */
   int32_t nconz;             /* passive tracers                             */
   int32_t istot_max;         /* transport sub-step limit (scal3sh: 1000)    */
@@ -103,6 +104,7 @@ typedef struct shy_params {
   float hsigma;              /* depth limit of the sigma layers (hsigma)    */
   int32_t wetdry;            /* 1: wetting and drying of elements (setweg) */
   float hzmin, hzon, volmin; /* its thresholds       def_para.f90:744-746,1762 */
+  float rlin;                /* strength of the advective terms (ilin 0) :590 */
 } shy_params;
 
 /* Host views of one basin's state, reference layouts.  NULL members are

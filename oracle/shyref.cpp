@@ -446,6 +446,7 @@ struct Model {
   // wetting and drying (mod_geom_dynamic :: iwegv, iwetv, inodv)
   std::vector<int> iwegv, iwetv, inodv;
   std::vector<double> uov, vov;             // barotropic transports of the old level
+  std::vector<double> uprv, vprv;           // nodal velocities (mod_hydro_print), make_prvel
   double dtime_weg = -1.;                   // setweg's dtime_old
   shy_step_info info{};
   // solver controls
@@ -685,6 +686,54 @@ void set_explicit(Model &m) {
           m.fxv[(size_t)ie * nlv + l - 1] -= rdist * ai * (ui - u);
           m.fyv[(size_t)ie * nlv + l - 1] -= rdist * ai * (vi - v);
         }
+      }
+    }
+  }
+  if (m.p.ilin == 0) {
+    // set_advective (explicit.f90:685-861) with itlin 0, ihwadv 0 (no
+    // vertical momentum advection) and rdistv = rcomputev = 1 (nadist 0):
+    // set_momentum_flux (:588-683) first gives every node layer the momentum
+    // flowing into it, weighted by the inflow, or, with outflow only, its
+    // velocity from the last step's nodal velocities (uprv) times its old
+    // thickness; each element layer then takes the upwind difference over
+    // the vertices it receives flow from
+    const size_t nn = (size_t)nlv * m.nkn;
+    std::vector<double> saux(nn, 0.), momx(nn, 0.), momy(nn, 0.);
+    for (int ie = 0; ie < m.nel; ie++) {
+      const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+      for (int l = 0; l < m.ilhv[ie]; l++) {
+        const double ut = m.utlov[(size_t)ie * nlv + l], vt = m.vtlov[(size_t)ie * nlv + l];
+        for (int ii = 0; ii < 3; ii++) {
+          const size_t kl = (size_t)m.nen3v[3 * ie + ii] * nlv + l;
+          const double f = ut * e[3 + ii] + vt * e[6 + ii];   // > 0: flux into the node
+          if (f > 0.) { saux[kl] += f; momx[kl] += f * ut; momy[kl] += f * vt; }
+        }
+      }
+    }
+    for (int k = 0; k < m.nkn; k++)
+      for (int l = 0; l < m.ilhkv[k]; l++) {
+        const size_t kl = (size_t)k * nlv + l;
+        if (saux[kl] > 0.) { momx[kl] /= saux[kl]; momy[kl] /= saux[kl]; }
+        else { momx[kl] = m.uprv[kl] * m.hdkov[kl]; momy[kl] = m.vprv[kl] * m.hdkov[kl]; }
+      }
+    const double rlin = m.p.rlin;
+    for (int ie = 0; ie < m.nel; ie++) {
+      const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+      for (int l = 0; l < m.ilhv[ie]; l++) {
+        const size_t el = (size_t)ie * nlv + l;
+        const double h = m.hdeov[el], ut = m.utlov[el], vt = m.vtlov[el];
+        const double uc = ut / h, vc = vt / h;
+        double xadv = 0., yadv = 0.;
+        for (int ii = 0; ii < 3; ii++) {
+          const size_t kl = (size_t)m.nen3v[3 * ie + ii] * nlv + l;
+          const double f = ut * e[3 + ii] + vt * e[6 + ii];
+          if (f < 0.) {                        // flux out of the node, into the element
+            xadv += f * (momx[kl] / h - uc);
+            yadv += f * (momy[kl] / h - vc);
+          }
+        }
+        m.fxv[el] += rlin * xadv;
+        m.fyv[el] += rlin * yadv;
       }
     }
   }
@@ -1491,6 +1540,32 @@ void baro2l(Model &m) {
   }
 }
 
+// uvtopr (transforms.f90:214-270), the part of make_prvel (:553-566) that
+// the next step reads: nodal velocities as the area-weighted mean of the
+// element velocities ulnv = utlnv/hdenv (ttov, :98-122) over the elements
+// in the system
+void uvtopr(Model &m) {
+  const int nlv = m.nlv;
+  const size_t nn = (size_t)nlv * m.nkn;
+  m.uprv.assign(nn, 0.); m.vprv.assign(nn, 0.);
+  std::vector<double> vv(nn, 0.);
+  for (int ie = 0; ie < m.nel; ie++) {
+    if (m.iwegv[ie] != 0) continue;
+    const double aj = m.ev[(size_t)ie * SHY_EVDIM + 9];
+    for (int l = 0; l < m.ilhv[ie]; l++) {
+      const size_t el = (size_t)ie * nlv + l;
+      const double h = m.hdenv[el];
+      const double ul = h > 0. ? m.utlnv[el] / h : 0., vl = h > 0. ? m.vtlnv[el] / h : 0.;
+      for (int ii = 0; ii < 3; ii++) {
+        const size_t kl = (size_t)m.nen3v[3 * ie + ii] * nlv + l;
+        vv[kl] += aj; m.uprv[kl] += aj * ul; m.vprv[kl] += aj * vl;
+      }
+    }
+  }
+  for (size_t i = 0; i < nn; i++)
+    if (vv[i] > 0.) { m.uprv[i] /= vv[i]; m.vprv[i] /= vv[i]; }
+}
+
 int init_state(Model &m) {
   m.zenv.assign((size_t)3 * m.nel, 0.);
   for (int ie = 0; ie < m.nel; ie++)
@@ -1514,6 +1589,7 @@ int init_state(Model &m) {
   m.wlnv.assign((size_t)(m.nlv + 1) * m.nkn, 0.);
   m.rhov.assign((size_t)m.nlv * m.nkn, 0.);
   if (m.p.ibarcl > 0) for (int it = 0; it < 3; it++) rhoset(m);   // barocl(0): rhoset_shell(3)
+  uvtopr(m);                                      // make_prvel (initialize.f90:1656)
   m.info.volume = masscont(m);
   m.tbnd = m.tempv; m.sbnd = m.saltv; m.cbnd = m.conzv;   // boundary values: initial columns
   return SHY_OK;
@@ -1565,6 +1641,7 @@ int step(Model &m) {
   st = setdepth(m, m.hdknv, m.hdenv, m.zenv);     // make_new_depth
   if (st) return st;
   hydro_vertical(m);
+  uvtopr(m);                                      // compute_velocities (hydrodynamic.f90:473)
   m.info.volume = masscont(m);                    // vol_mass(1)
   // run_scalar (shyfem_subs.f90:975-1028): T and S, then rho, then tracers
   int istot = 1;

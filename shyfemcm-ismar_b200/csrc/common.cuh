@@ -43,6 +43,8 @@ struct BasinPar {
   float hsigma;               // depth limit of the sigma layers
   int wetdry;                 // wetting and drying of elements (z-layers)
   float hzmin, hzon, volmin;  // its thresholds
+  int adv;                    // explicit momentum advection (ilin = 0)
+  float rlin;                 // its strength
 };
 
 // per-basin results of the last step (device memory)
@@ -62,6 +64,7 @@ struct Dev {
   int nbasin, NKN, NEL, NLV, S, nsc_max;
   int col_threads;              // column kernel: 1 one thread per column, 0 one warp segment
   int any_wd;                   // some basin has wetting and drying (thread-per-column forms)
+  float2 *mom;                  // (NKN*NLV) node momentum {momentxv, momentyv} when a basin advects
   BasinPar *par;
   BasinOut *out;
   // mesh (static)

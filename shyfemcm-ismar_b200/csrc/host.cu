@@ -259,6 +259,7 @@ struct shygpu_model {
   bool cor = false;
   bool has_rho = false;              // some basin updates rho' from transported T and S
   bool any_wd = false;               // some basin has wetting and drying
+  bool any_adv = false;              // some basin has momentum advection (ilin = 0)
   std::vector<BasinPar> par;
   std::vector<int> nlv_b;
   Arena arena;
@@ -642,8 +643,11 @@ static Dev dev_for_step(const shygpu_model *m, int newi) {
 
 static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P, int *NLVo) {
   int64_t nkn = 0, nel = 0, NLV = 1, nnz = 0, nsc = 0;
+  bool adv = false, wd = false;
   for (int b = 0; b < nbasin; b++) {
     nkn += B[b].nkn; nel += B[b].nel;
+    adv |= P[b].ilin == 0;
+    wd |= P[b].wetdry != 0;
     NLV = std::max<int64_t>(NLV, B[b].nlv);
     nnz += 7LL * B[b].nkn + 16;
     nsc = std::max<int64_t>(nsc, (P[b].itemp ? 1 : 0) + (P[b].isalt ? 1 : 0) + std::max(0, P[b].nconz));
@@ -652,6 +656,8 @@ static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P,
   int64_t el = nel * (4 * 16 + 8 * 4 + 12 * 4 + 4 * 4 + NLV * 4 * (2 * 2 + 2 * 1 + 2 + 1 + 2 + 1)) ;
   int64_t nd = nkn * (4 * 12 + 8 * 6 + 40 + NLV * 4 * (2 + 1 + 1) + (NLV + 1) * 4 * 3 + nsc * NLV * 4 * 3);
   int64_t sy = nnz * (4 + 8 + 4 + 4 * 3);
+  if (adv) nd += nkn * NLV * 8;              // node momentum
+  if (wd) { el += nel * 8; nd += nkn * 5; }  // dry marks, counters, node kinds
   return el + nd + sy;
 }
 
@@ -717,7 +723,6 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     if (bs.ntide > SHY_MAX_TIDE) return bail(fail(SHY_EARG, "basin %d: ntide above %d", b, SHY_MAX_TIDE));
     if (Pp[b].nconz < 0 || Pp[b].nconz > SHY_MAX_CONZ) return bail(fail(SHY_EARG, "basin %d: nconz", b));
     if (Pp[b].ireib != 0 && Pp[b].ireib != 5) return bail(fail(SHY_EARG, "basin %d: ireib=%d not supported (0 or 5)", b, Pp[b].ireib));
-    if (Pp[b].ilin == 0) return bail(fail(SHY_EARG, "basin %d: non-linear momentum (ilin=0) not supported", b));
     if (!(Pp[b].dt > 0)) return bail(fail(SHY_EARG, "basin %d: dt must be positive", b));
     if (Pp[b].nsigma != 0 && Pp[b].nsigma != bs.nlv)
       return bail(fail(SHY_EARG, "basin %d: nsigma=%d: z-layers (0) or pure sigma layers (nlv) only", b, Pp[b].nsigma));
@@ -883,6 +888,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     bp.wetdry = p.wetdry ? 1 : 0;
     bp.hzmin = p.hzmin; bp.hzon = p.hzon; bp.volmin = p.volmin;
     m->any_wd |= bp.wetdry != 0;
+    bp.adv = p.ilin == 0 ? 1 : 0; bp.rlin = p.rlin;
+    m->any_adv |= bp.adv != 0;
     bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
     int ns = 0;
     if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }
@@ -953,6 +960,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   if (m->any_wd && (A.alloc(&d.iweg, NEL) || A.alloc(&d.iwet, NEL) || A.alloc(&d.inod, NKN) ||
                     A.upload(&d.kfull, kfull)))
     return bail(SHY_ECAPACITY);
+  if (m->any_adv && A.alloc(&d.mom, (size_t)NKN * NLV)) return bail(SHY_ECAPACITY);
   for (int i = 0; i < 2; i++) {
     if (A.alloc(&m->zbuf[i], NKN) || A.alloc(&m->zebuf[i], (size_t)3 * NEL) ||
         A.alloc(&m->ubuf[i], EL) || A.alloc(&m->vbuf[i], EL) || A.alloc(&m->hkbuf[i], NL) ||
@@ -1161,6 +1169,7 @@ extern "C" int shygpu_get_state(shygpu_model *m, int32_t ib, shy_state *s) {
 // the step
 // ---------------------------------------------------------------------------
 static int enqueue_hydro(shygpu_model *m, const Dev &d) {
+  if (m->any_adv) launch_node(d, m->kbas, 5, 0, 0, m->stream);   // set_momentum_flux
   if (m->any_wd) launch_wetdry(d, m->kbas, 0, -1, m->stream);    // set_dry
   launch_elem(d, 0, 0, m->stream, m->cor);
   ZetaArgs za{};
@@ -1198,7 +1207,7 @@ static int enqueue_scalar(shygpu_model *m, Dev d, int sc_cur, int *nconz) {
 
 // launches of one step apart from the transport sub-steps
 static int count_launches(const shygpu_model *m) {
-  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0) + (m->has_rho ? 1 : 0) + (m->any_wd ? 1 : 0);
+  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0) + (m->has_rho ? 1 : 0) + (m->any_wd ? 1 : 0) + (m->any_adv ? 1 : 0);
 }
 
 static int enqueue_step(shygpu_model *m) {
@@ -1387,6 +1396,7 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
     Dev d = dev_for_step(m, 1 - m->cur);
     int kind[32], n = 0;
     cudaEventRecord(ev[n], m->stream);
+    if (m->any_adv) launch_node(d, m->kbas, 5, 0, 0, m->stream);    // node momentum, timed with the column
     if (m->any_wd) launch_wetdry(d, m->kbas, 0, -1, m->stream);     // set_dry, timed with the column
     launch_elem(d, 0, 0, m->stream, m->cor); kind[n] = 0; cudaEventRecord(ev[++n], m->stream);
     ZetaArgs za{};

@@ -107,6 +107,21 @@ __global__ void __launch_bounds__(256) k_column(Dev d) {
       fy -= ai * (vi - vvi);
     }
   }
+  if (P.adv && act) {                    // set_advective (:685-861), ihwadv 0
+    const float uc = uui / hhi, vc = vvi / hhi;
+    float xadv = 0.f, yadv = 0.f;
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) {
+      const float f = uui * (float)b[ii] + vvi * (float)c[ii];
+      if (f < 0.f) {                     // flux out of the node, into the element
+        const float2 mk = d.mom[(size_t)kn[ii] * NLV + lane];
+        xadv += f * (mk.x / hhi - uc);
+        yadv += f * (mk.y / hhi - vc);
+      }
+    }
+    fx += P.rlin * xadv;
+    fy += P.rlin * yadv;
+  }
   if (P.ibarcl > 0 && P.ibarcl != 3 && P.ibarcl != 5) {
     // set_barocl_new_interface for z-layers (explicit.f90:1226-1530)
     float br = 0.f, cr = 0.f;

@@ -178,6 +178,58 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
 }
 
 // ===========================================================================
+// k_moment: the node momentum of the step's advective terms (set_momentum_flux,
+// explicit.f90:588-683), for basins with ilin = 0, from the old level at
+// the start of the step.  Per node layer (one lane each): the momentum that
+// flows in, weighted by the inflow f = U b + V c > 0 of each incident element
+// layer; with outflow only, the node's velocity times its thickness, the
+// velocity (uprv) being the area-weighted mean of U/h over the incident
+// elements in the system (uvtopr, transforms.f90:214-270, computed by the
+// reference at the end of the last step, which these old arrays hold).
+// Launched before the set_dry pass, so the wet marks are the last step's.
+// Sums in FP32 in element order, as the reference's real arrays.
+// ===========================================================================
+template <int S>
+__global__ void __launch_bounds__(256) k_moment(Dev d, const int *kbas) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  if (k >= d.NKN) return;
+  const int NLV = d.NLV;
+  const BasinPar &P = d.par[kbas[k]];
+  if (!P.adv) return;
+  const bool wd = P.wetdry && P.nsigma == 0;
+  float saux = 0.f, mx = 0.f, my = 0.f, vv = 0.f, up = 0.f, vp = 0.f;
+  for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
+    const int4 ix = d.incx[p];
+    const int e = ix.x, ii = ix.y & 3, le = ix.y >> 2;
+    if (lane >= le) continue;
+    const size_t oe = (size_t)e * NLV + lane;
+    const float ut = d.uo[oe], vt = d.vo[oe];
+    const float *evp = d.ev8 + (size_t)e * 8;
+    const float f = ut * evp[ii] + vt * evp[3 + ii];       // > 0: flux into the node
+    if (f > 0.f) { saux += f; mx += f * ut; my += f * vt; }
+    if (!wd || d.iweg[e] == 0) {
+      const float aj = evp[6], h = d.heo[oe];
+      vv += aj;
+      up += aj * (h > 0.f ? ut / h : 0.f);
+      vp += aj * (h > 0.f ? vt / h : 0.f);
+    }
+  }
+  if (lane >= NLV) return;
+  const size_t o = (size_t)k * NLV + lane;
+  float2 m = make_float2(0.f, 0.f);
+  if (lane < d.ilhkv[k]) {
+    if (saux > 0.f) m = make_float2(mx / saux, my / saux);
+    else if (vv > 0.f) {
+      const float h = d.hko[o];
+      m = make_float2(up / vv * h, vp / vv * h);
+    }
+  }
+  d.mom[o] = m;
+}
+
+// ===========================================================================
 // k_stab: conzstab stability index per node, max-reduced per basin/scalar
 // ===========================================================================
 template <int S>

@@ -76,6 +76,7 @@ static void launch_node_S(const Dev &d, const int *kbas, int which, int a, int b
       break;
     case 3: k_rhoset<S><<<blocks, threads, 0, st>>>(d, kbas); break;
     case 4: k_rho<S><<<blocks, threads, 0, st>>>(d, kbas); break;
+    case 5: k_moment<S><<<blocks, threads, 0, st>>>(d, kbas); break;
   }
 }
 

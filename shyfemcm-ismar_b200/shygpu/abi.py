@@ -50,6 +50,7 @@ class ShyParams(C.Structure):
         ("solver_rtol", C.c_float), ("solver_atol", C.c_float), ("solver_maxit", C.c_int32),
         ("nsigma", C.c_int32), ("hsigma", C.c_float),
         ("wetdry", C.c_int32), ("hzmin", C.c_float), ("hzon", C.c_float), ("volmin", C.c_float),
+        ("rlin", C.c_float),
     ]
 
 
@@ -134,6 +135,7 @@ def make_params(case, **over):
     s.hzmin = float(p.get("hzmin", 0.01))
     s.hzon = float(p.get("hzon", 0.10))
     s.volmin = float(p.get("volmin", 1.0))
+    s.rlin = float(p.get("rlin", 1.0))
     return s
 
 

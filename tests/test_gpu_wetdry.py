@@ -12,8 +12,8 @@ counters and the node kinds must be equal and the levels within ZETA_TOL;
 that first difference must sit at such a tie (a vertex within TIE of a
 threshold).  One decision a step apart moves the flooding front and, over
 the flat, the decisions after it: from there on the levels may differ by
-centimetres at the front (FRONT_TOL) and a few dry marks (DRY_DIFF), while
-the volume stays within 1e-4."""
+centimetres at the front (FRONT_TOL) and inside the wet domain (INNER_TOL)
+and a few dry marks (DRY_DIFF), while the volume stays within 1e-4."""
 import numpy as np
 import pytest
 
@@ -27,25 +27,42 @@ ZETA_TOL = 1.0e-3          # m, on nodes in the system in both runs
 TIE = 1.0e-4               # m, a threshold tie: far above the solver tolerance
 FRONT_TOL = 0.1            # m, after a tie: the front shifted by a step or more
 DRY_DIFF = 0.02            # fraction of the elements whose dry mark may differ after a tie
+INNER_TOL = 0.1            # m, after a tie: nodes inside the wet domain of both runs
+# With momentum advection (ilin = 0) the upwind choices (inflow f > 0 at a
+# node) switch discontinuously where the flow stagnates, and rounding picks
+# the branch: the oracle against itself, with 1e-6 m of noise in the initial
+# levels, first decides differently at step 319 of the cycle and then
+# differs by 7 cm at the front.  The GPU's first tie comes earlier (its
+# whole state carries FP32 rounding); after it the front nodes, whose level
+# in a run where their elements are dry comes from the dry Laplacian, may
+# differ by decimetres, so only nodes inside both wet domains are compared,
+# and the volume within 1e-3.
 
 
 def levels(g, o):
     return g.get_state(0)["znv"].astype(np.float64), o.state()["znv"]
 
 
-def at_a_tie(c, e, zs):
-    """Whether element e has a vertex (or, for the mean-depth rule, a mean)
-    within TIE of hzoff, hzmin or hzon in any of the level sets zs."""
+def at_a_tie(c, e, was_dry, z_old, z_new):
+    """Whether a decision on element e sits within TIE of its threshold in
+    one of the runs: a wet element leaves on a vertex below hzoff at the old
+    level (setweg 2) or below hzmin at the new one (setweg 1); a dry one
+    comes back on its vertices, or their mean, reaching hzon at the old
+    level (setweg 3), and may leave again at the new one."""
     p = cases_params(c)
     hm = c["hm3v"][e].astype(np.float64)
     kn = c["nen3v"][e] - 1
-    thr = np.array([p["hzoff"], p["hzmin"], p["hzon"]])
-    for z in zs:
+
+    def near(x, t):
+        return float(np.min(np.abs(np.atleast_1d(x) - t))) <= TIE
+
+    for z in z_old:
         hz = z[kn] + hm
-        d = np.abs(np.r_[hz, hz.mean()][:, None] - thr[None, :])
-        if d.min() <= TIE:
+        if was_dry and (near(hz, p["hzon"]) or near(hz.mean(), p["hzon"])):
             return True
-    return False
+        if not was_dry and near(hz, p["hzoff"]):
+            return True
+    return any(near(z[kn] + hm, p["hzmin"]) for z in z_new)
 
 
 def cases_params(c):
@@ -54,10 +71,12 @@ def cases_params(c):
     return p
 
 
-@pytest.mark.parametrize("nlv", [1, 4])
-def test_tidal_flat_dries_and_floods(nlv):
-    """One M2 period (750 steps of 60 s), compared after every step."""
+@pytest.mark.parametrize("nlv,ilin", [(1, 1), (4, 1), (1, 0)])
+def test_tidal_flat_dries_and_floods(nlv, ilin):
+    """One M2 period (750 steps of 60 s), compared after every step; with
+    momentum advection (ilin = 0) the nodal velocities skip dry elements."""
     c = cases.flat_case(nlv=nlv)
+    c["params"] = dict(c["params"], ilin=ilin)
     g = shygpu.Model(c)
     g.set_state(0)
     o = shyref.OracleModel(c)
@@ -68,6 +87,7 @@ def test_tidal_flat_dries_and_floods(nlv):
     first_tie, ndry = None, []
     for step in range(1, 751):
         zg0, zo0 = zg, zo
+        dry0 = gw[0] > 0
         g.run(1)
         o.run(1)
         gw, ow = g.wetdry(0), o.wetdry()
@@ -78,19 +98,23 @@ def test_tidal_flat_dries_and_floods(nlv):
         differ = np.nonzero((gw[0] != ow[0]) | (gw[1] != ow[1]))[0]
         if first_tie is None and len(differ):
             for e in differ:
-                assert at_a_tie(c, e, (zg0, zo0, zg, zo)), (step, e)
+                assert at_a_tie(c, e, dry0[e], (zg0, zo0), (zg, zo)), (step, e)
             first_tie = step
         if first_tie is None:
             np.testing.assert_array_equal(gw[2], ow[2])
             assert dz <= ZETA_TOL, (step, dz)
         else:
             assert ((gw[0] > 0) != (ow[0] > 0)).sum() <= DRY_DIFF * c["nel"], step
-            assert dz <= FRONT_TOL, (step, dz)
-    assert abs(g.info(0).volume / o.info().volume - 1.0) <= 1e-4
+            inner = (gw[2] == 0) & (ow[2] == 0)
+            assert np.abs(zg - zo)[inner].max() <= INNER_TOL, step
+            if ilin:
+                assert dz <= FRONT_TOL, (step, dz)
+    assert abs(g.info(0).volume / o.info().volume - 1.0) <= (1e-4 if ilin else 1e-3)
     assert min(ndry) == 0 and max(ndry) > 0.4 * c["nel"], ndry
-    # the stretch before a tie holds the flooding of the flat and its drying
-    # to the largest dry set of the cycle
-    assert first_tie is None or first_tie > int(np.argmax(ndry)) + 1, (first_tie, ndry)
+    if ilin:
+        # the stretch before a tie holds the flooding of the flat and its
+        # drying to the largest dry set of the cycle
+        assert first_tie is None or first_tie > int(np.argmax(ndry)) + 1, (first_tie, ndry)
 
 
 def test_tidal_flat_in_a_batch():
