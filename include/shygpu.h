@@ -105,6 +105,8 @@ typedef struct shy_params {
   int32_t wetdry;            /* 1: wetting and drying of elements (setweg) */
   float hzmin, hzon, volmin; /* its thresholds       def_para.f90:744-746,1762 */
   float rlin;                /* strength of the advective terms (ilin 0) :590 */
+  int32_t itvd;              /* horizontal transport: 0 upwind, 1 TVD with  */
+                             /*   node gradients (superbee)     :1053       */
 } shy_params;
 
 /* Host views of one basin's state, reference layouts.  NULL members are

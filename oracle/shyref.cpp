@@ -1164,11 +1164,87 @@ double conzstab(Model &m, double rkpar) {
   return stabind / m.p.rstol;
 }
 
+// tvd_grad_3d (tvd_admin.f90:478-550): node gradients of a scalar, the
+// area-weighted mean of the element gradients over the elements that have
+// the layer (itvd = 1)
+void tvd_grad_3d(const Model &m, const std::vector<double> &cc, std::vector<double> &gx,
+                 std::vector<double> &gy) {
+  const int nlv = m.nlv;
+  const size_t nn = (size_t)nlv * m.nkn;
+  gx.assign(nn, 0.); gy.assign(nn, 0.);
+  std::vector<double> aux(nn, 0.);
+  for (int ie = 0; ie < m.nel; ie++) {
+    const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+    const double area = e[9];
+    for (int l = 0; l < m.ilhv[ie]; l++) {
+      double ggx = 0., ggy = 0.;
+      for (int ii = 0; ii < 3; ii++) {
+        const size_t kl = (size_t)m.nen3v[3 * ie + ii] * nlv + l;
+        ggx += cc[kl] * e[3 + ii];
+        ggy += cc[kl] * e[6 + ii];
+        aux[kl] += area;
+      }
+      for (int ii = 0; ii < 3; ii++) {
+        const size_t kl = (size_t)m.nen3v[3 * ie + ii] * nlv + l;
+        gx[kl] += ggx * area;
+        gy[kl] += ggy * area;
+      }
+    }
+  }
+  for (size_t q = 0; q < nn; q++)
+    if (aux[q] > 0.) { gx[q] /= aux[q]; gy[q] /= aux[q]; }
+}
+
+// tvd_fluxes (tvd_admin.f90:673-838) with itvd = 1: the horizontal fluxes
+// fl(3) of element ie, layer l (1-based), from the concentrations cl of its
+// vertices, the node gradients and the element velocity (ulnv = utlnv/hdenv
+// of the new level), limited by superbee.  itot/isum as conz3d_element's
+// (number and index sum of the vertices with f < 0).
+void tvd_fluxes(const Model &m, int ie, int l, int itot, int isum, double dt, const double cl[3],
+                const std::vector<double> &gx, const std::vector<double> &gy, const double f[3],
+                double fl[3]) {
+  fl[0] = fl[1] = fl[2] = 0.;
+  if (itot < 1 || itot > 2) return;
+  const int nlv = m.nlv;
+  const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+  const size_t el = (size_t)ie * nlv + l - 1;
+  const double h = m.hdenv[el];
+  const double u = h > 0. ? m.utlnv[el] / h : 0., v = h > 0. ? m.vtlnv[el] / h : 0.;
+  const double aj = 24. * e[9];
+  const int itot2 = itot - 1, itot1 = 2 - itot;
+  const int ip = itot2 * (6 - isum) + itot1 * isum;
+  for (int ii = 1; ii <= 3; ii++) {
+    if (ii == ip) continue;
+    const int ic = itot2 * ii + itot1 * ip, id = itot2 * ip + itot1 * ii;
+    const double fact = -itot2 + itot1;
+    const double conc = cl[ic - 1], cond = cl[id - 1];
+    const int iop = 6 - (id + ic);                  // the vertex opposite side ic-id
+    const int tet1 = 1 + iop % 3;
+    double dx = aj * e[5 + iop];                    // ev(6+iop)
+    if (tet1 == id) dx = -dx;
+    double dy = aj * e[2 + iop];                    // ev(3+iop)
+    if (tet1 == ic) dy = -dy;
+    const double dis = e[15 + iop];                 // ev(16+iop): length of side ic-id
+    const double vel = std::fabs(u * dx + v * dy) / dis;
+    const double alfa = dt * vel / dis;
+    const size_t kc = (size_t)m.nen3v[3 * ie + ic - 1] * nlv + l - 1;
+    const double grad = 2. * (gx[kc] * dx + gy[kc] * dy);
+    const double rf = std::fabs(conc - cond) < 1.e-8 ? -1. : grad / (cond - conc) - 1.;
+    const double psi = std::max(0., std::max(std::min(1., 2. * rf), std::min(2., rf)));   // superbee
+    const double conf = conc + 0.5 * psi * (cond - conc) * (1. - alfa);
+    const double term = fact * conf * f[ii - 1];
+    fl[ic - 1] -= term;
+    fl[id - 1] += term;
+  }
+}
+
 // conz3d_omp (concentration_omp.f90:65-350) with conz3d_element (:355-755),
 // vertical_flux_ie (tvd_admin.f90:930-1019, no vertical TVD) and
-// conz3d_nodes (:757-888); itvd = 0, robs = 0, no sinking, no loading,
-// cbound unused because mfluxv = 0.
-void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int istot, int isact) {
+// conz3d_nodes (:757-888); itvd 0 or 1 (gx, gy: the node gradients of
+// tvd_grad_3d), robs = 0, no sinking, no loading, cbound unused because
+// mfluxv = 0.
+void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int istot, int isact,
+            const std::vector<double> &gx, const std::vector<double> &gy) {
   int nlv = m.nlv;
   double az = m.p.azpar, ad = m.p.adpar, aa = m.p.aapar;
   double azt = 1. - az, adt = 1. - ad, aat = 1. - aa;
@@ -1257,6 +1333,11 @@ void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int is
       } else {
         fl[0] = fl[1] = fl[2] = 0.;
       }
+      // horizontal TVD (:675-686): elements without an open-boundary vertex
+      if (m.p.itvd > 0 && m.bnd[kn[0]] <= 0 && m.bnd[kn[1]] <= 0 && m.bnd[kn[2]] <= 0) {
+        const double c3[3] = {H(cl, l, 0), H(cl, l, 1), H(cl, l, 2)};
+        tvd_fluxes(m, ie, l, itot, isum, dt, c3, gx, gy, f, fl);
+      }
       for (int ii = 0; ii < 3; ii++) {
         int k = kn[ii];
         double hmed = haver[l];
@@ -1312,10 +1393,12 @@ int scal3sh(Model &m, std::vector<double> &cnv, double rkpar, bool is_temp,
   *istot_out = istot;
   int istot_max = m.p.istot_max > 0 ? m.p.istot_max : 1000;
   if (istot > istot_max) return fail(SHY_EISTOT, "scal3sh: istot index too high");
+  std::vector<double> gx, gy;
   for (int isact = 1; isact <= istot; isact++) {
     if (!is_temp)
       for (auto &v : cnv) if (v < 1.e-15) v = 0.;
-    conz3d(m, cnv, m.p.dt, rkpar, istot, isact);
+    if (m.p.itvd == 1) tvd_grad_3d(m, cnv, gx, gy);        // (concentration.f90:744)
+    conz3d(m, cnv, m.p.dt, rkpar, istot, isact, gx, gy);
     bndo_impbc(m, cnv, rbc);
   }
   return SHY_OK;

@@ -45,6 +45,7 @@ struct BasinPar {
   float hzmin, hzon, volmin;  // its thresholds
   int adv;                    // explicit momentum advection (ilin = 0)
   float rlin;                 // its strength
+  int itvd;                   // horizontal transport: 0 upwind, 1 TVD with node gradients
 };
 
 // per-basin results of the last step (device memory)
@@ -65,6 +66,8 @@ struct Dev {
   int col_threads;              // column kernel: 1 one thread per column, 0 one warp segment
   int any_wd;                   // some basin has wetting and drying (thread-per-column forms)
   float2 *mom;                  // (NKN*NLV) node momentum {momentxv, momentyv} when a basin advects
+  int any_tvd;                  // some basin transports with TVD (a gradient pass per sub-step)
+  float2 *tgrad;                // (nsc_max*NKN*NLV) node gradients {gx, gy} of the sub-step's scalars
   BasinPar *par;
   BasinOut *out;
   // mesh (static)

@@ -260,6 +260,7 @@ struct shygpu_model {
   bool has_rho = false;              // some basin updates rho' from transported T and S
   bool any_wd = false;               // some basin has wetting and drying
   bool any_adv = false;              // some basin has momentum advection (ilin = 0)
+  bool any_tvd = false;              // some basin transports with TVD (itvd = 1)
   std::vector<BasinPar> par;
   std::vector<int> nlv_b;
   Arena arena;
@@ -643,10 +644,11 @@ static Dev dev_for_step(const shygpu_model *m, int newi) {
 
 static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P, int *NLVo) {
   int64_t nkn = 0, nel = 0, NLV = 1, nnz = 0, nsc = 0;
-  bool adv = false, wd = false;
+  bool adv = false, wd = false, tvd = false;
   for (int b = 0; b < nbasin; b++) {
     nkn += B[b].nkn; nel += B[b].nel;
     adv |= P[b].ilin == 0;
+    tvd |= P[b].itvd == 1;
     wd |= P[b].wetdry != 0;
     NLV = std::max<int64_t>(NLV, B[b].nlv);
     nnz += 7LL * B[b].nkn + 16;
@@ -657,6 +659,7 @@ static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P,
   int64_t nd = nkn * (4 * 12 + 8 * 6 + 40 + NLV * 4 * (2 + 1 + 1) + (NLV + 1) * 4 * 3 + nsc * NLV * 4 * 3);
   int64_t sy = nnz * (4 + 8 + 4 + 4 * 3);
   if (adv) nd += nkn * NLV * 8;              // node momentum
+  if (tvd) nd += nsc * nkn * NLV * 8;        // TVD node gradients
   if (wd) { el += nel * 8; nd += nkn * 5; }  // dry marks, counters, node kinds
   return el + nd + sy;
 }
@@ -728,6 +731,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: nsigma=%d: z-layers (0) or pure sigma layers (nlv) only", b, Pp[b].nsigma));
     if (Pp[b].nsigma > 0 && Pp[b].ibarcl > 0)
       return bail(fail(SHY_EARG, "basin %d: baroclinic terms on sigma layers not supported", b));
+    if (Pp[b].itvd != 0 && Pp[b].itvd != 1)
+      return bail(fail(SHY_EARG, "basin %d: itvd=%d: upwind (0) or TVD with node gradients (1) only", b, Pp[b].itvd));
     if (Pp[b].wetdry && !(Pp[b].hzmin > 0.f && Pp[b].hzoff >= Pp[b].hzmin && Pp[b].hzon >= Pp[b].hzoff))
       return bail(fail(SHY_EARG, "basin %d: wetting and drying needs 0 < hzmin <= hzoff <= hzon", b));
     NLV = std::max(NLV, bs.nlv);
@@ -890,12 +895,14 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     m->any_wd |= bp.wetdry != 0;
     bp.adv = p.ilin == 0 ? 1 : 0; bp.rlin = p.rlin;
     m->any_adv |= bp.adv != 0;
+    bp.itvd = p.itvd;
     bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
     int ns = 0;
     if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }
     if (bp.isalt) { bp.rkpar[ns] = p.shpar; bp.is_temp[ns] = 0; ns++; }
     for (int c = 0; c < p.nconz; c++) { bp.rkpar[ns] = p.chpar; bp.is_temp[ns] = 0; ns++; }
     bp.nsc = ns;
+    m->any_tvd |= bp.itvd == 1 && ns > 0;
     nsc_max = std::max(nsc_max, ns);
     bp.istot_max = p.istot_max > 0 ? p.istot_max : 1000;
     bp.k0 = k0; bp.nk = nkn; bp.e0 = e0; bp.ne = nel; bp.nlv = nlv;
@@ -924,6 +931,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   d.nbasin = nbasin; d.NKN = NKN; d.NEL = NEL; d.NLV = NLV; d.S = m->S; d.nsc_max = nsc_max;
   d.col_threads = 1;
   d.any_wd = m->any_wd ? 1 : 0;
+  d.any_tvd = m->any_tvd ? 1 : 0;
   ST_TRY(A.upload(&d.par, m->par) ? bail(SHY_ECAPACITY) : 0);
   std::vector<BasinOut> outs(nbasin);
   memset(outs.data(), 0, sizeof(BasinOut) * nbasin);
@@ -961,6 +969,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
                     A.upload(&d.kfull, kfull)))
     return bail(SHY_ECAPACITY);
   if (m->any_adv && A.alloc(&d.mom, (size_t)NKN * NLV)) return bail(SHY_ECAPACITY);
+  if (m->any_tvd && A.alloc(&d.tgrad, (size_t)nsc_max * NKN * NLV)) return bail(SHY_ECAPACITY);
   for (int i = 0; i < 2; i++) {
     if (A.alloc(&m->zbuf[i], NKN) || A.alloc(&m->zebuf[i], (size_t)3 * NEL) ||
         A.alloc(&m->ubuf[i], EL) || A.alloc(&m->vbuf[i], EL) || A.alloc(&m->hkbuf[i], NL) ||
@@ -1188,6 +1197,13 @@ static void enqueue_scalar_head(shygpu_model *m, const Dev &d) {
   launch_reduce(d, 0, 1, m->stream);
 }
 
+// one transport sub-step j (-1: the device's counter): the TVD node
+// gradients of its input first, where a basin transports with TVD
+static void launch_substep(shygpu_model *m, const Dev &d, int j) {
+  if (m->any_tvd) launch_node(d, m->kbas, 6, j, 0, m->stream);
+  launch_node(d, m->kbas, 2, j, 0, m->stream);
+}
+
 // eager sub-step loop: the host reads the step's largest sub-step count
 static int enqueue_scalar(shygpu_model *m, Dev d, int sc_cur, int *nconz) {
   enqueue_scalar_head(m, d);
@@ -1198,8 +1214,8 @@ static int enqueue_scalar(shygpu_model *m, Dev d, int sc_cur, int *nconz) {
     CUDA_TRY(cudaStreamSynchronize(m->stream));
     d.sc_in = m->scbuf[sc_cur];
     d.sc_out = m->scbuf[1 - sc_cur];
-    for (int j = 0; j < imax && j < 1000; j++) launch_node(d, m->kbas, 2, j, 0, m->stream);
-    *nconz = imax;
+    for (int j = 0; j < imax && j < 1000; j++) launch_substep(m, d, j);
+    *nconz = imax * (m->any_tvd ? 2 : 1);
     if (m->has_rho) { launch_node(d, m->kbas, 4, 0, 0, m->stream); *nconz += 1; }
   }
   return SHY_OK;
@@ -1294,7 +1310,7 @@ static int build_graph(shygpu_model *m, int cur, int sc_cur) {
     Dev db = d;
     db.sc_in = m->scbuf[sc_cur];
     db.sc_out = m->scbuf[1 - sc_cur];
-    launch_node(db, m->kbas, 2, -1, 0, m->stream);    // sub-step index from the device
+    launch_substep(m, db, -1);                        // sub-step index from the device
     launch_subctl(db, h, m->stream);
     cudaGraph_t gb = nullptr;
     e = cudaStreamEndCapture(m->stream, &gb);
@@ -1416,7 +1432,7 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
       d.sc_in = m->scbuf[m->sc_cur];
       d.sc_out = m->scbuf[1 - m->sc_cur];
       for (int j = 0; j < imax && n < 30; j++) {
-        launch_node(d, m->kbas, 2, j, 0, m->stream);
+        launch_substep(m, d, j);                      // with its TVD gradients
         kind[n] = 6; cudaEventRecord(ev[++n], m->stream);
       }
       if (m->has_rho) { launch_node(d, m->kbas, 4, 0, 0, m->stream); kind[n] = 7; cudaEventRecord(ev[++n], m->stream); }

@@ -32,6 +32,106 @@ __device__ __forceinline__ float clipc(float v, bool is_temp) {
   return (!is_temp && v < 1.e-15f) ? 0.f : v;   // scal3sh: where(cnv < 1e-15) cnv = 0
 }
 
+// the sub-step's input columns of every scalar (sub-step isact, 1-based)
+__device__ __forceinline__ const float *conz_input(const Dev &d, int isact) {
+  return isact == 1 ? d.sc_in : (isact & 1 ? d.scr1 : d.scr0);
+}
+
+// ===========================================================================
+// k_tvdgrad: node gradients of the sub-step's scalars for the horizontal TVD
+// scheme (tvd_grad_3d, tvd_admin.f90:478-550, itvd = 1): per node layer the
+// area-weighted mean of the gradients of the incident elements that have
+// the layer, from the clipped input (scal3sh clips before it,
+// concentration.f90:736-744).  One warp segment per node column, lane =
+// layer; FP32 sums in element order.
+// ===========================================================================
+template <int S>
+__global__ void __launch_bounds__(256) k_tvdgrad(Dev d, const int *kbas, int j_arg) {
+  const int j = j_arg >= 0 ? j_arg : *d.subj;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  const int NLV = d.NLV;
+  if (k >= d.NKN || lane >= NLV) return;
+  const int b = kbas[k];
+  const BasinPar &P = d.par[b];
+  if (P.itvd != 1) return;
+  const BasinOut &O = d.out[b];
+  const int isact = j + 1;
+  const float *cin = conz_input(d, isact);
+  const size_t SN = (size_t)d.NKN * NLV, o = (size_t)k * NLV + lane;
+  const int pbeg = d.inc_ptr[k], pend = d.inc_ptr[k + 1];
+  for (int s = 0; s < P.nsc; s++) {
+    if (isact > (int)O.stab[s]) continue;        // no sub-step of this scalar
+    const bool istmp = P.is_temp[s] != 0;
+    const float *cs = cin + s * SN;
+    const float cown = clipc(cs[o], istmp);
+    float gx = 0.f, gy = 0.f, ar = 0.f;
+    for (int p = pbeg; p < pend; p++) {
+      const int4 ix = d.incx[p];
+      const int e = ix.x, ii = ix.y & 3;
+      if (lane >= (ix.y >> 2)) continue;
+      const float *evp = d.ev8 + (size_t)e * 8;
+      const float ca = clipc(cs[(size_t)ix.z * NLV + lane], istmp);
+      const float cb = clipc(cs[(size_t)ix.w * NLV + lane], istmp);
+      const float c3[3] = {ii == 0 ? cown : ca, ii == 1 ? cown : (ii == 0 ? ca : cb), ii == 2 ? cown : cb};
+      const float ggx = c3[0] * evp[0] + c3[1] * evp[1] + c3[2] * evp[2];
+      const float ggy = c3[0] * evp[3] + c3[1] * evp[4] + c3[2] * evp[5];
+      const float area = evp[6];
+      gx += ggx * area;
+      gy += ggy * area;
+      ar += area;
+    }
+    d.tgrad[s * SN + o] = ar > 0.f ? make_float2(gx / ar, gy / ar) : make_float2(0.f, 0.f);
+  }
+}
+
+// tvd_fluxes (tvd_admin.f90:673-838), itvd = 1: the horizontal flux of
+// vertex `own` (0..2) of an element layer, replacing the upwind one.  The
+// pairs (ic, id) of the one vertex with outflow (itot 1) or inflow (itot 2)
+// and each other vertex carry the concentration of ic corrected towards id
+// by the superbee limiter of the ratio of the gradient at ic (node
+// gradients, g) to the difference along the side.  kv: node of each vertex,
+// u, v: the element's velocity, aj24 = 24 ev(10) (twice the area); the side
+// length is aj24 |(b, c)| of the opposite vertex (ev(17..19)).
+__device__ __forceinline__ float tvd_flux_own(int own, int itot, int isum, const float (&f3)[3],
+                                              const float (&c3)[3], const float (&bb)[3],
+                                              const float (&cc)[3], const int (&kv)[3], float aj24,
+                                              float u, float v, float dt, const float2 *g, int NLV,
+                                              int lane) {
+  if (itot < 1 || itot > 2) return 0.f;
+  const int itot2 = itot - 1, itot1 = 2 - itot;
+  const int ip = itot2 * (6 - isum) + itot1 * isum;          // 1-based
+  const float fact = (float)(itot1 - itot2);
+  float fl = 0.f;
+#pragma unroll
+  for (int ii = 1; ii <= 3; ii++) {
+    if (ii == ip) continue;
+    const int ic = itot2 * ii + itot1 * ip, id = itot2 * ip + itot1 * ii;
+    if (ic != own + 1 && id != own + 1) continue;            // no share of vertex own
+    const float conc = sel3(c3, ic - 1), cond = sel3(c3, id - 1);
+    const int iop = 6 - (id + ic);                           // the vertex opposite side ic-id
+    const int tet1 = 1 + iop % 3;
+    const float bo = sel3(bb, iop - 1), co = sel3(cc, iop - 1);
+    float dx = aj24 * co;
+    if (tet1 == id) dx = -dx;
+    float dy = aj24 * bo;
+    if (tet1 == ic) dy = -dy;
+    const float dis = aj24 * sqrtf(bo * bo + co * co);
+    const float vel = fabsf(u * dx + v * dy) / dis;
+    const float alfa = dt * vel / dis;
+    const int kc = ic == 1 ? kv[0] : (ic == 2 ? kv[1] : kv[2]);
+    const float2 gc = g[(size_t)kc * NLV + lane];
+    const float grad = 2.f * (gc.x * dx + gc.y * dy);
+    const float rf = fabsf(conc - cond) < 1.e-8f ? -1.f : grad / (cond - conc) - 1.f;
+    const float psi = fmaxf(0.f, fmaxf(fminf(1.f, 2.f * rf), fminf(2.f, rf)));   // superbee
+    const float conf = conc + 0.5f * psi * (cond - conc) * (1.f - alfa);
+    const float term = fact * conf * sel3(f3, ii - 1);
+    fl += (ic == own + 1) ? -term : term;
+  }
+  return fl;
+}
+
 template <int S, int NR>
 __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg) {
   const int j = j_arg >= 0 ? j_arg : *d.subj;   // sub-step index: argument or device counter
@@ -78,7 +178,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
     const float rstot = istot;
     const float rso = (isact - 1) / rstot, rsn = isact / rstot, rsot = 1.f - rso, rsnt = 1.f - rsn;
     const float dt = (float)P.dt / rstot;
-    const float *cin_base = isact == 1 ? d.sc_in : (isact & 1 ? d.scr1 : d.scr0);
+    const float *cin_base = conz_input(d, isact);
     float *cout_base = isact == istot ? d.sc_out : (isact & 1 ? d.scr0 : d.scr1);
     // node column: thickness, vertical diffusion conductances
     const float hold = rso * hkn + rsot * hko, hnew = rsn * hkn + rsnt * hko;
@@ -131,6 +231,18 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
         const float dfh = anyrk ? d.difhv[oe] : 0.f;
         const int kja = ix.z, kjb = ix.w;
         const float fii = sel3(f3, ii);
+        // horizontal TVD (concentration_omp.f90:675-686) where no vertex is
+        // on an open boundary, with the element velocity of the new level
+        const bool tvd = P.itvd == 1 && !isbnd && d.kbnd[kja] <= 0 && d.kbnd[kjb] <= 0;
+        float ue = 0.f, ve = 0.f;
+        int kv[3] = {k, k, k};
+        if (tvd) {
+          const float hn = d.hen[oe];
+          if (hn > 0.f) { ue = d.un[oe] / hn; ve = d.vn[oe] / hn; }
+          kv[0] = ii == 0 ? k : kja;
+          kv[1] = ii == 1 ? k : (ii == 0 ? kja : kjb);
+          kv[2] = ii == 2 ? k : kjb;
+        }
 #pragma unroll
         for (int r = 0; r < NR; r++) {
           if (sidx[r] < 0) continue;
@@ -146,6 +258,9 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
             const float fc = fii * cl[r];
             fl = (ii == 5 - isum) ? fc - (f3[0] * c3[0] + f3[1] * c3[1] + f3[2] * c3[2]) : fc;
           } else fl = 0.f;
+          if (tvd)
+            fl = tvd_flux_own(ii, itot, isum, f3, c3, bb, cc, kv, 24.f * e1.z, ue, ve, dt,
+                              d.tgrad + sidx[r] * SN, NLV, lane);
           float hdif = 0.f;
           if (rk[r] != 0.f) {
             float wdiff = 0.f;

@@ -77,6 +77,7 @@ static void launch_node_S(const Dev &d, const int *kbas, int which, int a, int b
     case 3: k_rhoset<S><<<blocks, threads, 0, st>>>(d, kbas); break;
     case 4: k_rho<S><<<blocks, threads, 0, st>>>(d, kbas); break;
     case 5: k_moment<S><<<blocks, threads, 0, st>>>(d, kbas); break;
+    case 6: k_tvdgrad<S><<<blocks, threads, 0, st>>>(d, kbas, a); break;
   }
 }
 
@@ -138,7 +139,7 @@ void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStr
 __global__ void k_subctl(Dev d, cudaGraphConditionalHandle h) {
   const int nj = *d.subj + 1;
   *d.subj = nj;
-  *d.nsub_launched += 2;
+  *d.nsub_launched += d.any_tvd ? 3 : 2;
   cudaGraphSetConditional(h, nj < *d.imax ? 1u : 0u);
 }
 

@@ -241,3 +241,31 @@ def test_momentum_advection(small3d, shape):
     lin = shyref.OracleModel(with_params(c, ilin=1))
     lin.run(n)
     assert np.abs(lin.state()["utlnv"] - so["utlnv"])[me].max() > 10e-3 * umax
+
+
+@pytest.mark.parametrize("shape", ["basin3d", "lagoon30"])
+def test_tvd_transport(small3d, shape):
+    """itvd = 1: horizontal TVD fluxes (tvd_fluxes, tvd_admin.f90:673-838)
+    with node gradients recomputed before every sub-step (tvd_grad_3d
+    :478-550): temperature and salinity of the 3D basin, three tracers on
+    the 30-layer sigma lagoon."""
+    if shape == "basin3d":
+        c, n, fields = with_params(small3d, itvd=1), 120, ("tempv", "saltv")
+    else:
+        c, n, fields = with_params(cases.lagoon_case(nkn_target=900, nlv=30), itvd=1), 80, ("conzv",)
+    g, o = run_both(c, n)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    m = active_mask(c)
+    for f in fields:
+        a, r = sg[f], so[f]
+        if f == "conzv":
+            a, r = a[:, m], r[:, m]
+        else:
+            a, r = a[m], r[m]
+        rel = np.abs(a - r).max() / np.abs(r).max()
+        assert rel <= TRACER_RTOL, (f, rel)
+    up = shyref.OracleModel(with_params(c, itvd=0))
+    up.run(n)
+    f = fields[-1]
+    assert np.abs(up.state()[f] - so[f]).max() > 100 * TRACER_RTOL * np.abs(so[f]).max()
