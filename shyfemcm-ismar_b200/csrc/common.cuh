@@ -103,8 +103,9 @@ struct Dev {
   unsigned char *kfull;
   float4 *cg4[2];                 // device-wide CG: {r, w = A D^-1 r, s, 1/diag} per row, two generations
   float2 *cg2;                    // device-wide CG: {p, e} per row
-  // element system written by the column kernel (SoA): hia[c*NEL+e], hik[c*NEL+e]
-  float *hia, *hik;
+  // element system written by the column kernel, 12 floats per element:
+  // hia (3x3, row-major, [e*12 + 3i+j]) then hik ([e*12 + 9 + i])
+  float *hia;
   // state, [0] = new, [1] = old (swapped per step)
   float *zn, *zo;             // [k]
   float *zen, *zeo;           // [e*3+ii]
@@ -339,6 +340,16 @@ __device__ __forceinline__ void pcr_solve_c(double a, double2 b, double c, doubl
 __device__ __forceinline__ void atomic_max_pos(float *addr, float v) {
   // v >= 0: the ordering of non-negative IEEE floats matches their int bits
   atomicMax(reinterpret_cast<int *>(addr), __float_as_int(v));
+}
+
+// the element system of element e in its 12-float record (three 16-byte
+// stores): a row of zeta equations gathers it from one or two sectors
+__device__ __forceinline__ void store_elem_system(const Dev &d, int e, const double (&hia)[3][3],
+                                                  const double (&hik)[3]) {
+  float4 *p = reinterpret_cast<float4 *>(d.hia + (size_t)e * 12);
+  p[0] = make_float4((float)hia[0][0], (float)hia[0][1], (float)hia[0][2], (float)hia[1][0]);
+  p[1] = make_float4((float)hia[1][1], (float)hia[1][2], (float)hia[2][0], (float)hia[2][1]);
+  p[2] = make_float4((float)hia[2][2], (float)hik[0], (float)hik[1], (float)hik[2]);
 }
 
 }  // namespace shy

@@ -956,8 +956,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       A.alloc(&d.p32, NKN) || A.alloc(&d.q32, NKN) || A.alloc(&d.z32, NKN) ||
       A.alloc(&d.e32, NKN) || A.alloc(&d.s32, NKN) || A.alloc(&d.t32, NKN) ||
       A.alloc(&d.rh32, NKN) || A.alloc(&d.v32, NKN) || A.alloc(&d.cg4[0], NKN) ||
-      A.alloc(&d.cg4[1], NKN) || A.alloc(&d.cg2, NKN + 2) || A.alloc(&d.hia, (size_t)9 * NEL) ||
-      A.alloc(&d.hik, (size_t)3 * NEL) || A.alloc(&d.unv, NEL) || A.alloc(&d.vnv, NEL) ||
+      A.alloc(&d.cg4[1], NKN) || A.alloc(&d.cg2, NKN + 2) || A.alloc(&d.hia, (size_t)12 * NEL) || A.alloc(&d.unv, NEL) || A.alloc(&d.vnv, NEL) ||
       A.alloc(&d.usv, EL) || A.alloc(&d.vsv, EL) ||
       A.alloc(&d.wl, (size_t)NKN * (NLV + 1)) || A.alloc(&d.rho, NL) || A.alloc(&d.ddx, EL) ||
       A.alloc(&d.ddxi, m->cor ? EL : 1) || A.alloc(&d.cbnd, NSC) || A.alloc(&d.vol_node, NKN) ||
@@ -1182,7 +1181,7 @@ static int enqueue_hydro(shygpu_model *m, const Dev &d) {
   if (m->any_wd) launch_wetdry(d, m->kbas, 0, -1, m->stream);    // set_dry
   launch_elem(d, 0, 0, m->stream, m->cor);
   ZetaArgs za{};
-  za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
+  za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hia + 9; za.cs = 1; za.es = 12;
   za.explicit_mode = 0; za.inner_rtol = m->inner_rtol; za.max_outer = m->max_outer; za.sym = m->sym;
   ST_TRY(launch_zeta_plan(m, d, za));
   launch_elem(d, 1, 0, m->stream, m->cor);
@@ -1416,7 +1415,7 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
     if (m->any_wd) launch_wetdry(d, m->kbas, 0, -1, m->stream);     // set_dry, timed with the column
     launch_elem(d, 0, 0, m->stream, m->cor); kind[n] = 0; cudaEventRecord(ev[++n], m->stream);
     ZetaArgs za{};
-    za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hik; za.cs = m->NEL; za.es = 1;
+    za.zguess = d.zo; za.zprev = d.zn; za.hia = d.hia; za.hik = d.hia + 9; za.cs = 1; za.es = 12;
     za.inner_rtol = m->inner_rtol; za.max_outer = m->max_outer; za.sym = m->sym;
     if ((st = launch_zeta_plan(m, d, za)) != SHY_OK) break;
     kind[n] = 1; cudaEventRecord(ev[++n], m->stream);

@@ -217,12 +217,7 @@ __global__ void __launch_bounds__(256) k_column(Dev d) {
         hik[i] = rw * hia[i][i];
       }
     }
-#pragma unroll
-    for (int n = 0; n < 3; n++) {
-#pragma unroll
-      for (int m = 0; m < 3; m++) d.hia[(size_t)(3 * n + m) * d.NEL + e] = (float)hia[n][m];
-      d.hik[(size_t)n * d.NEL + e] = (float)hik[n];
-    }
+    store_elem_system(d, e, hia, hik);
   }
 }
 

@@ -20,7 +20,7 @@
 
 namespace shy {
 
-template <int L, bool COR>
+template <int L, bool COR, bool ADV>
 __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.NEL) return;
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
         fy -= ai * (vi - vvi);
       }
     }
-    if (P.adv) {                         // set_advective (:685-861), ihwadv 0
+    if (ADV && P.adv) {                  // set_advective (:685-861), ihwadv 0
       const float uc = uui / hhi, vc = vvi / hhi;
       float xadv = 0.f, yadv = 0.f;
 #pragma unroll
@@ -269,12 +269,7 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
       hik[i] = rw * hia[i][i];
     }
   }
-#pragma unroll
-  for (int n = 0; n < 3; n++) {
-#pragma unroll
-    for (int m = 0; m < 3; m++) d.hia[(size_t)(3 * n + m) * d.NEL + e] = (float)hia[n][m];
-    d.hik[(size_t)n * d.NEL + e] = (float)hik[n];
-  }
+  store_elem_system(d, e, hia, hik);
 }
 
 }  // namespace shy

@@ -154,13 +154,14 @@ __device__ __forceinline__ void wd_dry_system(const Dev &d, int e) {
   double b[3], c[3];
   for (int i = 0; i < 3; i++) { b[i] = evp[i]; c[i] = evp[3 + i]; }
   const double hh999 = 12. * (double)evp[6];
+  double hia[3][3], hik[3];
   for (int n = 0; n < 3; n++) {
     const int in = __ldcg(&d.inod[kn[n]]);
     const bool keep = in == 0 || in == -2;
-    for (int m = 0; m < 3; m++)
-      d.hia[(size_t)(3 * n + m) * d.NEL + e] = keep ? (float)(hh999 * (b[n] * b[m] + c[n] * c[m])) : 0.f;
-    d.hik[(size_t)n * d.NEL + e] = 0.f;
+    for (int m = 0; m < 3; m++) hia[n][m] = keep ? hh999 * (b[n] * b[m] + c[n] * c[m]) : 0.;
+    hik[n] = 0.;
   }
+  store_elem_system(d, e, hia, hik);
 }
 
 // setweg(1) for one element after a solve (:265-290): out when a vertex is

@@ -115,7 +115,8 @@ __device__ __forceinline__ void assemble_row(const Dev &d, const ZetaArgs &za, i
     for (int t = d.slot_ptr[s]; t < d.slot_ptr[s + 1]; t++) {
       const int src = d.slot_src[t];
       const int e = src / 9, c = src - 9 * e;
-      v += (double)__ldcg(&za.hia[(size_t)c * za.cs + (size_t)e * za.es]);
+      const float *ph = &za.hia[(size_t)c * za.cs + (size_t)e * za.es];
+      v += (double)(wd ? __ldcg(ph) : *ph);      // dry systems are written in this launch
     }
     d.val64[s] = v;
     d.val32[s] = (float)v;
@@ -125,7 +126,8 @@ __device__ __forceinline__ void assemble_row(const Dev &d, const ZetaArgs &za, i
   for (int p = d.inc_ptr[i]; p < d.inc_ptr[i + 1]; p++) {
     const int q = d.inc[p];
     const int e = q / 3, ii = q - 3 * e;
-    rhs += (double)__ldcg(&za.hik[(size_t)ii * za.cs + (size_t)e * za.es]);
+    const float *pk = &za.hik[(size_t)ii * za.cs + (size_t)e * za.es];
+    rhs += (double)(wd ? __ldcg(pk) : *pk);
   }
   // adjust_mass_flux (bnd_routines.f90:1185-1210): with wetting and drying
   // (wd) no flux enters a node out of the system

@@ -84,8 +84,12 @@ static void launch_node_S(const Dev &d, const int *kbas, int which, int a, int b
 template <int L>
 static void launch_column_t(const Dev &d, cudaStream_t st, bool cor) {
   const int blocks = (d.NEL + 127) / 128;
-  if (cor) k_column_t<L, true><<<blocks, 128, 0, st>>>(d);
-  else k_column_t<L, false><<<blocks, 128, 0, st>>>(d);
+  // the advective terms as a separate instance: the plain one keeps its registers
+  if (d.mom) {
+    if (cor) k_column_t<L, true, true><<<blocks, 128, 0, st>>>(d);
+    else k_column_t<L, false, true><<<blocks, 128, 0, st>>>(d);
+  } else if (cor) k_column_t<L, true, false><<<blocks, 128, 0, st>>>(d);
+  else k_column_t<L, false, false><<<blocks, 128, 0, st>>>(d);
 }
 
 void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool cor) {
