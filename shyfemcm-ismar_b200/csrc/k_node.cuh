@@ -98,37 +98,38 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
   const double z = d.zn[k];
   const float *hld = d.hldv + (size_t)b * NLV;
   const float *hlv = d.hlv + (size_t)b * NLV;
-  double hsum[L], vf[L], va[L];
+  // sums in FP32 in element order, as the reference's real hdkn and vf
+  // (setdepth, hydro_vertical); va, the area of the elements with the layer,
+  // is static (Dev::avol)
+  float hsum[L], vf[L];
   double hsig_h = 0.;                         // sigma: depth of the last incident element's vertex
 #pragma unroll
-  for (int l = 0; l < L; l++) { hsum[l] = 0.; vf[l] = 0.; va[l] = 0.; }
+  for (int l = 0; l < L; l++) { hsum[l] = 0.f; vf[l] = 0.f; }
   for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
     const int4 ix = d.incx[p];
     const int e = ix.x, ii = ix.y & 3, le = ix.y >> 2;
     const float *evp = d.ev8 + (size_t)e * 8;
-    const double aj = evp[6];
-    const double areafv = 4. * aj;            // 12*aj/3
+    const float aj = evp[6];
+    const float areafv = 4.f * aj;            // 12*aj/3
     const float4 hm = d.hm3v[e];
-    const double htot = ii == 0 ? hm.x : (ii == 1 ? hm.y : hm.z);
-    const double bb = evp[ii], cc = evp[3 + ii];
+    const float htot = ii == 0 ? hm.x : (ii == 1 ? hm.y : hm.z);
+    const float bb = evp[ii], cc = evp[3 + ii];
     const size_t oe = (size_t)e * NLV;
-    const double hbot = le >= 2 ? htot - hlv[le - 2] : 0.;
+    const float hbot = le >= 2 ? htot - hlv[le - 2] : 0.f;
     hsig_h = htot;
     // setdepth takes the element's vertex level (a dry element's differs)
-    const double ze = P.wetdry ? (double)d.zen[3 * e + ii] : z;
+    const float ze = P.wetdry ? d.zen[3 * e + ii] : (float)z;
 #pragma unroll
     for (int l = 0; l < L; l++) {
       if (l >= le) break;
-      double hl;
+      float hl;
       if (le == 1) hl = htot + ze;
-      else if (l < le - 1) hl = (double)hld[l] + (l == 0 ? ze : 0.);
+      else if (l < le - 1) hl = hld[l] + (l == 0 ? ze : 0.f);
       else hl = hbot;
       hsum[l] += areafv * hl;
       if (!init_only) {
-        const double ff = (double)d.usv[oe + l] * bb + (double)d.vsv[oe + l] * cc;   // az*ffn + azt*ffo
-        const double aj4 = 4. * aj;
-        vf[l] += 3. * aj4 * ff;
-        va[l] += aj4;
+        const float ff = d.usv[oe + l] * bb + d.vsv[oe + l] * cc;   // az*ffn + azt*ffo
+        vf[l] += 3.f * areafv * ff;
       }
     }
   }
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
     if (l >= NLV) continue;
     const bool act = l < lmax;
     area[l] = act ? (double)d.areakv[o + l] : 0.;
-    double hk = act && area[l] > 0. ? hsum[l] / area[l] : 0.;
+    double hk = act && area[l] > 0. ? (double)(hsum[l] / (float)area[l]) : 0.;
     if (P.nsigma > 0 && act) hk = -(fmin(hsig_h, (double)P.hsigma) + z) * (double)hld[l];   // sigma (:1019-1025)
     hkf[l] = (float)hk;
     if (act && !(hkf[l] > 0.f)) bad = true;
@@ -165,12 +166,16 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
     if (act && P.nlv > 1) {
       const double voln = (double)(hkf[l] * (float)area[l]);
       const double volo = (double)(d.hko[o + l] * (float)area[l]);
-      dv = vf[l] - (voln - volo) / P.dt;
+      dv = (double)vf[l] - (voln - volo) / P.dt;
     }
     acc += dv;
     double wtop = acc;
     if (l == 0) wtop = 0.;                     // wlnv(lmin-1) = 0
-    if (l >= 1 && act && va[l] > 0.) wtop /= va[l];
+    if (l >= 1 && act) {
+      const float2 av = d.avol[o + l];         // aj4 over the elements with layer l
+      const double va = (double)av.x + (double)av.y;
+      if (va > 0.) wtop /= va;
+    }
     if (!act || wzero) wtop = 0.;
     d.wl[(size_t)k * I + l] = (float)wtop;
   }
