@@ -96,6 +96,7 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
   const bool thr = (d.col_threads || d.any_wd) && d.NLV <= 16;
   if (which == 0 && thr) {
     if (d.NLV <= 8) launch_column_t<8>(d, st, cor);
+    else if (d.NLV <= 12) launch_column_t<12>(d, st, cor);
     else launch_column_t<16>(d, st, cor);
     return;
   }
@@ -124,6 +125,7 @@ void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStr
   if (which == 0 && (d.col_threads || d.any_wd) && d.NLV <= 16) {
     const int blocks = (d.NKN + 127) / 128;
     if (d.NLV <= 8) k_node_t<8><<<blocks, 128, 0, st>>>(d, kbas, a);
+    else if (d.NLV <= 12) k_node_t<12><<<blocks, 128, 0, st>>>(d, kbas, a);
     else k_node_t<16><<<blocks, 128, 0, st>>>(d, kbas, a);
     return;
   }
