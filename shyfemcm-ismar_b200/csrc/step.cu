@@ -107,6 +107,7 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
     } else {
       const int blocks = (d.NEL + 127) / 128;            // 4 warps of 32 elements
       if (d.NLV <= 8) k_final_w<8><<<blocks, 128, 0, st>>>(d, init_only);
+      else if (d.NLV <= 12) k_final_w<12><<<blocks, 128, 0, st>>>(d, init_only);
       else k_final_w<16><<<blocks, 128, 0, st>>>(d, init_only);
     }
     return;
