@@ -107,6 +107,8 @@ typedef struct shy_params {
   float rlin;                /* strength of the advective terms (ilin 0) :590 */
   int32_t itvd;              /* horizontal transport: 0 upwind, 1 TVD with  */
                              /*   node gradients (superbee)     :1053       */
+  int32_t itvdv;             /* vertical transport: 0 upwind, 1 TVD          */
+                             /*   (superbee; needs aapar = 0)   :1054       */
 } shy_params;
 
 /* Host views of one basin's state, reference layouts.  NULL members are

@@ -1239,7 +1239,7 @@ void tvd_fluxes(const Model &m, int ie, int l, int itot, int isum, double dt, co
 }
 
 // conz3d_omp (concentration_omp.f90:65-350) with conz3d_element (:355-755),
-// vertical_flux_ie (tvd_admin.f90:930-1019, no vertical TVD) and
+// vertical_flux_ie (tvd_admin.f90:930-1019, itvdv 0 or 1) and
 // conz3d_nodes (:757-888); itvd 0 or 1 (gx, gy: the node gradients of
 // tvd_grad_3d), robs = 0, no sinking, no loading, cbound unused because
 // mfluxv = 0.
@@ -1279,12 +1279,30 @@ void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int is
       }
     }
     for (int ii = 0; ii < 3; ii++) H(wl, ilevel, ii) = 0.;
-    // vertical_flux_ie
+    // vertical_flux_ie (tvd_admin.f90:930-1019): upwind, or with itvdv the
+    // superbee-limited value between the upwind and downwind layers, the
+    // far-upwind layer of this element's column giving the gradient ratio
     for (int ii = 0; ii < 3; ii++) {
       for (int l = jlevel; l <= ilevel - 1; l++) {
         double w = H(wl, l, ii);
         double conc = w > 0. ? H(cl, l + 1, ii) : H(cl, l, ii);
-        H(vflux, l, ii) = w * conc;
+        double conf = conc;
+        if (m.p.itvdv > 0) {
+          double cond, conu;
+          if (w > 0.) {
+            cond = H(cl, l, ii);
+            conu = l + 2 <= ilevel ? H(cl, l + 2, ii) : cond;
+          } else {
+            cond = H(cl, l + 1, ii);
+            conu = l - 1 >= jlevel ? H(cl, l - 1, ii) : cond;
+          }
+          const double hdis = 0.5 * (H(hold, l, ii) + H(hold, l + 1, ii));
+          const double alfa = dt * std::fabs(w) / hdis;
+          const double rf = std::fabs(conc - cond) < 1.e-8 ? -1. : (cond - conu) / (cond - conc) - 1.;
+          const double psi = std::max(0., std::max(std::min(1., 2. * rf), std::min(2., rf)));
+          conf = conc + 0.5 * psi * (cond - conc) * (1. - alfa);
+        }
+        H(vflux, l, ii) = w * conf;
       }
       H(vflux, jlevel - 1, ii) = 0.;
       H(vflux, ilevel, ii) = 0.;

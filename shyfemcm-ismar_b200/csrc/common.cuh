@@ -46,6 +46,7 @@ struct BasinPar {
   int adv;                    // explicit momentum advection (ilin = 0)
   float rlin;                 // its strength
   int itvd;                   // horizontal transport: 0 upwind, 1 TVD with node gradients
+  int itvdv;                  // vertical transport: 0 upwind, 1 TVD
 };
 
 // per-basin results of the last step (device memory)

@@ -731,6 +731,10 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: nsigma=%d: z-layers (0) or pure sigma layers (nlv) only", b, Pp[b].nsigma));
     if (Pp[b].nsigma > 0 && Pp[b].ibarcl > 0)
       return bail(fail(SHY_EARG, "basin %d: baroclinic terms on sigma layers not supported", b));
+    if (Pp[b].itvdv != 0 && Pp[b].itvdv != 1)
+      return bail(fail(SHY_EARG, "basin %d: itvdv=%d: upwind (0) or TVD (1) only", b, Pp[b].itvdv));
+    if (Pp[b].itvdv == 1 && Pp[b].aapar != 0.f)   // concentration_omp.f90:218-226
+      return bail(fail(SHY_EARG, "basin %d: vertical TVD (itvdv=1) needs aapar = 0", b));
     if (Pp[b].itvd != 0 && Pp[b].itvd != 1)
       return bail(fail(SHY_EARG, "basin %d: itvd=%d: upwind (0) or TVD with node gradients (1) only", b, Pp[b].itvd));
     if (Pp[b].wetdry && !(Pp[b].hzmin > 0.f && Pp[b].hzoff >= Pp[b].hzmin && Pp[b].hzon >= Pp[b].hzoff))
@@ -895,7 +899,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     m->any_wd |= bp.wetdry != 0;
     bp.adv = p.ilin == 0 ? 1 : 0; bp.rlin = p.rlin;
     m->any_adv |= bp.adv != 0;
-    bp.itvd = p.itvd;
+    bp.itvd = p.itvd; bp.itvdv = p.itvdv;
     bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
     int ns = 0;
     if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }

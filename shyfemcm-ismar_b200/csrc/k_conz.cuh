@@ -132,6 +132,15 @@ __device__ __forceinline__ float tvd_flux_own(int own, int itot, int isum, const
   return fl;
 }
 
+// the interface value of vertical TVD (vertical_flux_ie,
+// tvd_admin.f90:976-1004): from the upwind layer towards the downwind one,
+// limited by superbee of the ratio to the far-upwind difference
+__device__ __forceinline__ float tvd_v(float conc, float cond, float conu, float alfa) {
+  const float rf = fabsf(conc - cond) < 1.e-8f ? -1.f : (cond - conu) / (cond - conc) - 1.f;
+  const float psi = fmaxf(0.f, fmaxf(fminf(1.f, 2.f * rf), fminf(2.f, rf)));
+  return conc + 0.5f * psi * (cond - conc) * (1.f - alfa);
+}
+
 template <int S, int NR>
 __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg) {
   const int j = j_arg >= 0 ? j_arg : *d.subj;   // sub-step index: argument or device counter
@@ -162,6 +171,12 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
   const float wb = act ? d.wl[(size_t)k * I + lane + 1] : 0.f;
   const float2 av = act ? d.avol[o] : make_float2(0.f, 0.f);
   const float At = av.x, A = av.x + av.y;      // continuing elements, all elements
+  // vertical TVD: the far-upwind layer of an element's column exists only
+  // where the element continues, so the bottom interface splits At into the
+  // elements continuing below layer l+1 and those ending at it
+  const bool tvdv = P.itvdv == 1;
+  float2 avn = make_float2(0.f, 0.f);
+  if (tvdv) { avn.x = seg_down<S>(av.x, 1); avn.y = seg_down<S>(av.y, 1); }
   const bool isbnd = d.kbnd[k] > 0;
   const int pbeg = d.inc_ptr[k], pend = d.inc_ptr[k + 1];
   const bool up_ok = lane > 0, dn_ok = lane + 1 < lmax;
@@ -286,9 +301,32 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
 #pragma unroll
     for (int r = 0; r < NR; r++) {
       const float c = cl[r];
-      const float vtop = up_ok ? wt * (wt > 0.f ? c : cm1[r]) : 0.f;
-      const float vbot = wb * (wb > 0.f ? cp1[r] : c);
-      const float fw = aat * (A * vtop - At * vbot);
+      float topw, botw;                               // interface fluxes times their element weights
+      if (!tvdv) {
+        const float vtop = up_ok ? wt * (wt > 0.f ? c : cm1[r]) : 0.f;
+        const float vbot = wb * (wb > 0.f ? cp1[r] : c);
+        topw = A * vtop;
+        botw = At * vbot;
+      } else {
+        const float cm2 = seg_up<S>(c, 2), cp2 = seg_down<S>(c, 2);
+        topw = 0.f;
+        if (up_ok) {
+          const float alfa = dt * fabsf(wt) / (0.5f * (holdm + hold));
+          if (wt > 0.f)
+            topw = wt * (At * tvd_v(c, cm1[r], cp1[r], alfa) + av.y * tvd_v(c, cm1[r], cm1[r], alfa));
+          else
+            topw = A * wt * tvd_v(cm1[r], c, lane >= 2 ? cm2 : c, alfa);
+        }
+        botw = 0.f;
+        if (dn_ok) {
+          const float alfa = dt * fabsf(wb) / (0.5f * (hold + holdp));
+          if (wb > 0.f)
+            botw = wb * (avn.x * tvd_v(cp1[r], c, cp2, alfa) + avn.y * tvd_v(cp1[r], c, c, alfa));
+          else
+            botw = At * wb * tvd_v(c, cp1[r], up_ok ? cm1[r] : cp1[r], alfa);
+        }
+      }
+      const float fw = aat * (topw - botw);
       const float fd = adt * (At * (c - cp1[r]) * hmobot - A * (cm1[r] - c) * hmotop);
       res[r] = A * hold * c + dt * (hs[r] - fw - fd);
     }

@@ -50,7 +50,7 @@ class ShyParams(C.Structure):
         ("solver_rtol", C.c_float), ("solver_atol", C.c_float), ("solver_maxit", C.c_int32),
         ("nsigma", C.c_int32), ("hsigma", C.c_float),
         ("wetdry", C.c_int32), ("hzmin", C.c_float), ("hzon", C.c_float), ("volmin", C.c_float),
-        ("rlin", C.c_float), ("itvd", C.c_int32),
+        ("rlin", C.c_float), ("itvd", C.c_int32), ("itvdv", C.c_int32),
     ]
 
 
@@ -137,6 +137,7 @@ def make_params(case, **over):
     s.volmin = float(p.get("volmin", 1.0))
     s.rlin = float(p.get("rlin", 1.0))
     s.itvd = int(p.get("itvd", 0))
+    s.itvdv = int(p.get("itvdv", 0))
     return s
 
 

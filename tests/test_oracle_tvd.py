@@ -42,3 +42,26 @@ def test_tvd_keeps_bounds_and_variance():
         assert np.var(out[1][t][act]) > np.var(out[0][t][act])
     # the fluxes differ from upwind by far more than rounding
     assert np.abs(out[1] - out[0]).max() > 1e-2 * (hi - lo)
+
+
+def test_vertical_tvd_keeps_more_stratification():
+    """itvdv = 1 (vertical_flux_ie, tvd_admin.f90:930-1019, with aapar = 0
+    as the reference requires): a uniform tracer stays uniform, and on the
+    wind-driven stratified basin the temperature and salinity columns keep
+    more of their vertical variance than with upwind fluxes."""
+    var = {}
+    for itvdv in (0, 1):
+        c = cases.basin3d_case(nkn_target=1500, nlv=12)
+        c["params"] = dict(c["params"], itvdv=itvdv, aapar=0.0)
+        o = shyref.OracleModel(c)
+        o.run(200)
+        s, il = o.state(), c["ilhkv"]
+        var[itvdv] = [np.mean([np.var(s[f][k, :il[k]]) for k in range(c["nkn"]) if il[k] > 1])
+                      for f in ("tempv", "saltv")]
+    assert var[1][0] > 1.1 * var[0][0] and var[1][1] > 1.1 * var[0][1], var
+    c = lagoon(0, conz=5.0)
+    c["params"] = dict(c["params"], itvdv=1, aapar=0.0)
+    o = shyref.OracleModel(c)
+    o.run(40)
+    act = np.arange(12)[None, :] < c["ilhkv"][:, None]
+    assert np.abs(o.state()["conzv"][:, act] - 5.0).max() <= 1e-6
