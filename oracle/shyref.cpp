@@ -447,6 +447,10 @@ struct Model {
   std::vector<int> iwegv, iwetv, inodv;
   std::vector<double> uov, vov;             // barotropic transports of the old level
   std::vector<double> uprv, vprv;           // nodal velocities (mod_hydro_print), make_prvel
+  // itvd = 2: per element and ordered vertex pair (c, d) the element holding
+  // the point 2 x_c - x_d and its barycentric weights there (tvd_upwind_init_elem)
+  std::vector<int> tvdup_e;                 // [6*ie + slot], -1 outside the basin
+  std::vector<double> tvdup_xi;             // [3*(6*ie + slot) + i]
   double dtime_weg = -1.;                   // setweg's dtime_old
   shy_step_info info{};
   // solver controls
@@ -1195,14 +1199,53 @@ void tvd_grad_3d(const Model &m, const std::vector<double> &cc, std::vector<doub
     if (aux[q] > 0.) { gx[q] /= aux[q]; gy[q] /= aux[q]; }
 }
 
-// tvd_fluxes (tvd_admin.f90:673-838) with itvd = 1: the horizontal fluxes
+// the slot of the ordered vertex pair (c, d), c != d, among an element's six
+inline int tvd_slot(int c, int d) { return 2 * c + ((d - c + 3) % 3 - 1); }
+
+// tvd_upwind_init_elem (tvd_admin.f90:361-476): for every element and
+// ordered pair (c, d) of its vertices, the point beyond c opposite d,
+// 2 x_c - x_d (kept in single precision as the reference's real x, y), the
+// element that holds it (the lowest-numbered one where several touch it;
+// none outside the basin) and the point's natural coordinates there
+// (xy2xi/adjust_xi, evgeom.f90:531-660: clipped to [0,1], summing to 1).
+// A brute-force search: the oracle runs on small meshes.
+void tvd_upwind_init(Model &m, const std::vector<double> &x, const std::vector<double> &y) {
+  m.tvdup_e.assign((size_t)6 * m.nel, -1);
+  m.tvdup_xi.assign((size_t)18 * m.nel, 0.);
+  for (int ie = 0; ie < m.nel; ie++)
+    for (int c = 0; c < 3; c++)
+      for (int d = 0; d < 3; d++) {
+        if (d == c) continue;
+        const int kc = m.nen3v[3 * ie + c], kd = m.nen3v[3 * ie + d];
+        const double xu = (double)(float)(2. * x[kc] - x[kd]), yu = (double)(float)(2. * y[kc] - y[kd]);
+        const int sl = 6 * ie + tvd_slot(c, d);
+        for (int je = 0; je < m.nel; je++) {
+          const int *k = &m.nen3v[3 * je];
+          const double x1 = x[k[0]], y1 = y[k[0]], x2 = x[k[1]], y2 = y[k[1]], x3 = x[k[2]], y3 = y[k[2]];
+          const double det = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1);
+          double l[3];
+          l[1] = ((xu - x1) * (y3 - y1) - (x3 - x1) * (yu - y1)) / det;
+          l[2] = ((x2 - x1) * (yu - y1) - (xu - x1) * (y2 - y1)) / det;
+          l[0] = 1. - l[1] - l[2];
+          if (l[0] < -1e-9 || l[1] < -1e-9 || l[2] < -1e-9) continue;
+          double sum = 0.;
+          for (int i = 0; i < 3; i++) { l[i] = std::min(1., std::max(0., l[i])); sum += l[i]; }
+          m.tvdup_e[sl] = je;
+          for (int i = 0; i < 3; i++) m.tvdup_xi[(size_t)3 * sl + i] = l[i] / sum;
+          break;
+        }
+      }
+}
+
+// tvd_fluxes (tvd_admin.f90:673-838), itvd 1 or 2: the horizontal fluxes
 // fl(3) of element ie, layer l (1-based), from the concentrations cl of its
-// vertices, the node gradients and the element velocity (ulnv = utlnv/hdenv
-// of the new level), limited by superbee.  itot/isum as conz3d_element's
+// vertices, the element velocity (ulnv = utlnv/hdenv of the new level) and
+// either the node gradients gx, gy (itvd 1) or the value of cv at the point
+// beyond the upwind vertex (itvd 2), limited by superbee.  itot/isum as conz3d_element's
 // (number and index sum of the vertices with f < 0).
 void tvd_fluxes(const Model &m, int ie, int l, int itot, int isum, double dt, const double cl[3],
                 const std::vector<double> &gx, const std::vector<double> &gy, const double f[3],
-                double fl[3]) {
+                const std::vector<double> &cv, double fl[3]) {
   fl[0] = fl[1] = fl[2] = 0.;
   if (itot < 1 || itot > 2) return;
   const int nlv = m.nlv;
@@ -1227,8 +1270,23 @@ void tvd_fluxes(const Model &m, int ie, int l, int itot, int isum, double dt, co
     const double dis = e[15 + iop];                 // ev(16+iop): length of side ic-id
     const double vel = std::fabs(u * dx + v * dy) / dis;
     const double alfa = dt * vel / dis;
-    const size_t kc = (size_t)m.nen3v[3 * ie + ic - 1] * nlv + l - 1;
-    const double grad = 2. * (gx[kc] * dx + gy[kc] * dy);
+    double grad;
+    if (m.p.itvd == 2) {
+      // the value at the point beyond ic opposite id (tvd_get_upwind_c
+      // :608-671), or cond where that point has no layer l
+      double conu = cond;
+      const int sl = 6 * ie + tvd_slot(ic - 1, id - 1);
+      const int je = m.tvdup_e[sl];
+      if (je >= 0 && m.ilhv[je] >= l) {
+        conu = 0.;
+        for (int i = 0; i < 3; i++)
+          conu += m.tvdup_xi[(size_t)3 * sl + i] * cv[(size_t)m.nen3v[3 * je + i] * nlv + l - 1];
+      }
+      grad = cond - conu;
+    } else {
+      const size_t kc = (size_t)m.nen3v[3 * ie + ic - 1] * nlv + l - 1;
+      grad = 2. * (gx[kc] * dx + gy[kc] * dy);
+    }
     const double rf = std::fabs(conc - cond) < 1.e-8 ? -1. : grad / (cond - conc) - 1.;
     const double psi = std::max(0., std::max(std::min(1., 2. * rf), std::min(2., rf)));   // superbee
     const double conf = conc + 0.5 * psi * (cond - conc) * (1. - alfa);
@@ -1354,7 +1412,7 @@ void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int is
       // horizontal TVD (:675-686): elements without an open-boundary vertex
       if (m.p.itvd > 0 && m.bnd[kn[0]] <= 0 && m.bnd[kn[1]] <= 0 && m.bnd[kn[2]] <= 0) {
         const double c3[3] = {H(cl, l, 0), H(cl, l, 1), H(cl, l, 2)};
-        tvd_fluxes(m, ie, l, itot, isum, dt, c3, gx, gy, f, fl);
+        tvd_fluxes(m, ie, l, itot, isum, dt, c3, gx, gy, f, cn1, fl);
       }
       for (int ii = 0; ii < 3; ii++) {
         int k = kn[ii];
@@ -1865,6 +1923,7 @@ void *shyref_create(const shy_basin *B, const shy_params *P) {
   std::vector<double> x = dv(B->xgv, nkn), y = dv(B->ygv, nkn);
   m->ev.assign((size_t)SHY_EVDIM * nel, 0.);
   if (set_ev(nkn, nel, m->nen3v.data(), x.data(), y.data(), m->ev.data())) { delete m; return nullptr; }
+  if (P->itvd == 2) tvd_upwind_init(*m, x, y);
   m->hm3v = dv(B->hm3v, (size_t)3 * nel);
   m->hev.assign(nel, 0.);
   for (int ie = 0; ie < nel; ie++)   // element depth: mean of vertex depths (hev)

@@ -69,6 +69,7 @@ struct Dev {
   float2 *mom;                  // (NKN*NLV) node momentum {momentxv, momentyv} when a basin advects
   int any_tvd;                  // some basin transports with TVD (a gradient pass per sub-step)
   float2 *tgrad;                // (nsc_max*NKN*NLV) node gradients {gx, gy} of the sub-step's scalars
+  int4 *tvdup;                  // (6*NEL) itvd = 2: {element, xi0, xi1, xi2 as float bits} per vertex pair
   BasinPar *par;
   BasinOut *out;
   // mesh (static)

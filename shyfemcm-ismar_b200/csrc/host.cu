@@ -644,11 +644,12 @@ static Dev dev_for_step(const shygpu_model *m, int newi) {
 
 static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P, int *NLVo) {
   int64_t nkn = 0, nel = 0, NLV = 1, nnz = 0, nsc = 0;
-  bool adv = false, wd = false, tvd = false;
+  bool adv = false, wd = false, tvd = false, up = false;
   for (int b = 0; b < nbasin; b++) {
     nkn += B[b].nkn; nel += B[b].nel;
     adv |= P[b].ilin == 0;
     tvd |= P[b].itvd == 1;
+    up |= P[b].itvd == 2;
     wd |= P[b].wetdry != 0;
     NLV = std::max<int64_t>(NLV, B[b].nlv);
     nnz += 7LL * B[b].nkn + 16;
@@ -660,6 +661,7 @@ static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P,
   int64_t sy = nnz * (4 + 8 + 4 + 4 * 3);
   if (adv) nd += nkn * NLV * 8;              // node momentum
   if (tvd) nd += nsc * nkn * NLV * 8;        // TVD node gradients
+  if (up) el += nel * 96;                    // TVD upwind points
   if (wd) { el += nel * 8; nd += nkn * 5; }  // dry marks, counters, node kinds
   return el + nd + sy;
 }
@@ -702,6 +704,72 @@ static int check_cluster_shape(int CL, int threads, size_t smem) {
   return SHY_OK;
 }
 
+// For horizontal TVD with upwind points (itvd = 2; tvd_upwind_init_elem,
+// tvd_admin.f90:361-476): per element and ordered vertex pair (c, d), slot
+// 2c + ((d - c + 3) % 3 - 1), the element holding the point 2 x_c - x_d
+// (rounded to single precision as the reference's real x, y) and the
+// point's natural coordinates in it, clipped to [0,1] and summing to 1
+// (xy2xi/adjust_xi, evgeom.f90:531-660).  Where several elements touch the
+// point the lowest-numbered one holds it; outside the basin none does (-1).
+// Candidates come from a uniform grid of element bounding boxes.
+static void build_tvd_upwind(int nkn, int nel, const int *nv, const float *xg, const float *yg, int e0,
+                             int4 *tab) {
+  double x0 = xg[0], x1 = xg[0], y0 = yg[0], y1 = yg[0];
+  for (int k = 1; k < nkn; k++) {
+    x0 = std::min(x0, (double)xg[k]); x1 = std::max(x1, (double)xg[k]);
+    y0 = std::min(y0, (double)yg[k]); y1 = std::max(y1, (double)yg[k]);
+  }
+  const int ng = std::max(1, (int)std::sqrt((double)nel / 2.));
+  const double cx = std::max(x1 - x0, 1e-9) / ng, cy = std::max(y1 - y0, 1e-9) / ng;
+  auto cell = [&](double v, double o, double c) { return std::min(ng - 1, std::max(0, (int)((v - o) / c))); };
+  std::vector<std::vector<int>> grid((size_t)ng * ng);
+  for (int ie = 0; ie < nel; ie++) {
+    const int *k = nv + 3 * ie;
+    double ax = xg[k[0]], bx = ax, ay = yg[k[0]], by = ay;
+    for (int i = 1; i < 3; i++) {
+      ax = std::min(ax, (double)xg[k[i]]); bx = std::max(bx, (double)xg[k[i]]);
+      ay = std::min(ay, (double)yg[k[i]]); by = std::max(by, (double)yg[k[i]]);
+    }
+    for (int gy = cell(ay, y0, cy); gy <= cell(by, y0, cy); gy++)
+      for (int gx = cell(ax, x0, cx); gx <= cell(bx, x0, cx); gx++) grid[(size_t)gy * ng + gx].push_back(ie);
+  }
+  for (int ie = 0; ie < nel; ie++)
+    for (int c = 0; c < 3; c++)
+      for (int d = 0; d < 3; d++) {
+        if (d == c) continue;
+        const int kc = nv[3 * ie + c], kd = nv[3 * ie + d];
+        const double xu = (double)(float)(2. * (double)xg[kc] - (double)xg[kd]);
+        const double yu = (double)(float)(2. * (double)yg[kc] - (double)yg[kd]);
+        int4 &t = tab[(size_t)6 * ie + 2 * c + ((d - c + 3) % 3 - 1)];
+        t = make_int4(-1, 0, 0, 0);
+        if (xu < x0 || xu > x1 || yu < y0 || yu > y1) continue;
+        int best = -1;
+        double lb[3] = {0., 0., 0.};
+        for (int je : grid[(size_t)cell(yu, y0, cy) * ng + cell(xu, x0, cx)]) {
+          if (best >= 0 && je > best) continue;
+          const int *k = nv + 3 * je;
+          const double xa = xg[k[0]], ya = yg[k[0]], xb = xg[k[1]], yb = yg[k[1]], xc = xg[k[2]], yc = yg[k[2]];
+          const double det = (xb - xa) * (yc - ya) - (xc - xa) * (yb - ya);
+          double l[3];
+          l[1] = ((xu - xa) * (yc - ya) - (xc - xa) * (yu - ya)) / det;
+          l[2] = ((xb - xa) * (yu - ya) - (xu - xa) * (yb - ya)) / det;
+          l[0] = 1. - l[1] - l[2];
+          if (l[0] < -1e-9 || l[1] < -1e-9 || l[2] < -1e-9) continue;
+          best = je;
+          for (int i = 0; i < 3; i++) lb[i] = l[i];
+        }
+        if (best < 0) continue;
+        double sum = 0.;
+        for (int i = 0; i < 3; i++) { lb[i] = std::min(1., std::max(0., lb[i])); sum += lb[i]; }
+        int xb[3];
+        for (int i = 0; i < 3; i++) {
+          const float f = (float)(lb[i] / sum);
+          memcpy(&xb[i], &f, sizeof f);
+        }
+        t = make_int4(e0 + best, xb[0], xb[1], xb[2]);
+      }
+}
+
 static int next_pow2(int n) {
   int s = 1;
   while (s < n) s <<= 1;
@@ -735,8 +803,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: itvdv=%d: upwind (0) or TVD (1) only", b, Pp[b].itvdv));
     if (Pp[b].itvdv == 1 && Pp[b].aapar != 0.f)   // concentration_omp.f90:218-226
       return bail(fail(SHY_EARG, "basin %d: vertical TVD (itvdv=1) needs aapar = 0", b));
-    if (Pp[b].itvd != 0 && Pp[b].itvd != 1)
-      return bail(fail(SHY_EARG, "basin %d: itvd=%d: upwind (0) or TVD with node gradients (1) only", b, Pp[b].itvd));
+    if (Pp[b].itvd < 0 || Pp[b].itvd > 2)
+      return bail(fail(SHY_EARG, "basin %d: itvd=%d: upwind (0), TVD with node gradients (1) or upwind points (2)", b, Pp[b].itvd));
     if (Pp[b].wetdry && !(Pp[b].hzmin > 0.f && Pp[b].hzoff >= Pp[b].hzmin && Pp[b].hzon >= Pp[b].hzoff))
       return bail(fail(SHY_EARG, "basin %d: wetting and drying needs 0 < hzmin <= hzoff <= hzon", b));
     NLV = std::max(NLV, bs.nlv);
@@ -757,6 +825,9 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   std::vector<float> visv((size_t)NKN * (NLV + 1), 0.f), difv((size_t)NKN * (NLV + 1), 0.f);
   std::vector<float> taux(NKN), tauy(NKN), ppv(NKN), rqv(NKN), areakv((size_t)NKN * NLV, 0.f);
   std::vector<float2> avol((size_t)NKN * NLV, make_float2(0.f, 0.f));
+  bool any_up = false;                                  // some basin uses itvd = 2
+  for (int b = 0; b < nbasin; b++) any_up |= Pp[b].itvd == 2;
+  std::vector<int4> tvdup(any_up ? (size_t)6 * NEL : 0);
   std::vector<float> hlv((size_t)nbasin * NLV, 0.f), hldv((size_t)nbasin * NLV, 0.f), tide;
   std::vector<int> rowptr(1, 0), col, slot_ptr(1, 0), slot_src, inc_ptr(1, 0), inc;
   std::vector<int4> incx;
@@ -771,6 +842,9 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     ST_TRY(compute_ev(nkn, nel, bs.nen3v, bs.xgv, bs.ygv, ev));
     std::vector<int> nv((size_t)3 * nel);
     for (size_t i = 0; i < nv.size(); i++) nv[i] = bs.nen3v[i] - 1;
+    if (p.itvd == 2) build_tvd_upwind(nkn, nel, nv.data(), bs.xgv, bs.ygv, e0, tvdup.data() + (size_t)6 * e0);
+    else if (any_up)
+      for (size_t i = 0; i < (size_t)6 * nel; i++) tvdup[(size_t)6 * e0 + i] = make_int4(-1, 0, 0, 0);
     {   // nodes whose fan of elements closes (angles sum to 360 degrees, setnod)
       std::vector<double> wink(nkn, 0.);
       for (int ie = 0; ie < nel; ie++)
@@ -973,6 +1047,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     return bail(SHY_ECAPACITY);
   if (m->any_adv && A.alloc(&d.mom, (size_t)NKN * NLV)) return bail(SHY_ECAPACITY);
   if (m->any_tvd && A.alloc(&d.tgrad, (size_t)nsc_max * NKN * NLV)) return bail(SHY_ECAPACITY);
+  if (any_up && A.upload(&d.tvdup, tvdup)) return bail(SHY_ECAPACITY);
   for (int i = 0; i < 2; i++) {
     if (A.alloc(&m->zbuf[i], NKN) || A.alloc(&m->zebuf[i], (size_t)3 * NEL) ||
         A.alloc(&m->ubuf[i], EL) || A.alloc(&m->vbuf[i], EL) || A.alloc(&m->hkbuf[i], NL) ||

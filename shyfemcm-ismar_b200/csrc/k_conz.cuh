@@ -86,19 +86,22 @@ __global__ void __launch_bounds__(256) k_tvdgrad(Dev d, const int *kbas, int j_a
   }
 }
 
-// tvd_fluxes (tvd_admin.f90:673-838), itvd = 1: the horizontal flux of
+// tvd_fluxes (tvd_admin.f90:673-838), itvd 1 or 2: the horizontal flux of
 // vertex `own` (0..2) of an element layer, replacing the upwind one.  The
 // pairs (ic, id) of the one vertex with outflow (itot 1) or inflow (itot 2)
 // and each other vertex carry the concentration of ic corrected towards id
-// by the superbee limiter of the ratio of the gradient at ic (node
-// gradients, g) to the difference along the side.  kv: node of each vertex,
+// by the superbee limiter of the ratio of the upwind difference to the
+// difference along the side: the node gradient at ic (g, itvd 1), or the
+// value at the point beyond ic opposite id interpolated in the element
+// holding it (Dev::tvdup, itvd 2).  kv: node of each vertex,
 // u, v: the element's velocity, aj24 = 24 ev(10) (twice the area); the side
 // length is aj24 |(b, c)| of the opposite vertex (ev(17..19)).
 __device__ __forceinline__ float tvd_flux_own(int own, int itot, int isum, const float (&f3)[3],
                                               const float (&c3)[3], const float (&bb)[3],
                                               const float (&cc)[3], const int (&kv)[3], float aj24,
                                               float u, float v, float dt, const float2 *g, int NLV,
-                                              int lane) {
+                                              int lane, const Dev &d, int e, int itvd, const float *cs,
+                                              bool istmp) {
   if (itot < 1 || itot > 2) return 0.f;
   const int itot2 = itot - 1, itot1 = 2 - itot;
   const int ip = itot2 * (6 - isum) + itot1 * isum;          // 1-based
@@ -120,9 +123,24 @@ __device__ __forceinline__ float tvd_flux_own(int own, int itot, int isum, const
     const float dis = aj24 * sqrtf(bo * bo + co * co);
     const float vel = fabsf(u * dx + v * dy) / dis;
     const float alfa = dt * vel / dis;
-    const int kc = ic == 1 ? kv[0] : (ic == 2 ? kv[1] : kv[2]);
-    const float2 gc = g[(size_t)kc * NLV + lane];
-    const float grad = 2.f * (gc.x * dx + gc.y * dy);
+    float grad;
+    if (itvd == 1) {
+      const int kc = ic == 1 ? kv[0] : (ic == 2 ? kv[1] : kv[2]);
+      const float2 gc = g[(size_t)kc * NLV + lane];
+      grad = 2.f * (gc.x * dx + gc.y * dy);
+    } else {
+      // itvd 2: the value at the point beyond ic opposite id
+      // (tvd_get_upwind_c, tvd_admin.f90:608-671), cond where it has no layer
+      float conu = cond;
+      const int4 t = d.tvdup[(size_t)e * 6 + 2 * (ic - 1) + ((id - ic + 3) % 3 - 1)];
+      if (t.x >= 0 && lane < d.ilhv[t.x]) {
+        const int4 tn = d.enode[t.x];
+        conu = __int_as_float(t.y) * clipc(cs[(size_t)tn.x * NLV + lane], istmp) +
+               __int_as_float(t.z) * clipc(cs[(size_t)tn.y * NLV + lane], istmp) +
+               __int_as_float(t.w) * clipc(cs[(size_t)tn.z * NLV + lane], istmp);
+      }
+      grad = cond - conu;
+    }
     const float rf = fabsf(conc - cond) < 1.e-8f ? -1.f : grad / (cond - conc) - 1.f;
     const float psi = fmaxf(0.f, fmaxf(fminf(1.f, 2.f * rf), fminf(2.f, rf)));   // superbee
     const float conf = conc + 0.5f * psi * (cond - conc) * (1.f - alfa);
@@ -248,7 +266,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
         const float fii = sel3(f3, ii);
         // horizontal TVD (concentration_omp.f90:675-686) where no vertex is
         // on an open boundary, with the element velocity of the new level
-        const bool tvd = P.itvd == 1 && !isbnd && d.kbnd[kja] <= 0 && d.kbnd[kjb] <= 0;
+        const bool tvd = P.itvd >= 1 && !isbnd && d.kbnd[kja] <= 0 && d.kbnd[kjb] <= 0;
         float ue = 0.f, ve = 0.f;
         int kv[3] = {k, k, k};
         if (tvd) {
@@ -275,7 +293,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
           } else fl = 0.f;
           if (tvd)
             fl = tvd_flux_own(ii, itot, isum, f3, c3, bb, cc, kv, 24.f * e1.z, ue, ve, dt,
-                              d.tgrad + sidx[r] * SN, NLV, lane);
+                              d.tgrad + sidx[r] * SN, NLV, lane, d, e, P.itvd, cs, istmp[r]);
           float hdif = 0.f;
           if (rk[r] != 0.f) {
             float wdiff = 0.f;

@@ -243,16 +243,19 @@ def test_momentum_advection(small3d, shape):
     assert np.abs(lin.state()["utlnv"] - so["utlnv"])[me].max() > 10e-3 * umax
 
 
+@pytest.mark.parametrize("itvd", [1, 2])
 @pytest.mark.parametrize("shape", ["basin3d", "lagoon30"])
-def test_tvd_transport(small3d, shape):
-    """itvd = 1: horizontal TVD fluxes (tvd_fluxes, tvd_admin.f90:673-838)
+def test_tvd_transport(small3d, shape, itvd):
+    """Horizontal TVD fluxes (tvd_fluxes, tvd_admin.f90:673-838): itvd 1
     with node gradients recomputed before every sub-step (tvd_grad_3d
-    :478-550): temperature and salinity of the 3D basin, three tracers on
-    the 30-layer sigma lagoon."""
+    :478-550), itvd 2 with the value at the point beyond the upwind vertex
+    (tvd_upwind_init_elem :361-476, tvd_get_upwind_c :608-671): temperature
+    and salinity of the 3D basin, three tracers on the 30-layer sigma
+    lagoon."""
     if shape == "basin3d":
-        c, n, fields = with_params(small3d, itvd=1), 120, ("tempv", "saltv")
+        c, n, fields = with_params(small3d, itvd=itvd), 120, ("tempv", "saltv")
     else:
-        c, n, fields = with_params(cases.lagoon_case(nkn_target=900, nlv=30), itvd=1), 80, ("conzv",)
+        c, n, fields = with_params(cases.lagoon_case(nkn_target=900, nlv=30), itvd=itvd), 80, ("conzv",)
     g, o = run_both(c, n)
     sg, so = g.get_state(0), o.state()
     assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
@@ -265,10 +268,11 @@ def test_tvd_transport(small3d, shape):
             a, r = a[m], r[m]
         rel = np.abs(a - r).max() / np.abs(r).max()
         assert rel <= TRACER_RTOL, (f, rel)
+    # the limiter changes the tracers by far more than the parity tolerance
     up = shyref.OracleModel(with_params(c, itvd=0))
     up.run(n)
     f = fields[-1]
-    assert np.abs(up.state()[f] - so[f]).max() > 100 * TRACER_RTOL * np.abs(so[f]).max()
+    assert np.abs(up.state()[f] - so[f]).max() > 10 * TRACER_RTOL * np.abs(so[f]).max()
 
 
 @pytest.mark.parametrize("shape", ["basin3d", "lagoon30"])

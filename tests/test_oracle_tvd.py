@@ -65,3 +65,27 @@ def test_vertical_tvd_keeps_more_stratification():
     o.run(40)
     act = np.arange(12)[None, :] < c["ilhkv"][:, None]
     assert np.abs(o.state()["conzv"][:, act] - 5.0).max() <= 1e-6
+
+
+def test_upwind_point_tvd():
+    """itvd = 2 (tvd_upwind_init_elem and tvd_get_upwind_c,
+    tvd_admin.f90:361-476, 608-671): the limiter's upwind difference from
+    the value at the point beyond the upwind vertex.  A uniform tracer stays
+    uniform; the tracers keep more variance than with upwind fluxes and stay
+    within their initial range."""
+    c = lagoon(2, conz=5.0)
+    o = shyref.OracleModel(c)
+    o.run(40)
+    act = np.arange(12)[None, :] < c["ilhkv"][:, None]
+    assert np.abs(o.state()["conzv"][:, act] - 5.0).max() <= 1e-6
+    out = {}
+    for itvd in (0, 2):
+        o = shyref.OracleModel(lagoon(itvd))
+        o.run(80)
+        out[itvd] = o.state()["conzv"]
+    c2 = lagoon(2)
+    lo, hi = float(c2["conzv"].min()), float(c2["conzv"].max())
+    tol = 1e-3 * (hi - lo)
+    assert out[2][:, act].min() >= lo - tol and out[2][:, act].max() <= hi + tol
+    for t in range(out[2].shape[0]):
+        assert np.var(out[2][t][act]) > np.var(out[0][t][act])
