@@ -204,6 +204,15 @@ int shygpu_step_info(shygpu_model *model, int32_t ibasin, shy_step_info *info);
 int shygpu_set_forcing(shygpu_model *model, int32_t ibasin, const float *tauxnv,
                        const float *tauynv, const float *ppv, const float *rqv);
 
+/* Water-level nudging of basin ib (hydro_zeta, hydrodynamic.f90:612,
+ * 677-679): andgzv(nkn), the per-node contribution that the reference's
+ * nudge_zeta (nudge.f90:300-338) makes from its observation stations,
+ * enters each element's right-hand side as 4 aj dt andgzv.  The caller
+ * computes it from its observations; it stays in force until set again.
+ * The first call for a model allocates the array and rebuilds its step
+ * graph.                                                                   */
+int shygpu_set_nudging(shygpu_model *model, int32_t ibasin, const float *andgzv);
+
 /* Tuning options by name: "use_graph" (CUDA-graph replay of whole steps,
  * the transport sub-step loop as a device-driven conditional node; default
  * 1), "cluster_size" and "zeta_threads" (shape of the per-basin cluster of

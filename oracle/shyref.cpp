@@ -447,6 +447,7 @@ struct Model {
   std::vector<int> iwegv, iwetv, inodv;
   std::vector<double> uov, vov;             // barotropic transports of the old level
   std::vector<double> uprv, vprv;           // nodal velocities (mod_hydro_print), make_prvel
+  std::vector<double> andgzv;               // water-level nudging contribution per node (mod_nudging)
   // itvd = 2: per element and ordered vertex pair (c, d) the element holding
   // the point 2 x_c - x_d and its barycentric weights there (tvd_upwind_init_elem)
   std::vector<int> tvdup_e;                 // [6*ie + slot], -1 outside the basin
@@ -902,7 +903,7 @@ void element_system(Model &m, int ie, int kn[3], double hia[3][3], double hik[3]
     kn[i] = m.nen3v[3 * ie + i];
     b[i] = e[3 + i]; c[i] = e[6 + i];
     z[i] = m.zeov[3 * ie + i];
-    zndg[i] = 0.;                       // andgzv: no nudging
+    zndg[i] = m.andgzv.empty() ? 0. : m.andgzv[kn[i]];   // andgzv (nudge.f90:333)
   }
   int ilevel = m.ilhv[ie];
   double aj = e[9];
@@ -1997,6 +1998,15 @@ int shyref_wetdry(void *h, int *iwegv, int *iwetv, int *inodv) {
     if (iwetv) iwetv[ie] = m->iwetv.empty() ? 0 : m->iwetv[ie];
   }
   if (inodv) for (int k = 0; k < m->nkn; k++) inodv[k] = m->inodv.empty() ? 0 : m->inodv[k];
+  return SHY_OK;
+}
+
+// the nudging contribution andgzv per node (nudge_zeta, nudge.f90:300-338,
+// computed by the caller from its observations); NULL clears it
+int shyref_set_nudging(void *h, const float *andgzv) {
+  Model &m = *(Model *)h;
+  if (!andgzv) { m.andgzv.clear(); return SHY_OK; }
+  m.andgzv.assign(andgzv, andgzv + m.nkn);
   return SHY_OK;
 }
 

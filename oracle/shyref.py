@@ -39,6 +39,7 @@ def _lib():
     lib.shyref_destroy.argtypes = [C.c_void_p]
     lib.shyref_set_state.argtypes = [C.c_void_p, C.POINTER(abi.ShyState)]
     lib.shyref_run.argtypes = [C.c_void_p, C.c_int]
+    lib.shyref_set_nudging.argtypes = [C.c_void_p, C.c_void_p]
     lib.shyref_step_info.argtypes = [C.c_void_p, C.POINTER(abi.ShyStepInfo)]
     lib.shyref_get_state64.argtypes = [C.c_void_p] + [d_p] * 11
     lib.shyref_last_system.argtypes = [C.c_void_p, i_p, d_p, d_p]
@@ -177,6 +178,12 @@ class OracleModel:
         lib.shyref_wetdry(self.h, iweg.ctypes.data_as(i32), iwet.ctypes.data_as(i32),
                           inod.ctypes.data_as(i32))
         return iweg, iwet, inod
+
+    def set_nudging(self, andgzv):
+        """The water-level nudging contribution per node (andgzv), or None."""
+        a = None if andgzv is None else np.ascontiguousarray(andgzv, np.float32)
+        self._andg = a
+        check(lib.shyref_set_nudging(self.h, None if a is None else a.ctypes.data), "set_nudging")
 
     def last_system(self):
         nnz = C.c_int(0)

@@ -70,6 +70,7 @@ struct Dev {
   int any_tvd;                  // some basin transports with TVD (a gradient pass per sub-step)
   float2 *tgrad;                // (nsc_max*NKN*NLV) node gradients {gx, gy} of the sub-step's scalars
   int4 *tvdup;                  // (6*NEL) itvd = 2: {element, xi0, xi1, xi2 as float bits} per vertex pair
+  float *andg;                  // (NKN) water-level nudging contribution andgzv, or null (none set)
   BasinPar *par;
   BasinOut *out;
   // mesh (static)

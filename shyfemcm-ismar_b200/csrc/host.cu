@@ -1476,6 +1476,18 @@ extern "C" int shygpu_set_forcing(shygpu_model *m, int32_t ib, const float *taux
   return SHY_OK;
 }
 
+extern "C" int shygpu_set_nudging(shygpu_model *m, int32_t ib, const float *andgzv) {
+  if (!m || ib < 0 || ib >= m->nbasin || !andgzv) return fail(SHY_EARG, "set_nudging: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  if (!m->base.andg) {             // first use: the array (zeros elsewhere) and new graphs that read it
+    CUDA_TRY(cudaStreamSynchronize(m->stream));
+    if (m->arena.alloc(&m->base.andg, (size_t)m->NKN)) return SHY_ECAPACITY;
+    drop_graphs(m);
+  }
+  CUDA_TRY(cudaMemcpyAsync(m->base.andg + bp.k0, andgzv, (size_t)bp.nk * 4, cudaMemcpyHostToDevice, m->stream));
+  return SHY_OK;
+}
+
 extern "C" void *shygpu_model_stream(shygpu_model *m) { return m ? (void *)m->stream : nullptr; }
 
 extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_out, int32_t *count_out) {

@@ -253,7 +253,9 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
       const double acn = c[n] * (b[m] * dcb + c[m] * dcc);
       hia[n][m] = aj * ((n == m ? 4. : 0.) + 12. * delta * (abn + acn));
     }
-    hik[n] = hia[n][0] * z[0] + hia[n][1] * z[1] + hia[n][2] * z[2] + 12. * aj * dt * (ut * b[n] + vt * c[n]);
+    // the nudging term 4 aj dt andgzv (hydrodynamic.f90:677-679), where set
+    const double andg = d.andg ? 4. * aj * dt * (double)d.andg[kn[n]] : 0.;
+    hik[n] = hia[n][0] * z[0] + hia[n][1] * z[1] + hia[n][2] * z[2] + andg + 12. * aj * dt * (ut * b[n] + vt * c[n]);
   }
   // level boundary conditions (:688-704), rzv at the new time (sp111)
   const double tnew = d.out[en.w].dtime + dt;

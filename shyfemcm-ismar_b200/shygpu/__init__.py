@@ -74,6 +74,7 @@ def lib():
     L.shygpu_new_step.argtypes = [C.c_void_p]
     L.shygpu_step_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyStepInfo)]
     L.shygpu_get_wetdry.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3
+    L.shygpu_set_nudging.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     L.shygpu_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
     L.shygpu_get_option.argtypes = [C.c_void_p, C.c_char_p]
     L.shygpu_get_option.restype = C.c_double
@@ -200,6 +201,12 @@ class Model:
                 raise ValueError("forcing arrays must be contiguous float32")
         check(lib().shygpu_set_forcing(self.h, ib, p(tauxnv), p(tauynv), p(ppv), p(rqv)),
               "set_forcing")
+
+    def set_nudging(self, ib, andgzv):
+        """Water-level nudging contribution andgzv (per node, float32) of basin ib."""
+        a = np.ascontiguousarray(andgzv, np.float32)
+        check(lib().shygpu_set_nudging(self.h, ib, a.ctypes.data), "set_nudging")
+        lib().shygpu_sync(self.h)
 
     KERNELS = ("column", "zeta", "final", "node", "stab", "reduce", "conz", "rho")
 

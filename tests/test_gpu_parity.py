@@ -298,3 +298,28 @@ def test_vertical_tvd_transport(small3d, shape):
     up.run(n)
     f = fields[0]
     assert np.abs(up.state()[f] - so[f]).max() > 10 * TRACER_RTOL * np.abs(so[f]).max()
+
+
+def test_water_level_nudging(channel):
+    """andgzv (hydrodynamic.f90:612, 677-679): a per-node nudging
+    contribution in the element right-hand sides, set through
+    shygpu_set_nudging after the model's step graph exists (the first call
+    rebuilds it)."""
+    c = channel
+    andg = (2e-4 * np.sin(c["xgv"] / 1.5e3) * np.cos(c["ygv"] / 700.0)).astype(np.float32)
+    g = shygpu.Model(c)
+    g.set_state(0)
+    g.run(10)
+    o = shyref.OracleModel(c)
+    o.run(10)
+    g.set_nudging(0, andg)
+    o.set_nudging(andg)
+    g.run(1430)                      # to the day's end, as the channel test (not at slack water)
+    o.run(1430)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    umax = np.abs(so["utlnv"]).max()
+    assert np.abs(sg["utlnv"] - so["utlnv"]).max() <= 1e-3 * umax
+    free = shyref.OracleModel(c)
+    free.run(1440)
+    assert np.abs(free.state()["znv"] - so["znv"]).max() > 5 * ZETA_TOL
