@@ -100,7 +100,9 @@ typedef struct shy_params {
   float solver_atol;         /*   (sparskit_admin.f90:270-277: 1e-8, 1e-8)  */
   int32_t solver_maxit;      /* iteration limit (sparskit_admin.f90:141)    */
   int32_t nsigma;            /* sigma layers (levels :: nsigma): 0 z-layers, */
-                             /*   nlv pure sigma (hlv/hldv sigma values < 0) */
+                             /*   nlv pure sigma (hlv/hldv sigma values < 0),*/
+                             /*   between: hybrid, z-layers below hsigma and */
+                             /*   hlv(nsigma) = hsigma (initialize.f90:556)  */
   float hsigma;              /* depth limit of the sigma layers (hsigma)    */
   int32_t wetdry;            /* 1: wetting and drying of elements (setweg) */
   float hzmin, hzon, volmin; /* its thresholds       def_para.f90:744-746,1762 */

@@ -513,79 +513,61 @@ void set_ieltv(Model &m) {
     }
 }
 
-// setdepth (elems_dealing.f90:930-1160) for z-layers (nsigma = 0) and for
-// pure sigma layers (nsigma = nlv), without z-adaptive layers
-// (compute_zadaptive_info returns nadapt = ladapt = 0, zadaptutil.f90:321-324).
+// setdepth (elems_dealing.f90:930-1160) for z-layers (nsigma = 0), pure
+// sigma layers (nsigma = nlv) and hybrid layers (nsigma sigma layers down to
+// hsigma, z-layers below), without z-adaptive layers (compute_zadaptive_info
+// returns nadapt = ladapt = 0, zadaptutil.f90:321-324).  Sigma layers take
+// the fraction -hldv(l) of the total depth min(h, hsigma) + z: at the nodes
+// from each element's vertex values in element order, the last element
+// writing (:1010-1025), at the elements from hev and the mean water level
+// (:1075-1085).  z-layers take their nominal thickness, the first one (with
+// no sigma layers above) plus z, the last one down to the bottom; at the
+// nodes as area-weighted means over the elements (:1026-1050, 1129-1140).
 int setdepth(Model &m, std::vector<double> &hdkn, std::vector<double> &hden,
              const std::vector<double> &zenv) {
-  int nlv = m.nlv;
+  const int nlv = m.nlv, nsigma = m.p.nsigma;
+  const double hsigma = (double)(float)(m.p.hsigma > 0.f ? m.p.hsigma : 10000.f);
   hdkn.assign((size_t)nlv * m.nkn, 0.);
   hden.assign((size_t)nlv * m.nel, 0.);
-  if (m.p.nsigma > 0) {
-    // sigma layers: the thickness is the sigma fraction -hldv(l) of the
-    // total depth min(h, hsigma) + z, at the nodes from each element's
-    // vertex values in element order (:1010-1025, the last element writes),
-    // at the elements from hev and the mean water level (:1075-1085)
-    const double hsigma = (double)(float)(m.p.hsigma > 0.f ? m.p.hsigma : 10000.f);
-    for (int ie = 0; ie < m.nel; ie++) {
-      double zmed = 0.;
-      for (int ii = 0; ii < 3; ii++) {
-        const int k = m.nen3v[3 * ie + ii];
-        const double z = zenv[3 * ie + ii];
-        zmed += z;
-        const double hsig = std::min(m.hm3v[3 * ie + ii], hsigma) + z;
-        for (int l = 1; l <= m.p.nsigma; l++) hdkn[(size_t)k * nlv + l - 1] = -hsig * m.hldv[l - 1];
-      }
-      zmed /= 3.;
-      const double hsig = std::min(m.hev[ie], hsigma) + zmed;
-      for (int l = 1; l <= m.p.nsigma; l++) {
-        hden[(size_t)ie * nlv + l - 1] = -hsig * m.hldv[l - 1];
-        if (hden[(size_t)ie * nlv + l - 1] <= 0.) return fail(SHY_EDEPTH, "setdepth: no layer depth in element");
-      }
-    }
-    for (int k = 0; k < m.nkn; k++)
-      for (int l = 1; l <= m.ilhkv[k]; l++)
-        if (hdkn[(size_t)k * nlv + l - 1] <= 0.) return fail(SHY_EDEPTH, "setdepth: no layer depth in node");
-    return SHY_OK;
-  }
-  double hl[3][SHY_MAX_LAYERS > 64 ? SHY_MAX_LAYERS : 64];
   for (int ie = 0; ie < m.nel; ie++) {
-    double areafv = 12. * m.ev[(size_t)ie * SHY_EVDIM + 9] / 3.;
-    int lmax = m.ilhv[ie], lmin = 1;
+    const double areafv = 12. * m.ev[(size_t)ie * SHY_EVDIM + 9] / 3.;
+    const int lmax = m.ilhv[ie], lmin = 1;
     double zmed = 0.;
     for (int ii = 0; ii < 3; ii++) {
-      int k = m.nen3v[3 * ie + ii];
-      int lmink = 1;
-      double htot = m.hm3v[3 * ie + ii];
-      double z = zenv[3 * ie + ii];
+      const int k = m.nen3v[3 * ie + ii];
+      const int lmink = 1;
+      const double htot = m.hm3v[3 * ie + ii];
+      const double z = zenv[3 * ie + ii];
       zmed += z;
+      const double hsig = std::min(htot, hsigma) + z;
+      for (int l = 1; l <= nsigma; l++) hdkn[(size_t)k * nlv + l - 1] = -hsig * m.hldv[l - 1];
+      if (lmax <= nsigma) continue;
       if (lmax == lmin) {
-        hl[ii][lmin] = htot + z;
-        hdkn[(size_t)k * nlv + lmin - 1] += areafv * hl[ii][lmin];
+        hdkn[(size_t)k * nlv + lmin - 1] += areafv * (htot + z);
       } else {
-        int levmin = lmink;
-        for (int l = levmin; l <= lmax - 1; l++) {
-          hl[ii][l] = m.hldv[l - 1];
-          hdkn[(size_t)k * nlv + l - 1] += areafv * hl[ii][l];
-        }
-        hl[ii][lmink] += z;
-        hdkn[(size_t)k * nlv + lmink - 1] += areafv * z;
-        double hlast = htot - m.hlv[lmax - 2];
+        const int levmin = nsigma + lmink;
+        for (int l = levmin; l <= lmax - 1; l++) hdkn[(size_t)k * nlv + l - 1] += areafv * m.hldv[l - 1];
+        if (levmin == lmink) hdkn[(size_t)k * nlv + lmink - 1] += areafv * z;
+        const double hlast = htot - m.hlv[lmax - 2];
         if (hlast < 0.) return fail(SHY_EDEPTH, "setdepth: last layer negative");
-        hl[ii][lmax] = hlast;
-        hdkn[(size_t)k * nlv + lmax - 1] += areafv * hl[ii][lmax];
+        hdkn[(size_t)k * nlv + lmax - 1] += areafv * hlast;
       }
     }
     zmed /= 3.;
-    double htot = m.hev[ie];
-    if (lmax == lmin) {
-      hden[(size_t)ie * nlv + lmin - 1] = htot + zmed;
-    } else {
-      for (int l = lmin; l <= lmax - 1; l++) hden[(size_t)ie * nlv + l - 1] = m.hldv[l - 1];
-      hden[(size_t)ie * nlv + lmin - 1] += zmed;
-      double hlast = htot - m.hlv[lmax - 2];
-      if (hlast < 0.) return fail(SHY_EDEPTH, "setdepth: last layer negative");
-      hden[(size_t)ie * nlv + lmax - 1] = hlast;
+    const double htot = m.hev[ie];
+    const double hsig = std::min(htot, hsigma) + zmed;
+    for (int l = 1; l <= nsigma; l++) hden[(size_t)ie * nlv + l - 1] = -hsig * m.hldv[l - 1];
+    if (lmax > nsigma) {
+      if (lmax == lmin) {
+        hden[(size_t)ie * nlv + lmin - 1] = htot + zmed;
+      } else {
+        const int levmin = nsigma + lmin;
+        for (int l = levmin; l <= lmax - 1; l++) hden[(size_t)ie * nlv + l - 1] = m.hldv[l - 1];
+        if (levmin == lmin) hden[(size_t)ie * nlv + lmin - 1] += zmed;
+        const double hlast = htot - m.hlv[lmax - 2];
+        if (hlast < 0.) return fail(SHY_EDEPTH, "setdepth: last layer negative");
+        hden[(size_t)ie * nlv + lmax - 1] = hlast;
+      }
     }
     for (int l = lmin; l <= lmax; l++)
       if (hden[(size_t)ie * nlv + l - 1] <= 0.)
@@ -593,8 +575,8 @@ int setdepth(Model &m, std::vector<double> &hdkn, std::vector<double> &hden,
                                     " layer " + std::to_string(l));
   }
   for (int k = 0; k < m.nkn; k++) {
-    for (int l = 1; l <= m.ilhkv[k]; l++) {
-      double a = m.areakv[(size_t)k * nlv + l - 1];
+    for (int l = nsigma + 1; l <= m.ilhkv[k]; l++) {
+      const double a = m.areakv[(size_t)k * nlv + l - 1];
       if (a > 0.) hdkn[(size_t)k * nlv + l - 1] /= a;
       else break;
     }
@@ -1918,7 +1900,7 @@ void *shyref_create(const shy_basin *B, const shy_params *P) {
   m->nkn = B->nkn; m->nel = B->nel; m->nlv = B->nlv; m->p = *P;
   int nkn = m->nkn, nel = m->nel, nlv = m->nlv;
   if (nlv < 1 || nlv > SHY_MAX_LAYERS) { fail(SHY_EARG, "shyref_create: nlv"); delete m; return nullptr; }
-  if (P->nsigma != 0 && P->nsigma != nlv) { fail(SHY_EARG, "shyref_create: nsigma 0 or nlv"); delete m; return nullptr; }
+  if (P->nsigma < 0 || P->nsigma > nlv) { fail(SHY_EARG, "shyref_create: nsigma outside 0..nlv"); delete m; return nullptr; }
   m->nen3v.resize((size_t)3 * nel);
   for (size_t i = 0; i < m->nen3v.size(); i++) m->nen3v[i] = B->nen3v[i] - 1;
   std::vector<double> x = dv(B->xgv, nkn), y = dv(B->ygv, nkn);

@@ -39,7 +39,7 @@ struct BasinPar {
   int maxit;
   int has_cor;
   int is_temp[kMaxScal];      // scalar s is temperature (no clipping at 1e-15)
-  int nsigma;                 // 0: z-layers; nlv: pure sigma layers
+  int nsigma;                 // sigma layers on top (0: z-layers; nlv: pure sigma; between: hybrid)
   float hsigma;               // depth limit of the sigma layers
   int wetdry;                 // wetting and drying of elements (z-layers)
   float hzmin, hzon, volmin;  // its thresholds

@@ -795,8 +795,10 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     if (Pp[b].nconz < 0 || Pp[b].nconz > SHY_MAX_CONZ) return bail(fail(SHY_EARG, "basin %d: nconz", b));
     if (Pp[b].ireib != 0 && Pp[b].ireib != 5) return bail(fail(SHY_EARG, "basin %d: ireib=%d not supported (0 or 5)", b, Pp[b].ireib));
     if (!(Pp[b].dt > 0)) return bail(fail(SHY_EARG, "basin %d: dt must be positive", b));
-    if (Pp[b].nsigma != 0 && Pp[b].nsigma != bs.nlv)
-      return bail(fail(SHY_EARG, "basin %d: nsigma=%d: z-layers (0) or pure sigma layers (nlv) only", b, Pp[b].nsigma));
+    if (Pp[b].nsigma < 0 || Pp[b].nsigma > bs.nlv)
+      return bail(fail(SHY_EARG, "basin %d: nsigma=%d outside 0..nlv", b, Pp[b].nsigma));
+    if (Pp[b].nsigma > 0 && Pp[b].nsigma < bs.nlv && !(bs.hlv[Pp[b].nsigma - 1] == (Pp[b].hsigma > 0.f ? Pp[b].hsigma : 10000.f)))
+      return bail(fail(SHY_EARG, "basin %d: hybrid levels: hlv(nsigma) must be hsigma (initialize.f90:556)", b));
     if (Pp[b].nsigma > 0 && Pp[b].ibarcl > 0)
       return bail(fail(SHY_EARG, "basin %d: baroclinic terms on sigma layers not supported", b));
     if (Pp[b].itvdv != 0 && Pp[b].itvdv != 1)

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256) k_final(Dev d, int init_only) {
   const float *hlv = d.hlv + (size_t)en.w * NLV;
   double h = 0.;
   if (act) {
-    if (P.nsigma > 0) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[lane];   // :1079-1083
+    if (lane < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[lane];   // :1079-1083
     else if (ilevel == 1) h = hm.w + zmed;
     else if (lane < ilevel - 1) h = (double)hld[lane] + (lane == 0 ? zmed : 0.);
     else h = (double)hm.w - hlv[ilevel - 2];
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
   for (int l = 0; l < NLV; l++) {
     double h = 0.;
     if (l < ilevel) {
-      if (P.nsigma > 0) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // :1079-1083
+      if (l < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // sigma layers (:1079-1083)
       else if (ilevel == 1) h = hm.w + zmed;
       else if (l < ilevel - 1) h = (double)hld[l] + (l == 0 ? zmed : 0.);
       else h = (double)hm.w - hlv[ilevel - 2];
@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(128) k_final_w(Dev d, int init_only) {
     for (int l = 0; l < NLV; l++) {
       double h = 0.;
       if (l < ilevel) {
-        if (P.nsigma > 0) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // :1079-1083
+        if (l < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // sigma layers (:1079-1083)
         else if (ilevel == 1) h = hm.w + zmed;
         else if (l < ilevel - 1) h = (double)hld[l] + (l == 0 ? zmed : 0.);
         else h = (double)hm.w - hlv[ilevel - 2];

@@ -55,7 +55,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   const size_t o = (size_t)k * NLV + lane;
   const double area = act ? (double)d.areakv[o] : 0.;
   double hk = act && area > 0. ? hsum / area : 0.;
-  if (P.nsigma > 0 && act) hk = -(fmin(hsig_h, (double)P.hsigma) + z) * hldl;   // sigma (:1019-1025)
+  if (lane < P.nsigma && act) hk = -(fmin(hsig_h, (double)P.hsigma) + z) * hldl;   // sigma layers (:1019-1025)
   float hkf = (float)hk;
   if (act && !(hkf > 0.f) && valid) set_status(&d.out[b], SHY_EDEPTH);
   if (valid && lane < NLV) d.hkn[o] = act ? hkf : 0.f;
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
     const bool act = l < lmax;
     area[l] = act ? (double)d.areakv[o + l] : 0.;
     double hk = act && area[l] > 0. ? (double)(hsum[l] / (float)area[l]) : 0.;
-    if (P.nsigma > 0 && act) hk = -(fmin(hsig_h, (double)P.hsigma) + z) * (double)hld[l];   // sigma (:1019-1025)
+    if (l < P.nsigma && act) hk = -(fmin(hsig_h, (double)P.hsigma) + z) * (double)hld[l];   // sigma layers (:1019-1025)
     hkf[l] = (float)hk;
     if (act && !(hkf[l] > 0.f)) bad = true;
     d.hkn[o + l] = act ? hkf[l] : 0.f;

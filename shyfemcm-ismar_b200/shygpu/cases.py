@@ -248,6 +248,40 @@ def lagoon_case(nkn_target=3000, lx=12.0e3, ly=6.0e3, seed=7, dt=30.0, nlv=30, n
     return _finish(case)
 
 
+def hybrid_lagoon_case(nkn_target=900, nsigma=6, hsigma=8.0, dz=3.0, seed=7, dt=30.0, ntracer=3,
+                       hmin=1.5, hmax=30.0):
+    """The lagoon on hybrid layers: `nsigma` equal sigma layers down to
+    `hsigma`, z-layers of `dz` below (hlv(nsigma) = hsigma, as the
+    reference's level set-up makes it, initialize.f90:550-558).  Elements
+    deeper than hsigma on average get a flat bottom at their mean depth
+    (flatten_hm3v, depth_util.f90:603-629); an element has the nsigma
+    sigma layers, plus the z-layers down to its depth when it is deeper than
+    hsigma (set_ilhv, initialize.f90:787-836)."""
+    c = lagoon_case(nkn_target=nkn_target, seed=seed, dt=dt, nlv=nsigma, ntracer=ntracer,
+                    hmin=hmin, hmax=hmax)
+    nkn, nel = c["nkn"], c["nel"]
+    hm3v = np.asarray(c["hm3v"], np.float64).copy()
+    hev = hm3v.mean(axis=1)
+    deep = hev > hsigma
+    hm3v[deep] = hev[deep][:, None]
+    nz = int(math.ceil((hev.max() - hsigma) / dz)) if deep.any() else 0
+    nlv = nsigma + nz
+    hlv = np.r_[-np.arange(1, nsigma, dtype=np.float64) / nsigma, hsigma, hsigma + dz * np.arange(1, nz + 1)]
+    hldv = np.r_[np.full(nsigma, -1.0 / nsigma), np.full(nz, dz)]
+    ilhv = np.full(nel, nsigma, np.int32)
+    for e in np.nonzero(deep)[0]:
+        ilhv[e] = nsigma + int(np.argmax(hlv[nsigma:] >= hev[e])) + 1
+    ilhkv = np.zeros(nkn, np.int32)
+    np.maximum.at(ilhkv, c["nen3v"].ravel() - 1, np.repeat(ilhv, 3))
+    conz = np.repeat(c["conzv"][:, :, :1], nlv, axis=2)
+    c.update(name=f"lagoon_hybrid_{nkn}x{nlv}", nlv=nlv, hm3v=hm3v.astype(np.float32), hlv=hlv, hldv=hldv,
+             ilhv=ilhv, ilhkv=ilhkv, conzv=conz)
+    c["params"] = dict(c["params"], nsigma=nsigma, hsigma=hsigma)
+    for k in ("visv", "difv", "tempv", "saltv", "znv", "utlnv", "vtlnv"):
+        c.pop(k, None)
+    return _finish(c)
+
+
 def flat_case(nx=41, ny=9, lx=8.0e3, ly=1.6e3, seed=9, dt=60.0, nlv=1, ampli=1.0,
               hdeep=3.0, hshallow=-0.6):
     """Tidal flat for wetting and drying: a channel deepening linearly from

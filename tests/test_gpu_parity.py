@@ -323,3 +323,26 @@ def test_water_level_nudging(channel):
     free = shyref.OracleModel(c)
     free.run(1440)
     assert np.abs(free.state()["znv"] - so["znv"]).max() > 5 * ZETA_TOL
+
+
+@pytest.mark.parametrize("column_threads", [1, 0])
+def test_hybrid_sigma_z_layers(column_threads):
+    """Hybrid layers (setdepth, elems_dealing.f90:1010-1050, 1075-1105): six
+    sigma layers down to hsigma = 8 m, 3 m z-layers below, flat-bottomed
+    deep elements; three tracers; the thread-per-column and warp-segment
+    kernels."""
+    c = cases.hybrid_lagoon_case()
+    g, o = run_both(c, 80, column_threads=column_threads)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    m = active_mask(c)
+    assert np.abs(sg["hdknv"] - so["hdknv"])[m].max() <= 1e-4 * np.abs(so["hdknv"]).max()
+    me = active_mask(c, node=False)
+    assert np.abs(sg["hdenv"] - so["hdenv"])[me].max() <= 1e-4 * np.abs(so["hdenv"]).max()
+    umax = np.abs(so["utlnv"]).max()
+    assert np.abs(sg["utlnv"] - so["utlnv"]).max() <= 1e-3 * umax
+    cmax = np.abs(so["conzv"]).max()
+    assert np.abs(sg["conzv"] - so["conzv"]).max() <= TRACER_RTOL * cmax
+    wmax = np.abs(so["wlnv"]).max()
+    assert np.abs(sg["wlnv"] - so["wlnv"]).max() <= 2e-3 * wmax
+    assert abs(g.info(0).volume - o.info().volume) <= 1e-6 * o.info().volume
