@@ -206,6 +206,17 @@ int shygpu_step_info(shygpu_model *model, int32_t ibasin, shy_step_info *info);
 int shygpu_set_forcing(shygpu_model *model, int32_t ibasin, const float *tauxnv,
                        const float *tauynv, const float *ppv, const float *rqv);
 
+/* Checkpoints (restart.f90:445-660, made exact): every device array of the
+ * model and its time-level indices, copied to or from a host buffer of
+ * shygpu_checkpoint_bytes(model) bytes.  A checkpoint loads into the model
+ * that saved it or into one made from the same basins and parameters (and
+ * the same shygpu_set_nudging calls); the run then continues bit for bit.
+ * Loading into a model with other arrays fails with SHY_EARG.  Both calls
+ * wait for the model's stream.                                             */
+int64_t shygpu_checkpoint_bytes(const shygpu_model *model);
+int shygpu_checkpoint_save(shygpu_model *model, void *buf, int64_t nbytes);
+int shygpu_checkpoint_load(shygpu_model *model, const void *buf, int64_t nbytes);
+
 /* Water-level nudging of basin ib (hydro_zeta, hydrodynamic.f90:612,
  * 677-679): andgzv(nkn), the per-node contribution that the reference's
  * nudge_zeta (nudge.f90:300-338) makes from its observation stations,

@@ -213,6 +213,7 @@ static std::vector<T> padded(const std::vector<T> &v, size_t extra, T fill) {
 
 struct Arena {
   std::vector<void *> ptrs;
+  std::vector<size_t> sizes;         // bytes of each allocation (checkpoints)
   int64_t bytes = 0;
   template <typename T>
   int alloc(T **p, size_t n) {
@@ -222,6 +223,7 @@ struct Arena {
     if (e != cudaSuccess) return fail(SHY_ECAPACITY, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T), cudaGetErrorString(e));
     cudaMemset(*p, 0, n * sizeof(T));
     ptrs.push_back(*p);
+    sizes.push_back(n * sizeof(T));
     bytes += (int64_t)(n * sizeof(T));
     return SHY_OK;
   }
@@ -238,6 +240,7 @@ struct Arena {
   void release() {
     for (void *p : ptrs) cudaFree(p);
     ptrs.clear();
+    sizes.clear();
     bytes = 0;
   }
 };
@@ -1475,6 +1478,74 @@ extern "C" int shygpu_set_forcing(shygpu_model *m, int32_t ib, const float *taux
   if (tauy) CUDA_TRY(cudaMemcpyAsync(m->base.tauy + bp.k0, tauy, nb, cudaMemcpyHostToDevice, m->stream));
   if (ppv) CUDA_TRY(cudaMemcpyAsync(m->base.ppv + bp.k0, ppv, nb, cudaMemcpyHostToDevice, m->stream));
   if (rqv) CUDA_TRY(cudaMemcpyAsync(m->base.rqv + bp.k0, rqv, nb, cudaMemcpyHostToDevice, m->stream));
+  return SHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// checkpoints: every device array of the model (state of both time levels,
+// the derived and static arrays, per-basin results and counters) with the
+// time-level indices, so that a model made from the same inputs continues
+// bit for bit (the restart of restart.f90:445-660, exact)
+// ---------------------------------------------------------------------------
+struct CkptHeader {
+  uint64_t magic;
+  int32_t version, nalloc;
+  int64_t bytes;
+  int32_t cur, sc_cur, state_set, nbasin;
+};
+static const uint64_t kCkptMagic = 0x5348594750554350ull;   // "SHYGPUCP"
+
+extern "C" int64_t shygpu_checkpoint_bytes(const shygpu_model *m) {
+  if (!m) return -1;
+  return (int64_t)sizeof(CkptHeader) + (int64_t)sizeof(int64_t) * (int64_t)m->arena.ptrs.size() + m->arena.bytes;
+}
+
+extern "C" int shygpu_checkpoint_save(shygpu_model *m, void *buf, int64_t nbytes) {
+  if (!m || !buf || nbytes < shygpu_checkpoint_bytes(m)) return fail(SHY_EARG, "checkpoint_save: bad arguments or buffer too small");
+  if (!m->state_set) return fail(SHY_ESTATE, "checkpoint_save: set_state has not been called");
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  char *p = (char *)buf;
+  CkptHeader h{kCkptMagic, 1, (int32_t)m->arena.ptrs.size(), m->arena.bytes, m->cur, m->sc_cur, 1, m->nbasin};
+  memcpy(p, &h, sizeof h);
+  p += sizeof h;
+  for (size_t i = 0; i < m->arena.sizes.size(); i++) {
+    const int64_t sz = (int64_t)m->arena.sizes[i];
+    memcpy(p, &sz, sizeof sz);
+    p += sizeof sz;
+  }
+  for (size_t i = 0; i < m->arena.ptrs.size(); i++) {
+    CUDA_TRY(cudaMemcpy(p, m->arena.ptrs[i], m->arena.sizes[i], cudaMemcpyDeviceToHost));
+    p += m->arena.sizes[i];
+  }
+  return SHY_OK;
+}
+
+extern "C" int shygpu_checkpoint_load(shygpu_model *m, const void *buf, int64_t nbytes) {
+  if (!m || !buf || nbytes < (int64_t)sizeof(CkptHeader)) return fail(SHY_EARG, "checkpoint_load: bad arguments");
+  const char *p = (const char *)buf;
+  CkptHeader h;
+  memcpy(&h, p, sizeof h);
+  p += sizeof h;
+  if (h.magic != kCkptMagic || h.version != 1) return fail(SHY_EARG, "checkpoint_load: not a checkpoint of this library");
+  if (h.nalloc != (int32_t)m->arena.ptrs.size() || h.bytes != m->arena.bytes || h.nbasin != m->nbasin ||
+      nbytes < shygpu_checkpoint_bytes(m))
+    return fail(SHY_EARG, "checkpoint_load: the checkpoint is of a model with other arrays (same basins, "
+                          "parameters and nudging calls needed)");
+  for (size_t i = 0; i < m->arena.sizes.size(); i++) {
+    int64_t sz;
+    memcpy(&sz, p, sizeof sz);
+    p += sizeof sz;
+    if (sz != (int64_t)m->arena.sizes[i]) return fail(SHY_EARG, "checkpoint_load: array %zu differs in size", i);
+  }
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  for (size_t i = 0; i < m->arena.ptrs.size(); i++) {
+    CUDA_TRY(cudaMemcpy(m->arena.ptrs[i], p, m->arena.sizes[i], cudaMemcpyHostToDevice));
+    p += m->arena.sizes[i];
+  }
+  drop_graphs(m);
+  m->cur = h.cur;
+  m->sc_cur = h.sc_cur;
+  m->state_set = h.state_set != 0;
   return SHY_OK;
 }
 

@@ -75,6 +75,10 @@ def lib():
     L.shygpu_step_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyStepInfo)]
     L.shygpu_get_wetdry.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3
     L.shygpu_set_nudging.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.shygpu_checkpoint_bytes.argtypes = [C.c_void_p]
+    L.shygpu_checkpoint_bytes.restype = C.c_int64
+    L.shygpu_checkpoint_save.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    L.shygpu_checkpoint_load.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
     L.shygpu_set_option.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
     L.shygpu_get_option.argtypes = [C.c_void_p, C.c_char_p]
     L.shygpu_get_option.restype = C.c_double
@@ -207,6 +211,18 @@ class Model:
         a = np.ascontiguousarray(andgzv, np.float32)
         check(lib().shygpu_set_nudging(self.h, ib, a.ctypes.data), "set_nudging")
         lib().shygpu_sync(self.h)
+
+    def checkpoint(self):
+        """Every device array of the model, as a host byte array."""
+        n = lib().shygpu_checkpoint_bytes(self.h)
+        buf = np.empty(n, np.uint8)
+        check(lib().shygpu_checkpoint_save(self.h, buf.ctypes.data, n), "checkpoint_save")
+        return buf
+
+    def restore(self, buf):
+        """Load a checkpoint of this model or of one made from the same inputs."""
+        b = np.ascontiguousarray(buf, np.uint8)
+        check(lib().shygpu_checkpoint_load(self.h, b.ctypes.data, b.size), "checkpoint_load")
 
     KERNELS = ("column", "zeta", "final", "node", "stab", "reduce", "conz", "rho")
 
