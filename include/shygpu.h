@@ -206,6 +206,19 @@ int shygpu_step_info(shygpu_model *model, int32_t ibasin, shy_step_info *info);
 int shygpu_set_forcing(shygpu_model *model, int32_t ibasin, const float *tauxnv,
                        const float *tauynv, const float *ppv, const float *rqv);
 
+/* Whole-model transfers for pipelined serving (no reference counterpart:
+ * the reference runs one basin per process).  set_forcing_all copies the
+ * forcing of every basin, concatenated in basin order (NKN values per
+ * array, NULL skips one); get_levels copies the water level of every basin
+ * of the latest enqueued step the same way.  Both are enqueued on the
+ * model's stream and return at once: with pinned host buffers they overlap
+ * the host's work, run in order with the steps enqueued around them, and
+ * are complete after shygpu_sync.  The host buffers must stay untouched
+ * until then.                                                              */
+int shygpu_set_forcing_all(shygpu_model *model, const float *tauxnv, const float *tauynv,
+                           const float *ppv, const float *rqv);
+int shygpu_get_levels(shygpu_model *model, float *znv);
+
 /* Checkpoints (restart.f90:445-660, made exact): every device array of the
  * model and its time-level indices, copied to or from a host buffer of
  * shygpu_checkpoint_bytes(model) bytes.  A checkpoint loads into the model

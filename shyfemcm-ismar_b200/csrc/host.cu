@@ -1549,6 +1549,28 @@ extern "C" int shygpu_checkpoint_load(shygpu_model *m, const void *buf, int64_t 
   return SHY_OK;
 }
 
+// whole-model transfers for pipelined serving: one copy per array for all
+// basins (concatenated in basin order), enqueued on the model's stream
+// without waiting, so they overlap the host's work and order with the
+// steps around them
+extern "C" int shygpu_set_forcing_all(shygpu_model *m, const float *taux, const float *tauy, const float *ppv,
+                                      const float *rqv) {
+  if (!m) return fail(SHY_EARG, "set_forcing_all: model is NULL");
+  const size_t nb = (size_t)m->NKN * 4;
+  if (taux) CUDA_TRY(cudaMemcpyAsync(m->base.taux, taux, nb, cudaMemcpyHostToDevice, m->stream));
+  if (tauy) CUDA_TRY(cudaMemcpyAsync(m->base.tauy, tauy, nb, cudaMemcpyHostToDevice, m->stream));
+  if (ppv) CUDA_TRY(cudaMemcpyAsync(m->base.ppv, ppv, nb, cudaMemcpyHostToDevice, m->stream));
+  if (rqv) CUDA_TRY(cudaMemcpyAsync(m->base.rqv, rqv, nb, cudaMemcpyHostToDevice, m->stream));
+  return SHY_OK;
+}
+
+extern "C" int shygpu_get_levels(shygpu_model *m, float *znv) {
+  if (!m || !znv) return fail(SHY_EARG, "get_levels: bad arguments");
+  if (!m->state_set) return fail(SHY_ESTATE, "get_levels: set_state has not been called");
+  CUDA_TRY(cudaMemcpyAsync(znv, m->zbuf[m->cur], (size_t)m->NKN * 4, cudaMemcpyDeviceToHost, m->stream));
+  return SHY_OK;
+}
+
 extern "C" int shygpu_set_nudging(shygpu_model *m, int32_t ib, const float *andgzv) {
   if (!m || ib < 0 || ib >= m->nbasin || !andgzv) return fail(SHY_EARG, "set_nudging: bad arguments");
   const BasinPar &bp = m->par[ib];

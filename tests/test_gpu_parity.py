@@ -346,3 +346,35 @@ def test_hybrid_sigma_z_layers(column_threads):
     wmax = np.abs(so["wlnv"]).max()
     assert np.abs(sg["wlnv"] - so["wlnv"]).max() <= 2e-3 * wmax
     assert abs(g.info(0).volume - o.info().volume) <= 1e-6 * o.info().volume
+
+
+def test_whole_model_transfers():
+    """shygpu_set_forcing_all / shygpu_enqueue / shygpu_get_levels (one copy
+    for all basins, nothing waited for until shygpu_sync) give the bits of
+    the per-basin calls with a wait after each."""
+    import ctypes as C
+    cs = [cases.basin3d_case(nkn_target=n, nlv=6, seed=s, baroclinic=False, ts=False)
+          for n, s in ((700, 21), (1200, 22))]
+    rng = np.random.default_rng(3)
+    winds = [[rng.normal(0, 1e-4, c["nkn"]).astype(np.float32) for c in cs] for _ in range(6)]
+    a = shygpu.Model(cs)
+    a.set_state_all()
+    for w in winds:
+        for b in range(len(cs)):
+            a.set_forcing(b, tauxnv=w[b], tauynv=-w[b])
+        a.run(1)
+    ref = np.concatenate([a.get_state(b)["znv"] for b in range(len(cs))])
+    g = shygpu.Model(cs)
+    g.set_state_all()
+    lib = shygpu.lib()
+    out = np.zeros(sum(c["nkn"] for c in cs), np.float32)
+    keep = []
+    for w in winds:
+        tx = np.concatenate(w)
+        ty = -tx
+        keep += [tx, ty]
+        shygpu.check(lib.shygpu_set_forcing_all(g.h, tx.ctypes.data, ty.ctypes.data, None, None), "forcing")
+        shygpu.check(lib.shygpu_enqueue(g.h, 1), "enqueue")
+        shygpu.check(lib.shygpu_get_levels(g.h, out.ctypes.data), "levels")
+    shygpu.check(lib.shygpu_sync(g.h), "sync")
+    assert np.array_equal(out, ref)
