@@ -230,6 +230,26 @@ int64_t shygpu_checkpoint_bytes(const shygpu_model *model);
 int shygpu_checkpoint_save(shygpu_model *model, void *buf, int64_t nbytes);
 int shygpu_checkpoint_load(shygpu_model *model, const void *buf, int64_t nbytes);
 
+/* conz3d_omp (concentration_omp.f90:65-76) with its argument list, by value
+ * and with the model and basin in front: one transport sub-step (isact of
+ * istot) of one scalar of basin ib on the model's current hydrodynamic
+ * state, for a host that keeps its own scal3sh loop and calls this where
+ * it called conz3d_omp (concentration.f90:748) after shygpu_hydro.  cn1
+ * (nlvddi, nkn) is read and overwritten with the new concentration; the
+ * open-boundary values stay to the caller (bndo_setbc), gradxv/gradyv are
+ * the caller's tvd_grad_3d result for itvd = 1.  Scalar nudging (robs),
+ * sinking (wsink, wsinkv) and loading (rload) are refused with SHY_EARG;
+ * co1 and cbound are not read (no boundary mass fluxes on this path).
+ * nlvddi and nlev must be the basin's nlv, azpar the model's.  The first
+ * call allocates the call's device arrays.                                 */
+int shygpu_conz3d(shygpu_model *model, int32_t ibasin, float *cn1, float *co1, double ddt,
+                  float rkpar, const float *difhv, const float *difv, float difmol,
+                  const float *cbound, int32_t itvd, int32_t itvdv, const float *gradxv,
+                  const float *gradyv, const float *cobs, float robs, const float *rtauv,
+                  float wsink, const float *wsinkv, float rload, const float *load,
+                  float azpar, float adpar, float aapar, int32_t istot, int32_t isact,
+                  int32_t nlvddi, int32_t nlev);
+
 /* Water-level nudging of basin ib (hydro_zeta, hydrodynamic.f90:612,
  * 677-679): andgzv(nkn), the per-node contribution that the reference's
  * nudge_zeta (nudge.f90:300-338) makes from its observation stations,

@@ -71,6 +71,7 @@ struct Dev {
   float2 *tgrad;                // (nsc_max*NKN*NLV) node gradients {gx, gy} of the sub-step's scalars
   int4 *tvdup;                  // (6*NEL) itvd = 2: {element, xi0, xi1, xi2 as float bits} per vertex pair
   float *andg;                  // (NKN) water-level nudging contribution andgzv, or null (none set)
+  int conz_free_bnd;            // 1: k_conz leaves open-boundary values to the caller (shygpu_conz3d)
   BasinPar *par;
   BasinOut *out;
   // mesh (static)

@@ -271,6 +271,12 @@ struct shygpu_model {
   int *kbas = nullptr;               // node -> basin
   float *zbuf[2], *zebuf[2], *ubuf[2], *vbuf[2], *hkbuf[2], *hebuf[2], *scbuf[2];
   int cur = 0, sc_cur = 0;
+  // shygpu_conz3d scratch (made on its first call): input and output
+  // columns, diffusivities, gradients, per-basin parameters and results
+  float *cz_in = nullptr, *cz_out = nullptr, *cz_difhv = nullptr, *cz_difv = nullptr;
+  float2 *cz_grad = nullptr;
+  BasinPar *cz_par = nullptr;
+  BasinOut *cz_outp = nullptr;
   cudaStream_t stream = nullptr;
   // options
   int nsub = 2, use_graph = 1, max_outer = 12, sym = 1;
@@ -1467,6 +1473,86 @@ extern "C" int shygpu_scalar(shygpu_model *m) {
   if (m->nsc_max > 0) m->sc_cur = 1 - m->sc_cur;
   CUDA_TRY(cudaGetLastError());
   return check_outputs(m);
+}
+
+// conz3d_omp (concentration_omp.f90:65-350) at its own boundary: one
+// transport sub-step (isact of istot) of one scalar of basin ib on the
+// model's current hydrodynamic state (after shygpu_hydro), with the
+// reference's argument list.  cn1 (nlvddi, nkn) is read and overwritten;
+// the open-boundary values are left to the caller's scal3sh loop
+// (bndo_setbc).  Sinking, loading and scalar nudging are refused; cbound and
+// co1 are not needed (no boundary mass fluxes; co1 is the reference's
+// scratch).
+extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1, double ddt, float rkpar,
+                             const float *difhv, const float *difv, float difmol, const float *cbound,
+                             int32_t itvd, int32_t itvdv, const float *gradxv, const float *gradyv,
+                             const float *cobs, float robs, const float *rtauv, float wsink, const float *wsinkv,
+                             float rload, const float *load, float azpar, float adpar, float aapar,
+                             int32_t istot, int32_t isact, int32_t nlvddi, int32_t nlev) {
+  (void)co1; (void)cbound; (void)cobs; (void)rtauv; (void)load;
+  if (!m || ib < 0 || ib >= m->nbasin || !cn1 || !difhv || !difv) return fail(SHY_EARG, "conz3d: bad arguments");
+  if (!m->state_set) return fail(SHY_ESTATE, "conz3d: set_state has not been called");
+  const BasinPar &bp = m->par[ib];
+  if (nlvddi != bp.nlv || nlev != bp.nlv) return fail(SHY_EARG, "conz3d: nlvddi and nlev must be the basin's nlv");
+  if (istot < 1 || isact < 1 || isact > istot) return fail(SHY_EARG, "conz3d: 1 <= isact <= istot");
+  if (robs != 0.f || wsink != 0.f || wsinkv || rload != 0.f)
+    return fail(SHY_EARG, "conz3d: scalar nudging, sinking and loading are not supported");
+  if (itvd < 0 || itvd > 2 || itvdv < 0 || itvdv > 1) return fail(SHY_EARG, "conz3d: itvd 0..2, itvdv 0..1");
+  if (itvdv == 1 && aapar != 0.f) return fail(SHY_EARG, "conz3d: vertical TVD needs aapar = 0");
+  if (itvd == 1 && (!gradxv || !gradyv)) return fail(SHY_EARG, "conz3d: itvd = 1 needs gradxv, gradyv");
+  if (itvd == 2 && bp.itvd != 2) return fail(SHY_EARG, "conz3d: itvd = 2 needs a basin created with itvd = 2");
+  if (azpar != bp.az) return fail(SHY_EARG, "conz3d: azpar differs from the model's");
+  const int NLV = m->NLV, nlv = bp.nlv;
+  const size_t SN = (size_t)m->NKN * NLV;
+  cudaStream_t st = m->stream;
+  if (!m->cz_in) {
+    CUDA_TRY(cudaStreamSynchronize(st));
+    Arena &A = m->arena;
+    if (A.alloc(&m->cz_in, SN) || A.alloc(&m->cz_out, SN) || A.alloc(&m->cz_difhv, (size_t)m->NEL * NLV) ||
+        A.alloc(&m->cz_difv, (size_t)m->NKN * (NLV + 1)) || A.alloc(&m->cz_grad, SN) ||
+        A.alloc(&m->cz_par, (size_t)m->nbasin) || A.alloc(&m->cz_outp, (size_t)m->nbasin))
+      return SHY_ECAPACITY;
+  }
+  // the sub-step's parameters: basin ib transports one scalar, unclipped
+  // (scal3sh clips before the call), the others nothing
+  std::vector<BasinPar> par = m->par;
+  for (int b = 0; b < m->nbasin; b++) par[b].nsc = 0;
+  BasinPar &P = par[ib];
+  P.nsc = 1; P.is_temp[0] = 1; P.rkpar[0] = rkpar; P.dt = ddt; P.difmol = difmol;
+  P.ad = adpar; P.aa = aapar; P.itvd = itvd; P.itvdv = itvdv;
+  std::vector<BasinOut> out(m->nbasin);
+  memset(out.data(), 0, sizeof(BasinOut) * m->nbasin);
+  out[ib].stab[0] = (float)istot;
+  CUDA_TRY(cudaMemcpyAsync(m->cz_par, par.data(), sizeof(BasinPar) * m->nbasin, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(m->cz_outp, out.data(), sizeof(BasinOut) * m->nbasin, cudaMemcpyHostToDevice, st));
+  ST_TRY(copy_cols(m->cz_in, cn1, bp.nk, nlv, NLV, bp.k0, true, st));
+  ST_TRY(copy_cols(m->cz_difhv, difhv, bp.ne, nlv, NLV, bp.e0, true, st));
+  ST_TRY(copy_cols(m->cz_difv, difv, bp.nk, nlv + 1, NLV + 1, bp.k0, true, st));
+  if (itvd == 1) {
+    std::vector<float2> g((size_t)bp.nk * NLV, make_float2(0.f, 0.f));
+    for (int k = 0; k < bp.nk; k++)
+      for (int l = 0; l < nlv; l++)
+        g[(size_t)k * NLV + l] = make_float2(gradxv[(size_t)k * nlv + l], gradyv[(size_t)k * nlv + l]);
+    CUDA_TRY(cudaMemcpy(m->cz_grad + (size_t)bp.k0 * NLV, g.data(), sizeof(float2) * g.size(), cudaMemcpyHostToDevice));
+  }
+  Dev d = dev_for_step(m, m->cur);     // the state hydro just produced is "new"
+  d.par = m->cz_par; d.out = m->cz_outp;
+  d.difhv = m->cz_difhv; d.difv = m->cz_difv; d.tgrad = m->cz_grad;
+  d.nsc_max = 1; d.conz_free_bnd = 1;
+  // k_conz reads sub-step isact from sc_in (isact 1) or the scratch of its
+  // parity and writes sc_out (isact = istot) or the other scratch
+  d.sc_in = m->cz_in; d.sc_out = m->cz_out;
+  if (isact & 1) { d.scr1 = m->cz_in; d.scr0 = m->cz_out; }
+  else { d.scr0 = m->cz_in; d.scr1 = m->cz_out; }
+  launch_node(d, m->kbas, 2, isact - 1, 0, st);
+  g_launches += 1;
+  CUDA_TRY(cudaGetLastError());
+  ST_TRY(copy_cols(m->cz_out, cn1, bp.nk, nlv, NLV, bp.k0, false, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  BasinOut o;
+  CUDA_TRY(cudaMemcpy(&o, m->cz_outp + ib, sizeof o, cudaMemcpyDeviceToHost));
+  if (o.status) return fail(o.status, "conz3d: basin %d: status %d", ib, o.status);
+  return SHY_OK;
 }
 
 extern "C" int shygpu_set_forcing(shygpu_model *m, int32_t ib, const float *taux, const float *tauy,

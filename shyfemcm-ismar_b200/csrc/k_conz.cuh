@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
       if (sidx[r] < 0) continue;
       const int s = sidx[r];
       float cf = act ? res[r] : 0.f;
-      if (act && isbnd) cf = d.cbnd[s * SN + o];      // bndo_impbc
+      if (act && isbnd && !d.conz_free_bnd) cf = d.cbnd[s * SN + o];      // bndo_impbc
       if (valid && lane < NLV) cout_base[s * SN + o] = cf;
     }
   }

@@ -75,6 +75,11 @@ def lib():
     L.shygpu_step_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyStepInfo)]
     L.shygpu_get_wetdry.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3
     L.shygpu_set_nudging.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.shygpu_conz3d.argtypes = ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_float,
+                                 C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int32, C.c_int32,
+                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_float,
+                                 C.c_void_p, C.c_float, C.c_void_p, C.c_float, C.c_float, C.c_float,
+                                 C.c_int32, C.c_int32, C.c_int32, C.c_int32])
     L.shygpu_set_forcing_all.argtypes = [C.c_void_p] + [C.c_void_p] * 4
     L.shygpu_get_levels.argtypes = [C.c_void_p, C.c_void_p]
     L.shygpu_checkpoint_bytes.argtypes = [C.c_void_p]

@@ -378,3 +378,38 @@ def test_whole_model_transfers():
         shygpu.check(lib.shygpu_get_levels(g.h, out.ctypes.data), "levels")
     shygpu.check(lib.shygpu_sync(g.h), "sync")
     assert np.array_equal(out, ref)
+
+
+def test_conz3d_entry_reproduces_run_scalar():
+    """shygpu_conz3d driven by the reference's scal3sh loop (clip, conz3d_omp,
+    boundary values, per sub-step; concentration.f90:727-770) after
+    shygpu_hydro gives the bits of the whole-phase shygpu_scalar."""
+    c = cases.lagoon_case(nkn_target=900, nlv=12, ntracer=1)
+    p = c["params"]
+    m = shygpu.Model(c)
+    m.set_state(0)
+    m.run(4)
+    ck = m.checkpoint()
+    m.hydro()
+    m.scalar()
+    ref = m.get_state(0)["conzv"][0]
+    istot = m.info(0).istot
+    m.restore(ck)
+    cn = np.ascontiguousarray(m.get_state(0)["conzv"][0])
+    m.hydro()
+    lib = shygpu.lib()
+    nlv = c["nlv"]
+    difhv = np.ones((c["nel"], nlv), np.float32)
+    difv = np.ascontiguousarray(c["difv"], np.float32)
+    cb = np.asarray(c["conzv"][0], np.float32)          # boundary values: the initial columns
+    bnd = c["bnd_index"] > 0
+    assert istot >= 1
+    for isact in range(1, istot + 1):
+        cn[cn < 1e-15] = 0.0
+        shygpu.check(lib.shygpu_conz3d(
+            m.h, 0, cn.ctypes.data, None, float(p["dt"]), float(p["chpar"]), difhv.ctypes.data,
+            difv.ctypes.data, float(p["difmol"]), None, 0, 0, None, None, None, 0.0, None, 0.0, None,
+            0.0, None, float(p["azpar"]), float(p["adpar"]), float(p["aapar"]), istot, isact, nlv, nlv),
+            "conz3d")
+        cn[bnd] = cb[bnd]
+    assert np.array_equal(cn, ref)
