@@ -219,6 +219,21 @@ int shygpu_set_forcing_all(shygpu_model *model, const float *tauxnv, const float
                            const float *ppv, const float *rqv);
 int shygpu_get_levels(shygpu_model *model, float *znv);
 
+/* Hydro output of basin ib in the reference's .shy format (io_shy.f90,
+ * shy_util.f90:450-480, 1210-1250: the header of shyfem_init_hydro_file,
+ * then per shygpu_shy_write the water level at nodes and element vertices
+ * and the transports U, V of the current state).  basin is the
+ * description the model was made from (mesh arrays for the header).  Each
+ * write enqueues its device-to-host copies on the model's stream into one
+ * of two pinned buffers and returns; a writer thread writes the records
+ * once the copies are done, so output overlaps the next steps.  close
+ * waits for the writes and reports any error.                              */
+typedef struct shygpu_shyfile shygpu_shyfile;
+int shygpu_shy_open(shygpu_model *model, int32_t ibasin, const shy_basin *basin, const char *path,
+                    int32_t date, int32_t time, const char *title, shygpu_shyfile **file);
+int shygpu_shy_write(shygpu_shyfile *file);
+int shygpu_shy_close(shygpu_shyfile *file);
+
 /* Checkpoints (restart.f90:445-660, made exact): every device array of the
  * model and its time-level indices, copied to or from a host buffer of
  * shygpu_checkpoint_bytes(model) bytes.  A checkpoint loads into the model

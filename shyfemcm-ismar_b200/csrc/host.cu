@@ -13,7 +13,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <condition_variable>
+#include <mutex>
 #include <queue>
+#include <thread>
 #include <vector>
 
 #include "../../include/shygpu.h"
@@ -1655,6 +1658,201 @@ extern "C" int shygpu_get_levels(shygpu_model *m, float *znv) {
   if (!m->state_set) return fail(SHY_ESTATE, "get_levels: set_state has not been called");
   CUDA_TRY(cudaMemcpyAsync(znv, m->zbuf[m->cur], (size_t)m->NKN * 4, cudaMemcpyDeviceToHost, m->stream));
   return SHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// hydro output in the reference's .shy format (io_shy.f90:1550-1681,
+// shy_util.f90:450-480, 1210-1250): Fortran unformatted sequential records
+// (a 4-byte length before and after each), the header of
+// shyfem_init_hydro_file (ftype 1, npr 3, nvar 4), then per output time
+// the records of shy_write_hydro_records: water level at the nodes and at
+// the element vertices (ivar 1), transports U and V (ivar 3), 3D values
+// written layer-fastest over the active layers only (vals2linear).  The
+// device-to-host copies of a snapshot are enqueued on the model's stream
+// into one of two pinned buffers and a writer thread waits for them and
+// writes, so output overlaps the following steps.
+// ---------------------------------------------------------------------------
+struct shygpu_shyfile {
+  shygpu_model *m = nullptr;
+  int ib = 0, nk = 0, ne = 0, nlv = 0;
+  FILE *fp = nullptr;
+  std::vector<int> ilhv, ilhkv;
+  struct Slot {
+    float *z = nullptr, *ze = nullptr, *u = nullptr, *v = nullptr;
+    BasinOut *out = nullptr;
+    cudaEvent_t ev = nullptr;
+    bool busy = false;
+  } slot[2];
+  int next = 0;
+  std::thread worker;
+  std::mutex mu;
+  std::condition_variable cv;
+  std::queue<int> jobs;
+  bool stop = false, io_error = false;
+};
+
+static bool shy_rec(FILE *fp, const void *p, int32_t nbytes) {
+  return fwrite(&nbytes, 4, 1, fp) == 1 && (nbytes == 0 || fwrite(p, 1, (size_t)nbytes, fp) == (size_t)nbytes) &&
+         fwrite(&nbytes, 4, 1, fp) == 1;
+}
+
+template <typename T> static bool shy_rec_v(FILE *fp, const std::vector<T> &v) {
+  return shy_rec(fp, v.data(), (int32_t)(v.size() * sizeof(T)));
+}
+
+static bool shy_write_slot(shygpu_shyfile *f, const shygpu_shyfile::Slot &sl) {
+  FILE *fp = f->fp;
+  const double dtime = sl.out->dtime;
+  auto head = [&](int32_t ivar, int32_t n, int32_t mm, int32_t lmax) {
+    char b[24];
+    memcpy(b, &dtime, 8);
+    const int32_t iv[4] = {ivar, n, mm, lmax};
+    memcpy(b + 8, iv, 16);
+    return shy_rec(fp, b, 24);
+  };
+  auto lin = [&](const float *c) {          // vals2linear: active layers of each element
+    std::vector<float> r;
+    r.reserve((size_t)f->ne * f->nlv);
+    for (int e = 0; e < f->ne; e++)
+      for (int l = 0; l < std::min(f->nlv, f->ilhv[e]); l++) r.push_back(c[(size_t)e * f->nlv + l]);
+    return r;
+  };
+  bool ok = head(1, f->nk, 1, 1) && shy_rec(fp, sl.z, f->nk * 4) &&
+            head(1, f->ne, 3, 1) && shy_rec(fp, sl.ze, f->ne * 12);
+  if (f->nlv > 1) {
+    ok = ok && head(3, f->ne, 1, f->nlv) && shy_rec_v(fp, lin(sl.u)) && head(3, f->ne, 1, f->nlv) &&
+         shy_rec_v(fp, lin(sl.v));
+  } else {
+    ok = ok && head(3, f->ne, 1, 1) && shy_rec(fp, sl.u, f->ne * 4) && head(3, f->ne, 1, 1) &&
+         shy_rec(fp, sl.v, f->ne * 4);
+  }
+  return ok && fflush(fp) == 0;
+}
+
+static void shy_worker(shygpu_shyfile *f) {
+  for (;;) {
+    int j;
+    {
+      std::unique_lock<std::mutex> lk(f->mu);
+      f->cv.wait(lk, [&] { return f->stop || !f->jobs.empty(); });
+      if (f->jobs.empty()) return;
+      j = f->jobs.front();
+      f->jobs.pop();
+    }
+    auto &sl = f->slot[j];
+    const bool ok = cudaEventSynchronize(sl.ev) == cudaSuccess && shy_write_slot(f, sl);
+    {
+      std::lock_guard<std::mutex> lk(f->mu);
+      if (!ok) f->io_error = true;
+      sl.busy = false;
+    }
+    f->cv.notify_all();
+  }
+}
+
+static void shy_free(shygpu_shyfile *f) {
+  for (auto &sl : f->slot) {
+    if (sl.z) cudaFreeHost(sl.z);
+    if (sl.ze) cudaFreeHost(sl.ze);
+    if (sl.u) cudaFreeHost(sl.u);
+    if (sl.v) cudaFreeHost(sl.v);
+    if (sl.out) cudaFreeHost(sl.out);
+    if (sl.ev) cudaEventDestroy(sl.ev);
+  }
+  if (f->fp) fclose(f->fp);
+  delete f;
+}
+
+extern "C" int shygpu_shy_open(shygpu_model *m, int32_t ib, const shy_basin *bs, const char *path, int32_t date,
+                               int32_t time, const char *title, shygpu_shyfile **out) {
+  if (!m || ib < 0 || ib >= m->nbasin || !bs || !path || !out) return fail(SHY_EARG, "shy_open: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  if (bs->nkn != bp.nk || bs->nel != bp.ne || bs->nlv != bp.nlv) return fail(SHY_EARG, "shy_open: basin %d differs", ib);
+  auto *f = new shygpu_shyfile();
+  f->m = m; f->ib = ib; f->nk = bp.nk; f->ne = bp.ne; f->nlv = bp.nlv;
+  f->ilhv.assign(bs->ilhv, bs->ilhv + bp.ne);
+  f->ilhkv.assign(bs->ilhkv, bs->ilhkv + bp.nk);
+  for (auto &sl : f->slot) {
+    if (cudaMallocHost((void **)&sl.z, (size_t)bp.nk * 4) != cudaSuccess ||
+        cudaMallocHost((void **)&sl.ze, (size_t)bp.ne * 12) != cudaSuccess ||
+        cudaMallocHost((void **)&sl.u, (size_t)bp.ne * bp.nlv * 4) != cudaSuccess ||
+        cudaMallocHost((void **)&sl.v, (size_t)bp.ne * bp.nlv * 4) != cudaSuccess ||
+        cudaMallocHost((void **)&sl.out, sizeof(BasinOut)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess) {
+      shy_free(f);
+      return fail(SHY_ECAPACITY, "shy_open: pinned host buffers");
+    }
+  }
+  f->fp = fopen(path, "wb");
+  if (!f->fp) { shy_free(f); return fail(SHY_EARG, "shy_open: cannot open %s", path); }
+  // header (io_shy.f90:1577-1598); simpar = hzmin, hzoff, nzadapt, dtaver
+  const int32_t nk = bp.nk, ne = bp.ne, nlv = bp.nlv;
+  const int32_t idv[2] = {1617, 14}, ftype = 1, pars[5] = {nk, ne, 3, nlv, 4}, nfix = 0, dt2[2] = {date, time};
+  const int32_t nsimpar = 4;
+  const float simpar[4] = {bp.hzmin, bp.hzoff, 0.f, 0.f};
+  char ttl[80], ver[80];
+  memset(ttl, ' ', 80); memset(ver, ' ', 80);
+  if (title) memcpy(ttl, title, std::min<size_t>(80, strlen(title)));
+  const char *v = "shygpu (B200 step of SHYFEM)";
+  memcpy(ver, v, strlen(v));
+  std::vector<int32_t> nen(bs->nen3v, bs->nen3v + (size_t)3 * ne), ipev(ne), ipv(nk), iarv(ne, 0), iarnv(nk, 0);
+  for (int i = 0; i < ne; i++) ipev[i] = i + 1;
+  for (int i = 0; i < nk; i++) ipv[i] = i + 1;
+  std::vector<float> xg(bs->xgv, bs->xgv + nk), yg(bs->ygv, bs->ygv + nk), hm(bs->hm3v, bs->hm3v + (size_t)3 * ne),
+      hl(bs->hlv, bs->hlv + nlv);
+  bool ok = shy_rec(f->fp, idv, 8) && shy_rec(f->fp, &ftype, 4) && shy_rec(f->fp, pars, 20) &&
+            shy_rec(f->fp, &nfix, 4) && shy_rec(f->fp, dt2, 8) && shy_rec(f->fp, &nsimpar, 4) &&
+            shy_rec(f->fp, simpar, 16) && shy_rec(f->fp, ttl, 80) && shy_rec(f->fp, ver, 80) &&
+            shy_rec(f->fp, nullptr, 0) && shy_rec_v(f->fp, nen) && shy_rec_v(f->fp, ipev) && shy_rec_v(f->fp, ipv) &&
+            shy_rec_v(f->fp, iarv) && shy_rec_v(f->fp, iarnv) && shy_rec_v(f->fp, xg) && shy_rec_v(f->fp, yg) &&
+            shy_rec_v(f->fp, hm) && shy_rec_v(f->fp, hl) && shy_rec_v(f->fp, f->ilhv) && shy_rec_v(f->fp, f->ilhkv) &&
+            shy_rec(f->fp, nullptr, 0);
+  if (!ok) { shy_free(f); return fail(SHY_EARG, "shy_open: write error on %s", path); }
+  f->worker = std::thread(shy_worker, f);
+  *out = f;
+  return SHY_OK;
+}
+
+extern "C" int shygpu_shy_write(shygpu_shyfile *f) {
+  if (!f) return fail(SHY_EARG, "shy_write: file is NULL");
+  shygpu_model *m = f->m;
+  const BasinPar &bp = m->par[f->ib];
+  const int j = f->next;
+  {
+    std::unique_lock<std::mutex> lk(f->mu);
+    f->cv.wait(lk, [&] { return !f->slot[j].busy; });
+    if (f->io_error) return fail(SHY_EARG, "shy_write: an earlier write failed");
+    f->slot[j].busy = true;
+  }
+  auto &sl = f->slot[j];
+  const int c = m->cur, NLV = m->NLV;
+  cudaStream_t st = m->stream;
+  CUDA_TRY(cudaMemcpyAsync(sl.z, m->zbuf[c] + bp.k0, (size_t)bp.nk * 4, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaMemcpyAsync(sl.ze, m->zebuf[c] + 3 * (size_t)bp.e0, (size_t)bp.ne * 12, cudaMemcpyDeviceToHost, st));
+  ST_TRY(copy_cols(m->ubuf[c], sl.u, bp.ne, bp.nlv, NLV, bp.e0, false, st));
+  ST_TRY(copy_cols(m->vbuf[c], sl.v, bp.ne, bp.nlv, NLV, bp.e0, false, st));
+  CUDA_TRY(cudaMemcpyAsync(sl.out, m->base.out + f->ib, sizeof(BasinOut), cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaEventRecord(sl.ev, st));
+  {
+    std::lock_guard<std::mutex> lk(f->mu);
+    f->jobs.push(j);
+  }
+  f->cv.notify_all();
+  f->next = 1 - j;
+  return SHY_OK;
+}
+
+extern "C" int shygpu_shy_close(shygpu_shyfile *f) {
+  if (!f) return SHY_OK;
+  {
+    std::lock_guard<std::mutex> lk(f->mu);
+    f->stop = true;
+  }
+  f->cv.notify_all();
+  if (f->worker.joinable()) f->worker.join();
+  const bool err = f->io_error;
+  shy_free(f);
+  return err ? fail(SHY_EARG, "shy_close: a write failed") : SHY_OK;
 }
 
 extern "C" int shygpu_set_nudging(shygpu_model *m, int32_t ib, const float *andgzv) {

@@ -80,6 +80,10 @@ def lib():
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_float,
                                  C.c_void_p, C.c_float, C.c_void_p, C.c_float, C.c_float, C.c_float,
                                  C.c_int32, C.c_int32, C.c_int32, C.c_int32])
+    L.shygpu_shy_open.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyBasin), C.c_char_p, C.c_int32,
+                                  C.c_int32, C.c_char_p, C.POINTER(C.c_void_p)]
+    L.shygpu_shy_write.argtypes = [C.c_void_p]
+    L.shygpu_shy_close.argtypes = [C.c_void_p]
     L.shygpu_set_forcing_all.argtypes = [C.c_void_p] + [C.c_void_p] * 4
     L.shygpu_get_levels.argtypes = [C.c_void_p, C.c_void_p]
     L.shygpu_checkpoint_bytes.argtypes = [C.c_void_p]
@@ -218,6 +222,20 @@ class Model:
         a = np.ascontiguousarray(andgzv, np.float32)
         check(lib().shygpu_set_nudging(self.h, ib, a.ctypes.data), "set_nudging")
         lib().shygpu_sync(self.h)
+
+    def shy_open(self, ib, path, date=0, time=0, title=""):
+        """Hydro output of basin ib in the reference's .shy format; returns a
+        handle for shy_write/shy_close."""
+        h = C.c_void_p()
+        check(lib().shygpu_shy_open(self.h, ib, C.byref(self._basins[ib]), str(path).encode(), date, time,
+                                    title.encode(), C.byref(h)), "shy_open")
+        return h
+
+    def shy_write(self, f):
+        check(lib().shygpu_shy_write(f), "shy_write")
+
+    def shy_close(self, f):
+        check(lib().shygpu_shy_close(f), "shy_close")
 
     def checkpoint(self):
         """Every device array of the model, as a host byte array."""
