@@ -384,6 +384,12 @@ int shygpu_serve_status(shygpu_server *server, int64_t request_id,
 int shygpu_serve_result(shygpu_server *server, int64_t request_id,
                         shy_state *out, shy_step_info *info);
 int shygpu_serve_release(shygpu_server *server, int64_t request_id);
+/* Preempt a running request: it stops after its quantum in flight, its
+ * device arrays are saved to host memory (shygpu_checkpoint_save), its
+ * device memory is freed, and it queues behind the requests already
+ * waiting (an urgent request submitted before the call is admitted first);
+ * when admitted again it continues bit for bit.                            */
+int shygpu_serve_preempt(shygpu_server *server, int64_t request_id);
 int64_t shygpu_serve_used(shygpu_server *server);   /* admitted footprint */
 int shygpu_serve_destroy(shygpu_server *server);
 

@@ -19,6 +19,7 @@
 // process.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdarg>
 #include <cstdint>
@@ -68,6 +69,10 @@ struct Request {
   shygpu_model *m = nullptr;
   cudaEvent_t ev = nullptr;
   bool in_flight = false;
+  // a preempted run's device arrays (shygpu_checkpoint_save), loaded back
+  // when it is admitted again
+  std::vector<unsigned char> ckpt;
+  int32_t preemptions = 0;
   // results
   std::vector<float> rz, ru, rv, rt, rs, rc;
   shy_step_info info{};
@@ -195,14 +200,22 @@ static void retire(shygpu_server *s, Request *r, bool ok) {
 
 static bool admit(shygpu_server *s, Request *r) {
   if (shygpu_create(1, &r->b, &r->p, &r->m) != SHY_OK) { r->error = shygpu_last_error(); return false; }
-  shy_state st{};
-  st.znv = r->z0.empty() ? nullptr : r->z0.data();
-  st.utlnv = r->u0.empty() ? nullptr : r->u0.data();
-  st.vtlnv = r->v0.empty() ? nullptr : r->v0.data();
-  st.tempv = r->t0.empty() ? nullptr : r->t0.data();
-  st.saltv = r->s0.empty() ? nullptr : r->s0.data();
-  st.conzv = r->c0.empty() ? nullptr : r->c0.data();
-  if (shygpu_set_state(r->m, 0, &st) != SHY_OK) { r->error = shygpu_last_error(); return false; }
+  if (!r->ckpt.empty()) {           // a preempted run continues where it stopped
+    if (shygpu_checkpoint_load(r->m, r->ckpt.data(), (int64_t)r->ckpt.size()) != SHY_OK) {
+      r->error = shygpu_last_error();
+      return false;
+    }
+    std::vector<unsigned char>().swap(r->ckpt);
+  } else {
+    shy_state st{};
+    st.znv = r->z0.empty() ? nullptr : r->z0.data();
+    st.utlnv = r->u0.empty() ? nullptr : r->u0.data();
+    st.vtlnv = r->v0.empty() ? nullptr : r->v0.data();
+    st.tempv = r->t0.empty() ? nullptr : r->t0.data();
+    st.saltv = r->s0.empty() ? nullptr : r->s0.data();
+    st.conzv = r->c0.empty() ? nullptr : r->c0.data();
+    if (shygpu_set_state(r->m, 0, &st) != SHY_OK) { r->error = shygpu_last_error(); return false; }
+  }
   if (cudaEventCreateWithFlags(&r->ev, cudaEventDisableTiming) != cudaSuccess) {
     r->error = "event creation failed";
     return false;
@@ -266,7 +279,7 @@ extern "C" int shygpu_serve_progress(shygpu_server *s, int32_t block, int32_t *n
       finished++;
       continue;
     }
-    const int32_t q = std::min(s->quantum, r->nsteps);
+    const int32_t q = std::min(s->quantum, r->nsteps - r->enqueued);
     if (shygpu_enqueue(r->m, q) != SHY_OK ||
         cudaEventRecord(r->ev, (cudaStream_t)shygpu_model_stream(r->m)) != cudaSuccess) {
       r->error = shygpu_last_error();
@@ -274,13 +287,52 @@ extern "C" int shygpu_serve_progress(shygpu_server *s, int32_t block, int32_t *n
       finished++;
       continue;
     }
-    r->enqueued = q;
+    r->enqueued += q;
     r->in_flight = true;
     s->active.push_back(r);
   }
   if (n_active) *n_active = (int32_t)s->active.size();
   if (n_queued) *n_queued = (int32_t)s->queue.size();
   if (n_done) *n_done = finished;
+  return SHY_OK;
+}
+
+// Preemption: an active run is stopped after its quantum in flight, its
+// device arrays go to host memory (an exact checkpoint) and its device
+// memory is freed, so the requests already waiting are admitted first; it
+// queues behind them and, once admitted again, continues bit for bit.
+extern "C" int shygpu_serve_preempt(shygpu_server *s, int64_t id) {
+  if (!s) return sfail(SHY_EARG, "serve_preempt: server is NULL");
+  std::lock_guard<std::mutex> lock(s->mu);
+  auto it = s->all.find(id);
+  if (it == s->all.end()) return sfail(SHY_EARG, "serve_preempt: unknown request %lld", (long long)id);
+  Request *r = it->second.get();
+  if (r->state != Q_ACTIVE) return sfail(SHY_ESTATE, "serve_preempt: request %lld is not running", (long long)id);
+  if (r->in_flight) {
+    cudaEventSynchronize(r->ev);
+    r->in_flight = false;
+  }
+  int st = shygpu_sync(r->m);
+  if (st == SHY_OK) {
+    const int64_t n = shygpu_checkpoint_bytes(r->m);
+    r->ckpt.resize((size_t)n);
+    st = shygpu_checkpoint_save(r->m, r->ckpt.data(), n);
+  }
+  auto pos = std::find(s->active.begin(), s->active.end(), r);
+  if (pos != s->active.end()) s->active.erase(pos);
+  if (st != SHY_OK) {
+    r->error = shygpu_last_error();
+    retire(s, r, false);
+    return sfail(st, "serve_preempt: request %lld failed: %s", (long long)id, r->error.c_str());
+  }
+  shygpu_destroy(r->m);
+  r->m = nullptr;
+  cudaEventDestroy(r->ev);
+  r->ev = nullptr;
+  s->used -= r->footprint;
+  r->state = Q_QUEUED;
+  r->preemptions++;
+  s->queue.push_back(r);
   return SHY_OK;
 }
 

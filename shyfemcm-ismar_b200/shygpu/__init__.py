@@ -84,6 +84,7 @@ def lib():
                                   C.c_int32, C.c_char_p, C.POINTER(C.c_void_p)]
     L.shygpu_shy_write.argtypes = [C.c_void_p]
     L.shygpu_shy_close.argtypes = [C.c_void_p]
+    L.shygpu_serve_preempt.argtypes = [C.c_void_p, C.c_int64]
     L.shygpu_set_forcing_all.argtypes = [C.c_void_p] + [C.c_void_p] * 4
     L.shygpu_get_levels.argtypes = [C.c_void_p, C.c_void_p]
     L.shygpu_checkpoint_bytes.argtypes = [C.c_void_p]
@@ -324,6 +325,11 @@ class Server:
             del self._cases[rid]
         out = {k: buf.arrays[k] for k in ("znv", "utlnv", "vtlnv", "tempv", "saltv", "conzv")}
         return out, info
+
+    def preempt(self, rid):
+        """Stop a running request, keep its state in host memory, queue it behind
+        the requests already waiting."""
+        check(lib().shygpu_serve_preempt(self.h, rid), "serve_preempt")
 
     def used(self):
         return lib().shygpu_serve_used(self.h)

@@ -52,3 +52,32 @@ def test_results_same_alone_and_in_the_mix():
             assert np.array_equal(got["tempv"], ref["tempv"]) and np.array_equal(got["saltv"], ref["saltv"])
     assert srv.used() == 0
     srv.close()
+
+
+def test_preempted_run_resumes_exactly():
+    """shygpu_serve_preempt: a long run is stopped to make room for an urgent
+    one (one run fits at a time), then continues from its checkpoint; both
+    results equal the runs alone, bit for bit."""
+    c_long = cases.basin3d_case(nkn_target=1500, nlv=12, seed=41)       # T/S, baroclinic
+    c_urgent = cases.channel_case()
+    budget = max(shygpu.footprint([c_long]), shygpu.footprint([c_urgent])) + 1
+    srv = shygpu.Server(budget, max_active=1, quantum_steps=5)
+    a = srv.submit(c_long, 40)
+    for _ in range(3):
+        srv.progress(block=True)
+    assert srv.status(a)[0] == shygpu.Server.ACTIVE
+    b = srv.submit(c_urgent, 30)
+    srv.preempt(a)                       # b, already waiting, goes first; a queues behind it
+    assert srv.used() == 0
+    for _ in range(10000):
+        srv.progress(block=True)
+        if all(srv.status(i)[0] >= shygpu.Server.DONE for i in (a, b)):
+            break
+    assert srv.status(b)[4] <= srv.status(a)[4]      # the urgent run finished first
+    for i, (c, n) in ((a, (c_long, 40)), (b, (c_urgent, 30))):
+        assert srv.status(i)[0] == shygpu.Server.DONE
+        got, info = srv.result(i)
+        ref = alone(c, n)
+        for f in ("znv", "utlnv", "vtlnv"):
+            assert np.array_equal(got[f], ref[f]), (i, f)
+    srv.close()
