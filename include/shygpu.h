@@ -111,6 +111,8 @@ typedef struct shy_params {
                              /*   node gradients (superbee)     :1053       */
   int32_t itvdv;             /* vertical transport: 0 upwind, 1 TVD          */
                              /*   (superbee; needs aapar = 0)   :1054       */
+  int32_t ihwadv;            /* vertical advection of momentum with ilin 0:  */
+                             /*   0 none, 1 upwind, 2 centred   :1350       */
 } shy_params;
 
 /* Host views of one basin's state, reference layouts.  NULL members are

@@ -704,23 +704,65 @@ void set_explicit(Model &m) {
         else { momx[kl] = m.uprv[kl] * m.hdkov[kl]; momy[kl] = m.vprv[kl] * m.hdkov[kl]; }
       }
     const double rlin = m.p.rlin;
+    const int ihwadv = m.p.ihwadv;
     for (int ie = 0; ie < m.nel; ie++) {
       const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
-      for (int l = 0; l < m.ilhv[ie]; l++) {
+      const int lmax = m.ilhv[ie];
+      // old velocities of the column (ulov = utlov/hdeov, ttov)
+      auto ul = [&](int l, bool y) {
+        const size_t el = (size_t)ie * nlv + l;
+        const double h = m.hdeov[el];
+        return h > 0. ? (y ? m.vtlov[el] : m.utlov[el]) / h : 0.;
+      };
+      double wtop = 0.;
+      for (int l = 0; l < lmax; l++) {
         const size_t el = (size_t)ie * nlv + l;
         const double h = m.hdeov[el], ut = m.utlov[el], vt = m.vtlov[el];
         const double uc = ut / h, vc = vt / h;
-        double xadv = 0., yadv = 0.;
+        double xadv = 0., yadv = 0., wbot = 0.;
         for (int ii = 0; ii < 3; ii++) {
-          const size_t kl = (size_t)m.nen3v[3 * ie + ii] * nlv + l;
+          const int k = m.nen3v[3 * ie + ii];
+          const size_t kl = (size_t)k * nlv + l;
+          wbot += m.wlnv[(size_t)k * (nlv + 1) + l + 1];       // old w at the layer's bottom
           const double f = ut * e[3 + ii] + vt * e[6 + ii];
           if (f < 0.) {                        // flux out of the node, into the element
             xadv += f * (momx[kl] / h - uc);
             yadv += f * (momy[kl] / h - vc);
           }
         }
-        m.fxv[el] += rlin * xadv;
-        m.fyv[el] += rlin * yadv;
+        // vertical advection of momentum (:776-833)
+        double zxadv = 0., zyadv = 0.;
+        if (ihwadv > 0) {
+          wbot /= 3.;
+          if (l == lmax - 1) wbot = 0.;
+          if (ihwadv == 1) {                   // upwind
+            const int lt = wtop > 0. ? l : l - 1;
+            zxadv = lt >= 0 ? wtop * ul(lt, false) : 0.;
+            zyadv = lt >= 0 ? wtop * ul(lt, true) : 0.;
+            const int lb = wbot > 0. ? l + 1 : l;
+            zxadv -= lb < lmax ? wbot * ul(lb, false) : 0.;
+            zyadv -= lb < lmax ? wbot * ul(lb, true) : 0.;
+          } else {                             // centred
+            const double dz = m.hdeov[el];
+            double utop = 0., ubot = 0., vtop = 0., vbot = 0.;
+            if (l > 0) {
+              const double dztt = m.hdeov[el - 1];
+              utop = (ul(l - 1, false) * dztt + ul(l, false) * dz) / (dztt + dz);
+              vtop = (ul(l - 1, true) * dztt + ul(l, true) * dz) / (dztt + dz);
+            }
+            if (l < lmax - 1) {
+              const double dzbb = m.hdeov[el + 1];
+              ubot = (ul(l, false) * dz + ul(l + 1, false) * dzbb) / (dz + dzbb);
+              vbot = (ul(l, true) * dz + ul(l + 1, true) * dzbb) / (dz + dzbb);
+            }
+            const double wlay = 0.5 * (wtop + wbot);
+            zxadv = wlay * (utop - ubot);
+            zyadv = wlay * (vtop - vbot);
+          }
+          wtop = wbot;
+        }
+        m.fxv[el] += rlin * (xadv + zxadv);
+        m.fyv[el] += rlin * (yadv + zyadv);
       }
     }
   }

@@ -47,7 +47,30 @@ struct BasinPar {
   float rlin;                 // its strength
   int itvd;                   // horizontal transport: 0 upwind, 1 TVD with node gradients
   int itvdv;                  // vertical transport: 0 upwind, 1 TVD
+  int ihwadv;                 // vertical momentum advection (with adv): 0 none, 1 upwind, 2 centred
 };
+
+// set_advective's vertical term (explicit.f90:776-833) of one layer from
+// the old velocities U/h of the layer and its neighbours (um, up: above
+// and below, 0 where absent) and the old w at its top and bottom (wt, wb:
+// vertex means, 0 at the surface and at the element's bottom)
+__device__ __forceinline__ float2 vert_momentum_adv(int ihwadv, float wt, float wb, bool has_up, bool has_dn,
+                                                    float u, float v, float h, float um, float vm, float hm,
+                                                    float up, float vp, float hp) {
+  if (ihwadv == 1) {
+    float zx = 0.f, zy = 0.f;
+    if (wt > 0.f) { zx = wt * u; zy = wt * v; }
+    else if (has_up) { zx = wt * um; zy = wt * vm; }
+    if (wb > 0.f) { if (has_dn) { zx -= wb * up; zy -= wb * vp; } }
+    else { zx -= wb * u; zy -= wb * v; }
+    return make_float2(zx, zy);
+  }
+  float ut = 0.f, vt = 0.f, ub = 0.f, vb = 0.f;
+  if (has_up) { ut = (um * hm + u * h) / (hm + h); vt = (vm * hm + v * h) / (hm + h); }
+  if (has_dn) { ub = (u * h + up * hp) / (h + hp); vb = (v * h + vp * hp) / (h + hp); }
+  const float wl = 0.5f * (wt + wb);
+  return make_float2(wl * (ut - ub), wl * (vt - vb));
+}
 
 // per-basin results of the last step (device memory)
 struct BasinOut {

@@ -813,6 +813,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: hybrid levels: hlv(nsigma) must be hsigma (initialize.f90:556)", b));
     if (Pp[b].nsigma > 0 && Pp[b].ibarcl > 0)
       return bail(fail(SHY_EARG, "basin %d: baroclinic terms on sigma layers not supported", b));
+    if (Pp[b].ihwadv < 0 || Pp[b].ihwadv > 2)
+      return bail(fail(SHY_EARG, "basin %d: ihwadv=%d: 0, 1 (upwind) or 2 (centred)", b, Pp[b].ihwadv));
     if (Pp[b].itvdv != 0 && Pp[b].itvdv != 1)
       return bail(fail(SHY_EARG, "basin %d: itvdv=%d: upwind (0) or TVD (1) only", b, Pp[b].itvdv));
     if (Pp[b].itvdv == 1 && Pp[b].aapar != 0.f)   // concentration_omp.f90:218-226
@@ -987,7 +989,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     m->any_wd |= bp.wetdry != 0;
     bp.adv = p.ilin == 0 ? 1 : 0; bp.rlin = p.rlin;
     m->any_adv |= bp.adv != 0;
-    bp.itvd = p.itvd; bp.itvdv = p.itvdv;
+    bp.itvd = p.itvd; bp.itvdv = p.itvdv; bp.ihwadv = p.ilin == 0 ? p.ihwadv : 0;
     bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
     int ns = 0;
     if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }

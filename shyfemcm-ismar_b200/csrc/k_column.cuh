@@ -107,7 +107,18 @@ __global__ void __launch_bounds__(256) k_column(Dev d) {
       fy -= ai * (vi - vvi);
     }
   }
-  if (P.adv && act) {                    // set_advective (:685-861), ihwadv 0
+  // vertical advection of momentum: w at the bottom of each lane's layer,
+  // and from the lane above at its top (shuffles by the whole segment)
+  float adv_wb = 0.f, adv_wt = 0.f;
+  if (P.adv && P.ihwadv > 0) {
+    const int I1 = NLV + 1;
+    if (act && lane + 1 < ilevel)
+      adv_wb = (d.wl[(size_t)kn[0] * I1 + lane + 1] + d.wl[(size_t)kn[1] * I1 + lane + 1] +
+                d.wl[(size_t)kn[2] * I1 + lane + 1]) * (1.f / 3.f);
+    adv_wt = seg_up<S>(adv_wb, 1);
+    if (lane == 0) adv_wt = 0.f;
+  }
+  if (P.adv && act) {                    // set_advective (:685-861)
     const float uc = uui / hhi, vc = vvi / hhi;
     float xadv = 0.f, yadv = 0.f;
 #pragma unroll
@@ -118,6 +129,14 @@ __global__ void __launch_bounds__(256) k_column(Dev d) {
         xadv += f * (mk.x / hhi - uc);
         yadv += f * (mk.y / hhi - vc);
       }
+    }
+    if (P.ihwadv > 0) {                  // vertical advection of momentum (:776-833)
+      const bool has_up = lane > 0, has_dn = lane + 1 < ilevel;
+      const float2 z = vert_momentum_adv(P.ihwadv, adv_wt, adv_wb, has_up, has_dn, uui / hhi, vvi / hhi, hhi,
+                                         has_up ? uuim / hhim : 0.f, has_up ? vvim / hhim : 0.f, hhim,
+                                         has_dn ? uuip / hhip : 0.f, has_dn ? vvip / hhip : 0.f, hhip);
+      xadv += z.x;
+      yadv += z.y;
     }
     fx += P.rlin * xadv;
     fy += P.rlin * yadv;

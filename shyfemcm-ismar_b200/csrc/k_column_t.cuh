@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
   float cp[L];
   float dp0[L], dp1[L], dp2[L];            // real: rhs ppx, ppy, h
   float2 cpc[COR ? L : 1], dq0[COR ? L : 1], dq1[COR ? L : 1];   // complex: ppx+i ppy, h
+  float adv_wtop = 0.f;                    // vertical momentum advection: w at the layer's top
   float alev_t = P.vismol;
   if (0 < ilevel)
     alev_t += (d.visv[(size_t)kn[0] * I] + d.visv[(size_t)kn[1] * I] + d.visv[(size_t)kn[2] * I]) * (1.f / 3.f);
@@ -142,6 +143,19 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
           xadv += f * (mk.x / hhi - uc);
           yadv += f * (mk.y / hhi - vc);
         }
+      }
+      if (P.ihwadv > 0) {                // vertical advection of momentum (:776-833)
+        const int I1 = NLV + 1;
+        float wb = 0.f;
+        if (!blast)
+          wb = (d.wl[(size_t)kn[0] * I1 + l + 1] + d.wl[(size_t)kn[1] * I1 + l + 1] +
+                d.wl[(size_t)kn[2] * I1 + l + 1]) * (1.f / 3.f);
+        const float2 z = vert_momentum_adv(P.ihwadv, adv_wtop, wb, !bfirst, !blast, uui / hhi, vvi / hhi, hhi,
+                                           bfirst ? 0.f : uuim / hhim, bfirst ? 0.f : vvim / hhim, hhim,
+                                           blast ? 0.f : uuip / hhip, blast ? 0.f : vvip / hhip, hhip);
+        xadv += z.x;
+        yadv += z.y;
+        adv_wtop = wb;
       }
       fx += P.rlin * xadv;
       fy += P.rlin * yadv;

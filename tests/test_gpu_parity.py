@@ -413,3 +413,21 @@ def test_conz3d_entry_reproduces_run_scalar():
             "conz3d")
         cn[bnd] = cb[bnd]
     assert np.array_equal(cn, ref)
+
+
+@pytest.mark.parametrize("ihwadv", [1, 2])
+@pytest.mark.parametrize("column_threads", [1, 0])
+def test_vertical_momentum_advection(ihwadv, column_threads):
+    """ilin = 0 with vertical advection of momentum (set_advective,
+    explicit.f90:776-833): upwind (1) or centred (2) from the old w at the
+    element's vertices, in the thread-per-column and warp-segment kernels."""
+    c = with_params(cases.basin3d_case(nkn_target=1500, nlv=12, dt=60.0, wind=5.0), ilin=0, ihwadv=ihwadv)
+    g, o = run_both(c, 120, column_threads=column_threads)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    me = active_mask(c, node=False)
+    umax = np.abs(so["utlnv"][me]).max()
+    assert np.abs(sg["utlnv"] - so["utlnv"])[me].max() <= 1e-3 * umax
+    flat = shyref.OracleModel(with_params(c, ihwadv=0))
+    flat.run(120)
+    assert np.abs(flat.state()["utlnv"] - so["utlnv"])[me].max() > 10e-3 * umax
