@@ -71,6 +71,25 @@ def units_per_step(case_list):
     return sum(c["nkn"] * c["nlv"] for c in case_list)
 
 
+def reduce_over_ranks(x, world, op="max", device="cuda"):
+    """x reduced over the ranks of the job (max for times, sum for work);
+    the value itself on one rank."""
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def replica_throughput(units, steps, seconds, world, device="cuda"):
+    """Whole-job units per second of replicas: every rank's own units (its
+    replica's ensemble) summed, over the slowest rank's time."""
+    total = reduce_over_ranks(units * steps, world, "sum", device)
+    return total / reduce_over_ranks(seconds, world, "max", device)
+
+
 def workload_config(workload, case_list, l2):
     if workload == "basin3d":
         c = case_list[0]
@@ -436,12 +455,9 @@ def main():
     ms_total = sum(e0.elapsed_time(e1) for e0, e1 in zip(ev0, ev1))
     barrier()
     clocks = sampler.summary(t_wall0, t_wall1)
-    if world > 1:
-        t = torch.tensor([ms_total], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    value = replica_throughput(units, a.steps, ms_total / 1000.0, world)
+    ms_total = 1000.0 * reduce_over_ranks(ms_total / 1000.0, world, "max")
     ms_step = ms_total / a.steps
-    value = world * units * a.steps / (ms_total / 1000.0)
 
     # ---- end to end through the public API: forcing in from pinned host
     #      memory and the water level of every basin out, every step ----
@@ -469,11 +485,7 @@ def main():
         shygpu.check(lib.shygpu_get_levels(model.h, ring[i % 4].data_ptr()), "get_levels")
     shygpu.check(lib.shygpu_sync(model.h), "sync")
     e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * units * e2e_steps / e2e_s
+    e2e_value = replica_throughput(units, e2e_steps, e2e_s, world)
 
     # The reference-style form, basin by basin with a wait after each call
     # (shygpu_set_forcing per basin, shygpu_run(1), shygpu_get_state per
@@ -499,11 +511,7 @@ def main():
         for b in range(nb):
             shygpu.check(lib.shygpu_get_state(model.h, b, C.byref(states[b])), "get_state")
     pb_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([pb_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        pb_s = float(t.item())
-    pb_value = world * units * pb_steps / pb_s
+    pb_value = replica_throughput(units, pb_steps, pb_s, world)
 
     # ---- live per-kernel times for the roofline (eager launches with events) ----
     prof = model.profile_steps(20)
