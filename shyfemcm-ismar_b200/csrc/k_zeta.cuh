@@ -105,6 +105,11 @@ __device__ __forceinline__ void cluster_sum_w0(cg::cluster_group &cl, const floa
   par ^= 1;
 }
 
+// the fraction of the outer target the FP32 inner solve goes down to
+__device__ __forceinline__ double tfrac(const ZetaArgs &za) {
+  return za.tol_frac > 0.f ? (double)za.tol_frac : 0.25;
+}
+
 // one row of the assembly: FP64 gather of the element entries of every slot
 // (element order), the rhs, the diagonal
 __device__ __forceinline__ void assemble_row(const Dev &d, const ZetaArgs &za, int i, float dtf,
@@ -224,7 +229,7 @@ __global__ void __launch_bounds__(1024) k_zeta_sm(Dev d, ZetaArgs za, ZetaShape 
       rn = sqrt(acc[0]);
     }
     if (rn <= tol) { conv = true; break; }
-    const double itol2 = fmax((double)za.inner_rtol * rn, 0.25 * tol) * fmax((double)za.inner_rtol * rn, 0.25 * tol);
+    const double itol2 = fmax((double)za.inner_rtol * rn, tfrac(za) * tol) * fmax((double)za.inner_rtol * rn, tfrac(za) * tol);
     // Chronopoulos-Gear CG, Jacobi preconditioner (u = D^-1 r, w = A u)
     for (int li = tid; li < nloc; li += nth) {
       const float u = sdv[li] * sr[li];

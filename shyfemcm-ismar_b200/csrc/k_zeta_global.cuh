@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(1024) k_zeta(Dev d, ZetaArgs za, int CL) {
         if (rep == 0) resid0 = rn;
       }
       if (rn <= tol) { conv = true; break; }
-      const double itol = fmax((double)za.inner_rtol * rn, 0.25 * tol);
+      const double itol = fmax((double)za.inner_rtol * rn, tfrac(za) * tol);
       if (za.sym) {
         // Chronopoulos-Gear CG with vectors in global memory
         for (int i = r0 + tid; i < r1; i += nth) {

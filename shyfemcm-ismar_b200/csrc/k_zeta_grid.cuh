@@ -252,7 +252,7 @@ __device__ __forceinline__ void grid_transition(GridState &g, const double (&tot
       if (rn <= g.tol) { g.conv = 1; g.stage = G_FINISH; }
       else if (g.outer >= za.max_outer) g.stage = G_FINISH;
       else {
-        const double it = fmax((double)za.inner_rtol * rn, 0.25 * g.tol);
+        const double it = fmax((double)za.inner_rtol * rn, tfrac(za) * g.tol);
         g.itol2 = it * it;
         g.stage = G_SPMV0;
       }

@@ -18,6 +18,7 @@ struct ZetaArgs {
   int cs, es;
   int explicit_mode;    // system_set_explicit: diagonal (lumped) solve
   float inner_rtol;     // FP32 inner iterations reduce the residual by this factor
+  float tol_frac;       // ... or reach this fraction of the outer target (0: 0.25)
   int max_outer;        // FP64 refinement sweeps
   int sym;              // 1: CG (symmetric system), 0: BiCGStab
 };
