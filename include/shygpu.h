@@ -279,9 +279,18 @@ int shygpu_set_nudging(shygpu_model *model, int32_t ibasin, const float *andgzv)
 /* Tuning options by name: "use_graph" (CUDA-graph replay of whole steps,
  * the transport sub-step loop as a device-driven conditional node; default
  * 1), "cluster_size" and "zeta_threads" (shape of the per-basin cluster of
- * the zeta solve), "inner_rtol" (residual reduction of each FP32 Krylov
- * sweep), "max_outer" (FP64 refinement sweeps), "symmetric" (CG instead of
- * BiCGStab; refused when Coriolis makes the system non-symmetric).        */
+ * the zeta solve), "zeta_variant" (0 cluster solver with vectors in global
+ * memory, 1 shared-memory clusters where every basin fits, 2 one
+ * device-wide cooperative solve), "zeta_stage" (device-wide solve with
+ * TMA-staged tiles), "inner_rtol" (residual reduction of each FP32 Krylov
+ * sweep, default 1e-4), "inner_tol_frac" (an FP32 sweep also stops at this
+ * fraction of the outer target, default 0.75), "max_outer" (FP64
+ * refinement sweeps), "symmetric" (CG instead of BiCGStab; refused when
+ * Coriolis makes the system non-symmetric), "column_threads" (1 one thread
+ * per element column for up to 16 layers, 0 one warp segment),
+ * "zeta_barrier_timeout_test" (failure detection: the device-wide solve's
+ * barrier waits for an arrival that never comes and reports SHY_ECUDA).
+ * Every change rebuilds the step graphs at the next step.                  */
 int shygpu_set_option(shygpu_model *model, const char *name, double value);
 double shygpu_get_option(shygpu_model *model, const char *name);
 
