@@ -50,7 +50,7 @@ def parse():
     p.add_argument("--steps", type=int, default=400)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="shygpu", choices=["shygpu", "reference"])
-    p.add_argument("--workload", default="ensemble", choices=["ensemble", "basin3d", "serve"])
+    p.add_argument("--workload", default="ensemble", choices=["ensemble", "basin3d", "lagoon", "serve"])
     p.add_argument("--serve-requests", type=int, default=30,
                    help="serve workload: requests of the Poisson stream (20/min)")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -62,6 +62,8 @@ def make_cases(workload, rank=0, first=None):
     from shygpu import cases
     if workload == "basin3d":
         return [cases.basin3d_case(nkn_target=20000, seed=2 + 1000 * rank)]
+    if workload == "lagoon":
+        return [cases.lagoon_case(nkn_target=250000, nlv=30, seed=7 + 1000 * rank)]
     if workload == "serve":
         return [c for _, c, _ in cases.serve_requests(first or 30, seed=5 + 1000 * rank)]
     return cases.ensemble_cases(64, seed=4 + 1000 * rank, first=first)
@@ -91,6 +93,11 @@ def replica_throughput(units, steps, seconds, world, device="cuda"):
 
 
 def workload_config(workload, case_list, l2):
+    if workload == "lagoon":
+        c = case_list[0]
+        return {"workload": "lagoon_sigma_tracers", "nkn": c["nkn"], "nel": c["nel"],
+                "nlv": c["nlv"], "layers": "sigma", "dt_s": c["params"]["dt"], "tracers": 3,
+                "forcing": "M2 0.5 m + S2 0.3 m", "l2": l2}
     if workload == "basin3d":
         c = case_list[0]
         return {"workload": "basin3d_baroclinic_ts", "nkn": c["nkn"], "nel": c["nel"],

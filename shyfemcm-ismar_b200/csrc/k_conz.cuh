@@ -241,9 +241,9 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
     }
     // horizontal fluxes: sum over the incident elements of aj4*(3*fl - hdif)
     if (act) {
-#pragma unroll 2
+#pragma unroll 4
       for (int p = pbeg; p < pend; p++) {
-        const int4 ix = d.incx[p];           // element, vertex | layers, other two nodes
+        const int4 ix = __ldg(&d.incx[p]);   // element, vertex | layers, other two nodes
         const int e = ix.x, ii = ix.y & 3;
         if (lane >= (ix.y >> 2)) continue;
         const float4 e0 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8);
@@ -251,7 +251,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
         const float bb[3] = {e0.x, e0.y, e0.z}, cc[3] = {e0.w, e1.x, e1.y};
         const float aj4 = 4.f * e1.z;
         const size_t oe = (size_t)e * NLV + lane;
-        const float us = d.usv[oe], vs = d.vsv[oe];
+        const float us = __ldg(&d.usv[oe]), vs = __ldg(&d.vsv[oe]);
         float f3[3];
         int itot = 0, isum = 0;
 #pragma unroll
@@ -260,8 +260,8 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
           if (f3[jj] < 0.f) { itot++; isum += jj + 1; }
         }
         if (itot == 0 && !anyrk) continue;      // no horizontal flux for this vertex
-        const float hmed = anyrk ? rso * d.hen[oe] + rsot * d.heo[oe] : 0.f;
-        const float dfh = anyrk ? d.difhv[oe] : 0.f;
+        const float hmed = anyrk ? rso * __ldg(&d.hen[oe]) + rsot * __ldg(&d.heo[oe]) : 0.f;
+        const float dfh = anyrk ? __ldg(&d.difhv[oe]) : 0.f;
         const int kja = ix.z, kjb = ix.w;
         const float fii = sel3(f3, ii);
         // horizontal TVD (concentration_omp.f90:675-686) where no vertex is
@@ -280,8 +280,8 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
         for (int r = 0; r < NR; r++) {
           if (sidx[r] < 0) continue;
           const float *cs = cin_base + sidx[r] * SN;
-          const float ca = clipc(cs[(size_t)kja * NLV + lane], istmp[r]);
-          const float cb = clipc(cs[(size_t)kjb * NLV + lane], istmp[r]);
+          const float ca = clipc(__ldg(&cs[(size_t)kja * NLV + lane]), istmp[r]);
+          const float cb = clipc(__ldg(&cs[(size_t)kjb * NLV + lane]), istmp[r]);
           // concentrations of vertices 0,1,2 (own value at ii, the others in order)
           const float c3[3] = {ii == 0 ? cl[r] : ca, ii == 1 ? cl[r] : (ii == 0 ? ca : cb), ii == 2 ? cl[r] : cb};
           float fl;
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
           if (rk[r] != 0.f) {
             float wdiff = 0.f;
 #pragma unroll
-            for (int iii = 0; iii < 3; iii++) wdiff += d.wdif[(size_t)e * 9 + 3 * iii + ii] * c3[iii];
+            for (int iii = 0; iii < 3; iii++) wdiff += __ldg(&d.wdif[(size_t)e * 9 + 3 * iii + ii]) * c3[iii];
             hdif = 3.f * rk[r] * dfh * hmed * wdiff;
           }
           hs[r] += aj4 * (3.f * fl - hdif);
