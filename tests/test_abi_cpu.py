@@ -49,3 +49,20 @@ def test_no_cpu_fallback_without_device(channel):
 
 def test_footprint_positive(small3d):
     assert shygpu.footprint([small3d]) > 0
+
+
+def test_header_is_plain_c99(tmp_path):
+    """include/shygpu.h is a C ABI: it compiles as strict C99 (a Fortran
+    iso_c_binding or cgo host includes it from C)."""
+    import shutil
+    import subprocess
+    from pathlib import Path
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "use.c"
+    src.write_text('#include "shygpu.h"\nint main(void) { return shygpu_last_error() == 0; }\n')
+    inc = Path(__file__).resolve().parents[1] / "include"
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                        "-I", str(inc), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
