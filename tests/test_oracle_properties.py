@@ -44,3 +44,30 @@ def test_closed_basin_conserves_volume_and_tracer_mass():
     assert abs(v1 / v0 - 1.0) < 1e-12
     for a, b in zip(m0, m1):
         assert abs(b / a - 1.0) < 1e-12
+
+
+def test_tidal_channel_matches_the_standing_wave():
+    """A closed channel of length L forced by a tide at its mouth holds the
+    standing long wave z(x) = A cos(k (L - x)) / cos(k L), k = omega /
+    sqrt(g H): with k L = 0.9 the tide at the closed end is 1/cos(0.9) = 1.61
+    times the mouth's.  Bottom friction lowers that a little; the oracle
+    must be within 5% after eight periods of spin-up."""
+    import math
+    H, A = 10.0, 0.1
+    k = (2 * math.pi / cases.M2_PERIOD) / math.sqrt(9.81 * H)
+    L = 0.9 / k
+    c = cases.channel_case(nx=91, ny=4, lx=L, ly=3e3, ampli=A, depth=H, ddepth=0.0)
+    c["params"] = dict(c["params"], dt=120.0)
+    o = shyref.OracleModel(c)
+    per = int(cases.M2_PERIOD / 120.0)
+    o.run(8 * per)
+    x = c["xgv"]
+    far, near = x > 0.97 * L, x < 0.03 * L
+    a_far = a_near = 0.0
+    for _ in range(per):
+        o.run(1)
+        z = o.state()["znv"]
+        a_far = max(a_far, float(np.abs(z[far]).max()))
+        a_near = max(a_near, float(np.abs(z[near]).max()))
+    ratio = a_far / a_near
+    assert abs(ratio / (1.0 / math.cos(0.9)) - 1.0) < 0.05, ratio
