@@ -71,3 +71,37 @@ def test_tidal_channel_matches_the_standing_wave():
         a_near = max(a_near, float(np.abs(z[near]).max()))
     ratio = a_far / a_near
     assert abs(ratio / (1.0 / math.cos(0.9)) - 1.0) < 0.05, ratio
+
+
+def test_inertial_oscillation_with_quadratic_friction():
+    """Coriolis and bottom friction (hydro_intern, chezy.f90 ireib 5) against
+    their analytic solution: a uniform flow in the middle of a wide, flat
+    basin turns clockwise at the inertial frequency f (pointing south,
+    west, north a quarter, half and three quarters of 2 pi / f later) while
+    quadratic friction slows it as |U|(t) = U0 / (1 + cd U0 t / h^2)."""
+    import math
+    f, h, u0 = 1.0e-4, 20.0, 0.1
+    c = cases.channel_case(nx=31, ny=31, lx=2.0e6, ly=2.0e6, ampli=0.0, depth=h, ddepth=0.0)
+    c["bnd_index"] = np.zeros_like(c["bnd_index"])
+    c["tide"] = np.zeros((0, 1, 4), np.float32)
+    c["fcorv"] = np.full(c["nel"], f, np.float32)
+    c["utlnv"] = np.full((c["nel"], 1), u0 * h, np.float32)
+    c["params"] = dict(c["params"], dt=60.0)
+    cd = float(c["params"]["czdef"])
+    xe = c["xgv"][c["nen3v"] - 1].mean(1)
+    ye = c["ygv"][c["nen3v"] - 1].mean(1)
+    mid = int(np.argmin((xe - 1.0e6) ** 2 + (ye - 1.0e6) ** 2))
+    o = shyref.OracleModel(c)
+    period = 2 * math.pi / f
+    done = 0
+    for q, angle in ((1, -90.0), (2, 180.0), (3, 90.0)):
+        n = int(round(q * period / 4 / 60.0))
+        o.run(n - done)
+        done = n
+        s = o.state()
+        U, V = float(s["utlnv"][mid, 0]), float(s["vtlnv"][mid, 0])
+        d = (math.degrees(math.atan2(V, U)) - angle + 180.0) % 360.0 - 180.0
+        assert abs(d) < 1.0, (q, d)
+        t = n * 60.0
+        expect = u0 * h / (1.0 + cd * u0 * h * t / h ** 2)
+        assert abs(math.hypot(U, V) / expect - 1.0) < 0.01, (q, math.hypot(U, V), expect)
