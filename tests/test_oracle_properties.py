@@ -105,3 +105,37 @@ def test_inertial_oscillation_with_quadratic_friction():
         t = n * 60.0
         expect = u0 * h / (1.0 + cd * u0 * h * t / h ** 2)
         assert abs(math.hypot(U, V) / expect - 1.0) < 0.01, (q, math.hypot(U, V), expect)
+
+
+def test_vertical_diffusion_spreads_as_the_heat_equation():
+    """conz3d's implicit vertical diffusion (concentration_omp.f90:566-611,
+    conz3d_nodes) on a still, flat column of 32 sigma layers: a Gaussian
+    tracer's variance grows by 2 K t, as the diffusion equation says (the
+    implicit scheme keeps that moment relation exactly on a uniform grid),
+    and its mass stays."""
+    nlv, H, K, s0, zc = 32, 16.0, 1e-3, 1.0, 8.0
+    c = cases.lagoon_case(nkn_target=300, nlv=nlv, ntracer=1)
+    c["hm3v"] = np.full_like(c["hm3v"], H)
+    c["tide"] = np.zeros_like(c["tide"])
+    c["tauxnv"] = np.zeros(c["nkn"], np.float32)
+    c["difv"] = np.full((c["nkn"], nlv + 1), K, np.float32)
+    dz = H / nlv
+    zmid = (np.arange(nlv) + 0.5) * dz
+    prof = np.exp(-(zmid - zc) ** 2 / (2 * s0 ** 2))
+    c["conzv"] = np.repeat(prof[None, None, :], c["nkn"], axis=1).astype(np.float32)
+    c["params"] = dict(c["params"], difmol=0.0, chpar=0.0)
+    o = shyref.OracleModel(c)
+    k = int(np.argmin(np.abs(c["xgv"] - c["xgv"].mean()) + np.abs(c["ygv"] - c["ygv"].mean())))
+
+    def moments(col):
+        m0 = col.sum()
+        m1 = (col * zmid).sum() / m0
+        return m0, (col * (zmid - m1) ** 2).sum() / m0
+
+    m0a, v0 = moments(o.state()["conzv"][0][k])
+    n = 40
+    o.run(n)
+    m0b, v1 = moments(o.state()["conzv"][0][k])
+    t = n * float(c["params"]["dt"])
+    assert abs((v1 - v0) / (2 * K * t) - 1.0) < 1e-3
+    assert abs(m0b / m0a - 1.0) < 1e-9
