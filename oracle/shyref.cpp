@@ -448,6 +448,14 @@ struct Model {
   std::vector<double> uov, vov;             // barotropic transports of the old level
   std::vector<double> uprv, vprv;           // nodal velocities (mod_hydro_print), make_prvel
   std::vector<double> andgzv;               // water-level nudging contribution per node (mod_nudging)
+  // conz3d_omp's source terms for one tracer (concentration_omp.f90:92-98):
+  // nudging to cobs at rate robs*rtauv, settling at wsink*wsinkv, loading
+  // rload*load; all (nkn, nlv) rows but wsinkv (nkn, nlv+1), interfaces 0..nlv
+  struct ScalarTerms {
+    int itr = -1;
+    double robs = 0., wsink = 0., rload = 0.;
+    std::vector<double> cobs, rtauv, wsinkv, load;
+  } sterm;
   // itvd = 2: per element and ordered vertex pair (c, d) the element holding
   // the point 2 x_c - x_d and its barycentric weights there (tvd_upwind_init_elem)
   std::vector<int> tvdup_e;                 // [6*ie + slot], -1 outside the basin
@@ -1106,9 +1114,9 @@ double masscont(Model &m) {
   return total;
 }
 
-// conzstab (concentration.f90:1573-2080) restricted to robs = 0, no sinking,
-// no point sources: the transport stability index with ddt = 1.
-double conzstab(Model &m, double rkpar) {
+// conzstab (concentration.f90:1573-2080) without point sources, settling
+// from tm (or none): the transport stability index with ddt = 1.
+double conzstab(Model &m, double rkpar, const Model::ScalarTerms *tm = nullptr) {
   int nlv = m.nlv;
   double az = m.p.azpar, azt = 1. - az, ad = m.p.adpar, adt = 1. - ad, aa = m.p.aapar, aat = 1. - aa;
   const double dt = 1.;      // ddt = 1, istot = isact = 1 -> rso = 0, rsn = 1
@@ -1133,6 +1141,8 @@ double conzstab(Model &m, double rkpar) {
         H(hold, l, ii) = ho;                 // rso = 0
         H(hnew, l, ii) = hn;                 // rsn = 1
         H(wl, l, ii) = m.wlnv[(size_t)k * (nlv + 1) + l];
+        if (tm && tm->wsink != 0.)           // settling (concentration.f90:1860)
+          H(wl, l, ii) -= tm->wsink * tm->wsinkv[(size_t)k * (nlv + 1) + l];
       }
     }
     for (int ii = 0; ii < 3; ii++) H(wl, ilevel, ii) = 0.;
@@ -1324,10 +1334,11 @@ void tvd_fluxes(const Model &m, int ie, int l, int itot, int isum, double dt, co
 // conz3d_omp (concentration_omp.f90:65-350) with conz3d_element (:355-755),
 // vertical_flux_ie (tvd_admin.f90:930-1019, itvdv 0 or 1) and
 // conz3d_nodes (:757-888); itvd 0 or 1 (gx, gy: the node gradients of
-// tvd_grad_3d), robs = 0, no sinking, no loading, cbound unused because
-// mfluxv = 0.
+// tvd_grad_3d); cbound unused because mfluxv = 0.  tm (or null) carries the
+// nudging, settling and loading terms; its load is updated where deposition
+// takes less than asked (conz3d_nodes :819-829).
 void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int istot, int isact,
-            const std::vector<double> &gx, const std::vector<double> &gy) {
+            const std::vector<double> &gx, const std::vector<double> &gy, Model::ScalarTerms *tm = nullptr) {
   int nlv = m.nlv;
   double az = m.p.azpar, ad = m.p.adpar, aa = m.p.aapar;
   double azt = 1. - az, adt = 1. - ad, aat = 1. - aa;
@@ -1359,6 +1370,8 @@ void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int is
         H(hnew, l, ii) = rsn * hn + rsnt * ho;
         H(cl, l, ii) = cn1[(size_t)k * nlv + l - 1];
         H(wl, l, ii) = m.wlnv[(size_t)k * (nlv + 1) + l];
+        if (tm && tm->wsink != 0.)                 // settling (:496)
+          H(wl, l, ii) -= tm->wsink * tm->wsinkv[(size_t)k * (nlv + 1) + l];
       }
     }
     for (int ii = 0; ii < 3; ii++) H(wl, ilevel, ii) = 0.;
@@ -1442,8 +1455,16 @@ void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int is
       for (int ii = 0; ii < 3; ii++) {
         int k = kn[ii];
         double hmed = haver[l];
+        // nudging (:694-698): an = 0, so the relaxation is explicit and
+        // finu, the implicit part of the diagonal (:729), is zero
+        double fnudge = 0.;
+        if (tm && tm->robs != 0.) {
+          size_t q = (size_t)k * nlv + l - 1;
+          fnudge = tm->robs * tm->rtauv[q] * (tm->cobs[q] - H(cl, l, ii));
+        }
         double cexpl = aj4 * (H(hold, l, ii) * H(cl, l, ii) +
-                              dt * (3. * fl[ii] - fw[ii] - rk3 * hmed * wdiff[ii] - fd[ii]));
+                              dt * (H(hold, l, ii) * fnudge + 3. * fl[ii] - fw[ii] - rk3 * hmed * wdiff[ii] -
+                                    fd[ii]));
         double alow = aj4 * dt * H(clm, l, ii);
         double ahigh = aj4 * dt * H(clp, l, ii);
         double adiag = aj4 * dt * H(clc, l, ii) + aj4 * H(hnew, l, ii);
@@ -1457,6 +1478,23 @@ void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int is
     int ilevel = m.ilhkv[k], jlevel = 1;
     double *cnk = &cn[(size_t)k * nlv];
     double *cd = &cdiag[(size_t)k * nlv], *clo = &clow[(size_t)k * nlv], *chi = &chigh[(size_t)k * nlv];
+    // loading (:816-833) on the assembled mass: a source adds dt*loading; a
+    // sink removes at most what an exponential decay over dt leaves, and the
+    // load is cut to what was taken.  cload <= cn holds by construction, so
+    // the reference's check on it (:827) never fires.
+    for (int l = jlevel; tm && tm->rload != 0. && l <= ilevel; l++) {
+      double &load = tm->load[(size_t)k * nlv + l - 1];
+      double loading = tm->rload * load;
+      if (loading == 0.) continue;
+      if (loading < 0.) {
+        double cload = 0.;
+        if (cnk[l - 1] > 0.) cload = cnk[l - 1] * (1. - std::exp(dt * loading / cnk[l - 1]));
+        else if (cnk[l - 1] < 0.) cnk[l - 1] = 0.;
+        loading = -cload / dt;
+        if (tm->rload > 0.) load = loading / tm->rload;
+      }
+      cnk[l - 1] += dt * loading;
+    }
     if ((aa == 0. && ad == 0.) || nlv == 1) {
       for (int l = jlevel; l <= ilevel; l++)
         if (cd[l - 1] != 0.) cnk[l - 1] = cnk[l - 1] / cd[l - 1];
@@ -1487,8 +1525,8 @@ void bndo_impbc(Model &m, std::vector<double> &cnv, const std::vector<double> &r
 }
 
 int scal3sh(Model &m, std::vector<double> &cnv, double rkpar, bool is_temp,
-            const std::vector<double> &rbc, int *istot_out) {
-  double sindex = conzstab(m, rkpar);
+            const std::vector<double> &rbc, int *istot_out, Model::ScalarTerms *tm = nullptr) {
+  double sindex = conzstab(m, rkpar, tm);
   double rindex = m.p.dt * sindex;
   int istot = 1 + (int)rindex;
   *istot_out = istot;
@@ -1499,7 +1537,7 @@ int scal3sh(Model &m, std::vector<double> &cnv, double rkpar, bool is_temp,
     if (!is_temp)
       for (auto &v : cnv) if (v < 1.e-15) v = 0.;
     if (m.p.itvd == 1) tvd_grad_3d(m, cnv, gx, gy);        // (concentration.f90:744)
-    conz3d(m, cnv, m.p.dt, rkpar, istot, isact, gx, gy);
+    conz3d(m, cnv, m.p.dt, rkpar, istot, isact, gx, gy, tm);
     bndo_impbc(m, cnv, rbc);
   }
   return SHY_OK;
@@ -1837,7 +1875,7 @@ int step(Model &m) {
                           m.conzv.begin() + (size_t)(ic + 1) * m.nlv * m.nkn);
     std::vector<double> cb(m.cbnd.begin() + (size_t)ic * m.nlv * m.nkn,
                            m.cbnd.begin() + (size_t)(ic + 1) * m.nlv * m.nkn);
-    st = scal3sh(m, c, m.p.chpar, false, cb, &istot);
+    st = scal3sh(m, c, m.p.chpar, false, cb, &istot, m.sterm.itr == ic ? &m.sterm : nullptr);
     if (st) return st;
     std::copy(c.begin(), c.end(), m.conzv.begin() + (size_t)ic * m.nlv * m.nkn);
   }
@@ -2031,6 +2069,33 @@ int shyref_set_nudging(void *h, const float *andgzv) {
   Model &m = *(Model *)h;
   if (!andgzv) { m.andgzv.clear(); return SHY_OK; }
   m.andgzv.assign(andgzv, andgzv + m.nkn);
+  return SHY_OK;
+}
+
+// conz3d_omp's source terms for tracer itr (itr < 0: none): arrays (nkn,
+// nlv) but wsinkv (nkn, nlv+1); an array whose factor is zero is unused.
+// load is read back with shyref_get_load after deposition has cut it.
+int shyref_set_scalar_terms(void *h, int itr, const float *cobs, float robs, const float *rtauv, float wsink,
+                            const float *wsinkv, float rload, const float *load) {
+  Model &m = *(Model *)h;
+  Model::ScalarTerms t;
+  t.itr = itr;
+  const size_t n = (size_t)m.nkn * m.nlv, n1 = (size_t)m.nkn * (m.nlv + 1);
+  if (itr >= 0) {
+    if ((robs != 0.f && (!cobs || !rtauv)) || (wsink != 0.f && !wsinkv) || (rload != 0.f && !load))
+      return fail(SHY_EARG, "set_scalar_terms: a term without its array");
+    t.robs = robs; t.wsink = wsink; t.rload = rload;
+    if (robs != 0.f) { t.cobs.assign(cobs, cobs + n); t.rtauv.assign(rtauv, rtauv + n); }
+    if (wsink != 0.f) t.wsinkv.assign(wsinkv, wsinkv + n1);
+    if (rload != 0.f) t.load.assign(load, load + n);
+  }
+  m.sterm = std::move(t);
+  return SHY_OK;
+}
+
+int shyref_get_load(void *h, double *load) {
+  Model &m = *(Model *)h;
+  std::copy(m.sterm.load.begin(), m.sterm.load.end(), load);
   return SHY_OK;
 }
 

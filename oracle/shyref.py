@@ -40,6 +40,9 @@ def _lib():
     lib.shyref_set_state.argtypes = [C.c_void_p, C.POINTER(abi.ShyState)]
     lib.shyref_run.argtypes = [C.c_void_p, C.c_int]
     lib.shyref_set_nudging.argtypes = [C.c_void_p, C.c_void_p]
+    lib.shyref_set_scalar_terms.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_float, C.c_void_p,
+                                            C.c_float, C.c_void_p, C.c_float, C.c_void_p]
+    lib.shyref_get_load.argtypes = [C.c_void_p, d_p]
     lib.shyref_step_info.argtypes = [C.c_void_p, C.POINTER(abi.ShyStepInfo)]
     lib.shyref_get_state64.argtypes = [C.c_void_p] + [d_p] * 11
     lib.shyref_last_system.argtypes = [C.c_void_p, i_p, d_p, d_p]
@@ -184,6 +187,23 @@ class OracleModel:
         a = None if andgzv is None else np.ascontiguousarray(andgzv, np.float32)
         self._andg = a
         check(lib.shyref_set_nudging(self.h, None if a is None else a.ctypes.data), "set_nudging")
+
+    def set_scalar_terms(self, itr, cobs=None, robs=0.0, rtauv=None, wsink=0.0, wsinkv=None,
+                         rload=0.0, load=None):
+        """conz3d_omp's nudging (cobs, robs, rtauv), settling (wsink, wsinkv)
+        and loading (rload, load) for tracer itr; arrays (nkn, nlv), wsinkv
+        (nkn, nlv+1).  itr < 0 removes them."""
+        f = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)
+        arrs = [f(cobs), f(rtauv), f(wsinkv), f(load)]
+        p = [None if a is None else a.ctypes.data for a in arrs]
+        check(lib.shyref_set_scalar_terms(self.h, itr, p[0], robs, p[1], wsink, p[2], rload, p[3]),
+              "set_scalar_terms")
+
+    def load(self):
+        """The loading array after deposition has cut it, (nkn, nlv)."""
+        out = np.zeros((self.case["nkn"], self.case["nlv"]))
+        check(lib.shyref_get_load(self.h, dptr(out)), "get_load")
+        return out
 
     def last_system(self):
         nnz = C.c_int(0)
