@@ -255,16 +255,22 @@ int shygpu_checkpoint_load(shygpu_model *model, const void *buf, int64_t nbytes)
  * it called conz3d_omp (concentration.f90:748) after shygpu_hydro.  cn1
  * (nlvddi, nkn) is read and overwritten with the new concentration; the
  * open-boundary values stay to the caller (bndo_setbc), gradxv/gradyv are
- * the caller's tvd_grad_3d result for itvd = 1.  Scalar nudging (robs),
- * sinking (wsink, wsinkv) and loading (rload) are refused with SHY_EARG;
- * co1 and cbound are not read (no boundary mass fluxes on this path).
- * nlvddi and nlev must be the basin's nlv, azpar the model's.  The first
- * call allocates the call's device arrays.                                 */
+ * the caller's tvd_grad_3d result for itvd = 1.  Scalar nudging relaxes
+ * toward cobs (nlvddi, nkn) at robs*rtauv, explicitly (an = 0,
+ * concentration_omp.f90:694-709); settling lowers the vertical velocity by
+ * wsink*wsinkv (0:nlvddi, nkn) (:496); loading adds rload*load (nlvddi, nkn)
+ * in mass per second and, for a sink, takes at most an exponential decay
+ * of the layer's mass over the sub-step, writing the load it took back
+ * into load (conz3d_nodes :816-833).  An array whose factor is 0 is not
+ * read.  co1 and cbound are not read (no boundary mass fluxes on this
+ * path).  nlvddi and nlev must be the basin's nlv, azpar the model's.  The
+ * first call (and the first with a source term) allocates the call's
+ * device arrays.                                                          */
 int shygpu_conz3d(shygpu_model *model, int32_t ibasin, float *cn1, float *co1, double ddt,
                   float rkpar, const float *difhv, const float *difv, float difmol,
                   const float *cbound, int32_t itvd, int32_t itvdv, const float *gradxv,
                   const float *gradyv, const float *cobs, float robs, const float *rtauv,
-                  float wsink, const float *wsinkv, float rload, const float *load,
+                  float wsink, const float *wsinkv, float rload, float *load,
                   float azpar, float adpar, float aapar, int32_t istot, int32_t isact,
                   int32_t nlvddi, int32_t nlev);
 

@@ -95,6 +95,12 @@ struct Dev {
   int4 *tvdup;                  // (6*NEL) itvd = 2: {element, xi0, xi1, xi2 as float bits} per vertex pair
   float *andg;                  // (NKN) water-level nudging contribution andgzv, or null (none set)
   int conz_free_bnd;            // 1: k_conz leaves open-boundary values to the caller (shygpu_conz3d)
+  // shygpu_conz3d's source terms (k_conz<S, 1, true> only): nudging to
+  // cz_obs at rate cz_robs*cz_tau, settling cz_wsink*cz_wsv (NKN*(NLV+1)),
+  // loading cz_rload*cz_load, which deposition cuts in place
+  const float *cz_obs, *cz_tau, *cz_wsv;
+  float *cz_load;
+  float cz_robs, cz_wsink, cz_rload;
   BasinPar *par;
   BasinOut *out;
   // mesh (static)

@@ -278,6 +278,9 @@ struct shygpu_model {
   // columns, diffusivities, gradients, per-basin parameters and results
   float *cz_in = nullptr, *cz_out = nullptr, *cz_difhv = nullptr, *cz_difv = nullptr;
   float2 *cz_grad = nullptr;
+  // its source terms (made on the first call that has one): observations,
+  // relaxation rates, loads, settling velocities
+  float *cz_obs = nullptr, *cz_tau = nullptr, *cz_load = nullptr, *cz_wsv = nullptr;
   BasinPar *cz_par = nullptr;
   BasinOut *cz_outp = nullptr;
   cudaStream_t stream = nullptr;
@@ -1495,23 +1498,25 @@ extern "C" int shygpu_scalar(shygpu_model *m) {
 // model's current hydrodynamic state (after shygpu_hydro), with the
 // reference's argument list.  cn1 (nlvddi, nkn) is read and overwritten;
 // the open-boundary values are left to the caller's scal3sh loop
-// (bndo_setbc).  Sinking, loading and scalar nudging are refused; cbound and
-// co1 are not needed (no boundary mass fluxes; co1 is the reference's
-// scratch).
+// (bndo_setbc).  Scalar nudging (cobs, robs, rtauv), settling (wsink,
+// wsinkv) and loading (rload, load) run in the kernel's source-term
+// instance; load is written back where deposition cut it.  cbound and co1
+// are not needed (no boundary mass fluxes; co1 is the reference's scratch).
 extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1, double ddt, float rkpar,
                              const float *difhv, const float *difv, float difmol, const float *cbound,
                              int32_t itvd, int32_t itvdv, const float *gradxv, const float *gradyv,
                              const float *cobs, float robs, const float *rtauv, float wsink, const float *wsinkv,
-                             float rload, const float *load, float azpar, float adpar, float aapar,
+                             float rload, float *load, float azpar, float adpar, float aapar,
                              int32_t istot, int32_t isact, int32_t nlvddi, int32_t nlev) {
-  (void)co1; (void)cbound; (void)cobs; (void)rtauv; (void)load;
+  (void)co1; (void)cbound;
   if (!m || ib < 0 || ib >= m->nbasin || !cn1 || !difhv || !difv) return fail(SHY_EARG, "conz3d: bad arguments");
   if (!m->state_set) return fail(SHY_ESTATE, "conz3d: set_state has not been called");
   const BasinPar &bp = m->par[ib];
   if (nlvddi != bp.nlv || nlev != bp.nlv) return fail(SHY_EARG, "conz3d: nlvddi and nlev must be the basin's nlv");
   if (istot < 1 || isact < 1 || isact > istot) return fail(SHY_EARG, "conz3d: 1 <= isact <= istot");
-  if (robs != 0.f || wsink != 0.f || wsinkv || rload != 0.f)
-    return fail(SHY_EARG, "conz3d: scalar nudging, sinking and loading are not supported");
+  if ((robs != 0.f && (!cobs || !rtauv)) || (wsink != 0.f && !wsinkv) || (rload != 0.f && !load))
+    return fail(SHY_EARG, "conz3d: robs needs cobs and rtauv, wsink wsinkv, rload load");
+  const bool terms = robs != 0.f || wsink != 0.f || rload != 0.f;
   if (itvd < 0 || itvd > 2 || itvdv < 0 || itvdv > 1) return fail(SHY_EARG, "conz3d: itvd 0..2, itvdv 0..1");
   if (itvdv == 1 && aapar != 0.f) return fail(SHY_EARG, "conz3d: vertical TVD needs aapar = 0");
   if (itvd == 1 && (!gradxv || !gradyv)) return fail(SHY_EARG, "conz3d: itvd = 1 needs gradxv, gradyv");
@@ -1526,6 +1531,13 @@ extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1
     if (A.alloc(&m->cz_in, SN) || A.alloc(&m->cz_out, SN) || A.alloc(&m->cz_difhv, (size_t)m->NEL * NLV) ||
         A.alloc(&m->cz_difv, (size_t)m->NKN * (NLV + 1)) || A.alloc(&m->cz_grad, SN) ||
         A.alloc(&m->cz_par, (size_t)m->nbasin) || A.alloc(&m->cz_outp, (size_t)m->nbasin))
+      return SHY_ECAPACITY;
+  }
+  if (terms && !m->cz_obs) {
+    CUDA_TRY(cudaStreamSynchronize(st));
+    Arena &A = m->arena;
+    if (A.alloc(&m->cz_obs, SN) || A.alloc(&m->cz_tau, SN) || A.alloc(&m->cz_load, SN) ||
+        A.alloc(&m->cz_wsv, (size_t)m->NKN * (NLV + 1)))
       return SHY_ECAPACITY;
   }
   // the sub-step's parameters: basin ib transports one scalar, unclipped
@@ -1554,15 +1566,24 @@ extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1
   d.par = m->cz_par; d.out = m->cz_outp;
   d.difhv = m->cz_difhv; d.difv = m->cz_difv; d.tgrad = m->cz_grad;
   d.nsc_max = 1; d.conz_free_bnd = 1;
+  if (robs != 0.f) {
+    ST_TRY(copy_cols(m->cz_obs, cobs, bp.nk, nlv, NLV, bp.k0, true, st));
+    ST_TRY(copy_cols(m->cz_tau, rtauv, bp.nk, nlv, NLV, bp.k0, true, st));
+  }
+  if (wsink != 0.f) ST_TRY(copy_cols(m->cz_wsv, wsinkv, bp.nk, nlv + 1, NLV + 1, bp.k0, true, st));
+  if (rload != 0.f) ST_TRY(copy_cols(m->cz_load, load, bp.nk, nlv, NLV, bp.k0, true, st));
+  d.cz_obs = m->cz_obs; d.cz_tau = m->cz_tau; d.cz_wsv = m->cz_wsv; d.cz_load = m->cz_load;
+  d.cz_robs = robs; d.cz_wsink = wsink; d.cz_rload = rload;
   // k_conz reads sub-step isact from sc_in (isact 1) or the scratch of its
   // parity and writes sc_out (isact = istot) or the other scratch
   d.sc_in = m->cz_in; d.sc_out = m->cz_out;
   if (isact & 1) { d.scr1 = m->cz_in; d.scr0 = m->cz_out; }
   else { d.scr0 = m->cz_in; d.scr1 = m->cz_out; }
-  launch_node(d, m->kbas, 2, isact - 1, 0, st);
+  launch_node(d, m->kbas, terms ? 7 : 2, isact - 1, 0, st);
   g_launches += 1;
   CUDA_TRY(cudaGetLastError());
   ST_TRY(copy_cols(m->cz_out, cn1, bp.nk, nlv, NLV, bp.k0, false, st));
+  if (rload != 0.f) ST_TRY(copy_cols(m->cz_load, load, bp.nk, nlv, NLV, bp.k0, false, st));
   CUDA_TRY(cudaStreamSynchronize(st));
   BasinOut o;
   CUDA_TRY(cudaMemcpy(&o, m->cz_outp + ib, sizeof o, cudaMemcpyDeviceToHost));

@@ -159,7 +159,12 @@ __device__ __forceinline__ float tvd_v(float conc, float cond, float conu, float
   return conc + 0.5f * psi * (cond - conc) * (1.f - alfa);
 }
 
-template <int S, int NR>
+// EX: the instance of shygpu_conz3d with conz3d_omp's source terms (one
+// scalar): settling lowers the interface velocities by wsink*wsinkv
+// (concentration_omp.f90:496); nudging adds dt*aj4*hold*robs*rtau*(cobs - c)
+// per element (:694-709; an = 0, so nothing implicit); loading acts on the
+// assembled mass before the vertical solve (conz3d_nodes :816-833).
+template <int S, int NR, bool EX = false>
 __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg) {
   const int j = j_arg >= 0 ? j_arg : *d.subj;   // sub-step index: argument or device counter
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -185,8 +190,14 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
   const float hko = act ? d.hko[o] : 0.f, hkn = act ? d.hkn[o] : 0.f;
   const float rvptop = act ? d.difv[(size_t)k * I + lane] + P.difmol : 0.f;
   const float rvpbot = act ? d.difv[(size_t)k * I + lane + 1] + P.difmol : 0.f;
-  const float wt = act ? d.wl[(size_t)k * I + lane] : 0.f;
-  const float wb = act ? d.wl[(size_t)k * I + lane + 1] : 0.f;
+  float wt = act ? d.wl[(size_t)k * I + lane] : 0.f;
+  float wb = act ? d.wl[(size_t)k * I + lane + 1] : 0.f;
+  if constexpr (EX) {
+    if (act && d.cz_wsink != 0.f) {
+      wt -= d.cz_wsink * d.cz_wsv[(size_t)k * I + lane];
+      wb -= d.cz_wsink * d.cz_wsv[(size_t)k * I + lane + 1];
+    }
+  }
   const float2 av = act ? d.avol[o] : make_float2(0.f, 0.f);
   const float At = av.x, A = av.x + av.y;      // continuing elements, all elements
   // vertical TVD: the far-upwind layer of an element's column exists only
@@ -346,7 +357,25 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
       }
       const float fw = aat * (topw - botw);
       const float fd = adt * (At * (c - cp1[r]) * hmobot - A * (cm1[r] - c) * hmotop);
-      res[r] = A * hold * c + dt * (hs[r] - fw - fd);
+      float q = hs[r] - fw - fd;
+      if constexpr (EX)                               // nudging, summed over the elements
+        if (act && d.cz_robs != 0.f) q += A * hold * (d.cz_robs * d.cz_tau[o] * (d.cz_obs[o] - c));
+      res[r] = A * hold * c + dt * q;
+    }
+    if constexpr (EX) {
+      // loading on the node layer's mass: sources add dt*loading; a sink
+      // takes what an exponential decay over dt leaves and cuts the load
+      if (act && valid && d.cz_rload != 0.f) {
+        float loading = d.cz_rload * d.cz_load[o];
+        if (loading < 0.f) {
+          float cload = 0.f;
+          if (res[0] > 0.f) cload = res[0] * (1.f - expf(dt * loading / res[0]));
+          else if (res[0] < 0.f) res[0] = 0.f;
+          loading = -cload / dt;
+          if (d.cz_rload > 0.f) d.cz_load[o] = loading / d.cz_rload;
+        }
+        res[0] += dt * loading;
+      }
     }
     // vertical system of the node column (conz3d_nodes :841-868)
     if ((P.aa == 0.f && P.ad == 0.f) || P.nlv == 1) {

@@ -26,7 +26,8 @@ struct ZetaArgs {
 // which: 0 k_column, 1 k_final
 void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool cor);
 // which: 0 k_node(init_only=a), 1 k_stab, 2 k_conz(j=a, nsub=b), 3 k_rhoset,
-// 4 k_rho, 5 k_moment, 6 k_tvdgrad(j=a)
+// 4 k_rho, 5 k_moment, 6 k_tvdgrad(j=a), 7 k_conz with conz3d_omp's source
+// terms (j=a, one scalar)
 void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStream_t st);
 void launch_reduce(const Dev &d, int nsub, int advance, cudaStream_t st);
 // wetting and drying: 0 set_dry at the step's start, 1 the initial state's

@@ -78,6 +78,7 @@ static void launch_node_S(const Dev &d, const int *kbas, int which, int a, int b
     case 4: k_rho<S><<<blocks, threads, 0, st>>>(d, kbas); break;
     case 5: k_moment<S><<<blocks, threads, 0, st>>>(d, kbas); break;
     case 6: k_tvdgrad<S><<<blocks, threads, 0, st>>>(d, kbas, a); break;
+    case 7: k_conz<S, 1, true><<<blocks, threads, 0, st>>>(d, kbas, a); break;   // shygpu_conz3d's source terms
   }
 }
 

@@ -415,6 +415,59 @@ def test_conz3d_entry_reproduces_run_scalar():
     assert np.array_equal(cn, ref)
 
 
+def test_conz3d_entry_source_terms():
+    """shygpu_conz3d with scalar nudging, settling and loading
+    (concentration_omp.f90:496, 694-709; conz3d_nodes :816-833), driven by
+    the scal3sh loop for one step of the lagoon, against the oracle's step
+    with the same terms; the load that deposition took comes back in load."""
+    from test_oracle_properties import node_areas
+    c = cases.lagoon_case(nkn_target=900, nlv=12, ntracer=1)
+    p = c["params"]
+    nkn, nlv, dt = c["nkn"], c["nlv"], float(p["dt"])
+    rng = np.random.default_rng(11)
+    c0 = np.asarray(c["conzv"][0], np.float32)
+    cobs = (c0 + rng.uniform(1.0, 5.0, c0.shape)).astype(np.float32)
+    rtauv = np.full((nkn, nlv), 1.0 / 1800.0, np.float32)
+    wsinkv = rng.uniform(0.0, 2e-4, (nkn, nlv + 1)).astype(np.float32)
+    mass = node_areas(c) * float(c0.mean())
+    load = (rng.uniform(-0.5, 0.01, (nkn, nlv)) * mass / dt).astype(np.float32)
+    o = shyref.OracleModel(c)
+    o.set_scalar_terms(0, cobs=cobs, robs=1.0, rtauv=rtauv, wsink=1.0, wsinkv=wsinkv, rload=1.0, load=load)
+    o.run(1)
+    so = o.state()["conzv"][0]
+    m = shygpu.Model(c)
+    m.set_state(0)
+    ck = m.checkpoint()
+    m.hydro()
+    m.scalar()
+    plain = m.get_state(0)["conzv"][0]
+    istot = m.info(0).istot
+    assert istot == o.info().istot
+    m.restore(ck)
+    m.hydro()
+    lib = shygpu.lib()
+    cn = c0.copy()                                  # c0 keeps the boundary values
+    difhv = np.ones((c["nel"], nlv), np.float32)
+    difv = np.ascontiguousarray(c["difv"], np.float32)
+    bnd = c["bnd_index"] > 0
+    gl = load.copy()
+    for isact in range(1, istot + 1):
+        cn[cn < 1e-15] = 0.0
+        shygpu.check(lib.shygpu_conz3d(
+            m.h, 0, cn.ctypes.data, None, dt, float(p["chpar"]), difhv.ctypes.data, difv.ctypes.data,
+            float(p["difmol"]), None, 0, 0, None, None, cobs.ctypes.data, 1.0, rtauv.ctypes.data, 1.0,
+            wsinkv.ctypes.data, 1.0, gl.ctypes.data, float(p["azpar"]), float(p["adpar"]),
+            float(p["aapar"]), istot, isact, nlv, nlv), "conz3d")
+        cn[bnd] = c0[bnd]
+    cmax = np.abs(so).max()
+    act = active_mask(c)
+    assert np.abs(cn - so)[act].max() <= TRACER_RTOL * cmax
+    assert np.abs(cn - plain)[act].max() > 10 * TRACER_RTOL * cmax
+    lo = o.load()
+    assert np.abs(gl - lo)[act].max() <= TRACER_RTOL * np.abs(load).max()
+    assert np.abs(gl - load)[act].max() > 10 * TRACER_RTOL * np.abs(load).max()
+
+
 @pytest.mark.parametrize("ihwadv", [1, 2])
 @pytest.mark.parametrize("column_threads", [1, 0])
 def test_vertical_momentum_advection(ihwadv, column_threads):
