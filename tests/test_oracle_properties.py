@@ -2,6 +2,7 @@
 still water stays still, and a closed basin keeps its volume and every
 tracer's mass while wind moves the water."""
 import numpy as np
+import pytest
 
 import shyref
 from shygpu import cases
@@ -139,3 +140,27 @@ def test_vertical_diffusion_spreads_as_the_heat_equation():
     t = n * float(c["params"]["dt"])
     assert abs((v1 - v0) / (2 * K * t) - 1.0) < 1e-3
     assert abs(m0b / m0a - 1.0) < 1e-9
+
+
+@pytest.mark.parametrize("itvd", [0, 2])
+def test_transport_makes_no_new_extrema(itvd):
+    """Upwind transport (itvd 0) and the TVD scheme with the upwind point
+    (itvd 2, tvd_get_upwind_c, tvd_admin.f90:608-671) keep a tracer inside
+    its initial range over 600 steps of the tidal lagoon (no horizontal
+    diffusion, whose weights are not positive on every triangle).  The
+    gradient form (itvd 1) is not bounded in the reference either: its
+    far-upwind value is the node gradient extrapolated along the side
+    (tvd_fluxes :790-795), which can lie outside the local range."""
+    c = cases.lagoon_case(nkn_target=900, nlv=6, ntracer=1)
+    c["params"] = dict(c["params"], chpar=0.0, itvd=itvd)
+    c0 = np.asarray(c["conzv"][0])
+    lo, hi = c0.min(), c0.max()
+    o = shyref.OracleModel(c)
+    act = np.arange(c["nlv"])[None, :] < c["ilhkv"][:, None]
+    moved = 0.0
+    for _ in range(20):
+        o.run(30)
+        cn = o.state()["conzv"][0][act]
+        assert cn.min() >= lo - 1e-12 * hi and cn.max() <= hi * (1 + 1e-12)
+        moved = max(moved, np.abs(cn - c0[act]).max())
+    assert moved > 0.1 * hi
