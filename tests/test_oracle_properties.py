@@ -1,6 +1,8 @@
-"""Analytic properties of the oracle's step (the survey's test strategy):
-still water stays still, and a closed basin keeps its volume and every
-tracer's mass while wind moves the water."""
+"""Analytic and size-independent properties of the oracle's step: still
+water stays still; a closed basin keeps its volume and every tracer's mass
+while wind moves the water; a standing tide, an inertial oscillation and
+vertical diffusion follow their closed forms; upwind transport makes no
+new extrema."""
 import numpy as np
 import pytest
 
