@@ -80,3 +80,23 @@ def test_loading_adds_sources_and_decays_sinks():
     got = o.load()
     cut = np.where(L < 0, -M0 * (1 - np.exp(dt * L / M0)) / dt, L)
     assert np.abs(got - cut)[inner].max() < 1e-9 * np.abs(L).max()
+
+
+def test_fast_settling_sub_steps_the_transport():
+    """Settling enters the stability index (conzstab, concentration.f90:1860):
+    a settling speed that crosses more than one surface layer per step
+    splits the step into istot sub-steps, and the surface layer drains by
+    (1 - dt ws / (istot h)) per sub-step."""
+    c = still_case()
+    nkn, nlv, dt, c0 = c["nkn"], c["nlv"], float(c["params"]["dt"]), 2.0
+    ws = float(np.float32(0.15))
+    o = shyref.OracleModel(c)
+    o.set_scalar_terms(0, wsink=1.0, wsinkv=np.full((nkn, nlv + 1), ws, np.float32))
+    o.run(1)
+    istot = o.info().istot
+    hl = 8.0 / nlv
+    assert istot >= 1 + int(dt * ws / hl)
+    cn = o.state()["conzv"][0]
+    inner = c["bnd_index"] <= 0
+    want = c0 * (1 - dt * ws / (istot * hl)) ** istot
+    assert np.abs(cn[inner, 0] - want).max() < 1e-9
