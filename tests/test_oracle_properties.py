@@ -29,8 +29,17 @@ def test_still_water_stays_still():
     assert np.abs(s["znv"]).max() == 0.0 and np.abs(s["utlnv"]).max() == 0.0
 
 
-def test_closed_basin_conserves_volume_and_tracer_mass():
+@pytest.mark.parametrize("itvd,itvdv", [(0, 0), (1, 0), (2, 1)])
+def test_closed_basin_conserves_volume_and_tracer_mass(itvd, itvdv):
+    """Every horizontal flux leaves one vertex and enters another, and every
+    vertical flux is shared by the two layers of its interface, with the
+    upwind scheme and with both TVD forms alike.  The gradient TVD form
+    (itvd 1) undershoots below zero in places, and scal3sh's clip of
+    concentrations below 1e-15 (concentration.f90:736-740) then adds a
+    little mass: there the budget may only grow, by round-off sizes."""
     c = cases.lagoon_case(nkn_target=900, nlv=12)
+    if itvd or itvdv:
+        c["params"] = dict(c["params"], itvd=itvd, itvdv=itvdv, aapar=0.0)
     c["bnd_index"] = np.zeros_like(c["bnd_index"])
     c["tide"] = np.zeros((0, 2, 4), np.float32)
     c["tauxnv"] = np.full(c["nkn"], 2e-4, np.float32)
@@ -46,7 +55,10 @@ def test_closed_basin_conserves_volume_and_tracer_mass():
     assert np.abs(o.state()["znv"]).max() > 0.01          # the wind has moved the water
     assert abs(v1 / v0 - 1.0) < 1e-12
     for a, b in zip(m0, m1):
-        assert abs(b / a - 1.0) < 1e-12
+        if itvd == 1:
+            assert -1e-12 < b / a - 1.0 < 1e-9
+        else:
+            assert abs(b / a - 1.0) < 1e-12
 
 
 def test_tidal_channel_matches_the_standing_wave():
