@@ -240,7 +240,8 @@ int shygpu_shy_close(shygpu_shyfile *file);
  * model and its time-level indices, copied to or from a host buffer of
  * shygpu_checkpoint_bytes(model) bytes.  A checkpoint loads into the model
  * that saved it or into one made from the same basins and parameters (and
- * the same calls that add arrays: shygpu_set_nudging, shygpu_conz3d); the run
+ * the same calls that add arrays: shygpu_set_nudging, shygpu_conz3d, and
+ * shygpu_conz3d with a source term); the run
  * then continues bit for bit.
  * Loading into a model with other arrays fails with SHY_EARG.  Both calls
  * wait for the model's stream.                                             */

@@ -1652,7 +1652,8 @@ extern "C" int shygpu_checkpoint_load(shygpu_model *m, const void *buf, int64_t 
   if (h.nalloc != (int32_t)m->arena.ptrs.size() || h.bytes != m->arena.bytes || h.nbasin != m->nbasin ||
       nbytes < shygpu_checkpoint_bytes(m))
     return fail(SHY_EARG, "checkpoint_load: the checkpoint is of a model with other arrays (same basins, "
-                          "parameters, and the same first calls of shygpu_set_nudging and shygpu_conz3d, needed)");
+                          "parameters, and the same first calls of shygpu_set_nudging, shygpu_conz3d and "
+                          "shygpu_conz3d with a source term, needed)");
   for (size_t i = 0; i < m->arena.sizes.size(); i++) {
     int64_t sz;
     memcpy(&sz, p, sizeof sz);
