@@ -1115,7 +1115,7 @@ double masscont(Model &m) {
 }
 
 // conzstab (concentration.f90:1573-2080) without point sources, settling
-// from tm (or none): the transport stability index with ddt = 1.
+// and nudging from tm (or none): the transport stability index with ddt = 1.
 double conzstab(Model &m, double rkpar, const Model::ScalarTerms *tm = nullptr) {
   int nlv = m.nlv;
   double az = m.p.azpar, azt = 1. - az, ad = m.p.adpar, adt = 1. - ad, aa = m.p.aapar, aat = 1. - aa;
@@ -1181,6 +1181,8 @@ double conzstab(Model &m, double rkpar, const Model::ScalarTerms *tm = nullptr) 
         chigh[(size_t)k * nlv + l - 1] += cadv;
         clow[(size_t)k * nlv + l - 1] += chdiff;
         cn[(size_t)k * nlv + l - 1] += cvdiff;
+        if (tm && tm->robs != 0.)            // nudging (concentration.f90:1985)
+          co[(size_t)k * nlv + l - 1] += dt * aj4 * hmed * tm->robs * tm->rtauv[(size_t)k * nlv + l - 1];
       }
     }
     for (int l = 1; l <= ilevel; l++)

@@ -100,3 +100,22 @@ def test_fast_settling_sub_steps_the_transport():
     inner = c["bnd_index"] <= 0
     want = c0 * (1 - dt * ws / (istot * hl)) ** istot
     assert np.abs(cn[inner, 0] - want).max() < 1e-9
+
+
+def test_strong_nudging_sub_steps_the_transport():
+    """Nudging enters the stability index as a source flux (conzstab,
+    concentration.f90:1985): a relaxation faster than the step splits it
+    into istot sub-steps, each relaxing explicitly by dt rtau / istot."""
+    c = still_case()
+    nkn, nlv, dt, c0 = c["nkn"], c["nlv"], float(c["params"]["dt"]), 2.0
+    r = float(np.float32(2.5 / dt))
+    o = shyref.OracleModel(c)
+    o.set_scalar_terms(0, cobs=np.full((nkn, nlv), 5.0, np.float32), robs=1.0,
+                       rtauv=np.full((nkn, nlv), r, np.float32))
+    o.run(1)
+    istot = o.info().istot
+    assert istot == 1 + int(dt * r)
+    cn = o.state()["conzv"][0]
+    inner = c["bnd_index"] <= 0
+    want = 5.0 + (c0 - 5.0) * (1 - dt * r / istot) ** istot
+    assert np.abs(cn[inner] - want).max() < 1e-9
