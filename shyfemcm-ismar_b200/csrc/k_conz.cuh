@@ -363,8 +363,9 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
       res[r] = A * hold * c + dt * q;
     }
     if constexpr (EX) {
-      // loading on the node layer's mass: sources add dt*loading; a sink
-      // takes what an exponential decay over dt leaves and cuts the load
+      // loading on the node layer's mass: a source adds dt*loading; a sink
+      // removes at most what an exponential decay over dt would, and the
+      // load is cut to what it removed
       if (act && valid && d.cz_rload != 0.f) {
         float loading = d.cz_rload * d.cz_load[o];
         if (loading < 0.f) {
