@@ -224,6 +224,35 @@ class Model:
         check(lib().shygpu_set_nudging(self.h, ib, a.ctypes.data), "set_nudging")
         lib().shygpu_sync(self.h)
 
+    def conz3d(self, ib, cn1, ddt, rkpar, difhv, difv, difmol, azpar, adpar, aapar, istot, isact,
+               itvd=0, itvdv=0, gradxv=None, gradyv=None, cobs=None, robs=0.0, rtauv=None,
+               wsink=0.0, wsinkv=None, rload=0.0, load=None):
+        """conz3d_omp (concentration_omp.f90:65-76): one transport sub-step
+        (isact of istot) of one scalar of basin ib on the state hydro() made.
+        cn1 is overwritten with the new concentration, and load where
+        deposition took less than asked.  Arrays are C-contiguous float32 of
+        shape (nkn, nlv), but difhv (nel, nlv) and difv, wsinkv (nkn, nlv+1);
+        the open-boundary values stay to the caller, as in scal3sh."""
+        c = self.cases[ib]
+        nkn, nel, nlv = c["nkn"], c["nel"], c["nlv"]
+        arrays = dict(cn1=(cn1, (nkn, nlv)), difhv=(difhv, (nel, nlv)), difv=(difv, (nkn, nlv + 1)),
+                      gradxv=(gradxv, (nkn, nlv)), gradyv=(gradyv, (nkn, nlv)), cobs=(cobs, (nkn, nlv)),
+                      rtauv=(rtauv, (nkn, nlv)), wsinkv=(wsinkv, (nkn, nlv + 1)), load=(load, (nkn, nlv)))
+        for name, (a, shape) in arrays.items():
+            if a is None:
+                continue
+            if not isinstance(a, np.ndarray) or a.dtype != np.float32 or not a.flags.c_contiguous \
+                    or a.shape != shape:
+                raise ValueError(f"conz3d: {name} must be a C-contiguous float32 array of shape {shape}")
+
+        def p(a):
+            return None if a is None else a.ctypes.data
+        check(lib().shygpu_conz3d(self.h, ib, p(cn1), None, float(ddt), float(rkpar), p(difhv), p(difv),
+                                  float(difmol), None, int(itvd), int(itvdv), p(gradxv), p(gradyv),
+                                  p(cobs), float(robs), p(rtauv), float(wsink), p(wsinkv), float(rload),
+                                  p(load), float(azpar), float(adpar), float(aapar), int(istot),
+                                  int(isact), nlv, nlv), "conz3d")
+
     def shy_open(self, ib, path, date=0, time=0, title=""):
         """Hydro output of basin ib in the reference's .shy format; returns a
         handle for shy_write/shy_close."""
