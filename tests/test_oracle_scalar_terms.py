@@ -119,3 +119,27 @@ def test_strong_nudging_sub_steps_the_transport():
     inner = c["bnd_index"] <= 0
     want = 5.0 + (c0 - 5.0) * (1 - dt * r / istot) ** istot
     assert np.abs(cn[inner] - want).max() < 1e-9
+
+
+def test_settling_keeps_tracer_mass_in_a_moving_closed_basin():
+    """Settling only moves mass between layers: the surface and the bottom
+    interfaces carry none (wl(0) unused, wl(ilevel) = 0,
+    concentration_omp.f90:503-515), so a closed basin under wind keeps its
+    tracer mass while the tracer settles."""
+    c = cases.lagoon_case(nkn_target=900, nlv=8, ntracer=1)
+    c["bnd_index"] = np.zeros_like(c["bnd_index"])
+    c["tide"] = np.zeros((0, 2, 4), np.float32)
+    c["tauxnv"] = np.full(c["nkn"], 2e-4, np.float32)
+    nkn, nlv = c["nkn"], c["nlv"]
+    A = node_areas(c)
+    o = shyref.OracleModel(c)
+    o.set_scalar_terms(0, wsink=1.0, wsinkv=np.full((nkn, nlv + 1), 1e-3, np.float32))
+
+    def mass(s):
+        return (s["conzv"][0] * s["hdknv"] * A).sum(), (s["conzv"][0][:, 0] * s["hdknv"][:, 0] * A[:, 0]).sum()
+
+    m0, top0 = mass(o.state())
+    o.run(40)
+    m1, top1 = mass(o.state())
+    assert abs(m1 / m0 - 1.0) < 1e-12
+    assert top1 < 0.9 * top0                              # the surface layer has drained
