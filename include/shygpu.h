@@ -357,7 +357,12 @@ int shygpu_simsys_iterations(void);
  * symmetric != 0, else BiCGStab, FP32 inside FP64 refinement, stop when
  * ||r|| <= rtol*||r0|| + atol); its work vectors live in a fixed 5 MiB
  * array inside the library.  At most 65536 rows and 524288 stored entries:
- * larger systems return SHY_ECAPACITY.  The first call on a device, with
+ * larger systems return SHY_ECAPACITY.  The kernel checks the CSR arrays
+ * before it writes anything (rowptr[0] = 0, rowptr[n] = nnz, no row of
+ * negative length, columns in [0, n)) and returns SHY_EARG otherwise.
+ * maxit bounds the Krylov iterations of the whole call, summed over its
+ * refinement rounds (at most 12), and the returned status always describes
+ * the returned x.  The first call on a device, with
  * that device current, looks the array up and must come before any stream
  * capture begins.  There is one such array per device, so calls that
  * overlap on one device race: serialise them.  x may equal x0.  The call

@@ -19,6 +19,10 @@
 // Limits and rules of use:
 //  * at most kStaticMaxRows rows and kStaticMaxNnz stored entries; larger
 //    systems are refused with SHY_ECAPACITY before anything runs;
+//  * CSR arrays that do not describe n rows and nnz entries (rowptr[n] !=
+//    nnz, a decreasing rowptr, a column outside [0, n)) are refused with
+//    SHY_EARG by the kernel before it writes anything;
+//  * maxit counts Krylov iterations over all refinement rounds of a call;
 //  * the first call on a device (with that device current) looks the scratch
 //    array up with cudaGetSymbolAddress; make that first call before any
 //    stream capture begins;
@@ -67,7 +71,7 @@ constexpr size_t kStaticScratchBytes = kOffVec + kNumVec * kVecBytes;   // 5.0 M
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
 struct StaticArgs {
-  int n;
+  int n, nnz;
   const int *rowptr, *col;
   const double *val, *rhs;
   const float *x0;
@@ -139,6 +143,27 @@ __global__ void __launch_bounds__(1024) k_csr_static(StaticArgs a) {
   const int r0 = min(a.n, rank * chunk), r1 = min(a.n, r0 + chunk);
   const int tid = threadIdx.x, nth = blockDim.x;
 
+  // The CSR arrays are checked before anything is written: rowptr starts at
+  // 0 and ends at nnz, no row has a negative length or reaches past nnz, and
+  // every column lies in [0, n).  Every CTA takes the same sum, so a bad
+  // matrix ends every CTA here, before the FP32 copy below writes val32.
+  {
+    double bad[1] = {0.};
+    if (rank == 0 && tid == 0 && (a.rowptr[0] != 0 || a.rowptr[a.n] != a.nnz)) bad[0] += 1.;
+    for (int i = r0 + tid; i < r1; i += nth) {
+      const int k0 = a.rowptr[i], k1 = a.rowptr[i + 1];
+      if (k0 < 0 || k1 < k0 || k1 > a.nnz) { bad[0] += 1.; continue; }
+      for (int k = k0; k < k1; k++)
+        if ((unsigned)a.col[k] >= (unsigned)a.n) bad[0] += 1.;
+    }
+    csum<1>(cl, bad, wsum, slots, bc, par, CL);
+    if (bad[0] != 0.) {
+      if (rank == 0 && tid == 0) a.out->status = SHY_EARG;
+      cl.sync();   // peers may still read this CTA's slots
+      return;
+    }
+  }
+
   // FP32 copy of the matrix, Jacobi diagonal (FP64 inverse), FP64 start
   for (int i = r0 + tid; i < r1; i += nth) {
     double diag = 0.;
@@ -155,7 +180,11 @@ __global__ void __launch_bounds__(1024) k_csr_static(StaticArgs a) {
   double tol = 0., rn = 0.;
   int iters = 0, outer = 0;
   bool conv = false;
-  for (outer = 0; outer < a.max_outer; outer++) {
+  // Each round computes the FP64 residual of x64, stops when it meets the
+  // target, and otherwise solves for a correction.  The residual after the
+  // last correction is computed too, so the status always describes the x
+  // that is returned.  maxit bounds the Krylov iterations of the whole call.
+  for (outer = 0;; outer++) {
     double acc[1] = {0.};
     for (int i = r0 + tid; i < r1; i += nth) {
       double res = a.rhs[i];
@@ -168,6 +197,7 @@ __global__ void __launch_bounds__(1024) k_csr_static(StaticArgs a) {
     if (outer == 0) tol = a.rtol * rn + a.atol;
     if (outer == 0 && rank == 0 && tid == 0) a.out->resid0 = rn;
     if (rn <= tol) { conv = true; break; }
+    if (outer == a.max_outer || iters >= a.maxit) break;
     const double itol = fmax((double)a.inner_rtol * rn, 0.25 * tol);
     if (a.sym) {
       // Chronopoulos-Gear CG on the correction e
@@ -185,7 +215,7 @@ __global__ void __launch_bounds__(1024) k_csr_static(StaticArgs a) {
       }
       csum<2>(cl, g2, wsum, slots, bc, par, CL);
       double gamma = g2[0], alpha = gamma / g2[1], beta = 0.;
-      for (int it = 0; it < a.maxit; it++) {
+      while (iters < a.maxit) {
         const float fa = (float)alpha, fb = (float)beta;
         for (int i = r0 + tid; i < r1; i += nth) {
           const float pp = a.z[i] + fb * a.p[i];
@@ -223,7 +253,7 @@ __global__ void __launch_bounds__(1024) k_csr_static(StaticArgs a) {
       }
       csum<1>(cl, a1, wsum, slots, bc, par, CL);
       double rho = 1., alpha = 1., omega = 1.;
-      for (int it = 0; it < a.maxit; it++) {
+      while (iters < a.maxit) {
         double g1[1] = {0.};
         for (int i = r0 + tid; i < r1; i += nth) g1[0] += (double)a.rh[i] * a.r[i];
         csum<1>(cl, g1, wsum, slots, bc, par, CL);
@@ -367,7 +397,7 @@ extern "C" int shygpu_csr_solve_static(int32_t n, int32_t nnz, const int32_t *ro
   cudaStream_t st = (cudaStream_t)stream;
 
   StaticArgs a;
-  a.n = n; a.rowptr = rowptr; a.col = col; a.val = val; a.rhs = rhs; a.x0 = x0; a.x = x;
+  a.n = n; a.nnz = nnz; a.rowptr = rowptr; a.col = col; a.val = val; a.rhs = rhs; a.x0 = x0; a.x = x;
   a.rtol = rtol; a.atol = atol; a.maxit = maxit; a.sym = symmetric != 0;
   a.max_outer = 12; a.inner_rtol = 1e-4f;
   a.out = (StaticOut *)(base + kOffOut);
@@ -403,6 +433,12 @@ extern "C" int shygpu_csr_solve_static(int32_t n, int32_t nnz, const int32_t *ro
     return shy::external_fail(SHY_ECUDA, msg);
   }
   if (iterations) *iterations = o.iters;
+  if (o.status == SHY_EARG) {
+    snprintf(msg, sizeof msg,
+             "csr_solve_static: rowptr/col are not a CSR matrix of %d rows and %d entries "
+             "(rowptr[0] = 0, rowptr[n] = nnz, rows of non-negative length, columns in [0, n))", n, nnz);
+    return shy::external_fail(SHY_EARG, msg);
+  }
   if (o.status != SHY_OK) {
     snprintf(msg, sizeof msg, "csr_solve_static: no convergence (residual %.3g from %.3g after %d iterations)",
              o.resid, o.resid0, o.iters);

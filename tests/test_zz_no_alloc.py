@@ -14,7 +14,7 @@ import shygpu
 import shyref
 from shygpu import cases
 
-SHY_OK, SHY_ECAPACITY = 0, 9
+SHY_OK, SHY_EARG, SHY_ENOCONV, SHY_ECAPACITY = 0, 1, 3, 9
 MAX_ROWS, MAX_NNZ = 65536, 524288
 
 
@@ -117,3 +117,112 @@ def test_static_solve_matches_simsys_twice(size):
         assert np.abs(xs - z_ref).max() <= tol
     assert torch.equal(outs[0], outs[1])          # the second call starts from clean scratch
     assert free[0] == free[1]                      # no device memory taken by the second call
+
+
+def laplacian_csr(nx, ny, shift):
+    """The 5-point Laplacian of an nx x ny grid plus shift on the diagonal:
+    symmetric positive definite, condition number about 8 / shift."""
+    n = nx * ny
+    rowptr, col, val = [0], [], []
+    for j in range(ny):
+        for i in range(nx):
+            k = j * nx + i
+            ent = {k: 4.0 + shift}
+            for di, dj in ((-1, 0), (1, 0), (0, -1), (0, 1)):
+                if 0 <= i + di < nx and 0 <= j + dj < ny:
+                    ent[k + dj * nx + di] = -1.0
+            for c in sorted(ent):
+                col.append(c)
+                val.append(ent[c])
+            rowptr.append(len(col))
+    return np.array(rowptr, np.int32), np.array(col, np.int32), np.array(val, np.float64), n
+
+
+def device_system(rowptr, col, val, rhs, x0):
+    import torch
+    dev = torch.device("cuda:0")
+    return (torch.from_numpy(rowptr).to(dev), torch.from_numpy(col).to(dev),
+            torch.from_numpy(val).to(dev), torch.from_numpy(rhs).to(dev),
+            torch.from_numpy(x0).to(dev))
+
+
+@pytest.mark.gpu
+def test_static_solve_symmetric_cg_twice():
+    """symmetric != 0 takes the CG branch: a shifted 2D Laplacian solved
+    twice, against a direct FP64 solve, with no device memory taken."""
+    import torch
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as sla
+    rowptr, col, val, n = laplacian_csr(96, 80, 0.05)
+    rng = np.random.default_rng(11)
+    rhs = rng.uniform(-1, 1, n)
+    x_ref = sla.spsolve(sp.csr_matrix((val, col, rowptr), shape=(n, n)).tocsc(), rhs)
+    t_rowptr, t_col, t_val, t_rhs, t_x0 = device_system(rowptr, col, val, rhs, np.zeros(n, np.float32))
+    outs = [torch.full((n,), float("nan"), dtype=torch.float32, device="cuda:0") for _ in range(2)]
+    torch.cuda.synchronize()
+    f = solve_fn()
+    free = []
+    for x in outs:
+        it = C.c_int32(-1)
+        rc = f(n, len(col), t_rowptr.data_ptr(), t_col.data_ptr(), t_val.data_ptr(), t_rhs.data_ptr(),
+               t_x0.data_ptr(), x.data_ptr(), 1e-8, 1e-8, 1000, 1, None, C.byref(it))
+        assert rc == SHY_OK, last_error()
+        assert 0 < it.value <= 1000
+        free.append(torch.cuda.mem_get_info()[0])
+    for x in outs:
+        assert np.abs(x.cpu().numpy() - x_ref).max() <= 1e-5 * np.abs(x_ref).max()
+    assert torch.equal(outs[0], outs[1])
+    assert free[0] == free[1]
+
+
+@pytest.mark.gpu
+def test_static_solve_maxit_counts_the_whole_call():
+    """maxit bounds the iterations of all refinement rounds together; a budget
+    equal to the iterations an unbounded call took gives the same answer."""
+    import torch
+    rowptr, col, val, n = laplacian_csr(64, 64, 0.01)
+    rhs = np.random.default_rng(12).uniform(-1, 1, n)
+    t_rowptr, t_col, t_val, t_rhs, t_x0 = device_system(rowptr, col, val, rhs, np.zeros(n, np.float32))
+    f = solve_fn()
+
+    def run(maxit, sym):
+        x = torch.zeros(n, dtype=torch.float32, device="cuda:0")
+        it = C.c_int32(-1)
+        rc = f(n, len(col), t_rowptr.data_ptr(), t_col.data_ptr(), t_val.data_ptr(), t_rhs.data_ptr(),
+               t_x0.data_ptr(), x.data_ptr(), 1e-8, 1e-8, maxit, sym, None, C.byref(it))
+        return rc, it.value, x
+
+    for sym in (1, 0):
+        rc, k, x_full = run(1000, sym)
+        assert rc == SHY_OK, last_error()
+        rc, k2, x_k = run(k, sym)
+        assert rc == SHY_OK, last_error()
+        assert k2 == k and torch.equal(x_k, x_full)
+        rc, k3, _ = run(3, sym)
+        assert rc == SHY_ENOCONV and k3 == 3
+
+
+@pytest.mark.gpu
+def test_static_solve_refuses_inconsistent_csr():
+    """rowptr[n] must equal nnz and every column must lie in [0, n): the
+    kernel checks before it writes, so the scratch array is never overrun."""
+    import torch
+    rowptr, col, val, n = laplacian_csr(20, 20, 0.1)
+    rhs = np.ones(n)
+    t_rowptr, t_col, t_val, t_rhs, t_x0 = device_system(rowptr, col, val, rhs, np.zeros(n, np.float32))
+    f = solve_fn()
+    x = torch.full((n,), 7.0, dtype=torch.float32, device="cuda:0")
+    it = C.c_int32(-1)
+    rc = f(n, len(col) - 1, t_rowptr.data_ptr(), t_col.data_ptr(), t_val.data_ptr(), t_rhs.data_ptr(),
+           t_x0.data_ptr(), x.data_ptr(), 1e-8, 1e-8, 100, 1, None, C.byref(it))
+    assert rc == SHY_EARG and "rowptr[n] = nnz" in last_error()
+    bad_col = col.copy()
+    bad_col[5] = n
+    t_bad = torch.from_numpy(bad_col).to("cuda:0")
+    rc = f(n, len(col), t_rowptr.data_ptr(), t_bad.data_ptr(), t_val.data_ptr(), t_rhs.data_ptr(),
+           t_x0.data_ptr(), x.data_ptr(), 1e-8, 1e-8, 100, 1, None, C.byref(it))
+    assert rc == SHY_EARG
+    assert bool((x == 7.0).all())          # nothing written to the result
+    rc = f(n, len(col), t_rowptr.data_ptr(), t_col.data_ptr(), t_val.data_ptr(), t_rhs.data_ptr(),
+           t_x0.data_ptr(), x.data_ptr(), 1e-8, 1e-8, 1000, 1, None, C.byref(it))
+    assert rc == SHY_OK, last_error()      # the next good call works
