@@ -3,13 +3,16 @@
 
 Default workload at N=1 (the batched ensemble): 64 independent basins with
 node counts log-uniform in 5k..100k (2.1M nodes, 4.2M triangles in total),
-each a jittered triangle mesh with Gaussian-bump bathymetry 5..60 m and 10
-z-layers, uniform wind of 10 m/s plus a seeded per-basin perturbation of
-sigma 3 m/s, M2 0.5 m level boundary, dt = 60 s; seeded synthetic input of
+each made like the 2D tidal channel (100 m jittered triangle mesh at a
+seeded aspect ratio, depth 10 m +- 2 m, M2 0.5 m level boundary, quadratic
+friction) with 10 z-layers, and a uniform wind of 10 m/s plus a seeded
+per-basin perturbation of sigma 3 m/s, dt = 60 s; seeded synthetic input of
 that shape (no dataset ships with the reference).  All basins advance in
 one CUDA-graph step.  One bench "step" is one model time step (hydro, the
 body of shyfem_run's loop) of every basin.  Beside it the line reports the
-plain single-run form: the same basins advanced one model at a time.
+plain single-run form: the same basins advanced one model at a time, and
+the accuracy of the timed run: the first `--check-steps` steps of its
+smallest, median and largest basins against the FP64 oracle.
 
 `--workload basin3d` times the 3D baroclinic basin instead (~20k nodes, 20
 z-layers, temperature and salinity transported, dt = 120 s).
@@ -55,6 +58,8 @@ def parse():
                    help="serve workload: requests of the Poisson stream (20/min)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--check-steps", type=int, default=60,
+                   help="steps of the accuracy check against the oracle (0: none)")
     return p.parse_args()
 
 
@@ -69,8 +74,34 @@ def make_cases(workload, rank=0, first=None):
     return cases.ensemble_cases(64, seed=4 + 1000 * rank, first=first)
 
 
+def case_specs(workload, rank=0):
+    """The cases of make_cases as specs the oracle's worker processes build
+    themselves (name of the constructor in shygpu.cases, its arguments)."""
+    if workload == "basin3d":
+        return [("basin3d_case", dict(nkn_target=20000, seed=2 + 1000 * rank))]
+    if workload == "lagoon":
+        return [("lagoon_case", dict(nkn_target=250000, nlv=30, seed=7 + 1000 * rank))]
+    if workload == "ensemble":
+        return [("ensemble_cases", dict(n=64, seed=4 + 1000 * rank, only=[i])) for i in range(64)]
+    raise ValueError(workload)
+
+
+def check_members(workload, case_list):
+    """Indices of the basins the accuracy check compares: the smallest, the
+    median and the largest of the ensemble; the one basin otherwise."""
+    if len(case_list) == 1:
+        return [0]
+    order = np.argsort([c["nkn"] for c in case_list], kind="stable")
+    return sorted({int(order[0]), int(order[len(order) // 2]), int(order[-1])})
+
+
 def units_per_step(case_list):
     return sum(c["nkn"] * c["nlv"] for c in case_list)
+
+
+def active_units_per_step(case_list):
+    """Node-layers that hold water: the layers above each node's bottom."""
+    return sum(int(c["ilhkv"].sum()) for c in case_list)
 
 
 def reduce_over_ranks(x, world, op="max", device="cuda"):
@@ -92,22 +123,31 @@ def replica_throughput(units, steps, seconds, world, device="cuda"):
     return total / reduce_over_ranks(seconds, world, "max", device)
 
 
-def workload_config(workload, case_list, l2):
+L2_NOTE = "inputs larger than L2; the GPU arm also writes 256 MiB between timed steps"
+
+
+def workload_config(workload, case_list, world=1):
+    """The workload as both arms report it (the same dict for the same
+    cases)."""
+    act = {"active_node_layers": active_units_per_step(case_list),
+           "active_fraction": active_units_per_step(case_list) / units_per_step(case_list),
+           "l2": L2_NOTE, "parallelism": f"replicas{world}"}
     if workload == "lagoon":
         c = case_list[0]
-        return {"workload": "lagoon_sigma_tracers", "nkn": c["nkn"], "nel": c["nel"],
-                "nlv": c["nlv"], "layers": "sigma", "dt_s": c["params"]["dt"], "tracers": 3,
-                "forcing": "M2 0.5 m + S2 0.3 m", "l2": l2}
+        return dict({"workload": "lagoon_sigma_tracers", "nkn": c["nkn"], "nel": c["nel"],
+                     "nlv": c["nlv"], "layers": "sigma", "dt_s": c["params"]["dt"], "tracers": 3,
+                     "forcing": "M2 0.5 m + S2 0.3 m"}, **act)
     if workload == "basin3d":
         c = case_list[0]
-        return {"workload": "basin3d_baroclinic_ts", "nkn": c["nkn"], "nel": c["nel"],
-                "nlv": c["nlv"], "dt_s": c["params"]["dt"], "tracers": "T,S",
-                "forcing": "10 m/s wind, M2 0.3 m", "l2": l2}
-    return {"workload": "ensemble_64_basins_5k_100k_nodes", "basins": len(case_list),
-            "nkn_total": sum(c["nkn"] for c in case_list),
-            "nel_total": sum(c["nel"] for c in case_list), "nlv": case_list[0]["nlv"],
-            "dt_s": case_list[0]["params"]["dt"], "forcing": "10 +- 3 m/s wind, M2 0.5 m",
-            "l2": l2}
+        return dict({"workload": "basin3d_baroclinic_ts", "nkn": c["nkn"], "nel": c["nel"],
+                     "nlv": c["nlv"], "dt_s": c["params"]["dt"], "tracers": "T,S",
+                     "forcing": "10 m/s wind, M2 0.3 m"}, **act)
+    return dict({"workload": "ensemble_64_basins_5k_100k_nodes", "basins": len(case_list),
+                 "nkn_total": sum(c["nkn"] for c in case_list),
+                 "nel_total": sum(c["nel"] for c in case_list), "nlv": case_list[0]["nlv"],
+                 "depth_m": "10 +- 2", "layers": "z: 2 m surface layer, 1 m below",
+                 "dt_s": case_list[0]["params"]["dt"], "forcing": "10 +- 3 m/s wind, M2 0.5 m",
+                 "seed": 4}, **act)
 
 
 def plain_gpu(case_list, steps, lib):
@@ -206,6 +246,12 @@ def algorithmic_bytes(case_list, infos, nsc, cor=False):
               + max(i.refinements, 1) * (12 * 7 * c["nkn"] + 20 * c["nkn"])
               for c, i in zip(case_list, infos))
     b = {}
+    # the zeta solve counted as the survey of the path counts its compulsory
+    # traffic: assembly and right-hand side about 100 B per node, then per
+    # Krylov iteration about 80 B per node for CG (two vector streams of
+    # eight bytes, the matrix row, ~7 entries) or 150 B for BiCGStab
+    b_it = 150 if cor else 80
+    b["zeta_survey"] = sum(c["nkn"] * (100 + b_it * i.krylov_iters) for c, i in zip(case_list, infos))
     b["column"] = NL * (24 + (4 if cor else 0)) + nel * (12 + 32 + 16 + 8 + 48) + NK * 4 + NI * 4 + nkn * 12
     b["zeta"] = nel * (48 + 36 + 12) + nnz * (4 + 12 + 4) + nkn * (4 + 4 + 4 + 4 + 20) + kry
     b["final"] = NL * (24 + (4 if cor else 0)) + nel * (12 + 32 + 16 + 16 + 4 + 8 + 12) + nkn * 4
@@ -228,53 +274,85 @@ def load_peak():
 # ---------------------------------------------------------------------------
 # CPU baseline / reference arm: the oracle on host cores
 # ---------------------------------------------------------------------------
-def _oracle_worker(args):
-    workload, seed_rank, nsteps, warm = args
+def oracle_pool():
     sys.path.insert(0, str(ROOT / "oracle"))
-    sys.path.insert(0, str(ROOT / "shyfemcm-ismar_b200"))
-    import shyref
-    cl = make_cases(workload, seed_rank, first=2)
-    ms = [shyref.OracleModel(c) for c in cl]
-    for m in ms:
-        m.run(warm)
-    t0 = time.perf_counter()
-    for m in ms:
-        m.run(nsteps)
-    dt = time.perf_counter() - t0
-    return units_per_step(cl) * nsteps, dt
+    import oracle_pool as op
+    return op
 
 
-def cpu_baseline(workload, nproc, nsteps, warm=1):
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(nproc) as pool:
-        res = pool.map(_oracle_worker, [(workload, 10 + i, nsteps, warm) for i in range(nproc)])
-    wall = time.perf_counter() - t0
-    units = sum(r[0] for r in res)
-    tmax = max(r[1] for r in res)
-    return units / tmax, tmax, wall
+def cpu_timing(workload, case_list, nsteps, warm, nproc, rank=0):
+    """The oracle advancing the workload's own basins: each process takes a
+    share of the basins (largest first to the least loaded), advances them
+    `warm` untimed and `nsteps` timed steps; units over the slowest
+    process's time."""
+    op = oracle_pool()
+    specs = case_specs(workload, rank)
+    units, secs, used = op.time_steps(specs, [c["nkn"] * c["nlv"] for c in case_list], nsteps, warm, nproc)
+    return units / secs, secs, used
 
 
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
+    if a.workload == "serve":
+        print(json.dumps({"impl": "reference", "unavailable": "the serving workload has no CPU arm"}), flush=True)
+        return
     nproc = os.cpu_count() or 1
-    # each bench step: one time step of each of nproc independent replicas
+    # each bench step: one time step of every basin of the workload
     steps = max(1, a.steps if a.steps <= 40 else 20)
-    value, tmax, wall = cpu_baseline(a.workload, nproc, steps, warm=min(a.warmup, 2))
-    cl = make_cases(a.workload, first=2)
+    warm = min(max(a.warmup, 1), 2)
+    case_list = make_cases(a.workload, 0)
+    value, tmax, used = cpu_timing(a.workload, case_list, steps, warm, nproc)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC,
-            "n_gpus": a.gpus, "steps": steps, "warmup": min(a.warmup, 2),
+            "n_gpus": a.gpus, "steps": steps, "warmup": warm,
             "ms_per_step": 1000.0 * tmax / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(a.workload, cl, "n/a (CPU)"),
-            "cpu_baseline": {"value": value, "unit": METRIC, "cores": nproc, "kind": "port",
-                             "sample": f"{steps} steps of {nproc} independent replicas, one per core; "
-                                       "FP64 C++ restatement of the reference step (oracle/shyref.cpp)"},
+            "config": workload_config(a.workload, case_list, world),
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": used, "kind": "port",
+                             "host_cpu": host_cpu(),
+                             "sample": f"{steps} time steps of every basin of the workload (the GPU arm's "
+                                       f"basins), dealt over {used} processes, one per host core; FP64 C++ "
+                                       "restatement of the reference step (oracle/shyref.cpp, -O3)"},
             "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def host_cpu():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def accuracy(case_list, picks, gpu_states, gpu_volumes, oracle_results):
+    """Largest differences of the checked basins from the oracle: water
+    level [m], transports relative to the largest transport component, tracers
+    relative to theirs (None without tracers), volume relative."""
+    dz = du = dv = 0.0
+    dc = None
+    for i, sg, vg, o in zip(picks, gpu_states, gpu_volumes, oracle_results):
+        c, so = case_list[i], o["state"]
+        dz = max(dz, float(np.abs(sg["znv"] - so["znv"]).max()))
+        me = np.arange(c["nlv"])[None, :] < c["ilhv"][:, None]
+        umax = max(np.abs(so["utlnv"][me]).max(), np.abs(so["vtlnv"][me]).max(), 1e-30)
+        for f in ("utlnv", "vtlnv"):
+            du = max(du, float(np.abs(sg[f] - so[f])[me].max() / umax))
+        mk = np.arange(c["nlv"])[None, :] < c["ilhkv"][:, None]
+        p = c["params"]
+        fs = (["tempv"] if p["itemp"] else []) + (["saltv"] if p["isalt"] else []) + \
+             (["conzv"] if p["nconz"] > 0 else [])
+        for f in fs:
+            a, b = sg[f], so[f]
+            m = mk if a.ndim == 2 else np.broadcast_to(mk, a.shape)
+            r = float(np.abs(a - b)[m].max() / max(np.abs(b[m]).max(), 1e-30))
+            dc = r if dc is None else max(dc, r)
+        dv = max(dv, abs(vg - o["volume"]) / o["volume"])
+    return {"zeta_err_m": dz, "transport_rel_err": du, "tracer_rel_err": dc, "volume_rel_err": dv}
 
 
 # ---------------------------------------------------------------------------
@@ -425,10 +503,25 @@ def main():
     os.environ.setdefault("SHYGPU_NO_BUILD", "1")
     os.environ["CUDA_VISIBLE_DEVICES_HINT"] = str(local)
 
-    case_list = make_cases(a.workload, rank)
+    # The accuracy check of the timed run: the oracle advances the checked
+    # basins in spawned processes while the GPU runs (rank 0 only).
+    check_pool = None
+    if rank == 0 and a.check_steps > 0:
+        op = oracle_pool()
+        picks_spec = case_specs(a.workload, rank)
+        case_list = make_cases(a.workload, rank)
+        picks = check_members(a.workload, case_list)
+        check_pool = op.run_states([picks_spec[i] for i in picks], a.check_steps, wait=False)
+    else:
+        case_list = make_cases(a.workload, rank)
     model = shygpu.Model(case_list)
     model.set_state_all()
     stream = torch.cuda.ExternalStream(model.stream())
+    check_gpu = None
+    if check_pool is not None:
+        # the first steps of the timed run itself, read back before timing
+        model.run(a.check_steps)
+        check_gpu = ([model.get_state(i) for i in picks], [model.info(i).volume for i in picks])
     units = units_per_step(case_list)
     L2_FLUSH = 256 << 20
     flush = torch.empty(L2_FLUSH // 4, dtype=torch.float32, device="cuda")
@@ -465,6 +558,18 @@ def main():
     value = replica_throughput(units, a.steps, ms_total / 1000.0, world)
     ms_total = 1000.0 * reduce_over_ranks(ms_total / 1000.0, world, "max")
     ms_step = ms_total / a.steps
+
+    check = None
+    if check_pool is not None:
+        pl, res = check_pool
+        try:
+            results = res.get()
+        finally:
+            pl.close()
+            pl.join()
+        check = dict(accuracy(case_list, picks, check_gpu[0], check_gpu[1], results),
+                     steps=a.check_steps, basins=picks, nkn=[case_list[i]["nkn"] for i in picks],
+                     against="FP64 oracle (oracle/shyref.cpp), the same basins from the same initial state")
 
     # ---- end to end through the public API: forcing in from pinned host
     #      memory and the water level of every basin out, every step ----
@@ -529,7 +634,8 @@ def main():
     dom = max(prof, key=lambda k: prof[k][0])
     dom_ms, dom_n = prof[dom]
     peak, peak_kind = load_peak()
-    achieved = algo[dom] / (dom_ms / dom_n / 1000.0) / 1e9
+    dom_bytes = algo["zeta_survey"] if dom == "zeta" else algo[dom]
+    achieved = dom_bytes / (dom_ms / dom_n / 1000.0) / 1e9
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
@@ -547,9 +653,7 @@ def main():
         "steps": a.steps, "warmup": max(a.warmup, 3), "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": dict(workload_config(a.workload, case_list,
-                                       "flushed between timed steps (256 MiB write)"),
-                       parallelism=f"replicas{world}"),
+        "config": workload_config(a.workload, case_list, world),
         "gpu_launches": int(launches),
         "clocks": clocks,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": h2d,
@@ -561,7 +665,13 @@ def main():
                                       "every basin, waiting after each call"}},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                      "peak_source": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic},
+                     "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes,
+                     "bytes_model": ("zeta: 100 B per node for assembly + 80 B per node per CG "
+                                     "iteration, each basin with its own iteration count")
+                     if dom == "zeta" else "compulsory traffic of the kernel's arrays",
+                     "achieved_design_bytes": (algo["zeta"] / (dom_ms / dom_n / 1000.0) / 1e9)
+                     if dom == "zeta" else None},
+        "accuracy": check,
         "kernels": kernels,
         "solver": {"krylov_iters_last_step": infos[0].krylov_iters,
                    "refinements": infos[0].refinements, "resid": infos[0].resid},
@@ -573,13 +683,16 @@ def main():
                              "form": "one model per basin, basins advanced one after the other"}
         line["batched_over_plain"] = value / pv
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        nproc = 1
-        v, tmax, _ = cpu_baseline(a.workload, nproc, 20, warm=1)
-        what = ("the first 2 basins of an ensemble drawn by the same generator"
-                if a.workload == "ensemble" else "the same basin")
-        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": nproc, "kind": "port",
-                                "sample": f"20 time steps of {what}, FP64 C++ restatement "
-                                          "of the reference step (oracle/shyref.cpp), 1 thread"}
+        # a bounded sample: about 20 s of CPU work at the oracle's ~1.8e6
+        # node*layer*steps/s per core, over every basin of the workload
+        nproc = os.cpu_count() or 1
+        csteps = int(max(1, min(20, round(20 * 1.8e6 / units))))
+        v, tmax, used = cpu_timing(a.workload, case_list, csteps, 1, nproc)
+        line["cpu_baseline"] = {"value": v, "unit": METRIC, "cores": used, "kind": "port",
+                                "host_cpu": host_cpu(),
+                                "sample": f"{csteps} time steps of every basin of the timed workload, "
+                                          f"dealt over {used} processes, one per host core; FP64 C++ "
+                                          "restatement of the reference step (oracle/shyref.cpp, -O3)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     model.close()

@@ -16,6 +16,17 @@
 // is l (Dev::avol).  Only the horizontal fluxes (and horizontal diffusion)
 // need the loop over the incident elements.  Scalars with the same sub-step
 // count share that loop and one PCR solve of the vertical system.  FP32.
+//
+// Increment form.  The node layer's system M c' = M_old c + dt F(c) is
+// solved for the increment d = c' - c: every flux is evaluated on the
+// concentrations shifted by the node's own value (c_j - c), which gives the
+// same flux minus c times the flow (the schemes, upwind and superbee TVD, are
+// shift-equivariant), and c times the continuity residual of the node layer,
+// r = A (h_old - h_new) + dt (sum of flows), is added back.  In exact
+// arithmetic this is the conservative update of conz3d; in FP32 it rounds
+// relative to the increment instead of relative to the mass A h c, so a
+// uniform field stays uniform and the drift against the FP64 reference
+// stays at the rounding of the stored values.
 // Included by step.cu.
 #pragma once
 #include "common.cuh"
@@ -101,7 +112,7 @@ __device__ __forceinline__ float tvd_flux_own(int own, int itot, int isum, const
                                               const float (&cc)[3], const int (&kv)[3], float aj24,
                                               float u, float v, float dt, const float2 *g, int NLV,
                                               int lane, const Dev &d, int e, int itvd, const float *cs,
-                                              bool istmp) {
+                                              bool istmp, float csh) {
   if (itot < 1 || itot > 2) return 0.f;
   const int itot2 = itot - 1, itot1 = 2 - itot;
   const int ip = itot2 * (6 - isum) + itot1 * isum;          // 1-based
@@ -130,14 +141,15 @@ __device__ __forceinline__ float tvd_flux_own(int own, int itot, int isum, const
       grad = 2.f * (gc.x * dx + gc.y * dy);
     } else {
       // itvd 2: the value at the point beyond ic opposite id
-      // (tvd_get_upwind_c, tvd_admin.f90:608-671), cond where it has no layer
+      // (tvd_get_upwind_c, tvd_admin.f90:608-671), cond where it has no layer;
+      // shifted by csh like c3 (the interpolation weights sum to one)
       float conu = cond;
       const int4 t = d.tvdup[(size_t)e * 6 + 2 * (ic - 1) + ((id - ic + 3) % 3 - 1)];
       if (t.x >= 0 && lane < d.ilhv[t.x]) {
         const int4 tn = d.enode[t.x];
-        conu = __int_as_float(t.y) * clipc(cs[(size_t)tn.x * NLV + lane], istmp) +
-               __int_as_float(t.z) * clipc(cs[(size_t)tn.y * NLV + lane], istmp) +
-               __int_as_float(t.w) * clipc(cs[(size_t)tn.z * NLV + lane], istmp);
+        conu = __int_as_float(t.y) * (clipc(cs[(size_t)tn.x * NLV + lane], istmp) - csh) +
+               __int_as_float(t.z) * (clipc(cs[(size_t)tn.y * NLV + lane], istmp) - csh) +
+               __int_as_float(t.w) * (clipc(cs[(size_t)tn.z * NLV + lane], istmp) - csh);
       }
       grad = cond - conu;
     }
@@ -251,6 +263,9 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
       hs[r] = 0.f;
     }
     // horizontal fluxes: sum over the incident elements of aj4*(3*fl - hdif)
+    // on the shifted concentrations, and of aj4*3*fl for a unit field (the
+    // horizontal flow into the node layer)
+    float hs1 = 0.f;
     if (act) {
 #pragma unroll 4
       for (int p = pbeg; p < pend; p++) {
@@ -275,6 +290,9 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
         const float dfh = anyrk ? __ldg(&d.difhv[oe]) : 0.f;
         const int kja = ix.z, kjb = ix.w;
         const float fii = sel3(f3, ii);
+        // upwind flux of a unit field (the same for TVD on a divergence-free element)
+        const float fl1 = itot == 1 ? fii : (itot == 2 ? ((ii == 5 - isum) ? fii - (f3[0] + f3[1] + f3[2]) : fii) : 0.f);
+        hs1 += aj4 * 3.f * fl1;
         // horizontal TVD (concentration_omp.f90:675-686) where no vertex is
         // on an open boundary, with the element velocity of the new level
         const bool tvd = P.itvd >= 1 && !isbnd && d.kbnd[kja] <= 0 && d.kbnd[kjb] <= 0;
@@ -291,20 +309,19 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
         for (int r = 0; r < NR; r++) {
           if (sidx[r] < 0) continue;
           const float *cs = cin_base + sidx[r] * SN;
-          const float ca = clipc(__ldg(&cs[(size_t)kja * NLV + lane]), istmp[r]);
-          const float cb = clipc(__ldg(&cs[(size_t)kjb * NLV + lane]), istmp[r]);
-          // concentrations of vertices 0,1,2 (own value at ii, the others in order)
-          const float c3[3] = {ii == 0 ? cl[r] : ca, ii == 1 ? cl[r] : (ii == 0 ? ca : cb), ii == 2 ? cl[r] : cb};
+          const float ca = clipc(__ldg(&cs[(size_t)kja * NLV + lane]), istmp[r]) - cl[r];
+          const float cb = clipc(__ldg(&cs[(size_t)kjb * NLV + lane]), istmp[r]) - cl[r];
+          // shifted concentrations of vertices 0,1,2 (own value 0 at ii, the others in order)
+          const float c3[3] = {ii == 0 ? 0.f : ca, ii == 1 ? 0.f : (ii == 0 ? ca : cb), ii == 2 ? 0.f : cb};
           float fl;
           if (itot == 1) fl = fii * sel3(c3, isum - 1);
           else if (itot == 2) {
             // flux into the vertex with f >= 0 balances the two outflows
-            const float fc = fii * cl[r];
-            fl = (ii == 5 - isum) ? fc - (f3[0] * c3[0] + f3[1] * c3[1] + f3[2] * c3[2]) : fc;
+            fl = (ii == 5 - isum) ? -(f3[0] * c3[0] + f3[1] * c3[1] + f3[2] * c3[2]) : 0.f;
           } else fl = 0.f;
           if (tvd)
             fl = tvd_flux_own(ii, itot, isum, f3, c3, bb, cc, kv, 24.f * e1.z, ue, ve, dt,
-                              d.tgrad + sidx[r] * SN, NLV, lane, d, e, P.itvd, cs, istmp[r]);
+                              d.tgrad + sidx[r] * SN, NLV, lane, d, e, P.itvd, cs, istmp[r], cl[r]);
           float hdif = 0.f;
           if (rk[r] != 0.f) {
             float wdiff = 0.f;
@@ -326,52 +343,60 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
     const float clo = A * dt * clmm;
     const float chi = At * dt * clpp;
     const float cdg = A * (dt * clc_b + hnew) + At * dt * clc_x;
+    // continuity residual of the node layer: A (h_old - h_new) + dt (flow
+    // in); h_new - h_old = (hkn - hko) / istot, the difference exact in FP32
+    const float rcont = act ? -A * ((hkn - hko) / rstot) + dt * (hs1 - (A * w0 - At * wb)) : 0.f;
     float res[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) {
       const float c = cl[r];
+      const float cm = up_ok ? cm1[r] - c : 0.f, cp = dn_ok ? cp1[r] - c : 0.f;   // shifted
       float topw, botw;                               // interface fluxes times their element weights
       if (!tvdv) {
-        const float vtop = up_ok ? wt * (wt > 0.f ? c : cm1[r]) : 0.f;
-        const float vbot = wb * (wb > 0.f ? cp1[r] : c);
+        const float vtop = up_ok ? wt * (wt > 0.f ? 0.f : cm) : 0.f;
+        const float vbot = wb * (wb > 0.f ? cp : 0.f);
         topw = A * vtop;
         botw = At * vbot;
       } else {
-        const float cm2 = seg_up<S>(c, 2), cp2 = seg_down<S>(c, 2);
+        const float cm2r = seg_up<S>(c, 2), cp2r = seg_down<S>(c, 2);   // every lane shuffles
+        const float cm2 = (lane >= 2 ? cm2r : c) - c, cp2 = cp2r - c;
         topw = 0.f;
         if (up_ok) {
           const float alfa = dt * fabsf(wt) / (0.5f * (holdm + hold));
           if (wt > 0.f)
-            topw = wt * (At * tvd_v(c, cm1[r], cp1[r], alfa) + av.y * tvd_v(c, cm1[r], cm1[r], alfa));
+            topw = wt * (At * tvd_v(0.f, cm, cp, alfa) + av.y * tvd_v(0.f, cm, cm, alfa));
           else
-            topw = A * wt * tvd_v(cm1[r], c, lane >= 2 ? cm2 : c, alfa);
+            topw = A * wt * tvd_v(cm, 0.f, cm2, alfa);
         }
         botw = 0.f;
         if (dn_ok) {
           const float alfa = dt * fabsf(wb) / (0.5f * (hold + holdp));
           if (wb > 0.f)
-            botw = wb * (avn.x * tvd_v(cp1[r], c, cp2, alfa) + avn.y * tvd_v(cp1[r], c, c, alfa));
+            botw = wb * (avn.x * tvd_v(cp, 0.f, cp2, alfa) + avn.y * tvd_v(cp, 0.f, 0.f, alfa));
           else
-            botw = At * wb * tvd_v(c, cp1[r], up_ok ? cm1[r] : cp1[r], alfa);
+            botw = At * wb * tvd_v(0.f, cp, up_ok ? cm : cp, alfa);
         }
       }
       const float fw = aat * (topw - botw);
-      const float fd = adt * (At * (c - cp1[r]) * hmobot - A * (cm1[r] - c) * hmotop);
-      float q = hs[r] - fw - fd;
+      const float fd = adt * (-At * cp * hmobot - A * cm * hmotop);
+      const float fi = A * clmm * cm + At * clpp * cp;   // implicit vertical terms on the shifted values
+      float q = hs[r] - fw - fd - fi;
       if constexpr (EX)                               // nudging, summed over the elements
         if (act && d.cz_robs != 0.f) q += A * hold * (d.cz_robs * d.cz_tau[o] * (d.cz_obs[o] - c));
-      res[r] = A * hold * c + dt * q;
+      res[r] = act ? c * rcont + dt * q : 0.f;        // right-hand side of the increment
     }
     if constexpr (EX) {
-      // loading on the node layer's mass: a source adds dt*loading; a sink
-      // removes at most what an exponential decay over dt would, and the
-      // load is cut to what it removed
+      // loading on the node layer's mass M = A h_old c + dt q: a source adds
+      // dt*loading; a sink removes at most what an exponential decay over dt
+      // would, and the load is cut to what it removed
       if (act && valid && d.cz_rload != 0.f) {
+        const float c = cl[0];
+        const float mass = res[0] + (up_ok ? clo * cm1[0] : 0.f) + cdg * c + (dn_ok ? chi * cp1[0] : 0.f);
         float loading = d.cz_rload * d.cz_load[o];
         if (loading < 0.f) {
           float cload = 0.f;
-          if (res[0] > 0.f) cload = res[0] * (1.f - expf(dt * loading / res[0]));
-          else if (res[0] < 0.f) res[0] = 0.f;
+          if (mass > 0.f) cload = mass * (1.f - expf(dt * loading / mass));
+          else if (mass < 0.f) res[0] -= mass;
           loading = -cload / dt;
           if (d.cz_rload > 0.f) d.cz_load[o] = loading / d.cz_rload;
         }
@@ -392,7 +417,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
     for (int r = 0; r < NR; r++) {
       if (sidx[r] < 0) continue;
       const int s = sidx[r];
-      float cf = act ? res[r] : 0.f;
+      float cf = act ? cl[r] + res[r] : 0.f;         // old value plus increment
       if (act && isbnd && !d.conz_free_bnd) cf = d.cbnd[s * SN + o];      // bndo_impbc
       if (valid && lane < NLV) cout_base[s * SN + o] = cf;
     }

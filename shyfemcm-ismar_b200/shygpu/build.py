@@ -44,17 +44,20 @@ def stale():
 def build(verbose=False, force=False):
     if not force and not stale():
         return LIB
-    objs = []
+    objs, procs = [], []
     build_dir = PKG / "_build"
     build_dir.mkdir(exist_ok=True)
-    for src in SOURCES:
+    for src in SOURCES:          # the translation units compile concurrently
         obj = build_dir / (Path(src).stem + ".o")
         cmd = [nvcc(), *NVCC_FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             cmd += ["-Xptxas", "-v"]
             print(" ".join(cmd))
-        subprocess.check_call(cmd)
+        procs.append((cmd, subprocess.Popen(cmd)))
         objs.append(str(obj))
+    failed = [cmd for cmd, pr in procs if pr.wait() != 0]
+    if failed:
+        raise subprocess.CalledProcessError(1, failed[0])
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", str(tmp),
            "-lcudart"]

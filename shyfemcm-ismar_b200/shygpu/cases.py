@@ -312,20 +312,62 @@ def flat_case(nx=41, ny=9, lx=8.0e3, ly=1.6e3, seed=9, dt=60.0, nlv=1, ampli=1.0
     return _finish(case)
 
 
-def ensemble_cases(n, nkn_lo=5000, nkn_hi=100000, nlv=10, seed=4, dt=60.0, first=None):
-    """Independent basins with log-uniform node counts and seeded aspect
-    ratios and wind perturbations (sigma = 3 m/s).  `first` builds only the
-    first members of the same ensemble."""
+def ensemble_member_case(nkn_target, aspect, seed, wind, dt=60.0, nlv=10, spacing=100.0,
+                         ampli=0.5, depth=10.0, ddepth=2.0, top=2.0):
+    """One member of the batched ensemble, made as the 2D channel is: a
+    jittered triangle mesh of `spacing` (100 m) on a rectangle of the given
+    aspect ratio, each quad split on a seeded diagonal, depth 10 m plus a
+    seeded smooth perturbation of +-2 m, M2 of 0.5 m on the x = 0 boundary,
+    quadratic friction; then `nlv` z-layers (a `top` m surface layer, wide
+    enough for the tide and the wind set-down, 1 m layers below, the last
+    one reaching the bottom) and a uniform wind of speed `wind` along x."""
+    ny = max(3, int(round(math.sqrt(nkn_target / aspect))))
+    nx = max(3, int(round(nkn_target / ny)))
+    lx, ly = (nx - 1) * spacing, (ny - 1) * spacing
+    x, y, nen3v, ii, jj = structured_triangles(nx, ny, lx, ly, 0.2, seed)
+    rng = np.random.default_rng(seed + 101)
+    hk = depth + _smooth_field(x, y, rng, scale=ddepth)
+    nkn, nel = x.size, nen3v.shape[0]
+    hm3v = hk[nen3v - 1]
+    hlv, hldv = z_layers(np.r_[top, np.ones(nlv - 1)])
+    hlv[-1] = max(hlv[-1], hk.max() + 1.0)
+    hldv[-1] = hlv[-1] - hlv[-2]
+    ilhv, ilhkv = layer_counts(nen3v, hm3v, hlv, hldv, nkn)
+    bnd = np.zeros(nkn, np.int32)
+    bnd[ii == 0] = 1
+    tide = np.array([[[ampli, M2_PERIOD, 0.0, 0.0]]], np.float32)
+    rhoair, cd = 1.225, 2.5e-3
+    taux = rhoair / 1025.0 * cd * wind * abs(wind)
+    case = dict(name=f"member_{nkn}x{nlv}", nkn=nkn, nel=nel, nlv=nlv, nen3v=nen3v,
+                xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
+                bnd_index=bnd, tide=tide, seed=seed, params=dict(dt=dt),
+                tauxnv=np.full(nkn, taux, np.float32))
+    return _finish(case)
+
+
+def ensemble_cases(n, nkn_lo=5000, nkn_hi=100000, nlv=10, seed=4, dt=60.0, first=None, only=None):
+    """The batched ensemble: `n` independent basins with node counts
+    log-uniform in [nkn_lo, nkn_hi], each made like the 2D channel
+    (`ensemble_member_case`: 100 m jittered mesh, depth 10 +- 2 m, M2 0.5 m)
+    at a seeded aspect ratio in [2, 6], with 10 z-layers and a seeded wind
+    of 10 m/s plus a perturbation of sigma 3 m/s.  `first` builds only the
+    first members of the same ensemble, `only` the members of the given
+    indices (in that order)."""
+    draws = ensemble_draws(n, nkn_lo, nkn_hi, seed)
+    idx = list(range(n if first is None else min(first, n))) if only is None else list(only)
+    return [ensemble_member_case(draws[m][0], draws[m][1], seed * 1000 + m, draws[m][2], dt=dt, nlv=nlv)
+            for m in idx]
+
+
+def ensemble_draws(n, nkn_lo=5000, nkn_hi=100000, seed=4):
+    """The seeded (node count, aspect ratio, wind speed) of each member."""
     rng = np.random.default_rng(seed)
     out = []
-    for m in range(n if first is None else min(first, n)):
+    for _ in range(n):
         nk = int(math.exp(rng.uniform(math.log(nkn_lo), math.log(nkn_hi))))
         aspect = rng.uniform(2.0, 6.0)
-        ly = 2.0e3 * math.sqrt(nk / 793.0)
-        c = basin3d_case(nkn_target=nk, lx=aspect * ly, ly=ly, seed=seed * 1000 + m, dt=dt,
-                         nlv=nlv, ampli=0.5, wind=10.0 + 3.0 * rng.standard_normal(),
-                         baroclinic=False, ts=False)
-        out.append(c)
+        wind = 10.0 + 3.0 * rng.standard_normal()
+        out.append((nk, aspect, wind))
     return out
 
 
