@@ -70,7 +70,11 @@ typedef struct shy_basin {
   const float *difv;            /* (0:nlv,nkn) vertical diffusivity         */
   const float *tauxnv, *tauynv; /* (nkn) wind stress / rho0  (mod_meteo)    */
   const float *ppv;             /* (nkn) atmospheric pressure term          */
-  const float *rqv;             /* (nkn) flux boundary values (system_add_rhs) */
+  const float *rqv;             /* (nkn) discharge of flux boundaries and point */
+                                /*   sources [m^3/s]: the zeta right-hand side  */
+                                /*   (system_add_rhs) and, spread over the      */
+                                /*   node's layers by volume (set_mass_flux,    */
+                                /*   mfluxv), w and the transport               */
   const int32_t *bnd_index;     /* (nkn) 0 or the level-boundary number b>0 */
   int32_t nbnd, ntide;          /* level boundaries, constituents each      */
   const float *tide;            /* (4,ntide,nbnd): ampli, period, phase, zref
@@ -263,8 +267,11 @@ int shygpu_checkpoint_load(shygpu_model *model, const void *buf, int64_t nbytes)
  * in mass per second and, for a sink, takes at most an exponential decay
  * of the layer's mass over the sub-step, writing the load it took back
  * into load (conz3d_nodes :816-833).  An array whose factor is 0 is not
- * read.  co1 and cbound are not read (no boundary mass fluxes on this
- * path).  nlvddi and nlev must be the basin's nlv, azpar the model's.  The
+ * read.  cbound (nlvddi, nkn) is the concentration that inflows bring at
+ * nodes with a discharge (the basin's rqv, spread over the layers as
+ * mfluxv; :805-813); NULL lets them bring the node's own concentration.
+ * co1 is not read (the reference's scratch).  nlvddi and nlev must be the
+ * basin's nlv, azpar the model's.  The
  * first call (and the first with a source term) allocates the call's
  * device arrays.                                                          */
 int shygpu_conz3d(shygpu_model *model, int32_t ibasin, float *cn1, float *co1, double ddt,
@@ -283,6 +290,16 @@ int shygpu_conz3d(shygpu_model *model, int32_t ibasin, float *cn1, float *co1, d
  * The first call for a model allocates the array and rebuilds its step
  * graph.                                                                   */
 int shygpu_set_nudging(shygpu_model *model, int32_t ibasin, const float *andgzv);
+
+/* Boundary values of one scalar of basin ib, (nlv, nkn), as the reference's
+ * boundary input of that scalar (r3v of make_scal_flux, bnd_routines.f90:
+ * 1215-1300): imposed on the level-boundary nodes after every transport
+ * sub-step (bndo_impbc) and brought in by the inflows at nodes with a
+ * discharge (conz3d_nodes, concentration_omp.f90:805-813).  what: 0
+ * temperature, 1 salinity, 2 passive tracer itr.  shygpu_set_state sets
+ * them to the scalar's initial columns; call this after it.              */
+int shygpu_set_bound_scalar(shygpu_model *model, int32_t ibasin, int32_t what,
+                            int32_t itr, const float *values);
 
 /* Tuning options by name: "use_graph" (CUDA-graph replay of whole steps,
  * the transport sub-step loop as a device-driven conditional node; default

@@ -439,7 +439,9 @@ struct Model {
   std::vector<double> utlnv, vtlnv, utlov, vtlov, unv, vnv;
   std::vector<double> hdknv, hdkov, hdenv, hdeov, wlnv;
   std::vector<double> tempv, saltv, rhov, conzv;
-  std::vector<double> tbnd, sbnd, cbnd;     // scalar values imposed on level boundaries
+  std::vector<double> tbnd, sbnd, cbnd;     // scalar boundary values: imposed on level
+                                            // boundaries, brought in by inflows
+  std::vector<double> mfluxv;               // (nkn, nlv) discharge per node layer (set_mass_flux)
   std::vector<double> rfricv, fxv, fyv, ddxv, ddyv;
   std::vector<double> c2coo, rvec2d;
   double dtime = 0.;
@@ -1058,7 +1060,37 @@ void hydro_transports_final(Model &m) {
   }
 }
 
-// hydro_vertical (hydrodynamic.f90:1582-1781); mfluxv = 0 (no flux boundaries)
+// set_mass_flux (bnd_routines.f90:1035-1140) for nodes with a discharge
+// rqv [m^3/s]: mfluxv(l,k) = rqv(k) times the layer's share of the node's
+// volume at the start of the step (volnode(l,k,+1) when set_mass_flux runs,
+// before hydro: the old thickness), over all the node's layers (the levmin
+// and levmax of a boundary default to them); rqv itself stays the vertical
+// sum.  Distributed sources (rain, rqdsv) are not part of this path.
+void set_mass_flux(Model &m) {
+  const int nlv = m.nlv;
+  m.mfluxv.assign((size_t)nlv * m.nkn, 0.);
+  for (int k = 0; k < m.nkn; k++) {
+    if (m.rqv[k] == 0.) continue;
+    const int lmax = m.ilhkv[k];
+    double vtot = 0.;
+    for (int l = 1; l <= lmax; l++) vtot += m.hdkov[(size_t)k * nlv + l - 1] * m.areakv[(size_t)k * nlv + l - 1];
+    if (!(vtot > 0.)) continue;
+    for (int l = 1; l <= lmax; l++)
+      m.mfluxv[(size_t)k * nlv + l - 1] =
+          m.rqv[k] * (m.hdkov[(size_t)k * nlv + l - 1] * m.areakv[(size_t)k * nlv + l - 1] / vtot);
+  }
+}
+
+// adjust_mass_flux (bnd_routines.f90:1185-1210): no discharge at nodes out
+// of the wet system
+void adjust_mass_flux(Model &m) {
+  for (int k = 0; k < m.nkn; k++)
+    if (m.inodv[k] == -2)
+      for (int l = 0; l < m.nlv; l++) m.mfluxv[(size_t)k * m.nlv + l] = 0.;
+}
+
+// hydro_vertical (hydrodynamic.f90:1582-1781), with the discharge mfluxv of
+// each node layer (:1727)
 void hydro_vertical(Model &m) {
   int nlv = m.nlv;
   m.wlnv.assign((size_t)(nlv + 1) * m.nkn, 0.);
@@ -1087,7 +1119,7 @@ void hydro_vertical(Model &m) {
       double voln = m.hdknv[(size_t)k * nlv + l - 1] * m.areakv[(size_t)k * nlv + l - 1];
       double volo = m.hdkov[(size_t)k * nlv + l - 1] * m.areakv[(size_t)k * nlv + l - 1];
       double dvdt = (voln - volo) / dt;
-      double q = 0.;
+      double q = m.mfluxv[(size_t)k * nlv + l - 1];
       double wdiv = vf[(size_t)k * nlv + l - 1] + q;
       W(l - 1, k) = W(l, k) + wdiv - dvdt;
     }
@@ -1114,14 +1146,17 @@ double masscont(Model &m) {
   return total;
 }
 
-// conzstab (concentration.f90:1573-2080) without point sources, settling
-// and nudging from tm (or none): the transport stability index with ddt = 1.
+// conzstab (concentration.f90:1573-2080): the transport stability index with
+// ddt = 1, with the inflow of point sources (mfluxv > 0, :1801) and settling
+// and nudging from tm (or none).
 double conzstab(Model &m, double rkpar, const Model::ScalarTerms *tm = nullptr) {
   int nlv = m.nlv;
   double az = m.p.azpar, azt = 1. - az, ad = m.p.adpar, adt = 1. - ad, aa = m.p.aapar, aat = 1. - aa;
   const double dt = 1.;      // ddt = 1, istot = isact = 1 -> rso = 0, rsn = 1
   std::vector<double> cn((size_t)nlv * m.nkn, 0.), cdiag(cn.size(), 0.), clow(cn.size(), 0.),
       chigh(cn.size(), 0.), co(cn.size(), 0.);
+  for (size_t q = 0; q < co.size(); q++)
+    if (m.mfluxv[q] > 0.) co[q] = m.mfluxv[q];   // point sources
   for (int ie = 0; ie < m.nel; ie++) {
     const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
     int kn[3];
@@ -1336,11 +1371,13 @@ void tvd_fluxes(const Model &m, int ie, int l, int itot, int isum, double dt, co
 // conz3d_omp (concentration_omp.f90:65-350) with conz3d_element (:355-755),
 // vertical_flux_ie (tvd_admin.f90:930-1019, itvdv 0 or 1) and
 // conz3d_nodes (:757-888); itvd 0 or 1 (gx, gy: the node gradients of
-// tvd_grad_3d); cbound unused because mfluxv = 0.  tm (or null) carries the
-// nudging, settling and loading terms; its load is updated where deposition
-// takes less than asked (conz3d_nodes :819-829).
+// tvd_grad_3d).  cbound (nkn, nlv) is the concentration inflows bring at
+// nodes with a discharge (mfluxv).  tm (or null) carries the nudging,
+// settling and loading terms; its load is updated where deposition takes
+// less than asked (conz3d_nodes :819-829).
 void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int istot, int isact,
-            const std::vector<double> &gx, const std::vector<double> &gy, Model::ScalarTerms *tm = nullptr) {
+            const std::vector<double> &gx, const std::vector<double> &gy, const std::vector<double> &cbound,
+            Model::ScalarTerms *tm = nullptr) {
   int nlv = m.nlv;
   double az = m.p.azpar, ad = m.p.adpar, aa = m.p.aapar;
   double azt = 1. - az, adt = 1. - ad, aat = 1. - aa;
@@ -1480,6 +1517,15 @@ void conz3d(Model &m, std::vector<double> &cn1, double ddt, double rkpar, int is
     int ilevel = m.ilhkv[k], jlevel = 1;
     double *cnk = &cn[(size_t)k * nlv];
     double *cd = &cdiag[(size_t)k * nlv], *clo = &clow[(size_t)k * nlv], *chi = &chigh[(size_t)k * nlv];
+    // boundary mass flux (:805-813): an inflow brings cbound, an outflow at
+    // a boundary node the node's own concentration
+    if (m.rqv[k] != 0.)
+      for (int l = jlevel; l <= ilevel; l++) {
+        const size_t q = (size_t)k * nlv + l - 1;
+        const double qflux = m.mfluxv[q];
+        const double cconz = qflux < 0. ? cn1[q] : cbound[q];
+        cnk[l - 1] += dt * qflux * cconz;
+      }
     // loading (:816-833) on the assembled mass: a source adds dt*loading; a
     // sink removes at most what an exponential decay over dt leaves, and the
     // load is cut to what was taken.  cload <= cn holds by construction, so
@@ -1539,7 +1585,7 @@ int scal3sh(Model &m, std::vector<double> &cnv, double rkpar, bool is_temp,
     if (!is_temp)
       for (auto &v : cnv) if (v < 1.e-15) v = 0.;
     if (m.p.itvd == 1) tvd_grad_3d(m, cnv, gx, gy);        // (concentration.f90:744)
-    conz3d(m, cnv, m.p.dt, rkpar, istot, isact, gx, gy, tm);
+    conz3d(m, cnv, m.p.dt, rkpar, istot, isact, gx, gy, rbc, tm);
     bndo_impbc(m, cnv, rbc);
   }
   return SHY_OK;
@@ -1830,6 +1876,7 @@ int step(Model &m) {
   m.uov = m.unv; m.vov = m.vnv;
   m.hdkov = m.hdknv; m.hdeov = m.hdenv;
   set_rzv(m);                                     // sp111(2)
+  set_mass_flux(m);
   // hydro (hydrodynamic.f90:284-485)
   int st = bottom_friction(m);
   if (st) return st;
@@ -1853,6 +1900,7 @@ int step(Model &m) {
     if (!m.p.wetdry || setweg(m, 1, m.dtime) == 0) break;
   }
   m.info.krylov_iters = krylov;
+  if (m.p.wetdry) adjust_mass_flux(m);            // after the last setnod of the loop (:384)
   hydro_transports_final(m);
   for (int ie = 0; ie < m.nel; ie++)              // setzev: elements in the system
     if (!m.p.wetdry || m.iwegv[ie] == 0)
@@ -1999,6 +2047,7 @@ void *shyref_create(const shy_basin *B, const shy_params *P) {
   m->visv = dv(B->visv, (size_t)(nlv + 1) * nkn); m->difv = dv(B->difv, (size_t)(nlv + 1) * nkn);
   m->tauxnv = dv(B->tauxnv, nkn); m->tauynv = dv(B->tauynv, nkn);
   m->ppv = dv(B->ppv, nkn); m->rqv = dv(B->rqv, nkn);
+  m->mfluxv.assign((size_t)nkn * B->nlv, 0.);
   m->bnd.assign(nkn, 0);
   if (B->bnd_index) m->bnd.assign(B->bnd_index, B->bnd_index + nkn);
   m->nbnd = B->nbnd; m->ntide = B->ntide;
@@ -2092,6 +2141,22 @@ int shyref_set_scalar_terms(void *h, int itr, const float *cobs, float robs, con
     if (rload != 0.f) t.load.assign(load, load + n);
   }
   m.sterm = std::move(t);
+  return SHY_OK;
+}
+
+// boundary values of a scalar (what 0 temperature, 1 salinity, 2 tracer
+// itr), (nkn, nlv): imposed on level boundaries after each sub-step and
+// brought in by inflows (make_scal_flux's r3v, bnd_routines.f90:1215-1300)
+int shyref_set_bound_scalar(void *h, int what, int itr, const float *values) {
+  Model &m = *(Model *)h;
+  const size_t n = (size_t)m.nkn * m.nlv;
+  std::vector<double> *dst = nullptr;
+  size_t off = 0;
+  if (what == 0 && m.p.itemp) dst = &m.tbnd;
+  else if (what == 1 && m.p.isalt) dst = &m.sbnd;
+  else if (what == 2 && itr >= 0 && itr < m.p.nconz) { dst = &m.cbnd; off = (size_t)itr * n; }
+  if (!dst || !values) return fail(SHY_EARG, "set_bound_scalar: no such scalar");
+  for (size_t q = 0; q < n; q++) (*dst)[off + q] = values[q];
   return SHY_OK;
 }
 

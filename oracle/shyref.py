@@ -43,6 +43,7 @@ def _lib():
     lib.shyref_set_scalar_terms.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_float, C.c_void_p,
                                             C.c_float, C.c_void_p, C.c_float, C.c_void_p]
     lib.shyref_get_load.argtypes = [C.c_void_p, d_p]
+    lib.shyref_set_bound_scalar.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
     lib.shyref_step_info.argtypes = [C.c_void_p, C.POINTER(abi.ShyStepInfo)]
     lib.shyref_get_state64.argtypes = [C.c_void_p] + [d_p] * 11
     lib.shyref_last_system.argtypes = [C.c_void_p, i_p, d_p, d_p]
@@ -198,6 +199,14 @@ class OracleModel:
         p = [None if a is None else a.ctypes.data for a in arrs]
         check(lib.shyref_set_scalar_terms(self.h, itr, p[0], robs, p[1], wsink, p[2], rload, p[3]),
               "set_scalar_terms")
+
+    def set_bound_scalar(self, what, values, itr=0):
+        """Boundary values (nkn, nlv) of a scalar (what: 0 temperature, 1
+        salinity, 2 tracer itr): imposed on level boundaries, brought in by
+        inflows."""
+        a = np.ascontiguousarray(values, np.float32)
+        self._bound = a
+        check(lib.shyref_set_bound_scalar(self.h, int(what), int(itr), a.ctypes.data), "set_bound_scalar")
 
     def load(self):
         """The loading array after deposition has cut it, (nkn, nlv)."""

@@ -195,6 +195,24 @@ __device__ __forceinline__ float seg_max(float v) {
   for (int d = S / 2; d > 0; d >>= 1) v = fmaxf(v, __shfl_xor_sync(seg_mask<S>(), v, d, S));
   return v;
 }
+// set_mass_flux (bnd_routines.f90:1035-1140): the discharge rqv of node k
+// [m^3/s] spread over its layers by their volumes at the start of the step
+// (volnode(l,k,+1) when set_mass_flux runs, before hydro, is the old
+// thickness here) in FP32 like the reference's real volnode, the fractions in
+// FP64; zero where the node is out of the system (adjust_mass_flux).  One
+// lane per layer; `rq` is uniform over the segment, so the sum is taken by
+// every lane of a segment together or by none.
+template <int S, typename DevT>
+__device__ __forceinline__ float mflux_layer(const DevT &d, int k, bool act, size_t o, bool wetdry) {
+  const float rq = d.rqv[k];
+  if (rq == 0.f || (wetdry && d.inod[k] == -2)) return 0.f;
+  const float vol = act ? d.hko[o] * d.areakv[o] : 0.f;
+  double tot = (double)vol;
+#pragma unroll
+  for (int dd = S / 2; dd > 0; dd >>= 1) tot += __shfl_xor_sync(seg_mask<S>(), tot, dd, S);
+  return (act && tot > 0.) ? (float)((double)rq * ((double)vol / tot)) : 0.f;
+}
+
 // inclusive prefix sum from the top (lane 0) down
 template <int S, typename T>
 __device__ __forceinline__ T seg_scan_down(T v, int lane) {

@@ -281,6 +281,7 @@ struct shygpu_model {
   // its source terms (made on the first call that has one): observations,
   // relaxation rates, loads, settling velocities
   float *cz_obs = nullptr, *cz_tau = nullptr, *cz_load = nullptr, *cz_wsv = nullptr;
+  float *cz_cb = nullptr;         // conz3d's cbound for the inflows
   BasinPar *cz_par = nullptr;
   BasinOut *cz_outp = nullptr;
   cudaStream_t stream = nullptr;
@@ -1500,15 +1501,18 @@ extern "C" int shygpu_scalar(shygpu_model *m) {
 // the open-boundary values are left to the caller's scal3sh loop
 // (bndo_setbc).  Scalar nudging (cobs, robs, rtauv), settling (wsink,
 // wsinkv) and loading (rload, load) run in the kernel's source-term
-// instance; load is written back where deposition cut it.  cbound and co1
-// are not needed (no boundary mass fluxes; co1 is the reference's scratch).
+// instance; load is written back where deposition cut it.  cbound (nlvddi,
+// nkn) is the concentration that inflows at nodes with a discharge (the
+// basin's rqv, spread over the layers as mfluxv) bring in (:805-813); NULL
+// lets them bring the node's own concentration.  co1 is the reference's
+// scratch and is not needed.
 extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1, double ddt, float rkpar,
                              const float *difhv, const float *difv, float difmol, const float *cbound,
                              int32_t itvd, int32_t itvdv, const float *gradxv, const float *gradyv,
                              const float *cobs, float robs, const float *rtauv, float wsink, const float *wsinkv,
                              float rload, float *load, float azpar, float adpar, float aapar,
                              int32_t istot, int32_t isact, int32_t nlvddi, int32_t nlev) {
-  (void)co1; (void)cbound;
+  (void)co1;
   if (!m || ib < 0 || ib >= m->nbasin || !cn1 || !difhv || !difv) return fail(SHY_EARG, "conz3d: bad arguments");
   if (!m->state_set) return fail(SHY_ESTATE, "conz3d: set_state has not been called");
   const BasinPar &bp = m->par[ib];
@@ -1530,7 +1534,8 @@ extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1
     Arena &A = m->arena;
     if (A.alloc(&m->cz_in, SN) || A.alloc(&m->cz_out, SN) || A.alloc(&m->cz_difhv, (size_t)m->NEL * NLV) ||
         A.alloc(&m->cz_difv, (size_t)m->NKN * (NLV + 1)) || A.alloc(&m->cz_grad, SN) ||
-        A.alloc(&m->cz_par, (size_t)m->nbasin) || A.alloc(&m->cz_outp, (size_t)m->nbasin))
+        A.alloc(&m->cz_par, (size_t)m->nbasin) || A.alloc(&m->cz_outp, (size_t)m->nbasin) ||
+        A.alloc(&m->cz_cb, SN))
       return SHY_ECAPACITY;
   }
   if (terms && !m->cz_obs) {
@@ -1553,6 +1558,7 @@ extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1
   CUDA_TRY(cudaMemcpyAsync(m->cz_par, par.data(), sizeof(BasinPar) * m->nbasin, cudaMemcpyHostToDevice, st));
   CUDA_TRY(cudaMemcpyAsync(m->cz_outp, out.data(), sizeof(BasinOut) * m->nbasin, cudaMemcpyHostToDevice, st));
   ST_TRY(copy_cols(m->cz_in, cn1, bp.nk, nlv, NLV, bp.k0, true, st));
+  if (cbound) ST_TRY(copy_cols(m->cz_cb, cbound, bp.nk, nlv, NLV, bp.k0, true, st));
   ST_TRY(copy_cols(m->cz_difhv, difhv, bp.ne, nlv, NLV, bp.e0, true, st));
   ST_TRY(copy_cols(m->cz_difv, difv, bp.nk, nlv + 1, NLV + 1, bp.k0, true, st));
   if (itvd == 1) {
@@ -1566,6 +1572,7 @@ extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1
   d.par = m->cz_par; d.out = m->cz_outp;
   d.difhv = m->cz_difhv; d.difv = m->cz_difv; d.tgrad = m->cz_grad;
   d.nsc_max = 1; d.conz_free_bnd = 1;
+  d.cbnd = cbound ? m->cz_cb : m->cz_in;   // inflow concentration: cbound, or the node's own
   if (robs != 0.f) {
     ST_TRY(copy_cols(m->cz_obs, cobs, bp.nk, nlv, NLV, bp.k0, true, st));
     ST_TRY(copy_cols(m->cz_tau, rtauv, bp.nk, nlv, NLV, bp.k0, true, st));
@@ -1898,6 +1905,27 @@ extern "C" int shygpu_set_nudging(shygpu_model *m, int32_t ib, const float *andg
     drop_graphs(m);
   }
   CUDA_TRY(cudaMemcpyAsync(m->base.andg + bp.k0, andgzv, (size_t)bp.nk * 4, cudaMemcpyHostToDevice, m->stream));
+  return SHY_OK;
+}
+
+// The boundary values of one scalar of basin ib, (nlv, nkn) as the
+// reference's boundary input of that scalar (r3v of make_scal_flux,
+// bnd_routines.f90:1215-1300): imposed on level-boundary nodes after every
+// transport sub-step (bndo_impbc), and brought in by the inflows at nodes
+// with a discharge (conz3d_nodes, concentration_omp.f90:805-813).  what: 0
+// temperature, 1 salinity, 2 tracer itr.  shygpu_set_state sets them to the
+// initial columns; call this after it.
+extern "C" int shygpu_set_bound_scalar(shygpu_model *m, int32_t ib, int32_t what, int32_t itr,
+                                       const float *values) {
+  if (!m || ib < 0 || ib >= m->nbasin || !values || what < 0 || what > 2)
+    return fail(SHY_EARG, "set_bound_scalar: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  if (what == 2 && (itr < 0 || itr >= bp.nsc - bp.itemp - bp.isalt))
+    return fail(SHY_EARG, "set_bound_scalar: basin %d has no tracer %d", ib, itr);
+  const int sc = scalar_index(bp, what, itr);
+  if (sc < 0) return fail(SHY_EARG, "set_bound_scalar: basin %d does not transport scalar %d", ib, what);
+  const size_t SN = (size_t)m->NKN * m->NLV;
+  ST_TRY(copy_cols(m->base.cbnd + sc * SN, values, bp.nk, bp.nlv, m->NLV, bp.k0, true, m->stream));
   return SHY_OK;
 }
 

@@ -219,6 +219,8 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
   float2 avn = make_float2(0.f, 0.f);
   if (tvdv) { avn.x = seg_down<S>(av.x, 1); avn.y = seg_down<S>(av.y, 1); }
   const bool isbnd = d.kbnd[k] > 0;
+  // the node layer's share of the node's discharge (mfluxv, set_mass_flux)
+  const float qf = mflux_layer<S>(d, k, act, o, P.wetdry != 0);
   const int pbeg = d.inc_ptr[k], pend = d.inc_ptr[k + 1];
   const bool up_ok = lane > 0, dn_ok = lane + 1 < lmax;
   while (todo) {
@@ -345,7 +347,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
     const float cdg = A * (dt * clc_b + hnew) + At * dt * clc_x;
     // continuity residual of the node layer: A (h_old - h_new) + dt (flow
     // in); h_new - h_old = (hkn - hko) / istot, the difference exact in FP32
-    const float rcont = act ? -A * ((hkn - hko) / rstot) + dt * (hs1 - (A * w0 - At * wb)) : 0.f;
+    const float rcont = act ? -A * ((hkn - hko) / rstot) + dt * (hs1 + qf - (A * w0 - At * wb)) : 0.f;
     float res[NR];
 #pragma unroll
     for (int r = 0; r < NR; r++) {
@@ -381,6 +383,12 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
       const float fd = adt * (-At * cp * hmobot - A * cm * hmotop);
       const float fi = A * clmm * cm + At * clpp * cp;   // implicit vertical terms on the shifted values
       float q = hs[r] - fw - fd - fi;
+      // boundary mass flux (conz3d_nodes :805-813): an inflow brings the
+      // boundary concentration, an outflow takes the node's own (no change)
+      if (qf > 0.f && sidx[r] >= 0) {
+        const float cb = d.cbnd[sidx[r] * SN + o];
+        q += qf * (cb - c);
+      }
       if constexpr (EX)                               // nudging, summed over the elements
         if (act && d.cz_robs != 0.f) q += A * hold * (d.cz_robs * d.cz_tau[o] * (d.cz_obs[o] - c));
       res[r] = act ? c * rcont + dt * q : 0.f;        // right-hand side of the increment

@@ -64,12 +64,14 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   vol = seg_sum<S>(vol);
   if (lane == 0 && valid) d.vol_node[k] = vol;
   if (init_only) return;
-  // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771)
+  // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771),
+  // with the layer's share of the node's discharge (mfluxv, :1727)
   const int I = NLV + 1;
+  const float q = mflux_layer<S>(d, k, act, o, P.wetdry != 0);
   double dv = 0.;
   if (act && P.nlv > 1) {
     double voln = (double)(hkf * (float)area), volo = (double)(d.hko[o] * (float)area);
-    dv = vf - (voln - volo) / P.dt;
+    dv = vf + (double)q - (voln - volo) / P.dt;
   }
   double wtop = seg_scan_up<S>(dv, lane);      // flux through the top interface of layer lane
   if (lane == 0) wtop = 0.;                     // wlnv(lmin-1) = 0
@@ -155,8 +157,14 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
   if (bad) set_status(&d.out[b], SHY_EDEPTH);
   d.vol_node[k] = vol;
   if (init_only) return;
-  // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771)
+  // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771),
+  // with each layer's share of the node's discharge (set_mass_flux: by the
+  // layers' volumes at the start of the step; mfluxv, :1727)
   const bool wzero = P.nlv == 1 || d.kbnd[k] > 0;
+  const float rq = (P.wetdry && d.inod[k] == -2) ? 0.f : d.rqv[k];
+  double vtot = 0.;
+  if (rq != 0.f)
+    for (int l = 0; l < lmax; l++) vtot += (double)(d.hko[o + l] * d.areakv[o + l]);
   double acc = 0.;                             // flux through the top of layer l
 #pragma unroll
   for (int l = L - 1; l >= 0; l--) {
@@ -166,7 +174,8 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
     if (act && P.nlv > 1) {
       const double voln = (double)(hkf[l] * (float)area[l]);
       const double volo = (double)(d.hko[o + l] * (float)area[l]);
-      dv = (double)vf[l] - (voln - volo) / P.dt;
+      const float q = vtot > 0. ? (float)((double)rq * ((double)(d.hko[o + l] * d.areakv[o + l]) / vtot)) : 0.f;
+      dv = (double)vf[l] + (double)q - (voln - volo) / P.dt;
     }
     acc += dv;
     double wtop = acc;
@@ -255,6 +264,8 @@ __global__ void __launch_bounds__(256) k_stab(Dev d, const int *kbas) {
   const double hold = act ? (double)d.hko[o] : 0., hnew = act ? (double)d.hkn[o] : 0.;
   const double rvptop = act ? (double)d.difv[(size_t)k * I + lane] + P.difmol : 0.;
   const double rvpbot = act ? (double)d.difv[(size_t)k * I + lane + 1] + P.difmol : 0.;
+  // point sources: the inflow of the node layer (conzstab co, concentration.f90:1801)
+  const float qin = fmaxf(mflux_layer<S>(d, k, act, o, P.wetdry != 0), 0.f);
   float rk_prev = -1.f;
   float stab = 0.f;
   for (int s = 0; s < P.nsc; s++) {
@@ -298,7 +309,7 @@ __global__ void __launch_bounds__(256) k_stab(Dev d, const int *kbas) {
           cdiag += aj4 * fmin(hold, hnew);
         }
       }
-      double r = (act && cdiag > 0.) ? (chigh + clow + cn) / cdiag : 0.;
+      double r = (act && cdiag > 0.) ? (chigh + clow + cn + (double)qin) / cdiag : 0.;
       stab = seg_max<S>((float)r);
     }
     if (lane == 0 && valid && d.kbnd[k] == 0) atomic_max_pos(&d.out[b].stab[s], stab);

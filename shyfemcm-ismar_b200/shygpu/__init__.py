@@ -75,6 +75,7 @@ def lib():
     L.shygpu_step_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyStepInfo)]
     L.shygpu_get_wetdry.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3
     L.shygpu_set_nudging.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.shygpu_set_bound_scalar.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
     L.shygpu_conz3d.argtypes = ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_float,
                                  C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int32, C.c_int32,
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_float,
@@ -224,20 +225,34 @@ class Model:
         check(lib().shygpu_set_nudging(self.h, ib, a.ctypes.data), "set_nudging")
         lib().shygpu_sync(self.h)
 
+    def set_bound_scalar(self, ib, what, values, itr=0):
+        """Boundary values (nkn, nlv) of a scalar of basin ib (what: 0
+        temperature, 1 salinity, 2 tracer itr): imposed on level boundaries
+        and brought in by inflows.  Call after set_state."""
+        a = np.ascontiguousarray(values, np.float32)
+        c = self.cases[ib]
+        if a.shape != (c["nkn"], c["nlv"]):
+            raise ValueError(f"set_bound_scalar: values must have shape {(c['nkn'], c['nlv'])}")
+        check(lib().shygpu_set_bound_scalar(self.h, ib, int(what), int(itr), a.ctypes.data), "set_bound_scalar")
+        lib().shygpu_sync(self.h)
+
     def conz3d(self, ib, cn1, ddt, rkpar, difhv, difv, difmol, azpar, adpar, aapar, istot, isact,
                itvd=0, itvdv=0, gradxv=None, gradyv=None, cobs=None, robs=0.0, rtauv=None,
-               wsink=0.0, wsinkv=None, rload=0.0, load=None):
+               wsink=0.0, wsinkv=None, rload=0.0, load=None, cbound=None):
         """conz3d_omp (concentration_omp.f90:65-76): one transport sub-step
         (isact of istot) of one scalar of basin ib on the state hydro() made.
         cn1 is overwritten with the new concentration, and load where
         deposition took less than asked.  Arrays are C-contiguous float32 of
         shape (nkn, nlv), but difhv (nel, nlv) and difv, wsinkv (nkn, nlv+1);
-        the open-boundary values stay to the caller, as in scal3sh."""
+        cbound is what inflows bring where the basin has a discharge (None:
+        the node's own value); the open-boundary values stay to the caller,
+        as in scal3sh."""
         c = self.cases[ib]
         nkn, nel, nlv = c["nkn"], c["nel"], c["nlv"]
         arrays = dict(cn1=(cn1, (nkn, nlv)), difhv=(difhv, (nel, nlv)), difv=(difv, (nkn, nlv + 1)),
                       gradxv=(gradxv, (nkn, nlv)), gradyv=(gradyv, (nkn, nlv)), cobs=(cobs, (nkn, nlv)),
-                      rtauv=(rtauv, (nkn, nlv)), wsinkv=(wsinkv, (nkn, nlv + 1)), load=(load, (nkn, nlv)))
+                      rtauv=(rtauv, (nkn, nlv)), wsinkv=(wsinkv, (nkn, nlv + 1)), load=(load, (nkn, nlv)),
+                      cbound=(cbound, (nkn, nlv)))
         for name, (a, shape) in arrays.items():
             if a is None:
                 continue
@@ -248,7 +263,7 @@ class Model:
         def p(a):
             return None if a is None else a.ctypes.data
         check(lib().shygpu_conz3d(self.h, ib, p(cn1), None, float(ddt), float(rkpar), p(difhv), p(difv),
-                                  float(difmol), None, int(itvd), int(itvdv), p(gradxv), p(gradyv),
+                                  float(difmol), p(cbound), int(itvd), int(itvdv), p(gradxv), p(gradyv),
                                   p(cobs), float(robs), p(rtauv), float(wsink), p(wsinkv), float(rload),
                                   p(load), float(azpar), float(adpar), float(aapar), int(istot),
                                   int(isact), nlv, nlv), "conz3d")

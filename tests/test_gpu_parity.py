@@ -380,14 +380,84 @@ def test_whole_model_transfers():
     assert np.array_equal(out, ref)
 
 
-def test_conz3d_entry_reproduces_run_scalar():
+def far_end_nodes(c, n=3):
+    """Nodes at the basin's far end (largest x), mid-channel."""
+    x, y = c["xgv"], c["ygv"]
+    far = np.nonzero(x >= x.max() - 1.0)[0]
+    return far[np.argsort(np.abs(y[far] - y.mean()))][:n]
+
+
+def with_river(c, q_total, n=3):
+    c = dict(c)
+    rqv = np.zeros(c["nkn"], np.float32)
+    rqv[far_end_nodes(c, n)] = q_total / n
+    c["rqv"] = rqv
+    return c
+
+
+@pytest.mark.parametrize("shape", ["basin3d", "lagoon30"])
+def test_river_discharge(small3d, shape):
+    """A discharge at three nodes of the far end (set_mass_flux,
+    bnd_routines.f90:1035-1140): it enters the zeta system, the vertical
+    velocity through each layer's share (hydrodynamic.f90:1727) and the
+    transport with the scalars' boundary values (concentration_omp.f90:
+    805-813): a 5 degC fresh river into the baroclinic 3D basin (12 z-layers,
+    thread-per-column kernels), a river of tracer 5 into the 30-layer
+    lagoon (warp-segment kernels)."""
+    if shape == "basin3d":
+        c, n = with_river(small3d, 150.0), 120
+        bounds = [(0, "tempv", 5.0), (1, "saltv", 0.0)]
+    else:
+        c, n = with_river(cases.lagoon_case(nkn_target=900, nlv=30), 80.0), 80
+        bounds = [(2, "conzv", 5.0)]
+    g = shygpu.Model(c)
+    g.set_state(0)
+    o = shyref.OracleModel(c)
+    for what, f, v in bounds:
+        for itr in range(3 if what == 2 else 1):
+            b = np.full((c["nkn"], c["nlv"]), v, np.float32)
+            g.set_bound_scalar(0, what, b, itr)
+            o.set_bound_scalar(what, b, itr)
+    g.run(n)
+    o.run(n)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    me = active_mask(c, node=False)
+    umax = max(np.abs(so["utlnv"][me]).max(), np.abs(so["vtlnv"][me]).max())
+    assert np.abs(sg["utlnv"] - so["utlnv"])[me].max() <= 1e-3 * umax
+    wmax = np.abs(so["wlnv"]).max()
+    assert np.abs(sg["wlnv"] - so["wlnv"]).max() <= 2e-3 * wmax
+    m = active_mask(c)
+    for _, f, _ in bounds:
+        a, b = sg[f], so[f]
+        mm = m if a.ndim == 2 else np.broadcast_to(m, a.shape)
+        rel = np.abs(a - b)[mm].max() / np.abs(b[mm]).max()
+        assert rel <= TRACER_RTOL, (f, rel)
+    assert abs(g.info(0).volume - o.info().volume) <= 1e-6 * o.info().volume
+    # the river is felt: the water rose at its nodes, its tracer entered
+    k = far_end_nodes(c)[0]
+    f0 = bounds[0][1]
+    now = so[f0][0] if f0 == "conzv" else so[f0]
+    before = c[f0][0] if f0 == "conzv" else c[f0]
+    assert abs(now[k, 0] - before[k, 0]) > 1e-3
+
+
+@pytest.mark.parametrize("river", [False, True])
+def test_conz3d_entry_reproduces_run_scalar(river):
     """shygpu_conz3d driven by the reference's scal3sh loop (clip, conz3d_omp,
     boundary values, per sub-step; concentration.f90:727-770) after
-    shygpu_hydro gives the bits of the whole-phase shygpu_scalar."""
+    shygpu_hydro gives the bits of the whole-phase shygpu_scalar; with a
+    river, its cbound is what shygpu_set_bound_scalar gave the step."""
     c = cases.lagoon_case(nkn_target=900, nlv=12, ntracer=1)
+    if river:
+        c = with_river(c, 60.0)
     p = c["params"]
     m = shygpu.Model(c)
     m.set_state(0)
+    cb = np.asarray(c["conzv"][0], np.float32)          # boundary values: the initial columns
+    if river:
+        cb = np.full_like(cb, 7.0)
+        m.set_bound_scalar(0, 2, cb, 0)
     m.run(4)
     ck = m.checkpoint()
     m.hydro()
@@ -401,18 +471,20 @@ def test_conz3d_entry_reproduces_run_scalar():
     nlv = c["nlv"]
     difhv = np.ones((c["nel"], nlv), np.float32)
     difv = np.ascontiguousarray(c["difv"], np.float32)
-    cb = np.asarray(c["conzv"][0], np.float32)          # boundary values: the initial columns
+    cbp = np.ascontiguousarray(cb).ctypes.data if river else None
     bnd = c["bnd_index"] > 0
     assert istot >= 1
     for isact in range(1, istot + 1):
         cn[cn < 1e-15] = 0.0
         shygpu.check(lib.shygpu_conz3d(
             m.h, 0, cn.ctypes.data, None, float(p["dt"]), float(p["chpar"]), difhv.ctypes.data,
-            difv.ctypes.data, float(p["difmol"]), None, 0, 0, None, None, None, 0.0, None, 0.0, None,
+            difv.ctypes.data, float(p["difmol"]), cbp, 0, 0, None, None, None, 0.0, None, 0.0, None,
             0.0, None, float(p["azpar"]), float(p["adpar"]), float(p["aapar"]), istot, isact, nlv, nlv),
             "conz3d")
         cn[bnd] = cb[bnd]
     assert np.array_equal(cn, ref)
+    if river:
+        assert cn[far_end_nodes(c)[0], 0] > 1e-3
 
 
 def test_conz3d_entry_source_terms():
