@@ -556,3 +556,37 @@ def test_vertical_momentum_advection(ihwadv, column_threads):
     flat = shyref.OracleModel(with_params(c, ihwadv=0))
     flat.run(120)
     assert np.abs(flat.state()["utlnv"] - so["utlnv"])[me].max() > 10e-3 * umax
+
+
+@pytest.mark.parametrize("shape", ["basin3d", "lagoon30"])
+def test_horizontal_viscosity_and_diffusion(small3d, shape):
+    """Horizontal viscosity of momentum (ahpar, set_diff_horizontal,
+    explicit.f90:389-493) and horizontal diffusion of the scalars (thpar,
+    shpar, chpar: the wdifhv terms of conz3d_element) against the oracle,
+    through the thread-per-column kernels (12 z-layers) and the warp-segment
+    kernels (30 sigma layers)."""
+    if shape == "basin3d":
+        c, n, fields = with_params(small3d, ahpar=50.0, thpar=20.0, shpar=20.0), 120, ("tempv", "saltv")
+    else:
+        c, n, fields = with_params(cases.lagoon_case(nkn_target=900, nlv=30), ahpar=20.0, chpar=10.0), 80, ("conzv",)
+    g, o = run_both(c, n)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    me = active_mask(c, node=False)
+    umax = max(np.abs(so["utlnv"][me]).max(), np.abs(so["vtlnv"][me]).max())
+    for f in ("utlnv", "vtlnv"):
+        assert np.abs(sg[f] - so[f])[me].max() <= 1e-3 * umax, f
+    m = active_mask(c)
+    for f in fields:
+        a, b = sg[f], so[f]
+        mm = m if a.ndim == 2 else np.broadcast_to(m, a.shape)
+        rel = np.abs(a - b)[mm].max() / np.abs(b[mm]).max()
+        assert rel <= TRACER_RTOL, (f, rel)
+    # the terms act: the run differs from one without them
+    c0 = with_params(c, ahpar=0.0, thpar=0.0, shpar=0.0, chpar=0.0)
+    o0 = shyref.OracleModel(c0)
+    o0.run(n)
+    assert np.abs(o0.state()["utlnv"] - so["utlnv"])[me].max() > 1e-3 * umax
+    s0 = o0.state()
+    f = fields[0]
+    assert np.abs(s0[f] - so[f]).max() > 1e-3 * np.abs(so[f]).max()
