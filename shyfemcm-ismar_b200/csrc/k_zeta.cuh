@@ -113,7 +113,7 @@ __device__ __forceinline__ double tfrac(const ZetaArgs &za) {
 // one row of the assembly: FP64 gather of the element entries of every slot
 // (element order), the rhs, the diagonal
 __device__ __forceinline__ void assemble_row(const Dev &d, const ZetaArgs &za, int i, float dtf,
-                                             double &diag, double &rhs, bool wd = false) {
+                                             double &diag, double &rhs, bool wd = false, bool w32 = true) {
   diag = 0.;
   for (int s = d.rowptr[i]; s < d.rowptr[i + 1]; s++) {
     double v = 0.;
@@ -124,7 +124,7 @@ __device__ __forceinline__ void assemble_row(const Dev &d, const ZetaArgs &za, i
       v += (double)(wd ? __ldcg(ph) : *ph);      // dry systems are written in this launch
     }
     d.val64[s] = v;
-    d.val32[s] = (float)v;
+    if (w32) d.val32[s] = (float)v;            // the FP32 copy the cluster solvers iterate on
     if (d.col[s] == i) diag = v;
   }
   rhs = 0.;

@@ -10,14 +10,20 @@
 // sparskit_admin.f90:115-334, with the reference's stop test
 // ||r|| <= rtol*||r0|| + atol, spk_iters.f90:3304-3360): FP64 residual
 // refinement around Jacobi-preconditioned Chronopoulos-Gear CG in FP32, the
-// extrapolated start 2 z^n - z^(n-1).  Every basin runs its own state
+// extrapolated start 2 z^n - z^(n-1).  The FP32 iterations run on the
+// symmetrically scaled system S A S (S = D^-1/2), which is Jacobi-
+// preconditioned CG in another basis: its diagonal is one, so a row stores
+// only its off-diagonal entries (as 16-bit column offsets where every
+// offset fits) and no preconditioner, and a row's record is {r, w, s, p}
+// with the correction e beside it: 80 bytes per row and iteration for a
+// triangle mesh instead of 108.  Every basin runs its own state
 // machine; all basins advance in lock step through "super-steps" separated
 // by one grid barrier.  One CG iteration is one super-step: a row needs its
-// neighbours' new preconditioned residual u_j = D_j^-1 (r_j - a (w_j + b s_j))
-// for the product A u, and computes it from their values of the previous
-// iteration (kept in a second generation of the vectors) with the iteration
-// scalars a, b that every row of the basin shares, so no barrier separates
-// the vector update from the matrix-vector product.  In a super-step each
+// neighbours' new residual r_j - a (w_j + b s_j) for the product, and
+// computes it from their values of the previous iteration (kept in a
+// second generation of the vectors) with the iteration scalars a, b that
+// every row of the basin shares, so no barrier separates the vector update
+// from the matrix-vector product.  In a super-step each
 // tile does the work of its basin's stage and writes its partial sums; after
 // the barrier every CTA that holds a tile of the basin sums that basin's
 // partials in tile order (the same bits in every CTA, and the same alone or
@@ -96,31 +102,39 @@ __device__ __forceinline__ bool grid_barrier(const GridPlan &gp, unsigned bar, i
   return *s_ok != 0;
 }
 
-// the new preconditioned residual of a row from its values of the previous
-// iteration q = {r, w, s, 1/diag}: s' = w + b s, r' = r - a s', u' = r'/diag.
-// Rows and their neighbours evaluate the same expression, so the same bits.
-__device__ __forceinline__ float cg_unext(const float4 q, float fa, float fb, float &s_new, float &r_new) {
+// the new residual of a row from its record of the previous iteration q =
+// {r, w, s, p}: s' = w + b s, r' = r - a s'.  Rows and their neighbours
+// evaluate the same expression, so the same bits.
+__device__ __forceinline__ float cg_rnext(const float4 q, float fa, float fb, float &s_new) {
   s_new = q.y + fb * q.z;
-  r_new = q.x - fa * s_new;
-  return q.w * r_new;
+  return q.x - fa * s_new;
 }
 
-// one row of A u' in FP32, u' of every entry's row from the previous
-// generation (fa = fb = 0 and r only: u = r/diag); the row's entries are
+// column of off-diagonal entry k of row i
+template <bool C16>
+__device__ __forceinline__ int ocol(const GridPlan &gp, int i, int k) {
+  if constexpr (C16) return i + (int)gp.ocol16[k];
+  else return gp.ocol32[k];
+}
+
+// one row of (S A S) r' in FP32: the unit diagonal times the row's own new
+// residual, then the off-diagonal entries in slot order with r' of each
+// entry's row from the previous generation (fa = fb = 0: r' = r); entries
 // fetched eight at a time, all loads issued before the products
-// (memory-level parallelism for the short rows of a triangle mesh); the sum
-// runs in slot order
-__device__ __forceinline__ float grid_spmv_row(const Dev &d, int i, const float4 *qg, float fa, float fb) {
-  const int s0 = d.rowptr[i], s1 = d.rowptr[i + 1];
-  float w = 0.f;
+// (memory-level parallelism for the short rows of a triangle mesh)
+template <bool C16>
+__device__ __forceinline__ float grid_spmv_row(const GridPlan &gp, int i, const float4 *qg, float fa, float fb,
+                                               float own) {
+  const int s0 = gp.optr[i], s1 = gp.optr[i + 1];
+  float w = own;
   for (int s = s0; s < s1; s += 8) {
     int c[8];
     float v[8];
 #pragma unroll
     for (int k = 0; k < 8; k++) {
       const bool ok = s + k < s1;
-      c[k] = ok ? d.col[s + k] : i;
-      v[k] = ok ? d.val32[s + k] : 0.f;
+      c[k] = ok ? ocol<C16>(gp, i, s + k) : i;
+      v[k] = ok ? gp.oval[s + k] : 0.f;
     }
     float4 x[8];
 #pragma unroll
@@ -128,8 +142,8 @@ __device__ __forceinline__ float grid_spmv_row(const Dev &d, int i, const float4
 #pragma unroll
     for (int k = 0; k < 8; k++)
       if (s + k < s1) {
-        float sn, rn;
-        w += v[k] * cg_unext(x[k], fa, fb, sn, rn);
+        float sn;
+        w += v[k] * cg_rnext(x[k], fa, fb, sn);
       }
   }
   return w;
@@ -166,18 +180,18 @@ __device__ __forceinline__ double grid_resid_row(const Dev &d, int i) {
 // to 16 bytes; the arrays carry the slack) and moves a multiple of 16 bytes.
 // ---------------------------------------------------------------------------
 struct StageLayout {   // byte offsets inside one buffer
-  int row, col, val, q4, pe, bytes;
+  int row, col, val, q4, ev, bytes;
 };
 
-__host__ __device__ inline StageLayout stage_layout(int nzcap) {
+// cb: bytes per column index (2 or 4)
+__host__ __device__ inline StageLayout stage_layout(int nzcap, int cb) {
   StageLayout L;
   L.row = 0;
   L.col = L.row + (kGridTileRows + 8) * 4;
-  const int cb = ((nzcap + 8) * 4 + 15) & ~15;
-  L.val = L.col + cb;
-  L.q4 = L.val + cb;
-  L.pe = L.q4 + kGridTileRows * 16;
-  L.bytes = (L.pe + (kGridTileRows + 2) * 8 + 127) & ~127;
+  L.val = L.col + (((nzcap + 16) * cb + 15) & ~15);
+  L.q4 = L.val + (((nzcap + 8) * 4 + 15) & ~15);
+  L.ev = L.q4 + kGridTileRows * 16;
+  L.bytes = (L.ev + (kGridTileRows + 8) * 4 + 127) & ~127;
   return L;
 }
 
@@ -190,20 +204,27 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, int byte
                ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
-// thread 0: copy tile rows [a,e), entries [nz0,nz1) into the buffer at sbuf
-__device__ __forceinline__ void stage_issue(const Dev &d, const StageLayout &L, uint32_t sbuf, uint32_t mbar,
+// thread 0: copy tile rows [a,e), off-diagonal entries [nz0,nz1) into the
+// buffer at sbuf: every range is widened to 16-byte boundaries (the arrays
+// carry the slack), so each copy starts aligned and moves whole 16 bytes
+template <bool C16>
+__device__ __forceinline__ void stage_issue(const GridPlan &gp, const StageLayout &L, uint32_t sbuf, uint32_t mbar,
                                             int a, int e, int nz0, int nz1, const float4 *qg) {
+  constexpr int CA = C16 ? 8 : 4;                       // column indices per 16 bytes
   const int ra = a & ~3, rc = ((e + 1 - ra) + 3) & ~3;
-  const int ca = nz0 & ~3, cc = ((nz1 - ca) + 3) & ~3;
-  const int pa = a & ~1, pc = ((e - pa) + 1) & ~1;
-  const int bytes = rc * 4 + 2 * cc * 4 + (e - a) * 16 + pc * 8;
+  const int ka = nz0 & ~(CA - 1), kc = ((nz1 - ka) + CA - 1) & ~(CA - 1);
+  const int va = nz0 & ~3, vc = ((nz1 - va) + 3) & ~3;
+  const int ea = a & ~3, ec = ((e - ea) + 3) & ~3;
+  const int cbytes = kc * (C16 ? 2 : 4);
+  const int bytes = rc * 4 + cbytes + vc * 4 + (e - a) * 16 + ec * 4;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
-  bulk_g2s(sbuf + L.row, d.rowptr + ra, rc * 4, mbar);
-  bulk_g2s(sbuf + L.col, d.col + ca, cc * 4, mbar);
-  bulk_g2s(sbuf + L.val, d.val32 + ca, cc * 4, mbar);
+  bulk_g2s(sbuf + L.row, gp.optr + ra, rc * 4, mbar);
+  if constexpr (C16) bulk_g2s(sbuf + L.col, gp.ocol16 + ka, cbytes, mbar);
+  else bulk_g2s(sbuf + L.col, gp.ocol32 + ka, cbytes, mbar);
+  bulk_g2s(sbuf + L.val, gp.oval + va, vc * 4, mbar);
   bulk_g2s(sbuf + L.q4, qg + a, (e - a) * 16, mbar);
-  bulk_g2s(sbuf + L.pe, d.cg2 + pa, pc * 8, mbar);
+  bulk_g2s(sbuf + L.ev, gp.ecor + ea, ec * 4, mbar);
 }
 
 // bounded wait for an mbarrier phase; false when it did not complete
@@ -217,17 +238,18 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
-// A u' for one row from a staged tile: entries, and u' of rows inside the
-// tile, from shared memory; u' of rows outside it from global memory
-__device__ __forceinline__ float staged_spmv_row(const int *scol, const float *sval, int s0, int s1,
+// (S A S) r' for one row from a staged tile: entries, and r' of rows inside
+// the tile, from shared memory; r' of rows outside it from global memory
+template <bool C16>
+__device__ __forceinline__ float staged_spmv_row(const void *scol, const float *sval, int i, int s0, int s1,
                                                  const float4 *sq, int a, int R, const float4 *qg,
-                                                 float fa, float fb) {
-  float w = 0.f;
+                                                 float fa, float fb, float own) {
+  float w = own;
   for (int m = s0; m < s1; m++) {
-    const int c = scol[m];
+    const int c = C16 ? i + (int)static_cast<const short *>(scol)[m] : static_cast<const int *>(scol)[m];
     const float4 x = (unsigned)(c - a) < (unsigned)R ? sq[c - a] : qg[c];
-    float sn, rn;
-    w += sval[m] * cg_unext(x, fa, fb, sn, rn);
+    float sn;
+    w += sval[m] * cg_rnext(x, fa, fb, sn);
   }
   return w;
 }
@@ -252,8 +274,10 @@ __device__ __forceinline__ void grid_transition(GridState &g, const double (&tot
       if (rn <= g.tol) { g.conv = 1; g.stage = G_FINISH; }
       else if (g.outer >= za.max_outer) g.stage = G_FINISH;
       else {
+        // the FP32 sweep's target, moved into the norm of the scaled residual
+        // (tot[1] = ||S r||^2) by the ratio of the two norms at its start
         const double it = fmax((double)za.inner_rtol * rn, tfrac(za) * g.tol);
-        g.itol2 = it * it;
+        g.itol2 = tot[0] > 0. ? it * it * (tot[1] / tot[0]) : 0.;
         g.stage = G_SPMV0;
       }
     }
@@ -283,7 +307,7 @@ __device__ __forceinline__ void grid_transition(GridState &g, const double (&tot
 // TMA-staged shared memory (two buffers, the next tile's copy in flight
 // while one is worked; one CTA of 1024 threads per SM); otherwise straight
 // from global memory (two CTAs of 512 threads per SM).
-template <int NT, bool STAGED>
+template <int NT, bool STAGED, bool C16>
 __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArgs za, GridPlan gp) {
   constexpr int NW = NT / 32;
   __shared__ GridState gs[kGridMaxSlots];
@@ -299,7 +323,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
   const int nslot = gp.cnslot[c];
   const int t0 = gp.cptr[c], ntl = gp.cptr[c + 1] - t0;   // this CTA's tiles: clist[t0 ..]
   unsigned bar = 0;
-  const StageLayout SL = stage_layout(gp.nzcap);
+  const StageLayout SL = stage_layout(gp.nzcap, C16 ? 2 : 4);
   uint32_t mbar[2] = {0u, 0u}, sbuf[2] = {0u, 0u}, phase[2] = {0u, 0u};
   if (STAGED) {
     mbar[0] = smem_u32(dsm); mbar[1] = mbar[0] + 8;
@@ -337,8 +361,8 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
     const float dtf = (float)P.dt;
     for (int i = tl.x + tid; i < tl.y; i += nth) {
       double diag, rhs;
-      assemble_row(d, za, i, dtf, diag, rhs);
-      d.dinv32[i] = diag != 0. ? (float)(1. / diag) : 1.f;
+      assemble_row(d, za, i, dtf, diag, rhs, false, false);   // no FP32 copy of the full rows
+      gp.sd[i] = diag > 0. ? (float)(1. / sqrt(diag)) : 1.f;
       const double x0 = za.explicit_mode ? (diag != 0. ? rhs / diag : 0.) : (double)za.zguess[i];
       d.x64[i] = x0;
       if (za.explicit_mode) d.zn[i] = (float)x0;
@@ -364,7 +388,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
       if (iq < ntl) {
         const int4 tl = s_tile[iq];
         const int2 nz = s_tnz[iq];
-        stage_issue(d, SL, sbuf[b], mbar[b], tl.x, tl.y, nz.x, nz.y, d.cg4[gs[tl.w].cur]);
+        stage_issue<C16>(gp, SL, sbuf[b], mbar[b], tl.x, tl.y, nz.x, nz.y, d.cg4[gs[tl.w].cur]);
         iq++;
       }
     };
@@ -396,11 +420,13 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
         phase[b] ^= 1u;
         const unsigned char *buf = dsm + 128 + (size_t)b * SL.bytes;
         const int2 nz = s_tnz[q];
+        constexpr int CA = C16 ? 8 : 4;
         const int *srow = reinterpret_cast<const int *>(buf + SL.row) + (a - (a & ~3));
-        const int *scol = reinterpret_cast<const int *>(buf + SL.col) + (nz.x - (nz.x & ~3));
+        const void *scol = C16 ? (const void *)(reinterpret_cast<const short *>(buf + SL.col) + (nz.x - (nz.x & ~(CA - 1))))
+                               : (const void *)(reinterpret_cast<const int *>(buf + SL.col) + (nz.x - (nz.x & ~(CA - 1))));
         const float *sval = reinterpret_cast<const float *>(buf + SL.val) + (nz.x - (nz.x & ~3));
         const float4 *sq = reinterpret_cast<const float4 *>(buf + SL.q4);
-        const float2 *spe = reinterpret_cast<const float2 *>(buf + SL.pe) + (a - (a & ~1));
+        const float *sev = reinterpret_cast<const float *>(buf + SL.ev) + (a - (a & ~3));
         const float4 *qi = d.cg4[g.cur];
         float4 *qo = d.cg4[g.cur ^ 1];
         const int R = e - a;
@@ -409,74 +435,82 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
         for (int j = tid; j < R; j += nth) {
           const int i = a + j;
           const float4 me = sq[j];
-          const float w = staged_spmv_row(scol, sval, srow[j] - nz.x, srow[j + 1] - nz.x, sq, a, R, qi, fa, fb);
           if (stage == G_SPMV0) {
-            // w = A u with u = r/diag (fa = 0 and s = 0 leave r, so u = r/diag)
-            const float u = me.w * me.x;
-            qo[i] = make_float4(me.x, w, 0.f, me.w);
-            v[0] += (double)me.x * u;
-            v[1] += (double)w * u;
-            v[2] += (double)me.x * me.x;
+            // w = (S A S) r (fa = fb = 0 leave r)
+            const float w = staged_spmv_row<C16>(scol, sval, i, srow[j] - nz.x, srow[j + 1] - nz.x, sq, a, R, qi,
+                                                 0.f, 0.f, me.x);
+            qo[i] = make_float4(me.x, w, 0.f, 0.f);
+            v[0] += (double)me.x * me.x;
+            v[1] += (double)w * me.x;
           } else {
-            // p = u + b p, s = w + b s, e += a p, r -= a s, u = r/diag, w = A u
-            const float2 pe = spe[j];
-            const float p = me.w * me.x + fb * pe.x;
-            float sn, rn;
-            const float u = cg_unext(me, fa, fb, sn, rn);
-            qo[i] = make_float4(rn, w, sn, me.w);
-            d.cg2[i] = make_float2(p, pe.y + fa * p);
-            v[0] += (double)rn * u;
-            v[1] += (double)w * u;
-            v[2] += (double)rn * rn;
+            // p = r + b p, s = w + b s, e += a p, r -= a s, w = (S A S) r
+            const float p = me.x + fb * me.w;
+            float sn;
+            const float rn = cg_rnext(me, fa, fb, sn);
+            const float w = staged_spmv_row<C16>(scol, sval, i, srow[j] - nz.x, srow[j + 1] - nz.x, sq, a, R, qi,
+                                                 fa, fb, rn);
+            qo[i] = make_float4(rn, w, sn, p);
+            gp.ecor[i] = sev[j] + fa * p;
+            v[0] += (double)rn * rn;
+            v[1] += (double)w * rn;
           }
+          v[2] = v[0];
         }
         __syncthreads();                            // buffer b read by every thread
         if (tid == 0) issue_next(b);
         js++;
       } else if (stage == G_RES) {
+        // the FP64 residual t (its norm is the stop test's), the scaled S t
+        // the FP32 sweep starts from, a zero correction; the first pass of
+        // a solve also writes the scaled off-diagonal entries of its rows
         float4 *qo = d.cg4[g.cur];
+        const bool scale = g.first != 0;
         for (int i = a + tid; i < e; i += nth) {
           const double t = grid_resid_row(d, i);
-          qo[i] = make_float4((float)t, 0.f, 0.f, d.dinv32[i]);
-          d.cg2[i] = make_float2(0.f, 0.f);
+          const double sdi = (double)gp.sd[i];
+          if (scale)
+            for (int k = gp.optr[i]; k < gp.optr[i + 1]; k++)
+              gp.oval[k] = (float)(d.val64[gp.oslot[k]] * sdi * (double)gp.sd[ocol<C16>(gp, i, k)]);
+          const float rs = (float)(sdi * t);
+          qo[i] = make_float4(rs, 0.f, 0.f, 0.f);
+          gp.ecor[i] = 0.f;
           v[0] += t * t;
+          v[1] += (double)rs * rs;
         }
       } else if (stage == G_XTRP) {
         // z_guess = 2 z^n - z^{n-1}: smooth in time, a smaller starting residual
         for (int i = a + tid; i < e; i += nth) d.x64[i] = 2. * (double)za.zguess[i] - (double)za.zprev[i];
       } else if (stage == G_SPMV0) {
-        // w = A u with u = r/diag (fa = 0 and s = 0 leave r, so u = r/diag)
+        // w = (S A S) r (fa = fb = 0 leave r); p = s = 0
         const float4 *qi = d.cg4[g.cur];
         float4 *qo = d.cg4[g.cur ^ 1];
         for (int i = a + tid; i < e; i += nth) {
-          const float w = grid_spmv_row(d, i, qi, 0.f, 0.f);
           const float4 me = qi[i];
-          const float u = me.w * me.x;
-          qo[i] = make_float4(me.x, w, 0.f, me.w);
-          v[0] += (double)me.x * u;
-          v[1] += (double)w * u;
-          v[2] += (double)me.x * me.x;
+          const float w = grid_spmv_row<C16>(gp, i, qi, 0.f, 0.f, me.x);
+          qo[i] = make_float4(me.x, w, 0.f, 0.f);
+          v[0] += (double)me.x * me.x;
+          v[1] += (double)w * me.x;
         }
+        v[2] = v[0];
       } else if (stage == G_ITER) {
-        // p = u + b p, s = w + b s, e += a p, r -= a s, u = r/diag, w = A u
+        // p = r + b p, s = w + b s, e += a p, r -= a s, w = (S A S) r
         const float fa = (float)g.alpha, fb = (float)g.beta;
         const float4 *qi = d.cg4[g.cur];
         float4 *qo = d.cg4[g.cur ^ 1];
         for (int i = a + tid; i < e; i += nth) {
           const float4 me = qi[i];
-          const float2 pe = d.cg2[i];
-          const float p = me.w * me.x + fb * pe.x;
-          float sn, rn;
-          const float u = cg_unext(me, fa, fb, sn, rn);
-          const float w = grid_spmv_row(d, i, qi, fa, fb);
-          qo[i] = make_float4(rn, w, sn, me.w);
-          d.cg2[i] = make_float2(p, pe.y + fa * p);
-          v[0] += (double)rn * u;
-          v[1] += (double)w * u;
-          v[2] += (double)rn * rn;
+          const float p = me.x + fb * me.w;
+          float sn;
+          const float rn = cg_rnext(me, fa, fb, sn);
+          const float w = grid_spmv_row<C16>(gp, i, qi, fa, fb, rn);
+          qo[i] = make_float4(rn, w, sn, p);
+          gp.ecor[i] += fa * p;
+          v[0] += (double)rn * rn;
+          v[1] += (double)w * rn;
         }
+        v[2] = v[0];
       } else if (stage == G_FIX) {
-        for (int i = a + tid; i < e; i += nth) d.x64[i] += (double)d.cg2[i].y;
+        for (int i = a + tid; i < e; i += nth) d.x64[i] += (double)gp.sd[i] * (double)gp.ecor[i];
       } else if (stage == G_FINISH) {
         for (int i = a + tid; i < e; i += nth) d.zn[i] = (float)d.x64[i];
       }

@@ -60,10 +60,21 @@ struct GridPlan {
   const int4 *tile = nullptr;
   const int2 *btile = nullptr;
   const int *cslot = nullptr, *cnslot = nullptr, *cowner = nullptr;
-  const int2 *tnz = nullptr;       // per tile: its CSR entries rowptr[row0] .. rowptr[row1]
+  const int2 *tnz = nullptr;       // per tile: its off-diagonal entries optr[row0] .. optr[row1]
   const int *cptr = nullptr;       // CTA c works tiles clist[cptr[c]] .. clist[cptr[c+1]-1]
   const int *clist = nullptr;
-  int nzcap = 0;                   // most CSR entries of any tile (staged buffer size)
+  int nzcap = 0;                   // most off-diagonal entries of any tile (staged buffer size)
+  // the Jacobi-scaled system the FP32 iterations solve, S A S with S =
+  // D^-1/2: its diagonal is one and is not stored; the off-diagonal entries
+  // in CSR form (row pointers optr, columns as 16-bit offsets j - i when
+  // every offset fits, else absolute), their slots in the full CSR (oslot),
+  // their FP32 values (oval, written by the first residual pass of each
+  // solve), S per row (sd) and the FP32 correction per row (ecor)
+  const int *optr = nullptr;
+  const short *ocol16 = nullptr;
+  const int *ocol32 = nullptr;
+  const int *oslot = nullptr;
+  float *oval = nullptr, *sd = nullptr, *ecor = nullptr;
   double *partial = nullptr;       // [2][ntile][4] partial sums of the tiles
   unsigned *ctr = nullptr;         // [8]: barrier arrivals, 3 active counts, abort flag, release
   unsigned phantom = 0;            // arrivals the barrier waits for beyond its CTAs (0; 1 in the timeout test)
@@ -95,7 +106,7 @@ cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &g
 // CTAs of k_zeta_grid that fit the device at once (0 on error)
 int zeta_grid_capacity(bool staged, size_t smem);
 // dynamic shared memory of the staged form for tiles of at most nzcap entries
-size_t zeta_grid_stage_smem(int nzcap);
+size_t zeta_grid_stage_smem(int nzcap, bool c16);
 int zeta_grid_max_slots();   // basins one CTA can hold
 int zeta_grid_max_tiles();   // tiles one CTA can hold
 int zeta_grid_tile_rows();   // rows per tile

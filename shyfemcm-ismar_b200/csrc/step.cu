@@ -24,6 +24,8 @@
 //             node column, vertical system by PCR, bndo_impbc, and rhoset
 //             (baroclinic.f90:654-710) after the last sub-step.
 #include <cooperative_groups.h>
+
+#include <algorithm>
 #include <cstdint>
 #include <cstdio>
 
@@ -208,27 +210,40 @@ cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &g
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  if (staged) return cudaLaunchKernelEx(&cfg, k_zeta_grid<1024, true>, d, za, gp);
-  return cudaLaunchKernelEx(&cfg, k_zeta_grid<512, false>, d, za, gp);
+  const bool c16 = gp.ocol16 != nullptr;
+  if (staged) return c16 ? cudaLaunchKernelEx(&cfg, k_zeta_grid<1024, true, true>, d, za, gp)
+                         : cudaLaunchKernelEx(&cfg, k_zeta_grid<1024, true, false>, d, za, gp);
+  return c16 ? cudaLaunchKernelEx(&cfg, k_zeta_grid<512, false, true>, d, za, gp)
+             : cudaLaunchKernelEx(&cfg, k_zeta_grid<512, false, false>, d, za, gp);
 }
 
-size_t zeta_grid_stage_smem(int nzcap) { return 128 + 2 * (size_t)stage_layout(nzcap).bytes; }
+size_t zeta_grid_stage_smem(int nzcap, bool c16) {
+  return 128 + 2 * (size_t)stage_layout(nzcap, c16 ? 2 : 4).bytes;
+}
 
-int zeta_grid_capacity(bool staged, size_t smem) {
-  int dev = 0, nsm = 0, nb = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-  if (staged) {
-    if (cudaFuncSetAttribute(k_zeta_grid<1024, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess) {
-      cudaGetLastError();
-      return 0;
-    }
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_zeta_grid<1024, true>, 1024, smem) != cudaSuccess)
-      return 0;
-  } else if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_zeta_grid<512, false>, 512, 0) != cudaSuccess) {
+// resident CTAs of the device-wide solver; the fewer of its two column
+// forms, so a plan holds whichever it launches
+template <bool STAGED, bool C16>
+static int grid_blocks(size_t smem) {
+  constexpr int NT = STAGED ? 1024 : 512;
+  int nb = 0;
+  if (STAGED && cudaFuncSetAttribute(k_zeta_grid<NT, STAGED, C16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem) != cudaSuccess) {
+    cudaGetLastError();
     return 0;
   }
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_zeta_grid<NT, STAGED, C16>, NT, STAGED ? smem : 0) !=
+      cudaSuccess)
+    return 0;
+  return nb;
+}
+
+int zeta_grid_capacity(bool staged, size_t smem) {
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  const int nb = staged ? std::min(grid_blocks<true, true>(smem), grid_blocks<true, false>(smem))
+                        : std::min(grid_blocks<false, true>(0), grid_blocks<false, false>(0));
   return nb * nsm;
 }
 
