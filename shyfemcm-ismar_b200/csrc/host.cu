@@ -341,11 +341,12 @@ static void free_zeta_plan(shygpu_model *m) {
     if (c.d_blist) cudaFree(c.d_blist);
     if (c.grid) {
       cudaFree((void *)c.gp.tile); cudaFree((void *)c.gp.btile); cudaFree((void *)c.gp.cslot);
-      cudaFree((void *)c.gp.cnslot); cudaFree((void *)c.gp.cowner); cudaFree((void *)c.gp.tnz);
+      cudaFree((void *)c.gp.cnslot); cudaFree((void *)c.gp.cowner);
       cudaFree((void *)c.gp.cptr); cudaFree((void *)c.gp.clist);
       cudaFree(c.gp.partial); cudaFree(c.gp.ctr);
-      cudaFree((void *)c.gp.optr); cudaFree((void *)c.gp.ocol16); cudaFree((void *)c.gp.ocol32);
-      cudaFree((void *)c.gp.oslot); cudaFree(c.gp.oval); cudaFree(c.gp.sd); cudaFree(c.gp.ecor);
+      cudaFree((void *)c.gp.ecol16); cudaFree((void *)c.gp.ecol32); cudaFree((void *)c.gp.eslot);
+      cudaFree(c.gp.eval); cudaFree((void *)c.gp.xptr); cudaFree((void *)c.gp.xcol);
+      cudaFree((void *)c.gp.xslot); cudaFree(c.gp.xval); cudaFree(c.gp.sd); cudaFree(c.gp.ecor);
     }
   }
   m->zcl.clear();
@@ -370,23 +371,27 @@ static int build_grid_class(shygpu_model *m) {
   const int NKN = m->NKN;
   // the off-diagonal pattern of the scaled system: per row its entries
   // other than the diagonal, in CSR order, with their slots in the full CSR;
-  // columns as 16-bit offsets when every offset fits
-  std::vector<int> optr(NKN + 1, 0), oslot, ocol;
+  // the first eight in the row's block, the rest in the tail; columns as
+  // 16-bit offsets when every offset fits
+  constexpr int EW = 8;
+  std::vector<int> eslot((size_t)EW * NKN, -1), ecol((size_t)EW * NKN, 0), xptr(NKN + 1, 0), xcol, xslot;
   bool c16 = true;
   for (int i = 0; i < NKN; i++) {
+    int n = 0;
     for (int s = m->rowptr_h[i]; s < m->rowptr_h[i + 1]; s++) {
       const int j = m->col_h[s];
       if (j == i) continue;
-      oslot.push_back(s);
-      ocol.push_back(j);
       if (j - i < -32768 || j - i > 32767) c16 = false;
+      if (n < EW) { eslot[(size_t)EW * i + n] = s; ecol[(size_t)EW * i + n] = j; }
+      else { xcol.push_back(j); xslot.push_back(s); }
+      n++;
     }
-    optr[i + 1] = (int)oslot.size();
+    for (int k = std::min(n, EW); k < EW; k++) ecol[(size_t)EW * i + k] = i;   // padding: the row itself
+    xptr[i + 1] = (int)xcol.size();
   }
-  const size_t nod = oslot.size();
+  const size_t nx = xcol.size();
   std::vector<int4> tile;
-  std::vector<int2> btile(m->nbasin, make_int2(0, 0)), tnz;
-  int nzcap = 0;
+  std::vector<int2> btile(m->nbasin, make_int2(0, 0));
   const int TR = zeta_grid_tile_rows();
   for (int b = 0; b < m->nbasin; b++) {
     const BasinPar &bp = m->par[b];
@@ -394,14 +399,12 @@ static int build_grid_class(shygpu_model *m) {
     for (int r = 0; r < bp.nk; r += TR) {
       const int r0 = bp.k0 + r, r1 = bp.k0 + std::min(bp.nk, r + TR);
       tile.push_back(make_int4(r0, r1, b, 0));
-      tnz.push_back(make_int2(optr[r0], optr[r1]));
-      nzcap = std::max(nzcap, optr[r1] - optr[r0]);
     }
     btile[b].y = (int)tile.size();
   }
   // the TMA-staged form when asked for and its two buffers fit one CTA per SM
   bool staged = m->zstage != 0;
-  size_t smem = staged ? zeta_grid_stage_smem(nzcap, c16) : 0;
+  size_t smem = staged ? zeta_grid_stage_smem(c16) : 0;
   int cap = staged ? zeta_grid_capacity(true, smem) : 0;
   if (cap < 1) { staged = false; smem = 0; cap = zeta_grid_capacity(false, 0); }
   if (cap < 1) return fail(SHY_ECUDA, "zeta grid solver: no resident CTA fits the device");
@@ -467,38 +470,36 @@ static int build_grid_class(shygpu_model *m) {
   ST_TRY(upload_plan(&dcs, cslot)); c.gp.cslot = dcs;
   ST_TRY(upload_plan(&dcn, cnslot)); c.gp.cnslot = dcn;
   ST_TRY(upload_plan(&dco, cowner)); c.gp.cowner = dco;
-  int2 *dnz = nullptr;
-  ST_TRY(upload_plan(&dnz, tnz)); c.gp.tnz = dnz;
   int *dcp = nullptr, *dcl = nullptr;
   ST_TRY(upload_plan(&dcp, cptr)); c.gp.cptr = dcp;
   ST_TRY(upload_plan(&dcl, clist)); c.gp.clist = dcl;
-  c.gp.nzcap = nzcap;
-  // the scaled system's arrays, with 16 bytes of slack at the ends that the
-  // staged form's widened copies may touch
+  // the scaled system's arrays; the corrections carry 16 bytes of slack that
+  // the staged form's widened copies may touch
   {
-    int *dop = nullptr, *dos = nullptr;
-    std::vector<int> optr_pad(optr);
-    optr_pad.resize(NKN + 1 + 8, optr[NKN]);
-    ST_TRY(upload_plan(&dop, optr_pad)); c.gp.optr = dop;
-    std::vector<int> oslot_pad(oslot);
-    oslot_pad.resize(nod + 8, 0);
-    ST_TRY(upload_plan(&dos, oslot_pad)); c.gp.oslot = dos;
+    int *des = nullptr;
+    ST_TRY(upload_plan(&des, eslot)); c.gp.eslot = des;
     if (c16) {
-      std::vector<short> oc(nod + 16, 0);
+      std::vector<short> oc((size_t)EW * NKN);
       for (int i = 0; i < NKN; i++)
-        for (int k = optr[i]; k < optr[i + 1]; k++) oc[k] = (short)(ocol[k] - i);
+        for (int k = 0; k < EW; k++) oc[(size_t)EW * i + k] = (short)(ecol[(size_t)EW * i + k] - i);
       short *d16 = nullptr;
-      ST_TRY(upload_plan(&d16, oc)); c.gp.ocol16 = d16;
+      ST_TRY(upload_plan(&d16, oc)); c.gp.ecol16 = d16;
     } else {
-      std::vector<int> oc(ocol);
-      oc.resize(nod + 8, 0);
       int *d32 = nullptr;
-      ST_TRY(upload_plan(&d32, oc)); c.gp.ocol32 = d32;
+      ST_TRY(upload_plan(&d32, ecol)); c.gp.ecol32 = d32;
     }
-    CUDA_TRY(cudaMalloc(&c.gp.oval, sizeof(float) * (nod + 8)));
+    CUDA_TRY(cudaMalloc(&c.gp.eval, sizeof(float) * EW * (size_t)NKN));
+    CUDA_TRY(cudaMemset(c.gp.eval, 0, sizeof(float) * EW * (size_t)NKN));
+    c.gp.nx = (int)nx;
+    if (nx) {
+      int *dxp = nullptr, *dxc = nullptr, *dxs = nullptr;
+      ST_TRY(upload_plan(&dxp, xptr)); c.gp.xptr = dxp;
+      ST_TRY(upload_plan(&dxc, xcol)); c.gp.xcol = dxc;
+      ST_TRY(upload_plan(&dxs, xslot)); c.gp.xslot = dxs;
+      CUDA_TRY(cudaMalloc(&c.gp.xval, sizeof(float) * nx));
+    }
     CUDA_TRY(cudaMalloc(&c.gp.sd, sizeof(float) * (NKN + 8)));
     CUDA_TRY(cudaMalloc(&c.gp.ecor, sizeof(float) * (NKN + 8)));
-    CUDA_TRY(cudaMemset(c.gp.oval, 0, sizeof(float) * (nod + 8)));
     CUDA_TRY(cudaMemset(c.gp.ecor, 0, sizeof(float) * (NKN + 8)));
   }
   CUDA_TRY(cudaMalloc(&c.gp.partial, sizeof(double) * 8 * std::max<size_t>(tile.size(), 1)));
@@ -722,7 +723,7 @@ static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P,
   if (NLVo) *NLVo = (int)NLV;
   int64_t el = nel * (4 * 16 + 8 * 4 + 12 * 4 + 4 * 4 + NLV * 4 * (2 * 2 + 2 * 1 + 2 + 1 + 2 + 1)) ;
   int64_t nd = nkn * (4 * 12 + 8 * 6 + 40 + NLV * 4 * (2 + 1 + 1) + (NLV + 1) * 4 * 3 + nsc * NLV * 4 * 3);
-  int64_t sy = nnz * (4 + 8 + 4 + 4 * 3) + nkn * 84;   // + the device-wide solver's scaled system
+  int64_t sy = nnz * (4 + 8 + 4 + 4 * 3) + nkn * 104;  // + the device-wide solver's scaled system
   if (adv) nd += nkn * NLV * 8;              // node momentum
   if (tvd) nd += nsc * nkn * NLV * 8;        // TVD node gradients
   if (up) el += nel * 96;                    // TVD upwind points

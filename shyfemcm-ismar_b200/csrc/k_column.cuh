@@ -1,5 +1,5 @@
 // k_column.cuh -- hydro_transports / hydro_intern / hydro_zeta element part
-// Included by step.cu (one translation unit).
+// Included by step.cu.
 #pragma once
 #include "common.cuh"
 #include "physics.cuh"

@@ -27,7 +27,7 @@
 // relative to the increment instead of relative to the mass A h c, so a
 // uniform field stays uniform and the drift against the FP64 reference
 // stays at the rounding of the stored values.
-// Included by step.cu.
+// Included by node_launch.cuh.
 #pragma once
 #include "common.cuh"
 #include "physics.cuh"

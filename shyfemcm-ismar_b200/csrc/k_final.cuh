@@ -1,5 +1,5 @@
 // k_final.cuh -- hydro_transports_final, setzev, element layer thickness
-// Included by step.cu (one translation unit).
+// Included by step.cu.
 #pragma once
 #include "common.cuh"
 #include "k_wetdry.cuh"

@@ -1,5 +1,5 @@
 // k_node.cuh -- nodal layer thickness, vertical velocity, stability index, reductions, initial rho
-// Included by step.cu (one translation unit).
+// Included by node_launch.cuh.
 #pragma once
 #include "common.cuh"
 #include "physics.cuh"
@@ -319,7 +319,7 @@ __global__ void __launch_bounds__(256) k_stab(Dev d, const int *kbas) {
 // ===========================================================================
 // k_reduce: per basin (one block each): volume, sub-step counts, time
 // ===========================================================================
-__global__ void __launch_bounds__(1024) k_reduce(Dev d, int nsub, int advance) {
+static __global__ void __launch_bounds__(1024) k_reduce(Dev d, int nsub, int advance) {
   const int b = blockIdx.x;
   const BasinPar &P = d.par[b];
   BasinOut &O = d.out[b];

@@ -11,7 +11,7 @@
 // zeta system (hydrodynamic.f90:710-727, in k_zeta_global.cuh), their level
 // and barotropic transport follow from continuity (setuvd, in
 // k_final.cuh), and their transport is spread over the layers by
-// thickness (baro2l).  Included by step.cu.
+// thickness (baro2l).  Included by step.cu and step_zeta.cu.
 #pragma once
 #include "common.cuh"
 #include "physics.cuh"
@@ -30,7 +30,7 @@ __device__ __forceinline__ int wd_count(int iweg, int iwet, bool bnewtime) {
 
 // set_dry at the start of a step (shyfem_subs.f90:578): setweg(2) then
 // setweg(3) on the level of the step's start, neither at a new time
-__global__ void k_wd_set(Dev d) {
+static __global__ void k_wd_set(Dev d) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.NEL) return;
   const int4 en = d.enode[e];
@@ -65,7 +65,7 @@ __global__ void k_wd_set(Dev d) {
 // (init_z), then setweg(0) -- elements with a vertex below hzoff leave, and
 // vertex levels below the minimum depth zmin are raised to it
 // (wetdry.f90:232-252) -- for basins with wetting and drying
-__global__ void k_wd_init(Dev d, int basin) {
+static __global__ void k_wd_init(Dev d, int basin) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= d.NEL) return;
   const int4 en = d.enode[e];
@@ -100,7 +100,7 @@ __global__ void k_wd_init(Dev d, int basin) {
 // setznv (wetdry.f90:619-712) for basins with wetting and drying: a node's
 // level from its wet elements (the largest vertex level), else the
 // area-weighted mean over its dry elements
-__global__ void k_wd_znv(Dev d, const int *kbas, int basin) {
+static __global__ void k_wd_znv(Dev d, const int *kbas, int basin) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.NKN) return;
   if (basin >= 0 && kbas[k] != basin) return;

@@ -16,7 +16,7 @@
 // matrix-vector product reads only local shared memory.  Chronopoulos-Gear
 // CG: one fused reduction per iteration, the iteration scalars computed once
 // per CTA.  The global-memory variant is in k_zeta_global.cuh.
-// Included by step.cu.
+// Included by step_zeta.cu.
 #pragma once
 #include <cooperative_groups.h>
 

@@ -1,7 +1,7 @@
 // k_zeta_global.cuh -- zeta assembly + solve with the Krylov vectors in
 // global memory (any basin size; CG, or BiCGStab for non-symmetric systems
 // such as those with Coriolis).  Shares cluster_sum and assemble_row with
-// k_zeta.cuh.  Included by step.cu after k_zeta.cuh.
+// k_zeta.cuh.  Included by step_zeta.cu after k_zeta.cuh.
 #pragma once
 #include "k_zeta.cuh"
 

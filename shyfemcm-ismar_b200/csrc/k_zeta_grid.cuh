@@ -13,10 +13,12 @@
 // extrapolated start 2 z^n - z^(n-1).  The FP32 iterations run on the
 // symmetrically scaled system S A S (S = D^-1/2), which is Jacobi-
 // preconditioned CG in another basis: its diagonal is one, so a row stores
-// only its off-diagonal entries (as 16-bit column offsets where every
-// offset fits) and no preconditioner, and a row's record is {r, w, s, p}
-// with the correction e beside it: 80 bytes per row and iteration for a
-// triangle mesh instead of 108.  Every basin runs its own state
+// only its off-diagonal entries, in a fixed-width block of eight (16-bit
+// column offsets where every offset fits, a CSR tail for rows with more)
+// that a thread reads with three independent vector loads, and no
+// preconditioner; a row's record is {r, w, s, p} with the correction e
+// beside it: 88 bytes per row and iteration instead of 108, and one level
+// of dependent loads (row pointers) fewer.  Every basin runs its own state
 // machine; all basins advance in lock step through "super-steps" separated
 // by one grid barrier.  One CG iteration is one super-step: a row needs its
 // neighbours' new residual r_j - a (w_j + b s_j) for the product, and
@@ -37,7 +39,7 @@
 // Vectors written by other CTAs are read with ordinary (L1-cached) loads:
 // no CTA reads, in a super-step, what another writes in the same one, and
 // the barrier's acquire makes the previous super-step's writes visible.
-// Included by step.cu.
+// Included by step_zeta.cu.
 #pragma once
 #include "k_zeta.cuh"
 
@@ -110,43 +112,68 @@ __device__ __forceinline__ float cg_rnext(const float4 q, float fa, float fb, fl
   return q.x - fa * s_new;
 }
 
-// column of off-diagonal entry k of row i
+// columns of the eight entries of row i's block (padding: i)
 template <bool C16>
-__device__ __forceinline__ int ocol(const GridPlan &gp, int i, int k) {
-  if constexpr (C16) return i + (int)gp.ocol16[k];
-  else return gp.ocol32[k];
+__device__ __forceinline__ void ell_cols(const GridPlan &gp, int i, int (&c)[8]) {
+  if constexpr (C16) {
+    const int4 p = __ldg(reinterpret_cast<const int4 *>(gp.ecol16) + i);   // eight 16-bit offsets
+    const int w[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      c[2 * k] = i + (int)(short)(w[k] & 0xffff);
+      c[2 * k + 1] = i + (w[k] >> 16);            // arithmetic shift: the signed high half
+    }
+  } else {
+    const int4 p0 = __ldg(reinterpret_cast<const int4 *>(gp.ecol32) + 2 * i);
+    const int4 p1 = __ldg(reinterpret_cast<const int4 *>(gp.ecol32) + 2 * i + 1);
+    c[0] = p0.x; c[1] = p0.y; c[2] = p0.z; c[3] = p0.w;
+    c[4] = p1.x; c[5] = p1.y; c[6] = p1.z; c[7] = p1.w;
+  }
 }
 
 // one row of (S A S) r' in FP32: the unit diagonal times the row's own new
-// residual, then the off-diagonal entries in slot order with r' of each
-// entry's row from the previous generation (fa = fb = 0: r' = r); entries
-// fetched eight at a time, all loads issued before the products
-// (memory-level parallelism for the short rows of a triangle mesh)
+// residual, then the entries in slot order (the block, then the tail) with
+// r' of each entry's row from the previous generation (fa = fb = 0: r' =
+// r).  The block's columns and values come in three vector loads and its
+// eight neighbour records are all requested before the products; padding
+// entries point at the row itself with value 0.
 template <bool C16>
 __device__ __forceinline__ float grid_spmv_row(const GridPlan &gp, int i, const float4 *qg, float fa, float fb,
                                                float own) {
-  const int s0 = gp.optr[i], s1 = gp.optr[i + 1];
-  float w = own;
-  for (int s = s0; s < s1; s += 8) {
-    int c[8];
-    float v[8];
+  int c[8];
+  ell_cols<C16>(gp, i, c);
+  const float4 va = reinterpret_cast<const float4 *>(gp.eval)[2 * i];
+  const float4 vb = reinterpret_cast<const float4 *>(gp.eval)[2 * i + 1];
+  float4 x[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const bool ok = s + k < s1;
-      c[k] = ok ? ocol<C16>(gp, i, s + k) : i;
-      v[k] = ok ? gp.oval[s + k] : 0.f;
-    }
-    float4 x[8];
+  for (int k = 0; k < 8; k++) x[k] = qg[c[k]];
+  const float v[8] = {va.x, va.y, va.z, va.w, vb.x, vb.y, vb.z, vb.w};
+  float w = own, sn;
 #pragma unroll
-    for (int k = 0; k < 8; k++) x[k] = qg[c[k]];
-#pragma unroll
-    for (int k = 0; k < 8; k++)
-      if (s + k < s1) {
-        float sn;
-        w += v[k] * cg_rnext(x[k], fa, fb, sn);
-      }
-  }
+  for (int k = 0; k < 8; k++) w += v[k] * cg_rnext(x[k], fa, fb, sn);
+  if (gp.nx)
+    for (int k = gp.xptr[i]; k < gp.xptr[i + 1]; k++) w += gp.xval[k] * cg_rnext(qg[gp.xcol[k]], fa, fb, sn);
   return w;
+}
+
+// the first residual pass of a solve: the scaled FP32 entries of row i,
+// a_ij s_i s_j (0 on padding)
+template <bool C16>
+__device__ __forceinline__ void grid_scale_row(const Dev &d, const GridPlan &gp, int i) {
+  int c[8];
+  ell_cols<C16>(gp, i, c);
+  const double sdi = (double)gp.sd[i];
+  float v[8];
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const int slot = __ldg(&gp.eslot[8 * i + k]);
+    v[k] = slot >= 0 ? (float)(d.val64[slot] * sdi * (double)gp.sd[c[k]]) : 0.f;
+  }
+  reinterpret_cast<float4 *>(gp.eval)[2 * i] = make_float4(v[0], v[1], v[2], v[3]);
+  reinterpret_cast<float4 *>(gp.eval)[2 * i + 1] = make_float4(v[4], v[5], v[6], v[7]);
+  if (gp.nx)
+    for (int k = gp.xptr[i]; k < gp.xptr[i + 1]; k++)
+      gp.xval[k] = (float)(d.val64[gp.xslot[k]] * sdi * (double)gp.sd[gp.xcol[k]]);
 }
 
 // FP64 residual of one row: rhs - A*x
@@ -180,16 +207,15 @@ __device__ __forceinline__ double grid_resid_row(const Dev &d, int i) {
 // to 16 bytes; the arrays carry the slack) and moves a multiple of 16 bytes.
 // ---------------------------------------------------------------------------
 struct StageLayout {   // byte offsets inside one buffer
-  int row, col, val, q4, ev, bytes;
+  int col, val, q4, ev, bytes;
 };
 
-// cb: bytes per column index (2 or 4)
-__host__ __device__ inline StageLayout stage_layout(int nzcap, int cb) {
+// cb: bytes of one row's column block (16 for 16-bit offsets, 32 absolute)
+__host__ __device__ inline StageLayout stage_layout(int cb) {
   StageLayout L;
-  L.row = 0;
-  L.col = L.row + (kGridTileRows + 8) * 4;
-  L.val = L.col + (((nzcap + 16) * cb + 15) & ~15);
-  L.q4 = L.val + (((nzcap + 8) * 4 + 15) & ~15);
+  L.col = 0;
+  L.val = L.col + kGridTileRows * cb;
+  L.q4 = L.val + kGridTileRows * 32;
   L.ev = L.q4 + kGridTileRows * 16;
   L.bytes = (L.ev + (kGridTileRows + 8) * 4 + 127) & ~127;
   return L;
@@ -204,25 +230,22 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, int byte
                ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
 }
 
-// thread 0: copy tile rows [a,e), off-diagonal entries [nz0,nz1) into the
-// buffer at sbuf: every range is widened to 16-byte boundaries (the arrays
-// carry the slack), so each copy starts aligned and moves whole 16 bytes
+// thread 0: copy the blocks of tile rows [a,e) into the buffer at sbuf:
+// the column and value blocks and the {r, w, s, p} records are whole
+// 16-byte units per row, the corrections are widened to 16-byte boundaries
+// (the array carries the slack), so each copy starts aligned and moves
+// whole 16 bytes.  Tail entries are read from global memory.
 template <bool C16>
 __device__ __forceinline__ void stage_issue(const GridPlan &gp, const StageLayout &L, uint32_t sbuf, uint32_t mbar,
-                                            int a, int e, int nz0, int nz1, const float4 *qg) {
-  constexpr int CA = C16 ? 8 : 4;                       // column indices per 16 bytes
-  const int ra = a & ~3, rc = ((e + 1 - ra) + 3) & ~3;
-  const int ka = nz0 & ~(CA - 1), kc = ((nz1 - ka) + CA - 1) & ~(CA - 1);
-  const int va = nz0 & ~3, vc = ((nz1 - va) + 3) & ~3;
+                                            int a, int e, const float4 *qg) {
+  constexpr int CB = C16 ? 16 : 32;
   const int ea = a & ~3, ec = ((e - ea) + 3) & ~3;
-  const int cbytes = kc * (C16 ? 2 : 4);
-  const int bytes = rc * 4 + cbytes + vc * 4 + (e - a) * 16 + ec * 4;
+  const int bytes = (e - a) * (CB + 32 + 16) + ec * 4;
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
-  bulk_g2s(sbuf + L.row, gp.optr + ra, rc * 4, mbar);
-  if constexpr (C16) bulk_g2s(sbuf + L.col, gp.ocol16 + ka, cbytes, mbar);
-  else bulk_g2s(sbuf + L.col, gp.ocol32 + ka, cbytes, mbar);
-  bulk_g2s(sbuf + L.val, gp.oval + va, vc * 4, mbar);
+  if constexpr (C16) bulk_g2s(sbuf + L.col, gp.ecol16 + (size_t)8 * a, (e - a) * CB, mbar);
+  else bulk_g2s(sbuf + L.col, gp.ecol32 + (size_t)8 * a, (e - a) * CB, mbar);
+  bulk_g2s(sbuf + L.val, gp.eval + (size_t)8 * a, (e - a) * 32, mbar);
   bulk_g2s(sbuf + L.q4, qg + a, (e - a) * 16, mbar);
   bulk_g2s(sbuf + L.ev, gp.ecor + ea, ec * 4, mbar);
 }
@@ -238,19 +261,32 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
   return false;
 }
 
-// (S A S) r' for one row from a staged tile: entries, and r' of rows inside
-// the tile, from shared memory; r' of rows outside it from global memory
+// (S A S) r' for one row from a staged tile: the row's block, and r' of
+// rows inside the tile, from shared memory; r' of rows outside it and the
+// tail entries from global memory
 template <bool C16>
-__device__ __forceinline__ float staged_spmv_row(const void *scol, const float *sval, int i, int s0, int s1,
-                                                 const float4 *sq, int a, int R, const float4 *qg,
+__device__ __forceinline__ float staged_spmv_row(const GridPlan &gp, const unsigned char *buf, const StageLayout &L,
+                                                 int i, int j, int a, int R, const float4 *sq, const float4 *qg,
                                                  float fa, float fb, float own) {
-  float w = own;
-  for (int m = s0; m < s1; m++) {
-    const int c = C16 ? i + (int)static_cast<const short *>(scol)[m] : static_cast<const int *>(scol)[m];
-    const float4 x = (unsigned)(c - a) < (unsigned)R ? sq[c - a] : qg[c];
-    float sn;
-    w += sval[m] * cg_rnext(x, fa, fb, sn);
+  int c[8];
+  if constexpr (C16) {
+    const short *sc = reinterpret_cast<const short *>(buf + L.col) + 8 * j;
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] = i + (int)sc[k];
+  } else {
+    const int *sc = reinterpret_cast<const int *>(buf + L.col) + 8 * j;
+#pragma unroll
+    for (int k = 0; k < 8; k++) c[k] = sc[k];
   }
+  const float *sv = reinterpret_cast<const float *>(buf + L.val) + 8 * j;
+  float w = own, sn;
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    const float4 x = (unsigned)(c[k] - a) < (unsigned)R ? sq[c[k] - a] : qg[c[k]];
+    w += sv[k] * cg_rnext(x, fa, fb, sn);
+  }
+  if (gp.nx)
+    for (int k = gp.xptr[i]; k < gp.xptr[i + 1]; k++) w += gp.xval[k] * cg_rnext(qg[gp.xcol[k]], fa, fb, sn);
   return w;
 }
 
@@ -313,7 +349,6 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
   __shared__ GridState gs[kGridMaxSlots];
   __shared__ int4 s_tile[kGridMaxTiles];
   __shared__ int s_tid[kGridMaxTiles];
-  __shared__ int2 s_tnz[STAGED ? kGridMaxTiles : 1];
   __shared__ double wred[kGridMaxTiles * NW * 3];
   __shared__ int s_ok;
   __shared__ unsigned s_act;
@@ -323,7 +358,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
   const int nslot = gp.cnslot[c];
   const int t0 = gp.cptr[c], ntl = gp.cptr[c + 1] - t0;   // this CTA's tiles: clist[t0 ..]
   unsigned bar = 0;
-  const StageLayout SL = stage_layout(gp.nzcap, C16 ? 2 : 4);
+  const StageLayout SL = stage_layout(C16 ? 16 : 32);
   uint32_t mbar[2] = {0u, 0u}, sbuf[2] = {0u, 0u}, phase[2] = {0u, 0u};
   if (STAGED) {
     mbar[0] = smem_u32(dsm); mbar[1] = mbar[0] + 8;
@@ -348,7 +383,6 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
     const int t = gp.clist[t0 + tid];
     s_tid[tid] = t;
     s_tile[tid] = gp.tile[t];
-    if constexpr (STAGED) s_tnz[tid] = gp.tnz[t];
   }
   if (blockIdx.x == 0 && tid == 0 && d.imax) { *d.imax = 0; *d.subj = 0; }
   __syncthreads();
@@ -387,8 +421,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
       while (iq < ntl && !staged_stage(gs[s_tile[iq].w].stage)) iq++;
       if (iq < ntl) {
         const int4 tl = s_tile[iq];
-        const int2 nz = s_tnz[iq];
-        stage_issue<C16>(gp, SL, sbuf[b], mbar[b], tl.x, tl.y, nz.x, nz.y, d.cg4[gs[tl.w].cur]);
+        stage_issue<C16>(gp, SL, sbuf[b], mbar[b], tl.x, tl.y, d.cg4[gs[tl.w].cur]);
         iq++;
       }
     };
@@ -419,12 +452,6 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
         }
         phase[b] ^= 1u;
         const unsigned char *buf = dsm + 128 + (size_t)b * SL.bytes;
-        const int2 nz = s_tnz[q];
-        constexpr int CA = C16 ? 8 : 4;
-        const int *srow = reinterpret_cast<const int *>(buf + SL.row) + (a - (a & ~3));
-        const void *scol = C16 ? (const void *)(reinterpret_cast<const short *>(buf + SL.col) + (nz.x - (nz.x & ~(CA - 1))))
-                               : (const void *)(reinterpret_cast<const int *>(buf + SL.col) + (nz.x - (nz.x & ~(CA - 1))));
-        const float *sval = reinterpret_cast<const float *>(buf + SL.val) + (nz.x - (nz.x & ~3));
         const float4 *sq = reinterpret_cast<const float4 *>(buf + SL.q4);
         const float *sev = reinterpret_cast<const float *>(buf + SL.ev) + (a - (a & ~3));
         const float4 *qi = d.cg4[g.cur];
@@ -437,8 +464,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
           const float4 me = sq[j];
           if (stage == G_SPMV0) {
             // w = (S A S) r (fa = fb = 0 leave r)
-            const float w = staged_spmv_row<C16>(scol, sval, i, srow[j] - nz.x, srow[j + 1] - nz.x, sq, a, R, qi,
-                                                 0.f, 0.f, me.x);
+            const float w = staged_spmv_row<C16>(gp, buf, SL, i, j, a, R, sq, qi, 0.f, 0.f, me.x);
             qo[i] = make_float4(me.x, w, 0.f, 0.f);
             v[0] += (double)me.x * me.x;
             v[1] += (double)w * me.x;
@@ -447,8 +473,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
             const float p = me.x + fb * me.w;
             float sn;
             const float rn = cg_rnext(me, fa, fb, sn);
-            const float w = staged_spmv_row<C16>(scol, sval, i, srow[j] - nz.x, srow[j + 1] - nz.x, sq, a, R, qi,
-                                                 fa, fb, rn);
+            const float w = staged_spmv_row<C16>(gp, buf, SL, i, j, a, R, sq, qi, fa, fb, rn);
             qo[i] = make_float4(rn, w, sn, p);
             gp.ecor[i] = sev[j] + fa * p;
             v[0] += (double)rn * rn;
@@ -468,9 +493,7 @@ __global__ void __launch_bounds__(NT, STAGED ? 1 : 2) k_zeta_grid(Dev d, ZetaArg
         for (int i = a + tid; i < e; i += nth) {
           const double t = grid_resid_row(d, i);
           const double sdi = (double)gp.sd[i];
-          if (scale)
-            for (int k = gp.optr[i]; k < gp.optr[i + 1]; k++)
-              gp.oval[k] = (float)(d.val64[gp.oslot[k]] * sdi * (double)gp.sd[ocol<C16>(gp, i, k)]);
+          if (scale) grid_scale_row<C16>(d, gp, i);
           const float rs = (float)(sdi * t);
           qo[i] = make_float4(rs, 0.f, 0.f, 0.f);
           gp.ecor[i] = 0.f;

@@ -60,21 +60,26 @@ struct GridPlan {
   const int4 *tile = nullptr;
   const int2 *btile = nullptr;
   const int *cslot = nullptr, *cnslot = nullptr, *cowner = nullptr;
-  const int2 *tnz = nullptr;       // per tile: its off-diagonal entries optr[row0] .. optr[row1]
   const int *cptr = nullptr;       // CTA c works tiles clist[cptr[c]] .. clist[cptr[c+1]-1]
   const int *clist = nullptr;
-  int nzcap = 0;                   // most off-diagonal entries of any tile (staged buffer size)
   // the Jacobi-scaled system the FP32 iterations solve, S A S with S =
-  // D^-1/2: its diagonal is one and is not stored; the off-diagonal entries
-  // in CSR form (row pointers optr, columns as 16-bit offsets j - i when
-  // every offset fits, else absolute), their slots in the full CSR (oslot),
-  // their FP32 values (oval, written by the first residual pass of each
-  // solve), S per row (sd) and the FP32 correction per row (ecor)
-  const int *optr = nullptr;
-  const short *ocol16 = nullptr;
-  const int *ocol32 = nullptr;
-  const int *oslot = nullptr;
-  float *oval = nullptr, *sd = nullptr, *ecor = nullptr;
+  // D^-1/2: its diagonal is one and is not stored.  Each row's first eight
+  // off-diagonal entries sit in a fixed-width block of the row ([8*i + k]):
+  // columns as 16-bit offsets j - i when every offset fits (ecol16), else
+  // absolute (ecol32), padded with offset 0 / column i and value 0; rows
+  // with more entries keep the rest in a CSR tail (xptr, xcol; nx entries
+  // in all, 0: none).  The entries' slots in the full CSR (eslot, -1 on
+  // padding, xslot), their FP32 values (eval, xval: written by the first
+  // residual pass of each solve), S per row (sd) and the FP32 correction
+  // per row (ecor).
+  const short *ecol16 = nullptr;
+  const int *ecol32 = nullptr;
+  const int *eslot = nullptr;
+  float *eval = nullptr;
+  const int *xptr = nullptr, *xcol = nullptr, *xslot = nullptr;
+  float *xval = nullptr;
+  int nx = 0;
+  float *sd = nullptr, *ecor = nullptr;
   double *partial = nullptr;       // [2][ntile][4] partial sums of the tiles
   unsigned *ctr = nullptr;         // [8]: barrier arrivals, 3 active counts, abort flag, release
   unsigned phantom = 0;            // arrivals the barrier waits for beyond its CTAs (0; 1 in the timeout test)
@@ -105,8 +110,8 @@ cudaError_t launch_zeta_grid(const Dev &d, const ZetaArgs &za, const GridPlan &g
                              size_t smem, cudaStream_t st);
 // CTAs of k_zeta_grid that fit the device at once (0 on error)
 int zeta_grid_capacity(bool staged, size_t smem);
-// dynamic shared memory of the staged form for tiles of at most nzcap entries
-size_t zeta_grid_stage_smem(int nzcap, bool c16);
+// dynamic shared memory of the staged form (16-bit or absolute columns)
+size_t zeta_grid_stage_smem(bool c16);
 int zeta_grid_max_slots();   // basins one CTA can hold
 int zeta_grid_max_tiles();   // tiles one CTA can hold
 int zeta_grid_tile_rows();   // rows per tile

@@ -13,7 +13,7 @@ __device__ __forceinline__ void set_status(BasinOut *o, int code) {
 // UNESCO 1981 equation of state (Millero & Poisson 1981; Fofonoff & Millard
 // 1983), the formulation of sigma_stp (eq_state.f90:154-230): density at one
 // atmosphere and secant bulk modulus; p in bar; returns rho - 1000.
-__device__ double sigma_stp_d(double s, double t, double p) {
+__device__ inline double sigma_stp_d(double s, double t, double p) {
   double t2 = t * t, t3 = t2 * t, t4 = t3 * t, t5 = t4 * t;
   double s32 = sqrt(s * s * s);
   double rw = 999.842594 + 6.793952e-2 * t - 9.095290e-3 * t2 + 1.001685e-4 * t3

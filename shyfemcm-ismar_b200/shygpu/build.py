@@ -16,8 +16,9 @@ PKG = HERE.parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = HERE / "libshygpu.so"
-SOURCES = ["step.cu", "host.cu", "static_solve.cu", "serve.cu"]
-HEADERS = ["common.cuh", "launch.h", "physics.cuh", "k_column.cuh", "k_column_t.cuh", "k_final.cuh", "k_node.cuh", "k_conz.cuh", "k_zeta.cuh", "k_wetdry.cuh", "k_zeta_global.cuh", "k_zeta_grid.cuh"]
+SOURCES = ["step_node32.cu", "step_node16.cu", "step_zeta.cu", "step_node.cu", "step.cu", "host.cu",
+           "static_solve.cu", "serve.cu"]
+HEADERS = ["common.cuh", "launch.h", "physics.cuh", "node_launch.cuh", "k_column.cuh", "k_column_t.cuh", "k_final.cuh", "k_node.cuh", "k_conz.cuh", "k_zeta.cuh", "k_wetdry.cuh", "k_zeta_global.cuh", "k_zeta_grid.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
