@@ -10,9 +10,11 @@ per-basin perturbation of sigma 3 m/s, dt = 60 s; seeded synthetic input of
 that shape (no dataset ships with the reference).  All basins advance in
 one CUDA-graph step.  One bench "step" is one model time step (hydro, the
 body of shyfem_run's loop) of every basin.  Beside it the line reports the
-plain single-run form: the same basins advanced one model at a time, and
-the accuracy of the timed run: the first `--check-steps` steps of its
-smallest, median and largest basins against the FP64 oracle.
+plain single-run form: the same basins advanced one model at a time (each
+with the default launch plan), and the accuracy of the timed run: the
+first `--check-steps` steps of its smallest, median and largest basins
+against the FP64 oracle.  The timed model's launch shapes are chosen first
+by the library's autotuner (shygpu_autotune) on the same basins.
 
 `--workload basin3d` times the 3D baroclinic basin instead (~20k nodes, 20
 z-layers, temperature and salinity transported, dt = 120 s).
@@ -60,6 +62,7 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--check-steps", type=int, default=60,
                    help="steps of the accuracy check against the oracle (0: none)")
+    p.add_argument("--no-tune", action="store_true", help="keep the default launch plan (no shygpu_autotune)")
     return p.parse_args()
 
 
@@ -517,6 +520,14 @@ def main():
     model = shygpu.Model(case_list)
     model.set_state_all()
     stream = torch.cuda.ExternalStream(model.stream())
+    # the launch shapes chosen by the library's autotuner on these basins
+    # (its trials start from the initial state and leave it unchanged)
+    tuning = None
+    if not a.no_tune:
+        t0 = time.perf_counter()
+        choice, tms = model.autotune(steps=4)
+        tuning = {"choice": choice, "ms_per_step": tms, "seconds": time.perf_counter() - t0,
+                  "by": "shygpu_autotune (trials of the candidate plans on the timed basins)"}
     check_gpu = None
     if check_pool is not None:
         # the first steps of the timed run itself, read back before timing
@@ -672,6 +683,7 @@ def main():
                      "achieved_design_bytes": (algo["zeta"] / (dom_ms / dom_n / 1000.0) / 1e9)
                      if dom == "zeta" else None},
         "accuracy": check,
+        "tuning": tuning,
         "kernels": kernels,
         "solver": {"krylov_iters_last_step": infos[0].krylov_iters,
                    "refinements": infos[0].refinements, "resid": infos[0].resid},

@@ -313,11 +313,31 @@ int shygpu_set_bound_scalar(shygpu_model *model, int32_t ibasin, int32_t what,
  * refinement sweeps), "symmetric" (CG instead of BiCGStab; refused when
  * Coriolis makes the system non-symmetric), "column_threads" (1 one thread
  * per element column for up to 16 layers, 0 one warp segment),
+ * "zeta_tile_rows" (rows per tile of the device-wide solver, default 1024),
  * "zeta_barrier_timeout_test" (failure detection: the device-wide solve's
  * barrier waits for an arrival that never comes and reports SHY_ECUDA).
  * Every change rebuilds the step graphs at the next step.                  */
 int shygpu_set_option(shygpu_model *model, const char *name, double value);
 double shygpu_get_option(shygpu_model *model, const char *name);
+
+/* Autotuning of the launch shapes on the model's own basins (no counterpart
+ * in the reference, which runs on CPU cores).  Candidates are sets of the
+ * options above: the zeta solver's plan (zeta_variant, zeta_tile_rows,
+ * zeta_stage; symmetric systems without wetting and drying), the column
+ * kernels' form (column_threads; at most 16 layers) and the FP32 sweep's
+ * tolerance (inner_tol_frac).  Each trial starts from the model's current
+ * state (a host checkpoint), runs one untimed step and times `steps`
+ * steps; the search takes one group at a time over the best of the groups
+ * before it.  The model keeps the fastest candidate's options and the state
+ * it had.  The winner is cached per model shape (basins, rows to two
+ * digits, layers, solver, scalars, device) for the process, and appended to
+ * the file named by the environment variable SHYGPU_TUNE_FILE, if set, which
+ * later processes read; a cached shape is applied without trials.  choice
+ * (optional) receives the options as "name=value ...", ms_per_step
+ * (optional) the winner's time per step (-1 when it came from the cache).
+ * get_option(model, "tuned") is 1 afterwards.                             */
+int shygpu_autotune(shygpu_model *model, int32_t steps, char *choice, int32_t choice_len,
+                    double *ms_per_step);
 
 /* The CUDA stream every launch of the model goes to (cudaStream_t).      */
 void *shygpu_model_stream(shygpu_model *model);

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <string>
 #include <condition_variable>
+#include <map>
 #include <mutex>
 #include <queue>
 #include <thread>
@@ -289,6 +290,8 @@ struct shygpu_model {
   int nsub = 2, use_graph = 1, max_outer = 12, sym = 1;
   int zvariant = 1;                  // 1: shared-memory zeta solver when it fits
   int zstage = 0;                    // device-wide solver: 1 TMA-staged tiles when they fit
+  int ztile_rows = 0;                // device-wide solver: rows per tile (0: the default)
+  std::string tuned;                 // the options shygpu_autotune chose ("" before)
   int zbar_test = 0;                 // device-wide solver: 1 makes every grid barrier time out
   int zforce_CL = 0, zforce_threads = 0;   // > 0: one launch class with this shape
   std::vector<ZetaClass> zcl;        // launch classes of the zeta solver
@@ -392,7 +395,7 @@ static int build_grid_class(shygpu_model *m) {
   const size_t nx = xcol.size();
   std::vector<int4> tile;
   std::vector<int2> btile(m->nbasin, make_int2(0, 0));
-  const int TR = zeta_grid_tile_rows();
+  const int TR = m->ztile_rows > 0 ? m->ztile_rows : zeta_grid_tile_rows();
   for (int b = 0; b < m->nbasin; b++) {
     const BasinPar &bp = m->par[b];
     btile[b].x = (int)tile.size();
@@ -1188,8 +1191,23 @@ extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value
     ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
   }
   else if (n == "zeta_stage") {   // device-wide solver: 1 TMA-staged tiles, 0 global loads
+    if (iv && m->ztile_rows > zeta_grid_tile_rows())
+      return fail(SHY_EARG, "zeta_stage: staged tiles hold at most %d rows", zeta_grid_tile_rows());
     m->zstage = iv != 0;
     ST_TRY(build_zeta_plan(m, m->zforce_CL, m->zforce_threads));
+  }
+  else if (n == "zeta_tile_rows") {   // device-wide solver: rows per tile (0: the default)
+    if (iv != 0 && (iv < 128 || iv > 8192 || iv % 32)) return fail(SHY_EARG, "zeta_tile_rows: multiple of 32 in 128..8192");
+    if (iv > zeta_grid_tile_rows() && m->zstage)
+      return fail(SHY_EARG, "zeta_tile_rows: staged tiles hold at most %d rows", zeta_grid_tile_rows());
+    const int old_rows = m->ztile_rows;
+    m->ztile_rows = iv;
+    if (int st = build_zeta_plan(m, m->zforce_CL, m->zforce_threads)) {
+      m->ztile_rows = old_rows;
+      drop_graphs(m);
+      build_zeta_plan(m, m->zforce_CL, m->zforce_threads);
+      return st;
+    }
   }
   else if (n == "column_threads") {   // 1: one thread per column when it has at most 16 layers
     m->base.col_threads = iv != 0;
@@ -1226,6 +1244,8 @@ extern "C" double shygpu_get_option(shygpu_model *m, const char *name) {
   if (n == "zeta_variant") return m->zcl.empty() ? -1 : (m->zcl[0].grid ? 2 : (m->zcl[0].sm ? 1 : 0));
   if (n == "zeta_grid_ctas") return m->zcl.empty() ? -1 : m->zcl[0].G;
   if (n == "zeta_stage") return m->zcl.empty() || !m->zcl[0].grid ? m->zstage : (m->zcl[0].staged ? 1 : 0);
+  if (n == "zeta_tile_rows") return m->ztile_rows > 0 ? m->ztile_rows : zeta_grid_tile_rows();
+  if (n == "tuned") return m->tuned.empty() ? 0 : 1;
   if (n == "launches_per_step") return m->launches_per_step;
   return -1;
 }
@@ -2030,6 +2050,181 @@ extern "C" int shygpu_profile_steps(shygpu_model *m, int32_t nsteps, double *ms_
   if (st) return st;
   CUDA_TRY(cudaGetLastError());
   return check_outputs(m);
+}
+
+// ---------------------------------------------------------------------------
+// Autotuning of the launch shapes (no counterpart in the reference, which
+// runs on CPU cores).  A candidate is a set of options; each trial loads the
+// same host checkpoint of the model, runs one untimed step (which builds the
+// step graphs) and times `steps` steps with CUDA events on the model's
+// stream.  The search takes one group of options at a time (the zeta
+// solver's plan, the column kernels' form, the FP32 sweep's tolerance), each
+// over the best of the groups before it, and keeps the fastest candidate
+// that ran without error.  The model is left with the winner's options and
+// its state as it was before.  Winners are cached per model shape for the
+// rest of the process, and in the file SHYGPU_TUNE_FILE names, if any.
+// ---------------------------------------------------------------------------
+namespace {
+struct TuneOpt { const char *name; double value; };
+typedef std::vector<TuneOpt> TuneSet;
+std::mutex g_tune_mu;
+std::map<std::string, std::string> g_tune_cache;
+bool g_tune_file_read = false;
+
+std::string tune_key(const shygpu_model *m) {
+  // what decides the winner: basins, total rows to two digits, layers, the
+  // solver's symmetry, Coriolis, wetting and drying, transported scalars,
+  // and the device
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  long long rows = m->NKN, scale = 1;
+  while (rows >= 100) { rows /= 10; scale *= 10; }
+  char k[256];
+  snprintf(k, sizeof k, "nbasin=%d rows=%lld nlv=%d sym=%d cor=%d wd=%d nsc=%d sm=%d", m->nbasin, rows * scale,
+           m->NLV, (int)m->sym, (int)m->cor, (int)m->any_wd, m->nsc_max, nsm);
+  return k;
+}
+
+std::string tune_string(const TuneSet &t) {
+  std::string out;
+  for (const TuneOpt &o : t) {
+    char b[96];
+    snprintf(b, sizeof b, "%s%s=%g", out.empty() ? "" : " ", o.name, o.value);
+    out += b;
+  }
+  return out;
+}
+
+void tune_file_load() {
+  const char *fn = getenv("SHYGPU_TUNE_FILE");
+  g_tune_file_read = true;
+  if (!fn) return;
+  FILE *f = fopen(fn, "r");
+  if (!f) return;
+  char line[1024];
+  while (fgets(line, sizeof line, f)) {
+    char *tab = strchr(line, '\t');
+    if (!tab) continue;
+    *tab = 0;
+    std::string v(tab + 1);
+    while (!v.empty() && (v.back() == '\n' || v.back() == '\r')) v.pop_back();
+    g_tune_cache[line] = v;
+  }
+  fclose(f);
+}
+
+void tune_file_store(const std::string &key, const std::string &choice) {
+  const char *fn = getenv("SHYGPU_TUNE_FILE");
+  if (!fn) return;
+  FILE *f = fopen(fn, "a");
+  if (!f) return;
+  fprintf(f, "%s\t%s\n", key.c_str(), choice.c_str());
+  fclose(f);
+}
+}  // namespace
+
+// apply "name=value name=value ..." through shygpu_set_option
+static int apply_options(shygpu_model *m, const std::string &choice) {
+  size_t i = 0;
+  while (i < choice.size()) {
+    size_t j = choice.find(' ', i);
+    if (j == std::string::npos) j = choice.size();
+    const std::string item = choice.substr(i, j - i);
+    const size_t eq = item.find('=');
+    if (eq != std::string::npos) ST_TRY(shygpu_set_option(m, item.substr(0, eq).c_str(), atof(item.c_str() + eq + 1)));
+    i = j + 1;
+  }
+  return SHY_OK;
+}
+
+// one trial: the checkpoint, one untimed step, `steps` timed steps
+static int tune_trial(shygpu_model *m, const std::vector<char> &ck, int steps, float *ms) {
+  ST_TRY(shygpu_checkpoint_load(m, ck.data(), (int64_t)ck.size()));
+  ST_TRY(shygpu_enqueue(m, 1));
+  ST_TRY(check_outputs(m));
+  cudaEvent_t a, b;
+  CUDA_TRY(cudaEventCreate(&a));
+  CUDA_TRY(cudaEventCreate(&b));
+  int st = SHY_OK;
+  if (cudaEventRecord(a, m->stream) != cudaSuccess) st = fail(SHY_ECUDA, "autotune: event record failed");
+  if (!st) st = shygpu_enqueue(m, steps);
+  if (!st && cudaEventRecord(b, m->stream) != cudaSuccess) st = fail(SHY_ECUDA, "autotune: event record failed");
+  if (!st) st = check_outputs(m);
+  float t = 0.f;
+  if (!st && cudaEventElapsedTime(&t, a, b) != cudaSuccess) st = fail(SHY_ECUDA, "autotune: event timing failed");
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  *ms = t / (float)steps;
+  return st;
+}
+
+extern "C" int shygpu_autotune(shygpu_model *m, int32_t steps, char *choice, int32_t choice_len,
+                               double *ms_per_step) {
+  if (!m || steps < 1) return fail(SHY_EARG, "autotune: bad arguments");
+  if (!m->state_set) return fail(SHY_ESTATE, "autotune: set_state has not been called");
+  const std::string key = tune_key(m);
+  std::string cached;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    if (!g_tune_file_read) tune_file_load();
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) cached = it->second;
+  }
+  double best_ms = -1.;
+  if (!cached.empty()) {
+    ST_TRY(apply_options(m, cached));
+    m->tuned = cached;
+  } else {
+    std::vector<char> ck((size_t)shygpu_checkpoint_bytes(m));
+    ST_TRY(shygpu_checkpoint_save(m, ck.data(), (int64_t)ck.size()));
+    // the groups; each candidate sets every option of its group
+    std::vector<std::vector<TuneSet>> groups;
+    if (m->sym && !m->any_wd) {
+      groups.push_back({
+          {{"zeta_stage", 0}, {"zeta_tile_rows", 1024}, {"zeta_variant", 1}},
+          {{"zeta_stage", 0}, {"zeta_tile_rows", 512}, {"zeta_variant", 2}},
+          {{"zeta_stage", 0}, {"zeta_tile_rows", 1024}, {"zeta_variant", 2}},
+          {{"zeta_stage", 0}, {"zeta_tile_rows", 2048}, {"zeta_variant", 2}},
+          {{"zeta_stage", 1}, {"zeta_tile_rows", 1024}, {"zeta_variant", 2}},
+          {{"zeta_stage", 0}, {"zeta_tile_rows", 1024}, {"zeta_variant", 0}},
+      });
+    }
+    if (m->NLV <= 16 && !m->any_wd) groups.push_back({{{"column_threads", 1}}, {{"column_threads", 0}}});
+    groups.push_back({{{"inner_tol_frac", 0.5}}, {{"inner_tol_frac", 0.75}}, {{"inner_tol_frac", 0.9}}});
+    TuneSet chosen;
+    for (const auto &g : groups) {
+      const TuneSet *win = nullptr;
+      float win_ms = 0.f;
+      for (const TuneSet &cand : g) {
+        TuneSet all(chosen);
+        all.insert(all.end(), cand.begin(), cand.end());
+        float ms = 0.f;
+        int st = apply_options(m, tune_string(all));
+        if (!st) st = tune_trial(m, ck, steps, &ms);
+        if (!st && (!win || ms < win_ms)) { win = &cand; win_ms = ms; }
+      }
+      if (!win) {
+        apply_options(m, tune_string(chosen));
+        shygpu_checkpoint_load(m, ck.data(), (int64_t)ck.size());
+        return fail(SHY_ECUDA, "autotune: no candidate of a group ran");
+      }
+      chosen.insert(chosen.end(), win->begin(), win->end());
+      best_ms = win_ms;
+    }
+    ST_TRY(apply_options(m, tune_string(chosen)));
+    ST_TRY(shygpu_checkpoint_load(m, ck.data(), (int64_t)ck.size()));
+    m->tuned = tune_string(chosen);
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = m->tuned;
+    tune_file_store(key, m->tuned);
+  }
+  if (choice && choice_len > 0) {
+    strncpy(choice, m->tuned.c_str(), (size_t)choice_len - 1);
+    choice[choice_len - 1] = 0;
+  }
+  if (ms_per_step) *ms_per_step = best_ms;
+  return SHY_OK;
 }
 
 extern "C" int shygpu_get_wetdry(shygpu_model *m, int32_t ib, int32_t *iwegv, int32_t *iwetv, int32_t *inodv) {

@@ -76,6 +76,7 @@ def lib():
     L.shygpu_get_wetdry.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3
     L.shygpu_set_nudging.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     L.shygpu_set_bound_scalar.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
+    L.shygpu_autotune.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_double)]
     L.shygpu_conz3d.argtypes = ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_float,
                                  C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int32, C.c_int32,
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_float,
@@ -224,6 +225,16 @@ class Model:
         a = np.ascontiguousarray(andgzv, np.float32)
         check(lib().shygpu_set_nudging(self.h, ib, a.ctypes.data), "set_nudging")
         lib().shygpu_sync(self.h)
+
+    def autotune(self, steps=5):
+        """shygpu_autotune: time the candidate launch shapes on this model's
+        basins from its current state and keep the fastest; returns (the
+        chosen options as "name=value ...", ms per step of the winner or -1
+        when the shape was cached)."""
+        buf = C.create_string_buffer(512)
+        ms = C.c_double(0.0)
+        check(lib().shygpu_autotune(self.h, int(steps), buf, 512, C.byref(ms)), "autotune")
+        return buf.value.decode(), ms.value
 
     def set_bound_scalar(self, ib, what, values, itr=0):
         """Boundary values (nkn, nlv) of a scalar of basin ib (what: 0
