@@ -147,6 +147,11 @@ typedef struct shy_step_info {
   double resid;          /* final ||b - A z|| (FP64)                       */
   double volume;         /* total water volume, FP64 sum (vol_mass)        */
   double dtime;          /* model time of the state [s]                    */
+  double volume_budget;  /* FP64 volume budget: the initial volume plus    */
+                         /*   every step's dt times the flows into the     */
+                         /*   node columns (element fluxes of the zeta     */
+                         /*   equation, discharges), summed in FP64, so a  */
+                         /*   closed basin keeps it to FP64 round-off      */
 } shy_step_info;
 
 typedef struct shygpu_model shygpu_model;   /* opaque, device-resident    */

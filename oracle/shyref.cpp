@@ -1861,6 +1861,7 @@ int init_state(Model &m) {
   if (m.p.ibarcl > 0) for (int it = 0; it < 3; it++) rhoset(m);   // barocl(0): rhoset_shell(3)
   uvtopr(m);                                      // make_prvel (initialize.f90:1656)
   m.info.volume = masscont(m);
+  m.info.volume_budget = m.info.volume;   // the FP64 state's own volume is its budget
   m.tbnd = m.tempv; m.sbnd = m.saltv; m.cbnd = m.conzv;   // boundary values: initial columns
   return SHY_OK;
 }
@@ -1915,6 +1916,7 @@ int step(Model &m) {
   hydro_vertical(m);
   uvtopr(m);                                      // compute_velocities (hydrodynamic.f90:473)
   m.info.volume = masscont(m);                    // vol_mass(1)
+  m.info.volume_budget = m.info.volume;           // the FP64 state's own volume is its budget
   // run_scalar (shyfem_subs.f90:975-1028): T and S, then rho, then tracers
   int istot = 1;
   if (m.p.itemp) { st = scal3sh(m, m.tempv, m.p.thpar, true, m.tbnd, &istot); if (st) return st; }

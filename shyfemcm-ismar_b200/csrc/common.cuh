@@ -77,6 +77,7 @@ struct BasinOut {
   double dtime;
   double resid0, resid;
   double volume;
+  double vbudget;             // FP64 volume budget summed over the nodes (k_reduce)
   int status;
   int iters, refinements;
   int istot;
@@ -154,6 +155,8 @@ struct Dev {
   float *scr0, *scr1;         // intermediate transport sub-steps
   float *cbnd;                // boundary values of the scalars, same layout
   double *vol_node;           // [k]
+  double *vbud_node;          // [k] FP64 volume budget: the initial volume plus dt times every
+                              //     step's flow into the node column (element fluxes, discharge)
   float *stab_node;           // [s*NKN + k]
   int *imax;                  // largest transport sub-step count of the step (all basins)
   int *subj;                  // sub-step index of the device-driven sub-step loop

@@ -1109,7 +1109,7 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       A.alloc(&d.cg4[1], NKN) || A.alloc(&d.cg2, NKN + 2) || A.alloc(&d.hia, (size_t)12 * NEL) || A.alloc(&d.unv, NEL) || A.alloc(&d.vnv, NEL) ||
       A.alloc(&d.usv, EL) || A.alloc(&d.vsv, EL) ||
       A.alloc(&d.wl, (size_t)NKN * (NLV + 1)) || A.alloc(&d.rho, NL) || A.alloc(&d.ddx, EL) ||
-      A.alloc(&d.ddxi, m->cor ? EL : 1) || A.alloc(&d.cbnd, NSC) || A.alloc(&d.vol_node, NKN) ||
+      A.alloc(&d.ddxi, m->cor ? EL : 1) || A.alloc(&d.cbnd, NSC) || A.alloc(&d.vol_node, NKN) || A.alloc(&d.vbud_node, NKN) ||
       A.alloc(&d.scr0, nsc_max > 0 ? NSC : 1) || A.alloc(&d.scr1, nsc_max > 0 ? NSC : 1) ||
       A.alloc(&d.imax, 1) || A.alloc(&d.subj, 1) || A.alloc(&d.nsub_launched, 1) ||
       A.alloc(&d.stab_node, 1))
@@ -2255,6 +2255,7 @@ extern "C" int shygpu_step_info(shygpu_model *m, int32_t ib, shy_step_info *info
   info->resid0 = o.resid0;
   info->resid = o.resid;
   info->volume = o.volume;
+  info->volume_budget = o.vbudget;
   info->dtime = o.dtime;
   return SHY_OK;
 }

@@ -6,6 +6,22 @@
 
 namespace shy {
 
+// The FP64 volume budget of a node column: every step adds dt times the flow
+// into it, the element fluxes 3 * 4aj * (U b + V c) of the zeta equation
+// (az-weighted transports summed over the element's layers) and the node's
+// discharge.  The gradients come from the element's FP32 b, c with the last
+// vertex's taken as minus the sum of the other two, so that each element's
+// three fluxes cancel exactly and a closed basin's summed budget moves by
+// FP64 round-off only.
+__device__ __forceinline__ double2 budget_grad(const float *evp, int ii) {
+  if (ii < 2) return make_double2((double)evp[ii], (double)evp[3 + ii]);
+  return make_double2(-((double)evp[0] + (double)evp[1]), -((double)evp[3] + (double)evp[4]));
+}
+
+__device__ __forceinline__ double budget_discharge(const Dev &d, const BasinPar &P, int k) {
+  return (P.wetdry && d.inod[k] == -2) ? 0. : (double)d.rqv[k];
+}
+
 // ===========================================================================
 // k_node: nodal layer thickness, vertical velocity, node volume
 // ===========================================================================
@@ -26,6 +42,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   const float *hlv = d.hlv + (size_t)b * NLV;
   const double hldl = lane < NLV ? (double)hld[lane] : 0.;
   double hsum = 0., vf = 0., va = 0.;
+  double bud = 0.;                            // FP64 budget: this layer's flow into the node
   double hsig_h = 0.;                         // sigma: depth of the last incident element's vertex
 #pragma unroll 2
   for (int p = d.inc_ptr[k]; p < d.inc_ptr[k + 1]; p++) {
@@ -50,6 +67,8 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
       const double aj4 = 4. * aj;
       vf += 3. * aj4 * ff;
       va += aj4;
+      const double2 g = budget_grad(evp, ii);
+      bud += 3. * aj4 * ((double)d.usv[oe] * g.x + (double)d.vsv[oe] * g.y);
     }
   }
   const size_t o = (size_t)k * NLV + lane;
@@ -63,6 +82,11 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   double vol = act ? (double)(hkf * (float)area) : 0.;
   vol = seg_sum<S>(vol);
   if (lane == 0 && valid) d.vol_node[k] = vol;
+  bud = seg_sum<S>(act ? bud : 0.);
+  if (lane == 0 && valid) {
+    if (init_only) d.vbud_node[k] = vol;
+    else d.vbud_node[k] += P.dt * (bud + budget_discharge(d, P, k));
+  }
   if (init_only) return;
   // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771),
   // with the layer's share of the node's discharge (mfluxv, :1727)
@@ -104,6 +128,7 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
   // (setdepth, hydro_vertical); va, the area of the elements with the layer,
   // is static (Dev::avol)
   float hsum[L], vf[L];
+  double bud = 0.;                            // FP64 budget: the flow into the node column
   double hsig_h = 0.;                         // sigma: depth of the last incident element's vertex
 #pragma unroll
   for (int l = 0; l < L; l++) { hsum[l] = 0.f; vf[l] = 0.f; }
@@ -121,6 +146,7 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
     hsig_h = htot;
     // setdepth takes the element's vertex level (a dry element's differs)
     const float ze = P.wetdry ? d.zen[3 * e + ii] : (float)z;
+    double us = 0., vs = 0.;                  // the element's transports summed over its layers
 #pragma unroll
     for (int l = 0; l < L; l++) {
       if (l >= le) break;
@@ -132,7 +158,13 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
       if (!init_only) {
         const float ff = d.usv[oe + l] * bb + d.vsv[oe + l] * cc;   // az*ffn + azt*ffo
         vf[l] += 3.f * areafv * ff;
+        us += (double)d.usv[oe + l];
+        vs += (double)d.vsv[oe + l];
       }
+    }
+    if (!init_only) {
+      const double2 g = budget_grad(evp, ii);
+      bud += 3. * (4. * (double)aj) * (us * g.x + vs * g.y);
     }
   }
   const size_t o = (size_t)k * NLV;
@@ -156,6 +188,8 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
   }
   if (bad) set_status(&d.out[b], SHY_EDEPTH);
   d.vol_node[k] = vol;
+  if (init_only) d.vbud_node[k] = vol;
+  else d.vbud_node[k] += P.dt * (bud + budget_discharge(d, P, k));
   if (init_only) return;
   // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771),
   // with each layer's share of the node's discharge (set_mass_flux: by the
@@ -323,17 +357,25 @@ static __global__ void __launch_bounds__(1024) k_reduce(Dev d, int nsub, int adv
   const int b = blockIdx.x;
   const BasinPar &P = d.par[b];
   BasinOut &O = d.out[b];
-  __shared__ double part[1024];
-  double s = 0.;
-  for (int k = threadIdx.x; k < P.nk; k += blockDim.x) s += d.vol_node[P.k0 + k];
+  __shared__ double part[1024], partb[1024];
+  double s = 0., sb = 0.;
+  for (int k = threadIdx.x; k < P.nk; k += blockDim.x) {
+    s += d.vol_node[P.k0 + k];
+    sb += d.vbud_node[P.k0 + k];
+  }
   part[threadIdx.x] = s;
+  partb[threadIdx.x] = sb;
   __syncthreads();
   for (int w = 512; w > 0; w >>= 1) {
-    if (threadIdx.x < w) part[threadIdx.x] += part[threadIdx.x + w];
+    if (threadIdx.x < w) {
+      part[threadIdx.x] += part[threadIdx.x + w];
+      partb[threadIdx.x] += partb[threadIdx.x + w];
+    }
     __syncthreads();
   }
   if (threadIdx.x == 0) {
     O.volume = part[0];
+    O.vbudget = partb[0];
     if (advance) {
       int mx = 1;
       for (int sc = 0; sc < P.nsc; sc++) {

@@ -65,7 +65,7 @@ class ShyStepInfo(C.Structure):
     _fields_ = [
         ("status", C.c_int32), ("krylov_iters", C.c_int32), ("refinements", C.c_int32),
         ("istot", C.c_int32), ("resid0", C.c_double), ("resid", C.c_double),
-        ("volume", C.c_double), ("dtime", C.c_double),
+        ("volume", C.c_double), ("dtime", C.c_double), ("volume_budget", C.c_double),
     ]
 
 

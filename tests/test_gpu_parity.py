@@ -46,6 +46,7 @@ def test_channel_2d_one_day_tide(channel):
     ig, io = g.info(0), o.info()
     assert abs(ig.dtime - io.dtime) < 1e-6
     assert abs(ig.volume - io.volume) <= 1e-6 * io.volume
+    assert abs(ig.volume_budget - io.volume) <= 1e-6 * io.volume   # the FP64 budget, open boundary
 
 
 @pytest.mark.parametrize("column_threads", [1, 0])

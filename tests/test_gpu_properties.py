@@ -83,3 +83,26 @@ def test_uniform_tracers_stay_uniform(scheme):
             dev = np.abs(a[m] - v).max()
             assert dev <= 5e-6 * v, (c["name"], f, dev)
         g.close()
+
+
+def test_closed_basin_volume_budget_to_fp64_roundoff():
+    """The FP64 volume budget (shy_step_info.volume_budget: the initial
+    volume plus every step's dt times the element fluxes of the zeta
+    equation into each node column) of a closed basin under wind stays at
+    its initial value to FP64 round-off over 1200 steps, while the FP32
+    state's own volume (vol_mass) moves at FP32 round-off; the two agree to
+    FP32 accuracy."""
+    c = cases.basin3d_case(nkn_target=2000, nlv=8, baroclinic=False, ts=False)
+    c["bnd_index"] = np.zeros_like(c["bnd_index"])
+    c["tide"] = np.zeros((0, 1, 4), np.float32)
+    g = shygpu.Model(c)
+    g.set_state(0)
+    i0 = g.info(0)
+    b0, v0 = i0.volume_budget, i0.volume
+    assert b0 == v0
+    g.run(1200)
+    i1 = g.info(0)
+    assert np.abs(g.get_state(0)["znv"]).max() > 0.01        # the wind has moved the water
+    assert abs(i1.volume_budget / b0 - 1.0) <= 1e-12, i1.volume_budget / b0 - 1.0
+    assert abs(i1.volume / v0 - 1.0) <= 1e-5
+    assert abs(i1.volume / i1.volume_budget - 1.0) <= 1e-5
