@@ -114,7 +114,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
 // its layers (in element order, as k_node); then the node's layers in turn
 // ===========================================================================
 template <int L>
-__global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int init_only) {
+__global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int init_only) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.NKN) return;
   const int NLV = d.NLV, I = NLV + 1;
@@ -169,22 +169,21 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
   }
   const size_t o = (size_t)k * NLV;
   double vol = 0.;
-  float hkf[L];
-  double area[L];
+  float hkf[L];                               // the new thickness; the areas are read again below
   bool bad = false;
 #pragma unroll
   for (int l = 0; l < L; l++) {
-    hkf[l] = 0.f; area[l] = 0.;
+    hkf[l] = 0.f;
     if (l >= NLV) continue;
     const bool act = l < lmax;
-    area[l] = act ? (double)d.areakv[o + l] : 0.;
-    double hk = act && area[l] > 0. ? (double)(hsum[l] / (float)area[l]) : 0.;
+    const float areal = act ? d.areakv[o + l] : 0.f;
+    double hk = act && areal > 0.f ? (double)(hsum[l] / areal) : 0.;
     if (l < P.nsigma && act) hk = -(fmin(hsig_h, (double)P.hsigma) + z) * (double)hld[l];   // sigma layers (:1019-1025)
     hkf[l] = (float)hk;
     if (act && !(hkf[l] > 0.f)) bad = true;
     d.hkn[o + l] = act ? hkf[l] : 0.f;
     // node volume (masscont: sum of real hdknv*areakv in double)
-    vol += act ? (double)(hkf[l] * (float)area[l]) : 0.;
+    vol += act ? (double)(hkf[l] * areal) : 0.;
   }
   if (bad) set_status(&d.out[b], SHY_EDEPTH);
   d.vol_node[k] = vol;
@@ -206,8 +205,9 @@ __global__ void __launch_bounds__(128, 4) k_node_t(Dev d, const int *kbas, int i
     const bool act = l < lmax;
     double dv = 0.;
     if (act && P.nlv > 1) {
-      const double voln = (double)(hkf[l] * (float)area[l]);
-      const double volo = (double)(d.hko[o + l] * (float)area[l]);
+      const float areal = d.areakv[o + l];
+      const double voln = (double)(hkf[l] * areal);
+      const double volo = (double)(d.hko[o + l] * areal);
       const float q = vtot > 0. ? (float)((double)rq * ((double)(d.hko[o + l] * d.areakv[o + l]) / vtot)) : 0.f;
       dv = (double)vf[l] + (double)q - (voln - volo) / P.dt;
     }
