@@ -19,6 +19,7 @@ void launch_node_S(const Dev &d, const int *kbas, int which, int a, int b, cudaS
     case 2:   // right-hand sides per PCR: scalars transported together
       if (d.nsc_max <= 1) k_conz<S, 1><<<blocks, threads, 0, st>>>(d, kbas, a);
       else if (d.nsc_max <= 2) k_conz<S, 2><<<blocks, threads, 0, st>>>(d, kbas, a);
+      else if (d.nsc_max <= 3) k_conz<S, 3><<<blocks, threads, 0, st>>>(d, kbas, a);
       else if (d.nsc_max <= 4) k_conz<S, 4><<<blocks, threads, 0, st>>>(d, kbas, a);
       else k_conz<S, kMaxScal><<<blocks, threads, 0, st>>>(d, kbas, a);
       break;
