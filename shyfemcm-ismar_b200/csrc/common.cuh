@@ -92,6 +92,7 @@ struct Dev {
   int any_wd;                   // some basin has wetting and drying (thread-per-column forms)
   float2 *mom;                  // (NKN*NLV) node momentum {momentxv, momentyv} when a basin advects
   int any_tvd;                  // some basin transports with TVD (a gradient pass per sub-step)
+  int any_tvdv;                 // some basin transports with vertical TVD (itvdv = 1)
   float2 *tgrad;                // (nsc_max*NKN*NLV) node gradients {gx, gy} of the sub-step's scalars
   int4 *tvdup;                  // (6*NEL) itvd = 2: {element, xi0, xi1, xi2 as float bits} per vertex pair
   float *andg;                  // (NKN) water-level nudging contribution andgzv, or null (none set)
@@ -102,6 +103,11 @@ struct Dev {
   const float *cz_obs, *cz_tau, *cz_wsv;
   float *cz_load;
   float cz_robs, cz_wsink, cz_rload;
+  // the transport's element part, per element vertex and layer: cz_ef
+  // [((3e + ii) * nsc_max + s) * NLV + l] = 4aj (3 fl - hdif) of scalar s on
+  // concentrations shifted by vertex ii's, cz_ef1 [(3e + ii) * NLV + l] =
+  // 4aj 3 fl of a unit field (the horizontal flow into the vertex)
+  float *cz_ef, *cz_ef1;
   BasinPar *par;
   BasinOut *out;
   // mesh (static)

@@ -730,6 +730,7 @@ static int64_t footprint_of(int nbasin, const shy_basin *B, const shy_params *P,
   if (adv) nd += nkn * NLV * 8;              // node momentum
   if (tvd) nd += nsc * nkn * NLV * 8;        // TVD node gradients
   if (up) el += nel * 96;                    // TVD upwind points
+  if (nsc > 0) el += nel * 3 * (nsc + 1) * NLV * 4;   // the transport's element part
   if (wd) { el += nel * 8; nd += nkn * 5; }  // dry marks, counters, node kinds
   return el + nd + sy;
 }
@@ -1082,6 +1083,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   d.col_threads = 1;
   d.any_wd = m->any_wd ? 1 : 0;
   d.any_tvd = m->any_tvd ? 1 : 0;
+  d.any_tvdv = 0;
+  for (int b = 0; b < nbasin; b++) d.any_tvdv |= Pp[b].itvdv == 1 ? 1 : 0;
   ST_TRY(A.upload(&d.par, m->par) ? bail(SHY_ECAPACITY) : 0);
   std::vector<BasinOut> outs(nbasin);
   memset(outs.data(), 0, sizeof(BasinOut) * nbasin);
@@ -1119,6 +1122,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     return bail(SHY_ECAPACITY);
   if (m->any_adv && A.alloc(&d.mom, (size_t)NKN * NLV)) return bail(SHY_ECAPACITY);
   if (m->any_tvd && A.alloc(&d.tgrad, (size_t)nsc_max * NKN * NLV)) return bail(SHY_ECAPACITY);
+  if (nsc_max > 0 && (A.alloc(&d.cz_ef, (size_t)3 * NEL * nsc_max * NLV) || A.alloc(&d.cz_ef1, (size_t)3 * NEL * NLV)))
+    return bail(SHY_ECAPACITY);
   if (any_up && A.upload(&d.tvdup, tvdup)) return bail(SHY_ECAPACITY);
   for (int i = 0; i < 2; i++) {
     if (A.alloc(&m->zbuf[i], NKN) || A.alloc(&m->zebuf[i], (size_t)3 * NEL) ||
@@ -1391,7 +1396,7 @@ static int enqueue_scalar(shygpu_model *m, Dev d, int sc_cur, int *nconz) {
     d.sc_in = m->scbuf[sc_cur];
     d.sc_out = m->scbuf[1 - sc_cur];
     for (int j = 0; j < imax && j < 1000; j++) launch_substep(m, d, j);
-    *nconz = imax * (m->any_tvd ? 2 : 1);
+    *nconz = imax * (m->any_tvd ? 3 : 2);
     if (m->has_rho) { launch_node(d, m->kbas, 4, 0, 0, m->stream); *nconz += 1; }
   }
   return SHY_OK;
@@ -1605,6 +1610,10 @@ extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1
         A.alloc(&m->cz_par, (size_t)m->nbasin) || A.alloc(&m->cz_outp, (size_t)m->nbasin) ||
         A.alloc(&m->cz_cb, SN))
       return SHY_ECAPACITY;
+    // the element part's buffers, for a model that transports nothing itself
+    if (!m->base.cz_ef && (A.alloc(&m->base.cz_ef, (size_t)3 * m->NEL * NLV) ||
+                           A.alloc(&m->base.cz_ef1, (size_t)3 * m->NEL * NLV)))
+      return SHY_ECAPACITY;
   }
   if (terms && !m->cz_obs) {
     CUDA_TRY(cudaStreamSynchronize(st));
@@ -1639,6 +1648,8 @@ extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1
   Dev d = dev_for_step(m, m->cur);     // the state hydro just produced is "new"
   d.par = m->cz_par; d.out = m->cz_outp;
   d.difhv = m->cz_difhv; d.difv = m->cz_difv; d.tgrad = m->cz_grad;
+  if (itvd >= 1) d.any_tvd = 1;        // the TVD instance of the element part
+  if (itvdv == 1) d.any_tvdv = 1;      // the vertical-TVD instance of the node part
   d.nsc_max = 1; d.conz_free_bnd = 1;
   d.cbnd = cbound ? m->cz_cb : m->cz_in;   // inflow concentration: cbound, or the node's own
   if (robs != 0.f) {
@@ -1655,7 +1666,7 @@ extern "C" int shygpu_conz3d(shygpu_model *m, int32_t ib, float *cn1, float *co1
   if (isact & 1) { d.scr1 = m->cz_in; d.scr0 = m->cz_out; }
   else { d.scr0 = m->cz_in; d.scr1 = m->cz_out; }
   launch_node(d, m->kbas, terms ? 7 : 2, isact - 1, 0, st);
-  g_launches += 1;
+  g_launches += 2;                     // the element part and the node part
   CUDA_TRY(cudaGetLastError());
   ST_TRY(copy_cols(m->cz_out, cn1, bp.nk, nlv, NLV, bp.k0, false, st));
   if (rload != 0.f) ST_TRY(copy_cols(m->cz_load, load, bp.nk, nlv, NLV, bp.k0, false, st));

@@ -6,16 +6,20 @@
 // the level-boundary values of bndo_impbc (bndo.f90:700-760); and rhoset
 // (baroclinic.f90:654-710) once temperature and salinity are final.
 //
-// One warp segment per node column (lane = layer).  In conz3d_element the
-// storage, vertical-diffusion and vertical-advection terms of node k depend
-// on an element e only through its weight aj4 = 4*aj and through whether
-// layer l+1 exists in e (presentl(l+1), and wl(ilevel) = 0 at the element's
+// Two kernels per sub-step.  k_conz_el, one warp segment per element column
+// (lane = layer), computes each element's horizontal fluxes (upwind or TVD)
+// and horizontal diffusion into each of its three vertices for every scalar
+// of the sub-step and writes them per element vertex (Dev::cz_ef).  k_conz,
+// one warp segment per node column, sums them over the node's elements in
+// element order and does the rest.  In conz3d_element the storage,
+// vertical-diffusion and vertical-advection terms of node k depend on an
+// element e only through its weight aj4 = 4*aj and through whether layer
+// l+1 exists in e (presentl(l+1), and wl(ilevel) = 0 at the element's
 // bottom).  Their sum over the elements of k is therefore the node's own
 // column terms weighted by two static sums, A_t = sum of aj4 over elements
 // that continue below layer l and A_f = sum over elements whose bottom layer
-// is l (Dev::avol).  Only the horizontal fluxes (and horizontal diffusion)
-// need the loop over the incident elements.  Scalars with the same sub-step
-// count share that loop and one PCR solve of the vertical system.  FP32.
+// is l (Dev::avol).  Scalars with the same sub-step count share one PCR
+// solve of the vertical system.  FP32.
 //
 // Increment form.  The node layer's system M c' = M_old c + dt F(c) is
 // solved for the increment d = c' - c: every flux is evaluated on the
@@ -171,12 +175,114 @@ __device__ __forceinline__ float tvd_v(float conc, float cond, float conu, float
   return conc + 0.5f * psi * (cond - conc) * (1.f - alfa);
 }
 
+// ===========================================================================
+// k_conz_el: the element part of a sub-step (conz3d_element,
+// concentration_omp.f90:355-755, the horizontal terms :620-690): per element
+// layer and scalar with a sub-step now, the upwind flux (one vertex of
+// outflow, itot 1, or of inflow, itot 2) or the TVD flux (itvd 1, 2; not
+// where a vertex is on an open boundary) into each vertex, and horizontal
+// diffusion through wdifhv, all on concentrations shifted by that vertex's
+// own (the increment form, see k_conz), times 4aj; and the flux of a unit
+// field.  Zero on the layers the element lacks.
+// ===========================================================================
+template <int S, bool TVD>
+__global__ void __launch_bounds__(256) k_conz_el(Dev d, int j_arg) {
+  const int j = j_arg >= 0 ? j_arg : *d.subj;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int e = gt / S;
+  const int lane = threadIdx.x & (S - 1);
+  const int NLV = d.NLV;
+  if (e >= d.NEL || lane >= NLV) return;       // no shuffles in this kernel
+  const int4 en = d.enode[e];
+  const BasinPar &P = d.par[en.w];
+  const BasinOut &O = d.out[en.w];
+  const int nsc = P.nsc, isact = j + 1;
+  bool any = false;
+  for (int s = 0; s < nsc; s++) any |= isact <= (int)O.stab[s];
+  if (!any) return;
+  const bool act = lane < d.ilhv[e];
+  const size_t oe = (size_t)e * NLV + lane, e3 = (size_t)e * 3;
+  const size_t SN = (size_t)d.NKN * NLV;
+  const int NSCM = d.nsc_max;
+  const float4 e0 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8);
+  const float4 e1 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8 + 4);
+  const float bb[3] = {e0.x, e0.y, e0.z}, cc[3] = {e0.w, e1.x, e1.y};
+  const float aj4 = 4.f * e1.z;
+  const float us = act ? d.usv[oe] : 0.f, vs = act ? d.vsv[oe] : 0.f;
+  float f3[3];
+  int itot = 0, isum = 0;
+#pragma unroll
+  for (int jj = 0; jj < 3; jj++) {
+    f3[jj] = us * bb[jj] + vs * cc[jj];
+    if (f3[jj] < 0.f) { itot++; isum += jj + 1; }
+  }
+  // the flux of a unit field into each vertex (the same for TVD on a
+  // divergence-free element)
+#pragma unroll
+  for (int ii = 0; ii < 3; ii++) {
+    const float fii = f3[ii];
+    const float fl1 = itot == 1 ? fii : (itot == 2 ? ((ii == 5 - isum) ? fii - (f3[0] + f3[1] + f3[2]) : fii) : 0.f);
+    d.cz_ef1[(e3 + ii) * NLV + lane] = act ? aj4 * 3.f * fl1 : 0.f;
+  }
+  const int kv[3] = {en.x, en.y, en.z};
+  // TVD (the instance for models where a basin uses it): not where a vertex
+  // is on an open boundary
+  const bool tvd = TVD && P.itvd >= 1 && d.kbnd[kv[0]] <= 0 && d.kbnd[kv[1]] <= 0 && d.kbnd[kv[2]] <= 0;
+  float ue = 0.f, ve = 0.f;
+  if (tvd && act) {
+    const float hn = d.hen[oe];
+    if (hn > 0.f) { ue = d.un[oe] / hn; ve = d.vn[oe] / hn; }
+  }
+  const float *cin_base = conz_input(d, isact);
+  for (int s = 0; s < nsc; s++) {
+    if (isact > (int)O.stab[s]) continue;        // no sub-step of this scalar now
+    const float rstot = O.stab[s];
+    const float rso = (isact - 1) / rstot, rsot = 1.f - rso;
+    const float dt = (float)P.dt / rstot;
+    const bool istmp = P.is_temp[s] != 0;
+    const float rk = P.rkpar[s];
+    const float *cs = cin_base + s * SN;
+    float c3[3];
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) c3[ii] = act ? clipc(cs[(size_t)kv[ii] * NLV + lane], istmp) : 0.f;
+    float hmed = 0.f, dfh = 0.f;
+    if (rk != 0.f && act) {
+      hmed = rso * d.hen[oe] + rsot * d.heo[oe];
+      dfh = d.difhv[oe];
+    }
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) {
+      // concentrations shifted by vertex ii's own
+      const float c3s[3] = {c3[0] - c3[ii], c3[1] - c3[ii], c3[2] - c3[ii]};
+      float fl;
+      if (itot == 1) fl = f3[ii] * sel3(c3s, isum - 1);
+      else if (itot == 2)   // flux into the vertex with f >= 0 balances the two outflows
+        fl = (ii == 5 - isum) ? -(f3[0] * c3s[0] + f3[1] * c3s[1] + f3[2] * c3s[2]) : 0.f;
+      else fl = 0.f;
+      if constexpr (TVD) {
+        if (tvd && act)
+          fl = tvd_flux_own(ii, itot, isum, f3, c3s, bb, cc, kv, 24.f * e1.z, ue, ve, dt, d.tgrad + s * SN, NLV,
+                            lane, d, e, P.itvd, cs, istmp, c3[ii]);
+      }
+      float hdif = 0.f;
+      if (rk != 0.f) {
+        float wdiff = 0.f;
+#pragma unroll
+        for (int iii = 0; iii < 3; iii++) wdiff += d.wdif[(size_t)e * 9 + 3 * iii + ii] * c3s[iii];
+        hdif = 3.f * rk * dfh * hmed * wdiff;
+      }
+      d.cz_ef[((e3 + ii) * NSCM + s) * NLV + lane] = act ? aj4 * (3.f * fl - hdif) : 0.f;
+    }
+  }
+}
+
 // EX: the instance of shygpu_conz3d with conz3d_omp's source terms (one
 // scalar): settling lowers the interface velocities by wsink*wsinkv
 // (concentration_omp.f90:496); nudging adds dt*aj4*hold*robs*rtau*(cobs - c)
 // per element (:694-709; an = 0, so nothing implicit); loading acts on the
 // assembled mass before the vertical solve (conz3d_nodes :816-833).
-template <int S, int NR, bool EX = false>
+// TV: the instance with vertical TVD (models where a basin uses itvdv = 1)
+template <int S, int NR, bool EX, bool TV>
 __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg) {
   const int j = j_arg >= 0 ? j_arg : *d.subj;   // sub-step index: argument or device counter
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -215,7 +321,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
   // vertical TVD: the far-upwind layer of an element's column exists only
   // where the element continues, so the bottom interface splits At into the
   // elements continuing below layer l+1 and those ending at it
-  const bool tvdv = P.itvdv == 1;
+  const bool tvdv = TV && P.itvdv == 1;
   float2 avn = make_float2(0.f, 0.f);
   if (tvdv) { avn.x = seg_down<S>(av.x, 1); avn.y = seg_down<S>(av.y, 1); }
   const bool isbnd = d.kbnd[k] > 0;
@@ -247,16 +353,11 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
     const float hmntop = up_ok ? 2.f * rvptop / (hnewm + hnew) : 0.f;
     const float hmnbot = dn_ok ? 2.f * rvpbot / (hnew + hnewp) : 0.f;
     float cl[NR], cm1[NR], cp1[NR], hs[NR];
-    bool istmp[NR];
-    float rk[NR];
-    bool anyrk = false;
 #pragma unroll
     for (int r = 0; r < NR; r++) {
       const int s = sidx[r] < 0 ? 0 : sidx[r];
-      istmp[r] = P.is_temp[s] != 0;
-      rk[r] = sidx[r] < 0 ? 0.f : P.rkpar[s];
-      anyrk |= rk[r] != 0.f;
-      const float v = (act && sidx[r] >= 0) ? clipc(cin_base[s * SN + o], istmp[r]) : 0.f;
+      const bool istmp = P.is_temp[s] != 0;
+      const float v = (act && sidx[r] >= 0) ? clipc(cin_base[s * SN + o], istmp) : 0.f;
       cl[r] = v;
       cm1[r] = seg_up<S>(v, 1);
       cp1[r] = seg_down<S>(v, 1);
@@ -264,75 +365,20 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
       if (!dn_ok) cp1[r] = 0.f;
       hs[r] = 0.f;
     }
-    // horizontal fluxes: sum over the incident elements of aj4*(3*fl - hdif)
-    // on the shifted concentrations, and of aj4*3*fl for a unit field (the
-    // horizontal flow into the node layer)
+    // horizontal fluxes: the element part's values of this node's vertex in
+    // each incident element, summed in element order
     float hs1 = 0.f;
     if (act) {
+      const int NSCM = d.nsc_max;
 #pragma unroll 4
       for (int p = pbeg; p < pend; p++) {
         const int4 ix = __ldg(&d.incx[p]);   // element, vertex | layers, other two nodes
-        const int e = ix.x, ii = ix.y & 3;
         if (lane >= (ix.y >> 2)) continue;
-        const float4 e0 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8);
-        const float4 e1 = *reinterpret_cast<const float4 *>(d.ev8 + (size_t)e * 8 + 4);
-        const float bb[3] = {e0.x, e0.y, e0.z}, cc[3] = {e0.w, e1.x, e1.y};
-        const float aj4 = 4.f * e1.z;
-        const size_t oe = (size_t)e * NLV + lane;
-        const float us = __ldg(&d.usv[oe]), vs = __ldg(&d.vsv[oe]);
-        float f3[3];
-        int itot = 0, isum = 0;
+        const size_t ev = (size_t)ix.x * 3 + (ix.y & 3);
+        hs1 += d.cz_ef1[ev * NLV + lane];
 #pragma unroll
-        for (int jj = 0; jj < 3; jj++) {
-          f3[jj] = us * bb[jj] + vs * cc[jj];
-          if (f3[jj] < 0.f) { itot++; isum += jj + 1; }
-        }
-        if (itot == 0 && !anyrk) continue;      // no horizontal flux for this vertex
-        const float hmed = anyrk ? rso * __ldg(&d.hen[oe]) + rsot * __ldg(&d.heo[oe]) : 0.f;
-        const float dfh = anyrk ? __ldg(&d.difhv[oe]) : 0.f;
-        const int kja = ix.z, kjb = ix.w;
-        const float fii = sel3(f3, ii);
-        // upwind flux of a unit field (the same for TVD on a divergence-free element)
-        const float fl1 = itot == 1 ? fii : (itot == 2 ? ((ii == 5 - isum) ? fii - (f3[0] + f3[1] + f3[2]) : fii) : 0.f);
-        hs1 += aj4 * 3.f * fl1;
-        // horizontal TVD (concentration_omp.f90:675-686) where no vertex is
-        // on an open boundary, with the element velocity of the new level
-        const bool tvd = P.itvd >= 1 && !isbnd && d.kbnd[kja] <= 0 && d.kbnd[kjb] <= 0;
-        float ue = 0.f, ve = 0.f;
-        int kv[3] = {k, k, k};
-        if (tvd) {
-          const float hn = d.hen[oe];
-          if (hn > 0.f) { ue = d.un[oe] / hn; ve = d.vn[oe] / hn; }
-          kv[0] = ii == 0 ? k : kja;
-          kv[1] = ii == 1 ? k : (ii == 0 ? kja : kjb);
-          kv[2] = ii == 2 ? k : kjb;
-        }
-#pragma unroll
-        for (int r = 0; r < NR; r++) {
-          if (sidx[r] < 0) continue;
-          const float *cs = cin_base + sidx[r] * SN;
-          const float ca = clipc(__ldg(&cs[(size_t)kja * NLV + lane]), istmp[r]) - cl[r];
-          const float cb = clipc(__ldg(&cs[(size_t)kjb * NLV + lane]), istmp[r]) - cl[r];
-          // shifted concentrations of vertices 0,1,2 (own value 0 at ii, the others in order)
-          const float c3[3] = {ii == 0 ? 0.f : ca, ii == 1 ? 0.f : (ii == 0 ? ca : cb), ii == 2 ? 0.f : cb};
-          float fl;
-          if (itot == 1) fl = fii * sel3(c3, isum - 1);
-          else if (itot == 2) {
-            // flux into the vertex with f >= 0 balances the two outflows
-            fl = (ii == 5 - isum) ? -(f3[0] * c3[0] + f3[1] * c3[1] + f3[2] * c3[2]) : 0.f;
-          } else fl = 0.f;
-          if (tvd)
-            fl = tvd_flux_own(ii, itot, isum, f3, c3, bb, cc, kv, 24.f * e1.z, ue, ve, dt,
-                              d.tgrad + sidx[r] * SN, NLV, lane, d, e, P.itvd, cs, istmp[r], cl[r]);
-          float hdif = 0.f;
-          if (rk[r] != 0.f) {
-            float wdiff = 0.f;
-#pragma unroll
-            for (int iii = 0; iii < 3; iii++) wdiff += __ldg(&d.wdif[(size_t)e * 9 + 3 * iii + ii]) * c3[iii];
-            hdif = 3.f * rk[r] * dfh * hmed * wdiff;
-          }
-          hs[r] += aj4 * (3.f * fl - hdif);
-        }
+        for (int r = 0; r < NR; r++)
+          if (sidx[r] >= 0) hs[r] += d.cz_ef[(ev * NSCM + sidx[r]) * NLV + lane];
       }
     }
     // storage, vertical diffusion and vertical advection, summed over the
@@ -354,7 +400,7 @@ __global__ void __launch_bounds__(256) k_conz(Dev d, const int *kbas, int j_arg)
       const float c = cl[r];
       const float cm = up_ok ? cm1[r] - c : 0.f, cp = dn_ok ? cp1[r] - c : 0.f;   // shifted
       float topw, botw;                               // interface fluxes times their element weights
-      if (!tvdv) {
+      if (!TV || !tvdv) {
         const float vtop = up_ok ? wt * (wt > 0.f ? 0.f : cm) : 0.f;
         const float vbot = wb * (wb > 0.f ? cp : 0.f);
         topw = A * vtop;

@@ -12,7 +12,8 @@ namespace shy {
 // discharge.  The gradients come from the element's FP32 b, c with the last
 // vertex's taken as minus the sum of the other two, so that each element's
 // three fluxes cancel exactly and a closed basin's summed budget moves by
-// FP64 round-off only.
+// FP64 round-off only.  A level-boundary node has no continuity equation
+// (its level is imposed), so its budget is its volume at that level.
 __device__ __forceinline__ double2 budget_grad(const float *evp, int ii) {
   if (ii < 2) return make_double2((double)evp[ii], (double)evp[3 + ii]);
   return make_double2(-((double)evp[0] + (double)evp[1]), -((double)evp[3] + (double)evp[4]));
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   if (lane == 0 && valid) d.vol_node[k] = vol;
   bud = seg_sum<S>(act ? bud : 0.);
   if (lane == 0 && valid) {
-    if (init_only) d.vbud_node[k] = vol;
+    if (init_only || d.kbnd[k] > 0) d.vbud_node[k] = vol;   // level boundary: the imposed level's volume
     else d.vbud_node[k] += P.dt * (bud + budget_discharge(d, P, k));
   }
   if (init_only) return;
@@ -187,7 +188,7 @@ __global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int i
   }
   if (bad) set_status(&d.out[b], SHY_EDEPTH);
   d.vol_node[k] = vol;
-  if (init_only) d.vbud_node[k] = vol;
+  if (init_only || d.kbnd[k] > 0) d.vbud_node[k] = vol;     // level boundary: the imposed level's volume
   else d.vbud_node[k] += P.dt * (bud + budget_discharge(d, P, k));
   if (init_only) return;
   // hydro_vertical: w from continuity, bottom-up (hydrodynamic.f90:1711-1771),

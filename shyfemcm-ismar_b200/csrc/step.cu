@@ -107,7 +107,7 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
 __global__ void k_subctl(Dev d, cudaGraphConditionalHandle h) {
   const int nj = *d.subj + 1;
   *d.subj = nj;
-  *d.nsub_launched += d.any_tvd ? 3 : 2;
+  *d.nsub_launched += d.any_tvd ? 4 : 3;   // gradients, element part, node part, this
   cudaGraphSetConditional(h, nj < *d.imax ? 1u : 0u);
 }
 
