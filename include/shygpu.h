@@ -244,6 +244,35 @@ int shygpu_shy_open(shygpu_model *model, int32_t ibasin, const shy_basin *basin,
                     int32_t date, int32_t time, const char *title, shygpu_shyfile **file);
 int shygpu_shy_write(shygpu_shyfile *file);
 int shygpu_shy_close(shygpu_shyfile *file);
+/* Scalar output of basin ib in the same way: what 1, temperature and
+ * salinity (the ts.shy file of bcl_write_output, baroclinic.f90:1163-1190:
+ * records 11 salinity, 12 temperature, and 13 density when with_rho);
+ * what 2, the passive tracers (the conz.shy file of tracer_write,
+ * conz_admin.f90:535-575: record 10 for one tracer, 300 + i for several).
+ * Scalar files are ftype 2 with npr 1 (shyfem_init_scalar_file,
+ * shy_util.f90:484-518); each record holds the active layers of each node.
+ * shygpu_shy_write and shygpu_shy_close serve both kinds of file.          */
+int shygpu_shy_open_scalar(shygpu_model *model, int32_t ibasin, const shy_basin *basin,
+                           const char *path, int32_t date, int32_t time, const char *title,
+                           int32_t what, int32_t with_rho, shygpu_shyfile **file);
+
+/* Time series at chosen nodes of basin ib in the reference's .ext format
+ * (wrexta, extra.f90:254-575; records of io_ext.f90:468-575).  nodes are
+ * n basin node numbers (1-based, the knaus of the $extra section); names
+ * (optional) n blank-padded 80-character station names; atime0 the
+ * absolute time of the model's time origin, added to the model time of
+ * each record.  Per shygpu_ext_write one record per variable: 1 the nodal
+ * barotropic velocities and the water level, 2 the nodal velocities of each
+ * layer (uvtop0, uvtopr, transforms.f90:160-270: area-weighted means over
+ * the node's elements in the system), 12 temperature, 11 salinity, 13
+ * density (with_rho and T/S transported), 10 the tracer of a one-tracer
+ * basin.  A write waits for the model's stream.                           */
+typedef struct shygpu_extfile shygpu_extfile;
+int shygpu_ext_open(shygpu_model *model, int32_t ibasin, const shy_basin *basin, const char *path,
+                    int32_t n, const int32_t *nodes, const char *names, const char *title,
+                    double atime0, int32_t with_rho, shygpu_extfile **file);
+int shygpu_ext_write(shygpu_extfile *file);
+int shygpu_ext_close(shygpu_extfile *file);
 
 /* Checkpoints (restart.f90:445-660, made exact): every device array of the
  * model and its time-level indices, copied to or from a host buffer of

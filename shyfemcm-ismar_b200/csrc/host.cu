@@ -1795,10 +1795,13 @@ extern "C" int shygpu_get_levels(shygpu_model *m, float *znv) {
 struct shygpu_shyfile {
   shygpu_model *m = nullptr;
   int ib = 0, nk = 0, ne = 0, nlv = 0;
+  int kind = 0;                    // 0 hydro, 1 temperature/salinity(/density), 2 tracers
+  std::vector<int> ivars, scs;     // scalar files: the record ids and the scalars (-1: density)
   FILE *fp = nullptr;
   std::vector<int> ilhv, ilhkv;
   struct Slot {
     float *z = nullptr, *ze = nullptr, *u = nullptr, *v = nullptr;
+    float *sc = nullptr;           // scalar files: the variables, (nvar, nk, nlv)
     BasinOut *out = nullptr;
     cudaEvent_t ev = nullptr;
     bool busy = false;
@@ -1837,6 +1840,19 @@ static bool shy_write_slot(shygpu_shyfile *f, const shygpu_shyfile::Slot &sl) {
       for (int l = 0; l < std::min(f->nlv, f->ilhv[e]); l++) r.push_back(c[(size_t)e * f->nlv + l]);
     return r;
   };
+  if (f->kind != 0) {
+    // scalar files (shy_write_scalar_record): active node layers
+    bool ok = true;
+    for (size_t i = 0; i < f->ivars.size() && ok; i++) {
+      const float *c = sl.sc + i * (size_t)f->nk * f->nlv;
+      std::vector<float> r;
+      r.reserve((size_t)f->nk * f->nlv);
+      for (int k = 0; k < f->nk; k++)
+        for (int l = 0; l < std::min(f->nlv, f->ilhkv[k]); l++) r.push_back(c[(size_t)k * f->nlv + l]);
+      ok = head(f->ivars[i], f->nk, 1, f->nlv) && shy_rec_v(fp, r);
+    }
+    return ok && fflush(fp) == 0;
+  }
   bool ok = head(1, f->nk, 1, 1) && shy_rec(fp, sl.z, f->nk * 4) &&
             head(1, f->ne, 3, 1) && shy_rec(fp, sl.ze, f->ne * 12);
   if (f->nlv > 1) {
@@ -1876,6 +1892,7 @@ static void shy_free(shygpu_shyfile *f) {
     if (sl.ze) cudaFreeHost(sl.ze);
     if (sl.u) cudaFreeHost(sl.u);
     if (sl.v) cudaFreeHost(sl.v);
+    if (sl.sc) cudaFreeHost(sl.sc);
     if (sl.out) cudaFreeHost(sl.out);
     if (sl.ev) cudaEventDestroy(sl.ev);
   }
@@ -1883,31 +1900,41 @@ static void shy_free(shygpu_shyfile *f) {
   delete f;
 }
 
-extern "C" int shygpu_shy_open(shygpu_model *m, int32_t ib, const shy_basin *bs, const char *path, int32_t date,
-                               int32_t time, const char *title, shygpu_shyfile **out) {
-  if (!m || ib < 0 || ib >= m->nbasin || !bs || !path || !out) return fail(SHY_EARG, "shy_open: bad arguments");
+// open a .shy file of `kind` (0 hydro, 1 temperature/salinity/density, 2
+// tracers) with its pinned slots, write its header (io_shy.f90:1577-1598)
+static int shy_open_kind(shygpu_model *m, int32_t ib, const shy_basin *bs, const char *path, int32_t date,
+                         int32_t time, const char *title, int kind, const std::vector<int> &ivars,
+                         const std::vector<int> &scs, shygpu_shyfile **out) {
   const BasinPar &bp = m->par[ib];
   if (bs->nkn != bp.nk || bs->nel != bp.ne || bs->nlv != bp.nlv) return fail(SHY_EARG, "shy_open: basin %d differs", ib);
   auto *f = new shygpu_shyfile();
   f->m = m; f->ib = ib; f->nk = bp.nk; f->ne = bp.ne; f->nlv = bp.nlv;
+  f->kind = kind; f->ivars = ivars; f->scs = scs;
   f->ilhv.assign(bs->ilhv, bs->ilhv + bp.ne);
   f->ilhkv.assign(bs->ilhkv, bs->ilhkv + bp.nk);
   for (auto &sl : f->slot) {
-    if (cudaMallocHost((void **)&sl.z, (size_t)bp.nk * 4) != cudaSuccess ||
-        cudaMallocHost((void **)&sl.ze, (size_t)bp.ne * 12) != cudaSuccess ||
-        cudaMallocHost((void **)&sl.u, (size_t)bp.ne * bp.nlv * 4) != cudaSuccess ||
-        cudaMallocHost((void **)&sl.v, (size_t)bp.ne * bp.nlv * 4) != cudaSuccess ||
-        cudaMallocHost((void **)&sl.out, sizeof(BasinOut)) != cudaSuccess ||
-        cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) != cudaSuccess) {
+    bool ok = cudaMallocHost((void **)&sl.out, sizeof(BasinOut)) == cudaSuccess &&
+              cudaEventCreateWithFlags(&sl.ev, cudaEventDisableTiming) == cudaSuccess;
+    if (kind == 0)
+      ok = ok && cudaMallocHost((void **)&sl.z, (size_t)bp.nk * 4) == cudaSuccess &&
+           cudaMallocHost((void **)&sl.ze, (size_t)bp.ne * 12) == cudaSuccess &&
+           cudaMallocHost((void **)&sl.u, (size_t)bp.ne * bp.nlv * 4) == cudaSuccess &&
+           cudaMallocHost((void **)&sl.v, (size_t)bp.ne * bp.nlv * 4) == cudaSuccess;
+    else
+      ok = ok && cudaMallocHost((void **)&sl.sc, ivars.size() * (size_t)bp.nk * bp.nlv * 4) == cudaSuccess;
+    if (!ok) {
       shy_free(f);
       return fail(SHY_ECAPACITY, "shy_open: pinned host buffers");
     }
   }
   f->fp = fopen(path, "wb");
   if (!f->fp) { shy_free(f); return fail(SHY_EARG, "shy_open: cannot open %s", path); }
-  // header (io_shy.f90:1577-1598); simpar = hzmin, hzoff, nzadapt, dtaver
+  // header (io_shy.f90:1577-1598); simpar = hzmin, hzoff, nzadapt, dtaver;
+  // hydro files have 3 variables (npr 3: z at nodes and vertices, U, V),
+  // scalar files ftype 2, npr 1 (shyfem_init_scalar_file, shy_util.f90:484-518)
   const int32_t nk = bp.nk, ne = bp.ne, nlv = bp.nlv;
-  const int32_t idv[2] = {1617, 14}, ftype = 1, pars[5] = {nk, ne, 3, nlv, 4}, nfix = 0, dt2[2] = {date, time};
+  const int32_t ftype = kind == 0 ? 1 : 2, npr = kind == 0 ? 3 : 1, nvar = kind == 0 ? 4 : (int32_t)ivars.size();
+  const int32_t idv[2] = {1617, 14}, pars[5] = {nk, ne, npr, nlv, nvar}, nfix = 0, dt2[2] = {date, time};
   const int32_t nsimpar = 4;
   const float simpar[4] = {bp.hzmin, bp.hzoff, 0.f, 0.f};
   char ttl[80], ver[80];
@@ -1933,6 +1960,36 @@ extern "C" int shygpu_shy_open(shygpu_model *m, int32_t ib, const shy_basin *bs,
   return SHY_OK;
 }
 
+extern "C" int shygpu_shy_open(shygpu_model *m, int32_t ib, const shy_basin *bs, const char *path, int32_t date,
+                               int32_t time, const char *title, shygpu_shyfile **out) {
+  if (!m || ib < 0 || ib >= m->nbasin || !bs || !path || !out) return fail(SHY_EARG, "shy_open: bad arguments");
+  return shy_open_kind(m, ib, bs, path, date, time, title, 0, {}, {}, out);
+}
+
+// scalar files: what 1, temperature/salinity (ts.shy: records 11 salinity,
+// 12 temperature, 13 density when with_rho; bcl_write_output,
+// baroclinic.f90:1163-1190), what 2, the passive tracers (conz.shy: record
+// 10 for one tracer, 300 + i for several; tracer_write,
+// conz_admin.f90:535-575)
+extern "C" int shygpu_shy_open_scalar(shygpu_model *m, int32_t ib, const shy_basin *bs, const char *path,
+                                      int32_t date, int32_t time, const char *title, int32_t what,
+                                      int32_t with_rho, shygpu_shyfile **out) {
+  if (!m || ib < 0 || ib >= m->nbasin || !bs || !path || !out || (what != 1 && what != 2))
+    return fail(SHY_EARG, "shy_open_scalar: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  std::vector<int> ivars, scs;
+  if (what == 1) {
+    if (bp.isalt) { ivars.push_back(11); scs.push_back(scalar_index(bp, 1, 0)); }
+    if (bp.itemp) { ivars.push_back(12); scs.push_back(scalar_index(bp, 0, 0)); }
+    if (with_rho) { ivars.push_back(13); scs.push_back(-1); }
+  } else {
+    const int nc = bp.nsc - bp.itemp - bp.isalt;
+    for (int i = 0; i < nc; i++) { ivars.push_back(nc == 1 ? 10 : 300 + i + 1); scs.push_back(scalar_index(bp, 2, i)); }
+  }
+  if (ivars.empty()) return fail(SHY_EARG, "shy_open_scalar: basin %d has no such scalars", ib);
+  return shy_open_kind(m, ib, bs, path, date, time, title, what, ivars, scs, out);
+}
+
 extern "C" int shygpu_shy_write(shygpu_shyfile *f) {
   if (!f) return fail(SHY_EARG, "shy_write: file is NULL");
   shygpu_model *m = f->m;
@@ -1947,10 +2004,18 @@ extern "C" int shygpu_shy_write(shygpu_shyfile *f) {
   auto &sl = f->slot[j];
   const int c = m->cur, NLV = m->NLV;
   cudaStream_t st = m->stream;
-  CUDA_TRY(cudaMemcpyAsync(sl.z, m->zbuf[c] + bp.k0, (size_t)bp.nk * 4, cudaMemcpyDeviceToHost, st));
-  CUDA_TRY(cudaMemcpyAsync(sl.ze, m->zebuf[c] + 3 * (size_t)bp.e0, (size_t)bp.ne * 12, cudaMemcpyDeviceToHost, st));
-  ST_TRY(copy_cols(m->ubuf[c], sl.u, bp.ne, bp.nlv, NLV, bp.e0, false, st));
-  ST_TRY(copy_cols(m->vbuf[c], sl.v, bp.ne, bp.nlv, NLV, bp.e0, false, st));
+  if (f->kind == 0) {
+    CUDA_TRY(cudaMemcpyAsync(sl.z, m->zbuf[c] + bp.k0, (size_t)bp.nk * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(sl.ze, m->zebuf[c] + 3 * (size_t)bp.e0, (size_t)bp.ne * 12, cudaMemcpyDeviceToHost, st));
+    ST_TRY(copy_cols(m->ubuf[c], sl.u, bp.ne, bp.nlv, NLV, bp.e0, false, st));
+    ST_TRY(copy_cols(m->vbuf[c], sl.v, bp.ne, bp.nlv, NLV, bp.e0, false, st));
+  } else {
+    const size_t SN = (size_t)m->NKN * NLV;
+    for (size_t i = 0; i < f->scs.size(); i++) {
+      float *src = f->scs[i] < 0 ? m->base.rho : m->scbuf[m->sc_cur] + f->scs[i] * SN;
+      ST_TRY(copy_cols(src, sl.sc + i * (size_t)bp.nk * bp.nlv, bp.nk, bp.nlv, NLV, bp.k0, false, st));
+    }
+  }
   CUDA_TRY(cudaMemcpyAsync(sl.out, m->base.out + f->ib, sizeof(BasinOut), cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaEventRecord(sl.ev, st));
   {
@@ -1973,6 +2038,213 @@ extern "C" int shygpu_shy_close(shygpu_shyfile *f) {
   const bool err = f->io_error;
   shy_free(f);
   return err ? fail(SHY_EARG, "shy_close: a write failed") : SHY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// .ext files: time series at chosen nodes (wrexta, extra.f90:254-575; format
+// of io_ext.f90:468-575).  Header: (ext_type, version), (nodes, layers,
+// variables), the reference time, (href, hzmin, nzadapt), (title, version
+// string), (node numbers, depths, layer counts, x, y, names), the layer
+// depths.  Per write and variable one record: (time, ivar, m, lmax, n, the
+// active layers of each node for each of the m components).  Variables:
+// 1 the nodal barotropic velocities and the water level (uvtop0,
+// transforms.f90:160-210), 2 the nodal velocities of each layer (uvtopr
+// :214-270), 12 temperature, 11 salinity, 13 density (on request), 10 the
+// tracer of a one-tracer basin.  The nodal velocities are the area-weighted
+// means over the node's elements in the system of U/H (barotropic, with H
+// the element's mean depth plus level) and of each layer's U/h.  A write
+// reads the columns it needs on the model's stream and writes at once.
+// ---------------------------------------------------------------------------
+struct shygpu_extfile {
+  shygpu_model *m = nullptr;
+  int ib = 0, nlv = 0, n = 0;
+  std::vector<int> nodes;                    // basin-local node index of each station
+  std::vector<int> il;                       // its layer count
+  std::vector<std::vector<int>> elems;       // basin-local elements of each station's node
+  std::vector<float> hev, aj;                // per basin element: mean depth, aj (area/24)
+  std::vector<int> ilhv;
+  bool temp = false, salt = false, rho = false, conz = false;
+  int nvar = 0;
+  double atime0 = 0.;
+  FILE *fp = nullptr;
+};
+
+extern "C" int shygpu_ext_open(shygpu_model *m, int32_t ib, const shy_basin *bs, const char *path, int32_t n,
+                               const int32_t *nodes, const char *names, const char *title, double atime0,
+                               int32_t with_rho, shygpu_extfile **out) {
+  if (!m || ib < 0 || ib >= m->nbasin || !bs || !path || n < 1 || !nodes || !out)
+    return fail(SHY_EARG, "ext_open: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  if (bs->nkn != bp.nk || bs->nel != bp.ne || bs->nlv != bp.nlv) return fail(SHY_EARG, "ext_open: basin %d differs", ib);
+  for (int j = 0; j < n; j++)
+    if (nodes[j] < 1 || nodes[j] > bp.nk) return fail(SHY_EARG, "ext_open: node %d outside the basin", nodes[j]);
+  auto *f = new shygpu_extfile();
+  f->m = m; f->ib = ib; f->nlv = bp.nlv; f->n = n; f->atime0 = atime0;
+  f->temp = bp.itemp != 0; f->salt = bp.isalt != 0; f->rho = with_rho != 0 && bp.itemp && bp.isalt;
+  f->conz = bp.nsc - bp.itemp - bp.isalt == 1;
+  f->nvar = 2 + f->temp + f->salt + f->rho + f->conz;
+  f->ilhv.assign(bs->ilhv, bs->ilhv + bp.ne);
+  f->hev.resize(bp.ne);
+  f->aj.resize(bp.ne);
+  std::vector<float> ev((size_t)SHY_EVDIM * bp.ne);
+  if (int st = shygpu_set_ev(bp.nk, bp.ne, bs->nen3v, bs->xgv, bs->ygv, ev.data())) { delete f; return st; }
+  std::vector<char> want(bp.nk, 0);
+  for (int j = 0; j < n; j++) { f->nodes.push_back(nodes[j] - 1); want[nodes[j] - 1] = 1; }
+  std::vector<std::vector<int>> inc(bp.nk);
+  std::vector<float> hdep(n, 0.f);
+  for (int e = 0; e < bp.ne; e++) {
+    double hs = 0.;
+    for (int ii = 0; ii < 3; ii++) hs += bs->hm3v[3 * e + ii];
+    f->hev[e] = (float)(hs / 3.);
+    f->aj[e] = ev[(size_t)SHY_EVDIM * e + 9];
+    for (int ii = 0; ii < 3; ii++) {
+      const int k = bs->nen3v[3 * e + ii] - 1;
+      if (want[k]) inc[k].push_back(e);
+    }
+  }
+  std::vector<int32_t> knaus(n), il(n);
+  std::vector<float> x(n), y(n);
+  for (int j = 0; j < n; j++) {
+    const int k = f->nodes[j];
+    f->elems.push_back(inc[k]);
+    knaus[j] = k + 1;
+    il[j] = bs->ilhkv[k];
+    x[j] = bs->xgv[k];
+    y[j] = bs->ygv[k];
+    for (int e : inc[k])                     // hkv_max: the deepest vertex depth at the node
+      for (int ii = 0; ii < 3; ii++)
+        if (bs->nen3v[3 * e + ii] - 1 == k) hdep[j] = std::max(hdep[j], bs->hm3v[3 * e + ii]);
+  }
+  f->il.assign(il.begin(), il.end());
+  f->fp = fopen(path, "wb");
+  if (!f->fp) { delete f; return fail(SHY_EARG, "ext_open: cannot open %s", path); }
+  const int32_t h1[2] = {947336, 8}, h2[3] = {n, bp.nlv, f->nvar};
+  const float h4[3] = {0.f, bp.hzmin, 0.f};
+  char tv[160];
+  memset(tv, ' ', 160);
+  if (title) memcpy(tv, title, std::min<size_t>(80, strlen(title)));
+  const char *ver = "shygpu (B200 step of SHYFEM)";
+  memcpy(tv + 80, ver, strlen(ver));
+  std::vector<char> h6((size_t)n * (4 * 5 + 80), ' ');
+  char *q = h6.data();
+  memcpy(q, knaus.data(), 4 * n); q += 4 * n;
+  memcpy(q, hdep.data(), 4 * n); q += 4 * n;
+  memcpy(q, il.data(), 4 * n); q += 4 * n;
+  memcpy(q, x.data(), 4 * n); q += 4 * n;
+  memcpy(q, y.data(), 4 * n); q += 4 * n;
+  for (int j = 0; j < n; j++) {
+    if (names) {
+      const char *nm = names + (size_t)80 * j;
+      memcpy(q, nm, strnlen(nm, 80));
+    }
+    q += 80;
+  }
+  std::vector<float> hl(bs->hlv, bs->hlv + bp.nlv);
+  const bool ok = shy_rec(f->fp, h1, 8) && shy_rec(f->fp, h2, 12) && shy_rec(f->fp, &atime0, 8) &&
+                  shy_rec(f->fp, h4, 12) && shy_rec(f->fp, tv, 160) && shy_rec(f->fp, h6.data(), (int32_t)h6.size()) &&
+                  shy_rec_v(f->fp, hl) && fflush(f->fp) == 0;
+  if (!ok) { fclose(f->fp); delete f; return fail(SHY_EARG, "ext_open: write error on %s", path); }
+  *out = f;
+  return SHY_OK;
+}
+
+extern "C" int shygpu_ext_write(shygpu_extfile *f) {
+  if (!f) return fail(SHY_EARG, "ext_write: file is NULL");
+  shygpu_model *m = f->m;
+  const BasinPar &bp = m->par[f->ib];
+  const int c = m->cur, NLV = m->NLV, nlv = f->nlv, n = f->n;
+  cudaStream_t st = m->stream;
+  // the columns the stations need, copied on the model's stream
+  std::vector<int> elist;
+  for (const auto &v : f->elems) elist.insert(elist.end(), v.begin(), v.end());
+  std::sort(elist.begin(), elist.end());
+  elist.erase(std::unique(elist.begin(), elist.end()), elist.end());
+  const size_t ne = elist.size();
+  std::vector<float> U(ne * NLV), V(ne * NLV), H(ne * NLV), UB(ne), VB(ne), ZE(ne * 3);
+  std::vector<int> WEG(ne, 0);
+  for (size_t i = 0; i < ne; i++) {
+    const size_t ge = (size_t)bp.e0 + elist[i];
+    CUDA_TRY(cudaMemcpyAsync(&U[i * NLV], m->ubuf[c] + ge * NLV, NLV * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&V[i * NLV], m->vbuf[c] + ge * NLV, NLV * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&H[i * NLV], m->hebuf[c] + ge * NLV, NLV * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&UB[i], m->base.unv + ge, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&VB[i], m->base.vnv + ge, 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&ZE[i * 3], m->zebuf[c] + 3 * ge, 12, cudaMemcpyDeviceToHost, st));
+    if (m->any_wd) CUDA_TRY(cudaMemcpyAsync(&WEG[i], m->base.iweg + ge, 4, cudaMemcpyDeviceToHost, st));
+  }
+  const size_t SN = (size_t)m->NKN * NLV;
+  std::vector<float> Z(n), T(n * NLV), S(n * NLV), R(n * NLV), C(n * NLV);
+  for (int j = 0; j < n; j++) {
+    const size_t gk = (size_t)bp.k0 + f->nodes[j];
+    CUDA_TRY(cudaMemcpyAsync(&Z[j], m->zbuf[c] + gk, 4, cudaMemcpyDeviceToHost, st));
+    const float *scb = m->scbuf[m->sc_cur];
+    if (f->temp) CUDA_TRY(cudaMemcpyAsync(&T[j * NLV], scb + scalar_index(bp, 0, 0) * SN + gk * NLV, NLV * 4, cudaMemcpyDeviceToHost, st));
+    if (f->salt) CUDA_TRY(cudaMemcpyAsync(&S[j * NLV], scb + scalar_index(bp, 1, 0) * SN + gk * NLV, NLV * 4, cudaMemcpyDeviceToHost, st));
+    if (f->rho) CUDA_TRY(cudaMemcpyAsync(&R[j * NLV], m->base.rho + gk * NLV, NLV * 4, cudaMemcpyDeviceToHost, st));
+    if (f->conz) CUDA_TRY(cudaMemcpyAsync(&C[j * NLV], scb + scalar_index(bp, 2, 0) * SN + gk * NLV, NLV * 4, cudaMemcpyDeviceToHost, st));
+  }
+  BasinOut o;
+  CUDA_TRY(cudaMemcpyAsync(&o, m->base.out + f->ib, sizeof o, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  auto idx = [&](int e) { return (size_t)(std::lower_bound(elist.begin(), elist.end(), e) - elist.begin()); };
+  // vals(l, j, i) of the reference: lmax = nlv layers per node, m components
+  std::vector<float> v1((size_t)nlv * n * 3, 0.f), v2((size_t)nlv * n * 2, 0.f);
+  for (int j = 0; j < n; j++) {
+    double u0 = 0., w0 = 0., a0 = 0.;
+    std::vector<double> ul(nlv, 0.), vl(nlv, 0.), al(nlv, 0.);
+    for (int e : f->elems[j]) {
+      const size_t i = idx(e);
+      if (WEG[i] != 0) continue;
+      const double aj = f->aj[e];
+      const double hm = (double)f->hev[e] + ((double)ZE[i * 3] + ZE[i * 3 + 1] + ZE[i * 3 + 2]) / 3.;
+      a0 += aj; u0 += aj * UB[i] / hm; w0 += aj * VB[i] / hm;
+      for (int l = 0; l < std::min(nlv, f->ilhv[e]); l++) {
+        const double h = H[i * NLV + l];
+        if (!(h > 0.)) continue;
+        al[l] += aj; ul[l] += aj * U[i * NLV + l] / h; vl[l] += aj * V[i * NLV + l] / h;
+      }
+    }
+    v1[(size_t)nlv * j] = a0 > 0. ? (float)(u0 / a0) : 0.f;
+    v1[(size_t)nlv * (n + j)] = a0 > 0. ? (float)(w0 / a0) : 0.f;
+    v1[(size_t)nlv * (2 * n + j)] = Z[j];
+    for (int l = 0; l < nlv; l++) {
+      v2[(size_t)nlv * j + l] = al[l] > 0. ? (float)(ul[l] / al[l]) : 0.f;
+      v2[(size_t)nlv * (n + j) + l] = al[l] > 0. ? (float)(vl[l] / al[l]) : 0.f;
+    }
+  }
+  const double atime = f->atime0 + o.dtime;
+  auto rec = [&](int32_t ivar, int32_t mm, const float *vals) {   // vals(nlv, n, mm)
+    std::vector<float> lin;
+    for (int i = 0; i < mm; i++)
+      for (int j = 0; j < n; j++)
+        for (int l = 0; l < std::min(nlv, f->il[j]); l++) lin.push_back(vals[((size_t)i * n + j) * nlv + l]);
+    const int32_t hd[4] = {ivar, mm, nlv, (int32_t)lin.size()};
+    std::vector<char> b(8 + 16 + lin.size() * 4);
+    memcpy(b.data(), &atime, 8);
+    memcpy(b.data() + 8, hd, 16);
+    if (!lin.empty()) memcpy(b.data() + 24, lin.data(), lin.size() * 4);
+    return shy_rec(f->fp, b.data(), (int32_t)b.size());
+  };
+  auto cols = [&](const std::vector<float> &A) {   // node columns (n, NLV) -> vals(nlv, n, 1)
+    std::vector<float> v((size_t)nlv * n, 0.f);
+    for (int j = 0; j < n; j++)
+      for (int l = 0; l < nlv; l++) v[(size_t)nlv * j + l] = A[(size_t)j * NLV + l];
+    return v;
+  };
+  bool ok = rec(1, 3, v1.data()) && rec(2, 2, v2.data());
+  if (f->temp) ok = ok && rec(12, 1, cols(T).data());
+  if (f->salt) ok = ok && rec(11, 1, cols(S).data());
+  if (f->rho) ok = ok && rec(13, 1, cols(R).data());
+  if (f->conz) ok = ok && rec(10, 1, cols(C).data());
+  if (!ok || fflush(f->fp) != 0) return fail(SHY_EARG, "ext_write: write error");
+  return SHY_OK;
+}
+
+extern "C" int shygpu_ext_close(shygpu_extfile *f) {
+  if (!f) return SHY_OK;
+  const bool ok = fclose(f->fp) == 0;
+  delete f;
+  return ok ? SHY_OK : fail(SHY_EARG, "ext_close: close failed");
 }
 
 extern "C" int shygpu_set_nudging(shygpu_model *m, int32_t ib, const float *andgzv) {

@@ -77,6 +77,12 @@ def lib():
     L.shygpu_set_nudging.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
     L.shygpu_set_bound_scalar.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
     L.shygpu_autotune.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_double)]
+    L.shygpu_shy_open_scalar.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyBasin), C.c_char_p, C.c_int32,
+                                         C.c_int32, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(C.c_void_p)]
+    L.shygpu_ext_open.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyBasin), C.c_char_p, C.c_int32,
+                                  C.c_void_p, C.c_char_p, C.c_char_p, C.c_double, C.c_int32, C.POINTER(C.c_void_p)]
+    L.shygpu_ext_write.argtypes = [C.c_void_p]
+    L.shygpu_ext_close.argtypes = [C.c_void_p]
     L.shygpu_conz3d.argtypes = ([C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_double, C.c_float,
                                  C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_int32, C.c_int32,
                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_void_p, C.c_float,
@@ -286,6 +292,35 @@ class Model:
         check(lib().shygpu_shy_open(self.h, ib, C.byref(self._basins[ib]), str(path).encode(), date, time,
                                     title.encode(), C.byref(h)), "shy_open")
         return h
+
+    def shy_open_scalar(self, ib, path, what, with_rho=False, date=0, time=0, title=""):
+        """Scalar output of basin ib in the reference's .shy format: what 1
+        temperature/salinity (and density), 2 the passive tracers; returns a
+        handle for shy_write/shy_close."""
+        h = C.c_void_p()
+        check(lib().shygpu_shy_open_scalar(self.h, ib, C.byref(self._basins[ib]), str(path).encode(), date, time,
+                                           title.encode(), int(what), int(bool(with_rho)), C.byref(h)),
+              "shy_open_scalar")
+        return h
+
+    def ext_open(self, ib, path, nodes, names=None, atime0=0.0, with_rho=False, title=""):
+        """Time series at the basin's nodes `nodes` (1-based) in the .ext
+        format; returns a handle for ext_write/ext_close."""
+        nd = np.ascontiguousarray(nodes, np.int32)
+        nm = None
+        if names is not None:
+            nm = b"".join(str(x).encode()[:80].ljust(80) for x in names)
+        h = C.c_void_p()
+        check(lib().shygpu_ext_open(self.h, ib, C.byref(self._basins[ib]), str(path).encode(), nd.size,
+                                    nd.ctypes.data, nm, title.encode(), float(atime0), int(bool(with_rho)),
+                                    C.byref(h)), "ext_open")
+        return h
+
+    def ext_write(self, f):
+        check(lib().shygpu_ext_write(f), "ext_write")
+
+    def ext_close(self, f):
+        check(lib().shygpu_ext_close(f), "ext_close")
 
     def shy_write(self, f):
         check(lib().shygpu_shy_write(f), "shy_write")

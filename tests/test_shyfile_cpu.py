@@ -52,3 +52,29 @@ def test_reader_on_a_hand_made_file(tmp_path):
     np.testing.assert_array_equal(s["ze"], ze.reshape(2, 3))
     np.testing.assert_array_equal(s["u"], u)
     np.testing.assert_array_equal(s["v"], v)
+
+
+def test_ext_reader_on_a_hand_made_file(tmp_path):
+    """The .ext reader on records laid out as io_ext.f90:468-575 writes them:
+    two stations with 2 and 1 layers, one record of ivar 2 (m = 2)."""
+    from shygpu.shyfile import read_ext
+    n, lmax = 2, 2
+    il = np.array([2, 1], np.int32)
+    head = [np.array([947336, 8], np.int32).tobytes(), np.array([n, lmax, 2], np.int32).tobytes(),
+            np.float64(50.0).tobytes(), np.array([0, 0.01, 0], np.float32).tobytes(),
+            b"stations".ljust(80) + b"v".ljust(80),
+            np.array([3, 7], np.int32).tobytes() + np.array([4.5, 2.0], np.float32).tobytes() + il.tobytes()
+            + np.array([1, 2], np.float32).tobytes() + np.array([3, 4], np.float32).tobytes()
+            + b"s1".ljust(80) + b"s2".ljust(80),
+            np.array([1.0, 5.0], np.float32).tobytes()]
+    lin = np.array([1, 2, 3, 4, 5, 6], np.float32)           # u: 1 2 | 3 ; v: 4 5 | 6
+    body = [np.float64(110.0).tobytes() + np.array([2, 2, lmax, 6], np.int32).tobytes() + lin.tobytes()]
+    p = tmp_path / "t.ext"
+    p.write_bytes(b"".join(rec(b) for b in head + body))
+    r = read_ext(p)
+    assert (r["ext_type"], r["nvers"], r["n"], r["lmax"], r["nvar"], r["atime0"]) == (947336, 8, 2, 2, 2, 50.0)
+    assert r["names"] == ["s1", "s2"] and r["title"] == "stations"
+    np.testing.assert_array_equal(r["knaus"], [3, 7])
+    (s,) = r["records"]
+    assert (s["atime"], s["ivar"], s["m"]) == (110.0, 2, 2)
+    np.testing.assert_array_equal(s["values"], [[[1, 2], [3, 0]], [[4, 5], [6, 0]]])
