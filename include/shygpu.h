@@ -117,6 +117,12 @@ typedef struct shy_params {
                              /*   (superbee; needs aapar = 0)   :1054       */
   int32_t ihwadv;            /* vertical advection of momentum with ilin 0:  */
                              /*   0 none, 1 upwind, 2 centred   :1350       */
+  int32_t nzadapt;           /* z-layers whose top layers follow the level  */
+                             /*   (z-star, zadaptutil.f90): <= 1 plain z-   */
+                             /*   layers, >= nlv all layers, between: the   */
+                             /*   surface layers down to where the level    */
+                             /*   reaches (nzadapt at rest); z-layers only, */
+                             /*   no baroclinic terms, no wetting and drying */
 } shy_params;
 
 /* Host views of one basin's state, reference layouts.  NULL members are

@@ -523,10 +523,50 @@ void set_ieltv(Model &m) {
     }
 }
 
+// z-adaptive (z-star) layers of z-layer basins with nzadapt > 1
+// (zadaptutil.f90).  compute_rzmov_info (:100-117): the threshold factor.
+double zad_rzmov(int nlv, int nzadapt, const std::vector<double> &hlv) {
+  if (nzadapt <= 1) return 0.;
+  if (nzadapt >= nlv) return 10000.;
+  return hlv[nzadapt - 2] / (hlv[nzadapt - 1] - hlv[nzadapt - 2]);
+}
+
+// compute_nadapt_info (:212-240): the lowest layer that follows the level
+// z (1-based; 0: none) in a column of lmax layers
+int zad_levmax(double z, const std::vector<double> &hlv, int lmax, double rzmov) {
+  int nad = 0;
+  for (int l = 1; l <= lmax - 1; l++) {
+    const double hl = hlv[l - 1], hp = l > 1 ? hlv[l - 2] : 0.;
+    if (z <= -hl + rzmov * (hl - hp)) nad = l + 1;
+    else break;
+  }
+  return nad;
+}
+
+// the thickness of layer l (1-based) at an element vertex of level z and
+// depth htot (setdepth :1014-1055 with compute_zadaptive_info :321-380): the
+// layers down to levmax share the column hzad = hadapt + z in proportion to
+// their nominal thickness (the weights (hlv(l-1) - hlv(l)) / hadapt, with
+// the surface at 0 and, when levmax is the bottom layer, hadapt = htot);
+// below them z-layers, the first one plus z when no layer follows the level
+double zad_vertex_h(int l, double z, double htot, int lmax, int levmax, const Model &m) {
+  if (levmax > 0 && l <= levmax) {
+    const double had = levmax == lmax ? htot : m.hlv[levmax - 1];
+    const double htop = l == 1 ? 0. : m.hlv[l - 2], hbot = l == lmax ? htot : m.hlv[l - 1];
+    return -(had + z) * ((htop - hbot) / had);
+  }
+  if (lmax == 1) return htot + z;
+  if (l < lmax) return m.hldv[l - 1] + (levmax == 0 && l == 1 ? z : 0.);
+  return htot - m.hlv[lmax - 2];
+}
+
 // setdepth (elems_dealing.f90:930-1160) for z-layers (nsigma = 0), pure
 // sigma layers (nsigma = nlv) and hybrid layers (nsigma sigma layers down to
-// hsigma, z-layers below), without z-adaptive layers (compute_zadaptive_info
-// returns nadapt = ladapt = 0, zadaptutil.f90:321-324).  Sigma layers take
+// hsigma, z-layers below), and z-layers with z-adaptive surface layers
+// (nzadapt > 1, nsigma = 0; zad_vertex_h above; an element's layers down to
+// the deepest levmax of its vertices are the means of the vertex values).
+// Without nzadapt compute_zadaptive_info returns nadapt = ladapt = 0
+// (zadaptutil.f90:321-324).  Sigma layers take
 // the fraction -hldv(l) of the total depth min(h, hsigma) + z: at the nodes
 // from each element's vertex values in element order, the last element
 // writing (:1010-1025), at the elements from hev and the mean water level
@@ -539,6 +579,40 @@ int setdepth(Model &m, std::vector<double> &hdkn, std::vector<double> &hden,
   const double hsigma = (double)(float)(m.p.hsigma > 0.f ? m.p.hsigma : 10000.f);
   hdkn.assign((size_t)nlv * m.nkn, 0.);
   hden.assign((size_t)nlv * m.nel, 0.);
+  if (m.p.nzadapt > 1 && nsigma == 0) {
+    const double rzmov = zad_rzmov(nlv, m.p.nzadapt, m.hlv);
+    for (int ie = 0; ie < m.nel; ie++) {
+      const double areafv = 12. * m.ev[(size_t)ie * SHY_EVDIM + 9] / 3.;
+      const int lmax = m.ilhv[ie];
+      int lev[3];
+      double zmed = 0.;
+      for (int ii = 0; ii < 3; ii++) {
+        const int k = m.nen3v[3 * ie + ii];
+        const double z = zenv[3 * ie + ii], htot = m.hm3v[3 * ie + ii];
+        zmed += z;
+        lev[ii] = zad_levmax(z, m.hlv, lmax, rzmov);
+        for (int l = 1; l <= lmax; l++) hdkn[(size_t)k * nlv + l - 1] += areafv * zad_vertex_h(l, z, htot, lmax, lev[ii], m);
+      }
+      zmed /= 3.;
+      const int lad = std::max(lev[0], std::max(lev[1], lev[2]));
+      const double htot = m.hev[ie];
+      for (int l = 1; l <= lmax; l++) {
+        double h;
+        if (lad > 0 && l <= lad) {
+          h = 0.;
+          for (int ii = 0; ii < 3; ii++)
+            h += zad_vertex_h(l, zenv[3 * ie + ii], m.hm3v[3 * ie + ii], lmax, lev[ii], m);
+          h /= 3.;
+        } else if (lmax == 1) h = htot + zmed;
+        else if (l < lmax) h = m.hldv[l - 1] + (lad == 0 && l == 1 ? zmed : 0.);
+        else h = htot - m.hlv[lmax - 2];
+        if (!(h > 0.))
+          return fail(SHY_EDEPTH, "setdepth: no layer depth in element " + std::to_string(ie + 1) +
+                                      " layer " + std::to_string(l));
+        hden[(size_t)ie * nlv + l - 1] = h;
+      }
+    }
+  } else
   for (int ie = 0; ie < m.nel; ie++) {
     const double areafv = 12. * m.ev[(size_t)ie * SHY_EVDIM + 9] / 3.;
     const int lmax = m.ilhv[ie], lmin = 1;
@@ -2033,6 +2107,11 @@ void *shyref_create(const shy_basin *B, const shy_params *P) {
   int nkn = m->nkn, nel = m->nel, nlv = m->nlv;
   if (nlv < 1 || nlv > SHY_MAX_LAYERS) { fail(SHY_EARG, "shyref_create: nlv"); delete m; return nullptr; }
   if (P->nsigma < 0 || P->nsigma > nlv) { fail(SHY_EARG, "shyref_create: nsigma outside 0..nlv"); delete m; return nullptr; }
+  if (P->nzadapt > 1 && (P->nsigma > 0 || P->ibarcl > 0 || P->wetdry)) {
+    fail(SHY_EARG, "shyref_create: z-adaptive layers on z-layers without baroclinic terms or wetting and drying");
+    delete m;
+    return nullptr;
+  }
   m->nen3v.resize((size_t)3 * nel);
   for (size_t i = 0; i < m->nen3v.size(); i++) m->nen3v[i] = B->nen3v[i] - 1;
   std::vector<double> x = dv(B->xgv, nkn), y = dv(B->ygv, nkn);

@@ -48,6 +48,8 @@ struct BasinPar {
   int itvd;                   // horizontal transport: 0 upwind, 1 TVD with node gradients
   int itvdv;                  // vertical transport: 0 upwind, 1 TVD
   int ihwadv;                 // vertical momentum advection (with adv): 0 none, 1 upwind, 2 centred
+  int nzadapt;                // z-layers with z-adaptive surface layers when > 1
+  double rzmov;               // their threshold factor (compute_rzmov_info)
 };
 
 // set_advective's vertical term (explicit.f90:776-833) of one layer from

@@ -872,6 +872,9 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: baroclinic terms on sigma layers not supported", b));
     if (Pp[b].ihwadv < 0 || Pp[b].ihwadv > 2)
       return bail(fail(SHY_EARG, "basin %d: ihwadv=%d: 0, 1 (upwind) or 2 (centred)", b, Pp[b].ihwadv));
+    if (Pp[b].nzadapt > 1 && (Pp[b].nsigma > 0 || Pp[b].ibarcl > 0 || Pp[b].wetdry))
+      return bail(fail(SHY_EARG, "basin %d: z-adaptive layers (nzadapt > 1) on z-layers without baroclinic terms "
+                                 "or wetting and drying only", b));
     if (Pp[b].itvdv != 0 && Pp[b].itvdv != 1)
       return bail(fail(SHY_EARG, "basin %d: itvdv=%d: upwind (0) or TVD (1) only", b, Pp[b].itvdv));
     if (Pp[b].itvdv == 1 && Pp[b].aapar != 0.f)   // concentration_omp.f90:218-226
@@ -1047,6 +1050,14 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
     bp.adv = p.ilin == 0 ? 1 : 0; bp.rlin = p.rlin;
     m->any_adv |= bp.adv != 0;
     bp.itvd = p.itvd; bp.itvdv = p.itvdv; bp.ihwadv = p.ilin == 0 ? p.ihwadv : 0;
+    // z-adaptive surface layers (compute_rzmov_info, zadaptutil.f90:100-117)
+    bp.nzadapt = p.nzadapt > 1 ? p.nzadapt : 0;
+    bp.rzmov = 0.;
+    if (bp.nzadapt > 1) {
+      const float *hv = bs.hlv;
+      bp.rzmov = bp.nzadapt >= bs.nlv ? 10000.
+                                      : (double)hv[bp.nzadapt - 2] / ((double)hv[bp.nzadapt - 1] - (double)hv[bp.nzadapt - 2]);
+    }
     bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
     int ns = 0;
     if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }

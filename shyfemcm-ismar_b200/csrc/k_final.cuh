@@ -67,7 +67,12 @@ __global__ void __launch_bounds__(256) k_final(Dev d, int init_only) {
   const float *hlv = d.hlv + (size_t)en.w * NLV;
   double h = 0.;
   if (act) {
-    if (lane < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[lane];   // :1079-1083
+    if (P.nzadapt > 1) {                 // z-adaptive surface layers
+      const int lev[3] = {zad_levmax(zn3[0], hlv, ilevel, P.rzmov), zad_levmax(zn3[1], hlv, ilevel, P.rzmov),
+                          zad_levmax(zn3[2], hlv, ilevel, P.rzmov)};
+      h = zad_elem_h(lane, zn3, hm, ilevel, lev, hlv, hld, zmed);
+    }
+    else if (lane < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[lane];   // :1079-1083
     else if (ilevel == 1) h = hm.w + zmed;
     else if (lane < ilevel - 1) h = (double)hld[lane] + (lane == 0 ? zmed : 0.);
     else h = (double)hm.w - hlv[ilevel - 2];
@@ -168,10 +173,14 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
   const float *hld = d.hldv + (size_t)en.w * NLV;
   const float *hlv = d.hlv + (size_t)en.w * NLV;
   bool bad = false;
+  int lev[3] = {0, 0, 0};
+  if (P.nzadapt > 1)
+    for (int ii = 0; ii < 3; ii++) lev[ii] = zad_levmax(zv[ii], hlv, ilevel, P.rzmov);
   for (int l = 0; l < NLV; l++) {
     double h = 0.;
     if (l < ilevel) {
-      if (l < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // sigma layers (:1079-1083)
+      if (P.nzadapt > 1) h = zad_elem_h(l, zv, hm, ilevel, lev, hlv, hld, zmed);   // z-adaptive surface layers
+      else if (l < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // sigma layers (:1079-1083)
       else if (ilevel == 1) h = hm.w + zmed;
       else if (l < ilevel - 1) h = (double)hld[l] + (l == 0 ? zmed : 0.);
       else h = (double)hm.w - hlv[ilevel - 2];
@@ -268,10 +277,14 @@ __global__ void __launch_bounds__(128) k_final_w(Dev d, int init_only) {
     const float *hld = d.hldv + (size_t)en.w * NLV;
     const float *hlv = d.hlv + (size_t)en.w * NLV;
     bool bad = false;
+    int lev[3] = {0, 0, 0};
+    if (P.nzadapt > 1)
+      for (int ii = 0; ii < 3; ii++) lev[ii] = zad_levmax(zn3[ii], hlv, ilevel, P.rzmov);
     for (int l = 0; l < NLV; l++) {
       double h = 0.;
       if (l < ilevel) {
-        if (l < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // sigma layers (:1079-1083)
+        if (P.nzadapt > 1) h = zad_elem_h(l, zn3, hm, ilevel, lev, hlv, hld, zmed);   // z-adaptive surface layers
+        else if (l < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // sigma layers (:1079-1083)
         else if (ilevel == 1) h = hm.w + zmed;
         else if (l < ilevel - 1) h = (double)hld[l] + (l == 0 ? zmed : 0.);
         else h = (double)hm.w - hlv[ilevel - 2];

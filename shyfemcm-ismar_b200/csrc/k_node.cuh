@@ -57,7 +57,8 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
     const double htot = ii == 0 ? hm.x : (ii == 1 ? hm.y : hm.z);
     hsig_h = htot;
     double hl;
-    if (le == 1) hl = htot + z;
+    if (P.nzadapt > 1) hl = zad_vertex_h(lane, z, htot, le, zad_levmax(z, hlv, le, P.rzmov), hlv, hld);
+    else if (le == 1) hl = htot + z;
     else if (lane < le - 1) hl = hldl + (lane == 0 ? z : 0.);
     else hl = htot - hlv[le - 2];
     hsum += areafv * hl;
@@ -148,11 +149,13 @@ __global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int i
     // setdepth takes the element's vertex level (a dry element's differs)
     const float ze = P.wetdry ? d.zen[3 * e + ii] : (float)z;
     double us = 0., vs = 0.;                  // the element's transports summed over its layers
+    const int lev = P.nzadapt > 1 ? zad_levmax((double)ze, hlv, le, P.rzmov) : 0;
 #pragma unroll
     for (int l = 0; l < L; l++) {
       if (l >= le) break;
       float hl;
-      if (le == 1) hl = htot + ze;
+      if (P.nzadapt > 1) hl = (float)zad_vertex_h(l, (double)ze, (double)htot, le, lev, hlv, hld);
+      else if (le == 1) hl = htot + ze;
       else if (l < le - 1) hl = hld[l] + (l == 0 ? ze : 0.f);
       else hl = hbot;
       hsum[l] += areafv * hl;

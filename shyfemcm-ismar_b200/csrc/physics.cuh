@@ -46,4 +46,50 @@ __device__ __forceinline__ double level_bc(const Dev &d, const BasinPar &P, int 
   return (double)(float)z;
 }
 
+// z-adaptive (z-star) surface layers of z-layer basins with nzadapt > 1
+// (zadaptutil.f90).  compute_nadapt_info (:212-240): the lowest layer that
+// follows the level z (1-based; 0: none) in a column of lmax layers.
+__device__ __forceinline__ int zad_levmax(double z, const float *hlv, int lmax, double rzmov) {
+  int nad = 0;
+  for (int l = 1; l <= lmax - 1; l++) {
+    const double hl = hlv[l - 1], hp = l > 1 ? (double)hlv[l - 2] : 0.;
+    if (z <= -hl + rzmov * (hl - hp)) nad = l + 1;
+    else break;
+  }
+  return nad;
+}
+
+// layer l (0-based) at an element vertex of level z and depth htot (setdepth,
+// elems_dealing.f90:1014-1055, with compute_zadaptive_info :321-380): the
+// layers down to levmax share the column hadapt + z in proportion to their
+// nominal thickness (hadapt = hlv(levmax), or htot when levmax is the bottom
+// layer); below them z-layers, the first plus z when no layer follows z
+__device__ __forceinline__ double zad_vertex_h(int l, double z, double htot, int lmax, int levmax, const float *hlv,
+                                               const float *hld) {
+  const int l1 = l + 1;
+  if (levmax > 0 && l1 <= levmax) {
+    const double had = levmax == lmax ? htot : (double)hlv[levmax - 1];
+    const double htop = l1 == 1 ? 0. : (double)hlv[l1 - 2], hbot = l1 == lmax ? htot : (double)hlv[l1 - 1];
+    return -(had + z) * ((htop - hbot) / had);
+  }
+  if (lmax == 1) return htot + z;
+  if (l1 < lmax) return (double)hld[l] + (levmax == 0 && l1 == 1 ? z : 0.);
+  return htot - (double)hlv[lmax - 2];
+}
+
+// layer l (0-based) of an element: down to the deepest levmax of its
+// vertices the mean of the vertex values, below z-layers of its mean depth
+// hev and mean level zmed (setdepth :1087-1110)
+__device__ __forceinline__ double zad_elem_h(int l, const double (&z)[3], const float4 hm, int lmax,
+                                             const int (&lev)[3], const float *hlv, const float *hld, double zmed) {
+  const int lad = max(lev[0], max(lev[1], lev[2]));
+  const int l1 = l + 1;
+  if (lad > 0 && l1 <= lad)
+    return (zad_vertex_h(l, z[0], hm.x, lmax, lev[0], hlv, hld) + zad_vertex_h(l, z[1], hm.y, lmax, lev[1], hlv, hld) +
+            zad_vertex_h(l, z[2], hm.z, lmax, lev[2], hlv, hld)) / 3.;
+  if (lmax == 1) return (double)hm.w + zmed;
+  if (l1 < lmax) return (double)hld[l] + (lad == 0 && l1 == 1 ? zmed : 0.);
+  return (double)hm.w - (double)hlv[lmax - 2];
+}
+
 }  // namespace shy

@@ -51,7 +51,7 @@ class ShyParams(C.Structure):
         ("nsigma", C.c_int32), ("hsigma", C.c_float),
         ("wetdry", C.c_int32), ("hzmin", C.c_float), ("hzon", C.c_float), ("volmin", C.c_float),
         ("rlin", C.c_float), ("itvd", C.c_int32), ("itvdv", C.c_int32),
-        ("ihwadv", C.c_int32),
+        ("ihwadv", C.c_int32), ("nzadapt", C.c_int32),
     ]
 
 
@@ -140,6 +140,7 @@ def make_params(case, **over):
     s.itvd = int(p.get("itvd", 0))
     s.itvdv = int(p.get("itvdv", 0))
     s.ihwadv = int(p.get("ihwadv", 0))
+    s.nzadapt = int(p.get("nzadapt", 0))
     return s
 
 

@@ -10,6 +10,8 @@ seeded synthetic basin of the named shape:
 * `basin3d_case`   -- 3D baroclinic basin, ~20k nodes on 50 km x 30 km, 20
                       z-layers 1..5 m thick, Gaussian-bump bathymetry 5..60 m,
                       T/S linear in depth plus seeded noise, 10 m/s wind, M2 0.3 m.
+* `shelf_case`     -- tidal shelf on z-layers with three 1 m surface layers
+                      and an M2 of 1.5 m, for z-adaptive layers (nzadapt).
 * `ensemble_cases` -- independent basins with log-uniform node counts.
 
 All arrays use the reference's layouts: Fortran column-major `(nlv, nel)` /
@@ -309,6 +311,47 @@ def flat_case(nx=41, ny=9, lx=8.0e3, ly=1.6e3, seed=9, dt=60.0, nlv=1, ampli=1.0
     case = dict(name=f"flat_{nkn}x{nlv}", nkn=nkn, nel=nel, nlv=nlv, nen3v=nen3v,
                 xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
                 bnd_index=bnd, tide=tide, seed=seed, params=dict(dt=dt, wetdry=1))
+    return _finish(case)
+
+
+def shelf_case(nkn_target=1500, lx=20.0e3, ly=8.0e3, seed=11, dt=60.0, nzadapt=3, ampli=1.5,
+               hmin=5.0, hmax=40.0, ntracer=1, closed=False, wind=8.0):
+    """Tidal shelf on z-layers with thin surface layers for z-adaptive
+    layers (nzadapt, zadaptutil.f90): three 1 m layers on top, then 2, 3,
+    5, 8, 10 and 12 m; depth rising from `hmin` at the closed end to
+    `hmax` at the open boundary; M2 of `ampli` that falls first (phase of
+    half a period), so the level drops below the first layers' bottoms
+    within a quarter period: plain z-layers (nzadapt = 0) lose their first
+    layer there (setdepth stops), z-adaptive ones stretch.  `closed`
+    removes the boundary (a wind-driven closed basin); `ntracer` passive
+    tracers start as a front across the shelf."""
+    ny = max(3, int(round(math.sqrt(nkn_target * ly / lx))))
+    nx = max(3, int(round(nkn_target / ny)))
+    x, y, nen3v, ii, jj = structured_triangles(nx, ny, lx, ly, 0.2, seed)
+    rng = np.random.default_rng(seed + 606)
+    nkn, nel = x.size, nen3v.shape[0]
+    h = hmax + (hmin - hmax) * x / lx + _smooth_field(x, y, rng, scale=1.0)
+    hm3v = h[nen3v - 1]
+    hlv, hldv = z_layers([1.0, 1.0, 1.0, 2.0, 3.0, 5.0, 8.0, 10.0, 12.0])
+    hlv[-1] = max(hlv[-1], h.max() + 1.0)
+    nlv = len(hlv)
+    ilhv, ilhkv = layer_counts(nen3v, hm3v, hlv, hldv, nkn)
+    bnd = np.zeros(nkn, np.int32)
+    if not closed:
+        bnd[ii == 0] = 1
+    tide = np.array([[[ampli, M2_PERIOD, 0.5 * M2_PERIOD, 0.0]]], np.float32)
+    rhoair, cd = 1.225, 2.5e-3
+    tau = rhoair / 1025.0 * cd * wind * wind
+    conzv = np.zeros((ntracer, nkn, nlv), np.float32)
+    for t in range(ntracer):
+        front = 0.5 * (1.0 + np.tanh((x - lx * (0.3 + 0.2 * t)) / (0.05 * lx)))
+        conzv[t] = (front[:, None] * (1.0 + 0.1 * np.arange(nlv))[None, :]).astype(np.float32)
+    case = dict(name=f"shelf_{nkn}x{nlv}_za{nzadapt}", nkn=nkn, nel=nel, nlv=nlv, nen3v=nen3v,
+                xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
+                bnd_index=bnd, tide=tide, seed=seed,
+                params=dict(dt=dt, nzadapt=nzadapt, nconz=ntracer),
+                tauxnv=np.full(nkn, 0.6 * tau, np.float32), tauynv=np.full(nkn, 0.8 * tau, np.float32),
+                conzv=conzv)
     return _finish(case)
 
 
