@@ -123,6 +123,16 @@ typedef struct shy_params {
                              /*   surface layers down to where the level    */
                              /*   reaches (nzadapt at rest); z-layers only, */
                              /*   no baroclinic terms, no wetting and drying */
+  int32_t inohyd;            /* 1: non-hydrostatic pressure (nohydro.f90,   */
+                             /*   def_para.f90:1933): a 3D Poisson system  */
+                             /*   per step corrects level and transports;  */
+                             /*   no wetting and drying, no z-adaptive     */
+                             /*   layers                                   */
+  float aqpar;               /* its semi-implicit weight (0.5)      :1935   */
+  int32_t ivwadv;            /* vertical advection of w: 0 none, 1 upwind, */
+                             /*   2 centred differences              :1939  */
+  int32_t inhflx;            /* horizontal advection of w: 0 averaged, 1   */
+                             /*   upwind fluxes                     :1940   */
 } shy_params;
 
 /* Host views of one basin's state, reference layouts.  NULL members are

@@ -463,6 +463,16 @@ struct Model {
   std::vector<int> tvdup_e;                 // [6*ie + slot], -1 outside the basin
   std::vector<double> tvdup_xi;             // [3*(6*ie + slot) + i]
   double dtime_weg = -1.;                   // setweg's dtime_old
+  // non-hydrostatic pressure (mod_nohyd): qpov, qpnv (nkn, nlv) rows,
+  // qdistv (nkn) its weight near open boundaries (qhdist; 1 by default),
+  // wlov the old vertical velocity (copy_uvz), wnh the non-hydrostatic w
+  // of sp256wnh (nkn, nlv+1); the 3D system (coo_init_new's 3D part):
+  // nt3g row-block offsets, c3coo/rvec3d its values and right-hand side
+  std::vector<double> qpov, qpnv, qdistv, wlov, wnh;
+  std::vector<int> nt3g;
+  std::vector<double> c3coo, rvec3d;
+  int nh_iters = 0;
+  double nh_resid0 = 0., nh_resid = 0.;
   shy_step_info info{};
   // solver controls
   double rtol = 1e-8, atol = 1e-8;
@@ -879,6 +889,27 @@ void set_explicit(Model &m) {
       }
     }
   }
+  // nonhydro_set_explicit (nohydro.f90:526-586): the gradient of the old
+  // non-hydrostatic pressure times the old thickness, weight 1 - aqpar (the
+  // new pressure is zero here: nonhydro_copy cleared it at the step start)
+  if (m.p.inohyd) {
+    const double aqt = 1. - m.p.aqpar;
+    for (int ie = 0; ie < m.nel; ie++) {
+      const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+      for (int l = 1; l <= m.ilhv[ie]; l++) {
+        double qx = 0., qy = 0.;
+        for (int ii = 0; ii < 3; ii++) {
+          const int k = m.nen3v[3 * ie + ii];
+          const double qpo = m.qdistv[k] * m.qpov[(size_t)k * nlv + l - 1];
+          qx += e[3 + ii] * qpo;
+          qy += e[6 + ii] * qpo;
+        }
+        const double hhio = m.hdeov[(size_t)ie * nlv + l - 1];
+        m.fxv[(size_t)ie * nlv + l - 1] += aqt * hhio * qx;
+        m.fyv[(size_t)ie * nlv + l - 1] += aqt * hhio * qy;
+      }
+    }
+  }
 }
 
 // hydro_intern (hydrodynamic.f90:868-1416) for one element column
@@ -1209,6 +1240,322 @@ void hydro_vertical(Model &m) {
   for (int k = 0; k < m.nkn; k++)
     if (m.bnd[k] > 0)
       for (int l = 0; l <= nlv; l++) W(l, k) = 0.;
+}
+
+// ---------------------------------------------------------------------------
+// Non-hydrostatic pressure: nohydro.f90 and the 3D system of coo_matrix.f90 /
+// simsys_spkaux.f90.  The 3D unknowns are (nlv+2) per node, layer 0 and
+// layer nlv+1 being padding rows: unknown u(k,l) = k*(nlv+2) + l.
+// ---------------------------------------------------------------------------
+
+// coo_init_new's 3D part (coo_matrix.f90:180-247): row block k holds the
+// layer-0 diagonal, then per layer l the node's sorted neighbours at l with
+// (k,l-1), (k,l), (k,l+1) in the diagonal's place, then the layer-(nlv+1)
+// diagonal: ng*nlv + 2*nlv + 2 entries, row-sorted, so the COO is a CSR
+void coo3d_init(int nkn, int nlv, const std::vector<int> &ntg, std::vector<int> &nt3g) {
+  nt3g.assign(nkn + 1, 0);
+  for (int k = 0; k < nkn; k++) {
+    const int ng = ntg[k + 1] - ntg[k];
+    nt3g[k + 1] = nt3g[k] + (ng - 1) * nlv + 2 + 3 * nlv;
+  }
+}
+
+// loccoo3d (coo_matrix.f90:665-695), 0-based: the position of element entry
+// (i, j) of layer l (1..nlv) in the 3D COO; for i == j the (k,l-1) and
+// (k,l+1) couplings sit just before and after it
+int loc3d(const Model &m, int ie, int i, int j, int l) {
+  const int ki = m.nen3v[3 * ie + i];
+  const int ng = m.ntg[ki + 1] - m.ntg[ki];
+  const int mi = m.ijp[(size_t)9 * ie + 3 * i + i] - m.ntg[ki];   // diagonal's index in the row
+  const int mj = m.ijp[(size_t)9 * ie + 3 * i + j] - m.ntg[ki];
+  const int p3 = mj < mi ? mj : (mj == mi ? mi + 1 : mj + 2);
+  return m.nt3g[ki] + 1 + (l - 1) * (ng + 2) + p3;
+}
+
+// the CSR row pointer and columns of the 3D COO (coocsr of its row-sorted
+// entries), unknowns u(k,l) = k*(nlv+2) + l
+void coo3d_csr(const Model &m, std::vector<int> &ia, std::vector<int> &ja) {
+  const int nlv = m.nlv, n = (nlv + 2) * m.nkn;
+  ia.assign(n + 1, 0);
+  ja.assign(m.nt3g[m.nkn], 0);
+  int r = 0, p = 0;
+  for (int k = 0; k < m.nkn; k++) {
+    const int ng = m.ntg[k + 1] - m.ntg[k];
+    ia[r] = p; ja[p++] = k * (nlv + 2); r++;                     // layer 0
+    for (int l = 1; l <= nlv; l++) {
+      ia[r] = p;
+      for (int q = 0; q < ng; q++) {
+        const int kj = m.icol[m.ntg[k] + q];
+        if (kj == k) { ja[p++] = k * (nlv + 2) + l - 1; ja[p++] = k * (nlv + 2) + l; ja[p++] = k * (nlv + 2) + l + 1; }
+        else ja[p++] = kj * (nlv + 2) + l;
+      }
+      r++;
+    }
+    ia[r] = p; ja[p++] = k * (nlv + 2) + nlv + 1; r++;            // layer nlv+1
+  }
+  ia[r] = p;
+}
+
+// system_assemble_3d (simsys_spkaux.f90:597-635): mass(-1:1,3,3) as
+// mass[(d+1)*9 + 3*i + j], the three couplings added at kk-1, kk, kk+1
+void assemble_3d(Model &m, int ie, int l, const double *mass, const double *rhs) {
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 3; j++) {
+      const int kk = loc3d(m, ie, i, j, l);
+      m.c3coo[kk - 1] += mass[0 * 9 + 3 * i + j];
+      m.c3coo[kk] += mass[1 * 9 + 3 * i + j];
+      m.c3coo[kk + 1] += mass[2 * 9 + 3 * i + j];
+    }
+    m.rvec3d[(size_t)(m.nlv + 2) * m.nen3v[3 * ie + i] + l] += rhs[i];
+  }
+}
+
+// coo_adjust_3d (coo_matrix.f90:269-325): unit diagonal where no element
+// layer reached it, and on the padding rows
+void adjust_3d(Model &m) {
+  for (int ie = 0; ie < m.nel; ie++)
+    for (int i = 0; i < 3; i++)
+      for (int l = 1; l <= m.nlv; l++) {
+        const int kk = loc3d(m, ie, i, i, l);
+        if (m.c3coo[kk] == 0.) m.c3coo[kk] = 1.;
+      }
+  for (int k = 0; k < m.nkn; k++) {
+    m.c3coo[m.nt3g[k]] = 1.;
+    m.c3coo[m.nt3g[k + 1] - 1] = 1.;
+  }
+}
+
+// system_solve_3d + spk_solve_system (3D: the same ILUT(5, 0.01) and
+// BiCGStab as the zeta system, sparskit_admin.f90:115-334) + system_get_3d:
+// the guess is z(l,k) with zero padding rows; the solution goes back to z
+int solve_3d(Model &m, std::vector<double> &z /* (nkn, nlv) rows */) {
+  const int nlv = m.nlv, n = (nlv + 2) * m.nkn;
+  std::vector<int> ia, ja;
+  coo3d_csr(m, ia, ja);
+  Ilu M;
+  int st = ilut(n, ia.data(), ja.data(), m.c3coo.data(), 5, 0.01, M);
+  if (st) return st;
+  std::vector<double> x(n, 0.);
+  for (int k = 0; k < m.nkn; k++)
+    for (int l = 1; l <= nlv; l++) x[(size_t)k * (nlv + 2) + l] = z[(size_t)k * nlv + l - 1];
+  st = bcgstab(n, ia.data(), ja.data(), m.c3coo.data(), M, m.rvec3d.data(), x.data(), m.rtol, m.atol, m.maxmv,
+               &m.nh_iters, &m.nh_resid0, &m.nh_resid);
+  if (st) return st;
+  for (int k = 0; k < m.nkn; k++)
+    for (int l = 1; l <= nlv; l++) z[(size_t)k * nlv + l - 1] = x[(size_t)k * (nlv + 2) + l];
+  return SHY_OK;
+}
+
+// tridag (keps_util.f90:82-111): a sub-, b main, c super-diagonal
+int tridag(const double *a, const double *b, const double *c, const double *r, double *u, int n) {
+  std::vector<double> gam(n + 1);
+  if (b[0] == 0.) return fail(SHY_ESINGULAR, "tridag: matrix singular");
+  double bet = b[0];
+  u[0] = r[0] / bet;
+  for (int j = 1; j < n; j++) {
+    gam[j] = c[j - 1] / bet;
+    bet = b[j] - a[j] * gam[j];
+    if (bet == 0.) return fail(SHY_ESINGULAR, "tridag: matrix singular");
+    u[j] = (r[j] - a[j] * u[j - 1]) / bet;
+  }
+  for (int j = n - 2; j >= 0; j--) u[j] -= gam[j + 1] * u[j + 1];
+  return SHY_OK;
+}
+
+// sp256wnh (nohydro.f90:205-524): the vertical velocity from the vertical
+// momentum equation with the old non-hydrostatic pressure, horizontal
+// diffusion, horizontal advection (averaged, or upwind fluxes with
+// inhflx = 1), vertical advection (ivwadv 1 upwind, 2 centred) and implicit
+// vertical viscosity: one tridiagonal system per node over the interfaces
+// 1..lmax-1.  An element whose last layer is l makes interface l of its
+// nodes an identity row, over whatever came before it in element order.
+int sp256wnh(Model &m) {
+  const int nlv = m.nlv, I = nlv + 1;
+  const double dt = m.p.dt, aq = m.p.aqpar, aqt = 1. - aq, az = m.p.azpar, azt = 1. - az;
+  std::vector<double> wrhs((size_t)I * m.nkn, 0.), wdiag((size_t)I * m.nkn, 0.),
+      wdiagt((size_t)I * m.nkn, 0.), wdiagb((size_t)I * m.nkn, 0.);
+  auto WO = [&](int l, int k) { return m.wlov[(size_t)k * I + l]; };
+  for (int ie = 0; ie < m.nel; ie++) {
+    const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+    const int ilevel = m.ilhv[ie];
+    int kn[3];
+    double b[3], c[3];
+    for (int ii = 0; ii < 3; ii++) { kn[ii] = m.nen3v[3 * ie + ii]; b[ii] = e[3 + ii]; c[ii] = e[6 + ii]; }
+    const double aj4 = 4. * e[9];
+    for (int l = 1; l <= ilevel; l++) {
+      const bool blast = l == ilevel;
+      const size_t o = (size_t)ie * nlv + l - 1;
+      const double hdn = m.hdenv[o], hdo = m.hdeov[o];
+      const double utn = m.utlnv[o], uto = m.utlov[o], vtn = m.vtlnv[o], vto = m.vtlov[o];
+      double hdpn = 0., hdpo = 0., ubn = 0., ubo = 0., vbn = 0., vbo = 0., anu;
+      if (blast) anu = 0.5 * m.p.ahpar * m.difhv[o];
+      else {
+        hdpn = m.hdenv[o + 1]; hdpo = m.hdeov[o + 1];
+        ubn = m.utlnv[o + 1]; ubo = m.utlov[o + 1]; vbn = m.vtlnv[o + 1]; vbo = m.vtlov[o + 1];
+        anu = 0.5 * m.p.ahpar * (m.difhv[o] + m.difhv[o + 1]);
+      }
+      const double dzn = 0.5 * (hdn + hdpn), dzo = 0.5 * (hdo + hdpo);
+      const double us = 0.5 * (az * (utn + ubn) / dzn + azt * (uto + ubo) / dzo);
+      const double vs = 0.5 * (az * (vtn + vbn) / dzn + azt * (vto + vbo) / dzo);
+      double wl[3], f[3], fl[3] = {0., 0., 0.}, wb = 0., wc = 0., wsum = 0.;
+      int itot = 0, isum = 0;
+      for (int ii = 0; ii < 3; ii++) {
+        wl[ii] = WO(l, kn[ii]);
+        f[ii] = us * b[ii] + vs * c[ii];
+        if (f[ii] < 0.) { itot++; isum += ii + 1; }
+        wb += b[ii] * wl[ii]; wc += c[ii] * wl[ii]; wsum += wl[ii];
+      }
+      if (m.p.inhflx == 1) {
+        if (itot == 1) {
+          for (int ii = 0; ii < 3; ii++) fl[ii] = f[ii] * wl[isum - 1];
+        } else if (itot == 2) {
+          const int iz = 6 - isum - 1;
+          for (int ii = 0; ii < 3; ii++) fl[ii] = f[ii] * wl[ii];
+          fl[iz] = 0.;
+          fl[iz] = -(fl[0] + fl[1] + fl[2]);
+        }
+      }
+      for (int ii = 0; ii < 3; ii++) {
+        const int k = kn[ii];
+        const size_t r = (size_t)k * I + l;
+        const double wq = blast ? 0. : -aqt * m.qdistv[k] *
+                                           (m.qpov[(size_t)k * nlv + l - 1] - m.qpov[(size_t)k * nlv + l]) / dzo;
+        double wadvv = 0.;
+        if (m.p.ivwadv == 1 && !blast) {
+          const double wplus = 0.5 * (WO(l, k) + WO(l - 1, k)) / dzo;
+          wadvv = wplus > 0. ? wplus * WO(l, k) : wplus * WO(l - 1, k);
+          const double wminus = 0.5 * (WO(l, k) + WO(l + 1, k)) / dzo;
+          wadvv -= wminus > 0. ? wminus * WO(l + 1, k) : wminus * WO(l, k);
+        } else if (m.p.ivwadv >= 2 && !blast) {
+          wadvv = 0.5 * WO(l, k) * (WO(l - 1, k) - WO(l + 1, k)) / dzo;
+        }
+        const double wdifh = -3. * anu * (wb * b[ii] + wc * c[ii]);
+        const double wadvh = m.p.inhflx == 1 ? -3. * fl[ii] : -(b[ii] * us + c[ii] * vs) * wsum;
+        const double wr = dzn * (WO(l, k) + dt * (wq + wdifh - wadvh - wadvv));
+        wrhs[r] += aj4 * wr;
+        if (blast) {
+          wdiag[r] = 1.; wdiagt[r] = 0.; wdiagb[r] = 0.; wrhs[r] = 0.;
+        } else {
+          const double rnu = m.visv[r];
+          wdiag[r] += dzn * aj4 + dt * aj4 * rnu * (1. / hdn + 1. / hdpn);
+          wdiagt[r] -= dt * aj4 * rnu / hdn;
+          wdiagb[r] -= dt * aj4 * rnu / hdpn;
+        }
+      }
+    }
+  }
+  m.wnh.assign((size_t)I * m.nkn, 0.);
+  std::vector<double> sol(nlv + 1);
+  for (int k = 0; k < m.nkn; k++) {
+    const int lmax = m.ilhkv[k];
+    if (lmax > 2) {
+      const size_t r = (size_t)k * I + 1;
+      int st = tridag(&wdiagt[r], &wdiag[r], &wdiagb[r], &wrhs[r], sol.data(), lmax - 1);
+      if (st) return st;
+      for (int l = 1; l <= lmax - 1; l++) m.wnh[(size_t)k * I + l] = sol[l - 1];
+    }
+  }
+  return SHY_OK;
+}
+
+// nonhydro_prepare_matrix (nohydro.f90:589-753): per element layer the
+// Poisson element matrix of the non-hydrostatic pressure (horizontal
+// Laplacian times the layer thickness, vertical second differences across
+// the layer interfaces, the free-surface term on the first layer) and the
+// divergence of the predicted flow, assembled with system_assemble_3d
+void nh_prepare_matrix(Model &m) {
+  const int nlv = m.nlv, I = nlv + 1;
+  const double dt = m.p.dt, aq = m.p.aqpar, az = m.p.azpar, azt = 1. - az;
+  m.c3coo.assign(m.nt3g[m.nkn], 0.);                      // system_init
+  m.rvec3d.assign((size_t)(nlv + 2) * m.nkn, 0.);
+  std::vector<double> hld(nlv + 2, 0.);
+  double mass[27], rhs[3];
+  for (int ie = 0; ie < m.nel; ie++) {
+    const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+    for (int l = 1; l <= nlv; l++) hld[l] = m.hdenv[(size_t)ie * nlv + l - 1];
+    const double aj = e[9], aj4 = 4. * aj, aj12 = 12. * aj;
+    int kn[3];
+    double b[3], c[3];
+    for (int ii = 0; ii < 3; ii++) { kn[ii] = m.nen3v[3 * ie + ii]; b[ii] = e[3 + ii]; c[ii] = e[6 + ii]; }
+    const int lmax = m.ilhv[ie];
+    for (int l = 1; l <= lmax; l++) {
+      for (double &v : mass) v = 0.;
+      const double hd = hld[l], hdm = hld[l - 1], hdp = hld[l + 1];
+      double rhm = 2. / (hd + hdm), rhp = 2. / (hd + hdp);
+      if (l == 1) rhm = 0.;
+      if (l == lmax) rhp = 0.;
+      const double rhc = rhm + rhp;
+      for (int n = 0; n < 3; n++) {
+        for (int q = 0; q < 3; q++) {
+          mass[9 + 3 * n + q] = -aj12 * hd * dt * aq * az * (b[n] * b[q] + c[n] * c[q]);
+          if (n == q) {
+            mass[9 + 3 * n + q] -= aj4 * dt * aq * rhc;
+            mass[0 + 3 * n + q] = aj4 * dt * aq * rhm;
+            mass[18 + 3 * n + q] = aj4 * dt * aq * rhp;
+          }
+        }
+        const int k = kn[n];
+        const size_t o = (size_t)ie * nlv + l - 1;
+        const double fhn = m.utlnv[o] * b[n] + m.vtlnv[o] * c[n];
+        const double fho = m.utlov[o] * b[n] + m.vtlov[o] * c[n];
+        const double fvn = m.wnh[(size_t)k * I + l - 1] - m.wnh[(size_t)k * I + l];
+        const double ffh = -(az * fhn + azt * fho);
+        rhs[n] = aj4 * (3. * ffh + fvn);
+      }
+      if (l == 1)
+        for (int i = 0; i < 3; i++) {
+          const int k = kn[i];
+          mass[9 + 4 * i] -= aj4 / (m.p.grav * dt);
+          rhs[i] += aj4 * (m.znv[k] - m.zov[k]) / dt;
+        }
+      assemble_3d(m, ie, l, mass, rhs);
+    }
+  }
+  adjust_3d(m);
+}
+
+// nonhydro_correct_uveta (nohydro.f90:761-829): the water level moves by the
+// surface pressure over g, the transports by the pressure gradient times
+// aqpar dt and the layer thickness
+void nh_correct_uveta(Model &m) {
+  const int nlv = m.nlv;
+  const double aq = m.p.aqpar, dt = m.p.dt;
+  for (int k = 0; k < m.nkn; k++) m.znv[k] += m.qdistv[k] * m.qpnv[(size_t)k * nlv] / m.p.grav;
+  for (int ie = 0; ie < m.nel; ie++) {
+    const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
+    for (int l = 1; l <= m.ilhv[ie]; l++) {
+      double uq = 0., vq = 0.;
+      for (int ii = 0; ii < 3; ii++) {
+        const int k = m.nen3v[3 * ie + ii];
+        const double q = m.qdistv[k] * m.qpnv[(size_t)k * nlv + l - 1];
+        uq += e[3 + ii] * q;
+        vq += e[6 + ii] * q;
+      }
+      const size_t o = (size_t)ie * nlv + l - 1;
+      m.utlnv[o] -= aq * dt * uq * m.hdenv[o];
+      m.vtlnv[o] -= aq * dt * vq * m.hdenv[o];
+    }
+  }
+}
+
+// sp256wnh and nonhydro_adjust (nohydro.f90:109-183) with inhadj = 0: the
+// pressure from the 3D system (guess: zero, the cleared qpnv), the
+// correction of level and transports, setzev, make_new_depth, and the
+// pressure's first layer set to zero (the loop qpnv(l,k) - qpnv(1,k) zeroes
+// qpnv(1,k) first and then subtracts that zero from the layers below)
+int nonhydro_adjust(Model &m) {
+  int st = sp256wnh(m);
+  if (st) return st;
+  nh_prepare_matrix(m);
+  st = solve_3d(m, m.qpnv);
+  if (st) return st;
+  nh_correct_uveta(m);
+  for (int ie = 0; ie < m.nel; ie++)
+    for (int ii = 0; ii < 3; ii++) m.zenv[3 * ie + ii] = m.znv[m.nen3v[3 * ie + ii]];
+  st = setdepth(m, m.hdknv, m.hdenv, m.zenv);
+  if (st) return st;
+  for (int k = 0; k < m.nkn; k++) m.qpnv[(size_t)k * m.nlv] = 0.;
+  return SHY_OK;
 }
 
 // masscont (elems_dealing.f90:1191-1223) -> total volume in FP64
@@ -1931,6 +2278,9 @@ int init_state(Model &m) {
   m.zov = m.znv; m.zeov = m.zenv; m.utlov = m.utlnv; m.vtlov = m.vtlnv;
   m.hdkov = m.hdknv; m.hdeov = m.hdenv;
   m.wlnv.assign((size_t)(m.nlv + 1) * m.nkn, 0.);
+  m.wlov = m.wlnv;
+  m.qpov.assign((size_t)m.nlv * m.nkn, 0.);         // nonhydro_init
+  m.qpnv.assign((size_t)m.nlv * m.nkn, 0.);
   m.rhov.assign((size_t)m.nlv * m.nkn, 0.);
   if (m.p.ibarcl > 0) for (int it = 0; it < 3; it++) rhoset(m);   // barocl(0): rhoset_shell(3)
   uvtopr(m);                                      // make_prvel (initialize.f90:1656)
@@ -1950,6 +2300,11 @@ int step(Model &m) {
   m.zov = m.znv; m.zeov = m.zenv; m.utlov = m.utlnv; m.vtlov = m.vtlnv;
   m.uov = m.unv; m.vov = m.vnv;
   m.hdkov = m.hdknv; m.hdeov = m.hdenv;
+  m.wlov = m.wlnv;
+  if (m.p.inohyd) {                               // nonhydro_copy (shyfem_subs.f90:590)
+    m.qpov = m.qpnv;
+    std::fill(m.qpnv.begin(), m.qpnv.end(), 0.);
+  }
   set_rzv(m);                                     // sp111(2)
   set_mass_flux(m);
   // hydro (hydrodynamic.f90:284-485)
@@ -1987,6 +2342,10 @@ int step(Model &m) {
   }
   st = setdepth(m, m.hdknv, m.hdenv, m.zenv);     // make_new_depth
   if (st) return st;
+  if (m.p.inohyd) {                               // sp256wnh + nonhydro_adjust (:435-438)
+    st = nonhydro_adjust(m);
+    if (st) return st;
+  }
   hydro_vertical(m);
   uvtopr(m);                                      // compute_velocities (hydrodynamic.f90:473)
   m.info.volume = masscont(m);                    // vol_mass(1)
@@ -2112,6 +2471,12 @@ void *shyref_create(const shy_basin *B, const shy_params *P) {
     delete m;
     return nullptr;
   }
+  if (P->inohyd && (P->wetdry || P->nzadapt > 1 || !(P->aqpar > 0.f && P->aqpar <= 1.f))) {
+    fail(SHY_EARG, "shyref_create: non-hydrostatic pressure needs 0 < aqpar <= 1, no wetting and drying and "
+                   "no z-adaptive layers");
+    delete m;
+    return nullptr;
+  }
   m->nen3v.resize((size_t)3 * nel);
   for (size_t i = 0; i < m->nen3v.size(); i++) m->nen3v[i] = B->nen3v[i] - 1;
   std::vector<double> x = dv(B->xgv, nkn), y = dv(B->ygv, nkn);
@@ -2138,6 +2503,8 @@ void *shyref_create(const shy_basin *B, const shy_params *P) {
   diffweight(*m);
   set_ieltv(*m);
   if (coo_init(nkn, nel, m->nen3v.data(), m->ntg, m->icol, m->ijp)) { delete m; return nullptr; }
+  if (P->inohyd) coo3d_init(nkn, nlv, m->ntg, m->nt3g);
+  m->qdistv.assign(nkn, 1.);                  // qhdist with nqdist = 0
   m->rtol = P->solver_rtol > 0 ? P->solver_rtol : 1e-8;
   m->atol = P->solver_atol > 0 ? P->solver_atol : 1e-8;
   m->maxmv = P->solver_maxit > 0 ? P->solver_maxit : 1000;
@@ -2253,6 +2620,95 @@ int shyref_step_info(void *h, shy_step_info *info) {
   info->dtime = m.dtime;
   return SHY_OK;
 }
+
+// the weight of the non-hydrostatic pressure per node (qhdist, nohydro.f90:
+// 962-1040: 0 on open boundaries with nad > 0, rising to 1 inland)
+int shyref_set_nh_distance(void *h, const float *qdist) {
+  Model &m = *(Model *)h;
+  if (!qdist) return fail(SHY_EARG, "set_nh_distance: no array");
+  m.qdistv.assign(qdist, qdist + m.nkn);
+  return SHY_OK;
+}
+
+// the non-hydrostatic pressure qpnv (nkn, nlv) after the last step and the
+// w of sp256wnh (nkn, nlv+1); either may be NULL
+int shyref_get_nh(void *h, double *qpnv, double *wnh) {
+  Model &m = *(Model *)h;
+  if (qpnv) std::copy(m.qpnv.begin(), m.qpnv.end(), qpnv);
+  if (wnh) {
+    if (m.wnh.empty()) std::fill(wnh, wnh + (size_t)(m.nlv + 1) * m.nkn, 0.);
+    else std::copy(m.wnh.begin(), m.wnh.end(), wnh);
+  }
+  return SHY_OK;
+}
+
+// iterations and residuals of the last non-hydrostatic solve
+int shyref_nh_info(void *h, int *iters, double *resid0, double *resid) {
+  Model &m = *(Model *)h;
+  if (iters) *iters = m.nh_iters;
+  if (resid0) *resid0 = m.nh_resid0;
+  if (resid) *resid = m.nh_resid;
+  return SHY_OK;
+}
+
+// The 3D simsys interface on its own (system_assemble_3d, system_adjust_matrix_3d,
+// system_solve_3d, system_get_3d; simsys_spkaux.f90:495-716) over a mesh
+// of nkn nodes, nel elements (1-based nen3v) and nlv layers: the values of
+// the 3D COO (nt3g[nkn] entries) and its right-hand side ((nlv+2)*nkn)
+void *shyref_sys3d_create(int nkn, int nel, int nlv, const int *nen3v) {
+  Model *m = new Model();
+  m->nkn = nkn; m->nel = nel; m->nlv = nlv;
+  m->nen3v.resize((size_t)3 * nel);
+  for (size_t i = 0; i < m->nen3v.size(); i++) m->nen3v[i] = nen3v[i] - 1;
+  if (coo_init(nkn, nel, m->nen3v.data(), m->ntg, m->icol, m->ijp)) { delete m; return nullptr; }
+  coo3d_init(nkn, nlv, m->ntg, m->nt3g);
+  m->c3coo.assign(m->nt3g[nkn], 0.);
+  m->rvec3d.assign((size_t)(nlv + 2) * nkn, 0.);
+  return m;
+}
+
+int shyref_sys3d_nnz(void *h) { return ((Model *)h)->nt3g[((Model *)h)->nkn]; }
+
+// ie, l 1-based as the reference passes them; mass(-1:1,3,3) in Fortran order
+int shyref_sys3d_assemble(void *h, int ie, int l, const float *mass, const float *rhs) {
+  Model &m = *(Model *)h;
+  if (ie < 1 || ie > m.nel || l < 1 || l > m.nlv) return fail(SHY_EARG, "sys3d_assemble: ie or l out of range");
+  double ms[27], r[3];
+  for (int d = 0; d < 3; d++)
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) ms[d * 9 + 3 * i + j] = mass[d + 3 * i + 9 * j];
+  for (int i = 0; i < 3; i++) r[i] = rhs[i];
+  assemble_3d(m, ie - 1, l, ms, r);
+  return SHY_OK;
+}
+
+int shyref_sys3d_adjust(void *h) { adjust_3d(*(Model *)h); return SHY_OK; }
+
+// z (nkn, nlv) rows: the guess in, the solution out
+int shyref_sys3d_solve(void *h, double *z, int *iters) {
+  Model &m = *(Model *)h;
+  std::vector<double> zz(z, z + (size_t)m.nkn * m.nlv);
+  int st = solve_3d(m, zz);
+  if (iters) *iters = m.nh_iters;
+  if (st) return st;
+  std::copy(zz.begin(), zz.end(), z);
+  return SHY_OK;
+}
+
+int shyref_sys3d_get(void *h, double *val, double *rhs, int *ia, int *ja) {
+  Model &m = *(Model *)h;
+  if (val) std::copy(m.c3coo.begin(), m.c3coo.end(), val);
+  if (rhs) std::copy(m.rvec3d.begin(), m.rvec3d.end(), rhs);
+  if (ia || ja) {
+    std::vector<int> a, b;
+    coo3d_csr(m, a, b);
+    if (ia) std::copy(a.begin(), a.end(), ia);
+    if (ja) std::copy(b.begin(), b.end(), ja);
+  }
+  return SHY_OK;
+}
+
+void shyref_sys3d_destroy(void *h) { delete (Model *)h; }
 
 // matrix of the last assembly (for the assembly parity test)
 int shyref_last_system(void *h, int *nnz, double *val, double *rhs) {

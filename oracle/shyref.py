@@ -50,6 +50,17 @@ def _lib():
     lib.shyref_element_system.argtypes = [d_p, d_p] + [C.c_double] * 6 + [d_p] + [C.c_double] * 4 + [d_p, d_p]
     lib.shyref_spk_solve.argtypes = [C.c_int, i_p, i_p, d_p, d_p, d_p, C.c_double, C.c_double,
                                      C.c_int, i_p, d_p, d_p]
+    lib.shyref_set_nh_distance.argtypes = [C.c_void_p, C.c_void_p]
+    lib.shyref_get_nh.argtypes = [C.c_void_p, d_p, d_p]
+    lib.shyref_nh_info.argtypes = [C.c_void_p, i_p, d_p, d_p]
+    lib.shyref_sys3d_create.restype = C.c_void_p
+    lib.shyref_sys3d_create.argtypes = [C.c_int, C.c_int, C.c_int, i_p]
+    lib.shyref_sys3d_nnz.argtypes = [C.c_void_p]
+    lib.shyref_sys3d_assemble.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    lib.shyref_sys3d_adjust.argtypes = [C.c_void_p]
+    lib.shyref_sys3d_solve.argtypes = [C.c_void_p, d_p, i_p]
+    lib.shyref_sys3d_get.argtypes = [C.c_void_p, d_p, d_p, i_p, i_p]
+    lib.shyref_sys3d_destroy.argtypes = [C.c_void_p]
     return lib
 
 
@@ -214,6 +225,22 @@ class OracleModel:
         check(lib.shyref_get_load(self.h, dptr(out)), "get_load")
         return out
 
+    def set_nh_distance(self, qdist):
+        """The weight of the non-hydrostatic pressure per node (qhdist)."""
+        a = np.ascontiguousarray(qdist, np.float32)
+        self._qdist = a
+        check(lib.shyref_set_nh_distance(self.h, a.ctypes.data), "set_nh_distance")
+
+    def nh(self):
+        """(qpnv (nkn, nlv), wnh (nkn, nlv+1), (iters, resid0, resid)) of the last step."""
+        c = self.case
+        q = np.zeros((c["nkn"], c["nlv"]))
+        w = np.zeros((c["nkn"], c["nlv"] + 1))
+        check(lib.shyref_get_nh(self.h, dptr(q), dptr(w)), "get_nh")
+        it, r0, r = C.c_int(0), C.c_double(0), C.c_double(0)
+        lib.shyref_nh_info(self.h, C.byref(it), C.byref(r0), C.byref(r))
+        return q, w, (it.value, r0.value, r.value)
+
     def last_system(self):
         nnz = C.c_int(0)
         lib.shyref_last_system(self.h, C.byref(nnz), None, None)
@@ -225,4 +252,45 @@ class OracleModel:
     def __del__(self):
         if getattr(self, "h", None):
             lib.shyref_destroy(self.h)
+            self.h = None
+
+
+class System3D:
+    """The reference's 3D simsys interface (system_assemble_3d,
+    system_adjust_matrix_3d, system_solve_3d, system_get_3d) restated on the
+    CPU over one mesh: the 3D COO of coo_init_new and loccoo3d."""
+
+    def __init__(self, nkn, nel, nlv, nen3v):
+        self.nkn, self.nel, self.nlv = nkn, nel, nlv
+        nen = np.ascontiguousarray(nen3v, np.int32)
+        self.h = lib.shyref_sys3d_create(nkn, nel, nlv, iptr(nen))
+        if not self.h:
+            raise RuntimeError("sys3d_create: " + lib.shyref_last_error().decode())
+
+    def assemble(self, ie, l, mass, rhs):
+        """mass (3, 3, 3) indexed [d+1, i, j] for the reference's mass(d, i, j)."""
+        m = np.asfortranarray(np.asarray(mass, np.float32).transpose(0, 1, 2))
+        r = np.ascontiguousarray(rhs, np.float32)
+        check(lib.shyref_sys3d_assemble(self.h, ie, l, m.ctypes.data, r.ctypes.data), "sys3d_assemble")
+
+    def adjust(self):
+        lib.shyref_sys3d_adjust(self.h)
+
+    def solve(self, z0):
+        z = np.ascontiguousarray(z0, np.float64).copy()
+        it = C.c_int(0)
+        check(lib.shyref_sys3d_solve(self.h, dptr(z), C.byref(it)), "sys3d_solve")
+        return z, it.value
+
+    def matrix(self):
+        nnz = lib.shyref_sys3d_nnz(self.h)
+        n = (self.nlv + 2) * self.nkn
+        val, rhs = np.zeros(nnz), np.zeros(n)
+        ia, ja = np.zeros(n + 1, np.int32), np.zeros(nnz, np.int32)
+        lib.shyref_sys3d_get(self.h, dptr(val), dptr(rhs), iptr(ia), iptr(ja))
+        return ia, ja, val, rhs
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.shyref_sys3d_destroy(self.h)
             self.h = None

@@ -883,6 +883,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: itvd=%d: upwind (0), TVD with node gradients (1) or upwind points (2)", b, Pp[b].itvd));
     if (Pp[b].wetdry && !(Pp[b].hzmin > 0.f && Pp[b].hzoff >= Pp[b].hzmin && Pp[b].hzon >= Pp[b].hzoff))
       return bail(fail(SHY_EARG, "basin %d: wetting and drying needs 0 < hzmin <= hzoff <= hzon", b));
+    if (Pp[b].inohyd)
+      return bail(fail(SHY_EARG, "basin %d: non-hydrostatic pressure (inohyd) is not available in this build", b));
     NLV = std::max(NLV, bs.nlv);
   }
   m->nbasin = nbasin; m->NLV = NLV; m->S = next_pow2(NLV);

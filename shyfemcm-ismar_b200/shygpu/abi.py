@@ -52,6 +52,7 @@ class ShyParams(C.Structure):
         ("wetdry", C.c_int32), ("hzmin", C.c_float), ("hzon", C.c_float), ("volmin", C.c_float),
         ("rlin", C.c_float), ("itvd", C.c_int32), ("itvdv", C.c_int32),
         ("ihwadv", C.c_int32), ("nzadapt", C.c_int32),
+        ("inohyd", C.c_int32), ("aqpar", C.c_float), ("ivwadv", C.c_int32), ("inhflx", C.c_int32),
     ]
 
 
@@ -141,6 +142,10 @@ def make_params(case, **over):
     s.itvdv = int(p.get("itvdv", 0))
     s.ihwadv = int(p.get("ihwadv", 0))
     s.nzadapt = int(p.get("nzadapt", 0))
+    s.inohyd = int(p.get("inohyd", 0))
+    s.aqpar = float(p.get("aqpar", 0.5))
+    s.ivwadv = int(p.get("ivwadv", 0))
+    s.inhflx = int(p.get("inhflx", 0))
     return s
 
 

@@ -355,6 +355,31 @@ def shelf_case(nkn_target=1500, lx=20.0e3, ly=8.0e3, seed=11, dt=60.0, nzadapt=3
     return _finish(case)
 
 
+def seiche_case(lx=50.0, ly=10.0, nx=21, ny=5, depth=25.0, nlv=10, ampli=0.01, dt=0.1, inohyd=1,
+                seed=13, jitter=0.1):
+    """Standing wave in a deep closed basin, for the non-hydrostatic
+    pressure (nohydro.f90): a flat `depth` m basin `lx` m long, `nlv`
+    equal z-layers, no friction, no wind, linear momentum, the initial
+    level `ampli` cos(pi x / lx).  With k = pi / lx and k H near pi/2 the
+    hydrostatic period 2 pi / (k sqrt(g H)) and the non-hydrostatic one
+    2 pi / sqrt(g k tanh(k H)) differ by a quarter."""
+    x, y, nen3v, ii, jj = structured_triangles(nx, ny, lx, ly, jitter, seed)
+    x[ii == 0] = 0.0
+    x[ii == nx - 1] = lx
+    nkn, nel = x.size, nen3v.shape[0]
+    hm3v = np.full((nel, 3), depth, np.float32)
+    hlv, hldv = z_layers(np.full(nlv, depth / nlv))
+    hlv[-1] = depth + 1.0
+    hldv[-1] = hlv[-1] - (hlv[-2] if nlv > 1 else 0.0)
+    ilhv, ilhkv = layer_counts(nen3v, hm3v, hlv, hldv, nkn)
+    znv = (ampli * np.cos(np.pi * x / lx)).astype(np.float32)
+    case = dict(name=f"seiche_{nkn}x{nlv}_nh{inohyd}", nkn=nkn, nel=nel, nlv=nlv, nen3v=nen3v,
+                xgv=x, ygv=y, hm3v=hm3v, hlv=hlv, hldv=hldv, ilhv=ilhv, ilhkv=ilhkv,
+                bnd_index=np.zeros(nkn, np.int32), tide=np.zeros((0, 1, 4), np.float32), seed=seed,
+                params=dict(dt=dt, ireib=0, inohyd=inohyd), znv=znv)
+    return _finish(case)
+
+
 def ensemble_member_case(nkn_target, aspect, seed, wind, dt=60.0, nlv=10, spacing=100.0,
                          ampli=0.5, depth=10.0, ddepth=2.0, top=2.0):
     """One member of the batched ensemble, made as the 2D channel is: a
