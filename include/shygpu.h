@@ -226,6 +226,21 @@ int shygpu_get_wetdry(shygpu_model *model, int32_t ibasin, int32_t *iwegv,
                       int32_t *iwetv, int32_t *inodv);
 int shygpu_step_info(shygpu_model *model, int32_t ibasin, shy_step_info *info);
 
+/* Non-hydrostatic pressure of a basin made with inohyd = 1 (nohydro.f90).
+ * Each step, after the hydrostatic transports, solves the 3D pressure
+ * system (nonhydro_prepare_matrix, :589-753, from the w of sp256wnh,
+ * :205-524) and corrects levels and transports (nonhydro_correct_uveta,
+ * :761-829).  set_nh_distance replaces the per-node weight of the pressure
+ * (qdistv, made by qhdist :962-1040 from the open boundaries' nad; 1 by
+ * default), values in [0, 1].  get_nh_pressure copies the pressure the
+ * next step starts from, (nlv,nkn), first layer zero (qpnv after
+ * nonhydro_adjust).  nh_info gives the last solve's Krylov iterations,
+ * FP64 refinements and residuals (initial, final).                        */
+int shygpu_set_nh_distance(shygpu_model *model, int32_t ibasin, const float *qdistv);
+int shygpu_get_nh_pressure(shygpu_model *model, int32_t ibasin, float *qpnv);
+int shygpu_nh_info(shygpu_model *model, int32_t ibasin, int32_t *iters, int32_t *refinements,
+                   double *resid0, double *resid);
+
 /* Per-step forcing of a basin from host memory (pinned for overlap):
  * tauxnv, tauynv, ppv, rqv (nkn each); NULL members are left unchanged.
  * The copies are queued on the model's stream ahead of the next step,
@@ -432,6 +447,17 @@ int shygpu_simsys_set_tolerance(double rtol, double atol, int32_t maxit);
 int shygpu_simsys_get_matrix(int32_t *n, int32_t *nnz, int32_t *rowptr,
                              int32_t *col, double *val, double *rhs);
 int shygpu_simsys_iterations(void);
+/* The 3D system of the non-hydrostatic pressure and of poisson_3d
+ * (coo_init_new's 3D part, coo_matrix.f90:180-247): nlv layers (levels ::
+ * nlv, read by system_initialize from its module) are declared here before
+ * system_initialize_; 0 (the default) leaves the 3D system out, as the
+ * reference does without bsys3d.  Its unknowns are (nlv+2) per node, layer
+ * 0 and nlv+1 padding rows with a unit diagonal.                          */
+int shygpu_simsys_set_layers(int32_t nlv);
+/* The assembled 3D matrix of the last solve, CSR over (nlv+2)*nkn rows in
+ * the order of the reference's c3coo (FP64), and its right-hand side.     */
+int shygpu_simsys_get_matrix_3d(int32_t *n, int32_t *nnz, int32_t *rowptr,
+                                int32_t *col, double *val, double *rhs);
 
 /* Solve A x = rhs for one sparse system whose CSR arrays (0-based, rows with
  * their diagonal stored), right-hand side, start x0 and result x are all in
@@ -512,6 +538,20 @@ void system_add_rhs_(const float *dt, const int32_t *n, const float *array); /* 
 void system_solve_(const int32_t *n, const float *z);                        /* :454 */
 void system_get_(const int32_t *n, float *z);                                /* :638 */
 void system_finalize_(void);                        /* :722  */
+/* The 3D interface (simsys_spkaux.f90:495-716), used by nonhydro_prepare_
+ * matrix (nohydro.f90:589-753) and poisson_3d (poisson.f90:272-445):
+ * mass(-1:1,3,3) and rhs(3) of element ie, layer l, nodes kn (Fortran
+ * order, mass[(d+1) + 3*(i-1) + 9*(j-1)]) are added to the rows of layer l
+ * and their couplings to layers l-1 and l+1; adjust_matrix sets a unit
+ * diagonal where no element layer reached it; solve_3d takes z(nlvdi,n)
+ * as the guess and solves on the GPU (BiCGStab in FP32 inside FP64
+ * refinement, the stop test of system_solve_); get_3d copies the solution
+ * into z(nlvdi,n).                                                        */
+void system_assemble_3d_(const int32_t *ie, const int32_t *l, const int32_t *nlv, const int32_t *kn,
+                         const float *mass, const float *rhs);                          /* :597 */
+void system_adjust_matrix_3d_(void);                                                  /* :709 */
+void system_solve_3d_(const int32_t *n, const int32_t *nlvdi, const int32_t *nlv, const float *z); /* :495 */
+void system_get_3d_(const int32_t *n, const int32_t *nlvdi, const int32_t *nlv, float *z);        /* :657 */
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,9 @@ struct BasinPar {
   int ihwadv;                 // vertical momentum advection (with adv): 0 none, 1 upwind, 2 centred
   int nzadapt;                // z-layers with z-adaptive surface layers when > 1
   double rzmov;               // their threshold factor (compute_rzmov_info)
+  int inohyd;                 // non-hydrostatic pressure (nohydro.f90)
+  float aqpar;                // its semi-implicit weight
+  int ivwadv, inhflx;         // vertical / horizontal advection of w in sp256wnh
 };
 
 // set_advective's vertical term (explicit.f90:776-833) of one layer from
@@ -85,6 +88,8 @@ struct BasinOut {
   int istot;
   int steps;                  // steps completed since the state was set
   float stab[kMaxScal];       // stability index (as float bits, max-reduced)
+  int nh_iters, nh_refinements;   // the last non-hydrostatic pressure solve
+  double nh_resid0, nh_resid;
 };
 
 // everything a kernel needs, passed by value
@@ -98,6 +103,10 @@ struct Dev {
   float2 *tgrad;                // (nsc_max*NKN*NLV) node gradients {gx, gy} of the sub-step's scalars
   int4 *tvdup;                  // (6*NEL) itvd = 2: {element, xi0, xi1, xi2 as float bits} per vertex pair
   float *andg;                  // (NKN) water-level nudging contribution andgzv, or null (none set)
+  // non-hydrostatic pressure of the basins with inohyd = 1 (null when no
+  // basin has it): qp (NKN*NLV) the pressure of the last step as the next
+  // one reads it (qpov), qdist (NKN) its weight per node (qdistv)
+  float *qp, *qdist;
   int conz_free_bnd;            // 1: k_conz leaves open-boundary values to the caller (shygpu_conz3d)
   // shygpu_conz3d's source terms (k_conz<S, 1, true> only): nudging to
   // cz_obs at rate cz_robs*cz_tau, settling cz_wsink*cz_wsv (NKN*(NLV+1)),

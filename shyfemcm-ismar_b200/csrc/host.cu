@@ -268,6 +268,11 @@ struct shygpu_model {
   bool any_wd = false;               // some basin has wetting and drying
   bool any_adv = false;              // some basin has momentum advection (ilin = 0)
   bool any_tvd = false;              // some basin transports with TVD (itvd = 1)
+  bool any_nh = false;               // some basin has the non-hydrostatic pressure
+  NhSys nh;                          // its 3D system (rows of every such basin)
+  CsrGrid nhg;                       // the solver's work arrays
+  std::vector<int2> nh_rows;         // per basin its rows [x, y) (empty range: hydrostatic)
+  int nh_G = 0;                      // CTAs of the solver's launch at most
   std::vector<BasinPar> par;
   std::vector<int> nlv_b;
   Arena arena;
@@ -845,6 +850,65 @@ static int next_pow2(int n) {
   return s;
 }
 
+// The 3D system of the non-hydrostatic pressure (coo_init_new's 3D part,
+// coo_matrix.f90:180-247, without the padding layers and the layers below a
+// node's deepest element): for each active node layer (k, l) the 2D row's
+// columns at layer l, where that node has the layer, with (k,l-1), (k,l),
+// (k,l+1) in the diagonal's place; the same order in which k_nh_sys writes
+// the values.  Also the pressure, its weights (1: qhdist without nqdist)
+// and the solver's work arrays.
+static int build_nh(shygpu_model *m, const std::vector<int> &kbas, const std::vector<int> &ilhkv,
+                    const std::vector<int> &rowptr, const std::vector<int> &col) {
+  Arena &A = m->arena;
+  Dev &d = m->base;
+  const int NKN = m->NKN, NLV = m->NLV;
+  std::vector<int> roff(NKN, -1), rnode, rp(1, 0), cl;
+  m->nh_rows.assign(m->nbasin, make_int2(0, 0));
+  int nrow = 0;
+  for (int b = 0; b < m->nbasin; b++) {
+    const BasinPar &bp = m->par[b];
+    m->nh_rows[b] = make_int2(nrow, nrow);
+    if (!bp.inohyd) continue;
+    for (int k = bp.k0; k < bp.k0 + bp.nk; k++) { roff[k] = nrow; nrow += ilhkv[k]; }
+    m->nh_rows[b].y = nrow;
+  }
+  rnode.resize(nrow);
+  for (int k = 0; k < NKN; k++)
+    if (roff[k] >= 0)
+      for (int l = 1; l <= ilhkv[k]; l++) {
+        rnode[roff[k] + l - 1] = k;
+        for (int sl = rowptr[k]; sl < rowptr[k + 1]; sl++) {
+          const int kj = col[sl];
+          if (kj != k) { if (ilhkv[kj] >= l) cl.push_back(roff[kj] + l - 1); }
+          else {
+            if (l > 1) cl.push_back(roff[k] + l - 2);
+            cl.push_back(roff[k] + l - 1);
+            if (l < ilhkv[k]) cl.push_back(roff[k] + l);
+          }
+        }
+        rp.push_back((int)cl.size());
+      }
+  const size_t nnz = cl.size();
+  NhSys &s = m->nh;
+  CsrGrid &g = m->nhg;
+  s.nrow = nrow;
+  m->nh_G = std::max(1, nh_solve_capacity());
+  int *dkbas = nullptr, *droff = nullptr, *drnode = nullptr, *drp = nullptr, *dcl = nullptr;
+  if (A.upload(&dkbas, kbas) || A.upload(&droff, roff) || A.upload(&drnode, rnode) || A.upload(&drp, rp) ||
+      A.upload(&dcl, cl) || A.alloc(&s.val, nnz) || A.alloc(&s.rhs, nrow) || A.alloc(&s.x, nrow) ||
+      A.alloc(&s.wnh, (size_t)NKN * (NLV + 1)) || A.alloc(&d.qp, (size_t)NKN * NLV) ||
+      A.upload(&d.qdist, std::vector<float>(NKN, 1.f)) || A.alloc(&g.val32, nnz) || A.alloc(&g.dinv, nrow) ||
+      A.alloc(&g.x64, nrow) || A.alloc(&g.r, nrow) || A.alloc(&g.rh, nrow) || A.alloc(&g.p, nrow) ||
+      A.alloc(&g.v, nrow) || A.alloc(&g.s, nrow) || A.alloc(&g.t, nrow) || A.alloc(&g.z, nrow) ||
+      A.alloc(&g.q, nrow) || A.alloc(&g.e, nrow) || A.alloc(&g.part, (size_t)8 * m->nh_G) ||
+      A.alloc(&g.ctr, 4))
+    return SHY_ECAPACITY;
+  s.kbas = dkbas; s.roff = droff; s.rnode = drnode; s.rowptr = drp; s.col = dcl;
+  g.rowptr = drp; g.col = dcl; g.val = s.val; g.rhs = s.rhs; g.x = s.x;
+  CUDA_TRY(cudaMemset(d.qp, 0, sizeof(float) * NKN * NLV));
+  return SHY_OK;
+}
+
 extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_params *Pp,
                              shygpu_model **out) {
   if (!out) return fail(SHY_EARG, "create: model pointer is NULL");
@@ -883,8 +947,10 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: itvd=%d: upwind (0), TVD with node gradients (1) or upwind points (2)", b, Pp[b].itvd));
     if (Pp[b].wetdry && !(Pp[b].hzmin > 0.f && Pp[b].hzoff >= Pp[b].hzmin && Pp[b].hzon >= Pp[b].hzoff))
       return bail(fail(SHY_EARG, "basin %d: wetting and drying needs 0 < hzmin <= hzoff <= hzon", b));
-    if (Pp[b].inohyd)
-      return bail(fail(SHY_EARG, "basin %d: non-hydrostatic pressure (inohyd) is not available in this build", b));
+    if (Pp[b].inohyd && (Pp[b].wetdry || Pp[b].nzadapt > 1 || !(Pp[b].aqpar > 0.f && Pp[b].aqpar <= 1.f) ||
+                         Pp[b].ivwadv < 0 || Pp[b].ivwadv > 2 || Pp[b].inhflx < 0 || Pp[b].inhflx > 1))
+      return bail(fail(SHY_EARG, "basin %d: non-hydrostatic pressure (inohyd) needs 0 < aqpar <= 1, ivwadv 0..2, "
+                                 "inhflx 0..1, no wetting and drying and no z-adaptive layers", b));
     NLV = std::max(NLV, bs.nlv);
   }
   m->nbasin = nbasin; m->NLV = NLV; m->S = next_pow2(NLV);
@@ -1060,6 +1126,9 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       bp.rzmov = bp.nzadapt >= bs.nlv ? 10000.
                                       : (double)hv[bp.nzadapt - 2] / ((double)hv[bp.nzadapt - 1] - (double)hv[bp.nzadapt - 2]);
     }
+    bp.inohyd = p.inohyd ? 1 : 0;
+    bp.aqpar = p.aqpar; bp.ivwadv = p.ivwadv; bp.inhflx = p.inhflx;
+    m->any_nh |= bp.inohyd != 0;
     bp.itemp = p.itemp ? 1 : 0; bp.isalt = p.isalt ? 1 : 0;
     int ns = 0;
     if (bp.itemp) { bp.rkpar[ns] = p.thpar; bp.is_temp[ns] = 1; ns++; }
@@ -1138,6 +1207,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   if (nsc_max > 0 && (A.alloc(&d.cz_ef, (size_t)3 * NEL * nsc_max * NLV) || A.alloc(&d.cz_ef1, (size_t)3 * NEL * NLV)))
     return bail(SHY_ECAPACITY);
   if (any_up && A.upload(&d.tvdup, tvdup)) return bail(SHY_ECAPACITY);
+  if (m->any_nh)
+    if (int st = build_nh(m, kbas, ilhkv, rowptr, col)) return bail(st);
   for (int i = 0; i < 2; i++) {
     if (A.alloc(&m->zbuf[i], NKN) || A.alloc(&m->zebuf[i], (size_t)3 * NEL) ||
         A.alloc(&m->ubuf[i], EL) || A.alloc(&m->vbuf[i], EL) || A.alloc(&m->hkbuf[i], NL) ||
@@ -1314,6 +1385,8 @@ extern "C" int shygpu_set_state(shygpu_model *m, int32_t ib, const shy_state *s)
     for (int cc = 0; cc < bp.nsc - bp.itemp - bp.isalt; cc++)
       ST_TRY(copy_cols(m->scbuf[m->sc_cur] + scalar_index(bp, 2, cc) * SN, s->conzv + (size_t)cc * bp.nk * nlv,
                        bp.nk, nlv, NLV, bp.k0, true, st));
+  if (bp.inohyd)                   // nonhydro_init: no pressure yet
+    CUDA_TRY(cudaMemsetAsync(m->base.qp + (size_t)bp.k0 * NLV, 0, sizeof(float) * bp.nk * NLV, st));
   // boundary values of the scalars: the initial columns
   for (int sc = 0; sc < bp.nsc; sc++)
     CUDA_TRY(cudaMemcpyAsync(m->base.cbnd + sc * SN + (size_t)bp.k0 * NLV, m->scbuf[m->sc_cur] + sc * SN + (size_t)bp.k0 * NLV,
@@ -1371,6 +1444,41 @@ extern "C" int shygpu_get_state(shygpu_model *m, int32_t ib, shy_state *s) {
 // ---------------------------------------------------------------------------
 // the step
 // ---------------------------------------------------------------------------
+// sp256wnh and nonhydro_adjust (hydrodynamic.f90:435-438) for the basins with
+// inohyd = 1, after k_final and before k_node: w of the vertical momentum
+// equation, the 3D system, its solve per basin from a zero guess (the
+// cleared qpnv), the correction of levels and transports
+static int enqueue_nh(shygpu_model *m, const Dev &d) {
+  const NhSys &s = m->nh;
+  launch_nh(d, s, 0, m->stream);
+  launch_nh(d, s, 1, m->stream);
+  CUDA_TRY(cudaMemsetAsync(s.x, 0, sizeof(float) * s.nrow, m->stream));
+  for (int b = 0; b < m->nbasin; b++) {
+    const int2 rr = m->nh_rows[b];
+    if (rr.y <= rr.x) continue;
+    const BasinPar &bp = m->par[b];
+    CsrGrid g = m->nhg;
+    g.r0 = rr.x; g.r1 = rr.y;
+    g.out = d.out + b;
+    g.rtol = bp.rtol; g.atol = bp.atol; g.maxit = bp.maxit;
+    g.max_outer = m->max_outer; g.inner_rtol = m->inner_rtol;
+    const int G = std::min(m->nh_G, std::max(1, (rr.y - rr.x + 2047) / 2048));
+    cudaError_t e = launch_nh_solve(g, G, m->stream);
+    if (e != cudaSuccess) return fail(SHY_ECUDA, "non-hydrostatic solve launch: %s", cudaGetErrorString(e));
+  }
+  launch_nh(d, s, 2, m->stream);
+  launch_nh(d, s, 3, m->stream);
+  return SHY_OK;
+}
+
+// kernel launches of enqueue_nh
+static int nh_launches(const shygpu_model *m) {
+  if (!m->any_nh) return 0;
+  int n = 4;
+  for (const int2 &r : m->nh_rows) n += r.y > r.x ? 1 : 0;
+  return n;
+}
+
 static int enqueue_hydro(shygpu_model *m, const Dev &d) {
   if (m->any_adv) launch_node(d, m->kbas, 5, 0, 0, m->stream);   // set_momentum_flux
   if (m->any_wd) launch_wetdry(d, m->kbas, 0, -1, m->stream);    // set_dry
@@ -1380,6 +1488,7 @@ static int enqueue_hydro(shygpu_model *m, const Dev &d) {
   za.explicit_mode = 0; za.inner_rtol = m->inner_rtol; za.tol_frac = m->tol_frac; za.max_outer = m->max_outer; za.sym = m->sym;
   ST_TRY(launch_zeta_plan(m, d, za));
   launch_elem(d, 1, 0, m->stream, m->cor);
+  if (m->any_nh) ST_TRY(enqueue_nh(m, d));
   launch_node(d, m->kbas, 0, 0, 0, m->stream);
   return SHY_OK;
 }
@@ -1417,7 +1526,8 @@ static int enqueue_scalar(shygpu_model *m, Dev d, int sc_cur, int *nconz) {
 
 // launches of one step apart from the transport sub-steps
 static int count_launches(const shygpu_model *m) {
-  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0) + (m->has_rho ? 1 : 0) + (m->any_wd ? 1 : 0) + (m->any_adv ? 1 : 0);
+  return 4 + 1 + (m->nsc_max > 0 ? 1 : 0) + (m->has_rho ? 1 : 0) + (m->any_wd ? 1 : 0) + (m->any_adv ? 1 : 0) +
+         nh_launches(m);
 }
 
 static int enqueue_step(shygpu_model *m) {
@@ -1441,11 +1551,11 @@ static int check_outputs(shygpu_model *m) {
   for (int b = 0; b < m->nbasin; b++) {
     int s = m->out_h[b].status;
     if (s) {
-      const char *why = s == SHY_ENOCONV ? "zeta solve did not converge"
+      const char *why = s == SHY_ENOCONV ? "a Krylov solve (zeta or non-hydrostatic pressure) did not converge"
                         : s == SHY_EDEPTH ? "non-positive layer thickness"
                         : s == SHY_EISTOT ? "transport sub-steps above the limit or the captured sub-step budget (option 'substeps')"
                         : s == SHY_ESINGULAR ? "zero pivot in a vertical transport system"
-                        : s == SHY_ECUDA ? "a wait of the device-wide zeta solver ran out (grid barrier)"
+                        : s == SHY_ECUDA ? "a wait of a device-wide solver ran out (grid barrier)"
                         : "error";
       for (int q = 0; q < m->nbasin; q++)
         cudaMemsetAsync(&m->base.out[q].status, 0, sizeof(int), m->stream);
@@ -1563,7 +1673,7 @@ extern "C" int shygpu_hydro(shygpu_model *m) {
   if (!m || !m->state_set) return fail(SHY_ESTATE, "hydro: no state");
   Dev d = dev_for_step(m, 1 - m->cur);
   ST_TRY(enqueue_hydro(m, d));
-  g_launches += 4;
+  g_launches += 4 + nh_launches(m);
   m->cur = 1 - m->cur;
   CUDA_TRY(cudaGetLastError());
   return check_outputs(m);
@@ -2556,6 +2666,40 @@ extern "C" int shygpu_step_info(shygpu_model *m, int32_t ib, shy_step_info *info
   return SHY_OK;
 }
 
+extern "C" int shygpu_set_nh_distance(shygpu_model *m, int32_t ib, const float *qdist) {
+  if (!m || !qdist || ib < 0 || ib >= m->nbasin) return fail(SHY_EARG, "set_nh_distance: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  if (!bp.inohyd) return fail(SHY_EARG, "set_nh_distance: basin %d has no non-hydrostatic pressure", ib);
+  for (int k = 0; k < bp.nk; k++)
+    if (!(qdist[k] >= 0.f && qdist[k] <= 1.f)) return fail(SHY_EARG, "set_nh_distance: weights in [0, 1]");
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  CUDA_TRY(cudaMemcpy(m->base.qdist + bp.k0, qdist, sizeof(float) * bp.nk, cudaMemcpyHostToDevice));
+  return SHY_OK;
+}
+
+extern "C" int shygpu_get_nh_pressure(shygpu_model *m, int32_t ib, float *qpnv) {
+  if (!m || !qpnv || ib < 0 || ib >= m->nbasin) return fail(SHY_EARG, "get_nh_pressure: bad arguments");
+  const BasinPar &bp = m->par[ib];
+  if (!bp.inohyd) return fail(SHY_EARG, "get_nh_pressure: basin %d has no non-hydrostatic pressure", ib);
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  ST_TRY(copy_cols(m->base.qp, qpnv, bp.nk, bp.nlv, m->NLV, bp.k0, false, m->stream));
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  return SHY_OK;
+}
+
+extern "C" int shygpu_nh_info(shygpu_model *m, int32_t ib, int32_t *iters, int32_t *refinements, double *resid0,
+                              double *resid) {
+  if (!m || ib < 0 || ib >= m->nbasin) return fail(SHY_EARG, "nh_info: bad arguments");
+  BasinOut o;
+  CUDA_TRY(cudaStreamSynchronize(m->stream));
+  CUDA_TRY(cudaMemcpy(&o, m->base.out + ib, sizeof o, cudaMemcpyDeviceToHost));
+  if (iters) *iters = o.nh_iters;
+  if (refinements) *refinements = o.nh_refinements;
+  if (resid0) *resid0 = o.nh_resid0;
+  if (resid) *resid = o.nh_resid;
+  return SHY_OK;
+}
+
 // ===========================================================================
 // simsys: the reference's linear-system interface (simsys_spkaux.f90)
 // ===========================================================================
@@ -2578,6 +2722,17 @@ struct Simsys {
   int maxit = 1000;
   int last_iters = 0;
   cudaStream_t st = nullptr;
+  // the 3D system (bsys3d): nlv3 layers, unknowns (nlv3+2) per node; the
+  // 2D pattern's rows (rowptr2/col2) locate element entries as loccoo3d
+  // does; the COO values and right-hand side accumulate on the host in call
+  // order, as the reference's c3coo/rvec3d
+  int nlv3 = 0, n3 = 0;
+  std::vector<int> rowptr2, col2, nt3g, rowptr3, col3;
+  std::vector<double> c3, rvec3;
+  Arena arena3;
+  NhSys s3{};
+  CsrGrid g3{};
+  int G3 = 0;
 };
 Simsys g_sys;
 
@@ -2604,9 +2759,73 @@ extern "C" int shygpu_simsys_register(int32_t nkn, int32_t nel, const int32_t *n
   return SHY_OK;
 }
 
+extern "C" int shygpu_simsys_set_layers(int32_t nlv) {
+  if (nlv < 0 || nlv > 4096) return fail(SHY_EARG, "simsys_set_layers: nlv outside 0..4096");
+  g_sys.nlv3 = nlv;
+  g_sys.initialized = false;
+  return SHY_OK;
+}
+
 extern "C" int shygpu_simsys_set_tolerance(double rtol, double atol, int32_t maxit) {
   if (!(rtol > 0) || !(atol >= 0) || maxit < 1) return fail(SHY_EARG, "simsys_set_tolerance: bad arguments");
   g_sys.rtol = rtol; g_sys.atol = atol; g_sys.maxit = maxit;
+  return SHY_OK;
+}
+
+// coo_init_new's 3D part (coo_matrix.f90:180-247) in CSR form: row block
+// of node k = the layer-0 diagonal, per layer l the node's sorted
+// neighbours at l with (k,l-1), (k,l), (k,l+1) in the diagonal's place, the
+// layer-(nlv+1) diagonal; unknown u(k,l) = k*(nlv+2) + l.  The device holds
+// the pattern, the values, the right-hand side and the solver's work arrays.
+static int simsys3d_init(const Pattern &pt) {
+  Simsys &S = g_sys;
+  S.arena3.release();
+  if (S.nlv3 <= 0) return SHY_OK;
+  const int nkn = S.nkn, nlv = S.nlv3;
+  S.rowptr2 = pt.rowptr;
+  S.col2 = pt.col;
+  S.n3 = (nlv + 2) * nkn;
+  S.nt3g.assign(nkn + 1, 0);
+  S.rowptr3.assign(1, 0);
+  S.col3.clear();
+  for (int k = 0; k < nkn; k++) {
+    const int ng = pt.rowptr[k + 1] - pt.rowptr[k];
+    S.nt3g[k + 1] = S.nt3g[k] + ng * nlv + 2 * nlv + 2;
+    S.col3.push_back(k * (nlv + 2));
+    S.rowptr3.push_back((int)S.col3.size());
+    for (int l = 1; l <= nlv; l++) {
+      for (int q = pt.rowptr[k]; q < pt.rowptr[k + 1]; q++) {
+        const int kj = pt.col[q];
+        if (kj == k) {
+          S.col3.push_back(k * (nlv + 2) + l - 1);
+          S.col3.push_back(k * (nlv + 2) + l);
+          S.col3.push_back(k * (nlv + 2) + l + 1);
+        } else {
+          S.col3.push_back(kj * (nlv + 2) + l);
+        }
+      }
+      S.rowptr3.push_back((int)S.col3.size());
+    }
+    S.col3.push_back(k * (nlv + 2) + nlv + 1);
+    S.rowptr3.push_back((int)S.col3.size());
+  }
+  const size_t nnz = S.col3.size(), n = S.n3;
+  S.c3.assign(nnz, 0.);
+  S.rvec3.assign(n, 0.);
+  Arena &A = S.arena3;
+  NhSys &s = S.s3;
+  CsrGrid &g = S.g3;
+  int *drp = nullptr, *dcl = nullptr;
+  S.G3 = std::max(1, nh_solve_capacity());
+  if (A.upload(&drp, S.rowptr3) || A.upload(&dcl, S.col3) || A.alloc(&s.val, nnz) || A.alloc(&s.rhs, n) ||
+      A.alloc(&s.x, n) || A.alloc(&g.val32, nnz) || A.alloc(&g.dinv, n) || A.alloc(&g.x64, n) ||
+      A.alloc(&g.r, n) || A.alloc(&g.rh, n) || A.alloc(&g.p, n) || A.alloc(&g.v, n) || A.alloc(&g.s, n) ||
+      A.alloc(&g.t, n) || A.alloc(&g.z, n) || A.alloc(&g.q, n) || A.alloc(&g.e, n) ||
+      A.alloc(&g.part, (size_t)8 * S.G3) || A.alloc(&g.ctr, 4))
+    return SHY_ECAPACITY;
+  s.nrow = (int)n; s.rowptr = drp; s.col = dcl;
+  g.rowptr = drp; g.col = dcl; g.val = s.val; g.rhs = s.rhs; g.x = s.x;
+  g.r0 = 0; g.r1 = (int)n;
   return SHY_OK;
 }
 
@@ -2645,7 +2864,7 @@ static int simsys_init_impl() {
   if (!g_sys.st) CUDA_TRY(cudaStreamCreateWithFlags(&g_sys.st, cudaStreamNonBlocking));
   g_sys.initialized = true;
   g_sys.explicit_mode = false;
-  return SHY_OK;
+  return simsys3d_init(pt);
 }
 
 extern "C" void system_initialize_(void) {           // simsys_spkaux.f90:85
@@ -2657,6 +2876,8 @@ extern "C" void system_init_(void) {                  // :137 zero matrix and rh
   memset(g_sys.stage_h, 0, sizeof(float) * 12 * g_sys.nel);
   std::fill(g_sys.rqv_h.begin(), g_sys.rqv_h.end(), 0.f);
   g_sys.dt_rhs = 0.f;
+  std::fill(g_sys.c3.begin(), g_sys.c3.end(), 0.);
+  std::fill(g_sys.rvec3.begin(), g_sys.rvec3.end(), 0.);
 }
 
 extern "C" void system_set_explicit_(void) { g_sys.explicit_mode = true; }   // :160
@@ -2739,6 +2960,126 @@ extern "C" void system_get_(const int32_t *n, float *z) {           // :638
 }
 
 extern "C" void system_finalize_(void) {}                           // :722
+
+// loccoo3d (coo_matrix.f90:665-695), 0-based: the position of the entry of
+// row node ki, column node kj, layer l in the 3D COO; -1 if kj is not a
+// neighbour of ki
+static int loc3d(int ki, int kj, int l) {
+  const Simsys &S = g_sys;
+  const int *b = S.col2.data() + S.rowptr2[ki], *e = S.col2.data() + S.rowptr2[ki + 1];
+  const int *fi = std::lower_bound(b, e, ki), *fj = std::lower_bound(b, e, kj);
+  if (fj == e || *fj != kj) return -1;
+  const int ng = (int)(e - b), mi = (int)(fi - b), mj = (int)(fj - b);
+  const int p3 = mj < mi ? mj : (mj == mi ? mi + 1 : mj + 2);
+  return S.nt3g[ki] + 1 + (l - 1) * (ng + 2) + p3;
+}
+
+extern "C" void system_assemble_3d_(const int32_t *ie, const int32_t *l, const int32_t *nlv, const int32_t *kn,
+                                    const float *mass, const float *rhs) {   // simsys_spkaux.f90:597-635
+  Simsys &S = g_sys;
+  const int e = *ie - 1, lay = *l;
+  if (!S.initialized || S.nlv3 <= 0) { fail(SHY_ESTATE, "system_assemble_3d: no 3D system (shygpu_simsys_set_layers)"); simsys_stop("system_assemble_3d"); }
+  if (e < 0 || e >= S.nel || lay < 1 || lay > S.nlv3 || *nlv != S.nlv3) {
+    fail(SHY_EARG, "system_assemble_3d: element %d, layer %d or nlv %d outside the system", *ie, lay, *nlv);
+    simsys_stop("system_assemble_3d");
+  }
+  int k[3];
+  for (int i = 0; i < 3; i++) {
+    k[i] = kn[i] - 1;
+    if (k[i] != S.nv[3 * e + i]) {
+      fail(SHY_EARG, "system_assemble_3d: kn of element %d differ from the registered nen3v", *ie);
+      simsys_stop("system_assemble_3d");
+    }
+  }
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 3; j++) {
+      const int kk = loc3d(k[i], k[j], lay);
+      if (kk > 0) {
+        S.c3[kk - 1] += mass[0 + 3 * i + 9 * j];
+        S.c3[kk] += mass[1 + 3 * i + 9 * j];
+        S.c3[kk + 1] += mass[2 + 3 * i + 9 * j];
+      }
+    }
+    S.rvec3[(size_t)(S.nlv3 + 2) * k[i] + lay] += rhs[i];
+  }
+}
+
+extern "C" void system_adjust_matrix_3d_(void) {   // coo_adjust_3d (coo_matrix.f90:269-325)
+  Simsys &S = g_sys;
+  if (!S.initialized || S.nlv3 <= 0) { fail(SHY_ESTATE, "system_adjust_matrix_3d: no 3D system"); simsys_stop("system_adjust_matrix_3d"); }
+  for (int e = 0; e < S.nel; e++)
+    for (int i = 0; i < 3; i++)
+      for (int l = 1; l <= S.nlv3; l++) {
+        const int kk = loc3d(S.nv[3 * e + i], S.nv[3 * e + i], l);
+        if (S.c3[kk] == 0.) S.c3[kk] = 1.;
+      }
+  for (int k = 0; k < S.nkn; k++) {
+    S.c3[S.nt3g[k]] = 1.;
+    S.c3[S.nt3g[k + 1] - 1] = 1.;
+  }
+}
+
+static int simsys_solve_3d_impl(int n, int nlvdi, int nlv, const float *z) {
+  Simsys &S = g_sys;
+  if (!S.initialized || S.nlv3 <= 0) return fail(SHY_ESTATE, "system_solve_3d: no 3D system");
+  if (n != S.nkn || nlv != S.nlv3 || nlvdi < nlv)
+    return fail(SHY_EARG, "system_solve_3d: n=%d, nlv=%d, nlvdi=%d against a system of %d nodes and %d layers",
+                n, nlv, nlvdi, S.nkn, S.nlv3);
+  // the guess: z with zero padding rows (simsys_spkaux.f90:509-523)
+  std::vector<float> p(S.n3, 0.f);
+  for (int k = 0; k < n; k++)
+    for (int l = 1; l <= nlv; l++) p[(size_t)k * (nlv + 2) + l] = z[(size_t)k * nlvdi + l - 1];
+  cudaStream_t st = S.st;
+  CUDA_TRY(cudaMemcpyAsync(S.s3.val, S.c3.data(), sizeof(double) * S.c3.size(), cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.s3.rhs, S.rvec3.data(), sizeof(double) * S.n3, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemcpyAsync(S.s3.x, p.data(), sizeof(float) * S.n3, cudaMemcpyHostToDevice, st));
+  CUDA_TRY(cudaMemsetAsync(S.d.out, 0, sizeof(BasinOut), st));
+  CsrGrid g = S.g3;
+  g.out = S.d.out;
+  g.rtol = S.rtol; g.atol = S.atol; g.maxit = S.maxit;
+  const int G = std::min(S.G3, std::max(1, (S.n3 + 2047) / 2048));
+  cudaError_t e = launch_nh_solve(g, G, st);
+  if (e != cudaSuccess) return fail(SHY_ECUDA, "system_solve_3d launch: %s", cudaGetErrorString(e));
+  g_launches += 1;
+  BasinOut o;
+  CUDA_TRY(cudaMemcpyAsync(&o, S.d.out, sizeof o, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  S.last_iters = o.nh_iters;
+  if (o.status) return fail(o.status, "system_solve_3d: error solving matrix (status %d)", o.status);
+  return SHY_OK;
+}
+
+extern "C" void system_solve_3d_(const int32_t *n, const int32_t *nlvdi, const int32_t *nlv, const float *z) {
+  if (simsys_solve_3d_impl(*n, *nlvdi, *nlv, z)) simsys_stop("spk_solve_system");
+}
+
+extern "C" void system_get_3d_(const int32_t *n, const int32_t *nlvdi, const int32_t *nlv, float *z) {
+  Simsys &S = g_sys;
+  if (!S.initialized || S.nlv3 <= 0 || *n != S.nkn || *nlv != S.nlv3 || *nlvdi < *nlv) {
+    fail(SHY_EARG, "system_get_3d: no 3D system of this size");
+    simsys_stop("system_get_3d");
+  }
+  std::vector<float> x(S.n3);
+  if (cudaMemcpy(x.data(), S.s3.x, sizeof(float) * S.n3, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    fail(SHY_ECUDA, "system_get_3d: copy failed");
+    simsys_stop("system_get_3d");
+  }
+  for (int k = 0; k < *n; k++)
+    for (int l = 1; l <= *nlv; l++) z[(size_t)k * (*nlvdi) + l - 1] = x[(size_t)k * (*nlv + 2) + l];
+}
+
+extern "C" int shygpu_simsys_get_matrix_3d(int32_t *n, int32_t *nnz, int32_t *rowptr, int32_t *col, double *val,
+                                           double *rhs) {
+  const Simsys &S = g_sys;
+  if (!S.initialized || S.nlv3 <= 0) return fail(SHY_ESTATE, "simsys_get_matrix_3d: no 3D system");
+  if (n) *n = S.n3;
+  if (nnz) *nnz = (int32_t)S.col3.size();
+  if (rowptr) std::copy(S.rowptr3.begin(), S.rowptr3.end(), rowptr);
+  if (col) std::copy(S.col3.begin(), S.col3.end(), col);
+  if (val) CUDA_TRY(cudaMemcpy(val, S.s3.val, sizeof(double) * S.col3.size(), cudaMemcpyDeviceToHost));
+  if (rhs) CUDA_TRY(cudaMemcpy(rhs, S.s3.rhs, sizeof(double) * S.n3, cudaMemcpyDeviceToHost));
+  return SHY_OK;
+}
 
 extern "C" int shygpu_simsys_iterations(void) { return g_sys.last_iters; }
 

@@ -164,6 +164,18 @@ __global__ void __launch_bounds__(256) k_column(Dev d) {
     const float raux = P.grav / P.rowass;
     if (act) { fx += raux * hlayer * px; fy += raux * hlayer * py; }
   }
+  if (P.inohyd && act) {
+    // nonhydro_set_explicit (nohydro.f90:526-586): the old pressure's
+    // gradient times the old thickness, weight 1 - aqpar
+    float qx = 0.f, qy = 0.f;
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) {
+      const float q = d.qdist[kn[ii]] * d.qp[(size_t)kn[ii] * NLV + lane];
+      qx += (float)b[ii] * q; qy += (float)c[ii] * q;
+    }
+    fx += (1.f - P.aqpar) * hhi * qx;
+    fy += (1.f - P.aqpar) * hhi * qy;
+  }
 
   ppx += aat * uui - bbt * uuip - cct * uuim - (float)gammat * vvi + (float)(P.grav * hhi * bz) +
          (hhi / P.rowass) * (float)bpres + fx;

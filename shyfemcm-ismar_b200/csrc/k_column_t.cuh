@@ -178,6 +178,18 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
       fx += raux * hlayer * pxs;
       fy += raux * hlayer * pys;
     }
+    if (P.inohyd) {
+      // nonhydro_set_explicit (nohydro.f90:526-586): the old pressure's
+      // gradient times the old thickness, weight 1 - aqpar
+      float qx = 0.f, qy = 0.f;
+#pragma unroll
+      for (int ii = 0; ii < 3; ii++) {
+        const float q = d.qdist[kn[ii]] * d.qp[(size_t)kn[ii] * NLV + l];
+        qx += (float)b[ii] * q; qy += (float)c[ii] * q;
+      }
+      fx += (1.f - P.aqpar) * hhi * qx;
+      fy += (1.f - P.aqpar) * hhi * qy;
+    }
     ppx += aat * uui - bbt * uuip - cct * uuim - (float)gammat * vvi + (float)(P.grav * hhi * bz) +
            (hhi / P.rowass) * (float)bpres + fx;
     ppy += aat * vvi - bbt * vvip - cct * vvim + (float)gammat * uui + (float)(P.grav * hhi * cz) +

@@ -34,6 +34,44 @@ void launch_reduce(const Dev &d, int nsub, int advance, cudaStream_t st);
 // setweg(0) (and zenv from znv), 2 setznv; basin >= 0 limits 1 and 2 to it
 void launch_wetdry(const Dev &d, const int *kbas, int which, int basin, cudaStream_t st);
 void launch_subctl(const Dev &d, cudaGraphConditionalHandle h, cudaStream_t st);
+// the 3D system of the non-hydrostatic pressure over the basins with
+// inohyd = 1: one unknown per active node layer, row of node k and layer l
+// (1-based) roff[k] + l - 1; CSR with the rows of a basin contiguous
+struct NhSys {
+  int nrow = 0;
+  const int *kbas = nullptr;       // node -> basin
+  const int *roff = nullptr;       // [NKN] first row of node k, -1 in hydrostatic basins
+  const int *rnode = nullptr;      // [nrow] node of each row
+  const int *rowptr = nullptr, *col = nullptr;
+  double *val = nullptr, *rhs = nullptr;
+  float *x = nullptr;              // the pressure per row (solver output)
+  float *wnh = nullptr;            // [NKN*(NLV+1)] w of sp256wnh
+};
+
+// the device-wide CSR solver (k_nh_solve) over rows [r0, r1), whose columns
+// lie in the same range; x holds the guess and receives the solution
+struct CsrGrid {
+  int r0 = 0, r1 = 0;
+  const int *rowptr = nullptr, *col = nullptr;
+  const double *val = nullptr, *rhs = nullptr;
+  float *val32 = nullptr, *dinv = nullptr, *x = nullptr;
+  double *x64 = nullptr;
+  float *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr, *s = nullptr, *t = nullptr, *z = nullptr,
+        *q = nullptr, *e = nullptr;
+  double *part = nullptr;          // [2][G][4] partial sums
+  unsigned *ctr = nullptr;         // [4] barrier arrivals, release, abort
+  BasinOut *out = nullptr;         // nh_* fields and status of the basin solved
+  double rtol = 1e-8, atol = 1e-8;
+  int maxit = 1000, max_outer = 12;
+  float inner_rtol = 1e-4f;
+  long long spin_limit = 1LL << 24;
+};
+// which: 0 k_nh_w (sp256wnh), 1 k_nh_sys (the 3D system), 2 k_nh_node, 3 k_nh_elem
+void launch_nh(const Dev &d, const NhSys &s, int which, cudaStream_t st);
+// G CTAs (cooperative; clears a.ctr first)
+cudaError_t launch_nh_solve(const CsrGrid &a, int G, cudaStream_t st);
+int nh_solve_capacity();           // CTAs of k_nh_solve that fit the device at once
+
 // shape of the shared-memory zeta solver: CL CTAs of `threads` per basin,
 // rows per CTA (capacity) and nonzeros per CTA (capacity), dynamic smem
 struct ZetaShape {

@@ -75,6 +75,10 @@ def lib():
     L.shygpu_step_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyStepInfo)]
     L.shygpu_get_wetdry.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 3
     L.shygpu_set_nudging.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.shygpu_set_nh_distance.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.shygpu_get_nh_pressure.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.shygpu_nh_info.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.shygpu_set_bound_scalar.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
     L.shygpu_autotune.argtypes = [C.c_void_p, C.c_int32, C.c_char_p, C.c_int32, C.POINTER(C.c_double)]
     L.shygpu_shy_open_scalar.argtypes = [C.c_void_p, C.c_int32, C.POINTER(abi.ShyBasin), C.c_char_p, C.c_int32,
@@ -106,6 +110,12 @@ def lib():
     L.shygpu_simsys_register.argtypes = [C.c_int32, C.c_int32, abi.i32p]
     L.shygpu_simsys_set_tolerance.argtypes = [C.c_double, C.c_double, C.c_int32]
     L.shygpu_simsys_get_matrix.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)] + [C.c_void_p] * 4
+    L.shygpu_simsys_set_layers.argtypes = [C.c_int32]
+    L.shygpu_simsys_get_matrix_3d.argtypes = [C.POINTER(C.c_int32), C.POINTER(C.c_int32)] + [C.c_void_p] * 4
+    L.system_assemble_3d_.argtypes = [C.POINTER(C.c_int32)] * 3 + [abi.i32p, C.c_void_p, abi.f32p]
+    L.system_adjust_matrix_3d_.argtypes = []
+    L.system_solve_3d_.argtypes = [C.POINTER(C.c_int32)] * 3 + [abi.f32p]
+    L.system_get_3d_.argtypes = [C.POINTER(C.c_int32)] * 3 + [abi.f32p]
     L.shygpu_set_forcing.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 4
     L.shygpu_model_stream.argtypes = [C.c_void_p]
     L.shygpu_model_stream.restype = C.c_void_p
@@ -231,6 +241,23 @@ class Model:
         a = np.ascontiguousarray(andgzv, np.float32)
         check(lib().shygpu_set_nudging(self.h, ib, a.ctypes.data), "set_nudging")
         lib().shygpu_sync(self.h)
+
+    def set_nh_distance(self, ib, qdist):
+        """Weight of the non-hydrostatic pressure per node (qdistv, float32 in [0, 1])."""
+        a = np.ascontiguousarray(qdist, np.float32)
+        check(lib().shygpu_set_nh_distance(self.h, ib, a.ctypes.data), "set_nh_distance")
+
+    def nh(self, ib=0):
+        """(qpnv (nkn, nlv), (iters, refinements, resid0, resid)) of basin ib:
+        the non-hydrostatic pressure the next step starts from and the last
+        pressure solve."""
+        c = self.cases[ib]
+        q = np.zeros((c["nkn"], c["nlv"]), np.float32)
+        check(lib().shygpu_get_nh_pressure(self.h, ib, q.ctypes.data), "get_nh_pressure")
+        it, rf = C.c_int32(0), C.c_int32(0)
+        r0, r = C.c_double(0), C.c_double(0)
+        check(lib().shygpu_nh_info(self.h, ib, C.byref(it), C.byref(rf), C.byref(r0), C.byref(r)), "nh_info")
+        return q, (it.value, rf.value, r0.value, r.value)
 
     def autotune(self, steps=5):
         """shygpu_autotune: time the candidate launch shapes on this model's
@@ -530,6 +557,47 @@ class _Simsys:
 
     def iterations(self):
         return lib().shygpu_simsys_iterations()
+
+    def set_layers(self, nlv):
+        """Layers of the 3D system (0: none); before system_initialize."""
+        check(lib().shygpu_simsys_set_layers(int(nlv)), "simsys_set_layers")
+
+    def system_assemble_3d(self, ie, l, nlv, kn, mass, rhs):
+        """mass (3, 3, 3) indexed [d+1, i, j] for the reference's mass(d, i, j)."""
+        m = np.asfortranarray(np.asarray(mass, np.float32))
+        r = np.ascontiguousarray(rhs, np.float32)
+        k = np.ascontiguousarray(kn, np.int32)
+        a = [C.c_int32(int(v)) for v in (ie, l, nlv)]
+        lib().system_assemble_3d_(C.byref(a[0]), C.byref(a[1]), C.byref(a[2]), abi.ptr(k, abi.i32p),
+                                  m.ctypes.data, abi.ptr(r))
+
+    def system_adjust_matrix_3d(self):
+        lib().system_adjust_matrix_3d_()
+
+    def system_solve_3d(self, z):
+        """z (n, nlv): the guess."""
+        zz = np.ascontiguousarray(z, np.float32)
+        n, nlv = zz.shape
+        a = [C.c_int32(v) for v in (n, nlv, nlv)]
+        lib().system_solve_3d_(C.byref(a[0]), C.byref(a[1]), C.byref(a[2]), abi.ptr(zz))
+
+    def system_get_3d(self, n, nlv):
+        z = np.zeros((n, nlv), np.float32)
+        a = [C.c_int32(v) for v in (n, nlv, nlv)]
+        lib().system_get_3d_(C.byref(a[0]), C.byref(a[1]), C.byref(a[2]), abi.ptr(z))
+        return z
+
+    def get_matrix_3d(self):
+        n, nnz = C.c_int32(0), C.c_int32(0)
+        check(lib().shygpu_simsys_get_matrix_3d(C.byref(n), C.byref(nnz), None, None, None, None),
+              "simsys_get_matrix_3d")
+        rowptr = np.zeros(n.value + 1, np.int32)
+        col = np.zeros(nnz.value, np.int32)
+        val = np.zeros(nnz.value, np.float64)
+        rhs = np.zeros(n.value, np.float64)
+        check(lib().shygpu_simsys_get_matrix_3d(C.byref(n), C.byref(nnz), rowptr.ctypes.data, col.ctypes.data,
+                                                val.ctypes.data, rhs.ctypes.data), "simsys_get_matrix_3d")
+        return rowptr, col, val, rhs
 
 
 class ZetaSystem(C.Structure):

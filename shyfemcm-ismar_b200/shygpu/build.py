@@ -17,7 +17,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = HERE / "libshygpu.so"
 SOURCES = ["step_node32.cu", "step_node16.cu", "step_zeta.cu", "step_node.cu", "step.cu", "host.cu",
-           "static_solve.cu", "serve.cu"]
+           "static_solve.cu", "serve.cu", "nonhydro.cu"]
 HEADERS = ["common.cuh", "launch.h", "physics.cuh", "node_launch.cuh", "k_column.cuh", "k_column_t.cuh", "k_final.cuh", "k_node.cuh", "k_conz.cuh", "k_zeta.cuh", "k_wetdry.cuh", "k_zeta_global.cuh", "k_zeta_grid.cuh"]
 
 NVCC_FLAGS = [

@@ -380,6 +380,36 @@ def seiche_case(lx=50.0, ly=10.0, nx=21, ny=5, depth=25.0, nlv=10, ampli=0.01, d
     return _finish(case)
 
 
+def nh_basin_case(nkn_target=1500, lx=300.0, ly=150.0, seed=2, dt=0.5, nlv=12, hmin=5.0, hmax=30.0,
+                  sigma=True, wind=10.0, ts=True):
+    """Small closed basin for the non-hydrostatic pressure: `lx` x `ly` m,
+    Gaussian-bump bathymetry from `hmin` to `hmax` m, `nlv` sigma layers
+    (or z-layers of 1 to 5 m), uniform wind, T/S linear in depth plus seeded
+    noise (transported, no baroclinic terms), dt of half a second: the
+    horizontal scale of the flow is the depth's, where the pressure
+    matters."""
+    c = basin3d_case(nkn_target=nkn_target, lx=lx, ly=ly, seed=seed, dt=dt, nlv=nlv, ampli=0.0, wind=wind,
+                     baroclinic=False, ts=ts)
+    c["bnd_index"][:] = 0
+    c["tide"] = np.zeros((0, 1, 4), np.float32)
+    h = c["hm3v"].astype(np.float64)
+    c["hm3v"] = (hmin + (h - 5.0) * (hmax - hmin) / 55.0).astype(np.float32)
+    if sigma:
+        c["hlv"] = (-np.arange(1, nlv + 1) / nlv).astype(np.float32)
+        c["hldv"] = np.full(nlv, -1.0 / nlv, np.float32)
+        c["ilhv"][:] = nlv
+        c["ilhkv"][:] = nlv
+        c["params"] = dict(c["params"], nsigma=nlv)
+    else:
+        hlv, hldv = z_layers(np.linspace(1.0, 5.0, nlv) * hmax / np.linspace(1.0, 5.0, nlv).sum())
+        hlv[-1] = hmax + 1.0
+        c["hlv"], c["hldv"] = hlv.astype(np.float32), hldv.astype(np.float32)
+        c["ilhv"], c["ilhkv"] = layer_counts(c["nen3v"], c["hm3v"], hlv, hldv, c["nkn"])
+    c["params"] = dict(c["params"], inohyd=1)
+    c["name"] = f"nhbasin_{c['nkn']}x{nlv}_{'sigma' if sigma else 'z'}"
+    return c
+
+
 def ensemble_member_case(nkn_target, aspect, seed, wind, dt=60.0, nlv=10, spacing=100.0,
                          ampli=0.5, depth=10.0, ddepth=2.0, top=2.0):
     """One member of the batched ensemble, made as the 2D channel is: a
