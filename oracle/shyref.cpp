@@ -688,7 +688,8 @@ void rhoset(Model &m) {
   for (int k = 0; k < m.nkn; k++) {
     double depth = 0., presbc = 0.;
     for (int l = 1; l <= m.ilhkv[k]; l++) {
-      double hlayer = m.hldv[l - 1];          // z-layers: nominal thickness
+      // sigma layers: the old thickness; z-layers: the nominal one
+      double hlayer = l <= m.p.nsigma ? m.hdkov[(size_t)k * nlv + l - 1] : m.hldv[l - 1];
       double hh = 0.5 * hlayer;
       depth += hh;
       double rhop = m.rhov[(size_t)k * nlv + l - 1];
@@ -742,8 +743,9 @@ int bottom_friction(Model &m) {
 }
 
 // set_explicit (explicit.f90:123-213): horizontal viscosity
-// (set_diff_horizontal :389-493) and baroclinic pressure for z-layers
-// (set_barocl_new_interface :1226-1530 with nsigma = 0, no z-adaptation).
+// (set_diff_horizontal :389-493), the advective terms and the baroclinic
+// pressure (set_barocl_new_interface :1226-1530; z, sigma and hybrid
+// layers, no z-adaptation).
 void set_explicit(Model &m) {
   int nlv = m.nlv;
   m.fxv.assign((size_t)nlv * m.nel, 0.);
@@ -862,26 +864,98 @@ void set_explicit(Model &m) {
   }
   bool bbarcl = m.p.ibarcl > 0 && m.p.ibarcl != 3 && m.p.ibarcl != 5;
   if (bbarcl) {
+    // set_barocl_new_interface with bsigadjust (explicit.f90:1226-1530): on
+    // sigma layers (l <= nsigma) the interfaces move with the level, so the
+    // density gradient at interface l-1 is taken on the horizontal surface
+    // at the element's mean depth of that interface: at each vertex the
+    // density interpolated between the mid-layer depths of the node's
+    // column that bracket it (hkkom, from the old level and old node
+    // thickness), with the cases of vertices above the surface and below
+    // the bottom; on z-layers the mean of the layer gradients.
+    const int nsigma = m.p.nsigma;
     double raux = m.p.grav / m.p.rowass;
+    std::vector<double> hkko, hkkom;
+    if (nsigma > 0) {
+      hkko.assign((size_t)(nlv + 1) * m.nkn, 0.);
+      hkkom.assign((size_t)(nlv + 1) * m.nkn, 0.);
+      for (int k = 0; k < m.nkn; k++) {
+        double hkk = -m.zov[k];
+        hkko[(size_t)k * (nlv + 1)] = hkk;
+        hkkom[(size_t)k * (nlv + 1)] = hkk;
+        for (int l = 1; l <= m.ilhkv[k]; l++) {
+          hkk += m.hdkov[(size_t)k * nlv + l - 1];
+          hkko[(size_t)k * (nlv + 1) + l] = hkk;
+          hkkom[(size_t)k * (nlv + 1) + l] = 0.5 * (hkko[(size_t)k * (nlv + 1) + l] + hkko[(size_t)k * (nlv + 1) + l - 1]);
+        }
+      }
+    }
+    auto HO = [&](int l, int k) { return hkko[(size_t)k * (nlv + 1) + l]; };
+    auto HM = [&](int l, int k) { return hkkom[(size_t)k * (nlv + 1) + l]; };
+    auto RH = [&](int l, int k) { return m.rhov[(size_t)k * nlv + l - 1]; };
     for (int ie = 0; ie < m.nel; ie++) {
       const double *e = &m.ev[(size_t)ie * SHY_EVDIM];
       int lmax = m.ilhv[ie];
       double presbcx = 0., presbcy = 0., brup = 0., crup = 0., hhup = 0.;
       for (int l = 1; l <= lmax; l++) {
-        double hlayer = m.hldv[l - 1];
+        const bool bsigma = l <= nsigma;
+        double hlayer = bsigma ? m.hdeov[(size_t)ie * nlv + l - 1] : m.hldv[l - 1];
         double hh = 0.5 * hlayer;
         double hint = hh + hhup;
-        double br = 0., cr = 0.;
+        int llup[3] = {0, 0, 0}, lldown[3] = {0, 0, 0};
+        double helei = 0.;
+        if (bsigma) {
+          for (int ii = 0; ii < 3; ii++) helei += HO(l - 1, m.nen3v[3 * ie + ii]);
+          helei /= 3.;
+          for (int ii = 0; ii < 3; ii++) {
+            const int k = m.nen3v[3 * ie + ii], lkmax = m.ilhkv[k];
+            int ll;
+            if (helei < HO(l - 1, k)) {                  // look upwards
+              for (ll = l - 1; ll >= 1; ll--) if (helei > HO(ll - 1, k)) break;
+              if (ll <= 0) ll = 1;
+            } else if (helei > HO(l, k)) {             // look downwards
+              for (ll = l + 1; ll <= lkmax; ll++) if (helei < HO(ll, k)) break;
+              if (ll > lkmax) ll = lkmax;
+            } else {
+              ll = l;
+            }
+            if (helei < HM(ll, k)) { llup[ii] = ll == 1 ? 1 : ll - 1; lldown[ii] = ll; }
+            else { llup[ii] = ll; lldown[ii] = ll == lkmax ? lkmax : ll + 1; }
+          }
+        }
+        int nb = 0, nn = 0;
+        double br = 0., cr = 0., brl = 0., crl = 0.;
         for (int ii = 0; ii < 3; ii++) {
-          int k = m.nen3v[3 * ie + ii];
-          double rhop = m.rhov[(size_t)k * nlv + l - 1];
+          const int k = m.nen3v[3 * ie + ii], lkmax = m.ilhkv[k];
+          double rhop = RH(l, k);
+          if (l == nsigma) { brl += e[3 + ii] * rhop; crl += e[6 + ii] * rhop; }
+          if (bsigma) {
+            const int lu = llup[ii], ld = lldown[ii];
+            if (ld == 1) rhop = RH(1, k);
+            else if (lu >= lkmax) { nb++; nn += ii + 1; rhop = RH(lkmax, k); }
+            else {
+              const double hu = HM(lu, k), hd = HM(ld, k);
+              const double alpha = (helei - hu) / (hd - hu);
+              rhop = alpha * RH(ld, k) + (1. - alpha) * RH(lu, k);
+            }
+          }
           br += e[3 + ii] * rhop;
           cr += e[6 + ii] * rhop;
         }
         double brint, crint;
-        if (l == 1) { brint = br; crint = cr; }
+        if (bsigma) {
+          if (nb == 2) { brint = brup; crint = crup; }
+          else if (nb == 1) {                           // the gradient along the bottom side kept
+            const double b3 = e[3 + nn - 1], c3 = e[6 + nn - 1];
+            const double aux = 1. / (c3 * c3 + b3 * b3);
+            const double bn = aux * (brup * b3 + crup * c3) * b3, cn = aux * (brup * b3 + crup * c3) * c3;
+            const double bt = br - aux * (br * b3 + cr * c3) * b3, ct = cr - aux * (br * b3 + cr * c3) * c3;
+            brint = bn + bt; crint = cn + ct;
+          } else { brint = br; crint = cr; }
+        } else if (l == 1) { brint = br; crint = cr; }
         else { brint = 0.5 * (br + brup); crint = 0.5 * (cr + crup); }
-        brup = br; crup = cr; hhup = hh;
+        brup = br; crup = cr;
+        if (l == nsigma) { brup = brl; crup = crl; }
+        hhup = hh;
         presbcx += hint * brint;
         presbcy += hint * crint;
         m.fxv[(size_t)ie * nlv + l - 1] += raux * hlayer * presbcx;

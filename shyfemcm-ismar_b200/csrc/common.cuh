@@ -96,6 +96,10 @@ struct BasinOut {
 struct Dev {
   int nbasin, NKN, NEL, NLV, S, nsc_max;
   int col_threads;              // column kernel: 1 one thread per column, 0 one warp segment
+  int col_staged;               // thread-per-column kernel without Coriolis: 1 columns staged
+                                // through shared memory in coalesced passes, 0 read in place
+  int node_prefetch;            // thread-per-column node kernel: 1 each element's layers loaded
+                                // at once, 0 layer by layer
   int any_wd;                   // some basin has wetting and drying (thread-per-column forms)
   float2 *mom;                  // (NKN*NLV) node momentum {momentxv, momentyv} when a basin advects
   int any_tvd;                  // some basin transports with TVD (a gradient pass per sub-step)

@@ -932,8 +932,6 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
       return bail(fail(SHY_EARG, "basin %d: nsigma=%d outside 0..nlv", b, Pp[b].nsigma));
     if (Pp[b].nsigma > 0 && Pp[b].nsigma < bs.nlv && !(bs.hlv[Pp[b].nsigma - 1] == (Pp[b].hsigma > 0.f ? Pp[b].hsigma : 10000.f)))
       return bail(fail(SHY_EARG, "basin %d: hybrid levels: hlv(nsigma) must be hsigma (initialize.f90:556)", b));
-    if (Pp[b].nsigma > 0 && Pp[b].ibarcl > 0)
-      return bail(fail(SHY_EARG, "basin %d: baroclinic terms on sigma layers not supported", b));
     if (Pp[b].ihwadv < 0 || Pp[b].ihwadv > 2)
       return bail(fail(SHY_EARG, "basin %d: ihwadv=%d: 0, 1 (upwind) or 2 (centred)", b, Pp[b].ihwadv));
     if (Pp[b].nzadapt > 1 && (Pp[b].nsigma > 0 || Pp[b].ibarcl > 0 || Pp[b].wetdry))
@@ -1163,6 +1161,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   Dev &d = m->base;
   d.nbasin = nbasin; d.NKN = NKN; d.NEL = NEL; d.NLV = NLV; d.S = m->S; d.nsc_max = nsc_max;
   d.col_threads = 1;
+  d.col_staged = 1;
+  d.node_prefetch = 1;
   d.any_wd = m->any_wd ? 1 : 0;
   d.any_tvd = m->any_tvd ? 1 : 0;
   d.any_tvdv = 0;
@@ -1301,6 +1301,12 @@ extern "C" int shygpu_set_option(shygpu_model *m, const char *name, double value
   else if (n == "column_threads") {   // 1: one thread per column when it has at most 16 layers
     m->base.col_threads = iv != 0;
   }
+  else if (n == "column_staged") {    // thread-per-column kernel: 1 columns staged in shared memory
+    m->base.col_staged = iv != 0;
+  }
+  else if (n == "node_prefetch") {    // thread-per-column node kernel: 1 element layers loaded at once
+    m->base.node_prefetch = iv != 0;
+  }
   else if (n == "inner_rtol") { if (!(value > 0 && value < 1)) return fail(SHY_EARG, "inner_rtol in (0,1)"); m->inner_rtol = (float)value; }
   else if (n == "inner_tol_frac") {   // the FP32 inner solve stops at this fraction of the outer target
     if (!(value > 0 && value <= 1)) return fail(SHY_EARG, "inner_tol_frac in (0,1]");
@@ -1326,6 +1332,8 @@ extern "C" double shygpu_get_option(shygpu_model *m, const char *name) {
   if (n == "zeta_threads") return m->zcl.empty() ? -1 : m->zcl[0].threads;
   if (n == "zeta_classes") return (double)m->zcl.size();
   if (n == "column_threads") return m->base.col_threads;
+  if (n == "column_staged") return m->base.col_staged;
+  if (n == "node_prefetch") return m->base.node_prefetch;
   if (n == "inner_rtol") return m->inner_rtol;
   if (n == "inner_tol_frac") return m->tol_frac;
   if (n == "max_outer") return m->max_outer;
@@ -2596,7 +2604,11 @@ extern "C" int shygpu_autotune(shygpu_model *m, int32_t steps, char *choice, int
           {{"zeta_stage", 0}, {"zeta_tile_rows", 1024}, {"zeta_variant", 0}},
       });
     }
-    if (m->NLV <= 16 && !m->any_wd) groups.push_back({{{"column_threads", 1}}, {{"column_threads", 0}}});
+    if (m->NLV <= 16 && !m->any_wd)
+      groups.push_back({{{"column_threads", 1}, {"column_staged", 1}, {"node_prefetch", 1}},
+                        {{"column_threads", 1}, {"column_staged", 1}, {"node_prefetch", 0}},
+                        {{"column_threads", 1}, {"column_staged", 0}, {"node_prefetch", 0}},
+                        {{"column_threads", 0}}});
     groups.push_back({{{"inner_tol_frac", 0.5}}, {{"inner_tol_frac", 0.75}}, {{"inner_tol_frac", 0.9}}});
     TuneSet chosen;
     for (const auto &g : groups) {

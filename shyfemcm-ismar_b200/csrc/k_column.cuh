@@ -142,23 +142,63 @@ __global__ void __launch_bounds__(256) k_column(Dev d) {
     fy += P.rlin * yadv;
   }
   if (P.ibarcl > 0 && P.ibarcl != 3 && P.ibarcl != 5) {
-    // set_barocl_new_interface for z-layers (explicit.f90:1226-1530)
-    float br = 0.f, cr = 0.f;
+    // set_barocl_new_interface (explicit.f90:1226-1530): on z-layers the mean
+    // of the density gradients of the layers above and below an interface;
+    // on sigma layers the gradient on the horizontal surface at the
+    // element's mean depth of the interface (bsigadjust), with the cases of
+    // one or two vertices below the bottom.  Lane = layer.
+    const bool bsig = lane < P.nsigma;
+    float br = 0.f, cr = 0.f, brl = 0.f, crl = 0.f;
+    int nb = 0, nn = 0;
+    double helei = 0.;
+    if (P.nsigma > 0) {
+      // each vertex's depth of the layer's top interface (hkko): the old
+      // level and the old node thickness of the layers above
+#pragma unroll
+      for (int ii = 0; ii < 3; ii++) {
+        const double hk = act ? (double)d.hko[(size_t)kn[ii] * NLV + lane] : 0.;
+        helei += -(double)d.zo[kn[ii]] + seg_scan_down<S>(hk, lane) - hk;
+      }
+      helei /= 3.;
+    }
     if (act) {
 #pragma unroll
       for (int ii = 0; ii < 3; ii++) {
-        const float rp = d.rho[(size_t)kn[ii] * NLV + lane];
+        const int k = kn[ii];
+        float rp = d.rho[(size_t)k * NLV + lane];
+        if (lane + 1 == P.nsigma) { brl += (float)b[ii] * rp; crl += (float)c[ii] * rp; }
+        if (bsig) {
+          bool below;
+          rp = sigma_rho_at(d.hko + (size_t)k * NLV, d.rho + (size_t)k * NLV, -(double)d.zo[k], d.ilhkv[k], helei,
+                            &below);
+          if (below) { nb++; nn += ii + 1; }
+        }
         br += (float)b[ii] * rp; cr += (float)c[ii] * rp;
       }
     }
     const float *hld = d.hldv + (size_t)en.w * NLV;
-    const float hlayer = inl ? hld[lane] : 0.f;
+    const float hlayer = bsig ? hhi : (inl ? hld[lane] : 0.f);
     const float hh = 0.5f * hlayer;
-    float brup = seg_up<S>(br, 1), crup = seg_up<S>(cr, 1), hhup = seg_up<S>(hh, 1);
-    if (lane == 0) { brup = br; crup = cr; hhup = 0.f; }
+    // the layer above passes its gradient on (at layer nsigma the one
+    // before the interpolation); the first layer sees zero
+    const float brn = lane + 1 == P.nsigma ? brl : br, crn = lane + 1 == P.nsigma ? crl : cr;
+    float brup = seg_up<S>(brn, 1), crup = seg_up<S>(crn, 1), hhup = seg_up<S>(hh, 1);
+    if (lane == 0) { brup = 0.f; crup = 0.f; hhup = 0.f; }
     const float hint = hh + hhup;
-    float px = act ? hint * 0.5f * (br + brup) : 0.f;
-    float py = act ? hint * 0.5f * (cr + crup) : 0.f;
+    float brint, crint;
+    if (bsig) {
+      if (nb == 2) { brint = brup; crint = crup; }
+      else if (nb == 1) {
+        const float b3 = (float)b[nn - 1], c3 = (float)c[nn - 1];
+        const float aux = 1.f / (c3 * c3 + b3 * b3);
+        const float pu = aux * (brup * b3 + crup * c3), pc = aux * (br * b3 + cr * c3);
+        brint = pu * b3 + (br - pc * b3);
+        crint = pu * c3 + (cr - pc * c3);
+      } else { brint = br; crint = cr; }
+    } else if (lane == 0) { brint = br; crint = cr; }
+    else { brint = 0.5f * (br + brup); crint = 0.5f * (cr + crup); }
+    float px = act ? hint * brint : 0.f;
+    float py = act ? hint * crint : 0.f;
     px = seg_scan_down<S>(px, lane);
     py = seg_scan_down<S>(py, lane);
     const float raux = P.grav / P.rowass;

@@ -20,11 +20,41 @@
 
 namespace shy {
 
-template <int L, bool COR, bool ADV>
-__global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= d.NEL) return;
+//
+// W (staged, no Coriolis): the layer arrays of a warp's 32 element columns
+// (one contiguous run of 32*NLV values) move between global and shared
+// memory in coalesced passes of the whole warp, as k_final_w does; each
+// thread then reads and writes its own column in shared memory.  Without
+// it each load of layer l touches 32 sectors, one per column.
+template <int L, bool COR, bool ADV, bool W = false>
+__global__ void __launch_bounds__(128, W ? 4 : 3) k_column_t(Dev d) {
+  static_assert(!(W && COR), "the staged form has no Coriolis instance");
+  __shared__ float sbuf[W ? 4 : 1][W ? 3 : 1][W ? 32 * L : 1];
+  const int e0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if constexpr (!W) {
+    if (e0 >= d.NEL) return;
+  } else {
+    if (e0 - lane >= d.NEL) return;                   // whole warps only
+  }
+  const int w0 = e0 - lane;                           // first element of the warp
+  const int nw = W ? min(32, d.NEL - w0) : 32;
+  const bool valid = !W || lane < nw;
+  const int e = valid ? e0 : w0;                      // spare lanes work a copy of the first column
   const int NLV = d.NLV;
+  float *bH = sbuf[warp][0], *bU = sbuf[warp][1], *bV = sbuf[warp][2];
+  const int ol = lane * NLV;                          // this thread's column in the buffers
+  if constexpr (W) {
+    const size_t base = (size_t)w0 * NLV;
+    const int cnt = nw * NLV;
+    for (int j = lane; j < 32 * NLV; j += 32) {      // spare lanes' columns read as zero
+      const bool in = j < cnt;
+      bH[j] = in ? d.heo[base + j] : 0.f;
+      bU[j] = in ? d.uo[base + j] : 0.f;
+      bV[j] = in ? d.vo[base + j] : 0.f;
+    }
+    __syncwarp();
+  }
   const int4 en = d.enode[e];
   const BasinPar &P = d.par[en.w];
   const int kn[3] = {en.x, en.y, en.z};
@@ -53,14 +83,21 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
 
   // the column (inactive layers read as zero)
   const size_t o = (size_t)e * NLV;
-  float h[L], u[L], v[L];
+  // W: the layer values stay in shared memory (read where used, which
+  // frees the registers of three layer arrays); else in registers
+  float h[W ? 1 : L], u[W ? 1 : L], v[W ? 1 : L];
+  if constexpr (!W) {
 #pragma unroll
-  for (int l = 0; l < L; l++) {
-    const bool act = l < ilevel;
-    h[l] = act ? d.heo[o + l] : 0.f;
-    u[l] = act ? d.uo[o + l] : 0.f;
-    v[l] = act ? d.vo[o + l] : 0.f;
+    for (int l = 0; l < L; l++) {
+      const bool act = l < ilevel;
+      h[l] = act ? d.heo[o + l] : 0.f;
+      u[l] = act ? d.uo[o + l] : 0.f;
+      v[l] = act ? d.vo[o + l] : 0.f;
+    }
   }
+#define COL_H(i) (W ? ((i) < ilevel ? bH[ol + (i)] : 0.f) : h[W ? 0 : (i)])
+#define COL_U(i) (W ? ((i) < ilevel ? bU[ol + (i)] : 0.f) : u[W ? 0 : (i)])
+#define COL_V(i) (W ? ((i) < ilevel ? bV[ol + (i)] : 0.f) : v[W ? 0 : (i)])
   const int I = NLV + 1;
   const float aux = (float)dt * P.at;
   const bool explicit_visc = P.ahpar > 0.f;
@@ -78,18 +115,24 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
   if (0 < ilevel)
     alev_t += (d.visv[(size_t)kn[0] * I] + d.visv[(size_t)kn[1] * I] + d.visv[(size_t)kn[2] * I]) * (1.f / 3.f);
   float brm = 0.f, crm = 0.f, hhm = 0.f;   // baroclinic values of the layer above
+  // sigma layers: each vertex's depth of the current layer's top interface
+  // (hkko: the old level and the old node thickness summed from the top)
+  double hoi[3] = {0., 0., 0.};
+  if (barocl && P.nsigma > 0)
+#pragma unroll
+    for (int ii = 0; ii < 3; ii++) hoi[ii] = -(double)d.zo[kn[ii]];
   float pxs = 0.f, pys = 0.f;              // their running sums from the surface
 #pragma unroll
   for (int l = 0; l < L; l++) {
     if (l >= ilevel) break;
     const bool bfirst = l == 0, blast = l == ilevel - 1;
-    const float hhi = h[l], uui = u[l], vvi = v[l];
-    float hhip = blast ? 0.f : h[l + 1 < L ? l + 1 : l];
-    float uuip = blast ? uui : u[l + 1 < L ? l + 1 : l];
-    float vvip = blast ? vvi : v[l + 1 < L ? l + 1 : l];
-    const float hhim = bfirst ? 0.f : h[l > 0 ? l - 1 : 0];
-    const float uuim = bfirst ? uui : u[l > 0 ? l - 1 : 0];
-    const float vvim = bfirst ? vvi : v[l > 0 ? l - 1 : 0];
+    const float hhi = COL_H(l), uui = COL_U(l), vvi = COL_V(l);
+    float hhip = blast ? 0.f : COL_H(l + 1 < L ? l + 1 : l);
+    float uuip = blast ? uui : COL_U(l + 1 < L ? l + 1 : l);
+    float vvip = blast ? vvi : COL_V(l + 1 < L ? l + 1 : l);
+    const float hhim = bfirst ? 0.f : COL_H(l > 0 ? l - 1 : 0);
+    const float uuim = bfirst ? uui : COL_U(l > 0 ? l - 1 : 0);
+    const float vvim = bfirst ? vvi : COL_V(l > 0 ? l - 1 : 0);
     const float rhact = hhi > 0.f ? 1.f / hhi : 0.f;
     const float rhactp = hhip > 0.f ? 1.f / hhip : 0.f;
     const float rhactm = hhim > 0.f ? 1.f / hhim : 0.f;
@@ -161,20 +204,52 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
       fy += P.rlin * yadv;
     }
     if (barocl) {
-      // set_barocl_new_interface for z-layers (explicit.f90:1226-1530)
-      float br = 0.f, cr = 0.f;
+      // set_barocl_new_interface (explicit.f90:1226-1530): on z-layers the
+      // mean of the density gradients of the layers above and below an
+      // interface; on sigma layers the gradient on the horizontal surface
+      // at the element's mean depth of the interface (bsigadjust), with the
+      // cases of one or two vertices below the bottom
+      const bool bsig = l < P.nsigma;
+      float br = 0.f, cr = 0.f, brl = 0.f, crl = 0.f;
+      int nb = 0, nn = 0;
+      const double helei = (hoi[0] + hoi[1] + hoi[2]) / 3.;
 #pragma unroll
       for (int ii = 0; ii < 3; ii++) {
-        const float rp = d.rho[(size_t)kn[ii] * NLV + l];
+        const int k = kn[ii];
+        float rp = d.rho[(size_t)k * NLV + l];
+        if (l + 1 == P.nsigma) { brl += (float)b[ii] * rp; crl += (float)c[ii] * rp; }
+        if (bsig) {
+          bool below;
+          rp = sigma_rho_at(d.hko + (size_t)k * NLV, d.rho + (size_t)k * NLV, -(double)d.zo[k], d.ilhkv[k], helei,
+                            &below);
+          if (below) { nb++; nn += ii + 1; }
+        }
         br += (float)b[ii] * rp; cr += (float)c[ii] * rp;
       }
-      const float hlayer = hld[l];
+      const float hlayer = bsig ? hhi : hld[l];
       const float hh = 0.5f * hlayer;
-      const float brup = bfirst ? br : brm, crup = bfirst ? cr : crm, hhup = bfirst ? 0.f : hhm;
+      const float hhup = bfirst ? 0.f : hhm;
       const float hint = hh + hhup;
-      pxs += hint * 0.5f * (br + brup);
-      pys += hint * 0.5f * (cr + crup);
-      brm = br; crm = cr; hhm = hh;
+      float brint, crint;
+      if (bsig) {
+        if (nb == 2) { brint = brm; crint = crm; }
+        else if (nb == 1) {                // the gradient along the bottom side kept from above
+          const float b3 = (float)b[nn - 1], c3 = (float)c[nn - 1];
+          const float aux = 1.f / (c3 * c3 + b3 * b3);
+          const float pu = aux * (brm * b3 + crm * c3), pc = aux * (br * b3 + cr * c3);
+          brint = pu * b3 + (br - pc * b3);
+          crint = pu * c3 + (cr - pc * c3);
+        } else { brint = br; crint = cr; }
+      } else if (bfirst) { brint = br; crint = cr; }
+      else { brint = 0.5f * (br + brm); crint = 0.5f * (cr + crm); }
+      pxs += hint * brint;
+      pys += hint * crint;
+      brm = br; crm = cr;
+      if (l + 1 == P.nsigma) { brm = brl; crm = crl; }
+      hhm = hh;
+      if (P.nsigma > 0)
+#pragma unroll
+        for (int ii = 0; ii < 3; ii++) hoi[ii] += (double)d.hko[(size_t)kn[ii] * NLV + l];
       fx += raux * hlayer * pxs;
       fy += raux * hlayer * pys;
     }
@@ -248,16 +323,34 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
         solu = y0.x; solv = y0.y; hre = y1.x; him = y1.y;
       }
     }
-    const float uhat = act ? (float)(u[l] - dt * solu) : 0.f;
-    const float vhat = act ? (float)(v[l] - dt * solv) : 0.f;
-    d.un[o + l] = uhat;
-    d.vn[o + l] = vhat;
-    d.ddx[o + l] = act ? hre : 0.f;
+    const float ul = COL_U(l), vl = COL_V(l);
+    const float uhat = act ? (float)(ul - dt * solu) : 0.f;
+    const float vhat = act ? (float)(vl - dt * solv) : 0.f;
+    if constexpr (W) {
+      bU[ol + l] = uhat;                              // spare lanes write past the warp's run
+      bV[ol + l] = vhat;
+      bH[ol + l] = act ? hre : 0.f;
+    } else {
+      d.un[o + l] = uhat;
+      d.vn[o + l] = vhat;
+      d.ddx[o + l] = act ? hre : 0.f;
+    }
     if (COR) d.ddxi[o + l] = act ? him : 0.f;
     if (act) {
       dbb += (double)hre; dcb += (double)him;
-      uold += (double)u[l]; vold += (double)v[l];
+      uold += (double)ul; vold += (double)vl;
       uh += (double)uhat; vh += (double)vhat;
+    }
+  }
+
+  if constexpr (W) {
+    __syncwarp();
+    const size_t base = (size_t)w0 * NLV;
+    const int cnt = nw * NLV;
+    for (int j = lane; j < cnt; j += 32) {
+      d.un[base + j] = bU[j];
+      d.vn[base + j] = bV[j];
+      d.ddx[base + j] = bH[j];
     }
   }
 
@@ -297,7 +390,10 @@ __global__ void __launch_bounds__(128, 3) k_column_t(Dev d) {
       hik[i] = rw * hia[i][i];
     }
   }
-  store_elem_system(d, e, hia, hik);
+  if (valid) store_elem_system(d, e, hia, hik);
+#undef COL_H
+#undef COL_U
+#undef COL_V
 }
 
 }  // namespace shy

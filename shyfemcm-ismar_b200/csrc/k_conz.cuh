@@ -497,7 +497,8 @@ __global__ void __launch_bounds__(256) k_rho(Dev d, const int *kbas) {
   const size_t o = (size_t)k * NLV + lane;
   const size_t SN = (size_t)d.NKN * NLV;
   const float *hld = d.hldv + (size_t)b * NLV;
-  const double hh = lane < NLV ? 0.5 * (double)hld[lane] : 0.;
+  // sigma layers: the old thickness of the step (hdkov); z-layers: nominal
+  const double hh = lane < NLV ? 0.5 * (lane < P.nsigma ? (act ? (double)d.hko[o] : 0.) : (double)hld[lane]) : 0.;
   const double rold = act ? (double)d.rho[o] : 0.;
   const double dpresc = rold * P.grav * hh;
   const double depth = seg_scan_down<S>(act ? 2. * hh : 0., lane) - hh;

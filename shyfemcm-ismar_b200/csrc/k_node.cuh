@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
 // incident elements are walked once, each adding to the FP64 sums of all
 // its layers (in element order, as k_node); then the node's layers in turn
 // ===========================================================================
-template <int L>
+template <int L, bool PF = false>
 __global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int init_only) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.NKN) return;
@@ -150,6 +150,18 @@ __global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int i
     const float ze = P.wetdry ? d.zen[3 * e + ii] : (float)z;
     double us = 0., vs = 0.;                  // the element's transports summed over its layers
     const int lev = P.nzadapt > 1 ? zad_levmax((double)ze, hlv, le, P.rzmov) : 0;
+    // PF: the element's transports of every layer loaded at once (the
+    // layers below its bottom hold zeros), so their loads are in flight
+    // together; else each layer's as the loop reaches it
+    float ue[PF ? L : 1], ve[PF ? L : 1];
+    if constexpr (PF) {
+#pragma unroll
+      for (int l = 0; l < L; l++) {
+        const bool in = !init_only && l < NLV;
+        ue[l] = in ? d.usv[oe + l] : 0.f;
+        ve[l] = in ? d.vsv[oe + l] : 0.f;
+      }
+    }
 #pragma unroll
     for (int l = 0; l < L; l++) {
       if (l >= le) break;
@@ -160,10 +172,11 @@ __global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int i
       else hl = hbot;
       hsum[l] += areafv * hl;
       if (!init_only) {
-        const float ff = d.usv[oe + l] * bb + d.vsv[oe + l] * cc;   // az*ffn + azt*ffo
+        const float ul = PF ? ue[PF ? l : 0] : d.usv[oe + l], vl = PF ? ve[PF ? l : 0] : d.vsv[oe + l];
+        const float ff = ul * bb + vl * cc;   // az*ffn + azt*ffo
         vf[l] += 3.f * areafv * ff;
-        us += (double)d.usv[oe + l];
-        vs += (double)d.vsv[oe + l];
+        us += (double)ul;
+        vs += (double)vl;
       }
     }
     if (!init_only) {
@@ -422,7 +435,8 @@ __global__ void __launch_bounds__(256) k_rhoset(Dev d, const int *kbas) {
   const size_t SN = (size_t)d.NKN * NLV;
   const float *tv = d.sc_in, *sv = d.sc_in + SN;     // T is scalar 0, S scalar 1
   const float *hld = d.hldv + (size_t)b * NLV;
-  const double hh = lane < NLV ? 0.5 * (double)hld[lane] : 0.;
+  // sigma layers: the initial thickness (hdkov = hdknv at the start); z-layers: nominal
+  const double hh = lane < NLV ? 0.5 * (lane < P.nsigma ? (act ? (double)d.hkn[o] : 0.) : (double)hld[lane]) : 0.;
   const double depth = seg_scan_down<S>(act ? 2. * hh : 0., lane) - hh;
   double r = 0.;
   const double t = act ? (double)tv[o] : 0., sal = act ? (double)sv[o] : 0.;

@@ -92,4 +92,42 @@ __device__ __forceinline__ double zad_elem_h(int l, const double (&z)[3], const 
   return (double)hm.w - (double)hlv[lmax - 2];
 }
 
+// set_barocl_new_interface with bsigadjust (explicit.f90:1346-1440): the
+// density of node column k at depth `dep` below the rest level, for an
+// interface of sigma layers that does not lie on a horizontal surface.  The
+// column's interfaces are at -zo + the old layer thicknesses hk summed from
+// the top (hkko); the layer ll holding `dep` brackets it, with the layer
+// above or below, between their mid-layer depths (hkkom), and the density
+// is interpolated there; above the first mid-layer it is the first layer's
+// (ld = 1), below the last it is the last layer's and *below is set (nb).
+// The reference looks for ll from layer l up or down; for a column whose
+// interfaces increase with depth that finds the same layer as this scan
+// from the top.
+__device__ __forceinline__ float sigma_rho_at(const float *hk, const float *rho, double z0, int lkmax, double dep,
+                                              bool *below) {
+  *below = false;
+  int ll = lkmax;
+  double ho = z0;
+  for (int j = 1; j <= lkmax; j++) {
+    ho += hk[j - 1];
+    if (dep < ho) { ll = j; break; }
+  }
+  // hkkom of layers ll-1, ll and ll+1
+  double top = z0;
+  for (int j = 1; j < ll - 1; j++) top += hk[j - 1];
+  const double hop = ll >= 2 ? top + hk[ll - 2] : z0;            // hkko(ll-1)
+  const double hmm = ll >= 2 ? 0.5 * (top + hop) : z0;            // hkkom(ll-1)
+  const double hoc = hop + hk[ll - 1];                           // hkko(ll)
+  const double hmc = 0.5 * (hop + hoc);                          // hkkom(ll)
+  const double hmp = ll < lkmax ? 0.5 * (hoc + hoc + hk[ll]) : 0.;   // hkkom(ll+1)
+  int lu, ld;
+  double hu, hd;
+  if (dep < hmc) { lu = ll == 1 ? 1 : ll - 1; ld = ll; hu = ll == 1 ? hmc : hmm; hd = hmc; }
+  else { lu = ll; ld = ll == lkmax ? lkmax : ll + 1; hu = hmc; hd = ll == lkmax ? hmc : hmp; }
+  if (ld == 1) return rho[0];
+  if (lu >= lkmax) { *below = true; return rho[lkmax - 1]; }
+  const double alpha = (dep - hu) / (hd - hu);
+  return (float)(alpha * (double)rho[ld - 1] + (1. - alpha) * (double)rho[lu - 1]);
+}
+
 }  // namespace shy

@@ -66,8 +66,10 @@ static void launch_column_t(const Dev &d, cudaStream_t st, bool cor) {
   // the advective terms as a separate instance: the plain one keeps its registers
   if (d.mom) {
     if (cor) k_column_t<L, true, true><<<blocks, 128, 0, st>>>(d);
+    else if (d.col_staged) k_column_t<L, false, true, true><<<blocks, 128, 0, st>>>(d);
     else k_column_t<L, false, true><<<blocks, 128, 0, st>>>(d);
   } else if (cor) k_column_t<L, true, false><<<blocks, 128, 0, st>>>(d);
+  else if (d.col_staged) k_column_t<L, false, false, true><<<blocks, 128, 0, st>>>(d);
   else k_column_t<L, false, false><<<blocks, 128, 0, st>>>(d);
 }
 

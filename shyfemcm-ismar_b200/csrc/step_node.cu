@@ -22,9 +22,15 @@ extern template void launch_node_S<32>(const Dev &, const int *, int, int, int, 
 void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStream_t st) {
   if (which == 0 && (d.col_threads || d.any_wd) && d.NLV <= 16) {
     const int blocks = (d.NKN + 127) / 128;
-    if (d.NLV <= 8) k_node_t<8><<<blocks, 128, 0, st>>>(d, kbas, a);
-    else if (d.NLV <= 12) k_node_t<12><<<blocks, 128, 0, st>>>(d, kbas, a);
-    else k_node_t<16><<<blocks, 128, 0, st>>>(d, kbas, a);
+    if (d.node_prefetch) {
+      if (d.NLV <= 8) k_node_t<8, true><<<blocks, 128, 0, st>>>(d, kbas, a);
+      else if (d.NLV <= 12) k_node_t<12, true><<<blocks, 128, 0, st>>>(d, kbas, a);
+      else k_node_t<16, true><<<blocks, 128, 0, st>>>(d, kbas, a);
+    } else {
+      if (d.NLV <= 8) k_node_t<8><<<blocks, 128, 0, st>>>(d, kbas, a);
+      else if (d.NLV <= 12) k_node_t<12><<<blocks, 128, 0, st>>>(d, kbas, a);
+      else k_node_t<16><<<blocks, 128, 0, st>>>(d, kbas, a);
+    }
     return;
   }
   switch (d.S) {

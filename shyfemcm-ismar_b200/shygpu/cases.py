@@ -410,6 +410,36 @@ def nh_basin_case(nkn_target=1500, lx=300.0, ly=150.0, seed=2, dt=0.5, nlv=12, h
     return c
 
 
+def stratified_basin_case(nkn_target=1500, lx=30.0e3, ly=15.0e3, nlv=12, sigma=True, hmin=5.0, hmax=60.0,
+                          wind=0.0, noise=0.0, dt=60.0, seed=2):
+    """Closed basin on sigma layers (or z-layers) over Gaussian bumps from
+    `hmin` to `hmax` m, stably stratified: temperature 20 degC at the
+    surface falling by 10 degC over 60 m of depth (plus seeded noise of
+    `noise` degC), salinity 35, baroclinic pressure on, optional uniform
+    wind.  At rest, a horizontal stratification over a sloping bottom is
+    where sigma layers need the density gradient taken on horizontal
+    surfaces (set_barocl_new_interface's bsigadjust)."""
+    c = nh_basin_case(nkn_target=nkn_target, lx=lx, ly=ly, seed=seed, dt=dt, nlv=nlv, hmin=hmin, hmax=hmax,
+                      sigma=sigma, wind=wind, ts=True)
+    c["params"] = dict(c["params"], inohyd=0, ibarcl=1)
+    nkn = c["nkn"]
+    hk = np.zeros(nkn)
+    cnt = np.zeros(nkn)
+    np.add.at(hk, c["nen3v"].ravel() - 1, c["hm3v"].ravel())
+    np.add.at(cnt, c["nen3v"].ravel() - 1, 1)
+    hk /= cnt
+    if sigma:
+        zc = (np.arange(nlv)[None, :] + 0.5) / nlv * hk[:, None]
+    else:
+        hlv, hld = c["hlv"].astype(float), c["hldv"].astype(float)
+        zc = np.broadcast_to(hlv - 0.5 * hld, (nkn, nlv)).copy()
+    rng = np.random.default_rng(seed + 404)
+    c["tempv"] = (20.0 - 10.0 * zc / 60.0 + noise * rng.standard_normal((nkn, nlv))).astype(np.float32)
+    c["saltv"] = np.full((nkn, nlv), 35.0, np.float32)
+    c["name"] = f"stratified_{nkn}x{nlv}_{'sigma' if sigma else 'z'}"
+    return c
+
+
 def ensemble_member_case(nkn_target, aspect, seed, wind, dt=60.0, nlv=10, spacing=100.0,
                          ampli=0.5, depth=10.0, ddepth=2.0, top=2.0):
     """One member of the batched ensemble, made as the 2D channel is: a

@@ -591,3 +591,62 @@ def test_horizontal_viscosity_and_diffusion(small3d, shape):
     s0 = o0.state()
     f = fields[0]
     assert np.abs(s0[f] - so[f]).max() > 1e-3 * np.abs(so[f]).max()
+
+
+@pytest.mark.parametrize("ilin", [1, 0])
+def test_staged_column_kernel_equals_in_place(small3d, ilin):
+    """The thread-per-column kernel with its columns staged through shared
+    memory (the default without Coriolis) against the same kernel reading
+    its columns in place: the same arithmetic, so the same state up to the
+    compiler's choice of fused multiply-adds in either instance."""
+    c = dict(small3d)
+    c["params"] = dict(c["params"], ilin=ilin)
+    states = []
+    for staged in (1, 0):
+        g = shygpu.Model(c)
+        g.set_option("column_staged", staged)
+        assert g.get_option("column_staged") == staged
+        g.set_state(0)
+        g.run(60)
+        states.append(g.get_state(0))
+    for f in ("znv", "utlnv", "vtlnv", "tempv", "saltv"):
+        a, b = states[0][f], states[1][f]
+        assert np.abs(a - b).max() <= 1e-6 * max(np.abs(b).max(), 1e-6), f
+
+
+@pytest.mark.parametrize("column_threads", [1, 0])
+def test_sigma_baroclinic(column_threads):
+    """Baroclinic pressure on sigma layers (set_barocl_new_interface with
+    bsigadjust): a stratified basin over 5-60 m bumps under wind, with noise
+    in the temperature, on both column-kernel forms."""
+    c = cases.stratified_basin_case(sigma=True, wind=8.0, noise=0.2)
+    g, o = run_both(c, 120, column_threads=column_threads)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    m, me = active_mask(c), active_mask(c, node=False)
+    umax = max(np.abs(so["utlnv"][me]).max(), np.abs(so["vtlnv"][me]).max())
+    for f in ("utlnv", "vtlnv"):
+        assert np.abs(sg[f] - so[f])[me].max() <= 1e-3 * umax, f
+    rel = np.abs(sg["tempv"] - so["tempv"])[m].max() / np.abs(so["tempv"][m]).max()
+    assert rel <= TRACER_RTOL, rel
+    assert np.abs(sg["rhov"] - so["rhov"])[m].max() <= 1e-3
+
+
+def test_hybrid_baroclinic():
+    """Hybrid layers (sigma layers down to hsigma, z-layers below) with T/S
+    and the baroclinic pressure."""
+    c = cases.hybrid_lagoon_case()
+    nkn, nlv = c["nkn"], c["nlv"]
+    rng = np.random.default_rng(21)
+    c["tempv"] = (18.0 - 0.3 * np.arange(nlv)[None, :] + 0.1 * rng.standard_normal((nkn, nlv))).astype(np.float32)
+    c["saltv"] = (34.0 + 0.1 * np.arange(nlv)[None, :] + 0.05 * rng.standard_normal((nkn, nlv))).astype(np.float32)
+    c["params"] = dict(c["params"], ibarcl=1, itemp=1, isalt=1)
+    g, o = run_both(c, 80)
+    sg, so = g.get_state(0), o.state()
+    assert np.abs(sg["znv"] - so["znv"]).max() <= ZETA_TOL
+    m, me = active_mask(c), active_mask(c, node=False)
+    umax = max(np.abs(so["utlnv"][me]).max(), np.abs(so["vtlnv"][me]).max())
+    assert np.abs(sg["utlnv"] - so["utlnv"])[me].max() <= 1e-3 * umax
+    for f in ("tempv", "saltv"):
+        rel = np.abs(sg[f] - so[f])[m].max() / np.abs(so[f][m]).max()
+        assert rel <= TRACER_RTOL, (f, rel)
