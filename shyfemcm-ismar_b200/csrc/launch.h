@@ -64,7 +64,7 @@ struct CsrGrid {
   double rtol = 1e-8, atol = 1e-8;
   int maxit = 1000, max_outer = 12;
   float inner_rtol = 1e-4f;
-  long long spin_limit = 1LL << 24;
+  long long spin_limit = 1LL << 22;
 };
 // which: 0 k_nh_w (sp256wnh), 1 k_nh_sys (the 3D system), 2 k_nh_node, 3 k_nh_elem
 void launch_nh(const Dev &d, const NhSys &s, int which, cudaStream_t st);

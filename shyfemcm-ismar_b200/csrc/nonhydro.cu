@@ -257,16 +257,17 @@ __device__ __forceinline__ bool nh_barrier(const CsrGrid &a, unsigned bar, int *
   return *s_ok != 0;
 }
 
+// shared scratch of the sums; the barrier count and the parity of the
+// partial-sum slots are kept by every thread in its own registers (all
+// threads take the same barriers), so no thread updates them for another
 struct NhRed {
   double wsum[4 * 32];
   double bc[4];
   int ok;
-  unsigned bar;
-  int par;
 };
 
 template <int NV>
-__device__ __forceinline__ bool nh_gsum(const CsrGrid &a, double (&v)[NV], NhRed &sm) {
+__device__ __forceinline__ bool nh_gsum(const CsrGrid &a, double (&v)[NV], NhRed &sm, unsigned &bar, int &par) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int i = 0; i < NV; i++) {
@@ -277,7 +278,7 @@ __device__ __forceinline__ bool nh_gsum(const CsrGrid &a, double (&v)[NV], NhRed
   }
   __syncthreads();
   const int G = gridDim.x;
-  double *part = a.part + (size_t)sm.par * G * 4;
+  double *part = a.part + (size_t)par * G * 4;
   if (warp == 0) {
 #pragma unroll
     for (int i = 0; i < NV; i++) {
@@ -287,7 +288,7 @@ __device__ __forceinline__ bool nh_gsum(const CsrGrid &a, double (&v)[NV], NhRed
       if (lane == 0) part[(size_t)blockIdx.x * 4 + i] = x;
     }
   }
-  if (!nh_barrier(a, ++sm.bar, &sm.ok)) return false;
+  if (!nh_barrier(a, ++bar, &sm.ok)) return false;
   if (warp == 0) {
 #pragma unroll
     for (int i = 0; i < NV; i++) {
@@ -301,7 +302,7 @@ __device__ __forceinline__ bool nh_gsum(const CsrGrid &a, double (&v)[NV], NhRed
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < NV; i++) v[i] = sm.bc[i];
-  sm.par ^= 1;
+  par ^= 1;
   return true;
 }
 
@@ -313,7 +314,9 @@ __device__ __forceinline__ float nh_spmv(const CsrGrid &a, int i, const float *u
 
 __global__ void __launch_bounds__(512) k_nh_solve(CsrGrid a) {
   __shared__ NhRed sm;
-  if (threadIdx.x == 0) { sm.bar = 0; sm.par = 0; sm.ok = 1; }
+  unsigned bar = 0;     // grid barriers taken so far (the same in every thread)
+  int par = 0;          // slot set of the next partial sums
+  if (threadIdx.x == 0) sm.ok = 1;
   __syncthreads();
   const int n = a.r1 - a.r0, G = gridDim.x;
   const int chunk = (n + G - 1) / G;
@@ -331,7 +334,7 @@ __global__ void __launch_bounds__(512) k_nh_solve(CsrGrid a) {
     a.dinv[i] = diag != 0. ? (float)(1. / diag) : 1.f;
     a.x64[i] = (double)a.x[i];
   }
-  if (!nh_barrier(a, ++sm.bar, &sm.ok)) aborted = true;
+  if (!nh_barrier(a, ++bar, &sm.ok)) aborted = true;
 
   double tol = 0., rn = 0., rn0 = 0.;
   int iters = 0, outer = 0;
@@ -346,7 +349,7 @@ __global__ void __launch_bounds__(512) k_nh_solve(CsrGrid a) {
       a.p[i] = 0.f; a.v[i] = 0.f; a.e[i] = 0.f;
       acc[0] += res * res;
     }
-    if (!nh_gsum<1>(a, acc, sm)) { aborted = true; break; }
+    if (!nh_gsum<1>(a, acc, sm, bar, par)) { aborted = true; break; }
     rn = sqrt(acc[0]);
     if (outer == 0) { tol = a.rtol * rn + a.atol; rn0 = rn; }
     if (rn <= tol) { conv = true; break; }
@@ -362,14 +365,14 @@ __global__ void __launch_bounds__(512) k_nh_solve(CsrGrid a) {
         a.p[i] = pp;
         a.z[i] = a.dinv[i] * pp;
       }
-      if (!nh_barrier(a, ++sm.bar, &sm.ok)) { aborted = true; break; }
+      if (!nh_barrier(a, ++bar, &sm.ok)) { aborted = true; break; }
       double g1[1] = {0.};
       for (int i = c0 + tid; i < c1; i += nth) {
         const float vv = nh_spmv(a, i, a.z);
         a.v[i] = vv;
         g1[0] += (double)a.rh[i] * vv;
       }
-      if (!nh_gsum<1>(a, g1, sm)) { aborted = true; break; }
+      if (!nh_gsum<1>(a, g1, sm, bar, par)) { aborted = true; break; }
       alpha = g1[0] != 0. ? rho / g1[0] : 0.;
       const float fa = (float)alpha;
       for (int i = c0 + tid; i < c1; i += nth) {
@@ -377,7 +380,7 @@ __global__ void __launch_bounds__(512) k_nh_solve(CsrGrid a) {
         a.s[i] = ss;
         a.q[i] = a.dinv[i] * ss;
       }
-      if (!nh_barrier(a, ++sm.bar, &sm.ok)) { aborted = true; break; }
+      if (!nh_barrier(a, ++bar, &sm.ok)) { aborted = true; break; }
       double g2[2] = {0., 0.};
       for (int i = c0 + tid; i < c1; i += nth) {
         const float tt = nh_spmv(a, i, a.q);
@@ -385,7 +388,7 @@ __global__ void __launch_bounds__(512) k_nh_solve(CsrGrid a) {
         g2[0] += (double)tt * a.s[i];
         g2[1] += (double)tt * tt;
       }
-      if (!nh_gsum<2>(a, g2, sm)) { aborted = true; break; }
+      if (!nh_gsum<2>(a, g2, sm, bar, par)) { aborted = true; break; }
       omega = g2[1] > 0. ? g2[0] / g2[1] : 0.;
       const float fw = (float)omega;
       double g3[2] = {0., 0.};
@@ -396,14 +399,14 @@ __global__ void __launch_bounds__(512) k_nh_solve(CsrGrid a) {
         g3[0] += (double)rr * rr;
         g3[1] += (double)a.rh[i] * rr;
       }
-      if (!nh_gsum<2>(a, g3, sm)) { aborted = true; break; }
+      if (!nh_gsum<2>(a, g3, sm, bar, par)) { aborted = true; break; }
       iters++;
       rho1 = g3[1];
       if (sqrt(g3[0]) <= itol || omega == 0. || alpha == 0. || !(g3[0] == g3[0])) break;
     }
     if (aborted) break;
     for (int i = c0 + tid; i < c1; i += nth) a.x64[i] += (double)a.e[i];
-    if (!nh_barrier(a, ++sm.bar, &sm.ok)) { aborted = true; break; }
+    if (!nh_barrier(a, ++bar, &sm.ok)) { aborted = true; break; }
   }
   for (int i = c0 + tid; i < c1; i += nth) a.x[i] = (float)a.x64[i];
   if (blockIdx.x == 0 && tid == 0) {
