@@ -97,6 +97,10 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
   double dv = 0.;
   if (act && P.nlv > 1) {
     double voln = (double)(hkf * (float)area), volo = (double)(d.hko[o] * (float)area);
+    // a sigma layer's thickness moves with the level alone, -hldv (zn - zo):
+    // taken so, its change carries no rounding of the two FP32 thicknesses,
+    // which at short time steps would be most of the change
+    if (lane < P.nsigma) { voln = -hldl * (z - (double)d.zo[k]) * (double)(float)area; volo = 0.; }
     dv = vf + (double)q - (voln - volo) / P.dt;
   }
   double wtop = seg_scan_up<S>(dv, lane);      // flux through the top interface of layer lane
@@ -223,8 +227,12 @@ __global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int i
     double dv = 0.;
     if (act && P.nlv > 1) {
       const float areal = d.areakv[o + l];
-      const double voln = (double)(hkf[l] * areal);
-      const double volo = (double)(d.hko[o + l] * areal);
+      double voln = (double)(hkf[l] * areal);
+      double volo = (double)(d.hko[o + l] * areal);
+      // a sigma layer's thickness moves with the level alone, -hldv (zn -
+      // zo): taken so, its change carries no rounding of the two FP32
+      // thicknesses, which at short time steps would be most of the change
+      if (l < P.nsigma) { voln = -(double)hld[l] * (z - (double)d.zo[k]) * (double)areal; volo = 0.; }
       const float q = vtot > 0. ? (float)((double)rq * ((double)(d.hko[o + l] * d.areakv[o + l]) / vtot)) : 0.f;
       dv = (double)vf[l] + (double)q - (voln - volo) / P.dt;
     }
