@@ -252,11 +252,15 @@ int shygpu_set_forcing(shygpu_model *model, int32_t ibasin, const float *tauxnv,
  * the reference runs one basin per process).  set_forcing_all copies the
  * forcing of every basin, concatenated in basin order (NKN values per
  * array, NULL skips one); get_levels copies the water level of every basin
- * of the latest enqueued step the same way.  Both are enqueued on the
- * model's stream and return at once: with pinned host buffers they overlap
- * the host's work, run in order with the steps enqueued around them, and
- * are complete after shygpu_sync.  The host buffers must stay untouched
- * until then.                                                              */
+ * of the latest enqueued step the same way.  Both return at once and act
+ * in order with the steps enqueued around them; they are complete after
+ * shygpu_sync (or shygpu_run).  The copies run on two transfer streams of
+ * the model, so with pinned host buffers they overlap the steps as well as
+ * the host's work: the forcing of the next step goes up while the current
+ * one runs (through one of two device staging copies, allocated on first
+ * use and counted by shygpu_model_bytes), and a step's level comes down
+ * while the following step runs.  The host buffers must stay untouched
+ * until shygpu_sync.                                                        */
 int shygpu_set_forcing_all(shygpu_model *model, const float *tauxnv, const float *tauynv,
                            const float *ppv, const float *rqv);
 int shygpu_get_levels(shygpu_model *model, float *znv);

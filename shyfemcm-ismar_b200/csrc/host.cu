@@ -291,6 +291,18 @@ struct shygpu_model {
   BasinPar *cz_par = nullptr;
   BasinOut *cz_outp = nullptr;
   cudaStream_t stream = nullptr;
+  // the pipelined transfers of shygpu_set_forcing_all and shygpu_get_levels
+  // run on their own streams (made on first use), so that the copies of one
+  // step overlap the kernels of another: the forcing goes up into one of two
+  // device staging generations and is copied into place on the model's
+  // stream; a level copy reads the ping-pong level buffer that the next step
+  // does not write, and the step after it waits for the copy (lev_pending)
+  cudaStream_t xin = nullptr, xout = nullptr;
+  float *fstage[2][4] = {};
+  size_t fstage_bytes = 0;
+  cudaEvent_t ev_fin[2] = {}, ev_fused[2] = {}, ev_done = nullptr, ev_lev[2] = {};
+  bool fused_rec[2] = {false, false}, lev_pending[2] = {false, false};
+  int fgen = 0;
   // options
   int nsub = 2, use_graph = 1, max_outer = 12, sym = 1;
   int zvariant = 1;                  // 1: shared-memory zeta solver when it fits
@@ -745,7 +757,53 @@ extern "C" int64_t shygpu_footprint(int32_t nbasin, const shy_basin *basins, con
   return footprint_of(nbasin, basins, params, nullptr);
 }
 
-extern "C" int64_t shygpu_model_bytes(const shygpu_model *m) { return m ? m->arena.bytes : -1; }
+extern "C" int64_t shygpu_model_bytes(const shygpu_model *m) {
+  return m ? (int64_t)(m->arena.bytes + m->fstage_bytes) : -1;
+}
+
+// the streams and events of the pipelined transfers, made on first use
+static int xfer_setup(shygpu_model *m) {
+  if (m->xin) return SHY_OK;
+  CUDA_TRY(cudaStreamCreateWithFlags(&m->xin, cudaStreamNonBlocking));
+  CUDA_TRY(cudaStreamCreateWithFlags(&m->xout, cudaStreamNonBlocking));
+  for (int i = 0; i < 2; i++) {
+    CUDA_TRY(cudaEventCreateWithFlags(&m->ev_fin[i], cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&m->ev_fused[i], cudaEventDisableTiming));
+    CUDA_TRY(cudaEventCreateWithFlags(&m->ev_lev[i], cudaEventDisableTiming));
+  }
+  CUDA_TRY(cudaEventCreateWithFlags(&m->ev_done, cudaEventDisableTiming));
+  return SHY_OK;
+}
+
+// the model's stream waits for the level copies still reading level buffer
+// `which` (-1: both) before work that writes it is enqueued
+static int wait_levels(shygpu_model *m, int which) {
+  for (int i = 0; i < 2; i++)
+    if ((which < 0 || which == i) && m->lev_pending[i]) {
+      CUDA_TRY(cudaStreamWaitEvent(m->stream, m->ev_lev[i], 0));
+      m->lev_pending[i] = false;
+    }
+  return SHY_OK;
+}
+
+static void xfer_release(shygpu_model *m) {
+  if (!m->xin) return;
+  cudaStreamSynchronize(m->stream);         // the copies out of the staging arrays
+  cudaStreamSynchronize(m->xin);
+  cudaStreamSynchronize(m->xout);
+  for (int g = 0; g < 2; g++)
+    for (int a = 0; a < 4; a++)
+      if (m->fstage[g][a]) cudaFree(m->fstage[g][a]);
+  for (int i = 0; i < 2; i++) {
+    cudaEventDestroy(m->ev_fin[i]);
+    cudaEventDestroy(m->ev_fused[i]);
+    cudaEventDestroy(m->ev_lev[i]);
+  }
+  cudaEventDestroy(m->ev_done);
+  cudaStreamDestroy(m->xin);
+  cudaStreamDestroy(m->xout);
+  m->xin = m->xout = nullptr;
+}
 
 extern "C" int shygpu_destroy(shygpu_model *m) {
   if (!m) return SHY_OK;
@@ -761,6 +819,7 @@ extern "C" int shygpu_destroy(shygpu_model *m) {
     if (m->ev_join[i]) cudaEventDestroy(m->ev_join[i]);
   }
   if (m->ev_fork) cudaEventDestroy(m->ev_fork);
+  xfer_release(m);
   m->arena.release();
   if (m->stream) cudaStreamDestroy(m->stream);
   delete m;
@@ -1167,6 +1226,11 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   d.any_tvd = m->any_tvd ? 1 : 0;
   d.any_tvdv = 0;
   for (int b = 0; b < nbasin; b++) d.any_tvdv |= Pp[b].itvdv == 1 ? 1 : 0;
+  d.any_xt = 0;
+  for (int b = 0; b < nbasin; b++) {
+    const BasinPar &q = m->par[b];
+    d.any_xt |= (q.ahpar > 0.f || (q.ibarcl > 0 && q.ibarcl != 3 && q.ibarcl != 5) || q.inohyd) ? 1 : 0;
+  }
   ST_TRY(A.upload(&d.par, m->par) ? bail(SHY_ECAPACITY) : 0);
   std::vector<BasinOut> outs(nbasin);
   memset(outs.data(), 0, sizeof(BasinOut) * nbasin);
@@ -1378,6 +1442,7 @@ extern "C" int shygpu_set_state(shygpu_model *m, int32_t ib, const shy_state *s)
   cudaStream_t st = m->stream;
   const int c = m->cur;
   drop_graphs(m);
+  ST_TRY(wait_levels(m, -1));
   CUDA_TRY(cudaMemsetAsync(&m->base.out[ib].steps, 0, sizeof(int), st));   // no earlier level yet
   // a set-up of another basin derives this one's state too, and may have
   // flagged it while its levels were still unset
@@ -1554,6 +1619,10 @@ static void advance_host(shygpu_model *m) {
 }
 
 static int check_outputs(shygpu_model *m) {
+  if (m->xin) {
+    CUDA_TRY(cudaStreamSynchronize(m->xin));
+    CUDA_TRY(cudaStreamSynchronize(m->xout));
+  }
   CUDA_TRY(cudaMemcpyAsync(m->out_h.data(), m->base.out, sizeof(BasinOut) * m->nbasin, cudaMemcpyDeviceToHost, m->stream));
   CUDA_TRY(cudaStreamSynchronize(m->stream));
   for (int b = 0; b < m->nbasin; b++) {
@@ -1648,6 +1717,7 @@ extern "C" int shygpu_enqueue(shygpu_model *m, int32_t nsteps) {
   if (nsteps < 0) return fail(SHY_EARG, "enqueue: nsteps < 0");
   m->launches_per_step = count_launches(m);
   for (int i = 0; i < nsteps; i++) {
+    ST_TRY(wait_levels(m, 1 - m->cur));     // the step writes the other level buffer
     if (m->use_graph) {
       if (!m->graph[m->cur][m->sc_cur]) ST_TRY(build_graph(m, m->cur, m->sc_cur));
       CUDA_TRY(cudaGraphLaunch(m->graph[m->cur][m->sc_cur], m->stream));
@@ -1679,6 +1749,7 @@ extern "C" int shygpu_new_step(shygpu_model *m) {
 
 extern "C" int shygpu_hydro(shygpu_model *m) {
   if (!m || !m->state_set) return fail(SHY_ESTATE, "hydro: no state");
+  ST_TRY(wait_levels(m, 1 - m->cur));
   Dev d = dev_for_step(m, 1 - m->cur);
   ST_TRY(enqueue_hydro(m, d));
   g_launches += 4 + nh_launches(m);
@@ -1877,6 +1948,10 @@ extern "C" int shygpu_checkpoint_load(shygpu_model *m, const void *buf, int64_t 
     p += sizeof sz;
     if (sz != (int64_t)m->arena.sizes[i]) return fail(SHY_EARG, "checkpoint_load: array %zu differs in size", i);
   }
+  if (m->xout) {                               // level copies still reading the buffers
+    CUDA_TRY(cudaStreamSynchronize(m->xout));
+    m->lev_pending[0] = m->lev_pending[1] = false;
+  }
   CUDA_TRY(cudaStreamSynchronize(m->stream));
   for (size_t i = 0; i < m->arena.ptrs.size(); i++) {
     CUDA_TRY(cudaMemcpy(m->arena.ptrs[i], p, m->arena.sizes[i], cudaMemcpyHostToDevice));
@@ -1890,24 +1965,52 @@ extern "C" int shygpu_checkpoint_load(shygpu_model *m, const void *buf, int64_t 
 }
 
 // whole-model transfers for pipelined serving: one copy per array for all
-// basins (concatenated in basin order), enqueued on the model's stream
-// without waiting, so they overlap the host's work and order with the
-// steps around them
+// basins (concatenated in basin order), enqueued without waiting and
+// ordered with the steps around them.  The host-to-device copies run on
+// their own stream into a device staging generation (two, used in turn),
+// which the model's stream copies into place before the next step; so the
+// copy of step n+1's forcing overlaps step n.  The first call of a
+// generation allocates its staging arrays.
 extern "C" int shygpu_set_forcing_all(shygpu_model *m, const float *taux, const float *tauy, const float *ppv,
                                       const float *rqv) {
   if (!m) return fail(SHY_EARG, "set_forcing_all: model is NULL");
+  ST_TRY(xfer_setup(m));
   const size_t nb = (size_t)m->NKN * 4;
-  if (taux) CUDA_TRY(cudaMemcpyAsync(m->base.taux, taux, nb, cudaMemcpyHostToDevice, m->stream));
-  if (tauy) CUDA_TRY(cudaMemcpyAsync(m->base.tauy, tauy, nb, cudaMemcpyHostToDevice, m->stream));
-  if (ppv) CUDA_TRY(cudaMemcpyAsync(m->base.ppv, ppv, nb, cudaMemcpyHostToDevice, m->stream));
-  if (rqv) CUDA_TRY(cudaMemcpyAsync(m->base.rqv, rqv, nb, cudaMemcpyHostToDevice, m->stream));
+  const float *src[4] = {taux, tauy, ppv, rqv};
+  float *dst[4] = {m->base.taux, m->base.tauy, m->base.ppv, m->base.rqv};
+  const int g = m->fgen;
+  m->fgen ^= 1;
+  for (int a = 0; a < 4; a++)
+    if (src[a] && !m->fstage[g][a]) {
+      CUDA_TRY(cudaMalloc(&m->fstage[g][a], nb));
+      m->fstage_bytes += nb;
+    }
+  // the generation's last contents have been copied into place
+  if (m->fused_rec[g]) CUDA_TRY(cudaStreamWaitEvent(m->xin, m->ev_fused[g], 0));
+  for (int a = 0; a < 4; a++)
+    if (src[a]) CUDA_TRY(cudaMemcpyAsync(m->fstage[g][a], src[a], nb, cudaMemcpyHostToDevice, m->xin));
+  CUDA_TRY(cudaEventRecord(m->ev_fin[g], m->xin));
+  CUDA_TRY(cudaStreamWaitEvent(m->stream, m->ev_fin[g], 0));
+  for (int a = 0; a < 4; a++)
+    if (src[a]) CUDA_TRY(cudaMemcpyAsync(dst[a], m->fstage[g][a], nb, cudaMemcpyDeviceToDevice, m->stream));
+  CUDA_TRY(cudaEventRecord(m->ev_fused[g], m->stream));
+  m->fused_rec[g] = true;
   return SHY_OK;
 }
 
+// The level after the steps enqueued so far, copied on the transfer stream
+// once they are done; the next step runs meanwhile (it writes the other
+// level buffer) and the one after it waits for the copy.
 extern "C" int shygpu_get_levels(shygpu_model *m, float *znv) {
   if (!m || !znv) return fail(SHY_EARG, "get_levels: bad arguments");
   if (!m->state_set) return fail(SHY_ESTATE, "get_levels: set_state has not been called");
-  CUDA_TRY(cudaMemcpyAsync(znv, m->zbuf[m->cur], (size_t)m->NKN * 4, cudaMemcpyDeviceToHost, m->stream));
+  ST_TRY(xfer_setup(m));
+  const int c = m->cur;
+  CUDA_TRY(cudaEventRecord(m->ev_done, m->stream));
+  CUDA_TRY(cudaStreamWaitEvent(m->xout, m->ev_done, 0));
+  CUDA_TRY(cudaMemcpyAsync(znv, m->zbuf[c], (size_t)m->NKN * 4, cudaMemcpyDeviceToHost, m->xout));
+  CUDA_TRY(cudaEventRecord(m->ev_lev[c], m->xout));
+  m->lev_pending[c] = true;
   return SHY_OK;
 }
 

@@ -26,8 +26,12 @@ namespace shy {
 // memory in coalesced passes of the whole warp, as k_final_w does; each
 // thread then reads and writes its own column in shared memory.  Without
 // it each load of layer l touches 32 sectors, one per column.
-template <int L, bool COR, bool ADV, bool W = false>
-__global__ void __launch_bounds__(128, W ? 4 : 3) k_column_t(Dev d) {
+//
+// XT: the instance with the explicit terms that only some basins use
+// (horizontal viscosity, baroclinic pressure, the old non-hydrostatic
+// pressure); without them the plain barotropic column keeps fewer registers.
+template <int L, bool COR, bool ADV, bool W = false, bool XT = true>
+__global__ void __launch_bounds__(128, W ? (XT ? 4 : 5) : 3) k_column_t(Dev d) {
   static_assert(!(W && COR), "the staged form has no Coriolis instance");
   __shared__ float sbuf[W ? 4 : 1][W ? 3 : 1][W ? 32 * L : 1];
   const int e0 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -100,8 +104,8 @@ __global__ void __launch_bounds__(128, W ? 4 : 3) k_column_t(Dev d) {
 #define COL_V(i) (W ? ((i) < ilevel ? bV[ol + (i)] : 0.f) : v[W ? 0 : (i)])
   const int I = NLV + 1;
   const float aux = (float)dt * P.at;
-  const bool explicit_visc = P.ahpar > 0.f;
-  const bool barocl = P.ibarcl > 0 && P.ibarcl != 3 && P.ibarcl != 5;
+  const bool explicit_visc = XT && P.ahpar > 0.f;
+  const bool barocl = XT && P.ibarcl > 0 && P.ibarcl != 3 && P.ibarcl != 5;
   const float area = 12.f * (float)aj;
   const float *hld = d.hldv + (size_t)en.w * NLV;
   const float raux = P.grav / P.rowass;
@@ -253,7 +257,7 @@ __global__ void __launch_bounds__(128, W ? 4 : 3) k_column_t(Dev d) {
       fx += raux * hlayer * pxs;
       fy += raux * hlayer * pys;
     }
-    if (P.inohyd) {
+    if (XT && P.inohyd) {
       // nonhydro_set_explicit (nohydro.f90:526-586): the old pressure's
       // gradient times the old thickness, weight 1 - aqpar
       float qx = 0.f, qy = 0.f;

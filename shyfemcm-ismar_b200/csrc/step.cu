@@ -69,8 +69,10 @@ static void launch_column_t(const Dev &d, cudaStream_t st, bool cor) {
     else if (d.col_staged) k_column_t<L, false, true, true><<<blocks, 128, 0, st>>>(d);
     else k_column_t<L, false, true><<<blocks, 128, 0, st>>>(d);
   } else if (cor) k_column_t<L, true, false><<<blocks, 128, 0, st>>>(d);
-  else if (d.col_staged) k_column_t<L, false, false, true><<<blocks, 128, 0, st>>>(d);
-  else k_column_t<L, false, false><<<blocks, 128, 0, st>>>(d);
+  else if (d.col_staged) {
+    if (d.any_xt) k_column_t<L, false, false, true><<<blocks, 128, 0, st>>>(d);
+    else k_column_t<L, false, false, true, false><<<blocks, 128, 0, st>>>(d);
+  } else k_column_t<L, false, false><<<blocks, 128, 0, st>>>(d);
 }
 
 void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool cor) {

@@ -349,36 +349,60 @@ def test_hybrid_sigma_z_layers(column_threads):
     assert abs(g.info(0).volume - o.info().volume) <= 1e-6 * o.info().volume
 
 
-def test_whole_model_transfers():
+@pytest.mark.parametrize("pinned", [False, True])
+def test_whole_model_transfers(pinned):
     """shygpu_set_forcing_all / shygpu_enqueue / shygpu_get_levels (one copy
-    for all basins, nothing waited for until shygpu_sync) give the bits of
-    the per-basin calls with a wait after each."""
-    import ctypes as C
+    for all basins on the transfer streams, nothing waited for until
+    shygpu_sync) give, step for step, the bits of the per-basin calls with a
+    wait after each; with pinned host buffers the copies overlap the steps."""
     cs = [cases.basin3d_case(nkn_target=n, nlv=6, seed=s, baroclinic=False, ts=False)
           for n, s in ((700, 21), (1200, 22))]
     rng = np.random.default_rng(3)
-    winds = [[rng.normal(0, 1e-4, c["nkn"]).astype(np.float32) for c in cs] for _ in range(6)]
+    winds = [[rng.normal(0, 1e-4, c["nkn"]).astype(np.float32) for c in cs] for _ in range(8)]
     a = shygpu.Model(cs)
     a.set_state_all()
+    refs = []
     for w in winds:
         for b in range(len(cs)):
             a.set_forcing(b, tauxnv=w[b], tauynv=-w[b])
         a.run(1)
-    ref = np.concatenate([a.get_state(b)["znv"] for b in range(len(cs))])
+        refs.append(np.concatenate([a.get_state(b)["znv"] for b in range(len(cs))]))
     g = shygpu.Model(cs)
     g.set_state_all()
     lib = shygpu.lib()
-    out = np.zeros(sum(c["nkn"] for c in cs), np.float32)
+    n = sum(c["nkn"] for c in cs)
+    if pinned:
+        import torch
+        host = lambda a_: torch.from_numpy(np.ascontiguousarray(a_)).pin_memory()
+        outs = [torch.zeros(n, dtype=torch.float32).pin_memory() for _ in winds]
+        ptr = lambda t: t.data_ptr()
+        get = lambda t: t.numpy()
+    else:
+        host = np.ascontiguousarray
+        outs = [np.zeros(n, np.float32) for _ in winds]
+        ptr = lambda t: t.ctypes.data
+        get = lambda t: t
     keep = []
-    for w in winds:
-        tx = np.concatenate(w)
-        ty = -tx
+    for w, out in zip(winds, outs):
+        tx = host(np.concatenate(w))
+        ty = host(-np.concatenate(w))
         keep += [tx, ty]
-        shygpu.check(lib.shygpu_set_forcing_all(g.h, tx.ctypes.data, ty.ctypes.data, None, None), "forcing")
+        shygpu.check(lib.shygpu_set_forcing_all(g.h, ptr(tx), ptr(ty), None, None), "forcing")
         shygpu.check(lib.shygpu_enqueue(g.h, 1), "enqueue")
-        shygpu.check(lib.shygpu_get_levels(g.h, out.ctypes.data), "levels")
+        shygpu.check(lib.shygpu_get_levels(g.h, ptr(out)), "levels")
     shygpu.check(lib.shygpu_sync(g.h), "sync")
-    assert np.array_equal(out, ref)
+    for out, ref in zip(outs, refs):
+        assert np.array_equal(get(out), ref)
+    # a state set afterwards and a checkpoint restored over pending copies
+    # order with them
+    ck = g.checkpoint()
+    shygpu.check(lib.shygpu_enqueue(g.h, 1), "enqueue")
+    shygpu.check(lib.shygpu_get_levels(g.h, ptr(outs[0])), "levels")
+    g.restore(ck)
+    shygpu.check(lib.shygpu_sync(g.h), "sync")
+    assert np.array_equal(np.concatenate([g.get_state(b)["znv"] for b in range(len(cs))]), refs[-1])
+    assert g.nbytes() > 0
+    g.close()
 
 
 def far_end_nodes(c, n=3):
