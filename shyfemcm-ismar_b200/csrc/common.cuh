@@ -101,6 +101,7 @@ struct Dev {
   int node_prefetch;            // thread-per-column node kernel: 1 each element's layers loaded
                                 // at once, 0 layer by layer
   int any_wd;                   // some basin has wetting and drying (thread-per-column forms)
+  int any_zad;                  // some basin has z-adaptive layers (nzadapt > 1)
   int any_xt;                   // some basin has horizontal viscosity, baroclinic or
                                 // non-hydrostatic pressure (the column kernel's instance with them)
   float2 *mom;                  // (NKN*NLV) node momentum {momentxv, momentyv} when a basin advects

@@ -1226,6 +1226,8 @@ extern "C" int shygpu_create(int32_t nbasin, const shy_basin *B, const shy_param
   d.any_tvd = m->any_tvd ? 1 : 0;
   d.any_tvdv = 0;
   for (int b = 0; b < nbasin; b++) d.any_tvdv |= Pp[b].itvdv == 1 ? 1 : 0;
+  d.any_zad = 0;
+  for (int b = 0; b < nbasin; b++) d.any_zad |= m->par[b].nzadapt > 1 ? 1 : 0;
   d.any_xt = 0;
   for (int b = 0; b < nbasin; b++) {
     const BasinPar &q = m->par[b];

@@ -119,8 +119,12 @@ __global__ void __launch_bounds__(256) k_node(Dev d, const int *kbas, int init_o
 // incident elements are walked once, each adding to the FP64 sums of all
 // its layers (in element order, as k_node); then the node's layers in turn
 // ===========================================================================
-template <int L, bool PF = false>
-__global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int init_only) {
+//
+// ZA: the instance with z-adaptive layers; without them (every basin with
+// nzadapt <= 1) the thickness of a layer is a sum of nominal values and
+// the level, and the kernel keeps fewer registers.
+template <int L, bool PF = false, bool ZA = true>
+__global__ void __launch_bounds__(128, ZA ? 6 : 8) k_node_t(Dev d, const int *kbas, int init_only) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= d.NKN) return;
   const int NLV = d.NLV, I = NLV + 1;
@@ -153,7 +157,7 @@ __global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int i
     // setdepth takes the element's vertex level (a dry element's differs)
     const float ze = P.wetdry ? d.zen[3 * e + ii] : (float)z;
     double us = 0., vs = 0.;                  // the element's transports summed over its layers
-    const int lev = P.nzadapt > 1 ? zad_levmax((double)ze, hlv, le, P.rzmov) : 0;
+    const int lev = ZA && P.nzadapt > 1 ? zad_levmax((double)ze, hlv, le, P.rzmov) : 0;
     // PF: the element's transports of every layer loaded at once (the
     // layers below its bottom hold zeros), so their loads are in flight
     // together; else each layer's as the loop reaches it
@@ -170,7 +174,7 @@ __global__ void __launch_bounds__(128, 6) k_node_t(Dev d, const int *kbas, int i
     for (int l = 0; l < L; l++) {
       if (l >= le) break;
       float hl;
-      if (P.nzadapt > 1) hl = (float)zad_vertex_h(l, (double)ze, (double)htot, le, lev, hlv, hld);
+      if (ZA && P.nzadapt > 1) hl = (float)zad_vertex_h(l, (double)ze, (double)htot, le, lev, hlv, hld);
       else if (le == 1) hl = htot + ze;
       else if (l < le - 1) hl = hld[l] + (l == 0 ? ze : 0.f);
       else hl = hbot;

@@ -27,9 +27,15 @@ void launch_node(const Dev &d, const int *kbas, int which, int a, int b, cudaStr
       else if (d.NLV <= 12) k_node_t<12, true><<<blocks, 128, 0, st>>>(d, kbas, a);
       else k_node_t<16, true><<<blocks, 128, 0, st>>>(d, kbas, a);
     } else {
-      if (d.NLV <= 8) k_node_t<8><<<blocks, 128, 0, st>>>(d, kbas, a);
-      else if (d.NLV <= 12) k_node_t<12><<<blocks, 128, 0, st>>>(d, kbas, a);
-      else k_node_t<16><<<blocks, 128, 0, st>>>(d, kbas, a);
+      if (d.any_zad) {
+        if (d.NLV <= 8) k_node_t<8><<<blocks, 128, 0, st>>>(d, kbas, a);
+        else if (d.NLV <= 12) k_node_t<12><<<blocks, 128, 0, st>>>(d, kbas, a);
+        else k_node_t<16><<<blocks, 128, 0, st>>>(d, kbas, a);
+      } else {
+        if (d.NLV <= 8) k_node_t<8, false, false><<<blocks, 128, 0, st>>>(d, kbas, a);
+        else if (d.NLV <= 12) k_node_t<12, false, false><<<blocks, 128, 0, st>>>(d, kbas, a);
+        else k_node_t<16, false, false><<<blocks, 128, 0, st>>>(d, kbas, a);
+      }
     }
     return;
   }
