@@ -17,10 +17,13 @@ against the FP64 oracle.  The timed model's launch shapes are chosen first
 by the library's autotuner (shygpu_autotune) on the same basins.
 
 `--workload basin3d` times the 3D baroclinic basin instead (~20k nodes, 20
-z-layers, temperature and salinity transported, dt = 120 s).
+z-layers, temperature and salinity transported, dt = 120 s); `--workload
+lagoon` the 250k-node lagoon on 30 sigma layers with three tracers (dt =
+30 s); `--workload serve` a Poisson stream of forecast requests through the
+serving loop (latency p50/p99).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl shygpu|reference]
-                  [--workload ensemble|basin3d]
+                  [--workload ensemble|basin3d|lagoon|serve]
 
 N > 1 runs one process per GPU, each advancing its own replica (replicas
 only: the step has no exchange between basins), value = all ranks' units /
@@ -60,10 +63,14 @@ def parse():
                    help="serve workload: requests of the Poisson stream (20/min)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-plain", action="store_true")
-    p.add_argument("--check-steps", type=int, default=60,
-                   help="steps of the accuracy check against the oracle (0: none)")
+    p.add_argument("--check-steps", type=int, default=None,
+                   help="steps of the accuracy check against the oracle (0: none; default 60, on the lagoon 8, "
+                        "where an oracle step of its 250k nodes and 30 layers takes about 12 s)")
     p.add_argument("--no-tune", action="store_true", help="keep the default launch plan (no shygpu_autotune)")
-    return p.parse_args()
+    a = p.parse_args()
+    if a.check_steps is None:
+        a.check_steps = 8 if a.workload == "lagoon" else 60
+    return a
 
 
 def make_cases(workload, rank=0, first=None):
