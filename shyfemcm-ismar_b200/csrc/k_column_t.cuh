@@ -31,7 +31,7 @@ namespace shy {
 // (horizontal viscosity, baroclinic pressure, the old non-hydrostatic
 // pressure); without them the plain barotropic column keeps fewer registers.
 template <int L, bool COR, bool ADV, bool W = false, bool XT = true>
-__global__ void __launch_bounds__(128, W ? (XT ? 4 : 5) : 3) k_column_t(Dev d) {
+__global__ void __launch_bounds__(128, W ? (XT ? 4 : 6) : 3) k_column_t(Dev d) {
   static_assert(!(W && COR), "the staged form has no Coriolis instance");
   __shared__ float sbuf[W ? 4 : 1][W ? 3 : 1][W ? 32 * L : 1];
   const int e0 = blockIdx.x * blockDim.x + threadIdx.x;

@@ -198,8 +198,8 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
 // shared memory by the whole warp in coalesced passes; each thread then
 // works its own column in shared memory as k_final_t does.
 // ===========================================================================
-template <int L>
-__global__ void __launch_bounds__(128) k_final_w(Dev d, int init_only) {
+template <int L, bool ZA = true>
+__global__ void __launch_bounds__(128, ZA ? 1 : 6) k_final_w(Dev d, int init_only) {
   __shared__ float sb[4][5][32 * L];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w0 = (blockIdx.x * 4 + warp) * 32;         // first element of this warp
@@ -278,12 +278,12 @@ __global__ void __launch_bounds__(128) k_final_w(Dev d, int init_only) {
     const float *hlv = d.hlv + (size_t)en.w * NLV;
     bool bad = false;
     int lev[3] = {0, 0, 0};
-    if (P.nzadapt > 1)
+    if (ZA && P.nzadapt > 1)
       for (int ii = 0; ii < 3; ii++) lev[ii] = zad_levmax(zn3[ii], hlv, ilevel, P.rzmov);
     for (int l = 0; l < NLV; l++) {
       double h = 0.;
       if (l < ilevel) {
-        if (P.nzadapt > 1) h = zad_elem_h(l, zn3, hm, ilevel, lev, hlv, hld, zmed);   // z-adaptive surface layers
+        if (ZA && P.nzadapt > 1) h = zad_elem_h(l, zn3, hm, ilevel, lev, hlv, hld, zmed);   // z-adaptive surface layers
         else if (l < P.nsigma) h = -(fmin((double)hm.w, (double)P.hsigma) + zmed) * (double)hld[l];   // sigma layers (:1079-1083)
         else if (ilevel == 1) h = hm.w + zmed;
         else if (l < ilevel - 1) h = (double)hld[l] + (l == 0 ? zmed : 0.);

@@ -89,9 +89,15 @@ void launch_elem(const Dev &d, int which, int init_only, cudaStream_t st, bool c
       else k_final_t<false><<<(d.NEL + 255) / 256, 256, 0, st>>>(d, init_only);
     } else {
       const int blocks = (d.NEL + 127) / 128;            // 4 warps of 32 elements
-      if (d.NLV <= 8) k_final_w<8><<<blocks, 128, 0, st>>>(d, init_only);
-      else if (d.NLV <= 12) k_final_w<12><<<blocks, 128, 0, st>>>(d, init_only);
-      else k_final_w<16><<<blocks, 128, 0, st>>>(d, init_only);
+      if (d.any_zad) {
+        if (d.NLV <= 8) k_final_w<8><<<blocks, 128, 0, st>>>(d, init_only);
+        else if (d.NLV <= 12) k_final_w<12><<<blocks, 128, 0, st>>>(d, init_only);
+        else k_final_w<16><<<blocks, 128, 0, st>>>(d, init_only);
+      } else {
+        if (d.NLV <= 8) k_final_w<8, false><<<blocks, 128, 0, st>>>(d, init_only);
+        else if (d.NLV <= 12) k_final_w<12, false><<<blocks, 128, 0, st>>>(d, init_only);
+        else k_final_w<16, false><<<blocks, 128, 0, st>>>(d, init_only);
+      }
     }
     return;
   }
