@@ -29,7 +29,9 @@ namespace shy {
 //
 // XT: the instance with the explicit terms that only some basins use
 // (horizontal viscosity, baroclinic pressure, the old non-hydrostatic
-// pressure); without them the plain barotropic column keeps fewer registers.
+// pressure); without them the plain barotropic column keeps fewer registers
+// and runs six CTAs per SM (measured faster than five, where it has no
+// spills, on the 10-layer ensemble).
 template <int L, bool COR, bool ADV, bool W = false, bool XT = true>
 __global__ void __launch_bounds__(128, W ? (XT ? 4 : 6) : 3) k_column_t(Dev d) {
   static_assert(!(W && COR), "the staged form has no Coriolis instance");

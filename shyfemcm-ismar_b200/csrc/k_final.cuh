@@ -196,7 +196,10 @@ __global__ void __launch_bounds__(256) k_final_t(Dev d, int init_only) {
 // 32 element columns (one contiguous run of 32*NLV values, since a column
 // is contiguous and the elements are consecutive) moved between global and
 // shared memory by the whole warp in coalesced passes; each thread then
-// works its own column in shared memory as k_final_t does.
+// works its own column in shared memory as k_final_t does.  ZA: the
+// instance with z-adaptive layers; without them (every basin with
+// nzadapt <= 1) the element thickness needs no FP64 adaptive-layer terms
+// and the kernel keeps 80 registers, six CTAs per SM.
 // ===========================================================================
 template <int L, bool ZA = true>
 __global__ void __launch_bounds__(128, ZA ? 1 : 6) k_final_w(Dev d, int init_only) {
